@@ -1,0 +1,121 @@
+"""ctypes mirror of include/ftb200.h (the C ABI of the forward light tracer).
+
+The structures here must stay byte-identical to the header; tests/test_abi.py checks the
+sizes and field offsets against the compiled library.
+"""
+import ctypes as C
+
+FTB_OK = 0
+STATUS_NAMES = {
+    0: "FTB_OK", 1: "FTB_ERR_INVALID", 2: "FTB_ERR_NO_DEVICE", 3: "FTB_ERR_UNSUPPORTED",
+    4: "FTB_ERR_CUDA", 5: "FTB_ERR_OOM", 6: "FTB_ERR_DEVICE_LIMIT", 7: "FTB_ERR_TOO_LARGE",
+}
+
+SPEC_CONST, SPEC_TABLE, SPEC_CAUCHY, SPEC_SELLMEIER, SPEC_BLACKBODY = 0, 1, 2, 3, 4
+
+MAT_DIFFUSE = 0
+MAT_DIELECTRIC = 1
+MAT_MIRROR = 2
+MAT_HALF_MIRROR = 3
+MAT_GLOSSY = 4
+MAT_DIFFUSE_TRANSMIT = 11
+MAT_FILTER = 12
+
+EMIT_QUAD, EMIT_SPHERE = 0, 1
+BOUND_NONE, BOUND_BOX, BOUND_SPHERE = 0, 1, 2
+PRIORITY_UNSET = -(2 ** 31)
+
+FATE_ABSORBED, FATE_ESCAPED, FATE_RESIDUAL, FATE_SENSOR, FATE_DROPPED = 0, 1, 2, 3, 4
+
+D3 = C.c_double * 3
+
+
+class Spectrum(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n", C.c_int32), ("offset", C.c_int64),
+                ("p", C.c_double * 6)]
+
+
+class Material(C.Structure):
+    _fields_ = [("type", C.c_int32), ("priority", C.c_int32), ("reflect", C.c_int32),
+                ("ior", C.c_int32), ("absorb", C.c_int32), ("transmit", C.c_int32),
+                ("roughness", C.c_double)]
+
+
+class Emitter(C.Structure):
+    _fields_ = [("shape", C.c_int32), ("collimated", C.c_int32), ("cdf_n", C.c_int32),
+                ("spd", C.c_int32), ("cdf_offset", C.c_int64), ("step", C.c_double),
+                ("power", C.c_double), ("origin", D3), ("u", D3), ("v", D3),
+                ("normal", D3), ("area", C.c_double), ("radius", C.c_double),
+                ("beam", D3)]
+
+
+class Medium(C.Structure):
+    _fields_ = [("sigma_a", C.c_int32), ("sigma_s", C.c_int32), ("bound", C.c_int32),
+                ("pad0", C.c_int32), ("g", C.c_double), ("bmin", D3), ("bmax", D3),
+                ("center", D3), ("radius", C.c_double)]
+
+
+_PD = C.POINTER(C.c_double)
+_PI32 = C.POINTER(C.c_int32)
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("n_tris", C.c_int64), ("tri_v", _PD), ("tri_n", _PD), ("tri_mat", _PI32),
+                ("n_spheres", C.c_int64), ("sph", _PD), ("sph_mat", _PI32),
+                ("n_curves", C.c_int64), ("curve", _PD), ("curve_mat", _PI32),
+                ("n_mats", C.c_int32), ("n_spectra", C.c_int32),
+                ("mats", C.POINTER(Material)), ("spectra", C.POINTER(Spectrum)),
+                ("n_table", C.c_int64), ("table_w", _PD), ("table_v", _PD),
+                ("n_emitters", C.c_int32), ("n_media", C.c_int32),
+                ("emitters", C.POINTER(Emitter)), ("emitter_cdf", _PD),
+                ("media", C.POINTER(Medium))]
+
+
+class Camera(C.Structure):
+    _fields_ = [("eye", D3), ("u", D3), ("v", D3), ("w", D3), ("tan_half_x", C.c_double),
+                ("tan_half_y", C.c_double), ("res_x", C.c_int32), ("res_y", C.c_int32)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("n_photons", C.c_int64), ("seed_base", C.c_uint64),
+                ("max_bounce", C.c_int32), ("frac_bits", C.c_int32)]
+
+
+class Energy(C.Structure):
+    _fields_ = [("emitted", C.c_double), ("absorbed", C.c_double), ("sensor", C.c_double),
+                ("escaped", C.c_double), ("residual", C.c_double), ("fx", C.c_int64 * 5)]
+
+    def as_list(self):
+        return [self.emitted, self.absorbed, self.sensor, self.escaped, self.residual]
+
+
+class FilmInfo(C.Structure):
+    _fields_ = [("frac_bits", C.c_int32), ("pad0", C.c_int32), ("scale", C.c_double),
+                ("power_ref", C.c_double)]
+
+
+class Footprint(C.Structure):
+    _fields_ = [("scene_bytes", C.c_uint64), ("film_bytes", C.c_uint64),
+                ("wave_bytes", C.c_uint64), ("total_bytes", C.c_uint64)]
+
+
+class PhotonLog(C.Structure):
+    _fields_ = [("n_hits", C.c_int32), ("fate", C.c_int32), ("prim_hash", C.c_uint64),
+                ("beta", C.c_double), ("prims", C.c_int32 * 8)]
+
+
+STRUCTS = {
+    "ftb_spectrum": Spectrum, "ftb_material": Material, "ftb_emitter": Emitter,
+    "ftb_medium": Medium, "ftb_scene_desc": SceneDesc, "ftb_camera": Camera,
+    "ftb_render_params": RenderParams, "ftb_energy": Energy, "ftb_film_info": FilmInfo,
+    "ftb_footprint": Footprint, "ftb_photon_log": PhotonLog,
+}
+
+# every entry point declared in include/ftb200.h
+EXPORTS = [
+    "ftb_last_error", "ftb_abi_version", "ftb_available", "ftb_device_name", "ftb_mem_info",
+    "ftb_forward_supported", "ftb_camera_look_at", "ftb_emission_cdf", "ftb_scene_create",
+    "ftb_scene_destroy", "ftb_scene_footprint", "ftb_scene_power", "ftb_render_forward",
+    "ftb_render_forward_device", "ftb_session_begin", "ftb_session_batch",
+    "ftb_session_hits0", "ftb_session_download", "ftb_session_end", "ftb_trace_log",
+]

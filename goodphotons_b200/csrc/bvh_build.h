@@ -1,0 +1,37 @@
+// bvh_build.h -- host builder of the compressed 8-wide BVH.
+#pragma once
+#include <cfloat>
+#include <string>
+#include <vector>
+
+#include "ftb_layout.h"
+
+namespace ftb {
+
+struct Box {
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
+    double hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    void grow(const Box& b) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = b.lo[a] < lo[a] ? b.lo[a] : lo[a];
+            hi[a] = b.hi[a] > hi[a] ? b.hi[a] : hi[a];
+        }
+    }
+    void grow_point(const double* p) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = p[a] < lo[a] ? p[a] : lo[a];
+            hi[a] = p[a] > hi[a] ? p[a] : hi[a];
+        }
+    }
+};
+
+struct WideBvh {
+    std::vector<WNode> nodes;   // root at 0
+    std::vector<int> order;     // record i holds primitive order[i]
+};
+
+// Build over primitive boxes grown by `margin` (absolute, in scene units).
+bool build_wide_bvh(const std::vector<Box>& boxes, double margin, WideBvh& out,
+                    std::string& err);
+
+}  // namespace ftb

@@ -1,0 +1,777 @@
+// ftb_api.cpp -- host side of the C ABI declared in include/ftb200.h.
+//
+// Replaces the host half of the reference's forward GPU path: the scene bake
+// (buildUploadScene, render_cuda.cu:12692-13546), the launch (launchForward /
+// renderForwardCuda, render_cuda.cu:13683-13756) and the resident sessions
+// (render_cuda.cu:13763-13871).  Every failure is reported through a status code and
+// ftb_last_error(); nothing exits the process.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ftb200.h"
+#include "bvh_build.h"
+#include "ftb_kernels.h"
+#include "ftb_layout.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+ftb_status fail(ftb_status s, const std::string& m) {
+    g_err = m;
+    return s;
+}
+ftb_status cuda_fail(cudaError_t e, const char* what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? FTB_ERR_OOM : FTB_ERR_CUDA;
+}
+#define CK(call, what)                                  \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+constexpr double kLambdaMin = 360.0, kLambdaMax = 830.0;
+constexpr double kPi = 3.141592653589793;
+
+// ---- host restatements used at bake time ---------------------------------------------
+double blackbody_radiance(double kelvin, double lambda_nm) {   // spectrum.h:185-190
+    const double h = 6.62607015e-34, c = 2.99792458e8, kb = 1.380649e-23;
+    double l = lambda_nm * 1e-9;
+    double e = std::exp((h * c) / (l * kb * kelvin)) - 1.0;
+    return (2.0 * h * c * c) / (std::pow(l, 5.0) * e);
+}
+
+bool spec_valid(const ftb_scene_desc* d, int idx, std::string& why) {
+    if (idx < 0 || idx >= d->n_spectra || !d->spectra) { why = "spectrum index out of range"; return false; }
+    const ftb_spectrum& s = d->spectra[idx];
+    if (s.kind < FTB_SPEC_CONST || s.kind > FTB_SPEC_BLACKBODY) { why = "unknown spectrum kind"; return false; }
+    if (s.kind == FTB_SPEC_TABLE) {
+        if (s.n <= 0 || s.offset < 0 || s.offset + s.n > d->n_table || !d->table_w || !d->table_v) {
+            why = "table spectrum out of range"; return false;
+        }
+        for (int i = 1; i < s.n; ++i)
+            if (!(d->table_w[s.offset + i] > d->table_w[s.offset + i - 1])) {
+                why = "table spectrum wavelengths must be strictly increasing"; return false;
+            }
+    }
+    return true;
+}
+
+double spec_eval_host(const ftb_scene_desc* d, int idx, double w) {
+    const ftb_spectrum& s = d->spectra[idx];
+    switch (s.kind) {
+    case FTB_SPEC_CONST: return s.p[0];
+    case FTB_SPEC_TABLE: {   // tabulatedSpectrum (spectrum.h:264-281)
+        const double* x = d->table_w + s.offset;
+        const double* y = d->table_v + s.offset;
+        int n = s.n;
+        if (w <= x[0]) return y[0];
+        if (w >= x[n - 1]) return y[n - 1];
+        size_t lo = 0, hi = (size_t)n - 1;
+        while (lo + 1 < hi) { size_t mid = (lo + hi) / 2; (x[mid] <= w ? lo : hi) = mid; }
+        double w0 = x[lo], w1 = x[lo + 1], v0 = y[lo], v1 = y[lo + 1];
+        double f = (w1 > w0) ? (w - w0) / (w1 - w0) : 0.0;
+        return v0 + (v1 - v0) * f;
+    }
+    case FTB_SPEC_CAUCHY: { double um = w * 1e-3; return s.p[0] + s.p[1] / (um * um); }
+    case FTB_SPEC_SELLMEIER: {
+        double l2 = (w * 1e-3) * (w * 1e-3);
+        double n2 = 1.0 + s.p[0] * l2 / (l2 - s.p[3]) + s.p[1] * l2 / (l2 - s.p[4]) + s.p[2] * l2 / (l2 - s.p[5]);
+        return std::sqrt(n2 > 1.0 ? n2 : 1.0);
+    }
+    case FTB_SPEC_BLACKBODY: return blackbody_radiance(s.p[0], w) * s.p[1];
+    }
+    return 0.0;
+}
+
+struct V { double x, y, z; };
+V vsub(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+V vcross(V a, V b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+double vdot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+V vnorm(V a) { double l = std::sqrt(vdot(a, a)); return {a.x / l, a.y / l, a.z / l}; }
+
+}  // namespace
+
+// ---- scene object ----------------------------------------------------------------------
+struct ftb_scene {
+    int device = 0;
+    int sms = 148;
+    DevScene dev{};
+    std::vector<void*> allocs;
+    double power = 0.0;
+    uint64_t scene_bytes = 0;
+    std::mutex mu;   // one render at a time per scene
+    // cached render resources
+    cudaStream_t streams[2] = {nullptr, nullptr};
+    ftb::Wave waves[2]{};
+    int32_t wave_W = 0;
+    bool wave_log = false;
+    int64_t* film = nullptr;
+    size_t film_words = 0;
+    unsigned long long* tally = nullptr;
+    int32_t* status = nullptr;
+    ~ftb_scene() {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(device);
+        for (auto& w : waves) ftb::wave_free(w);
+        for (auto s : streams) if (s) cudaStreamDestroy(s);
+        if (film) cudaFree(film);
+        if (tally) cudaFree(tally);
+        if (status) cudaFree(status);
+        for (void* p : allocs) cudaFree(p);
+        cudaSetDevice(cur);
+    }
+};
+
+struct ftb_session {
+    ftb_scene* scene = nullptr;
+    std::vector<ftb_camera> cams;
+    std::vector<int64_t*> films;
+    unsigned long long* tally = nullptr;
+    int32_t max_bounce = 32;
+    int32_t frac_bits = 0;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = 0;
+    explicit DeviceGuard(int dev) { cudaGetDevice(&prev); cudaSetDevice(dev); }
+    ~DeviceGuard() { cudaSetDevice(prev); }
+};
+
+template <class T>
+ftb_status upload(ftb_scene* s, const T* host, size_t n, const T** out, const char* what) {
+    if (n == 0) { *out = nullptr; return FTB_OK; }
+    void* p = nullptr;
+    CK(cudaMalloc(&p, n * sizeof(T)), what);
+    s->allocs.push_back(p);
+    s->scene_bytes += n * sizeof(T);
+    CK(cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice), what);
+    *out = (const T*)p;
+    return FTB_OK;
+}
+
+bool mat_type_supported(int t) {
+    return t == FTB_MAT_DIFFUSE || t == FTB_MAT_DIELECTRIC || t == FTB_MAT_GLOSSY ||
+           t == FTB_MAT_DIFFUSE_TRANSMIT || t == FTB_MAT_FILTER;
+}
+
+// Validation shared by ftb_forward_supported and ftb_scene_create.  Returns FTB_OK,
+// FTB_ERR_INVALID (malformed) or FTB_ERR_UNSUPPORTED.
+ftb_status check_desc(const ftb_scene_desc* d) {
+    if (!d) return fail(FTB_ERR_INVALID, "null scene descriptor");
+    if (d->n_tris < 0 || d->n_spheres < 0 || d->n_curves < 0 || d->n_mats < 0 || d->n_spectra < 0 ||
+        d->n_emitters < 0 || d->n_media < 0 || d->n_table < 0)
+        return fail(FTB_ERR_INVALID, "negative count in scene descriptor");
+    if ((d->n_tris && (!d->tri_v || !d->tri_mat)) || (d->n_spheres && (!d->sph || !d->sph_mat)) ||
+        (d->n_curves && (!d->curve || !d->curve_mat)) || (d->n_mats && !d->mats) ||
+        (d->n_emitters && (!d->emitters || !d->emitter_cdf)) || (d->n_media && !d->media))
+        return fail(FTB_ERR_INVALID, "null array for a nonzero count");
+    int64_t np = d->n_tris + d->n_spheres + d->n_curves;
+    if (np > (int64_t)INT32_MAX / 2) return fail(FTB_ERR_TOO_LARGE, "too many primitives (max 2^30)");
+    std::string why;
+    for (int i = 0; i < d->n_spectra; ++i)
+        if (!spec_valid(d, i, why)) return fail(FTB_ERR_INVALID, "spectrum " + std::to_string(i) + ": " + why);
+    auto chk_slot = [&](int s) { return s >= -1 && s < d->n_spectra; };
+    for (int i = 0; i < d->n_mats; ++i) {
+        const ftb_material& m = d->mats[i];
+        if (!chk_slot(m.reflect) || !chk_slot(m.ior) || !chk_slot(m.absorb) || !chk_slot(m.transmit))
+            return fail(FTB_ERR_INVALID, "material " + std::to_string(i) + ": spectrum index out of range");
+        if (!mat_type_supported(m.type))
+            return fail(FTB_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": type " + std::to_string(m.type) +
+                        " is not on this path (mirror / half-mirror need the specular camera connectors)");
+        if (m.type == FTB_MAT_GLOSSY && !(m.roughness > 0.0))
+            return fail(FTB_ERR_UNSUPPORTED, "material " + std::to_string(i) +
+                        ": glossy with roughness <= 0 is a planar mirror (specular connector)");
+    }
+    for (int64_t i = 0; i < d->n_tris; ++i)
+        if (d->tri_mat[i] < 0 || d->tri_mat[i] >= d->n_mats) return fail(FTB_ERR_INVALID, "triangle material out of range");
+    for (int64_t i = 0; i < d->n_spheres; ++i) {
+        if (d->sph_mat[i] < 0 || d->sph_mat[i] >= d->n_mats) return fail(FTB_ERR_INVALID, "sphere material out of range");
+        if (d->mats[d->sph_mat[i]].type == FTB_MAT_DIELECTRIC)
+            return fail(FTB_ERR_UNSUPPORTED, "dielectric sphere: the reference splats it through its analytic "
+                        "sphere connector, which is not on this path");
+    }
+    for (int64_t i = 0; i < d->n_curves; ++i)
+        if (d->curve_mat[i] < 0 || d->curve_mat[i] >= d->n_mats) return fail(FTB_ERR_INVALID, "curve material out of range");
+    for (int i = 0; i < d->n_emitters; ++i) {
+        const ftb_emitter& e = d->emitters[i];
+        if (e.shape != FTB_EMIT_QUAD && e.shape != FTB_EMIT_SPHERE)
+            return fail(FTB_ERR_UNSUPPORTED, "emitter shape not supported (quad and sphere only)");
+        if (e.cdf_n < 1 || e.cdf_offset < 0 || !(e.step > 0.0))
+            return fail(FTB_ERR_INVALID, "emitter wavelength CDF malformed");
+    }
+    for (int i = 0; i < d->n_media; ++i) {
+        const ftb_medium& m = d->media[i];
+        if (m.sigma_a < 0 || m.sigma_a >= d->n_spectra || m.sigma_s < 0 || m.sigma_s >= d->n_spectra)
+            return fail(FTB_ERR_INVALID, "medium spectrum index out of range");
+        if (m.bound < FTB_BOUND_NONE || m.bound > FTB_BOUND_SPHERE) return fail(FTB_ERR_INVALID, "bad medium bound");
+    }
+    for (int i = 0; i < d->n_spectra; ++i) (void)i;
+    return FTB_OK;
+}
+
+int default_frac_bits(int64_t n) {
+    int lg = 0;
+    while (lg < 62 && ((int64_t)1 << lg) < n) ++lg;
+    int f = 62 - lg - 20;
+    return std::max(4, std::min(40, f));
+}
+
+DevCam dev_cam(const ftb_camera* c) {
+    DevCam d;
+    for (int i = 0; i < 3; ++i) { d.eye[i] = c->eye[i]; d.u[i] = c->u[i]; d.v[i] = c->v[i]; d.w[i] = c->w[i]; }
+    d.thx = c->tan_half_x; d.thy = c->tan_half_y; d.rx = c->res_x; d.ry = c->res_y;
+    return d;
+}
+
+ftb_status ensure_waves(ftb_scene* s, int32_t W, bool log) {
+    if (s->wave_W >= W && s->wave_log == log && s->waves[0].block) return FTB_OK;
+    for (auto& w : s->waves) ftb::wave_free(w);
+    s->wave_W = 0;
+    for (auto& w : s->waves) {
+        cudaError_t e = ftb::wave_alloc(w, W, log);
+        if (e != cudaSuccess) return cuda_fail(e, "wave allocation");
+    }
+    for (auto& st : s->streams)
+        if (!st) CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream create");
+    s->wave_W = W;
+    s->wave_log = log;
+    return FTB_OK;
+}
+
+ftb_status ensure_frame(ftb_scene* s, size_t words) {
+    if (!s->tally) CK(cudaMalloc(&s->tally, 8 * sizeof(unsigned long long)), "tally alloc");
+    if (!s->status) CK(cudaMalloc(&s->status, 64), "status alloc");
+    if (s->film_words < words) {
+        if (s->film) cudaFree(s->film);
+        s->film = nullptr;
+        s->film_words = 0;
+        CK(cudaMalloc(&s->film, words * sizeof(int64_t)), "film alloc");
+        s->film_words = words;
+    }
+    return FTB_OK;
+}
+
+int32_t pick_wave(int64_t n) {
+    int64_t W = std::min<int64_t>(n, (int64_t)1 << 22);
+    return (int32_t)std::max<int64_t>(W, 1);
+}
+
+// Trace n photons from seed_base into d_film / tally, on the scene's streams, and wait.
+ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t seed_base, int32_t max_bounce,
+                       int32_t frac_bits, int64_t* d_film, unsigned long long* d_tally, ftb_photon_log* d_logs,
+                       cudaStream_t user_stream) {
+    bool log = d_logs != nullptr;
+    int32_t W = pick_wave(n);
+    ftb_status st = ensure_waves(s, W, log);
+    if (st != FTB_OK) return st;
+    ftb::Frame f;
+    f.film = d_film;
+    f.tally = d_tally;
+    f.status = s->status;
+    f.film_scale_inv = std::ldexp(1.0, frac_bits) / s->power;
+    f.tally_scale_inv = std::ldexp(1.0, 32) / s->power;
+    DevCam dc = dev_cam(cam);
+    // hand off from the caller's stream (0 = legacy stream) to the two wave streams and back
+    cudaEvent_t ready = nullptr;
+    CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
+    CK(cudaEventRecord(ready, user_stream), "event record");
+    for (auto st2 : s->streams) CK(cudaStreamWaitEvent(st2, ready, 0), "stream wait");
+    int64_t done = 0;
+    int k = 0;
+    while (done < n) {
+        int32_t m = (int32_t)std::min<int64_t>(W, n - done);
+        ftb::Wave& w = s->waves[k & 1];
+        w.logs = d_logs;
+        w.log_base = (int64_t)seed_base;
+        cudaError_t e = ftb::launch_wave(s->dev, dc, w, f, seed_base + (uint64_t)done, m, max_bounce, s->sms,
+                                         s->streams[k & 1]);
+        if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+        done += m;
+        ++k;
+    }
+    for (auto st2 : s->streams) {
+        CK(cudaEventRecord(ready, st2), "event record");
+        CK(cudaStreamWaitEvent(user_stream, ready, 0), "stream wait");
+    }
+    cudaEventDestroy(ready);
+    return FTB_OK;
+}
+
+ftb_status read_status(ftb_scene* s) {
+    int32_t stv = 0;
+    CK(cudaMemcpy(&stv, s->status, 4, cudaMemcpyDeviceToHost), "status readback");
+    if (stv) {
+        std::string m = "device reported:";
+        if (stv & ftb::ST_STACK_OVERFLOW) m += " traversal stack overflow;";
+        if (stv & ftb::ST_FILM_SATURATED) m += " film fixed-point saturation (lower frac_bits);";
+        if (stv & ftb::ST_MEDIUM_STACK) m += " nested dielectrics deeper than 4;";
+        if (stv & ftb::ST_QUEUE_OVERFLOW) m += " shadow queue overflow;";
+        return fail(FTB_ERR_DEVICE_LIMIT, m);
+    }
+    return FTB_OK;
+}
+
+void tally_to_energy(const unsigned long long* fx, double power, ftb_energy* e, bool accumulate) {
+    double k = power * std::ldexp(1.0, -32);
+    double v[5];
+    for (int i = 0; i < 5; ++i) v[i] = (double)(long long)fx[i] * k;
+    if (accumulate) {
+        e->emitted += v[0]; e->absorbed += v[1]; e->sensor += v[2]; e->escaped += v[3]; e->residual += v[4];
+        for (int i = 0; i < 5; ++i) e->fx[i] += (int64_t)fx[i];
+    } else {
+        e->emitted = v[0]; e->absorbed = v[1]; e->sensor = v[2]; e->escaped = v[3]; e->residual = v[4];
+        for (int i = 0; i < 5; ++i) e->fx[i] = (int64_t)fx[i];
+    }
+}
+
+ftb_status check_params(const ftb_scene* s, const ftb_camera* cam, const ftb_render_params* p) {
+    if (!s || !cam || !p) return fail(FTB_ERR_INVALID, "null argument");
+    if (cam->res_x <= 0 || cam->res_y <= 0 || (int64_t)cam->res_x * cam->res_y > ((int64_t)1 << 28))
+        return fail(FTB_ERR_INVALID, "camera resolution out of range");
+    if (p->n_photons < 0) return fail(FTB_ERR_INVALID, "negative photon count");
+    if (p->max_bounce < 0 || p->max_bounce > 1024) return fail(FTB_ERR_INVALID, "max_bounce out of range [0, 1024]");
+    if (p->frac_bits > 56) return fail(FTB_ERR_INVALID, "frac_bits too large");
+    if (!(s->power > 0.0)) return fail(FTB_ERR_UNSUPPORTED, "scene emits no power");
+    return FTB_OK;
+}
+
+}  // namespace
+
+// ---- entry points ----------------------------------------------------------------------
+extern "C" {
+
+const char* ftb_last_error(void) { return g_err.c_str(); }
+int ftb_abi_version(void) { return FTB_ABI_VERSION; }
+
+int ftb_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n > 0 ? 1 : 0;
+}
+
+const char* ftb_device_name(void) {
+    static char name[256] = "none";
+    int n = 0;
+    if (cudaGetDeviceCount(&n) == cudaSuccess && n > 0) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, 0) == cudaSuccess) std::snprintf(name, sizeof name, "%s", p.name);
+    } else {
+        cudaGetLastError();
+    }
+    return name;
+}
+
+ftb_status ftb_mem_info(size_t* free_b, size_t* total_b) {
+    if (!free_b || !total_b) return fail(FTB_ERR_INVALID, "null argument");
+    if (!ftb_available()) return fail(FTB_ERR_NO_DEVICE, "no CUDA device");
+    CK(cudaMemGetInfo(free_b, total_b), "cudaMemGetInfo");
+    return FTB_OK;
+}
+
+int ftb_forward_supported(const ftb_scene_desc* desc) {
+    ftb_status s = check_desc(desc);
+    if (s == FTB_OK) return 1;
+    if (s == FTB_ERR_UNSUPPORTED) return 0;
+    return -1;
+}
+
+ftb_status ftb_camera_look_at(const double eye[3], const double target[3], const double up[3], double fov,
+                              int32_t rx, int32_t ry, ftb_camera* out) {
+    if (!eye || !target || !up || !out || rx <= 0 || ry <= 0) return fail(FTB_ERR_INVALID, "bad camera arguments");
+    // Camera::lookAt (camera.h:110-125)
+    V e{eye[0], eye[1], eye[2]};
+    V w = vnorm(vsub(V{target[0], target[1], target[2]}, e));
+    V u = vnorm(vcross(w, V{up[0], up[1], up[2]}));
+    V v = vcross(u, w);
+    double thy = std::tan(0.5 * fov * 3.141592653589793 / 180.0);
+    double thx = thy * (double)rx / (double)ry;
+    std::memset(out, 0, sizeof *out);
+    double* dst[4] = {out->eye, out->u, out->v, out->w};
+    V src[4] = {e, u, v, w};
+    for (int k = 0; k < 4; ++k) { dst[k][0] = src[k].x; dst[k][1] = src[k].y; dst[k][2] = src[k].z; }
+    out->tan_half_x = thx;
+    out->tan_half_y = thy;
+    out->res_x = rx;
+    out->res_y = ry;
+    return FTB_OK;
+}
+
+ftb_status ftb_emission_cdf(const ftb_spectrum* spd, const double* table_w, const double* table_v, double step,
+                            double* out_cdf, int32_t out_cap, int32_t* out_n, double* integral) {
+    if (!spd || !out_cdf || !out_n || !integral || !(step > 0.0)) return fail(FTB_ERR_INVALID, "bad arguments");
+    ftb_scene_desc d{};
+    ftb_spectrum one = *spd;
+    if (one.kind == FTB_SPEC_TABLE) {
+        d.table_w = table_w;
+        d.table_v = table_v;
+        d.n_table = one.offset + one.n;
+    }
+    d.spectra = &one;
+    d.n_spectra = 1;
+    std::string why;
+    if (!spec_valid(&d, 0, why)) return fail(FTB_ERR_INVALID, why);
+    // EmissionSampler::build (spectrum.h:357-369)
+    int n = (int)((kLambdaMax - kLambdaMin) / step);
+    if (n < 1 || n + 1 > out_cap) return fail(FTB_ERR_INVALID, "cdf buffer too small");
+    for (int i = 0; i <= n; ++i) out_cdf[i] = 0.0;
+    double acc = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double w = kLambdaMin + (i + 0.5) * step;
+        double v = spec_eval_host(&d, 0, w);
+        acc += std::max(0.0, v) * step;
+        out_cdf[i + 1] = acc;
+    }
+    *integral = acc;
+    if (acc > 0) for (int i = 0; i <= n; ++i) out_cdf[i] /= acc;
+    *out_n = n;
+    return FTB_OK;
+}
+
+ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene** out) {
+    if (!out) return fail(FTB_ERR_INVALID, "null output");
+    *out = nullptr;
+    ftb_status st = check_desc(d);
+    if (st != FTB_OK) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return fail(FTB_ERR_NO_DEVICE, "no CUDA device"); }
+    if (device < 0 || device >= ndev) return fail(FTB_ERR_INVALID, "device index out of range");
+    DeviceGuard guard(device);
+    auto s = new ftb_scene();
+    s->device = device;
+    {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, device) == cudaSuccess) s->sms = p.multiProcessorCount;
+    }
+    const int64_t nt = d->n_tris, ns = d->n_spheres, nc = d->n_curves, np = nt + ns + nc;
+    // primitive boxes and the scene's coordinate magnitude (for the traversal margin)
+    std::vector<ftb::Box> boxes((size_t)np);
+    double maxabs = 1.0;
+    auto see = [&](double v) { double a = std::fabs(v); if (a > maxabs) maxabs = a; };
+    for (int64_t i = 0; i < nt; ++i) {
+        const double* v = d->tri_v + 9 * i;
+        ftb::Box b;
+        for (int k = 0; k < 3; ++k) { b.grow_point(v + 3 * k); see(v[3 * k]); see(v[3 * k + 1]); see(v[3 * k + 2]); }
+        boxes[(size_t)i] = b;
+    }
+    for (int64_t i = 0; i < ns; ++i) {
+        const double* sp = d->sph + 4 * i;
+        ftb::Box b;
+        for (int a = 0; a < 3; ++a) { b.lo[a] = sp[a] - sp[3]; b.hi[a] = sp[a] + sp[3]; see(b.lo[a]); see(b.hi[a]); }
+        boxes[(size_t)(nt + i)] = b;
+    }
+    for (int64_t i = 0; i < nc; ++i) {
+        const double* c = d->curve + 10 * i;
+        ftb::Box b;   // curveSegBounds (curve.h:99-104)
+        for (int a = 0; a < 3; ++a) {
+            b.lo[a] = std::min(c[a] - c[6], c[3 + a] - c[7]);
+            b.hi[a] = std::max(c[a] + c[6], c[3 + a] + c[7]);
+            see(b.lo[a]); see(b.hi[a]);
+        }
+        boxes[(size_t)(nt + ns + i)] = b;
+    }
+    for (int i = 0; i < d->n_emitters; ++i) {
+        const ftb_emitter& e = d->emitters[i];
+        for (int a = 0; a < 3; ++a) { see(e.origin[a] + std::fabs(e.u[a]) + std::fabs(e.v[a]) + e.radius); }
+    }
+    double margin = std::ldexp(maxabs, -18);
+    ftb::WideBvh bvh;
+    std::string err;
+    if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err)) { delete s; return fail(FTB_ERR_INVALID, err); }
+    if (np == 0) {   // an empty root with no children
+        bvh.nodes.resize(1);
+        std::memset(&bvh.nodes[0], 0, sizeof(WNode));
+    }
+    // records in leaf order
+    std::vector<PrimRec> recs(bvh.order.size());
+    bool any_smooth = false;
+    for (size_t r = 0; r < bvh.order.size(); ++r) {
+        int p = bvh.order[r];
+        PrimRec& R = recs[r];
+        std::memset(&R, 0, sizeof R);
+        R.prim = p;
+        int ty, mat, smooth = 0;
+        if (p < nt) {
+            std::memcpy(R.d, d->tri_v + 9 * (size_t)p, 9 * sizeof(double));
+            ty = REC_TRI; mat = d->tri_mat[p];
+            if (d->tri_n) {
+                const double* n = d->tri_n + 9 * (size_t)p;
+                for (int k = 0; k < 9; ++k) if (n[k] != 0.0) smooth = 1;
+            }
+        } else if (p < nt + ns) {
+            std::memcpy(R.d, d->sph + 4 * (size_t)(p - nt), 4 * sizeof(double));
+            ty = REC_SPHERE; mat = d->sph_mat[p - nt];
+        } else {
+            std::memcpy(R.d, d->curve + 10 * (size_t)(p - nt - ns), 8 * sizeof(double));
+            ty = REC_CURVE; mat = d->curve_mat[p - nt - ns];
+        }
+        any_smooth |= smooth != 0;
+        R.info = mat | (ty << 24) | (smooth << 30);
+    }
+    std::vector<DevSpec> spec((size_t)d->n_spectra);
+    for (int i = 0; i < d->n_spectra; ++i) {
+        spec[i].kind = d->spectra[i].kind; spec[i].n = d->spectra[i].n; spec[i].offset = d->spectra[i].offset;
+        for (int k = 0; k < 6; ++k) spec[i].p[k] = d->spectra[i].p[k];
+    }
+    std::vector<DevMat> mats((size_t)d->n_mats);
+    for (int i = 0; i < d->n_mats; ++i) {
+        const ftb_material& m = d->mats[i];
+        mats[i] = DevMat{m.type, m.priority, m.reflect, m.ior, m.absorb, m.transmit, m.roughness};
+    }
+    DevScene& D = s->dev;
+    const WNode* dn; const PrimRec* dr;
+#define UP(host, n, out, what) do { ftb_status u_ = upload(s, host, n, out, what); if (u_ != FTB_OK) { delete s; return u_; } } while (0)
+    UP(bvh.nodes.data(), bvh.nodes.size(), &dn, "upload nodes");
+    UP(recs.data(), recs.size(), &dr, "upload records");
+    D.nodes = dn; D.recs = dr;
+    if (any_smooth) UP(d->tri_n, (size_t)nt * 9, &D.tri_n, "upload normals");
+    UP(spec.data(), spec.size(), &D.spec, "upload spectra");
+    UP(d->table_w, (size_t)d->n_table, &D.tw, "upload tables");
+    UP(d->table_v, (size_t)d->n_table, &D.tv, "upload tables");
+    UP(mats.data(), mats.size(), &D.mats, "upload materials");
+    // emitters: wavelength CDFs, then the power CDF (Scene::finalizeEmitters, scene.h:1499-1513)
+    std::vector<DevEmit> em((size_t)d->n_emitters);
+    std::vector<double> sel((size_t)d->n_emitters);
+    double tp = 0.0;
+    for (int i = 0; i < d->n_emitters; ++i) {
+        const ftb_emitter& e = d->emitters[i];
+        const double* cdf_dev = nullptr;
+        UP(d->emitter_cdf + e.cdf_offset, (size_t)e.cdf_n + 1, &cdf_dev, "upload emitter cdf");
+        DevEmit& o = em[i];
+        o.shape = e.shape; o.collimated = e.collimated; o.n = e.cdf_n; o.pad = 0;
+        o.step = e.step; o.power = e.power; o.radius = e.radius;
+        for (int a = 0; a < 3; ++a) {
+            o.origin[a] = e.origin[a]; o.u[a] = e.u[a]; o.v[a] = e.v[a]; o.normal[a] = e.normal[a]; o.beam[a] = e.beam[a];
+        }
+        o.cdf = cdf_dev;
+        tp += e.power;
+        sel[i] = tp;
+    }
+    if (tp > 0) for (auto& c : sel) c /= tp;
+    UP(em.data(), em.size(), &D.emit, "upload emitters");
+    UP(sel.data(), sel.size(), &D.emit_cdf, "upload emitter cdf");
+    std::vector<DevMed> med((size_t)d->n_media);
+    for (int i = 0; i < d->n_media; ++i) {
+        const ftb_medium& m = d->media[i];
+        DevMed& o = med[i];
+        o.sa = m.sigma_a; o.ss = m.sigma_s; o.bound = m.bound; o.pad = 0; o.g = m.g; o.radius = m.radius;
+        for (int a = 0; a < 3; ++a) { o.bmin[a] = m.bmin[a]; o.bmax[a] = m.bmax[a]; o.center[a] = m.center[a]; }
+    }
+    UP(med.data(), med.size(), &D.med, "upload media");
+#undef UP
+    D.n_nodes = (int32_t)bvh.nodes.size();
+    D.n_recs = (int32_t)recs.size();
+    D.n_mats = d->n_mats;
+    D.n_emit = d->n_emitters;
+    D.n_med = d->n_media;
+    D.n_spec = d->n_spectra;
+    D.n_tris = nt;
+    D.total_power = tp;
+    s->power = tp;
+    *out = s;
+    return FTB_OK;
+}
+
+ftb_status ftb_scene_destroy(ftb_scene* s) {
+    delete s;
+    return FTB_OK;
+}
+
+double ftb_scene_power(const ftb_scene* s) { return s ? s->power : 0.0; }
+
+ftb_status ftb_scene_footprint(const ftb_scene* s, int32_t rx, int32_t ry, ftb_footprint* out) {
+    if (!s || !out || rx <= 0 || ry <= 0) return fail(FTB_ERR_INVALID, "bad arguments");
+    out->scene_bytes = s->scene_bytes;
+    out->film_bytes = (uint64_t)rx * (uint64_t)ry * 4 * sizeof(int64_t);
+    out->wave_bytes = 2 * (uint64_t)ftb::wave_bytes(1 << 22, false);
+    out->total_bytes = out->scene_bytes + out->film_bytes + out->wave_bytes;
+    return FTB_OK;
+}
+
+ftb_status ftb_render_forward_device(ftb_scene* s, const ftb_camera* cam, const ftb_render_params* p,
+                                     int64_t* d_film, ftb_film_info* info, ftb_energy* energy, void* stream) {
+    ftb_status st = check_params(s, cam, p);
+    if (st != FTB_OK) return st;
+    if (!d_film) return fail(FTB_ERR_INVALID, "null film");
+    std::lock_guard<std::mutex> lk(s->mu);
+    DeviceGuard guard(s->device);
+    int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
+    st = ensure_frame(s, 0);
+    if (st != FTB_OK) return st;
+    cudaStream_t us = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(s->tally, 0, 8 * sizeof(unsigned long long), us), "memset");
+    CK(cudaMemsetAsync(s->status, 0, 64, us), "memset");
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, d_film, s->tally, nullptr, us);
+    if (st != FTB_OK) return st;
+    if (info) { info->frac_bits = frac; info->scale = s->power * std::ldexp(1.0, -frac); info->power_ref = s->power; }
+    if (energy) {
+        CK(cudaStreamSynchronize(us), "sync");
+        st = read_status(s);
+        if (st != FTB_OK) return st;
+        unsigned long long fx[5];
+        CK(cudaMemcpy(fx, s->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally readback");
+        tally_to_energy(fx, s->power, energy, true);
+    }
+    return FTB_OK;
+}
+
+ftb_status ftb_render_forward(ftb_scene* s, const ftb_camera* cam, const ftb_render_params* p, int64_t* film,
+                              ftb_film_info* info, ftb_energy* energy) {
+    ftb_status st = check_params(s, cam, p);
+    if (st != FTB_OK) return st;
+    if (!film) return fail(FTB_ERR_INVALID, "null film");
+    std::lock_guard<std::mutex> lk(s->mu);
+    DeviceGuard guard(s->device);
+    size_t words = (size_t)cam->res_x * cam->res_y * 4;
+    int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
+    st = ensure_frame(s, words);
+    if (st != FTB_OK) return st;
+    CK(cudaMemset(s->film, 0, words * sizeof(int64_t)), "memset film");
+    CK(cudaMemset(s->tally, 0, 8 * sizeof(unsigned long long)), "memset tally");
+    CK(cudaMemset(s->status, 0, 64), "memset status");
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->film, s->tally, nullptr, nullptr);
+    if (st != FTB_OK) return st;
+    CK(cudaDeviceSynchronize(), "render");
+    st = read_status(s);
+    if (st != FTB_OK) return st;
+    CK(cudaMemcpy(film, s->film, words * sizeof(int64_t), cudaMemcpyDeviceToHost), "film download");
+    if (info) { info->frac_bits = frac; info->scale = s->power * std::ldexp(1.0, -frac); info->power_ref = s->power; }
+    if (energy) {
+        unsigned long long fx[5];
+        CK(cudaMemcpy(fx, s->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally readback");
+        tally_to_energy(fx, s->power, energy, true);
+    }
+    return FTB_OK;
+}
+
+ftb_status ftb_trace_log(ftb_scene* s, const ftb_camera* cam, const ftb_render_params* p, ftb_photon_log* out) {
+    ftb_status st = check_params(s, cam, p);
+    if (st != FTB_OK) return st;
+    if (!out) return fail(FTB_ERR_INVALID, "null log buffer");
+    if (p->n_photons > ((int64_t)1 << 24)) return fail(FTB_ERR_TOO_LARGE, "ftb_trace_log: at most 2^24 photons per call");
+    std::lock_guard<std::mutex> lk(s->mu);
+    DeviceGuard guard(s->device);
+    size_t words = (size_t)cam->res_x * cam->res_y * 4;
+    int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
+    st = ensure_frame(s, words);
+    if (st != FTB_OK) return st;
+    ftb_photon_log* d_logs = nullptr;
+    size_t lb = (size_t)std::max<int64_t>(p->n_photons, 1) * sizeof(ftb_photon_log);
+    CK(cudaMalloc(&d_logs, lb), "log alloc");
+    cudaMemset(s->film, 0, words * sizeof(int64_t));
+    cudaMemset(s->tally, 0, 8 * sizeof(unsigned long long));
+    cudaMemset(s->status, 0, 64);
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->film, s->tally, d_logs, nullptr);
+    if (st == FTB_OK) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) st = cuda_fail(e, "trace_log");
+    }
+    if (st == FTB_OK) st = read_status(s);
+    if (st == FTB_OK) {
+        cudaError_t e = cudaMemcpy(out, d_logs, (size_t)p->n_photons * sizeof(ftb_photon_log), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_fail(e, "log download");
+    }
+    cudaFree(d_logs);
+    return st;
+}
+
+// ---- sessions ---------------------------------------------------------------------------
+ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cams, int32_t max_bounce,
+                             int32_t frac_bits, ftb_session** out) {
+    if (!s || !cams || n_cams < 1 || !out) return fail(FTB_ERR_INVALID, "bad session arguments");
+    if (max_bounce < 0 || max_bounce > 1024) return fail(FTB_ERR_INVALID, "max_bounce out of range");
+    DeviceGuard guard(s->device);
+    auto ss = new ftb_session();
+    ss->scene = s;
+    ss->max_bounce = max_bounce;
+    ss->frac_bits = frac_bits > 0 ? frac_bits : default_frac_bits((int64_t)1 << 36);
+    for (int c = 0; c < n_cams; ++c) {
+        if (cams[c].res_x <= 0 || cams[c].res_y <= 0) { delete ss; return fail(FTB_ERR_INVALID, "bad camera"); }
+        ss->cams.push_back(cams[c]);
+        int64_t* f = nullptr;
+        size_t words = (size_t)cams[c].res_x * cams[c].res_y * 4;
+        cudaError_t e = cudaMalloc(&f, words * sizeof(int64_t));
+        if (e == cudaSuccess) e = cudaMemset(f, 0, words * sizeof(int64_t));
+        if (e != cudaSuccess) { for (auto p : ss->films) cudaFree(p); delete ss; return cuda_fail(e, "session film"); }
+        ss->films.push_back(f);
+    }
+    cudaError_t e = cudaMalloc(&ss->tally, 8 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(ss->tally, 0, 8 * sizeof(unsigned long long));
+    if (e != cudaSuccess) { for (auto p : ss->films) cudaFree(p); delete ss; return cuda_fail(e, "session tally"); }
+    *out = ss;
+    return FTB_OK;
+}
+
+ftb_status ftb_session_batch(ftb_session* ss, int64_t n, uint64_t seed_base) {
+    if (!ss || n < 0) return fail(FTB_ERR_INVALID, "bad batch arguments");
+    ftb_scene* s = ss->scene;
+    std::lock_guard<std::mutex> lk(s->mu);
+    DeviceGuard guard(s->device);
+    ftb_status st = ensure_frame(s, 0);
+    if (st != FTB_OK) return st;
+    CK(cudaMemset(s->status, 0, 64), "memset status");
+    // Model B connections draw no random numbers (render.h:272-275), so tracing the same
+    // photon indices once per camera gives every camera exactly the film a shared pass would.
+    for (size_t c = 0; c < ss->cams.size(); ++c) {
+        unsigned long long* tally = (c == 0) ? ss->tally : s->tally;
+        st = run_photons(s, &ss->cams[c], n, seed_base, ss->max_bounce, ss->frac_bits, ss->films[c], tally, nullptr,
+                         nullptr);
+        if (st != FTB_OK) return st;
+    }
+    CK(cudaDeviceSynchronize(), "session batch");
+    return read_status(s);
+}
+
+ftb_status ftb_session_hits0(ftb_session* ss, double* hits) {
+    if (!ss || !hits) return fail(FTB_ERR_INVALID, "bad arguments");
+    DeviceGuard guard(ss->scene->device);
+    const ftb_camera& c = ss->cams[0];
+    size_t npix = (size_t)c.res_x * c.res_y;
+    std::vector<int64_t> buf(npix * 4);
+    CK(cudaMemcpy(buf.data(), ss->films[0], buf.size() * sizeof(int64_t), cudaMemcpyDeviceToHost), "hits");
+    for (size_t i = 0; i < npix; ++i) hits[i] = (double)buf[4 * i + 3];
+    return FTB_OK;
+}
+
+ftb_status ftb_session_download(ftb_session* ss, int32_t cam, int64_t* film, ftb_film_info* info, ftb_energy* energy) {
+    if (!ss || cam < 0 || cam >= (int32_t)ss->cams.size()) return fail(FTB_ERR_INVALID, "bad arguments");
+    DeviceGuard guard(ss->scene->device);
+    const ftb_camera& c = ss->cams[cam];
+    size_t words = (size_t)c.res_x * c.res_y * 4;
+    if (film) CK(cudaMemcpy(film, ss->films[cam], words * sizeof(int64_t), cudaMemcpyDeviceToHost), "download");
+    if (info) {
+        info->frac_bits = ss->frac_bits;
+        info->scale = ss->scene->power * std::ldexp(1.0, -ss->frac_bits);
+        info->power_ref = ss->scene->power;
+    }
+    if (energy) {
+        unsigned long long fx[5];
+        CK(cudaMemcpy(fx, ss->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally");
+        tally_to_energy(fx, ss->scene->power, energy, false);
+    }
+    return FTB_OK;
+}
+
+ftb_status ftb_session_end(ftb_session* ss) {
+    if (!ss) return FTB_OK;
+    DeviceGuard guard(ss->scene->device);
+    for (auto p : ss->films) cudaFree(p);
+    if (ss->tally) cudaFree(ss->tally);
+    delete ss;
+    return FTB_OK;
+}
+
+}  // extern "C"

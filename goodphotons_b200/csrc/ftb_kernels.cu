@@ -1,0 +1,1216 @@
+// ftb_kernels.cu -- sm_100a wavefront kernels of the forward pinhole light tracer.
+//
+// One wave of W photon paths is traced with four kernels:
+//   k_emit    seed the per-photon PCG32 stream, pick emitter / point / direction /
+//             wavelength, book `emitted`, queue the emitter's direct camera connection
+//             (reference: Renderer::tracePhoton emission, render.h:1827-1984)
+//   k_extend  closest hit of every active path over the 8-wide BVH (Scene::closestHit,
+//             scene.h:2194-2242)
+//   k_shade   media, interior absorption and the material interaction of one bounce;
+//             queues camera connections and compacts the surviving paths into the next
+//             active list (render.h:2013-2238)
+//   k_shadow  any-hit test of the queued connections (Scene::occluded, scene.h:2249) and
+//             the splat into the 64-bit fixed-point film (Film::add, scene_film.h:12)
+//
+// Numerics.  Everything that decides a path -- triangle/sphere/curve tests, hit points,
+// normals, BSDF sampling, Russian roulette, the camera projection -- is computed in fp64
+// in the reference's operation order, and this file is compiled with -fmad=false so no
+// product is fused.  Only the BVH culling runs in fp32, against boxes that were rounded
+// outward (see bvh_build.cpp) and with the ray interval widened by 2^-21, so it never
+// drops a primitive the fp64 test would accept.  Paths therefore follow the reference CPU
+// tracer photon for photon; the remaining differences are last-bit ones from CUDA's
+// exp/log/sin/cos/pow, and exact ties in t.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "ftb_kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace ftb {
+
+#define PI_D 3.141592653589793
+#define LAMBDA_MIN 360.0
+#define LAMBDA_MAX 830.0
+#define EPS_RAY 1e-6
+
+// ------------------------------------------------------------------ vectors (fp64) -----
+struct D3 { double x, y, z; };
+__device__ __forceinline__ D3 mk(double x, double y, double z) { D3 r; r.x = x; r.y = y; r.z = z; return r; }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ D3 operator*(D3 a, double s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ D3 operator/(D3 a, double s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ D3 neg(D3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double len(D3 a) { return sqrt(dot(a, a)); }
+__device__ __forceinline__ D3 normalize(D3 a) { return a / len(a); }
+__device__ __forceinline__ double comp(D3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+__device__ __forceinline__ D3 ld3(const double* p) { return mk(p[0], p[1], p[2]); }
+// reflect (linalg.h:82)
+__device__ __forceinline__ D3 reflect(D3 d, D3 n) { return d - n * (2.0 * dot(d, n)); }
+// onb (linalg.h:85-91)
+__device__ __forceinline__ void onb(D3 n, D3& t, D3& b) {
+    double sign = copysign(1.0, n.z);
+    double a = -1.0 / (sign + n.z);
+    double d = n.x * n.y * a;
+    t = mk(1.0 + sign * n.x * n.x * a, sign * d, -sign * n.x);
+    b = mk(d, sign + n.y * n.y * a, -n.y);
+}
+
+// ------------------------------------------------------------------ RNG (rng.h) --------
+struct Pcg { uint64_t s, inc; };
+__device__ __forceinline__ uint32_t pcg_next(Pcg& r) {
+    uint64_t old = r.s;
+    r.s = old * 6364136223846793005ULL + r.inc;
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((~rot + 1u) & 31));
+}
+__device__ __forceinline__ double uniform(Pcg& r) { return (pcg_next(r) >> 8) * (1.0 / 16777216.0); }
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+// seedUnit (rng.h:40) with the forward-tracer salt (main.cpp:11326)
+__device__ __forceinline__ Pcg seed_photon(uint64_t k) {
+    const uint64_t salt = 0x9E3779B97F4A7C15ULL;
+    Pcg r;
+    r.s = 0; r.inc = (mix64(k ^ salt) << 1u) | 1u;
+    pcg_next(r);
+    r.s += mix64(k + salt);
+    pcg_next(r);
+    return r;
+}
+
+// cosineHemisphere (rng.h:45-52)
+__device__ D3 cosine_hemisphere(D3 n, Pcg& rng) {
+    double u1 = uniform(rng), u2 = uniform(rng);
+    double r = sqrt(u1);
+    double phi = 6.283185307179586 * u2;
+    double lx = r * cos(phi), ly = r * sin(phi), lz = sqrt(1.0 - u1);
+    D3 t, b; onb(n, t, b);
+    return normalize(t * lx + b * ly + n * lz);
+}
+// glossyDirUV / sampleGlossy (render.h:46-64)
+__device__ D3 sample_glossy(D3 mdir, double roughness, Pcg& rng) {
+    double u1 = uniform(rng), u2 = uniform(rng);
+    if (u1 >= 1.0) return mdir;
+    double rr = roughness < 1e-3 ? 1e-3 : roughness;
+    double e = 2.0 / (rr * rr) - 2.0; if (e < 0) e = 0;
+    double cos_t = pow(u1, 1.0 / (e + 1.0));
+    double s = 1.0 - cos_t * cos_t;
+    double sin_t = sqrt(s > 0.0 ? s : 0.0);
+    double phi = 2.0 * PI_D * u2;
+    D3 t, b; onb(mdir, t, b);
+    return normalize(t * (sin_t * cos(phi)) + b * (sin_t * sin(phi)) + mdir * cos_t);
+}
+// hgPhase / sampleHG (phase.h:18-40)
+__device__ __forceinline__ double hg_phase(double cos_t, double g) {
+    double d = 1.0 + g * g - 2.0 * g * cos_t;
+    if (d < 1e-9) d = 1e-9;
+    return (1.0 - g * g) / (4.0 * PI_D * d * sqrt(d));
+}
+__device__ D3 sample_hg(D3 wi, double g, Pcg& rng) {
+    double u1 = uniform(rng), u2 = uniform(rng);
+    double cos_t;
+    if (fabs(g) < 1e-3) cos_t = 1.0 - 2.0 * u1;
+    else {
+        double sq = (1.0 - g * g) / (1.0 + g - 2.0 * g * u1);
+        cos_t = (1.0 + g * g - sq * sq) / (2.0 * g);
+    }
+    double s = 1.0 - cos_t * cos_t;
+    double sin_t = sqrt(s > 0.0 ? s : 0.0);
+    double phi = 2.0 * PI_D * u2;
+    D3 t, b; onb(wi, t, b);
+    return normalize(t * (sin_t * cos(phi)) + b * (sin_t * sin(phi)) + wi * cos_t);
+}
+
+// ------------------------------------------------------------------ spectra ------------
+__device__ double spec_eval(const DevScene& sc, int idx, double w) {
+    const DevSpec& s = sc.spec[idx];
+    switch (s.kind) {
+    case FTB_SPEC_CONST: return s.p[0];
+    case FTB_SPEC_TABLE: {   // tabulatedSpectrum (spectrum.h:264-281)
+        const double* x = sc.tw + s.offset;
+        const double* y = sc.tv + s.offset;
+        int n = s.n;
+        if (w <= x[0]) return y[0];
+        if (w >= x[n - 1]) return y[n - 1];
+        int lo = 0, hi = n - 1;
+        while (lo + 1 < hi) { int mid = (lo + hi) / 2; if (x[mid] <= w) lo = mid; else hi = mid; }
+        double w0 = x[lo], w1 = x[lo + 1], v0 = y[lo], v1 = y[lo + 1];
+        double f = (w1 > w0) ? (w - w0) / (w1 - w0) : 0.0;
+        return v0 + (v1 - v0) * f;
+    }
+    case FTB_SPEC_CAUCHY: { double um = w * 1e-3; return s.p[0] + s.p[1] / (um * um); }
+    case FTB_SPEC_SELLMEIER: {
+        double l2 = (w * 1e-3) * (w * 1e-3);
+        double n2 = 1.0 + s.p[0] * l2 / (l2 - s.p[3]) + s.p[1] * l2 / (l2 - s.p[4]) +
+                    s.p[2] * l2 / (l2 - s.p[5]);
+        return sqrt(n2 > 1.0 ? n2 : 1.0);
+    }
+    default: return 0.0;
+    }
+}
+__device__ __forceinline__ double spec_slot(const DevScene& sc, int s, double w, double dflt) {
+    return s >= 0 ? spec_eval(sc, s, w) : dflt;
+}
+__device__ __forceinline__ double clamp01(double x) { return x < 0 ? 0 : (x > 1 ? 1 : x); }
+
+// CIE 1931 multi-Gaussian fit (color.h:8-24)
+__device__ __forceinline__ double gauss_piece(double x, double mu, double s1, double s2) {
+    double t = (x - mu) * ((x < mu) ? s1 : s2);
+    return exp(-0.5 * t * t);
+}
+__device__ __forceinline__ double cie_x(double w) {
+    return 0.362 * gauss_piece(w, 442.0, 0.0624, 0.0374) + 1.056 * gauss_piece(w, 599.8, 0.0264, 0.0323) -
+           0.065 * gauss_piece(w, 501.1, 0.0490, 0.0382);
+}
+__device__ __forceinline__ double cie_y(double w) {
+    return 0.821 * gauss_piece(w, 568.8, 0.0213, 0.0247) + 0.286 * gauss_piece(w, 530.9, 0.0613, 0.0322);
+}
+__device__ __forceinline__ double cie_z(double w) {
+    return 1.217 * gauss_piece(w, 437.0, 0.0845, 0.0278) + 0.681 * gauss_piece(w, 459.0, 0.0385, 0.0725);
+}
+
+// ------------------------------------------------------------------ exact prim tests ---
+struct Shear { int kx, ky, kz; double sx, sy, sz; };
+// makeTriShear (geometry.h:261-276)
+__device__ __forceinline__ Shear make_shear(D3 d) {
+    Shear s;
+    double ax = fabs(d.x), ay = fabs(d.y), az = fabs(d.z);
+    if (ax >= ay && ax >= az) s.kz = 0; else if (ay >= az) s.kz = 1; else s.kz = 2;
+    s.kx = s.kz + 1; if (s.kx == 3) s.kx = 0;
+    s.ky = s.kx + 1; if (s.ky == 3) s.ky = 0;
+    if (comp(d, s.kz) < 0.0) { int t = s.kx; s.kx = s.ky; s.ky = t; }
+    s.sx = comp(d, s.kx) / comp(d, s.kz);
+    s.sy = comp(d, s.ky) / comp(d, s.kz);
+    s.sz = 1.0 / comp(d, s.kz);
+    return s;
+}
+// The reference recomputes an exactly-zero edge function in long double (x87, 64-bit
+// mantissa).  The device has no extended type: a*b - c*d is formed from exact products
+// (two FMA residuals), which has the same sign whenever the extended-precision result is
+// nonzero.  Reached only when a ray meets an edge line exactly.
+__device__ __forceinline__ double zero_fallback(double a, double b, double c, double d) {
+    double ph = a * b, qh = c * d;
+    double pl = fma(a, b, -ph), ql = fma(c, d, -qh);
+    return (ph - qh) + (pl - ql);
+}
+struct TriHitW { double u, v, w, inv_det; };
+// intersectTri acceptance (geometry.h:280-324); returns t or -1 (rejected)
+__device__ __forceinline__ bool tri_test(const Shear& sh, D3 ro, const double* v, double tmin,
+                                         double tbest, double& t_out, TriHitW* bw) {
+    D3 A = mk(v[0], v[1], v[2]) - ro, B = mk(v[3], v[4], v[5]) - ro, C = mk(v[6], v[7], v[8]) - ro;
+    double Akz = comp(A, sh.kz), Bkz = comp(B, sh.kz), Ckz = comp(C, sh.kz);
+    double Ax = comp(A, sh.kx) - sh.sx * Akz, Ay = comp(A, sh.ky) - sh.sy * Akz;
+    double Bx = comp(B, sh.kx) - sh.sx * Bkz, By = comp(B, sh.ky) - sh.sy * Bkz;
+    double Cx = comp(C, sh.kx) - sh.sx * Ckz, Cy = comp(C, sh.ky) - sh.sy * Ckz;
+    double U = Cx * By - Cy * Bx;
+    double V = Ax * Cy - Ay * Cx;
+    double W = Bx * Ay - By * Ax;
+    if (U == 0.0 || V == 0.0 || W == 0.0) {
+        if (U == 0.0) U = zero_fallback(Cx, By, Cy, Bx);
+        if (V == 0.0) V = zero_fallback(Ax, Cy, Ay, Cx);
+        if (W == 0.0) W = zero_fallback(Bx, Ay, By, Ax);
+    }
+    if ((U < 0.0 || V < 0.0 || W < 0.0) && (U > 0.0 || V > 0.0 || W > 0.0)) return false;
+    double det = U + V + W;
+    if (det == 0.0) return false;
+    double T = U * (sh.sz * Akz) + V * (sh.sz * Bkz) + W * (sh.sz * Ckz);
+    double inv_det = 1.0 / det;
+    double t = T * inv_det;
+    if (t < tmin || t >= tbest) return false;
+    t_out = t;
+    if (bw) { bw->u = U; bw->v = V; bw->w = W; bw->inv_det = inv_det; }
+    return true;
+}
+// intersectSphere acceptance (geometry.h:377-387)
+__device__ __forceinline__ bool sphere_test(D3 ro, D3 rd, const double* s, double tmin, double tbest,
+                                            double& t_out) {
+    D3 oc = ro - mk(s[0], s[1], s[2]);
+    double r = s[3];
+    double a = dot(rd, rd);
+    double b = 2.0 * dot(oc, rd);
+    double c = dot(oc, oc) - r * r;
+    double disc = b * b - 4.0 * a * c;
+    if (disc < 0.0) return false;
+    double sq = sqrt(disc);
+    double t = (-b - sq) / (2.0 * a);
+    if (t < tmin) t = (-b + sq) / (2.0 * a);
+    if (t < tmin || t >= tbest) return false;
+    t_out = t;
+    return true;
+}
+// makeCurveRay (curve.h:126-135)
+struct CurveRay { D3 dn; double inv_len; };
+__device__ __forceinline__ CurveRay make_curve_ray(D3 d) {
+    CurveRay c; c.dn = mk(0, 0, 1); c.inv_len = 1.0;
+    double l2 = dot(d, d);
+    if (l2 > 0.0) { double l = sqrt(l2); c.inv_len = 1.0 / l; c.dn = d * c.inv_len; }
+    return c;
+}
+struct CurveWin { double tn, y, shift; int piece; };
+__device__ __forceinline__ void offer(CurveWin& a, double inv_len, double tmin, double tbest, double tn,
+                                      int w, double y) {
+    if (tn >= a.tn) return;
+    double t = (tn + a.shift) * inv_len;
+    if (t < tmin || t >= tbest) return;
+    a.tn = tn; a.piece = w; a.y = y;
+}
+// curveSegCrossings<double> + intersectCurveSeg acceptance (curve.h:199-309)
+__device__ bool curve_test(const CurveRay& cr, D3 ro, const double* s, double tmin, double tbest,
+                           double& t_out, CurveWin* win) {
+    D3 rd = cr.dn;
+    D3 p0 = mk(s[0], s[1], s[2]), p1 = mk(s[3], s[4], s[5]);
+    double r0 = s[6], r1 = s[7];
+    CurveWin a; a.tn = DBL_MAX; a.y = 0.0; a.piece = -1;
+    D3 ba = p1 - p0;
+    double m0 = dot(ba, ba);
+    if (!(m0 > 0.0)) return false;
+    a.shift = dot(p0 - ro, rd);
+    D3 o = mk(ro.x + rd.x * a.shift, ro.y + rd.y * a.shift, ro.z + rd.z * a.shift);
+    D3 oa = o - p0, ob = o - p1;
+    double rr = r0 - r1;
+    double m1 = dot(ba, oa), m2 = dot(ba, rd), m3 = dot(rd, oa), m5 = dot(oa, oa);
+    double m6 = dot(ob, rd), m7 = dot(ob, ob);
+    double d2 = m0 - rr * rr;
+    const double il = cr.inv_len;
+    if (d2 > 0.0) {
+        double k2 = d2 - m2 * m2;
+        double k1 = d2 * m3 - m1 * m2 + m2 * rr * r0;
+        double k0 = d2 * m5 - m1 * m1 + m1 * rr * r0 * 2.0 - m0 * r0 * r0;
+        double h = k1 * k1 - k0 * k2;
+        if (h >= 0.0 && k2 != 0.0) {
+            double sq = sqrt(h);
+            double ta = (-sq - k1) / k2, tb = (sq - k1) / k2;
+            if (ta > tb) { double tmp = ta; ta = tb; tb = tmp; }
+            double base = m1 - r0 * rr;
+            double ya = base + ta * m2, yb = base + tb * m2;
+            if (ya > 0.0 && ya < d2) offer(a, il, tmin, tbest, ta, 0, ya);
+            if (yb > 0.0 && yb < d2) offer(a, il, tmin, tbest, tb, 0, yb);
+        }
+        double h1 = m3 * m3 - m5 + r0 * r0;
+        if (h1 > 0.0) {
+            double q = sqrt(h1), base = m1 - r0 * rr;
+            double ta = -m3 - q, tb = -m3 + q;
+            if (base + ta * m2 <= 0.0) offer(a, il, tmin, tbest, ta, 1, 0.0);
+            if (base + tb * m2 <= 0.0) offer(a, il, tmin, tbest, tb, 1, 0.0);
+        }
+        double h2 = m6 * m6 - m7 + r1 * r1;
+        if (h2 > 0.0) {
+            double q = sqrt(h2), base = m1 - r0 * rr;
+            double ta = -m6 - q, tb = -m6 + q;
+            if (base + ta * m2 >= d2) offer(a, il, tmin, tbest, ta, 2, d2);
+            if (base + tb * m2 >= d2) offer(a, il, tmin, tbest, tb, 2, d2);
+        }
+    } else {
+        bool use_p0 = (r0 >= r1);
+        double rc = use_p0 ? r0 : r1, mm = use_p0 ? m3 : m6, mq = use_p0 ? m5 : m7;
+        double hh = mm * mm - mq + rc * rc;
+        if (hh > 0.0) {
+            double q = sqrt(hh);
+            offer(a, il, tmin, tbest, -mm - q, use_p0 ? 1 : 2, use_p0 ? 0.0 : d2);
+            offer(a, il, tmin, tbest, -mm + q, use_p0 ? 1 : 2, use_p0 ? 0.0 : d2);
+        }
+    }
+    if (a.piece < 0) return false;
+    t_out = (a.tn + a.shift) * il;
+    if (win) *win = a;
+    return true;
+}
+
+__device__ __forceinline__ int rec_type(const PrimRec& r) { return (r.info >> 24) & 3; }
+__device__ __forceinline__ int rec_mat(const PrimRec& r) { return r.info & 0xffffff; }
+__device__ __forceinline__ bool rec_smooth(const PrimRec& r) { return (r.info >> 30) & 1; }
+
+__device__ __forceinline__ void load_rec(const PrimRec* recs, int i, PrimRec& r) {
+    const double2* p = reinterpret_cast<const double2*>(recs + i);
+    double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4);
+    r.d[0] = a.x; r.d[1] = a.y; r.d[2] = b.x; r.d[3] = b.y; r.d[4] = c.x; r.d[5] = c.y;
+    r.d[6] = d.x; r.d[7] = d.y; r.d[8] = e.x;
+    long long tail = __double_as_longlong(e.y);
+    r.prim = (int32_t)(tail & 0xffffffffLL);
+    r.info = (int32_t)(tail >> 32);
+}
+
+struct RayCtx {
+    D3 o, d;
+    Shear sh;
+    CurveRay cr;
+};
+
+__device__ __forceinline__ bool rec_test(const RayCtx& R, const PrimRec& r, double tmin, double tbest,
+                                         double& t) {
+    int ty = rec_type(r);
+    if (ty == REC_TRI) return tri_test(R.sh, R.o, r.d, tmin, tbest, t, nullptr);
+    if (ty == REC_SPHERE) return sphere_test(R.o, R.d, r.d, tmin, tbest, t);
+    return curve_test(R.cr, R.o, r.d, tmin, tbest, t, nullptr);
+}
+
+// Hit attributes of the winning record (geometry.h:325-368, :388-396, curve.h:310-335)
+struct Hit {
+    double t;
+    D3 p, n, ng;
+    int mat, prim;
+};
+__device__ void hit_attributes(const DevScene& sc, const RayCtx& R, const PrimRec& r, Hit& h) {
+    int ty = rec_type(r);
+    h.mat = rec_mat(r);
+    h.prim = r.prim;
+    double t = 0.0;
+    if (ty == REC_TRI) {
+        TriHitW w;
+        tri_test(R.sh, R.o, r.d, EPS_RAY, DBL_MAX, t, &w);
+        double b0 = w.u * w.inv_det, b1 = w.v * w.inv_det, b2 = w.w * w.inv_det;
+        D3 v0 = mk(r.d[0], r.d[1], r.d[2]), v1 = mk(r.d[3], r.d[4], r.d[5]), v2 = mk(r.d[6], r.d[7], r.d[8]);
+        D3 tgn = normalize(cross(v1 - v0, v2 - v0));     // Tri::finalize (geometry.h:52)
+        D3 n0 = tgn, n1 = tgn, n2 = tgn;
+        if (rec_smooth(r)) {
+            const double* nn = sc.tri_n + 9 * (size_t)r.prim;
+            D3 a = ld3(nn), b = ld3(nn + 3), c = ld3(nn + 6);
+            if (!(dot(a, a) < 1e-12)) n0 = a;
+            if (!(dot(b, b) < 1e-12)) n1 = b;
+            if (!(dot(c, c) < 1e-12)) n2 = c;
+        }
+        h.t = t;
+        h.p = R.o + R.d * t;
+        D3 ns = n0 * b0 + n1 * b1 + n2 * b2;
+        double nl = dot(ns, ns);
+        ns = (nl > 1e-18) ? ns * (1.0 / sqrt(nl)) : tgn;
+        D3 gn = (dot(tgn, ns) < 0.0) ? neg(tgn) : tgn;
+        bool flipped = !(dot(R.d, gn) < 0.0);
+        h.ng = gn;
+        h.n = flipped ? neg(ns) : ns;
+    } else if (ty == REC_SPHERE) {
+        sphere_test(R.o, R.d, r.d, EPS_RAY, DBL_MAX, t);
+        h.t = t;
+        h.p = R.o + R.d * t;
+        D3 ng = normalize(h.p - mk(r.d[0], r.d[1], r.d[2]));
+        h.ng = ng;
+        h.n = (!(dot(R.d, ng) < 0.0)) ? neg(ng) : ng;
+    } else {
+        CurveWin win;
+        curve_test(R.cr, R.o, r.d, EPS_RAY, DBL_MAX, t, &win);
+        h.t = t;
+        D3 rd = R.cr.dn;
+        D3 p0 = mk(r.d[0], r.d[1], r.d[2]), p1 = mk(r.d[3], r.d[4], r.d[5]);
+        D3 ba = p1 - p0;
+        double rr = r.d[6] - r.d[7];
+        double d2 = dot(ba, ba) - rr * rr;
+        D3 ro = R.o + rd * win.shift;
+        D3 oa = ro - p0, ob = ro - p1;
+        h.p = R.o + R.d * t;
+        D3 ng;
+        if (win.piece == 0) ng = (oa + rd * win.tn) * d2 - ba * win.y;
+        else if (win.piece == 1) ng = oa + rd * win.tn;
+        else ng = ob + rd * win.tn;
+        double nl = sqrt(dot(ng, ng));
+        ng = (nl > 1e-18) ? ng * (1.0 / nl) : normalize(ba);
+        h.ng = ng;
+        h.n = (dot(R.d, ng) < 0.0) ? ng : neg(ng);
+    }
+}
+
+// ------------------------------------------------------------------ traversal (fp32) ---
+struct RayF {
+    float ox, oy, oz, ix, iy, iz;
+    bool nx, ny, nz;   // direction component negative: near plane is the box's hi side
+};
+__device__ __forceinline__ RayF make_rayf(D3 o, D3 d) {
+    RayF r;
+    r.ox = (float)o.x; r.oy = (float)o.y; r.oz = (float)o.z;
+    float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
+    // a zero component is replaced by +-1e-20: the ray moves by at most 1e-20*t, far below
+    // the box margin, and the reciprocals stay finite (no inf*0 NaNs in the slab test)
+    dx = fabsf(dx) > 1e-20f ? dx : copysignf(1e-20f, dx);
+    dy = fabsf(dy) > 1e-20f ? dy : copysignf(1e-20f, dy);
+    dz = fabsf(dz) > 1e-20f ? dz : copysignf(1e-20f, dz);
+    r.ix = 1.0f / dx; r.iy = 1.0f / dy; r.iz = 1.0f / dz;
+    r.nx = dx < 0.0f; r.ny = dy < 0.0f; r.nz = dz < 0.0f;
+    return r;
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint2 w, int i) {
+    uint32_t word = (i < 4) ? w.x : w.y;
+    return (word >> (8 * (i & 3))) & 0xffu;
+}
+
+#define T_LO (1.0f - 4.76837158203125e-7f)   // 1 - 2^-21
+#define T_HI (1.0f + 4.76837158203125e-7f)
+
+// Test the 8 children of a node; returns the child-hit mask and fills tn[].
+__device__ __forceinline__ uint32_t node_children(const uint4 (&n)[5], const RayF& R, float tmin_f,
+                                                  float tmax_f, float (&tn)[8]) {
+    float px = __uint_as_float(n[0].x), py = __uint_as_float(n[0].y), pz = __uint_as_float(n[0].z);
+    float sx = __uint_as_float((n[0].w & 0xffu) << 23);
+    float sy = __uint_as_float(((n[0].w >> 8) & 0xffu) << 23);
+    float sz = __uint_as_float(((n[0].w >> 16) & 0xffu) << 23);
+    // t(q) = q * (s * inv) + (p - o) * inv
+    float ax = sx * R.ix, bx = (px - R.ox) * R.ix;
+    float ay = sy * R.iy, by = (py - R.oy) * R.iy;
+    float az = sz * R.iz, bz = (pz - R.oz) * R.iz;
+    uint2 lox = make_uint2(n[2].x, n[2].y), loy = make_uint2(n[2].z, n[2].w), loz = make_uint2(n[3].x, n[3].y);
+    uint2 hix = make_uint2(n[3].z, n[3].w), hiy = make_uint2(n[4].x, n[4].y), hiz = make_uint2(n[4].z, n[4].w);
+    if (R.nx) { uint2 t = lox; lox = hix; hix = t; }
+    if (R.ny) { uint2 t = loy; loy = hiy; hiy = t; }
+    if (R.nz) { uint2 t = loz; loz = hiz; hiz = t; }
+    uint2 meta = make_uint2(n[1].z, n[1].w);
+    uint32_t mask = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float tnx = __fmaf_rn((float)byte_of(lox, i), ax, bx);
+        float tfx = __fmaf_rn((float)byte_of(hix, i), ax, bx);
+        float tny = __fmaf_rn((float)byte_of(loy, i), ay, by);
+        float tfy = __fmaf_rn((float)byte_of(hiy, i), ay, by);
+        float tnz = __fmaf_rn((float)byte_of(loz, i), az, bz);
+        float tfz = __fmaf_rn((float)byte_of(hiz, i), az, bz);
+        float a = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin_f)) * T_LO;
+        float b = fminf(fminf(tfx, tfy), fminf(tfz, tmax_f)) * T_HI;
+        tn[i] = a;
+        if (a <= b && byte_of(meta, i) != 0) mask |= 1u << i;
+    }
+    return mask;
+}
+
+__device__ __forceinline__ void load_node(const WNode* nodes, uint32_t i, uint4 (&n)[5]) {
+    const uint4* p = reinterpret_cast<const uint4*>(nodes + i);
+    n[0] = __ldg(p); n[1] = __ldg(p + 1); n[2] = __ldg(p + 2); n[3] = __ldg(p + 3); n[4] = __ldg(p + 4);
+}
+
+// Closest hit: returns the record index (or -1) and t.
+__device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin, double& best_t,
+                                int32_t* status) {
+    RayF F = make_rayf(R.o, R.d);
+    float tmin_f = __double2float_rd(tmin);
+    best_t = DBL_MAX;
+    float tmax_f = FLT_MAX;
+    int best = -1;
+    uint32_t st_node[FTB_STACK];
+    float st_t[FTB_STACK];
+    int sp = 0;
+    uint32_t node = 0;
+    while (true) {
+        uint4 n[5];
+        load_node(sc.nodes, node, n);
+        float tn[8];
+        uint32_t hit = node_children(n, F, tmin_f, tmax_f, tn);
+        uint32_t imask = n[0].w >> 24;
+        uint32_t child_base = n[1].x, prim_base = n[1].y;
+        uint2 meta = make_uint2(n[1].z, n[1].w);
+        // leaves first: they can only shrink best_t
+        uint32_t leaves = hit & ~imask;
+        while (leaves) {
+            int i = __ffs(leaves) - 1;
+            leaves &= leaves - 1;
+            uint32_t m = byte_of(meta, i);
+            int cnt = m >> 5, off = m & 31;
+            for (int k = 0; k < cnt; ++k) {
+                PrimRec r;
+                int ri = (int)prim_base + off + k;
+                load_rec(sc.recs, ri, r);
+                double t;
+                if (rec_test(R, r, tmin, best_t, t)) { best_t = t; best = ri; tmax_f = __double2float_ru(t); }
+            }
+        }
+        // internal children: continue with the nearest, push the rest
+        uint32_t inner = hit & imask;
+        int next = -1;
+        float next_t = FLT_MAX;
+        while (inner) {
+            int i = __ffs(inner) - 1;
+            inner &= inner - 1;
+            float t = tn[i];
+            if (t > tmax_f * T_HI) continue;
+            uint32_t ci = child_base + (byte_of(meta, i) & 31);
+            if (next < 0) { next = (int)ci; next_t = t; continue; }
+            if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return best; }
+            if (t < next_t) { st_node[sp] = (uint32_t)next; st_t[sp] = next_t; ++sp; next = (int)ci; next_t = t; }
+            else { st_node[sp] = ci; st_t[sp] = t; ++sp; }
+        }
+        if (next >= 0) { node = (uint32_t)next; continue; }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (st_t[sp] <= tmax_f * T_HI) { node = st_node[sp]; found = true; break; }
+        }
+        if (!found) break;
+    }
+    return best;
+}
+
+// Any hit with t in [tmin, seg) (Scene::occluded, scene.h:2249-2271).
+__device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, double seg, int32_t* status) {
+    RayF F = make_rayf(R.o, R.d);
+    float tmin_f = __double2float_rd(tmin);
+    float tmax_f = __double2float_ru(seg);
+    uint32_t st_node[FTB_STACK];
+    int sp = 0;
+    uint32_t node = 0;
+    while (true) {
+        uint4 n[5];
+        load_node(sc.nodes, node, n);
+        float tn[8];
+        uint32_t hit = node_children(n, F, tmin_f, tmax_f, tn);
+        uint32_t imask = n[0].w >> 24;
+        uint32_t child_base = n[1].x, prim_base = n[1].y;
+        uint2 meta = make_uint2(n[1].z, n[1].w);
+        uint32_t leaves = hit & ~imask;
+        while (leaves) {
+            int i = __ffs(leaves) - 1;
+            leaves &= leaves - 1;
+            uint32_t m = byte_of(meta, i);
+            int cnt = m >> 5, off = m & 31;
+            for (int k = 0; k < cnt; ++k) {
+                PrimRec r;
+                load_rec(sc.recs, (int)prim_base + off + k, r);
+                double t;
+                if (rec_test(R, r, tmin, seg, t)) return true;
+            }
+        }
+        uint32_t inner = hit & imask;
+        int next = -1;
+        while (inner) {
+            int i = __ffs(inner) - 1;
+            inner &= inner - 1;
+            uint32_t ci = child_base + (byte_of(meta, i) & 31);
+            if (next < 0) { next = (int)ci; continue; }
+            if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return false; }
+            st_node[sp++] = ci;
+        }
+        if (next >= 0) { node = (uint32_t)next; continue; }
+        if (sp == 0) break;
+        node = st_node[--sp];
+    }
+    return false;
+}
+
+__device__ __forceinline__ RayCtx make_ray(D3 o, D3 d) {
+    RayCtx R;
+    R.o = o; R.d = d;
+    R.sh = make_shear(d);
+    R.cr = make_curve_ray(d);
+    return R;
+}
+
+// ------------------------------------------------------------------ media --------------
+__device__ __forceinline__ double med_sigma_t(const DevScene& sc, const DevMed& m, double lam) {
+    double v = spec_eval(sc, m.sa, lam) + spec_eval(sc, m.ss, lam);
+    return v > 0.0 ? v : 0.0;
+}
+__device__ __forceinline__ double med_albedo(const DevScene& sc, const DevMed& m, double lam) {
+    double s = spec_eval(sc, m.ss, lam); s = s > 0.0 ? s : 0.0;
+    double a = spec_eval(sc, m.sa, lam);
+    double t = s + (a > 0.0 ? a : 0.0);
+    return t > 0.0 ? s / t : 0.0;
+}
+// Medium::clipToBounds (scene.h:655-685)
+__device__ bool clip_to_bounds(const DevMed& m, D3 o, D3 d, double t0, double t1, double& ta, double& tb) {
+    if (m.bound == FTB_BOUND_NONE) { ta = t0; tb = t1; return t1 > t0; }
+    if (m.bound == FTB_BOUND_SPHERE) {
+        D3 oc = o - ld3(m.center);
+        double A = dot(d, d);
+        double B = 2.0 * dot(oc, d);
+        double C = dot(oc, oc) - m.radius * m.radius;
+        double disc = B * B - 4.0 * A * C;
+        if (disc <= 0.0 || A <= 0.0) return false;
+        double sd = sqrt(disc);
+        double s0 = (-B - sd) / (2.0 * A), s1 = (-B + sd) / (2.0 * A);
+        double lo = t0 > s0 ? t0 : s0, hi = t1 < s1 ? t1 : s1;
+        if (lo > hi) return false;
+        ta = lo; tb = hi; return tb > ta;
+    }
+    double lo = t0, hi = t1;
+    for (int a = 0; a < 3; ++a) {
+        double oa = comp(o, a), da = comp(d, a);
+        double mn = m.bmin[a], mx = m.bmax[a];
+        if (fabs(da) < 1e-12) { if (oa < mn || oa > mx) return false; continue; }
+        double inv = 1.0 / da;
+        double s0 = (mn - oa) * inv, s1 = (mx - oa) * inv;
+        if (s0 > s1) { double t = s0; s0 = s1; s1 = t; }
+        lo = (lo < s0) ? s0 : lo;
+        hi = (s1 < hi) ? s1 : hi;
+        if (lo > hi) return false;
+    }
+    ta = lo; tb = hi; return tb > ta;
+}
+// sampleMediaCollision, homogeneous (render.h:377-398, 444-458)
+__device__ bool sample_media_collision(const DevScene& sc, D3 o, D3 d, double dmax, double lam, Pcg& rng,
+                                       double& thit, int& which) {
+    double best = dmax; int w = -1;
+    for (int i = 0; i < sc.n_med; ++i) {
+        const DevMed& m = sc.med[i];
+        double st = med_sigma_t(sc, m, lam);
+        if (st <= 0.0) continue;
+        double ta, tb;
+        if (!clip_to_bounds(m, o, d, 0.0, dmax, ta, tb)) continue;
+        double t = ta - log(1.0 - uniform(rng)) / st;
+        if (t < tb && t < best) { best = t; w = i; }
+    }
+    if (w < 0) return false;
+    thit = best; which = w; return true;
+}
+// mediaTransmittance, homogeneous (render.h:403-421, 461-469)
+__device__ double media_transmittance(const DevScene& sc, D3 o, D3 d, double dist, double lam) {
+    double tr = 1.0;
+    for (int i = 0; i < sc.n_med; ++i) {
+        const DevMed& m = sc.med[i];
+        double st = med_sigma_t(sc, m, lam);
+        double mt = 1.0;
+        if (st > 0.0) {
+            double ta, tb;
+            if (clip_to_bounds(m, o, d, 0.0, dist, ta, tb)) mt = exp(-st * (tb - ta));
+        }
+        tr *= mt;
+        if (tr <= 0.0) break;
+    }
+    return tr;
+}
+
+// ------------------------------------------------------------------ camera -------------
+// Camera::project, rectilinear (camera.h:137-151)
+__device__ __forceinline__ bool cam_project(const DevCam& c, D3 p, int& px, int& py, double& cos_cam,
+                                            double& dist2) {
+    D3 d = p - ld3(c.eye);
+    double cz = dot(d, ld3(c.w));
+    if (cz <= 1e-9) return false;
+    double cx = dot(d, ld3(c.u)), cy = dot(d, ld3(c.v));
+    double ix = (cx / cz) / c.thx - 0.0;
+    double iy = (cy / cz) / c.thy;
+    if (ix < -1 || ix >= 1 || iy < -1 || iy >= 1) return false;
+    px = (int)((ix * 0.5 + 0.5) * c.rx);
+    py = (int)((iy * 0.5 + 0.5) * c.ry);
+    dist2 = dot(d, d);
+    cos_cam = cz / sqrt(dist2);
+    return true;
+}
+__device__ __forceinline__ double cam_pixel_solid_angle(const DevCam& c, double cos_cam) {
+    double ipa = 4.0 * c.thx * c.thy;
+    double ppa = ipa / ((double)c.rx * (double)c.ry);
+    return ppa * cos_cam * cos_cam * cos_cam;
+}
+
+// geometry.h:174-242
+__device__ __forceinline__ D3 oriented_geo_n(const Hit& h) { return (dot(h.ng, h.n) >= 0.0) ? h.ng : neg(h.ng); }
+__device__ __forceinline__ double shading_adjoint_corr(D3 wi, D3 wo, D3 ns, D3 ng) {
+    double denom = fabs(dot(wi, ng)) * fabs(dot(wo, ns));
+    if (denom <= 1e-8) return 1.0;
+    double num = fabs(dot(wi, ns)) * fabs(dot(wo, ng));
+    return num / denom;
+}
+__device__ __forceinline__ double shadow_terminator_g(D3 wi, D3 ns, D3 ng) {
+    double cos_ng_ns = dot(ng, ns);
+    if (cos_ng_ns >= 1.0 - 1e-7) return (dot(ng, wi) > 0.0) ? 1.0 : 0.0;
+    double cos_ng_wi = dot(ng, wi);
+    if (cos_ng_wi <= 0.0) return 0.0;
+    double denom = dot(ns, wi) * cos_ng_ns;
+    if (denom <= 1e-8) return 1.0;
+    double g = cos_ng_wi / denom;
+    if (g >= 1.0) return 1.0;
+    return g * g * (1.0 - g) + g;
+}
+
+// ------------------------------------------------------------------ shadow queue -------
+__device__ __forceinline__ int agg_inc(int32_t* ctr) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, (int)g.size());
+    return g.shfl(base, 0) + (int)g.thread_rank();
+}
+
+__device__ __forceinline__ void push_shadow(const Wave& w, const Frame& f, D3 o, D3 d, double tmax, double val,
+                                            double lam, int pix) {
+    int i = agg_inc(&w.counts[2]);
+    if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
+    w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
+    w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
+    w.smax[i] = tmax; w.sval[i] = val; w.slam[i] = lam; w.spix[i] = pix;
+}
+
+// connectGeom + connect, model B (render.h:499-559); the occlusion test is deferred to
+// k_shadow, the rest of the contribution is formed here in the reference's order.
+__device__ void connect_surface(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f, D3 p,
+                                D3 n, D3 ng, D3 wi, double lam, double beta, double rho) {
+    D3 to_cam = ld3(cam.eye) - p;
+    double dist = len(to_cam);
+    D3 wdir = to_cam / dist;
+    double cos_surf = dot(n, wdir);
+    if (cos_surf <= 0) return;
+    double stg = shadow_terminator_g(wdir, n, ng);
+    if (stg <= 0.0) return;
+    int px, py; double cos_cam, dist2;
+    if (!cam_project(cam, p, px, py, cos_cam, dist2)) return;
+    double omega = cam_pixel_solid_angle(cam, cos_cam);
+    double corr = shading_adjoint_corr(wi, wdir, n, ng);
+    double denom = dist2 * omega;
+    double fr = rho / PI_D;
+    double contrib = beta * fr * cos_surf * corr / denom * stg;
+    if (sc.n_med > 0) contrib *= media_transmittance(sc, p, wdir, dist, lam);
+    push_shadow(w, f, p + ng * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+}
+// connectVolume (render.h:584-600)
+__device__ void connect_volume(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f,
+                               const DevMed& m, D3 p, D3 win, double lam, double beta) {
+    D3 to_cam = ld3(cam.eye) - p;
+    double dist = len(to_cam);
+    D3 wdir = to_cam / dist;
+    int px, py; double cos_cam, dist2;
+    if (!cam_project(cam, p, px, py, cos_cam, dist2)) return;
+    double ph = hg_phase(dot(win, wdir), m.g);
+    double alb = med_albedo(sc, m, lam);
+    double omega = cam_pixel_solid_angle(cam, cos_cam);
+    double contrib = beta * alb * ph / (dist2 * omega);
+    contrib *= media_transmittance(sc, p, wdir, dist, lam);
+    push_shadow(w, f, p + wdir * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+}
+
+// ------------------------------------------------------------------ tallies ------------
+__device__ __forceinline__ long long to_fixed(double v, double scale_inv, int32_t* status) {
+    double s = v * scale_inv;
+    if (!(fabs(s) < 4.611686018427388e18)) {   // 2^62
+        atomicOr(status, ST_FILM_SATURATED);
+        return 0;
+    }
+    return __double2ll_rn(s);
+}
+
+// Sum a per-thread value over the block and add it to a global tally once per block.
+__device__ void block_tally(unsigned long long* dst, long long v) {
+    __shared__ long long red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        long long s = lane < nw ? red[lane] : 0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0 && s != 0) atomicAdd(dst, (unsigned long long)s);
+    }
+}
+
+enum { T_EMIT = 0, T_ABS = 1, T_SENSOR = 2, T_ESC = 3, T_RES = 4 };
+
+__device__ __forceinline__ uint64_t fnv_i32(uint64_t h, int32_t v) {
+    uint32_t u = (uint32_t)v;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { h ^= (u >> (8 * i)) & 0xffu; h *= 1099511628211ULL; }
+    return h;
+}
+
+// Per-slot instrumentation (parity tests only).
+__device__ __forceinline__ void log_finish(const Wave& w, int slot, uint64_t photon, int fate, double beta) {
+    if (!w.logs) return;
+    ftb_photon_log& L = w.logs[photon - (uint64_t)w.log_base];
+    L.n_hits = w.lnh[slot];
+    L.fate = fate;
+    L.prim_hash = w.lhash[slot];
+    L.beta = beta;
+    for (int k = 0; k < 8; ++k) L.prims[k] = w.lprims[k * w.W + slot];
+}
+
+// ------------------------------------------------------------------ kernels ------------
+__global__ void __launch_bounds__(128) k_emit(DevScene sc, DevCam cam, Wave w, Frame f, uint64_t photon0,
+                                              int32_t n, int32_t max_bounce) {
+    long long t_emit = 0, t_res = 0;
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        uint64_t k = photon0 + (uint64_t)slot;
+        Pcg rng = seed_photon(k);
+        if (w.logs) {
+            w.lhash[slot] = 1469598103934665603ULL; w.lnh[slot] = 0;
+            for (int q = 0; q < 8; ++q) w.lprims[q * w.W + slot] = -2;
+        }
+        if (sc.total_power <= 0.0 || sc.n_emit == 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        int ei = 0;
+        if (sc.n_emit > 1) {   // Scene::selectEmitter (scene.h:1851-1857)
+            double u = uniform(rng);
+            int lo = 0, hi = sc.n_emit - 1;
+            while (lo < hi) { int mid = (lo + hi) / 2; if (sc.emit_cdf[mid] < u) lo = mid + 1; else hi = mid; }
+            ei = lo;
+        }
+        const DevEmit& em = sc.emit[ei];
+        double u1 = uniform(rng), u2 = uniform(rng);
+        D3 origin, emit_n;
+        if (em.shape == FTB_EMIT_SPHERE) {   // Emitter::samplePoint (scene.h:815-880)
+            double z = 1.0 - 2.0 * u1;
+            double s = 1.0 - z * z;
+            double r = sqrt(s > 0.0 ? s : 0.0);
+            double phi = 2.0 * PI_D * u2;
+            D3 d = mk(r * cos(phi), r * sin(phi), z);
+            emit_n = d;
+            origin = ld3(em.origin) + d * em.radius;
+        } else {
+            origin = ld3(em.origin) + ld3(em.u) * u1 + ld3(em.v) * u2;
+            emit_n = ld3(em.normal);
+        }
+        D3 dir = em.collimated ? ld3(em.beam) : cosine_hemisphere(emit_n, rng);
+        // EmissionSampler::sampleAt (spectrum.h:374-383)
+        double u = uniform(rng);
+        int lo = 0, hi = em.n;
+        while (lo + 1 < hi) { int mid = (lo + hi) / 2; if (em.cdf[mid] <= u) lo = mid; else hi = mid; }
+        double c0 = em.cdf[lo], c1 = em.cdf[lo + 1];
+        double frac = (c1 > c0) ? (u - c0) / (c1 - c0) : 0.5;
+        double lam = LAMBDA_MIN + (lo + frac) * em.step;
+        double pdf = (c1 - c0) / em.step;
+        if (pdf <= 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
+        beta *= 1.0;
+        t_emit += to_fixed(beta, f.tally_scale_inv, f.status);
+        connect_surface(sc, cam, w, f, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
+        D3 ro = origin + dir * 1e-6;
+        if (max_bounce <= 0) {
+            t_res += to_fixed(beta, f.tally_scale_inv, f.status);
+            log_finish(w, slot, k, 2, beta);
+            continue;
+        }
+        w.rng_s[slot] = rng.s; w.rng_i[slot] = rng.inc;
+        w.ox[slot] = ro.x; w.oy[slot] = ro.y; w.oz[slot] = ro.z;
+        w.dx[slot] = dir.x; w.dy[slot] = dir.y; w.dz[slot] = dir.z;
+        w.lam[slot] = lam; w.beta[slot] = beta;
+        w.stk_n[slot] = 0;
+        int q = agg_inc(&w.counts[0]);
+        w.qa[q] = slot;
+    }
+    block_tally(&f.tally[T_EMIT], t_emit);
+    block_tally(&f.tally[T_RES], t_res);
+}
+
+__global__ void __launch_bounds__(128) k_extend(DevScene sc, Wave w, const int32_t* q, const int32_t* qcount,
+                                                int32_t* status) {
+    int nq = *qcount;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+        int slot = q[i];
+        RayCtx R = make_ray(mk(w.ox[slot], w.oy[slot], w.oz[slot]), mk(w.dx[slot], w.dy[slot], w.dz[slot]));
+        double t;
+        int rec = traverse_closest(sc, R, EPS_RAY, t, status);
+        w.hit_t[slot] = t;
+        w.hit_rec[slot] = rec;
+    }
+}
+
+// medium stack (medium_stack.h:17-47), kStkCap entries per slot
+struct Stk { int n; int2 e[kStkCap]; };
+__device__ __forceinline__ int stk_top_pri(const Stk& s) {
+    int bp = INT_MIN;
+    for (int i = 0; i < s.n; ++i) if (s.e[i].y > bp) bp = s.e[i].y;
+    return s.n ? bp : INT_MIN;
+}
+__device__ __forceinline__ int stk_top_mat(const Stk& s) {
+    int bp = INT_MIN, bm = -1;
+    for (int i = 0; i < s.n; ++i) if (s.e[i].y >= bp) { bp = s.e[i].y; bm = s.e[i].x; }
+    return bm;
+}
+__device__ __forceinline__ void stk_push(Stk& s, int mi, int p, int32_t* status) {
+    if (s.n < kStkCap) { s.e[s.n] = make_int2(mi, p); ++s.n; }
+    else atomicOr(status, ST_MEDIUM_STACK);
+}
+__device__ __forceinline__ void stk_pop_mat(Stk& s, int mi) {
+    for (int i = s.n - 1; i >= 0; --i)
+        if (s.e[i].x == mi) {
+            for (int j = i; j < s.n - 1; ++j) s.e[j] = s.e[j + 1];
+            --s.n; return;
+        }
+}
+
+__device__ __forceinline__ double mat_ior(const DevScene& sc, const DevMat& m, double lam) {
+    return m.ior >= 0 ? spec_eval(sc, m.ior, lam) : 1.5;
+}
+
+// refractOrReflect, stochastic branch (render.h:2657-2697)
+__device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hit& h, D3 d, double lam,
+                                   Pcg& rng, bool& transmitted, double ext_ior, D3& o_out, D3& d_out) {
+    double ngi = mat_ior(sc, m, lam);
+    bool entering = dot(d, h.ng) < 0.0;
+    D3 nl = entering ? h.ng : neg(h.ng);
+    double n1 = entering ? ext_ior : ngi;
+    double n2 = entering ? ngi : ext_ior;
+    double eta = n1 / n2;
+    double cos_i = -dot(d, nl);
+    double sin2t = eta * eta * (1.0 - cos_i * cos_i);
+    D3 out;
+    bool refracted = false;
+    if (sin2t > 1.0) out = reflect(d, nl);
+    else {
+        double cos_t = sqrt(1.0 - sin2t);
+        double rs = (n1 * cos_i - n2 * cos_t) / (n1 * cos_i + n2 * cos_t);
+        double rp = (n1 * cos_t - n2 * cos_i) / (n1 * cos_t + n2 * cos_i);
+        double R = 0.5 * (rs * rs + rp * rp);
+        if (uniform(rng) < R) out = reflect(d, nl);
+        else { out = d * eta + nl * (eta * cos_i - cos_t); refracted = true; }
+    }
+    out = normalize(out);
+    if (m.roughness > 1e-3) {
+        D3 pert = sample_glossy(out, m.roughness, rng);
+        bool ok = refracted ? (dot(pert, nl) < 0.0) : (dot(pert, nl) > 0.0);
+        if (ok) out = pert;
+    }
+    transmitted = refracted;
+    o_out = h.p + out * 1e-6;
+    d_out = out;
+}
+
+// One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
+__global__ void __launch_bounds__(128) k_shade(DevScene sc, DevCam cam, Wave w, Frame f, const int32_t* qin,
+                                               const int32_t* qin_count, int32_t* qout, int32_t* qout_count,
+                                               uint64_t photon0, int32_t bounce, int32_t max_bounce) {
+    long long t_abs = 0, t_esc = 0, t_res = 0;
+    int nq = *qin_count;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+        int slot = qin[i];
+        Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
+        D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
+        double lam = w.lam[slot], beta = w.beta[slot];
+        double ht = w.hit_t[slot];
+        int rec = w.hit_rec[slot];
+        Stk stk; stk.n = w.stk_n[slot];
+        for (int k = 0; k < stk.n; ++k) stk.e[k] = w.stk[k * w.W + slot];
+        if (w.logs) {
+            int nh = w.lnh[slot];
+            int prim = rec >= 0 ? sc.recs[rec].prim : -1;
+            w.lhash[slot] = fnv_i32(w.lhash[slot], prim);
+            if (nh < 8) w.lprims[nh * w.W + slot] = prim;
+            w.lnh[slot] = nh + 1;
+        }
+        int fate = -1;   // -1 continue, 0 absorbed, 1 escaped
+        bool valid = rec >= 0;
+        double d_surf = valid ? ht : 1e30;
+        double d_event = d_surf;
+        bool medium_event = false;
+        int scatter_med = -1;
+        D3 mp = mk(0, 0, 0);
+        if (sc.n_med > 0) {
+            double tm; int which;
+            if (sample_media_collision(sc, ro, rd, d_surf, lam, rng, tm, which)) {
+                d_event = tm; medium_event = true; scatter_med = which; mp = ro + rd * tm;
+            }
+        }
+        {   // Beer-Lambert inside the current dielectric (render.h:2063-2066)
+            int mi = stk_top_mat(stk);
+            double a = (mi >= 0) ? spec_slot(sc, sc.mats[mi].absorb, lam, 0.0) : 0.0;
+            if (a > 0.0) beta *= exp(-a * d_event);
+        }
+        D3 no = ro, nd = rd;
+        if (medium_event) {   // render.h:2105-2115
+            const DevMed& sm = sc.med[scatter_med];
+            connect_volume(sc, cam, w, f, sm, mp, rd, lam, beta);
+            if (uniform(rng) >= med_albedo(sc, sm, lam)) fate = 0;
+            else { nd = sample_hg(rd, sm.g, rng); no = mp; }
+        } else if (!valid) {
+            fate = 1;
+        } else {
+            PrimRec r;
+            load_rec(sc.recs, rec, r);
+            RayCtx R = make_ray(ro, rd);
+            Hit h;
+            hit_attributes(sc, R, r, h);
+            const DevMat& m = sc.mats[h.mat];
+            switch (m.type) {
+            case FTB_MAT_DIELECTRIC: {   // render.h:1612-1660
+                bool entering = dot(rd, h.ng) < 0.0;
+                int mi = h.mat, pr = m.priority;
+                bool has_pri = pr != INT_MIN;
+                bool transmitted = false;
+                if (entering) {
+                    int out_mat = stk_top_mat(stk), out_pri = stk_top_pri(stk);
+                    bool ranked = has_pri && (stk.n == 0 || (out_mat >= 0 && sc.mats[out_mat].priority != INT_MIN));
+                    if (ranked && stk.n != 0 && pr <= out_pri) {
+                        stk_push(stk, mi, pr, f.status);
+                        no = h.p + rd * 1e-6;
+                    } else {
+                        double ext = (ranked && out_mat >= 0) ? mat_ior(sc, sc.mats[out_mat], lam) : 1.0;
+                        refract_or_reflect(sc, m, h, rd, lam, rng, transmitted, ext, no, nd);
+                        if (transmitted) stk_push(stk, mi, pr, f.status);
+                    }
+                } else {
+                    Stk after = stk;
+                    stk_pop_mat(after, mi);
+                    int new_mat = stk_top_mat(after), new_pri = stk_top_pri(after);
+                    bool ranked = has_pri && (after.n == 0 || (new_mat >= 0 && sc.mats[new_mat].priority != INT_MIN));
+                    if (ranked && new_mat >= 0 && pr <= new_pri) {
+                        stk_pop_mat(stk, mi);
+                        no = h.p + rd * 1e-6;
+                    } else {
+                        double ext = (ranked && new_mat >= 0) ? mat_ior(sc, sc.mats[new_mat], lam) : 1.0;
+                        refract_or_reflect(sc, m, h, rd, lam, rng, transmitted, ext, no, nd);
+                        if (transmitted) stk_pop_mat(stk, mi);
+                    }
+                }
+                break;
+            }
+            case FTB_MAT_GLOSSY: {   // render.h:1725-1733
+                double rr = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
+                if (uniform(rng) >= rr) { fate = 0; break; }
+                D3 o = sample_glossy(reflect(rd, h.n), m.roughness, rng);
+                if (dot(o, h.n) <= 0) { fate = 0; break; }
+                no = h.p + h.n * 1e-6; nd = o;
+                break;
+            }
+            case FTB_MAT_FILTER: {   // render.h:1711-1723
+                double tt = clamp01(spec_slot(sc, m.transmit, lam, 0.0));
+                if (uniform(rng) >= tt) { fate = 0; break; }
+                no = h.p + rd * 1e-6;
+                break;
+            }
+            case FTB_MAT_DIFFUSE_TRANSMIT: {   // render.h:2180-2212
+                double rr = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
+                double rt = clamp01(spec_slot(sc, m.transmit, lam, 0.0));
+                double sum = rr + rt;
+                if (sum > 1.0) { rr /= sum; rt /= sum; sum = 1.0; }
+                D3 ngo = oriented_geo_n(h);
+                D3 wi = mk(-rd.x, -rd.y, -rd.z);
+                connect_surface(sc, cam, w, f, h.p, h.n, ngo, wi, lam, beta, rr);
+                connect_surface(sc, cam, w, f, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
+                double u = uniform(rng);
+                if (u < rr) {
+                    D3 wo = cosine_hemisphere(h.n, rng);
+                    beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
+                    no = h.p + h.n * 1e-6; nd = wo;
+                } else if (u < sum) {
+                    D3 wo = cosine_hemisphere(mk(-h.n.x, -h.n.y, -h.n.z), rng);
+                    beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
+                    no = h.p - h.n * 1e-6; nd = wo;
+                } else fate = 0;
+                break;
+            }
+            default: {   // Diffuse (render.h:2215-2236)
+                double rho = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
+                D3 ngo = oriented_geo_n(h);
+                D3 wi = mk(-rd.x, -rd.y, -rd.z);
+                connect_surface(sc, cam, w, f, h.p, h.n, ngo, wi, lam, beta, rho);
+                if (uniform(rng) >= rho) { fate = 0; break; }
+                D3 wo = cosine_hemisphere(h.n, rng);
+                beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
+                no = h.p + h.n * 1e-6; nd = wo;
+                break;
+            }
+            }
+        }
+        uint64_t photon = photon0 + (uint64_t)slot;
+        if (fate == 0) { t_abs += to_fixed(beta, f.tally_scale_inv, f.status); log_finish(w, slot, photon, 0, beta); continue; }
+        if (fate == 1) { t_esc += to_fixed(beta, f.tally_scale_inv, f.status); log_finish(w, slot, photon, 1, beta); continue; }
+        if (bounce + 1 >= max_bounce) {
+            t_res += to_fixed(beta, f.tally_scale_inv, f.status);
+            log_finish(w, slot, photon, 2, beta);
+            continue;
+        }
+        w.rng_s[slot] = rng.s;
+        w.ox[slot] = no.x; w.oy[slot] = no.y; w.oz[slot] = no.z;
+        w.dx[slot] = nd.x; w.dy[slot] = nd.y; w.dz[slot] = nd.z;
+        w.beta[slot] = beta;
+        w.stk_n[slot] = stk.n;
+        for (int k = 0; k < stk.n; ++k) w.stk[k * w.W + slot] = stk.e[k];
+        int qi = agg_inc(qout_count);
+        qout[qi] = slot;
+    }
+    block_tally(&f.tally[T_ABS], t_abs);
+    block_tally(&f.tally[T_ESC], t_esc);
+    block_tally(&f.tally[T_RES], t_res);
+}
+
+// Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
+__global__ void __launch_bounds__(128) k_shadow(DevScene sc, Wave w, Frame f) {
+    int n = w.counts[2];
+    if (n > w.S) n = w.S;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
+        double max_dist = w.smax[i];
+        RayCtx R = make_ray(o, d);
+        if (traverse_any(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status)) continue;
+        double lam = w.slam[i], c = w.sval[i];
+        double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
+        long long* px = reinterpret_cast<long long*>(f.film) + 4 * (size_t)w.spix[i];
+        atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, f.film_scale_inv, f.status));
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, f.film_scale_inv, f.status));
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, f.film_scale_inv, f.status));
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
+    }
+}
+
+// ------------------------------------------------------------------ host side ----------
+namespace {
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+}
+
+size_t wave_bytes(int32_t W, bool log) {
+    size_t w = (size_t)W, s = 2 * (size_t)W;
+    size_t b = 0;
+    b += 2 * align_up(8 * w);                 // rng
+    b += 8 * align_up(8 * w);                 // ray + lam + beta
+    b += align_up(4 * w) + align_up(8 * w * kStkCap);
+    b += align_up(8 * w) + align_up(4 * w);   // hit
+    b += 2 * align_up(4 * w) + align_up(64);  // queues + counts
+    b += 9 * align_up(8 * s) + align_up(4 * s);
+    if (log) b += align_up(8 * w) + align_up(4 * w) + align_up(4 * w * 8);
+    return b;
+}
+
+cudaError_t wave_alloc(Wave& w, int32_t W, bool log) {
+    w = Wave{};
+    w.W = W;
+    w.S = 2 * W;
+    w.bytes = wave_bytes(W, log);
+    cudaError_t e = cudaMalloc(&w.block, w.bytes);
+    if (e != cudaSuccess) { w.block = nullptr; return e; }
+    char* p = (char*)w.block;
+    auto take = [&](size_t n) { void* r = p; p += align_up(n); return r; };
+    size_t wn = (size_t)W, sn = (size_t)w.S;
+    w.rng_s = (uint64_t*)take(8 * wn); w.rng_i = (uint64_t*)take(8 * wn);
+    w.ox = (double*)take(8 * wn); w.oy = (double*)take(8 * wn); w.oz = (double*)take(8 * wn);
+    w.dx = (double*)take(8 * wn); w.dy = (double*)take(8 * wn); w.dz = (double*)take(8 * wn);
+    w.lam = (double*)take(8 * wn); w.beta = (double*)take(8 * wn);
+    w.stk_n = (int32_t*)take(4 * wn); w.stk = (int2*)take(8 * wn * kStkCap);
+    w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn);
+    w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
+    w.counts = (int32_t*)take(64);
+    w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
+    w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
+    w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
+    w.spix = (int32_t*)take(4 * sn);
+    if (log) {
+        w.lhash = (uint64_t*)take(8 * wn); w.lnh = (int32_t*)take(4 * wn); w.lprims = (int32_t*)take(4 * wn * 8);
+    }
+    return cudaSuccess;
+}
+
+void wave_free(Wave& w) {
+    if (w.block) cudaFree(w.block);
+    w.block = nullptr;
+}
+
+cudaError_t launch_wave(const DevScene& sc, const DevCam& cam, Wave& w, const Frame& f, uint64_t photon0,
+                        int32_t n, int32_t max_bounce, int32_t sms, cudaStream_t st) {
+    const int T = 128;
+    int blocks_emit = (n + T - 1) / T;
+    int grid = sms * 16;   // persistent-style grid for the queue-driven kernels
+    int gq = (n + T - 1) / T;
+    if (gq < grid) grid = gq < 1 ? 1 : gq;
+    cudaMemsetAsync(w.counts, 0, 64, st);
+    k_emit<<<blocks_emit, T, 0, st>>>(sc, cam, w, f, photon0, n, max_bounce);
+    k_shadow<<<grid, T, 0, st>>>(sc, w, f);
+    cudaMemsetAsync(&w.counts[2], 0, 4, st);
+    int32_t* qa = w.qa;
+    int32_t* qb = w.qb;
+    int32_t* ca = &w.counts[0];
+    int32_t* cb = &w.counts[1];
+    for (int b = 0; b < max_bounce; ++b) {
+        k_extend<<<grid, T, 0, st>>>(sc, w, qa, ca, f.status);
+        cudaMemsetAsync(cb, 0, 4, st);
+        k_shade<<<grid, T, 0, st>>>(sc, cam, w, f, qa, ca, qb, cb, photon0, b, max_bounce);
+        k_shadow<<<grid, T, 0, st>>>(sc, w, f);
+        cudaMemsetAsync(&w.counts[2], 0, 4, st);
+        int32_t* tq = qa; qa = qb; qb = tq;
+        int32_t* tc = ca; ca = cb; cb = tc;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace ftb

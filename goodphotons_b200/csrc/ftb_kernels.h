@@ -1,0 +1,63 @@
+// ftb_kernels.h -- host-callable launch API of the wavefront kernels (ftb_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ftb200.h"
+#include "ftb_layout.h"
+
+namespace ftb {
+
+// Device status word bits (Frame::status); any nonzero value fails the render.
+enum : int32_t {
+    ST_STACK_OVERFLOW = 1,    // traversal stack exhausted
+    ST_FILM_SATURATED = 2,    // a splat exceeded the fixed-point range
+    ST_MEDIUM_STACK = 4,      // nested-dielectric stack deeper than kStkCap
+    ST_QUEUE_OVERFLOW = 8     // shadow queue capacity exceeded
+};
+
+constexpr int kStkCap = 4;
+
+// Per-wave path state, queues and shadow-ray records (structure of arrays, W slots).
+struct Wave {
+    int32_t W;                 // slots
+    int32_t S;                 // shadow-record capacity
+    uint64_t* rng_s; uint64_t* rng_i;
+    double *ox, *oy, *oz, *dx, *dy, *dz, *lam, *beta;
+    int32_t* stk_n;            // medium-stack depth per slot
+    int2* stk;                 // [kStkCap][W] (material, priority)
+    double* hit_t;
+    int32_t* hit_rec;
+    int32_t* qa;               // active slot lists (ping-pong)
+    int32_t* qb;
+    int32_t* counts;           // [0] qa count, [1] qb count, [2] shadow count
+    double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
+    int32_t* spix;
+    // parity instrumentation (null unless logging)
+    uint64_t* lhash;
+    int32_t* lnh;
+    int32_t* lprims;           // [8][W]
+    ftb_photon_log* logs;      // output, indexed by photon - log_base
+    int64_t log_base;
+    void* block;               // the single allocation backing everything above
+    size_t bytes;
+};
+
+struct Frame {
+    int64_t* film;             // 4 words per pixel
+    unsigned long long* tally; // 5 fixed-point energy tallies
+    int32_t* status;
+    double film_scale_inv;     // 2^frac / power_ref
+    double tally_scale_inv;    // 2^32 / power_ref
+};
+
+size_t wave_bytes(int32_t W, bool log);
+cudaError_t wave_alloc(Wave& w, int32_t W, bool log);
+void wave_free(Wave& w);
+
+// Trace photons [photon0, photon0+n) (n <= W) through all bounces on `stream`.
+cudaError_t launch_wave(const DevScene& sc, const DevCam& cam, Wave& w, const Frame& f,
+                        uint64_t photon0, int32_t n, int32_t max_bounce, int32_t sms,
+                        cudaStream_t stream);
+
+}  // namespace ftb

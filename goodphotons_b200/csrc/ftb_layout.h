@@ -1,0 +1,95 @@
+// ftb_layout.h -- device-resident data layout shared by the host baker (ftb_api.cpp,
+// bvh_build.cpp) and the kernels (ftb_kernels.cu).
+//
+// HBM layout of a baked scene:
+//   nodes   : WNode[n_nodes], 80 B each, 16 B aligned -- compressed 8-wide BVH.  Child
+//             boxes are 8-bit quantized against the node's float grid (p, 2^e) and rounded
+//             outward, so the fp32 traversal never culls a primitive the exact fp64 test
+//             would accept.
+//   recs    : PrimRec[n_recs], 80 B each -- one record per primitive, in leaf order.
+//             Triangles keep their three vertices in double (the exact watertight test
+//             reads them); the last 8 B carry the global primitive index, material and
+//             type.  Leaf children of a node reference a contiguous run of records.
+//   tri_n   : optional per-triangle shading normals (9 doubles), by triangle index.
+//   spectra, tables, materials, emitters, media: small tables.
+#pragma once
+#include <stdint.h>
+
+#define FTB_WIDTH 8
+#define FTB_LEAF_MAX 4
+#define FTB_STACK 64
+
+enum { REC_TRI = 0, REC_SPHERE = 1, REC_CURVE = 2 };
+
+// meta byte of a child slot: 0 = empty; otherwise count<<5 | offset.  For an internal child
+// (imask bit set) count is 1 and offset is the child's index relative to child_base; for a
+// leaf child count is its number of records and offset is relative to prim_base.
+struct alignas(16) WNode {
+    float px, py, pz;
+    uint8_t ex, ey, ez, imask;   // exponents biased by 127 (float exponent field)
+    uint32_t child_base;
+    uint32_t prim_base;
+    uint8_t meta[8];
+    uint8_t qlo_x[8], qlo_y[8], qlo_z[8];
+    uint8_t qhi_x[8], qhi_y[8], qhi_z[8];
+};
+static_assert(sizeof(WNode) == 80, "WNode must be 80 bytes");
+
+// 80-byte primitive record.  d[9] holds two int32: prim (global index) and
+// info = mat | type << 24 | smooth << 30.
+struct alignas(16) PrimRec {
+    double d[9];
+    int32_t prim;
+    int32_t info;
+};
+static_assert(sizeof(PrimRec) == 80, "PrimRec must be 80 bytes");
+
+struct DevSpec {
+    int32_t kind, n;
+    int64_t offset;
+    double p[6];
+};
+
+struct DevMat {
+    int32_t type, priority, reflect, ior, absorb, transmit;
+    double roughness;
+};
+
+struct DevEmit {
+    int32_t shape, collimated, n, pad;
+    double step, power;
+    double origin[3], u[3], v[3], normal[3], beam[3];
+    double radius;
+    const double* cdf;
+};
+
+struct DevMed {
+    int32_t sa, ss, bound, pad;
+    double g;
+    double bmin[3], bmax[3], center[3];
+    double radius;
+};
+
+struct DevScene {
+    const WNode* nodes;
+    const PrimRec* recs;
+    const double* tri_n;      // 9 per triangle (global index) or null
+    const DevSpec* spec;
+    const double* tw;
+    const double* tv;
+    const DevMat* mats;
+    const DevEmit* emit;
+    const double* emit_cdf;   // selection CDF over emitters
+    const DevMed* med;
+    int32_t n_nodes, n_recs, n_mats, n_emit, n_med, n_spec;
+    int64_t n_tris;
+    double total_power;
+    int32_t root_is_leaf;     // scene with <= FTB_LEAF_MAX prims: root node is a leaf holder
+    int32_t pad;
+};
+
+struct DevCam {
+    double eye[3], u[3], v[3], w[3];
+    double thx, thy;
+    int32_t rx, ry;
+};

@@ -1,0 +1,187 @@
+"""Loader and thin Python wrappers over the C ABI (libftb200.so).
+
+The native library is the product; this module only binds it.  `load()` raises if the
+library is missing -- there is no Python or CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libftb200.so")
+_lib = None
+
+
+class FtbError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _sig(L, name, res, *args):
+    f = getattr(L, name)
+    f.restype = res
+    f.argtypes = list(args)
+
+
+def load(path=None):
+    """Load libftb200.so (build it with `python -m goodphotons_b200.build`)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or _LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(f"{p} is missing: run `python -m goodphotons_b200.build` first")
+    L = C.CDLL(p)
+    st = C.c_int
+    PS = C.c_void_p
+    _sig(L, "ftb_last_error", C.c_char_p)
+    _sig(L, "ftb_abi_version", C.c_int)
+    _sig(L, "ftb_available", C.c_int)
+    _sig(L, "ftb_device_name", C.c_char_p)
+    _sig(L, "ftb_mem_info", st, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t))
+    _sig(L, "ftb_forward_supported", C.c_int, C.POINTER(abi.SceneDesc))
+    _sig(L, "ftb_camera_look_at", st, C.POINTER(C.c_double), C.POINTER(C.c_double),
+         C.POINTER(C.c_double), C.c_double, C.c_int32, C.c_int32, C.POINTER(abi.Camera))
+    _sig(L, "ftb_emission_cdf", st, C.POINTER(abi.Spectrum), C.POINTER(C.c_double),
+         C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_int32,
+         C.POINTER(C.c_int32), C.POINTER(C.c_double))
+    _sig(L, "ftb_scene_create", st, C.POINTER(abi.SceneDesc), C.c_int32, C.POINTER(PS))
+    _sig(L, "ftb_scene_destroy", st, PS)
+    _sig(L, "ftb_scene_footprint", st, PS, C.c_int32, C.c_int32, C.POINTER(abi.Footprint))
+    _sig(L, "ftb_scene_power", C.c_double, PS)
+    _sig(L, "ftb_render_forward", st, PS, C.POINTER(abi.Camera), C.POINTER(abi.RenderParams),
+         C.POINTER(C.c_int64), C.POINTER(abi.FilmInfo), C.POINTER(abi.Energy))
+    _sig(L, "ftb_render_forward_device", st, PS, C.POINTER(abi.Camera),
+         C.POINTER(abi.RenderParams), C.c_void_p, C.POINTER(abi.FilmInfo),
+         C.POINTER(abi.Energy), C.c_void_p)
+    _sig(L, "ftb_session_begin", st, PS, C.POINTER(abi.Camera), C.c_int32, C.c_int32,
+         C.c_int32, C.POINTER(PS))
+    _sig(L, "ftb_session_batch", st, PS, C.c_int64, C.c_uint64)
+    _sig(L, "ftb_session_hits0", st, PS, C.POINTER(C.c_double))
+    _sig(L, "ftb_session_download", st, PS, C.c_int32, C.POINTER(C.c_int64),
+         C.POINTER(abi.FilmInfo), C.POINTER(abi.Energy))
+    _sig(L, "ftb_session_end", st, PS)
+    _sig(L, "ftb_trace_log", st, PS, C.POINTER(abi.Camera), C.POINTER(abi.RenderParams),
+         C.POINTER(abi.PhotonLog))
+    w = _Lib(L)
+    if path is None:
+        _lib = w
+    return w
+
+
+class _Lib:
+    """Pythonic view of the entry points (raises FtbError on a nonzero status)."""
+
+    def __init__(self, L):
+        self.L = L
+
+    def check(self, status):
+        if status != 0:
+            raise FtbError(status, self.L.ftb_last_error().decode())
+
+    def available(self):
+        return bool(self.L.ftb_available())
+
+    def device_name(self):
+        return self.L.ftb_device_name().decode()
+
+    def look_at(self, eye, target, up, fov, rx, ry):
+        cam = abi.Camera()
+        a = lambda v: (C.c_double * 3)(*v)
+        self.check(self.L.ftb_camera_look_at(a(eye), a(target), a(up), float(fov), rx, ry,
+                                             C.byref(cam)))
+        return cam
+
+    def emission_cdf(self, desc, spec, step):
+        s = desc.spectra[spec]
+        cap = int((830.0 - 360.0) / step) + 2
+        out = np.zeros(cap, dtype=np.float64)
+        n = C.c_int32()
+        integral = C.c_double()
+        tw = desc.table_w.ctypes.data_as(C.POINTER(C.c_double)) if len(desc.table_w) else None
+        tv = desc.table_v.ctypes.data_as(C.POINTER(C.c_double)) if len(desc.table_v) else None
+        self.check(self.L.ftb_emission_cdf(C.byref(s), tw, tv, float(step),
+                                           out.ctypes.data_as(C.POINTER(C.c_double)), cap,
+                                           C.byref(n), C.byref(integral)))
+        return out[: n.value + 1].copy(), integral.value
+
+    def supported(self, desc):
+        r = self.L.ftb_forward_supported(desc.ref())
+        return r, self.L.ftb_last_error().decode()
+
+
+class Scene:
+    """A baked, device-resident scene (ftb_scene_create)."""
+
+    def __init__(self, desc, device=0, lib=None):
+        self.lib = lib or load()
+        self.desc = desc
+        h = C.c_void_p()
+        self.lib.check(self.lib.L.ftb_scene_create(desc.ref(), device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.L.ftb_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def power(self):
+        return self.lib.L.ftb_scene_power(self.h)
+
+    def footprint(self, rx, ry):
+        fp = abi.Footprint()
+        self.lib.check(self.lib.L.ftb_scene_footprint(self.h, rx, ry, C.byref(fp)))
+        return fp
+
+    def render(self, cam, n, seed_base=0, max_bounce=8, frac_bits=0):
+        """One-shot render into a host film: returns (film int64 [ry, rx, 4], info, energy)."""
+        film = np.zeros((cam.res_y, cam.res_x, 4), dtype=np.int64)
+        p = abi.RenderParams(n, seed_base, max_bounce, frac_bits)
+        info, en = abi.FilmInfo(), abi.Energy()
+        self.lib.check(self.lib.L.ftb_render_forward(
+            self.h, C.byref(cam), C.byref(p), film.ctypes.data_as(C.POINTER(C.c_int64)),
+            C.byref(info), C.byref(en)))
+        return film, info, en
+
+    def render_device(self, cam, n, d_film_ptr, seed_base=0, max_bounce=8, frac_bits=0,
+                      stream=None, want_energy=False):
+        p = abi.RenderParams(n, seed_base, max_bounce, frac_bits)
+        info = abi.FilmInfo()
+        en = abi.Energy() if want_energy else None
+        self.lib.check(self.lib.L.ftb_render_forward_device(
+            self.h, C.byref(cam), C.byref(p), C.c_void_p(d_film_ptr), C.byref(info),
+            C.byref(en) if en is not None else None, C.c_void_p(stream or 0)))
+        return info, en
+
+    def trace_log(self, cam, n, seed_base=0, max_bounce=8):
+        logs = (abi.PhotonLog * max(1, n))()
+        p = abi.RenderParams(n, seed_base, max_bounce, 0)
+        self.lib.check(self.lib.L.ftb_trace_log(self.h, C.byref(cam), C.byref(p), logs))
+        return logs_to_numpy(logs, n)
+
+
+def logs_to_numpy(logs, n):
+    raw = np.ctypeslib.as_array(C.cast(logs, C.POINTER(C.c_uint8)), shape=(n * C.sizeof(abi.PhotonLog),))
+    dt = np.dtype([("n_hits", "<i4"), ("fate", "<i4"), ("prim_hash", "<u8"), ("beta", "<f8"),
+                   ("prims", "<i4", (8,))])
+    assert dt.itemsize == C.sizeof(abi.PhotonLog)
+    return np.frombuffer(raw.tobytes(), dtype=dt).copy()
+
+
+def film_to_xyz(film, info):
+    """int64 fixed-point film -> absolute XYZ sums (reference Film::xyz) and hits."""
+    xyz = film[..., :3].astype(np.float64) * info.scale
+    hits = film[..., 3].astype(np.float64)
+    return xyz, hits

@@ -1,0 +1,290 @@
+/*
+ * ftb200.h -- C ABI of the B200-native forward pinhole light tracer.
+ *
+ * This is the drop-in boundary for the ftrace (inhahe/GoodPhotons) mode-B GPU path.
+ * The reference exposes that path as a plain C++ API in src/render_cuda.h; every entry
+ * point below names the reference interface it replaces.  Unlike the reference, nothing
+ * here calls exit(): every function returns an ftb_status and the text of the last error
+ * is available from ftb_last_error() (thread-local).
+ *
+ * Conventions
+ *  - Plain pointers and sizes only; no C++ or torch types cross the boundary.
+ *  - All geometry and spectral inputs are double precision, exactly as the reference's
+ *    Scene holds them after FTSL load (scene.h), so a baked scene is bit-identical input.
+ *  - Host pointers unless the parameter name says d_ (device pointer on the scene's GPU).
+ *  - Films are 64-bit fixed point (see ftb_film_info): a pixel's sum does not depend on the
+ *    order in which photons land, so renders are bit-reproducible across launches, stream
+ *    counts and GPU counts.
+ *  - Primitive indices are global, in the reference's order (scene.h:2194-2234):
+ *    triangles, then spheres, then curve segments.
+ */
+#ifndef FTB200_H
+#define FTB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FTB_ABI_VERSION 1
+
+typedef enum ftb_status {
+    FTB_OK = 0,
+    FTB_ERR_INVALID = 1,      /* bad argument (null pointer, index out of range, ...) */
+    FTB_ERR_NO_DEVICE = 2,    /* no usable CUDA device */
+    FTB_ERR_UNSUPPORTED = 3,  /* scene uses a feature this path does not implement */
+    FTB_ERR_CUDA = 4,         /* a CUDA runtime call failed */
+    FTB_ERR_OOM = 5,          /* device allocation failed */
+    FTB_ERR_DEVICE_LIMIT = 6, /* a bounded device loop gave up (stack/queue overflow) */
+    FTB_ERR_TOO_LARGE = 7     /* request exceeds a documented maximum */
+} ftb_status;
+
+/* ---- spectra ------------------------------------------------------------------------
+ * A spectrum is a function of wavelength in nm (reference: `Spectrum`, spectrum.h:15).
+ * The kinds are the reference's closed-form builders, evaluated with the same arithmetic:
+ *   CONST      p[0]                                      constantSpectrum  spectrum.h:179
+ *   TABLE      piecewise linear over n (w,v) pairs        tabulatedSpectrum spectrum.h:264
+ *              stored at table_w/table_v[offset..offset+n), sorted by w, distinct w
+ *   CAUCHY     p[0] + p[1]/um^2                           cauchy            spectrum.h:243
+ *   SELLMEIER  p[0..5] = B1 B2 B3 C1 C2 C3                sellmeier         spectrum.h:233
+ *   BLACKBODY  Planck at p[0] kelvin, times p[1]          blackbody         spectrum.h:185
+ *              (host-side only: emission CDFs; not allowed as a material slot) */
+typedef enum ftb_spec_kind {
+    FTB_SPEC_CONST = 0,
+    FTB_SPEC_TABLE = 1,
+    FTB_SPEC_CAUCHY = 2,
+    FTB_SPEC_SELLMEIER = 3,
+    FTB_SPEC_BLACKBODY = 4
+} ftb_spec_kind;
+
+typedef struct ftb_spectrum {
+    int32_t kind;     /* ftb_spec_kind */
+    int32_t n;        /* TABLE: number of pairs */
+    int64_t offset;   /* TABLE: first pair in table_w/table_v */
+    double p[6];
+} ftb_spectrum;
+
+/* ---- materials ----------------------------------------------------------------------
+ * Type numbering equals the reference's MatType (scene.h:42) for the supported subset. */
+typedef enum ftb_mat_type {
+    FTB_MAT_DIFFUSE = 0,
+    FTB_MAT_DIELECTRIC = 1,
+    FTB_MAT_MIRROR = 2,
+    FTB_MAT_HALF_MIRROR = 3,
+    FTB_MAT_GLOSSY = 4,
+    FTB_MAT_DIFFUSE_TRANSMIT = 11,
+    FTB_MAT_FILTER = 12
+} ftb_mat_type;
+
+#define FTB_PRIORITY_UNSET INT32_MIN
+
+typedef struct ftb_material {
+    int32_t type;      /* ftb_mat_type */
+    int32_t priority;  /* nested-dielectric priority, FTB_PRIORITY_UNSET if unset */
+    int32_t reflect;   /* spectrum index: albedo / tint / reflect probability */
+    int32_t ior;       /* spectrum index: dielectric IOR (-1: constant 1.5) */
+    int32_t absorb;    /* spectrum index: interior sigma_a in 1/m (-1: none) */
+    int32_t transmit;  /* spectrum index: DiffuseTransmit albedo / Filter T (-1: zero) */
+    double roughness;  /* glossy lobe width; dielectric frosting when > 1e-3 */
+} ftb_material;
+
+/* ---- emitters -----------------------------------------------------------------------
+ * Area emitters as registered by Scene::addAreaLight / addSphereLight (scene.h:1306-1327).
+ * The wavelength CDF is the reference's EmissionSampler (spectrum.h:352-389): cdf_n+1
+ * values over [360, 830] nm in bins of `step` nm, at emitter_cdf[cdf_offset..].  `power`
+ * is emitIntegral*area*PI (scene.h:1509).  ftb_emission_cdf() computes both from an
+ * ftb_spectrum with the reference's arithmetic. */
+typedef enum ftb_emit_shape { FTB_EMIT_QUAD = 0, FTB_EMIT_SPHERE = 1 } ftb_emit_shape;
+
+typedef struct ftb_emitter {
+    int32_t shape;       /* ftb_emit_shape */
+    int32_t collimated;  /* quad only: every photon fires along beam[] */
+    int32_t cdf_n;       /* number of bins (cdf has cdf_n+1 entries) */
+    int32_t spd;         /* spectrum index of the SPD the cdf was built from (-1: n/a) */
+    int64_t cdf_offset;  /* into emitter_cdf */
+    double step;         /* bin width in nm */
+    double power;        /* selection weight and carried beta */
+    double origin[3], u[3], v[3], normal[3];
+    double area;
+    double radius;       /* sphere */
+    double beam[3];
+} ftb_emitter;
+
+/* ---- media --------------------------------------------------------------------------
+ * Homogeneous Henyey-Greenstein media (scene.h:422-688), optionally bounded by an AABB or
+ * a sphere.  sigma_a / sigma_s are spectrum indices in 1/m. */
+typedef enum ftb_bound { FTB_BOUND_NONE = 0, FTB_BOUND_BOX = 1, FTB_BOUND_SPHERE = 2 } ftb_bound;
+
+typedef struct ftb_medium {
+    int32_t sigma_a, sigma_s;
+    int32_t bound;       /* ftb_bound */
+    int32_t pad0;
+    double g;
+    double bmin[3], bmax[3];
+    double center[3];
+    double radius;
+} ftb_medium;
+
+/* ---- scene --------------------------------------------------------------------------
+ * tri_v:    n_tris x 9 doubles (v0 v1 v2), winding defines the geometric normal
+ * tri_n:    optional n_tris x 9 doubles of per-vertex shading normals (NULL: flat);
+ *           zero-length entries fall back to the geometric normal (geometry.h:51-55)
+ * sph:      n_spheres x 4 doubles (cx cy cz r)
+ * curve:    n_curves x 10 doubles (p0[3] p1[3] r0 r1 u0 u1): round cones (curve.h:85-92) */
+typedef struct ftb_scene_desc {
+    int64_t n_tris;
+    const double* tri_v;
+    const double* tri_n;
+    const int32_t* tri_mat;
+    int64_t n_spheres;
+    const double* sph;
+    const int32_t* sph_mat;
+    int64_t n_curves;
+    const double* curve;
+    const int32_t* curve_mat;
+    int32_t n_mats;
+    int32_t n_spectra;
+    const ftb_material* mats;
+    const ftb_spectrum* spectra;
+    int64_t n_table;
+    const double* table_w;
+    const double* table_v;
+    int32_t n_emitters;
+    int32_t n_media;
+    const ftb_emitter* emitters;
+    const double* emitter_cdf;
+    const ftb_medium* media;
+} ftb_scene_desc;
+
+/* ---- camera -------------------------------------------------------------------------
+ * Rectilinear pinhole (camera.h:58-213).  ftb_camera_look_at fills it like
+ * Camera::lookAt (camera.h:110). */
+typedef struct ftb_camera {
+    double eye[3], u[3], v[3], w[3];
+    double tan_half_x, tan_half_y;
+    int32_t res_x, res_y;
+} ftb_camera;
+
+/* ---- render parameters and outputs -------------------------------------------------- */
+typedef struct ftb_render_params {
+    int64_t n_photons;    /* photons traced by this call */
+    uint64_t seed_base;   /* absolute index of the first photon (render_cuda.h:65-68) */
+    int32_t max_bounce;   /* bounce cap (reference Renderer::maxBounce, render.h:301) */
+    int32_t frac_bits;    /* film fixed-point fraction bits; <=0 picks a safe default */
+} ftb_render_params;
+
+/* Energy report (reference EnergyReport, render.h:29-31).  Each tally is the sum of the
+ * photons' carried beta, kept in 64-bit fixed point with 32 fraction bits relative to the
+ * scene's total emitted power; the doubles are that sum converted back to absolute units. */
+typedef struct ftb_energy {
+    double emitted, absorbed, sensor, escaped, residual;
+    int64_t fx[5];        /* fixed-point tallies, same order */
+} ftb_energy;
+
+/* Film layout: 4 int64 words per pixel, row-major (py*res_x+px): X, Y, Z in fixed point,
+ * then the splat count (reference Film::hits).  The absolute XYZ sum of a pixel, as the
+ * reference Film::xyz holds it, is word * scale. */
+typedef struct ftb_film_info {
+    int32_t frac_bits;
+    int32_t pad0;
+    double scale;         /* power_ref * 2^-frac_bits */
+    double power_ref;     /* scene total emitted power */
+} ftb_film_info;
+
+typedef struct ftb_scene ftb_scene;       /* device-resident baked scene */
+typedef struct ftb_session ftb_session;   /* resident film(s) + scene */
+
+/* Memory estimate for admission control (the reference has only cudaMemInfo,
+ * render_cuda.h:32, and cudaMegakernelLocalBytes, render_cuda.h:40). */
+typedef struct ftb_footprint {
+    uint64_t scene_bytes;     /* BVH + primitive records + tables */
+    uint64_t film_bytes;      /* per camera film */
+    uint64_t wave_bytes;      /* path state + queues for one in-flight wave */
+    uint64_t total_bytes;
+} ftb_footprint;
+
+/* ---- entry points ------------------------------------------------------------------- */
+
+/* Last error message of this thread ("" if none). */
+const char* ftb_last_error(void);
+int ftb_abi_version(void);
+
+/* replaces cudaAvailable() (render_cuda.h:24) */
+int ftb_available(void);
+/* replaces cudaDeviceName() (render_cuda.h:27) */
+const char* ftb_device_name(void);
+/* replaces cudaMemInfo() (render_cuda.h:32) */
+ftb_status ftb_mem_info(size_t* free_bytes, size_t* total_bytes);
+/* replaces cudaForwardSupported() (render_cuda.h:56): 1 if supported, 0 if not (reason in
+ * ftb_last_error), negative on invalid input */
+int ftb_forward_supported(const ftb_scene_desc* desc);
+
+/* Camera::lookAt (camera.h:110) */
+ftb_status ftb_camera_look_at(const double eye[3], const double target[3],
+                              const double up[3], double fov_y_deg, int32_t res_x,
+                              int32_t res_y, ftb_camera* out);
+/* EmissionSampler::build (spectrum.h:357-369) over the reference band [360, 830] nm:
+ * fills cdf[0..n] (n = (830-360)/step) and *integral; `out_cdf` must hold n+1 doubles. */
+ftb_status ftb_emission_cdf(const ftb_spectrum* spd, const double* table_w,
+                            const double* table_v, double step, double* out_cdf,
+                            int32_t out_cap, int32_t* out_n, double* integral);
+
+/* Bake + upload a scene to device `device` (replaces buildUploadScene,
+ * render_cuda.cu:12692-13546).  The descriptor is only read during the call. */
+ftb_status ftb_scene_create(const ftb_scene_desc* desc, int32_t device, ftb_scene** out);
+ftb_status ftb_scene_destroy(ftb_scene* scene);
+ftb_status ftb_scene_footprint(const ftb_scene* scene, int32_t res_x, int32_t res_y,
+                               ftb_footprint* out);
+/* Total emitted power the film and energy fixed point are relative to. */
+double ftb_scene_power(const ftb_scene* scene);
+
+/* One-shot render into a HOST film (replaces renderForwardCuda, render_cuda.h:79-82, with
+ * camMode 'B' and heroC 1).  film: res_x*res_y*4 int64 (see ftb_film_info); the call
+ * OVERWRITES it.  energy is ACCUMULATED (+=), like the reference's eOut. */
+ftb_status ftb_render_forward(ftb_scene* scene, const ftb_camera* cam,
+                              const ftb_render_params* params, int64_t* film,
+                              ftb_film_info* info, ftb_energy* energy);
+
+/* Same, accumulating into a DEVICE film the caller owns (res_x*res_y*4 int64 on the
+ * scene's device, zero it first); frac_bits must match across accumulating calls.
+ * Asynchronous on `stream` (a cudaStream_t, NULL for the legacy stream) unless
+ * energy != NULL, which synchronizes. */
+ftb_status ftb_render_forward_device(ftb_scene* scene, const ftb_camera* cam,
+                                     const ftb_render_params* params, int64_t* d_film,
+                                     ftb_film_info* info, ftb_energy* energy, void* stream);
+
+/* Resident session (replaces sharedForwardGpuBegin/Batch/Hits0/Download/End,
+ * render_cuda.h:121-143).  Films and energy stay on the device between batches. */
+ftb_status ftb_session_begin(ftb_scene* scene, const ftb_camera* cams, int32_t n_cams,
+                             int32_t max_bounce, int32_t frac_bits, ftb_session** out);
+ftb_status ftb_session_batch(ftb_session* s, int64_t n_photons, uint64_t seed_base);
+/* hits of camera 0 as doubles (reference sharedForwardGpuHits0) */
+ftb_status ftb_session_hits0(ftb_session* s, double* hits);
+/* running totals; film_c (camera c) must hold res_x*res_y*4 int64.  Replaces energy. */
+ftb_status ftb_session_download(ftb_session* s, int32_t cam, int64_t* film,
+                                ftb_film_info* info, ftb_energy* energy);
+ftb_status ftb_session_end(ftb_session* s);
+
+/* ---- parity support (test instrumentation, not used on the timed path) --------------
+ * Per-photon event record, filled by ftb_trace_log for photons
+ * [seed_base, seed_base+n): the number of closest-hit queries (bounce iterations
+ * entered), a 64-bit FNV-1a hash over the sequence of hit primitive indices (-1 for a
+ * miss), the termination (0 absorbed, 1 escaped, 2 residual, 3 sensor, 4 dropped at
+ * emission), the final beta, and the first 8 primitive indices. */
+typedef struct ftb_photon_log {
+    int32_t n_hits;
+    int32_t fate;
+    uint64_t prim_hash;
+    double beta;
+    int32_t prims[8];
+} ftb_photon_log;
+
+ftb_status ftb_trace_log(ftb_scene* scene, const ftb_camera* cam,
+                         const ftb_render_params* params, ftb_photon_log* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FTB200_H */

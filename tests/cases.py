@@ -1,0 +1,58 @@
+"""Small seeded scenes shared by the parity tests and the golden-vector script."""
+import ctypes as C
+import hashlib
+
+import numpy as np
+
+from goodphotons_b200 import abi, scenes
+
+
+def make_materials(L):
+    """Every supported branch: glossy, filter, diffuse-transmit, nested dielectrics with
+    priority / interior absorption / frosting, a Sellmeier glass, a diffuse sphere and two
+    emitters (power-CDF selection draws)."""
+    sb = scenes.SceneBuilder()
+    scenes.cornell_box(sb, boxes=False)
+    glossy = sb.material(abi.MAT_GLOSSY, reflect=sb.const(0.8), roughness=0.3)
+    sb.box((1.45, 0.5), (0.5, 0.5), 0.5, 25.0, glossy)
+    filt = sb.material(abi.MAT_FILTER, transmit=sb.table([(400, 0.2), (550, 0.9), (700, 0.3)]))
+    sb.quad((0.2, 0.1, 1.6), (0.5, 0, 0), (0, 0.8, 0), filt)
+    trans = sb.material(abi.MAT_DIFFUSE_TRANSMIT, reflect=sb.const(0.4), transmit=sb.const(0.35))
+    sb.quad((1.3, 0.2, 1.7), (0.5, 0, 0.05), (0, 0.7, 0), trans)
+    outer = sb.material(abi.MAT_DIELECTRIC, ior=sb.cauchy(1.5, 0.0042), absorb=sb.const(0.3),
+                        roughness=0.05, priority=1)
+    scenes.glass_blob(sb, level=2, center=(0.7, 0.5, 0.9), radius=0.35, amp=0.04, seed=3, mat=outer)
+    inner = sb.material(abi.MAT_DIELECTRIC,
+                        ior=sb.sellmeier(1.03961212, 0.231792344, 1.01046945, 0.00600069867,
+                                         0.0200179144, 103.560653), priority=2)
+    scenes.glass_blob(sb, level=1, center=(0.7, 0.5, 0.9), radius=0.15, amp=0.0, seed=4, mat=inner)
+    sb.sphere((1.5, 1.2, 0.6), 0.15, sb.diffuse(sb.const(0.6)))
+    sb.sphere_light((0.4, 1.5, 1.4), 0.08, sb.blackbody(3000.0, 0.5))
+    return sb.build(L)
+
+
+CASES = {
+    # name: (builder, res, photons, max_bounce, seed_base)
+    "cornell": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 0),
+    "cornell_seed": (lambda L: scenes.make_cornell(L), 32, 4096, 8, 123456789),
+    "glass": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 0),
+    "fog_strands": (lambda L: scenes.make_fog_strands(L, n_strands=500), 32, 8192, 32, 0),
+    "materials": (make_materials, 32, 8192, 16, 7),
+}
+
+
+def camera(L, res):
+    return scenes.default_camera(L, res)
+
+
+def scene_hash(d):
+    h = hashlib.sha256()
+    for a in (d.tri_v, d.tri_mat, d.sph, d.sph_mat, d.curve, d.curve_mat, d.table_w, d.table_v,
+              d.emitter_cdf):
+        h.update(np.ascontiguousarray(a).tobytes())
+    if d.tri_n is not None:
+        h.update(d.tri_n.tobytes())
+    for arr, n in ((d.mats, d.n_mats), (d.spectra, d.n_spectra), (d.emitters, d.n_emitters),
+                   (d.media, d.n_media)):
+        h.update(C.string_at(C.addressof(arr), n * C.sizeof(arr._type_)))
+    return h.hexdigest()

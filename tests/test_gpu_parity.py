@@ -1,0 +1,140 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle and the reference's
+golden vectors.
+
+Tolerances, stated here because the film is fixed point and the oracle is double:
+  * per-photon hit-primitive sequence (count + 64-bit hash) and termination: identical for
+    all but at most max(1, 1e-5 * n) photons (grazing / exact-tie allowance);
+  * per-photon final beta: relative 1e-12 (CUDA's exp/log/sin/cos may differ from glibc in
+    the last bit);
+  * film: hits identical; XYZ within (hits * quantum + 1e-10 * |value|) per pixel, where the
+    quantum is the film's fixed-point step (ftb_film_info.scale);
+  * energy report: relative 1e-9 (32-bit fraction fixed point per photon).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from goodphotons_b200 import lib, scenes
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden(name):
+    return np.load(os.path.join(GOLDEN, name), allow_pickle=False)
+
+
+@pytest.fixture(scope="module")
+def scenes_cache(gpu):
+    out = {}
+    for name, (mk, res, n, mb, seed) in cases.CASES.items():
+        d = mk(gpu)
+        out[name] = (d, lib.Scene(d, 0, gpu))
+    yield out
+    for _, s in out.values():
+        s.close()
+
+
+def assert_film_close(film, info, xyz_ref, hits_ref):
+    xyz, hits = lib.film_to_xyz(film, info)
+    np.testing.assert_array_equal(hits, hits_ref)
+    tol = hits_ref[..., None] * info.scale + 1e-10 * np.abs(xyz_ref)
+    bad = np.abs(xyz - xyz_ref) > tol
+    assert not bad.any(), f"{bad.sum()} film values differ; max |d| {np.abs(xyz - xyz_ref).max()}"
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_film_and_energy_match_reference_golden(name, scenes_cache, gpu):
+    mk, res, n, mb, seed = cases.CASES[name]
+    d, sc = scenes_cache[name]
+    g = golden(f"trace_{name}.npz")
+    assert cases.scene_hash(d) == str(g["scene_hash"])
+    cam = cases.camera(gpu, res)
+    film, info, en = sc.render(cam, n, seed_base=seed, max_bounce=mb)
+    assert_film_close(film, info, g["xyz"], g["hits"])
+    np.testing.assert_allclose(en.as_list(), g["energy"], rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_per_photon_paths_match_oracle(name, scenes_cache, gpu, oracle):
+    mk, res, _, mb, seed = cases.CASES[name]
+    d, sc = scenes_cache[name]
+    n = 1 << 15
+    cam = cases.camera(gpu, res)
+    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=mb)
+    ol = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, threads=4)["logs"]
+    # multi-threaded oracle logs are per photon, so order is by photon index either way
+    same = (gl["n_hits"] == ol["n_hits"]) & (gl["prim_hash"] == ol["prim_hash"]) & (gl["fate"] == ol["fate"])
+    allowed = max(1, int(1e-5 * n))
+    assert (~same).sum() <= allowed, f"{(~same).sum()} of {n} photon paths differ; first {np.nonzero(~same)[0][:5]}"
+    np.testing.assert_allclose(gl["beta"][same], ol["beta"][same], rtol=1e-12, atol=0)
+    np.testing.assert_array_equal(gl["prims"][same], ol["prims"][same])
+
+
+def test_film_is_order_independent_and_linear(scenes_cache, gpu):
+    d, sc = scenes_cache["glass"]
+    cam = cases.camera(gpu, 64)
+    n = 300_000
+    a, info, ea = sc.render(cam, n, seed_base=11, max_bounce=16, frac_bits=30)
+    b, _, eb = sc.render(cam, n, seed_base=11, max_bounce=16, frac_bits=30)
+    np.testing.assert_array_equal(a, b)
+    assert list(ea.fx) == list(eb.fx)
+    p1, _, e1 = sc.render(cam, 123_457, seed_base=11, max_bounce=16, frac_bits=30)
+    p2, _, e2 = sc.render(cam, n - 123_457, seed_base=11 + 123_457, max_bounce=16, frac_bits=30)
+    np.testing.assert_array_equal(p1 + p2, a)
+    assert [x + y for x, y in zip(e1.fx, e2.fx)] == list(ea.fx)
+
+
+def test_session_accumulates_like_one_render(scenes_cache, gpu):
+    d, sc = scenes_cache["cornell"]
+    cams = [cases.camera(gpu, 48), gpu.look_at((1.2, 1.1, 5.0), (1.0, 1.0, 1.0), (0, 1, 0), 35.0, 40, 32)]
+    arr = (type(cams[0]) * 2)(*cams)
+    h = C.c_void_p()
+    gpu.check(gpu.L.ftb_session_begin(sc.h, arr, 2, 8, 28, C.byref(h)))
+    try:
+        gpu.check(gpu.L.ftb_session_batch(h, 50_000, 0))
+        gpu.check(gpu.L.ftb_session_batch(h, 70_000, 50_000))
+        films = []
+        for c, cam in enumerate(cams):
+            film = np.zeros((cam.res_y, cam.res_x, 4), dtype=np.int64)
+            gpu.check(gpu.L.ftb_session_download(h, c, film.ctypes.data_as(C.POINTER(C.c_int64)), None, None))
+            whole, _, _ = sc.render(cam, 120_000, seed_base=0, max_bounce=8, frac_bits=28)
+            np.testing.assert_array_equal(film, whole)
+            films.append(film)
+        hits = np.zeros(48 * 48)
+        gpu.check(gpu.L.ftb_session_hits0(h, hits.ctypes.data_as(C.POINTER(C.c_double))))
+        np.testing.assert_array_equal(hits.reshape(48, 48), films[0][..., 3].astype(np.float64))
+    finally:
+        gpu.L.ftb_session_end(h)
+
+
+def test_device_film_entry_point(scenes_cache, gpu):
+    torch = pytest.importorskip("torch")
+    d, sc = scenes_cache["materials"]
+    cam = cases.camera(gpu, 40)
+    film = torch.zeros((40, 40, 4), dtype=torch.int64, device="cuda:0")
+    info, en = sc.render_device(cam, 40_000, film.data_ptr(), seed_base=3, max_bounce=16, frac_bits=30,
+                                stream=torch.cuda.current_stream().cuda_stream, want_energy=True)
+    torch.cuda.synchronize()
+    host, _, en2 = sc.render(cam, 40_000, seed_base=3, max_bounce=16, frac_bits=30)
+    np.testing.assert_array_equal(film.cpu().numpy(), host)
+    assert list(en.fx) == list(en2.fx)
+
+
+def test_energy_conservation_full_size_cornell(gpu):
+    """Config-size run (2^24 photons, 256^2, 8 bounces): every photon's beta is booked once,
+    so emitted == absorbed + escaped + residual to within one fixed-point step per photon
+    (flat triangles: the shading-normal correction is 1 up to rounding)."""
+    d = scenes.make_cornell(gpu)
+    sc = lib.Scene(d, 0, gpu)
+    cam = scenes.default_camera(gpu, 256)
+    n = 1 << 24
+    film, info, en = sc.render(cam, n, max_bounce=8)
+    fx = list(en.fx)
+    assert fx[0] == n * (1 << 32)
+    assert abs(fx[0] - (fx[1] + fx[2] + fx[3] + fx[4])) <= n
+    assert film[..., 3].sum() > 0
+    sc.close()

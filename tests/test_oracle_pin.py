@@ -1,0 +1,106 @@
+"""Pin the CPU oracle (oracle/ftoracle.c) to the reference.
+
+1. Against the golden vectors in tests/golden/, produced by the reference's own tracer
+   (tests/golden/make_golden.py): bit-identical film, energy report and per-photon ray
+   counts / termination / final beta.
+2. Against the reference built in oracle/_ref (when present): the same, live, with other
+   photon ranges and with 4 threads (per-thread films merged in thread order).
+The product's host-side bake (ftb_camera_look_at, ftb_emission_cdf and the emitter power)
+is checked against the same golden values.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from goodphotons_b200 import scenes
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden(name):
+    return np.load(os.path.join(GOLDEN, name), allow_pickle=False)
+
+
+def test_rng_streams(oracle):
+    g = golden("streams.npz")
+    for k, u in zip(g["photon"], g["uniforms"]):
+        np.testing.assert_array_equal(oracle.uniforms(int(k), 16), u)
+
+
+def test_camera_bake(oracle, L):
+    g = golden("streams.npz")["camera"]
+    for cam in (oracle.look_at((1.0, 1.0, 5.4), (1.0, 1.0, 1.0), (0.0, 1.0, 0.0), 40.0, 256, 192),
+                L.look_at((1.0, 1.0, 5.4), (1.0, 1.0, 1.0), (0.0, 1.0, 0.0), 40.0, 256, 192)):
+        v = np.array(list(cam.eye) + list(cam.u) + list(cam.v) + list(cam.w) + [cam.tan_half_x, cam.tan_half_y])
+        np.testing.assert_array_equal(v, g)
+
+
+def test_emission_cdf_and_power(oracle, L):
+    g = golden("streams.npz")
+    d = scenes.make_cornell(L)
+    e = d.emitters[0]
+    cdf = d.emitter_cdf[e.cdf_offset:e.cdf_offset + e.cdf_n + 1]
+    np.testing.assert_array_equal(cdf, g["bb_cdf"])
+    assert e.power == float(g["bb_power"])
+    ocdf, ointeg = oracle.emission_cdf(d, e.spd)
+    np.testing.assert_array_equal(ocdf, g["bb_cdf"])
+    assert ointeg == float(g["bb_integral"])
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_trace_matches_golden(name, oracle, L):
+    mk, res, n, mb, seed = cases.CASES[name]
+    g = golden(f"trace_{name}.npz")
+    d = mk(L)
+    assert cases.scene_hash(d) == str(g["scene_hash"]), "scene generator drifted from the golden scene"
+    cam = cases.camera(L, res)
+    o = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, rays=True)
+    np.testing.assert_array_equal(o["energy"], g["energy"])
+    np.testing.assert_array_equal(o["xyz"], g["xyz"])
+    np.testing.assert_array_equal(o["hits"], g["hits"])
+    np.testing.assert_array_equal(o["rays"], g["rays"])
+    np.testing.assert_array_equal(o["logs"]["fate"], g["fate"])
+    np.testing.assert_array_equal(o["logs"]["beta"], g["beta"])
+
+
+@pytest.mark.parametrize("name", ["cornell", "materials", "fog_strands"])
+def test_trace_matches_reference_live(name, oracle, reference, L):
+    mk, res, n, mb, _ = cases.CASES[name]
+    d = mk(L)
+    cam = cases.camera(L, 48)
+    for seed, threads, count in ((555, 1, 6000), (10**9, 4, 20000)):
+        o = oracle.trace(d, cam, count, seed_base=seed, max_bounce=mb, threads=threads)
+        r = reference.trace(d, cam, count, seed_base=seed, max_bounce=mb, threads=threads)
+        np.testing.assert_array_equal(o["energy"], r["energy"])
+        np.testing.assert_array_equal(o["xyz"], r["xyz"])
+        np.testing.assert_array_equal(o["hits"], r["hits"])
+
+
+def test_closest_hit_known_answers(oracle, reference, L):
+    """Modelled on the reference's -checkbvh (main.cpp:448-473): random rays, the
+    closest hit's distance and material must agree."""
+    d = scenes.make_glass(L, level=3)
+    octx = oracle.prepare(d)
+    rctx = reference.prepare(d)
+    rng = np.random.default_rng(5)
+    try:
+        for _ in range(3000):
+            o = rng.uniform(0.05, 1.95, 3)
+            dv = rng.normal(size=3)
+            dv /= np.linalg.norm(dv)
+            m, t = reference.closest_hit(rctx, o, dv)
+            to = np.zeros(1)
+            import ctypes as C
+            p = oracle.L.fto_closest_hit(octx, o.ctypes.data_as(C.POINTER(C.c_double)),
+                                         dv.ctypes.data_as(C.POINTER(C.c_double)), 1e-6,
+                                         to.ctypes.data_as(C.POINTER(C.c_double)))
+            if m < 0:
+                assert p < 0
+            else:
+                assert to[0] == t
+                assert d.tri_mat[p] == m
+    finally:
+        oracle.L.fto_release(octx)
+        reference.L.ftr_release(rctx)

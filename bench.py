@@ -1,0 +1,395 @@
+"""Benchmark: photon paths/s of the forward pinhole light tracer on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload glass|cornell|fog_strands] [--level 7]
+
+Workload (default): the dispersive-caustics configuration -- the Cornell box holding a
+level-7 noise-displaced icosphere (327,680 triangles) of Cauchy glass n = 1.5 + 0.0042/um^2,
+1024x1024 film, 2^28 photons per frame, at most 16 bounces; seeded synthetic scene.
+A step is one frame: 2^28 photons traced from emission to termination on each GPU
+(weak scaling), plus, with N > 1, the frame-end NCCL sum of the int64 films.
+
+Reported (one JSON line on rank 0):
+  value        photons / s over the timed steps, device-resident inputs, max over ranks
+  e2e          the same through the C ABI call a user makes (ftb_render_forward): host
+               film in pinned memory, film download inside every step
+  roofline     the dominant kernel's algorithmic bytes / its CUDA-event duration, against
+               the measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  cpu_baseline the reference's own CPU tracer (oracle/_ref, "reference") or the oracle port
+               on this host's cores, over a bounded sample of the same workload
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (res, photons per frame, max bounce)
+    "glass": (1024, 1 << 28, 16),
+    "cornell": (256, 1 << 24, 8),
+    "fog_strands": (512, 1 << 26, 32),
+}
+METRIC = "photon paths/s on 1 B200"
+NODE_BYTES = 80     # WNode
+REC_BYTES = 80      # PrimRec
+RAY_IO_BYTES = 64   # extend: queue index 4 + ray 48 read, hit t 8 + record 4 written
+
+
+def make_scene(name, level, lib_):
+    from goodphotons_b200 import scenes
+    if name == "glass":
+        return scenes.make_glass(lib_, level=level)
+    if name == "cornell":
+        return scenes.make_cornell(lib_)
+    return scenes.make_fog_strands(lib_)
+
+
+def workload_config(args):
+    res, n, mb = WORKLOADS[args.workload]
+    cfg = {"workload": args.workload, "film": f"{res}x{res}", "photons_per_frame": n,
+           "max_bounce": mb, "seed": 0, "lambda": "sampled from the emitter SPD over 360-830 nm"}
+    if args.workload == "glass":
+        cfg.update(mesh=f"level-{args.level} icosphere r=0.4 m, 3-octave value noise 0.05 m",
+                   triangles=20 * 4 ** args.level, ior="Cauchy 1.5 + 0.0042/um^2")
+    return cfg, res, n, mb
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_ray(workload):
+    """dram bytes per closest-hit ray of the extend kernel, from the committed ncu summary
+    (profiles/k_extend_<workload>.md, line `dram_bytes_per_ray: <x>`), or None."""
+    p = os.path.join(ROOT, "profiles", f"k_extend_{workload}.md")
+    try:
+        for line in open(p):
+            if line.strip().startswith("dram_bytes_per_ray:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def calibrate(run, target_s):
+    """Photon count that takes about target_s: double a probe until it runs >= 1 s (so
+    thread start-up and film merge costs are amortized), then scale."""
+    n = 1 << 13
+    while True:
+        t = run(n, 1 << 40)
+        if t >= 1.0 or n >= (1 << 24):
+            return int(max(1 << 13, min(1 << 26, n * target_s / max(t, 1e-3))))
+        n *= 2
+
+
+def cpu_baseline(desc, cam, mb, target_s=12.0):
+    """The reference CPU tracer (oracle/_ref) on all host threads, else the oracle port."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_bind import Oracle, Reference
+    threads = os.cpu_count() or 1
+    if Reference.available():
+        impl, kind = Reference(), "reference"
+    else:
+        impl, kind = Oracle(), "port"
+    ctx = impl.prepare(desc)
+    try:
+        def run(n, seed):
+            t = time.perf_counter()
+            impl.trace(desc, cam, n, seed_base=seed, max_bounce=mb, threads=threads, ctx=ctx)
+            return time.perf_counter() - t
+        n = calibrate(run, target_s)
+        t = run(n, 1 << 41)
+    finally:
+        (impl.L.ftr_release if kind == "reference" else impl.L.fto_release)(ctx)
+    return {"value": n / t, "unit": "photon paths/s", "cores": threads, "kind": kind,
+            "sample": f"{n} photons of the same scene and film, seed_base 2^41, {t:.1f} s on {threads} threads"}
+
+
+def run_reference_arm(args):
+    """`--impl reference`: the reference's CPU implementation of the path on this host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from goodphotons_b200 import lib, scenes
+    cfg, res, _, mb = workload_config(args)
+    L = lib.load()
+    desc = make_scene(args.workload, args.level, L)
+    cam = scenes.default_camera(L, res)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_bind import Oracle, Reference
+    threads = os.cpu_count() or 1
+    impl, kind = (Reference(), "reference") if Reference.available() else (Oracle(), "port")
+    ctx = impl.prepare(desc)
+
+    def run(count, seed):
+        t = time.perf_counter()
+        impl.trace(desc, cam, count, seed_base=seed, max_bounce=mb, threads=threads, ctx=ctx)
+        return time.perf_counter() - t
+    per_step = calibrate(run, 8.0)
+    for w in range(args.warmup):
+        impl.trace(desc, cam, 1 << 13, seed_base=(1 << 45) + w * (1 << 13), max_bounce=mb, threads=threads, ctx=ctx)
+    times = []
+    for k in range(args.steps):
+        t = time.perf_counter()
+        impl.trace(desc, cam, per_step, seed_base=k * per_step, max_bounce=mb, threads=threads, ctx=ctx)
+        times.append(time.perf_counter() - t)
+    (impl.L.ftr_release if kind == "reference" else impl.L.fto_release)(ctx)
+    total = sum(times)
+    value = per_step * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "photon paths/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generator)",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "photon paths/s", "cores": threads, "kind": kind,
+                         "sample": f"{per_step} photons per step (bounded sample of the {cfg['photons_per_frame']}-photon frame)"},
+        "e2e": {"value": value, "unit": "photon paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="glass", choices=sorted(WORKLOADS))
+    ap.add_argument("--level", type=int, default=7)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--photons", type=int, default=0, help="photons per step (default: the workload's frame)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    from goodphotons_b200 import abi, lib, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    cfg, res, n, mb = workload_config(args)
+    if args.photons > 0:
+        n = args.photons
+        cfg["photons_per_frame"] = n
+    cfg["parallelism"] = f"photon-index shards x{world} (weak), NCCL int64 film sum at frame end" if world > 1 else "single GPU"
+    cfg["l2"] = "flushed between timed steps (256 MiB write)"
+    L = lib.load()
+    desc = make_scene(args.workload, args.level, L)
+    t = time.perf_counter()
+    sc = lib.Scene(desc, local, L)
+    bake_ms = 1e3 * (time.perf_counter() - t)
+    cam = scenes.default_camera(L, res)
+    dev = torch.device("cuda", local)
+    film = torch.zeros((res, res, 4), dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    frac = 0  # default: sized for the photon count
+
+    # counting pass (untimed): traversal work per closest-hit ray and per photon
+    sc.set_profiling(2)
+    n_count = min(n, 1 << 22)
+    sc.render_device(cam, n_count, film.data_ptr(), seed_base=1 << 50, max_bounce=mb,
+                     stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    cp = sc.profile(reset=True)
+    rays_c, nodes_c, recs_c = cp.counters[0], cp.counters[1], cp.counters[2]
+    bytes_per_ray = (nodes_c * NODE_BYTES + recs_c * REC_BYTES) / max(1, rays_c) + RAY_IO_BYTES
+    rays_per_photon = rays_c / n_count
+    sc.set_profiling(0)
+
+    def step(k):
+        film.zero_()
+        seed = (k * world + rank) * n
+        sc.render_device(cam, n, film.data_ptr(), seed_base=seed, max_bounce=mb, frac_bits=frac,
+                         stream=stream.cuda_stream)
+        if dist is not None:
+            dist.reduce(film, dst=0, op=dist.ReduceOp.SUM)
+
+    for w in range(args.warmup):
+        step(1000 + w)
+    torch.cuda.synchronize(dev)
+    sc.set_profiling(1)
+    sc.profile(reset=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record(stream)
+            step(k)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    prof = sc.profile(reset=True)
+    sc.set_profiling(0)
+    total_s = sum(step_ms) / 1e3
+    if dist is not None:
+        tt = torch.tensor([total_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_s = float(tt.item())
+    photons = n * args.steps * world
+    value = photons / total_s
+
+    # roofline of the dominant kernel (closest-hit traversal unless another dominates)
+    names = ["k_emit", "k_extend", "k_shade", "k_shadow"]
+    kms = list(prof.ms)
+    dom = int(np.argmax(kms))
+    peak, peak_kind = measured_peak()
+    rays_timed = rays_per_photon * n * args.steps
+    extend_launches = max(1, prof.launches[1])
+    bytes_launch = rays_timed * bytes_per_ray / extend_launches
+    avg_launch_s = kms[1] / 1e3 / extend_launches
+    achieved = bytes_launch / avg_launch_s / 1e9
+    traffic_ray = ncu_traffic_per_ray(args.workload)
+    roofline = {
+        "bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": round(achieved, 1),
+        "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+        "traffic": (round(traffic_ray * rays_timed / extend_launches) if traffic_ray else None),
+        "peak_source": f"{peak_kind} hbm_gbs (copy)",
+        "algorithmic_bytes_per_ray": round(bytes_per_ray, 1),
+        "node_visits_per_ray": round(nodes_c / max(1, rays_c), 3),
+        "record_tests_per_ray": round(recs_c / max(1, rays_c), 3),
+        "closest_hit_rays_per_photon": round(rays_per_photon, 4),
+        "shadow_rays_per_photon": round(cp.counters[3] / n_count, 4),
+        "kernel_share": {nm: round(x / max(1e-9, sum(kms)), 4) for nm, x in zip(names, kms)},
+        "dominant_kernel": names[dom],
+    }
+    gpu_launches = int(sum(prof.launches))
+
+    # end to end through the C ABI call with a pinned host film
+    e2e = None
+    host = torch.empty((res, res, 4), dtype=torch.int64, pin_memory=True)
+    e2e_steps = 0 if args.no_e2e else max(2, min(args.steps, 3))
+    host_np = host.numpy()
+    if e2e_steps:
+        sc.render(cam, 1 << 20, seed_base=1 << 52, max_bounce=mb, out=host_np)
+    torch.cuda.synchronize(dev)
+    e_times = []
+    for k in range(e2e_steps):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        sc.render(cam, n, seed_base=(1 << 53) + (k * world + rank) * n, max_bounce=mb, out=host_np)
+        e_times.append(time.perf_counter() - t)
+    e_total = sum(e_times)
+    if dist is not None:
+        tt = torch.tensor([e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e_total = float(tt.item())
+    e2e = None if not e2e_steps else {"value": n * e2e_steps * world / e_total, "unit": "photon paths/s",
+           "h2d_bytes_per_step": C.sizeof(abi.Camera) + C.sizeof(abi.RenderParams),
+           "d2h_bytes_per_step": res * res * 4 * 8 + C.sizeof(abi.Energy),
+           "call": "ftb_render_forward (resident scene, host film)", "bake_ms": round(bake_ms, 1)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(desc, cam, mb)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "photon paths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded scene generator; no dataset)", "config": cfg,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": gpu_launches,
+            "clocks": clocks.summary(),
+            "notes": "fp64 path arithmetic (reference order), fp32 conservative BVH culling, int64 fixed-point film",
+        }
+        print(json.dumps(line), flush=True)
+    sc.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -104,11 +104,16 @@ class PhotonLog(C.Structure):
                 ("beta", C.c_double), ("prims", C.c_int32 * 8)]
 
 
+class KernelProfile(C.Structure):
+    _fields_ = [("ms", C.c_double * 4), ("launches", C.c_int64 * 4), ("counters", C.c_uint64 * 6)]
+
+
 STRUCTS = {
     "ftb_spectrum": Spectrum, "ftb_material": Material, "ftb_emitter": Emitter,
     "ftb_medium": Medium, "ftb_scene_desc": SceneDesc, "ftb_camera": Camera,
     "ftb_render_params": RenderParams, "ftb_energy": Energy, "ftb_film_info": FilmInfo,
     "ftb_footprint": Footprint, "ftb_photon_log": PhotonLog,
+    "ftb_kernel_profile": KernelProfile,
 }
 
 # every entry point declared in include/ftb200.h
@@ -118,4 +123,5 @@ EXPORTS = [
     "ftb_scene_destroy", "ftb_scene_footprint", "ftb_scene_power", "ftb_render_forward",
     "ftb_render_forward_device", "ftb_session_begin", "ftb_session_batch",
     "ftb_session_hits0", "ftb_session_download", "ftb_session_end", "ftb_trace_log",
+    "ftb_scene_set_profiling", "ftb_scene_profile",
 ]

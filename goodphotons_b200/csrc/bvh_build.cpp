@@ -219,6 +219,7 @@ bool build_wide_bvh(const std::vector<Box>& boxes_in, double margin, WideBvh& ou
             nb.grow(c.box);
             for (int a = 0; a < 3; ++a) { clo[a][k] = c.box.lo[a]; chi[a][k] = c.box.hi[a]; }
             if (c.count > 0) {
+                if (prim_off > 31) { err = "leaf record offset exceeds 5 bits"; return false; }
                 w.meta[k] = (uint8_t)((c.count << 5) | prim_off);
                 for (int i = 0; i < c.count; ++i) out.order.push_back(B.idx[c.first + i]);
                 prim_off += c.count;
@@ -230,7 +231,6 @@ bool build_wide_bvh(const std::vector<Box>& boxes_in, double margin, WideBvh& ou
                 ++n_int;
             }
         }
-        if (prim_off > 31) { err = "wide node references more than 31 records"; return false; }
         float p[3]; int e[3];
         uint8_t* qlo[3] = {w.qlo_x, w.qlo_y, w.qlo_z};
         uint8_t* qhi[3] = {w.qhi_x, w.qhi_y, w.qhi_z};
@@ -243,6 +243,42 @@ bool build_wide_bvh(const std::vector<Box>& boxes_in, double margin, WideBvh& ou
         w.px = p[0]; w.py = p[1]; w.pz = p[2];
         w.ex = (uint8_t)(e[0] + 127); w.ey = (uint8_t)(e[1] + 127); w.ez = (uint8_t)(e[2] + 127);
         out.nodes[pd.wide] = w;
+    }
+    return true;
+}
+
+bool validate_wide_bvh(const WideBvh& b, int n_prims, std::string& err) {
+    const size_t nn = b.nodes.size(), nr = b.order.size();
+    if (nn == 0) { err = "BVH has no root"; return false; }
+    if ((int)nr != n_prims) { err = "BVH record count differs from primitive count"; return false; }
+    std::vector<char> seen_rec(nr, 0), seen_node(nn, 0);
+    seen_node[0] = 1;
+    for (size_t i = 0; i < nn; ++i) {
+        const WNode& w = b.nodes[i];
+        for (int k = 0; k < FTB_WIDTH; ++k) {
+            uint32_t m = w.meta[k];
+            if (!m) { if ((w.imask >> k) & 1) { err = "internal bit on an empty slot"; return false; } continue; }
+            uint32_t cnt = m >> 5, off = m & 31;
+            if ((w.imask >> k) & 1) {
+                uint64_t c = (uint64_t)w.child_base + off;
+                if (cnt != 1 || c >= nn || c <= i || seen_node[c]) { err = "bad child node index"; return false; }
+                seen_node[c] = 1;
+            } else {
+                if (cnt < 1 || cnt > FTB_LEAF_MAX) { err = "bad leaf size"; return false; }
+                for (uint32_t r = 0; r < cnt; ++r) {
+                    uint64_t ri = (uint64_t)w.prim_base + off + r;
+                    if (ri >= nr || seen_rec[ri]) { err = "bad record index"; return false; }
+                    seen_rec[ri] = 1;
+                }
+            }
+        }
+    }
+    for (size_t i = 0; i < nn; ++i) if (!seen_node[i]) { err = "unreachable node"; return false; }
+    for (size_t r = 0; r < nr; ++r) if (!seen_rec[r]) { err = "unreferenced record"; return false; }
+    std::vector<char> seen_prim((size_t)n_prims, 0);
+    for (int p : b.order) {
+        if (p < 0 || p >= n_prims || seen_prim[(size_t)p]) { err = "bad primitive permutation"; return false; }
+        seen_prim[(size_t)p] = 1;
     }
     return true;
 }

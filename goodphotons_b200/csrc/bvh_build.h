@@ -34,4 +34,8 @@ struct WideBvh {
 bool build_wide_bvh(const std::vector<Box>& boxes, double margin, WideBvh& out,
                     std::string& err);
 
+// Structural check run on every bake: child and record indices in range, every node
+// reachable once, every primitive referenced exactly once, children after parents.
+bool validate_wide_bvh(const WideBvh& b, int n_prims, std::string& err);
+
 }  // namespace ftb

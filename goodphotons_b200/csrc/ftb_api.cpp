@@ -102,6 +102,53 @@ V vnorm(V a) { double l = std::sqrt(vdot(a, a)); return {a.x / l, a.y / l, a.z /
 
 }  // namespace
 
+// ---- profiling sink -------------------------------------------------------------------
+namespace {
+struct ProfSink : ftb::LaunchSink {
+    struct Rec { int kernel; cudaEvent_t a, b; };
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<Rec> pending;
+    cudaEvent_t open[ftb::K_COUNT][2] = {};   // per kernel kind and stream slot
+    double ms[ftb::K_COUNT] = {0, 0, 0, 0};
+    int64_t launches[ftb::K_COUNT] = {0, 0, 0, 0};
+    cudaEvent_t take() {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    // launches on one stream are serialized, so the begin event of a kernel kind is
+    // paired with the next end event of the same kind on the same stream
+    std::vector<std::pair<cudaStream_t, cudaEvent_t>> begun[ftb::K_COUNT];
+    void mark(int k, bool end, cudaStream_t st) override {
+        cudaEvent_t e = take();
+        if (!e) return;
+        cudaEventRecord(e, st);
+        if (!end) { begun[k].push_back({st, e}); return; }
+        for (size_t i = 0; i < begun[k].size(); ++i)
+            if (begun[k][i].first == st) {
+                pending.push_back({k, begun[k][i].second, e});
+                begun[k].erase(begun[k].begin() + (long)i);
+                return;
+            }
+    }
+    void resolve() {
+        for (auto& r : pending) {
+            float t = 0.f;
+            cudaEventSynchronize(r.b);
+            if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) { ms[r.kernel] += t; launches[r.kernel]++; }
+        }
+        pending.clear();
+        used = 0;
+        for (auto& b : begun) b.clear();
+    }
+    ~ProfSink() override { for (auto e : pool) cudaEventDestroy(e); }
+};
+}  // namespace
+
 // ---- scene object ----------------------------------------------------------------------
 struct ftb_scene {
     int device = 0;
@@ -120,6 +167,9 @@ struct ftb_scene {
     size_t film_words = 0;
     unsigned long long* tally = nullptr;
     int32_t* status = nullptr;
+    int32_t prof_mode = 0;
+    ProfSink* prof = nullptr;
+    unsigned long long* stats = nullptr;   // device counters for profiling mode 2
     ~ftb_scene() {
         int cur = 0;
         cudaGetDevice(&cur);
@@ -129,6 +179,8 @@ struct ftb_scene {
         if (film) cudaFree(film);
         if (tally) cudaFree(tally);
         if (status) cudaFree(status);
+        if (stats) cudaFree(stats);
+        delete prof;
         for (void* p : allocs) cudaFree(p);
         cudaSetDevice(cur);
     }
@@ -281,6 +333,7 @@ ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t 
     ftb::Frame f;
     f.film = d_film;
     f.tally = d_tally;
+    f.stats = s->prof_mode == 2 ? s->stats : nullptr;
     f.status = s->status;
     f.film_scale_inv = std::ldexp(1.0, frac_bits) / s->power;
     f.tally_scale_inv = std::ldexp(1.0, 32) / s->power;
@@ -298,7 +351,7 @@ ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t 
         w.logs = d_logs;
         w.log_base = (int64_t)seed_base;
         cudaError_t e = ftb::launch_wave(s->dev, dc, w, f, seed_base + (uint64_t)done, m, max_bounce, s->sms,
-                                         s->streams[k & 1]);
+                                         s->streams[k & 1], s->prof_mode ? s->prof : nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         done += m;
         ++k;
@@ -491,6 +544,7 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     ftb::WideBvh bvh;
     std::string err;
     if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err)) { delete s; return fail(FTB_ERR_INVALID, err); }
+    if (np > 0 && !ftb::validate_wide_bvh(bvh, (int)np, err)) { delete s; return fail(FTB_ERR_INVALID, "BVH check: " + err); }
     if (np == 0) {   // an empty root with no children
         bvh.nodes.resize(1);
         std::memset(&bvh.nodes[0], 0, sizeof(WNode));
@@ -686,6 +740,39 @@ ftb_status ftb_trace_log(ftb_scene* s, const ftb_camera* cam, const ftb_render_p
     }
     cudaFree(d_logs);
     return st;
+}
+
+ftb_status ftb_scene_set_profiling(ftb_scene* s, int32_t mode) {
+    if (!s || mode < 0 || mode > 2) return fail(FTB_ERR_INVALID, "bad profiling arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    DeviceGuard guard(s->device);
+    if (mode && !s->prof) s->prof = new ProfSink();
+    if (mode == 2 && !s->stats) {
+        CK(cudaMalloc(&s->stats, 8 * sizeof(unsigned long long)), "stats alloc");
+        CK(cudaMemset(s->stats, 0, 8 * sizeof(unsigned long long)), "stats memset");
+    }
+    s->prof_mode = mode;
+    return FTB_OK;
+}
+
+ftb_status ftb_scene_profile(ftb_scene* s, ftb_kernel_profile* out, int32_t reset) {
+    if (!s || !out) return fail(FTB_ERR_INVALID, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    DeviceGuard guard(s->device);
+    std::memset(out, 0, sizeof *out);
+    if (s->prof) {
+        s->prof->resolve();
+        for (int k = 0; k < 4; ++k) { out->ms[k] = s->prof->ms[k]; out->launches[k] = s->prof->launches[k]; }
+        if (reset) for (int k = 0; k < 4; ++k) { s->prof->ms[k] = 0; s->prof->launches[k] = 0; }
+    }
+    if (s->stats) {
+        CK(cudaDeviceSynchronize(), "sync");
+        unsigned long long c[8];
+        CK(cudaMemcpy(c, s->stats, sizeof c, cudaMemcpyDeviceToHost), "stats readback");
+        for (int k = 0; k < 6; ++k) out->counters[k] = c[k];
+        if (reset) CK(cudaMemset(s->stats, 0, sizeof c), "stats reset");
+    }
+    return FTB_OK;
 }
 
 // ---- sessions ---------------------------------------------------------------------------

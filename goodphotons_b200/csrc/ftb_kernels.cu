@@ -486,9 +486,12 @@ __device__ __forceinline__ void load_node(const WNode* nodes, uint32_t i, uint4 
     n[0] = __ldg(p); n[1] = __ldg(p + 1); n[2] = __ldg(p + 2); n[3] = __ldg(p + 3); n[4] = __ldg(p + 4);
 }
 
+struct TravCount { unsigned long long nodes, recs; };
+
 // Closest hit: returns the record index (or -1) and t.
+template <bool COUNT>
 __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin, double& best_t,
-                                int32_t* status) {
+                                int32_t* status, TravCount& cnt) {
     RayF F = make_rayf(R.o, R.d);
     float tmin_f = __double2float_rd(tmin);
     best_t = DBL_MAX;
@@ -501,6 +504,7 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
     while (true) {
         uint4 n[5];
         load_node(sc.nodes, node, n);
+        if (COUNT) cnt.nodes++;
         float tn[8];
         uint32_t hit = node_children(n, F, tmin_f, tmax_f, tn);
         uint32_t imask = n[0].w >> 24;
@@ -512,11 +516,12 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
             int i = __ffs(leaves) - 1;
             leaves &= leaves - 1;
             uint32_t m = byte_of(meta, i);
-            int cnt = m >> 5, off = m & 31;
-            for (int k = 0; k < cnt; ++k) {
+            int nrec = m >> 5, off = m & 31;
+            for (int k = 0; k < nrec; ++k) {
                 PrimRec r;
                 int ri = (int)prim_base + off + k;
                 load_rec(sc.recs, ri, r);
+                if (COUNT) cnt.recs++;
                 double t;
                 if (rec_test(R, r, tmin, best_t, t)) { best_t = t; best = ri; tmax_f = __double2float_ru(t); }
             }
@@ -548,7 +553,9 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
 }
 
 // Any hit with t in [tmin, seg) (Scene::occluded, scene.h:2249-2271).
-__device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, double seg, int32_t* status) {
+template <bool COUNT>
+__device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, double seg, int32_t* status,
+                             TravCount& cnt) {
     RayF F = make_rayf(R.o, R.d);
     float tmin_f = __double2float_rd(tmin);
     float tmax_f = __double2float_ru(seg);
@@ -558,6 +565,7 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
     while (true) {
         uint4 n[5];
         load_node(sc.nodes, node, n);
+        if (COUNT) cnt.nodes++;
         float tn[8];
         uint32_t hit = node_children(n, F, tmin_f, tmax_f, tn);
         uint32_t imask = n[0].w >> 24;
@@ -568,10 +576,11 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
             int i = __ffs(leaves) - 1;
             leaves &= leaves - 1;
             uint32_t m = byte_of(meta, i);
-            int cnt = m >> 5, off = m & 31;
-            for (int k = 0; k < cnt; ++k) {
+            int nrec = m >> 5, off = m & 31;
+            for (int k = 0; k < nrec; ++k) {
                 PrimRec r;
                 load_rec(sc.recs, (int)prim_base + off + k, r);
+                if (COUNT) cnt.recs++;
                 double t;
                 if (rec_test(R, r, tmin, seg, t)) return true;
             }
@@ -884,17 +893,34 @@ __global__ void __launch_bounds__(128) k_emit(DevScene sc, DevCam cam, Wave w, F
     block_tally(&f.tally[T_RES], t_res);
 }
 
+__device__ void block_add3(unsigned long long* dst, unsigned long long a, unsigned long long b,
+                           unsigned long long c) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (a | b | c)) {
+        atomicAdd(dst, a); atomicAdd(dst + 1, b); atomicAdd(dst + 2, c);
+    }
+}
+
+template <bool COUNT>
 __global__ void __launch_bounds__(128) k_extend(DevScene sc, Wave w, const int32_t* q, const int32_t* qcount,
-                                                int32_t* status) {
+                                                Frame f) {
     int nq = *qcount;
+    TravCount cnt{0, 0};
+    unsigned long long rays = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
         int slot = q[i];
         RayCtx R = make_ray(mk(w.ox[slot], w.oy[slot], w.oz[slot]), mk(w.dx[slot], w.dy[slot], w.dz[slot]));
         double t;
-        int rec = traverse_closest(sc, R, EPS_RAY, t, status);
+        int rec = traverse_closest<COUNT>(sc, R, EPS_RAY, t, f.status, cnt);
         w.hit_t[slot] = t;
         w.hit_rec[slot] = rec;
+        if (COUNT) rays++;
     }
+    if (COUNT) block_add3(f.stats, rays, cnt.nodes, cnt.recs);
 }
 
 // medium stack (medium_stack.h:17-47), kStkCap entries per slot
@@ -1117,14 +1143,18 @@ __global__ void __launch_bounds__(128) k_shade(DevScene sc, DevCam cam, Wave w, 
 }
 
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
+template <bool COUNT>
 __global__ void __launch_bounds__(128) k_shadow(DevScene sc, Wave w, Frame f) {
     int n = w.counts[2];
     if (n > w.S) n = w.S;
+    TravCount cnt{0, 0};
+    unsigned long long rays = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
         double max_dist = w.smax[i];
         RayCtx R = make_ray(o, d);
-        if (traverse_any(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status)) continue;
+        if (COUNT) rays++;
+        if (traverse_any<COUNT>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         double lam = w.slam[i], c = w.sval[i];
         double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
         long long* px = reinterpret_cast<long long*>(f.film) + 4 * (size_t)w.spix[i];
@@ -1133,6 +1163,7 @@ __global__ void __launch_bounds__(128) k_shadow(DevScene sc, Wave w, Frame f) {
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, f.film_scale_inv, f.status));
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
     }
+    if (COUNT) block_add3(f.stats + 3, rays, cnt.nodes, cnt.recs);
 }
 
 // ------------------------------------------------------------------ host side ----------
@@ -1187,26 +1218,40 @@ void wave_free(Wave& w) {
 }
 
 cudaError_t launch_wave(const DevScene& sc, const DevCam& cam, Wave& w, const Frame& f, uint64_t photon0,
-                        int32_t n, int32_t max_bounce, int32_t sms, cudaStream_t st) {
+                        int32_t n, int32_t max_bounce, int32_t sms, cudaStream_t st, LaunchSink* sink) {
     const int T = 128;
     int blocks_emit = (n + T - 1) / T;
     int grid = sms * 16;   // persistent-style grid for the queue-driven kernels
     int gq = (n + T - 1) / T;
     if (gq < grid) grid = gq < 1 ? 1 : gq;
+    const bool count = f.stats != nullptr;
+    auto mark = [&](int k, bool end) { if (sink) sink->mark(k, end, st); };
+    auto shadow = [&]() {
+        mark(K_SHADOW, false);
+        if (count) k_shadow<true><<<grid, T, 0, st>>>(sc, w, f);
+        else k_shadow<false><<<grid, T, 0, st>>>(sc, w, f);
+        mark(K_SHADOW, true);
+        cudaMemsetAsync(&w.counts[2], 0, 4, st);
+    };
     cudaMemsetAsync(w.counts, 0, 64, st);
+    mark(K_EMIT, false);
     k_emit<<<blocks_emit, T, 0, st>>>(sc, cam, w, f, photon0, n, max_bounce);
-    k_shadow<<<grid, T, 0, st>>>(sc, w, f);
-    cudaMemsetAsync(&w.counts[2], 0, 4, st);
+    mark(K_EMIT, true);
+    shadow();
     int32_t* qa = w.qa;
     int32_t* qb = w.qb;
     int32_t* ca = &w.counts[0];
     int32_t* cb = &w.counts[1];
     for (int b = 0; b < max_bounce; ++b) {
-        k_extend<<<grid, T, 0, st>>>(sc, w, qa, ca, f.status);
+        mark(K_EXTEND, false);
+        if (count) k_extend<true><<<grid, T, 0, st>>>(sc, w, qa, ca, f);
+        else k_extend<false><<<grid, T, 0, st>>>(sc, w, qa, ca, f);
+        mark(K_EXTEND, true);
         cudaMemsetAsync(cb, 0, 4, st);
+        mark(K_SHADE, false);
         k_shade<<<grid, T, 0, st>>>(sc, cam, w, f, qa, ca, qb, cb, photon0, b, max_bounce);
-        k_shadow<<<grid, T, 0, st>>>(sc, w, f);
-        cudaMemsetAsync(&w.counts[2], 0, 4, st);
+        mark(K_SHADE, true);
+        shadow();
         int32_t* tq = qa; qa = qb; qb = tq;
         int32_t* tc = ca; ca = cb; cb = tc;
     }

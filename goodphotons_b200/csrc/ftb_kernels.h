@@ -46,6 +46,9 @@ struct Wave {
 struct Frame {
     int64_t* film;             // 4 words per pixel
     unsigned long long* tally; // 5 fixed-point energy tallies
+    unsigned long long* stats; // traversal counters (counting variant only, else null):
+                               // [0] closest-hit rays [1] their node visits [2] their record
+                               // tests [3] any-hit rays [4] node visits [5] record tests
     int32_t* status;
     double film_scale_inv;     // 2^frac / power_ref
     double tally_scale_inv;    // 2^32 / power_ref
@@ -55,9 +58,21 @@ size_t wave_bytes(int32_t W, bool log);
 cudaError_t wave_alloc(Wave& w, int32_t W, bool log);
 void wave_free(Wave& w);
 
-// Trace photons [photon0, photon0+n) (n <= W) through all bounces on `stream`.
+// Kernel ids for profiling.
+enum { K_EMIT = 0, K_EXTEND = 1, K_SHADE = 2, K_SHADOW = 3, K_COUNT = 4 };
+
+// Optional observer of kernel launches (profiling): called before and after every launch
+// on the launching stream, so it can record CUDA events there.
+struct LaunchSink {
+    virtual void mark(int kernel, bool end, cudaStream_t stream) = 0;
+    virtual ~LaunchSink() {}
+};
+
+// Trace photons [photon0, photon0+n) (n <= W) through all bounces on `stream`.  With
+// f.stats set, the counting variants of the traversal kernels run (slower; for traffic
+// accounting only).
 cudaError_t launch_wave(const DevScene& sc, const DevCam& cam, Wave& w, const Frame& f,
                         uint64_t photon0, int32_t n, int32_t max_bounce, int32_t sms,
-                        cudaStream_t stream);
+                        cudaStream_t stream, LaunchSink* sink = nullptr);
 
 }  // namespace ftb

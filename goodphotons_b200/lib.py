@@ -68,6 +68,8 @@ def load(path=None):
     _sig(L, "ftb_session_end", st, PS)
     _sig(L, "ftb_trace_log", st, PS, C.POINTER(abi.Camera), C.POINTER(abi.RenderParams),
          C.POINTER(abi.PhotonLog))
+    _sig(L, "ftb_scene_set_profiling", st, PS, C.c_int32)
+    _sig(L, "ftb_scene_profile", st, PS, C.POINTER(abi.KernelProfile), C.c_int32)
     w = _Lib(L)
     if path is None:
         _lib = w
@@ -145,9 +147,11 @@ class Scene:
         self.lib.check(self.lib.L.ftb_scene_footprint(self.h, rx, ry, C.byref(fp)))
         return fp
 
-    def render(self, cam, n, seed_base=0, max_bounce=8, frac_bits=0):
-        """One-shot render into a host film: returns (film int64 [ry, rx, 4], info, energy)."""
-        film = np.zeros((cam.res_y, cam.res_x, 4), dtype=np.int64)
+    def render(self, cam, n, seed_base=0, max_bounce=8, frac_bits=0, out=None):
+        """One-shot render into a host film: returns (film int64 [ry, rx, 4], info, energy).
+        `out` may be a preallocated (e.g. pinned) int64 array of that shape."""
+        film = out if out is not None else np.zeros((cam.res_y, cam.res_x, 4), dtype=np.int64)
+        assert film.dtype == np.int64 and film.shape == (cam.res_y, cam.res_x, 4) and film.flags.c_contiguous
         p = abi.RenderParams(n, seed_base, max_bounce, frac_bits)
         info, en = abi.FilmInfo(), abi.Energy()
         self.lib.check(self.lib.L.ftb_render_forward(
@@ -164,6 +168,14 @@ class Scene:
             self.h, C.byref(cam), C.byref(p), C.c_void_p(d_film_ptr), C.byref(info),
             C.byref(en) if en is not None else None, C.c_void_p(stream or 0)))
         return info, en
+
+    def set_profiling(self, mode):
+        self.lib.check(self.lib.L.ftb_scene_set_profiling(self.h, mode))
+
+    def profile(self, reset=True):
+        kp = abi.KernelProfile()
+        self.lib.check(self.lib.L.ftb_scene_profile(self.h, C.byref(kp), 1 if reset else 0))
+        return kp
 
     def trace_log(self, cam, n, seed_base=0, max_bounce=8):
         logs = (abi.PhotonLog * max(1, n))()

@@ -284,6 +284,23 @@ typedef struct ftb_photon_log {
 ftb_status ftb_trace_log(ftb_scene* scene, const ftb_camera* cam,
                          const ftb_render_params* params, ftb_photon_log* out);
 
+/* ---- profiling (measurement support; no counterpart in the reference, which times
+ * whole renders by wall clock) ---------------------------------------------------------
+ * mode 0: off.  mode 1: every kernel launch of this scene's renders is bracketed by CUDA
+ * events on its own stream; ftb_scene_profile sums the durations per kernel.  mode 2:
+ * additionally run the counting variants of the traversal kernels, which tally rays, BVH
+ * node visits and primitive-record tests (slower: never time a mode-2 render). */
+typedef struct ftb_kernel_profile {
+    double ms[4];          /* summed launch durations: emit, extend, shade, shadow */
+    int64_t launches[4];
+    uint64_t counters[6];  /* mode 2: closest-hit rays, their node visits, their record
+                              tests; any-hit rays, node visits, record tests */
+} ftb_kernel_profile;
+
+ftb_status ftb_scene_set_profiling(ftb_scene* scene, int32_t mode);
+/* Waits for the recorded events, returns the totals since the last reset. */
+ftb_status ftb_scene_profile(ftb_scene* scene, ftb_kernel_profile* out, int32_t reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -272,18 +272,18 @@ class SceneBuilder:
 # ---------------------------------------------------------------------------------------
 # Synthetic workloads
 # ---------------------------------------------------------------------------------------
-def _step_table(lo, hi, on=0.75, off=0.05):
+def _step_table(lo, hi, on=0.75, off=0.05, ramp=0.01):
     """Reflectance `on` over [lo, hi] nm and `off` elsewhere, as table breakpoints with a
-    0.01 nm ramp at each edge."""
-    return [(LAMBDA_MIN, off), (lo - 0.01, off), (lo, on), (hi, on), (hi + 0.01, off),
+    `ramp`-nm linear edge."""
+    return [(LAMBDA_MIN, off), (lo - ramp, off), (lo, on), (hi, on), (hi + ramp, off),
             (LAMBDA_MAX, off)]
 
 
-def cornell_box(sb: SceneBuilder, boxes=True, light_kelvin=6500.0):
+def cornell_box(sb: SceneBuilder, boxes=True, light_kelvin=6500.0, ramp=0.01):
     """2x2x2 m box of 5 quads (open at +z), 0.5x0.5 m blackbody ceiling light."""
     white = sb.diffuse(sb.const(0.75))
-    red = sb.diffuse(sb.table(_step_table(600.0, 780.0)))
-    green = sb.diffuse(sb.table(_step_table(500.0, 570.0)))
+    red = sb.diffuse(sb.table(_step_table(600.0, 780.0, ramp=ramp)))
+    green = sb.diffuse(sb.table(_step_table(500.0, 570.0, ramp=ramp)))
     sb.quad((0, 0, 0), (0, 0, 2), (2, 0, 0), white)    # floor (+y)
     sb.quad((0, 2, 0), (2, 0, 0), (0, 0, 2), white)    # ceiling (-y)
     sb.quad((0, 0, 0), (2, 0, 0), (0, 2, 0), white)    # back (+z)

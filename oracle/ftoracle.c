@@ -618,7 +618,7 @@ static int closest_hit(const fto_ctx* c, V3 ro, V3 rd, double tmin, Hit* hit) {
                 if (prim_test(c, p, &sh, &cr, ro, rd, tmin, best, NULL, &t)) { best = t; bestp = p; }
             }
         } else {
-            double tl, tr;
+            double tl = 0.0, tr = 0.0;
             int hl = box_hit(&c->nodes[n->left], ro, inv, tmin, best, &tl);
             int hr = box_hit(&c->nodes[n->right], ro, inv, tmin, best, &tr);
             if (sp + 2 > 128) { fail("oracle BVH stack overflow"); return -1; }

@@ -140,6 +140,9 @@ void ftr_look_at(const double* eye, const double* target, const double* up, doub
 
 double ftr_total_power(void* h) { return static_cast<Ref*>(h)->scene.totalPower; }
 
+/* The reference Scene behind a handle (for the drop-in shim test, oracle/shim_harness.cpp). */
+const void* ftr_scene(void* h) { return &static_cast<Ref*>(h)->scene; }
+
 /* emitter i: power, integral and its cdf (cap entries) */
 int ftr_emitter(void* h, int i, double* power, double* integral, double* cdf, int cap) {
     const Scene& s = static_cast<Ref*>(h)->scene;

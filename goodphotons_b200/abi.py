@@ -123,5 +123,6 @@ EXPORTS = [
     "ftb_scene_destroy", "ftb_scene_footprint", "ftb_scene_power", "ftb_render_forward",
     "ftb_render_forward_device", "ftb_session_begin", "ftb_session_batch",
     "ftb_session_hits0", "ftb_session_download", "ftb_session_end", "ftb_trace_log",
-    "ftb_scene_set_profiling", "ftb_scene_profile",
+    "ftb_scene_set_profiling", "ftb_scene_profile", "ftb_render_forward_noalloc",
 ]
+NOALLOC_MAX_PHOTONS = 32768

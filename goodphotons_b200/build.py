@@ -56,6 +56,7 @@ def build(verbose=False, force=False):
     units = [
         ("ftb_kernels.cu", [*ARCH, "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
                             "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3"]),
+        ("ftb_noalloc.cu", [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]),
         ("ftb_api.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC"]),
         ("bvh_build.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC"]),
     ]

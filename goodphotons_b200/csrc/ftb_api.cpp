@@ -404,6 +404,20 @@ ftb_status check_params(const ftb_scene* s, const ftb_camera* cam, const ftb_ren
 
 }  // namespace
 
+// ---- internal accessors (used by ftb_noalloc.cu) --------------------------------------
+namespace ftb {
+void set_last_error(const std::string& m) { g_err = m; }
+
+bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power) {
+    if (!s) return false;
+    *dev = s->dev;
+    *device = s->device;
+    *sms = s->sms;
+    *power = s->power;
+    return true;
+}
+}  // namespace ftb
+
 // ---- entry points ----------------------------------------------------------------------
 extern "C" {
 

@@ -1,0 +1,168 @@
+// ftb_noalloc.cu -- ftb_render_forward_noalloc: a render entry point that allocates no
+// device memory.
+//
+// Who needs it: hosts that own every byte of device memory and forbid allocation inside
+// their render callbacks (engine and DCC plug-in hosts with their own allocator), frame
+// loops that must not allocate once they are running, and callers for which a cudaMalloc /
+// cudaFree would synchronize the device in the middle of their own stream work.  Such a
+// caller creates the scene once at start-up and then renders with this entry point, which
+// only launches kernels and issues async memsets on the caller's stream.
+//
+// Its scratch -- the path state, queues and shadow records of one wave of photons, plus the
+// energy tallies and the status word -- lives in one file-scope __device__ array of
+// kNoAllocBytes (about 9.5 MB for kNoAllocPhotons = 32768 slots), which every GPU that loads
+// the library holds until the process exits.  Host code cannot use the array's name as a
+// device address (it is a host-side stand-in), so the first call on each device, with that
+// device current, resolves it with cudaGetSymbolAddress; make that first call before any
+// stream capture.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/ftb200.h"
+#include "ftb_kernels.h"
+#include "ftb_layout.h"
+
+namespace ftb {
+bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power);
+void set_last_error(const std::string& m);   // the text ftb_last_error() returns
+}
+
+namespace {
+
+constexpr int32_t kNoAllocPhotons = 1 << 15;
+
+constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Layout of one wave in the scratch array (same fields as ftb::wave_alloc).
+constexpr size_t wave_layout_bytes(size_t w) {
+    return 2 * al(8 * w) + 8 * al(8 * w) + al(4 * w) + al(8 * w * ftb::kStkCap) + al(8 * w) + al(4 * w) +
+           2 * al(4 * w) + al(64) + 9 * al(8 * 2 * w) + al(4 * 2 * w);
+}
+constexpr size_t kWaveBytes = wave_layout_bytes(kNoAllocPhotons);
+constexpr size_t kNoAllocBytes = kWaveBytes + al(8 * sizeof(unsigned long long)) + al(64);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_setup_mu;
+void* g_scratch_addr[256] = {};   // per device, resolved once
+
+ftb_status na_fail(ftb_status s, const std::string& m) {
+    ftb::set_last_error(m);
+    return s;
+}
+
+void carve(ftb::Wave& w, char* p, int32_t W) {
+    auto take = [&](size_t n) { void* r = p; p += al(n); return r; };
+    size_t wn = (size_t)W, sn = 2 * (size_t)W;
+    w = ftb::Wave{};
+    w.W = W;
+    w.S = (int32_t)sn;
+    w.rng_s = (uint64_t*)take(8 * wn); w.rng_i = (uint64_t*)take(8 * wn);
+    w.ox = (double*)take(8 * wn); w.oy = (double*)take(8 * wn); w.oz = (double*)take(8 * wn);
+    w.dx = (double*)take(8 * wn); w.dy = (double*)take(8 * wn); w.dz = (double*)take(8 * wn);
+    w.lam = (double*)take(8 * wn); w.beta = (double*)take(8 * wn);
+    w.stk_n = (int32_t*)take(4 * wn); w.stk = (int2*)take(8 * wn * ftb::kStkCap);
+    w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn);
+    w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
+    w.counts = (int32_t*)take(64);
+    w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
+    w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
+    w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
+    w.spix = (int32_t*)take(4 * sn);
+}
+
+int default_frac_bits(int64_t n) {   // the same default as the other render entry points
+    int lg = 0;
+    while (lg < 62 && ((int64_t)1 << lg) < n) ++lg;
+    int f = 62 - lg - 20;
+    return f < 4 ? 4 : (f > 40 ? 40 : f);
+}
+
+}  // namespace
+
+extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_camera* cam,
+                                                 const ftb_render_params* p, int64_t* d_film,
+                                                 ftb_film_info* info, ftb_energy* energy,
+                                                 void* stream) {
+    DevScene dev;
+    int device = 0, sms = 0;
+    double power = 0.0;
+    if (!scene || !cam || !p || !d_film) return na_fail(FTB_ERR_INVALID, "null argument");
+    if (!ftb::scene_internals(scene, &dev, &device, &sms, &power)) return na_fail(FTB_ERR_INVALID, "bad scene");
+    if (p->n_photons < 0 || p->max_bounce < 0 || p->max_bounce > 1024 || p->frac_bits > 56 ||
+        cam->res_x <= 0 || cam->res_y <= 0)
+        return na_fail(FTB_ERR_INVALID, "bad render parameters");
+    if (p->n_photons > kNoAllocPhotons)
+        return na_fail(FTB_ERR_TOO_LARGE, "ftb_render_forward_noalloc: at most " + std::to_string(kNoAllocPhotons) +
+                                              " photons per call (its scratch is a fixed device array); "
+                                              "split the render into calls with consecutive seed_base");
+    if (!(power > 0.0)) return na_fail(FTB_ERR_UNSUPPORTED, "scene emits no power");
+    if (device < 0 || device >= 256) return na_fail(FTB_ERR_INVALID, "device index out of range");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != device) cudaSetDevice(device);
+    char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_setup_mu);
+        if (!g_scratch_addr[device]) {
+            void* ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                if (prev != device) cudaSetDevice(prev);
+                return na_fail(FTB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            }
+            g_scratch_addr[device] = ptr;
+        }
+        base = (char*)g_scratch_addr[device];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    ftb::Wave w;
+    carve(w, base, kNoAllocPhotons);
+    unsigned long long* tally = (unsigned long long*)(base + kWaveBytes);
+    int32_t* status = (int32_t*)(base + kWaveBytes + al(8 * sizeof(unsigned long long)));
+    const int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
+    ftb::Frame f;
+    f.film = d_film;
+    f.tally = tally;
+    f.stats = nullptr;
+    f.status = status;
+    f.film_scale_inv = std::ldexp(1.0, frac) / power;
+    f.tally_scale_inv = std::ldexp(1.0, 32) / power;
+    DevCam dc;
+    for (int i = 0; i < 3; ++i) { dc.eye[i] = cam->eye[i]; dc.u[i] = cam->u[i]; dc.v[i] = cam->v[i]; dc.w[i] = cam->w[i]; }
+    dc.thx = cam->tan_half_x; dc.thy = cam->tan_half_y; dc.rx = cam->res_x; dc.ry = cam->res_y;
+    ftb_status out = FTB_OK;
+    cudaError_t e = cudaMemsetAsync(tally, 0, 8 * sizeof(unsigned long long), st);   // tallies start at zero
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 64, st);
+    if (e == cudaSuccess && p->n_photons > 0)
+        e = ftb::launch_wave(dev, dc, w, f, p->seed_base, (int32_t)p->n_photons, p->max_bounce, sms, st, nullptr);
+    if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    if (out == FTB_OK && info) {
+        info->frac_bits = frac;
+        info->scale = power * std::ldexp(1.0, -frac);
+        info->power_ref = power;
+    }
+    if (out == FTB_OK && energy) {
+        unsigned long long fx[5] = {0, 0, 0, 0, 0};
+        int32_t stv = 0;
+        e = cudaMemcpyAsync(fx, tally, sizeof fx, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&stv, status, sizeof stv, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("readback: ") + cudaGetErrorString(e));
+        else if (stv) out = na_fail(FTB_ERR_DEVICE_LIMIT, "device reported status " + std::to_string(stv));
+        else {
+            double k = power * std::ldexp(1.0, -32);
+            double v[5];
+            for (int i = 0; i < 5; ++i) v[i] = (double)(long long)fx[i] * k;
+            energy->emitted += v[0]; energy->absorbed += v[1]; energy->sensor += v[2];
+            energy->escaped += v[3]; energy->residual += v[4];
+            for (int i = 0; i < 5; ++i) energy->fx[i] += (int64_t)fx[i];
+        }
+    }
+    if (prev != device) cudaSetDevice(prev);
+    return out;
+}

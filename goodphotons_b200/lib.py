@@ -68,6 +68,9 @@ def load(path=None):
     _sig(L, "ftb_session_end", st, PS)
     _sig(L, "ftb_trace_log", st, PS, C.POINTER(abi.Camera), C.POINTER(abi.RenderParams),
          C.POINTER(abi.PhotonLog))
+    _sig(L, "ftb_render_forward_noalloc", st, PS, C.POINTER(abi.Camera),
+         C.POINTER(abi.RenderParams), C.c_void_p, C.POINTER(abi.FilmInfo),
+         C.POINTER(abi.Energy), C.c_void_p)
     _sig(L, "ftb_scene_set_profiling", st, PS, C.c_int32)
     _sig(L, "ftb_scene_profile", st, PS, C.POINTER(abi.KernelProfile), C.c_int32)
     w = _Lib(L)

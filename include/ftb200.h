@@ -284,6 +284,26 @@ typedef struct ftb_photon_log {
 ftb_status ftb_trace_log(ftb_scene* scene, const ftb_camera* cam,
                          const ftb_render_params* params, ftb_photon_log* out);
 
+/* ---- rendering without device allocation (no counterpart in the reference) ----------
+ * For callers that cannot call cudaMalloc: hosts that own all device memory and forbid
+ * allocation inside their render callbacks (engine / DCC plug-in hosts with their own
+ * allocator), frame loops that must not allocate once running, and code for which a
+ * cudaMalloc or cudaFree would synchronize the device mid-stream.  Create the scene once at
+ * start-up (ftb_scene_create allocates); then this call only launches kernels and async
+ * memsets on `stream`, accumulating into the caller's DEVICE film like
+ * ftb_render_forward_device.  Its scratch (one wave of path state, queues, shadow records,
+ * tallies and status: ~9.5 MB) is a fixed device array in the library, held by every GPU
+ * that loads the library until exit.  Limit: n_photons <= FTB_NOALLOC_MAX_PHOTONS per call
+ * (larger requests return FTB_ERR_TOO_LARGE; render more with consecutive seed_base).  The
+ * first call on a device resolves the array's device address (cudaGetSymbolAddress) with
+ * that device current: make it before any stream capture.  All calls share the one array,
+ * so calls that overlap on the GPU (other streams, other threads) race; serialize them.
+ * energy != NULL synchronizes `stream` and also checks the device status word. */
+#define FTB_NOALLOC_MAX_PHOTONS 32768
+ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_camera* cam,
+                                      const ftb_render_params* params, int64_t* d_film,
+                                      ftb_film_info* info, ftb_energy* energy, void* stream);
+
 /* ---- profiling (measurement support; no counterpart in the reference, which times
  * whole renders by wall clock) ---------------------------------------------------------
  * mode 0: off.  mode 1: every kernel launch of this scene's renders is bracketed by CUDA

@@ -105,7 +105,7 @@ class PhotonLog(C.Structure):
 
 
 class KernelProfile(C.Structure):
-    _fields_ = [("ms", C.c_double * 4), ("launches", C.c_int64 * 4), ("counters", C.c_uint64 * 6)]
+    _fields_ = [("ms", C.c_double * 4), ("launches", C.c_int64 * 4), ("counters", C.c_uint64 * 8)]
 
 
 STRUCTS = {

@@ -232,7 +232,7 @@ ftb_status check_desc(const ftb_scene_desc* d) {
         (d->n_emitters && (!d->emitters || !d->emitter_cdf)) || (d->n_media && !d->media))
         return fail(FTB_ERR_INVALID, "null array for a nonzero count");
     int64_t np = d->n_tris + d->n_spheres + d->n_curves;
-    if (np > (int64_t)INT32_MAX / 2) return fail(FTB_ERR_TOO_LARGE, "too many primitives (max 2^30)");
+    if (np > ((int64_t)1 << 29)) return fail(FTB_ERR_TOO_LARGE, "too many primitives (max 2^29)");
     std::string why;
     for (int i = 0; i < d->n_spectra; ++i)
         if (!spec_valid(d, i, why)) return fail(FTB_ERR_INVALID, "spectrum " + std::to_string(i) + ": " + why);
@@ -783,7 +783,7 @@ ftb_status ftb_scene_profile(ftb_scene* s, ftb_kernel_profile* out, int32_t rese
         CK(cudaDeviceSynchronize(), "sync");
         unsigned long long c[8];
         CK(cudaMemcpy(c, s->stats, sizeof c, cudaMemcpyDeviceToHost), "stats readback");
-        for (int k = 0; k < 6; ++k) out->counters[k] = c[k];
+        for (int k = 0; k < 8; ++k) out->counters[k] = c[k];
         if (reset) CK(cudaMemset(s->stats, 0, sizeof c), "stats reset");
     }
     return FTB_OK;

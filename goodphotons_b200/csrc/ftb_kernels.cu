@@ -446,39 +446,40 @@ __device__ __forceinline__ uint32_t byte_of(uint2 w, int i) {
 
 #define T_LO (1.0f - 4.76837158203125e-7f)   // 1 - 2^-21
 #define T_HI (1.0f + 4.76837158203125e-7f)
+#define T_CULL (1.0f + 1.9073486328125e-6f)  // 1 + 2^-19: covers the key's slot bits (< 8 ulps)
 
-// Test the 8 children of a node; returns the child-hit mask and fills tn[].
-__device__ __forceinline__ uint32_t node_children(const uint4 (&n)[5], const RayF& R, float tmin_f,
-                                                  float tmax_f, float (&tn)[8]) {
+struct NodeRay {   // per-node slab constants: t(q) = q * a + b
+    float ax, bx, ay, by, az, bz;
+    uint2 lox, loy, loz, hix, hiy, hiz, meta;
+};
+__device__ __forceinline__ NodeRay node_setup(const uint4 (&n)[5], const RayF& R) {
+    NodeRay N;
     float px = __uint_as_float(n[0].x), py = __uint_as_float(n[0].y), pz = __uint_as_float(n[0].z);
     float sx = __uint_as_float((n[0].w & 0xffu) << 23);
     float sy = __uint_as_float(((n[0].w >> 8) & 0xffu) << 23);
     float sz = __uint_as_float(((n[0].w >> 16) & 0xffu) << 23);
-    // t(q) = q * (s * inv) + (p - o) * inv
-    float ax = sx * R.ix, bx = (px - R.ox) * R.ix;
-    float ay = sy * R.iy, by = (py - R.oy) * R.iy;
-    float az = sz * R.iz, bz = (pz - R.oz) * R.iz;
-    uint2 lox = make_uint2(n[2].x, n[2].y), loy = make_uint2(n[2].z, n[2].w), loz = make_uint2(n[3].x, n[3].y);
-    uint2 hix = make_uint2(n[3].z, n[3].w), hiy = make_uint2(n[4].x, n[4].y), hiz = make_uint2(n[4].z, n[4].w);
-    if (R.nx) { uint2 t = lox; lox = hix; hix = t; }
-    if (R.ny) { uint2 t = loy; loy = hiy; hiy = t; }
-    if (R.nz) { uint2 t = loz; loz = hiz; hiz = t; }
-    uint2 meta = make_uint2(n[1].z, n[1].w);
-    uint32_t mask = 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        float tnx = __fmaf_rn((float)byte_of(lox, i), ax, bx);
-        float tfx = __fmaf_rn((float)byte_of(hix, i), ax, bx);
-        float tny = __fmaf_rn((float)byte_of(loy, i), ay, by);
-        float tfy = __fmaf_rn((float)byte_of(hiy, i), ay, by);
-        float tnz = __fmaf_rn((float)byte_of(loz, i), az, bz);
-        float tfz = __fmaf_rn((float)byte_of(hiz, i), az, bz);
-        float a = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin_f)) * T_LO;
-        float b = fminf(fminf(tfx, tfy), fminf(tfz, tmax_f)) * T_HI;
-        tn[i] = a;
-        if (a <= b && byte_of(meta, i) != 0) mask |= 1u << i;
-    }
-    return mask;
+    N.ax = sx * R.ix; N.bx = (px - R.ox) * R.ix;
+    N.ay = sy * R.iy; N.by = (py - R.oy) * R.iy;
+    N.az = sz * R.iz; N.bz = (pz - R.oz) * R.iz;
+    N.lox = make_uint2(n[2].x, n[2].y); N.loy = make_uint2(n[2].z, n[2].w); N.loz = make_uint2(n[3].x, n[3].y);
+    N.hix = make_uint2(n[3].z, n[3].w); N.hiy = make_uint2(n[4].x, n[4].y); N.hiz = make_uint2(n[4].z, n[4].w);
+    if (R.nx) { uint2 t = N.lox; N.lox = N.hix; N.hix = t; }
+    if (R.ny) { uint2 t = N.loy; N.loy = N.hiy; N.hiy = t; }
+    if (R.nz) { uint2 t = N.loz; N.loz = N.hiz; N.hiz = t; }
+    N.meta = make_uint2(n[1].z, n[1].w);
+    return N;
+}
+// Slab test of child i; returns the entry distance or +inf when missed / empty.
+__device__ __forceinline__ float child_t(const NodeRay& N, int i, float tmin_f, float tmax_f) {
+    float tnx = __fmaf_rn((float)byte_of(N.lox, i), N.ax, N.bx);
+    float tfx = __fmaf_rn((float)byte_of(N.hix, i), N.ax, N.bx);
+    float tny = __fmaf_rn((float)byte_of(N.loy, i), N.ay, N.by);
+    float tfy = __fmaf_rn((float)byte_of(N.hiy, i), N.ay, N.by);
+    float tnz = __fmaf_rn((float)byte_of(N.loz, i), N.az, N.bz);
+    float tfz = __fmaf_rn((float)byte_of(N.hiz, i), N.az, N.bz);
+    float a = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin_f)) * T_LO;
+    float b = fminf(fminf(tfx, tfy), fminf(tfz, tmax_f)) * T_HI;
+    return (a <= b && byte_of(N.meta, i) != 0) ? a : __int_as_float(0x7f800000);
 }
 
 __device__ __forceinline__ void load_node(const WNode* nodes, uint32_t i, uint4 (&n)[5]) {
@@ -486,118 +487,154 @@ __device__ __forceinline__ void load_node(const WNode* nodes, uint32_t i, uint4 
     n[0] = __ldg(p); n[1] = __ldg(p + 1); n[2] = __ldg(p + 2); n[3] = __ldg(p + 3); n[4] = __ldg(p + 4);
 }
 
-struct TravCount { unsigned long long nodes, recs; };
+struct TravCount { unsigned long long nodes, recs, exact; };
 
-// Closest hit: returns the record index (or -1) and t.
+
+// Stack entry: a node index, or (bit 31) a leaf: first record << 2 | (count - 1).
+#define LEAF_BIT 0x80000000u
+__device__ __forceinline__ uint32_t child_entry(uint32_t child_base, uint32_t prim_base, uint32_t imask,
+                                                uint2 meta, int i) {
+    uint32_t m = byte_of(meta, i);
+    if ((imask >> i) & 1u) return child_base + (m & 31u);
+    return LEAF_BIT | ((prim_base + (m & 31u)) << 2) | ((m >> 5) - 1u);
+}
+
+// One record: the exact fp64 acceptance test.
+template <bool COUNT>
+__device__ __forceinline__ bool record_hit(const DevScene& sc, const RayCtx& R, int ri, double tmin, double tbest,
+                                           double& t, TravCount& cnt) {
+    if (COUNT) { cnt.recs++; cnt.exact++; }
+    PrimRec r;
+    load_rec(sc.recs, ri, r);
+    return rec_test(R, r, tmin, tbest, t);
+}
+
+#define CSWAP(a, b) { uint32_t lo_ = min(a, b); b = max(a, b); a = lo_; }
+
+// Closest hit: returns the record index (or -1) and t.  Children of a node are visited near
+// to far (leaves and inner nodes alike, keys sorted by an 8-input network in registers);
+// entries farther than the current hit are culled when popped.  The loop is "while-while":
+// a lane steps through inner nodes until it holds a leaf, so the lanes of a warp run the
+// expensive leaf tests together rather than interleaved with node steps.
 template <bool COUNT>
 __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin, double& best_t,
                                 int32_t* status, TravCount& cnt) {
     RayF F = make_rayf(R.o, R.d);
-    float tmin_f = __double2float_rd(tmin);
+    const float tmin_f = __double2float_rd(tmin);
     best_t = DBL_MAX;
     float tmax_f = FLT_MAX;
     int best = -1;
-    uint32_t st_node[FTB_STACK];
+    uint32_t st_e[FTB_STACK];
     float st_t[FTB_STACK];
     int sp = 0;
-    uint32_t node = 0;
-    while (true) {
-        uint4 n[5];
-        load_node(sc.nodes, node, n);
-        if (COUNT) cnt.nodes++;
-        float tn[8];
-        uint32_t hit = node_children(n, F, tmin_f, tmax_f, tn);
-        uint32_t imask = n[0].w >> 24;
-        uint32_t child_base = n[1].x, prim_base = n[1].y;
-        uint2 meta = make_uint2(n[1].z, n[1].w);
-        // leaves first: they can only shrink best_t
-        uint32_t leaves = hit & ~imask;
-        while (leaves) {
-            int i = __ffs(leaves) - 1;
-            leaves &= leaves - 1;
-            uint32_t m = byte_of(meta, i);
-            int nrec = m >> 5, off = m & 31;
-            for (int k = 0; k < nrec; ++k) {
-                PrimRec r;
-                int ri = (int)prim_base + off + k;
-                load_rec(sc.recs, ri, r);
-                if (COUNT) cnt.recs++;
+    uint32_t cur = 0;
+    bool live = true;
+    while (live) {
+        while (!(cur & LEAF_BIT)) {
+            uint4 n[5];
+            load_node(sc.nodes, cur, n);
+            if (COUNT) cnt.nodes++;
+            NodeRay N = node_setup(n, F);
+            uint32_t k[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                float t = child_t(N, i, tmin_f, tmax_f);
+                k[i] = (t == __int_as_float(0x7f800000)) ? 0xffffffffu : ((__float_as_uint(t) & ~7u) | (uint32_t)i);
+            }
+            CSWAP(k[0], k[2]); CSWAP(k[1], k[3]); CSWAP(k[4], k[6]); CSWAP(k[5], k[7]);
+            CSWAP(k[0], k[4]); CSWAP(k[1], k[5]); CSWAP(k[2], k[6]); CSWAP(k[3], k[7]);
+            CSWAP(k[0], k[1]); CSWAP(k[2], k[3]); CSWAP(k[4], k[5]); CSWAP(k[6], k[7]);
+            CSWAP(k[2], k[4]); CSWAP(k[3], k[5]);
+            CSWAP(k[1], k[4]); CSWAP(k[3], k[6]);
+            CSWAP(k[1], k[2]); CSWAP(k[3], k[4]); CSWAP(k[5], k[6]);
+            const uint32_t imask = n[0].w >> 24, child_base = n[1].x, prim_base = n[1].y;
+#pragma unroll
+            for (int i = 7; i >= 1; --i) {
+                if (k[i] != 0xffffffffu) {
+                    if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return best; }
+                    st_e[sp] = child_entry(child_base, prim_base, imask, N.meta, (int)(k[i] & 7u));
+                    st_t[sp] = __uint_as_float(k[i] & ~7u);
+                    ++sp;
+                }
+            }
+            if (k[0] != 0xffffffffu) {
+                cur = child_entry(child_base, prim_base, imask, N.meta, (int)(k[0] & 7u));
+                continue;
+            }
+            bool found = false;
+            while (sp > 0) {
+                --sp;
+                if (st_t[sp] <= tmax_f * T_CULL) { cur = st_e[sp]; found = true; break; }
+            }
+            if (!found) { live = false; break; }
+        }
+        if (!live) break;
+        {   // leaf phase
+            int first = (int)((cur & ~LEAF_BIT) >> 2), count = (int)(cur & 3u) + 1;
+            for (int k = 0; k < count; ++k) {
                 double t;
-                if (rec_test(R, r, tmin, best_t, t)) { best_t = t; best = ri; tmax_f = __double2float_ru(t); }
+                if (record_hit<COUNT>(sc, R, first + k, tmin, best_t, t, cnt)) {
+                    best_t = t; best = first + k; tmax_f = __double2float_ru(t);
+                }
             }
         }
-        // internal children: continue with the nearest, push the rest
-        uint32_t inner = hit & imask;
-        int next = -1;
-        float next_t = FLT_MAX;
-        while (inner) {
-            int i = __ffs(inner) - 1;
-            inner &= inner - 1;
-            float t = tn[i];
-            if (t > tmax_f * T_HI) continue;
-            uint32_t ci = child_base + (byte_of(meta, i) & 31);
-            if (next < 0) { next = (int)ci; next_t = t; continue; }
-            if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return best; }
-            if (t < next_t) { st_node[sp] = (uint32_t)next; st_t[sp] = next_t; ++sp; next = (int)ci; next_t = t; }
-            else { st_node[sp] = ci; st_t[sp] = t; ++sp; }
-        }
-        if (next >= 0) { node = (uint32_t)next; continue; }
         bool found = false;
         while (sp > 0) {
             --sp;
-            if (st_t[sp] <= tmax_f * T_HI) { node = st_node[sp]; found = true; break; }
+            if (st_t[sp] <= tmax_f * T_CULL) { cur = st_e[sp]; found = true; break; }
         }
         if (!found) break;
     }
     return best;
 }
 
-// Any hit with t in [tmin, seg) (Scene::occluded, scene.h:2249-2271).
+// Any hit with t in [tmin, seg) (Scene::occluded, scene.h:2249-2271).  Order does not
+// change the answer, so children are taken in slot order, leaves first; the loop is
+// while-while like traverse_closest.
 template <bool COUNT>
 __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, double seg, int32_t* status,
                              TravCount& cnt) {
     RayF F = make_rayf(R.o, R.d);
-    float tmin_f = __double2float_rd(tmin);
-    float tmax_f = __double2float_ru(seg);
-    uint32_t st_node[FTB_STACK];
+    const float tmin_f = __double2float_rd(tmin);
+    const float tmax_f = __double2float_ru(seg);
+    uint32_t st_e[FTB_STACK];
     int sp = 0;
-    uint32_t node = 0;
-    while (true) {
-        uint4 n[5];
-        load_node(sc.nodes, node, n);
-        if (COUNT) cnt.nodes++;
-        float tn[8];
-        uint32_t hit = node_children(n, F, tmin_f, tmax_f, tn);
-        uint32_t imask = n[0].w >> 24;
-        uint32_t child_base = n[1].x, prim_base = n[1].y;
-        uint2 meta = make_uint2(n[1].z, n[1].w);
-        uint32_t leaves = hit & ~imask;
-        while (leaves) {
-            int i = __ffs(leaves) - 1;
-            leaves &= leaves - 1;
-            uint32_t m = byte_of(meta, i);
-            int nrec = m >> 5, off = m & 31;
-            for (int k = 0; k < nrec; ++k) {
-                PrimRec r;
-                load_rec(sc.recs, (int)prim_base + off + k, r);
-                if (COUNT) cnt.recs++;
-                double t;
-                if (rec_test(R, r, tmin, seg, t)) return true;
+    uint32_t cur = 0;
+    bool live = true;
+    while (live) {
+        while (!(cur & LEAF_BIT)) {
+            uint4 n[5];
+            load_node(sc.nodes, cur, n);
+            if (COUNT) cnt.nodes++;
+            NodeRay N = node_setup(n, F);
+            uint32_t hit = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (child_t(N, i, tmin_f, tmax_f) != __int_as_float(0x7f800000)) hit |= 1u << i;
+            const uint32_t imask = n[0].w >> 24, child_base = n[1].x, prim_base = n[1].y;
+            uint32_t order = (hit & ~imask) | ((hit & imask) << 8);
+            bool have_next = false;
+            uint32_t next = 0;
+            while (order) {
+                int b = __ffs(order) - 1;
+                order &= order - 1;
+                uint32_t e = child_entry(child_base, prim_base, imask, N.meta, b & 7);
+                if (!have_next) { next = e; have_next = true; continue; }
+                if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return false; }
+                st_e[sp++] = e;
             }
+            if (have_next) { cur = next; continue; }
+            if (sp == 0) { live = false; break; }
+            cur = st_e[--sp];
         }
-        uint32_t inner = hit & imask;
-        int next = -1;
-        while (inner) {
-            int i = __ffs(inner) - 1;
-            inner &= inner - 1;
-            uint32_t ci = child_base + (byte_of(meta, i) & 31);
-            if (next < 0) { next = (int)ci; continue; }
-            if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return false; }
-            st_node[sp++] = ci;
+        if (!live) break;
+        int first = (int)((cur & ~LEAF_BIT) >> 2), count = (int)(cur & 3u) + 1;
+        for (int k = 0; k < count; ++k) {
+            double t;
+            if (record_hit<COUNT>(sc, R, first + k, tmin, seg, t, cnt)) return true;
         }
-        if (next >= 0) { node = (uint32_t)next; continue; }
         if (sp == 0) break;
-        node = st_node[--sp];
+        cur = st_e[--sp];
     }
     return false;
 }
@@ -905,11 +942,25 @@ __device__ void block_add3(unsigned long long* dst, unsigned long long a, unsign
     }
 }
 
+__device__ void block_add1(unsigned long long* dst, unsigned long long a) {
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0 && a) atomicAdd(dst, a);
+}
+
+// Resident blocks per SM the traversal and shading kernels are compiled for (register
+// budget 65536 / (128 x minB)); chosen by measurement on B200.
+#ifndef FTB_TRAV_MINB
+#define FTB_TRAV_MINB 8
+#endif
+#ifndef FTB_SHADE_MINB
+#define FTB_SHADE_MINB 4
+#endif
+
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_extend(DevScene sc, Wave w, const int32_t* q, const int32_t* qcount,
+__global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(DevScene sc, Wave w, const int32_t* q, const int32_t* qcount,
                                                 Frame f) {
     int nq = *qcount;
-    TravCount cnt{0, 0};
+    TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
         int slot = q[i];
@@ -920,7 +971,10 @@ __global__ void __launch_bounds__(128) k_extend(DevScene sc, Wave w, const int32
         w.hit_rec[slot] = rec;
         if (COUNT) rays++;
     }
-    if (COUNT) block_add3(f.stats, rays, cnt.nodes, cnt.recs);
+    if (COUNT) {
+        block_add3(f.stats, rays, cnt.nodes, cnt.recs);
+        block_add1(f.stats + 6, cnt.exact);
+    }
 }
 
 // medium stack (medium_stack.h:17-47), kStkCap entries per slot
@@ -985,7 +1039,7 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 }
 
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
-__global__ void __launch_bounds__(128) k_shade(DevScene sc, DevCam cam, Wave w, Frame f, const int32_t* qin,
+__global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(DevScene sc, DevCam cam, Wave w, Frame f, const int32_t* qin,
                                                const int32_t* qin_count, int32_t* qout, int32_t* qout_count,
                                                uint64_t photon0, int32_t bounce, int32_t max_bounce) {
     long long t_abs = 0, t_esc = 0, t_res = 0;
@@ -1144,10 +1198,10 @@ __global__ void __launch_bounds__(128) k_shade(DevScene sc, DevCam cam, Wave w, 
 
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_shadow(DevScene sc, Wave w, Frame f) {
+__global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(DevScene sc, Wave w, Frame f) {
     int n = w.counts[2];
     if (n > w.S) n = w.S;
-    TravCount cnt{0, 0};
+    TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
@@ -1163,7 +1217,10 @@ __global__ void __launch_bounds__(128) k_shadow(DevScene sc, Wave w, Frame f) {
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, f.film_scale_inv, f.status));
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
     }
-    if (COUNT) block_add3(f.stats + 3, rays, cnt.nodes, cnt.recs);
+    if (COUNT) {
+        block_add3(f.stats + 3, rays, cnt.nodes, cnt.recs);
+        block_add1(f.stats + 7, cnt.exact);
+    }
 }
 
 // ------------------------------------------------------------------ host side ----------

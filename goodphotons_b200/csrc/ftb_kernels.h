@@ -46,9 +46,10 @@ struct Wave {
 struct Frame {
     int64_t* film;             // 4 words per pixel
     unsigned long long* tally; // 5 fixed-point energy tallies
-    unsigned long long* stats; // traversal counters (counting variant only, else null):
+    unsigned long long* stats; // traversal counters (counting variant only, else null), 8:
                                // [0] closest-hit rays [1] their node visits [2] their record
                                // tests [3] any-hit rays [4] node visits [5] record tests
+                               // [6] closest-hit / [7] any-hit exact (fp64) record tests
     int32_t* status;
     double film_scale_inv;     // 2^frac / power_ref
     double tally_scale_inv;    // 2^32 / power_ref

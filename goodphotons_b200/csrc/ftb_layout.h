@@ -84,8 +84,7 @@ struct DevScene {
     int32_t n_nodes, n_recs, n_mats, n_emit, n_med, n_spec;
     int64_t n_tris;
     double total_power;
-    int32_t root_is_leaf;     // scene with <= FTB_LEAF_MAX prims: root node is a leaf holder
-    int32_t pad;
+
 };
 
 struct DevCam {

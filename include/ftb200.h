@@ -313,8 +313,9 @@ ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_camera* cam,
 typedef struct ftb_kernel_profile {
     double ms[4];          /* summed launch durations: emit, extend, shade, shadow */
     int64_t launches[4];
-    uint64_t counters[6];  /* mode 2: closest-hit rays, their node visits, their record
-                              tests; any-hit rays, node visits, record tests */
+    uint64_t counters[8];  /* mode 2: closest-hit rays, their node visits, their record
+                              tests; any-hit rays, node visits, record tests; the record
+                              tests that reached the exact fp64 test (closest, any) */
 } ftb_kernel_profile;
 
 ftb_status ftb_scene_set_profiling(ftb_scene* scene, int32_t mode);

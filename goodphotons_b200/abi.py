@@ -104,6 +104,11 @@ class PhotonLog(C.Structure):
                 ("beta", C.c_double), ("prims", C.c_int32 * 8)]
 
 
+class Job(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("cam", Camera), ("d_film", C.c_void_p), ("n_photons", C.c_int64),
+                ("seed_base", C.c_uint64), ("max_bounce", C.c_int32), ("frac_bits", C.c_int32)]
+
+
 class KernelProfile(C.Structure):
     _fields_ = [("ms", C.c_double * 4), ("launches", C.c_int64 * 4), ("counters", C.c_uint64 * 8)]
 
@@ -113,7 +118,7 @@ STRUCTS = {
     "ftb_medium": Medium, "ftb_scene_desc": SceneDesc, "ftb_camera": Camera,
     "ftb_render_params": RenderParams, "ftb_energy": Energy, "ftb_film_info": FilmInfo,
     "ftb_footprint": Footprint, "ftb_photon_log": PhotonLog,
-    "ftb_kernel_profile": KernelProfile,
+    "ftb_kernel_profile": KernelProfile, "ftb_job": Job,
 }
 
 # every entry point declared in include/ftb200.h
@@ -124,5 +129,6 @@ EXPORTS = [
     "ftb_render_forward_device", "ftb_session_begin", "ftb_session_batch",
     "ftb_session_hits0", "ftb_session_download", "ftb_session_end", "ftb_trace_log",
     "ftb_scene_set_profiling", "ftb_scene_profile", "ftb_render_forward_noalloc",
+    "ftb_render_batch",
 ]
 NOALLOC_MAX_PHOTONS = 32768

@@ -149,6 +149,43 @@ struct ProfSink : ftb::LaunchSink {
 };
 }  // namespace
 
+// ---- job-table staging ------------------------------------------------------------------
+namespace {
+// Pinned host ring from which a wave's job table is copied to the device on the wave's
+// stream; an entry is reused only after its previous copy has completed.
+struct JobStage {
+    static constexpr int kRing = 4;
+    ftb::DevJob* host = nullptr;
+    cudaEvent_t ev[kRing] = {};
+    int next = 0;
+    cudaError_t init() {
+        if (host) return cudaSuccess;
+        cudaError_t e = cudaHostAlloc((void**)&host, sizeof(ftb::DevJob) * ftb::kWaveJobs * kRing, cudaHostAllocDefault);
+        if (e != cudaSuccess) { host = nullptr; return e; }
+        for (auto& v : ev) {
+            e = cudaEventCreateWithFlags(&v, cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    cudaError_t push(const ftb::DevJob* jobs, int n, ftb::DevJob* dst, cudaStream_t st) {
+        int e = next;
+        next = (next + 1) % kRing;
+        cudaError_t r = cudaEventSynchronize(ev[e]);
+        if (r != cudaSuccess) return r;
+        ftb::DevJob* h = host + (size_t)e * ftb::kWaveJobs;
+        std::memcpy(h, jobs, sizeof(ftb::DevJob) * (size_t)n);
+        r = cudaMemcpyAsync(dst, h, sizeof(ftb::DevJob) * (size_t)n, cudaMemcpyHostToDevice, st);
+        if (r != cudaSuccess) return r;
+        return cudaEventRecord(ev[e], st);
+    }
+    ~JobStage() {
+        for (auto v : ev) if (v) cudaEventDestroy(v);
+        if (host) cudaFreeHost(host);
+    }
+};
+}  // namespace
+
 // ---- scene object ----------------------------------------------------------------------
 struct ftb_scene {
     int device = 0;
@@ -161,6 +198,7 @@ struct ftb_scene {
     // cached render resources
     cudaStream_t streams[2] = {nullptr, nullptr};
     ftb::Wave waves[2]{};
+    JobStage stage[2];
     int32_t wave_W = 0;
     bool wave_log = false;
     int64_t* film = nullptr;
@@ -169,6 +207,8 @@ struct ftb_scene {
     int32_t* status = nullptr;
     int32_t prof_mode = 0;
     ProfSink* prof = nullptr;
+    unsigned long long* batch_tally = nullptr;   // 8 words per job of the last batch
+    size_t batch_cap = 0;
     unsigned long long* stats = nullptr;   // device counters for profiling mode 2
     ~ftb_scene() {
         int cur = 0;
@@ -180,6 +220,7 @@ struct ftb_scene {
         if (tally) cudaFree(tally);
         if (status) cudaFree(status);
         if (stats) cudaFree(stats);
+        if (batch_tally) cudaFree(batch_tally);
         delete prof;
         for (void* p : allocs) cudaFree(p);
         cudaSetDevice(cur);
@@ -299,6 +340,7 @@ ftb_status ensure_waves(ftb_scene* s, int32_t W, bool log) {
     }
     for (auto& st : s->streams)
         if (!st) CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream create");
+    for (auto& sg : s->stage) CK(sg.init(), "job staging");
     s->wave_W = W;
     s->wave_log = log;
     return FTB_OK;
@@ -322,38 +364,73 @@ int32_t pick_wave(int64_t n) {
     return (int32_t)std::max<int64_t>(W, 1);
 }
 
-// Trace n photons from seed_base into d_film / tally, on the scene's streams, and wait.
-ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t seed_base, int32_t max_bounce,
-                       int32_t frac_bits, int64_t* d_film, unsigned long long* d_tally, ftb_photon_log* d_logs,
-                       cudaStream_t user_stream) {
-    bool log = d_logs != nullptr;
-    int32_t W = pick_wave(n);
+ftb::DevJob make_job(const ftb_scene* s, const ftb_camera* cam, int64_t* d_film, unsigned long long* d_tally,
+                     int32_t frac_bits, int32_t max_bounce) {
+    ftb::DevJob J;
+    std::memset(&J, 0, sizeof J);
+    J.sc = s->dev;
+    J.cam = dev_cam(cam);
+    J.film = d_film;
+    J.tally = d_tally;
+    J.film_scale_inv = std::ldexp(1.0, frac_bits) / s->power;
+    J.tally_scale_inv = std::ldexp(1.0, 32) / s->power;
+    J.max_bounce = max_bounce;
+    return J;
+}
+
+// A piece of a job placed in one wave.
+struct Segment { int job; int64_t first; int32_t n; };
+
+// Pack jobs' photon ranges into waves of at most W slots and kWaveJobs segments, launch
+// them alternately on the scene's two streams (handing off from and back to `user_stream`).
+// `base[j]` is job j's DevJob template; each segment gets its photon0 / slot range.
+ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const std::vector<int64_t>& count,
+                    const std::vector<uint64_t>& seed, bool log, ftb_photon_log* d_logs, int64_t log_base,
+                    cudaStream_t user_stream) {
+    int64_t total = 0;
+    for (auto c : count) total += c;
+    int32_t W = pick_wave(total);
     ftb_status st = ensure_waves(s, W, log);
     if (st != FTB_OK) return st;
+    W = s->wave_W;
     ftb::Frame f;
-    f.film = d_film;
-    f.tally = d_tally;
     f.stats = s->prof_mode == 2 ? s->stats : nullptr;
     f.status = s->status;
-    f.film_scale_inv = std::ldexp(1.0, frac_bits) / s->power;
-    f.tally_scale_inv = std::ldexp(1.0, 32) / s->power;
-    DevCam dc = dev_cam(cam);
-    // hand off from the caller's stream (0 = legacy stream) to the two wave streams and back
     cudaEvent_t ready = nullptr;
     CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
     CK(cudaEventRecord(ready, user_stream), "event record");
     for (auto st2 : s->streams) CK(cudaStreamWaitEvent(st2, ready, 0), "stream wait");
-    int64_t done = 0;
+    size_t j = 0;
+    int64_t done_in_job = 0;
     int k = 0;
-    while (done < n) {
-        int32_t m = (int32_t)std::min<int64_t>(W, n - done);
+    std::vector<ftb::DevJob> table;
+    while (j < base.size()) {
+        table.clear();
+        int32_t slots = 0, max_bounce = 0;
+        while (j < base.size() && slots < W && (int)table.size() < ftb::kWaveJobs) {
+            int64_t left = count[j] - done_in_job;
+            if (left <= 0) { ++j; done_in_job = 0; continue; }
+            int32_t m = (int32_t)std::min<int64_t>(left, (int64_t)(W - slots));
+            ftb::DevJob J = base[j];
+            J.photon0 = seed[j] + (uint64_t)done_in_job;
+            J.slot0 = slots;
+            J.n = m;
+            table.push_back(J);
+            max_bounce = std::max(max_bounce, J.max_bounce);
+            slots += m;
+            done_in_job += m;
+            if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
+        }
+        if (table.empty()) break;
         ftb::Wave& w = s->waves[k & 1];
+        cudaStream_t ws = s->streams[k & 1];
         w.logs = d_logs;
-        w.log_base = (int64_t)seed_base;
-        cudaError_t e = ftb::launch_wave(s->dev, dc, w, f, seed_base + (uint64_t)done, m, max_bounce, s->sms,
-                                         s->streams[k & 1], s->prof_mode ? s->prof : nullptr);
+        w.log_base = log_base;
+        cudaError_t e = s->stage[k & 1].push(table.data(), (int)table.size(), w.jobs, ws);
+        if (e != cudaSuccess) return cuda_fail(e, "job table upload");
+        e = ftb::launch_wave(w, w.jobs, (int32_t)table.size(), slots, max_bounce, f, s->sms, ws,
+                             s->prof_mode ? s->prof : nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-        done += m;
         ++k;
     }
     for (auto st2 : s->streams) {
@@ -362,6 +439,14 @@ ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t 
     }
     cudaEventDestroy(ready);
     return FTB_OK;
+}
+
+// Trace n photons from seed_base into d_film / tally, on the scene's streams.
+ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t seed_base, int32_t max_bounce,
+                       int32_t frac_bits, int64_t* d_film, unsigned long long* d_tally, ftb_photon_log* d_logs,
+                       cudaStream_t user_stream) {
+    std::vector<ftb::DevJob> base{make_job(s, cam, d_film, d_tally, frac_bits, max_bounce)};
+    return run_jobs(s, base, {n}, {seed_base}, d_logs != nullptr, d_logs, (int64_t)seed_base, user_stream);
 }
 
 ftb_status read_status(ftb_scene* s) {
@@ -721,6 +806,62 @@ ftb_status ftb_render_forward(ftb_scene* s, const ftb_camera* cam, const ftb_ren
         unsigned long long fx[5];
         CK(cudaMemcpy(fx, s->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally readback");
         tally_to_energy(fx, s->power, energy, true);
+    }
+    return FTB_OK;
+}
+
+ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n, ftb_film_info* infos, ftb_energy* energies,
+                            void* stream) {
+    if (!jobs || n < 1) return fail(FTB_ERR_INVALID, "empty batch");
+    ftb_scene* s = jobs[0].scene;
+    if (!s) return fail(FTB_ERR_INVALID, "job 0: null scene");
+    for (int j = 0; j < n; ++j) {
+        const ftb_job& b = jobs[j];
+        if (!b.scene || !b.d_film) return fail(FTB_ERR_INVALID, "job " + std::to_string(j) + ": null scene or film");
+        if (b.scene->device != s->device) return fail(FTB_ERR_INVALID, "batch jobs must share one device");
+        ftb_render_params p{b.n_photons, b.seed_base, b.max_bounce, b.frac_bits};
+        ftb_status st = check_params(b.scene, &b.cam, &p);
+        if (st != FTB_OK) return fail(st, "job " + std::to_string(j) + ": " + g_err);
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    DeviceGuard guard(s->device);
+    ftb_status st = ensure_frame(s, 0);
+    if (st != FTB_OK) return st;
+    if (s->batch_cap < (size_t)n) {
+        if (s->batch_tally) cudaFree(s->batch_tally);
+        s->batch_tally = nullptr;
+        s->batch_cap = 0;
+        CK(cudaMalloc(&s->batch_tally, sizeof(unsigned long long) * 8 * (size_t)n), "batch tallies");
+        s->batch_cap = (size_t)n;
+    }
+    cudaStream_t us = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(s->batch_tally, 0, sizeof(unsigned long long) * 8 * (size_t)n, us), "memset");
+    CK(cudaMemsetAsync(s->status, 0, 64, us), "memset");
+    std::vector<ftb::DevJob> base;
+    std::vector<int64_t> count;
+    std::vector<uint64_t> seed;
+    for (int j = 0; j < n; ++j) {
+        const ftb_job& b = jobs[j];
+        int frac = b.frac_bits > 0 ? b.frac_bits : default_frac_bits(b.n_photons);
+        base.push_back(make_job(b.scene, &b.cam, b.d_film, s->batch_tally + 8 * (size_t)j, frac, b.max_bounce));
+        count.push_back(b.n_photons);
+        seed.push_back(b.seed_base);
+        if (infos) {
+            infos[j].frac_bits = frac;
+            infos[j].scale = b.scene->power * std::ldexp(1.0, -frac);
+            infos[j].power_ref = b.scene->power;
+        }
+    }
+    st = run_jobs(s, base, count, seed, false, nullptr, 0, us);
+    if (st != FTB_OK) return st;
+    if (energies) {
+        CK(cudaStreamSynchronize(us), "sync");
+        st = read_status(s);
+        if (st != FTB_OK) return st;
+        std::vector<unsigned long long> fx(8 * (size_t)n);
+        CK(cudaMemcpy(fx.data(), s->batch_tally, fx.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+           "tally readback");
+        for (int j = 0; j < n; ++j) tally_to_energy(&fx[8 * (size_t)j], jobs[j].scene->power, &energies[j], true);
     }
     return FTB_OK;
 }

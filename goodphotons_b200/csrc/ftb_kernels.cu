@@ -772,19 +772,20 @@ __device__ __forceinline__ int agg_inc(int32_t* ctr) {
     return g.shfl(base, 0) + (int)g.thread_rank();
 }
 
-__device__ __forceinline__ void push_shadow(const Wave& w, const Frame& f, D3 o, D3 d, double tmax, double val,
-                                            double lam, int pix) {
+__device__ __forceinline__ void push_shadow(const Wave& w, const Frame& f, int job, D3 o, D3 d, double tmax,
+                                            double val, double lam, int pix) {
     int i = agg_inc(&w.counts[2]);
     if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
     w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
     w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
     w.smax[i] = tmax; w.sval[i] = val; w.slam[i] = lam; w.spix[i] = pix;
+    w.sjob[i] = job;
 }
 
 // connectGeom + connect, model B (render.h:499-559); the occlusion test is deferred to
 // k_shadow, the rest of the contribution is formed here in the reference's order.
-__device__ void connect_surface(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f, D3 p,
-                                D3 n, D3 ng, D3 wi, double lam, double beta, double rho) {
+__device__ void connect_surface(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f, int job,
+                                D3 p, D3 n, D3 ng, D3 wi, double lam, double beta, double rho) {
     D3 to_cam = ld3(cam.eye) - p;
     double dist = len(to_cam);
     D3 wdir = to_cam / dist;
@@ -800,10 +801,10 @@ __device__ void connect_surface(const DevScene& sc, const DevCam& cam, const Wav
     double fr = rho / PI_D;
     double contrib = beta * fr * cos_surf * corr / denom * stg;
     if (sc.n_med > 0) contrib *= media_transmittance(sc, p, wdir, dist, lam);
-    push_shadow(w, f, p + ng * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+    push_shadow(w, f, job, p + ng * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
 }
 // connectVolume (render.h:584-600)
-__device__ void connect_volume(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f,
+__device__ void connect_volume(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f, int job,
                                const DevMed& m, D3 p, D3 win, double lam, double beta) {
     D3 to_cam = ld3(cam.eye) - p;
     double dist = len(to_cam);
@@ -815,7 +816,7 @@ __device__ void connect_volume(const DevScene& sc, const DevCam& cam, const Wave
     double omega = cam_pixel_solid_angle(cam, cos_cam);
     double contrib = beta * alb * ph / (dist2 * omega);
     contrib *= media_transmittance(sc, p, wdir, dist, lam);
-    push_shadow(w, f, p + wdir * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+    push_shadow(w, f, job, p + wdir * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
 }
 
 // ------------------------------------------------------------------ tallies ------------
@@ -846,6 +847,38 @@ __device__ void block_tally(unsigned long long* dst, long long v) {
 
 enum { T_EMIT = 0, T_ABS = 1, T_SENSOR = 2, T_ESC = 3, T_RES = 4 };
 
+// Per-thread energy tallies.  A single-job wave reduces them over the block once at the
+// end of the kernel; in a multi-job wave a thread flushes its sums to the job's tallies
+// whenever the job of the path it books changes (slots of one job are contiguous, so
+// this is rare) and at the end.
+struct TallyAcc {
+    int job;
+    long long v[5];
+};
+__device__ __forceinline__ void tally_init(TallyAcc& a) {
+    a.job = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) a.v[k] = 0;
+}
+__device__ __forceinline__ void tally_flush(TallyAcc& a, const DevJob* jobs) {
+    unsigned long long* t = jobs[a.job].tally;
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+        if (a.v[k]) { atomicAdd(t + k, (unsigned long long)a.v[k]); a.v[k] = 0; }
+}
+__device__ __forceinline__ void tally_add(TallyAcc& a, const DevJob* jobs, bool multi, int job, int k,
+                                          long long x) {
+    if (multi && job != a.job) { tally_flush(a, jobs); a.job = job; }
+    a.v[k] += x;
+}
+__device__ void block_tally(unsigned long long* dst, long long v);
+__device__ __forceinline__ void tally_finish(TallyAcc& a, const DevJob* jobs, bool multi) {
+    if (multi) { tally_flush(a, jobs); return; }
+    unsigned long long* t = jobs[0].tally;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) block_tally(t + k, a.v[k]);
+}
+
 __device__ __forceinline__ uint64_t fnv_i32(uint64_t h, int32_t v) {
     uint32_t u = (uint32_t)v;
 #pragma unroll
@@ -865,11 +898,22 @@ __device__ __forceinline__ void log_finish(const Wave& w, int slot, uint64_t pho
 }
 
 // ------------------------------------------------------------------ kernels ------------
-__global__ void __launch_bounds__(128) k_emit(DevScene sc, DevCam cam, Wave w, Frame f, uint64_t photon0,
-                                              int32_t n, int32_t max_bounce) {
-    long long t_emit = 0, t_res = 0;
-    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
-        uint64_t k = photon0 + (uint64_t)slot;
+__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, int32_t n_jobs,
+                                              int32_t n_slots, Frame f) {
+    const bool multi = n_jobs > 1;
+    TallyAcc acc;
+    tally_init(acc);
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n_slots; slot += gridDim.x * blockDim.x) {
+        int j = 0;
+        if (multi) {   // the job whose slot range holds this slot
+            int lo = 0, hi = n_jobs - 1;
+            while (lo < hi) { int mid = (lo + hi + 1) / 2; if (jobs[mid].slot0 <= slot) lo = mid; else hi = mid - 1; }
+            j = lo;
+            w.job[slot] = j;
+        }
+        const DevJob& J = jobs[j];
+        const DevScene& sc = J.sc;
+        uint64_t k = J.photon0 + (uint64_t)(slot - J.slot0);
         Pcg rng = seed_photon(k);
         if (w.logs) {
             w.lhash[slot] = 1469598103934665603ULL; w.lnh[slot] = 0;
@@ -910,11 +954,11 @@ __global__ void __launch_bounds__(128) k_emit(DevScene sc, DevCam cam, Wave w, F
         if (pdf <= 0) { log_finish(w, slot, k, 4, 0.0); continue; }
         double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
         beta *= 1.0;
-        t_emit += to_fixed(beta, f.tally_scale_inv, f.status);
-        connect_surface(sc, cam, w, f, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
+        tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(beta, J.tally_scale_inv, f.status));
+        connect_surface(sc, J.cam, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
         D3 ro = origin + dir * 1e-6;
-        if (max_bounce <= 0) {
-            t_res += to_fixed(beta, f.tally_scale_inv, f.status);
+        if (J.max_bounce <= 0) {
+            tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
             log_finish(w, slot, k, 2, beta);
             continue;
         }
@@ -926,8 +970,7 @@ __global__ void __launch_bounds__(128) k_emit(DevScene sc, DevCam cam, Wave w, F
         int q = agg_inc(&w.counts[0]);
         w.qa[q] = slot;
     }
-    block_tally(&f.tally[T_EMIT], t_emit);
-    block_tally(&f.tally[T_RES], t_res);
+    tally_finish(acc, jobs, multi);
 }
 
 __device__ void block_add3(unsigned long long* dst, unsigned long long a, unsigned long long b,
@@ -957,13 +1000,15 @@ __device__ void block_add1(unsigned long long* dst, unsigned long long a) {
 #endif
 
 template <bool COUNT>
-__global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(DevScene sc, Wave w, const int32_t* q, const int32_t* qcount,
-                                                Frame f) {
+__global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const DevJob* __restrict__ jobs,
+                                                              int32_t n_jobs, const int32_t* q,
+                                                              const int32_t* qcount, Frame f) {
     int nq = *qcount;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
         int slot = q[i];
+        const DevScene& sc = jobs[n_jobs > 1 ? w.job[slot] : 0].sc;
         RayCtx R = make_ray(mk(w.ox[slot], w.oy[slot], w.oz[slot]), mk(w.dx[slot], w.dy[slot], w.dz[slot]));
         double t;
         int rec = traverse_closest<COUNT>(sc, R, EPS_RAY, t, f.status, cnt);
@@ -1039,13 +1084,20 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 }
 
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
-__global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(DevScene sc, DevCam cam, Wave w, Frame f, const int32_t* qin,
-                                               const int32_t* qin_count, int32_t* qout, int32_t* qout_count,
-                                               uint64_t photon0, int32_t bounce, int32_t max_bounce) {
-    long long t_abs = 0, t_esc = 0, t_res = 0;
+__global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
+                                                               int32_t n_jobs, Frame f, const int32_t* qin,
+                                                               const int32_t* qin_count, int32_t* qout,
+                                                               int32_t* qout_count, int32_t bounce) {
+    const bool multi = n_jobs > 1;
+    TallyAcc acc;
+    tally_init(acc);
     int nq = *qin_count;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
         int slot = qin[i];
+        const int j = multi ? w.job[slot] : 0;
+        const DevJob& J = jobs[j];
+        const DevScene& sc = J.sc;
+        const DevCam& cam = J.cam;
         Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
         D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
         double lam = w.lam[slot], beta = w.beta[slot];
@@ -1081,7 +1133,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(DevScene sc, DevC
         D3 no = ro, nd = rd;
         if (medium_event) {   // render.h:2105-2115
             const DevMed& sm = sc.med[scatter_med];
-            connect_volume(sc, cam, w, f, sm, mp, rd, lam, beta);
+            connect_volume(sc, cam, w, f, j, sm, mp, rd, lam, beta);
             if (uniform(rng) >= med_albedo(sc, sm, lam)) fate = 0;
             else { nd = sample_hg(rd, sm.g, rng); no = mp; }
         } else if (!valid) {
@@ -1147,8 +1199,8 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(DevScene sc, DevC
                 if (sum > 1.0) { rr /= sum; rt /= sum; sum = 1.0; }
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface(sc, cam, w, f, h.p, h.n, ngo, wi, lam, beta, rr);
-                connect_surface(sc, cam, w, f, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
+                connect_surface(sc, cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr);
+                connect_surface(sc, cam, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
                 double u = uniform(rng);
                 if (u < rr) {
                     D3 wo = cosine_hemisphere(h.n, rng);
@@ -1165,7 +1217,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(DevScene sc, DevC
                 double rho = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface(sc, cam, w, f, h.p, h.n, ngo, wi, lam, beta, rho);
+                connect_surface(sc, cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho);
                 if (uniform(rng) >= rho) { fate = 0; break; }
                 D3 wo = cosine_hemisphere(h.n, rng);
                 beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
@@ -1174,11 +1226,19 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(DevScene sc, DevC
             }
             }
         }
-        uint64_t photon = photon0 + (uint64_t)slot;
-        if (fate == 0) { t_abs += to_fixed(beta, f.tally_scale_inv, f.status); log_finish(w, slot, photon, 0, beta); continue; }
-        if (fate == 1) { t_esc += to_fixed(beta, f.tally_scale_inv, f.status); log_finish(w, slot, photon, 1, beta); continue; }
-        if (bounce + 1 >= max_bounce) {
-            t_res += to_fixed(beta, f.tally_scale_inv, f.status);
+        uint64_t photon = J.photon0 + (uint64_t)(slot - J.slot0);
+        if (fate == 0) {
+            tally_add(acc, jobs, multi, j, T_ABS, to_fixed(beta, J.tally_scale_inv, f.status));
+            log_finish(w, slot, photon, 0, beta);
+            continue;
+        }
+        if (fate == 1) {
+            tally_add(acc, jobs, multi, j, T_ESC, to_fixed(beta, J.tally_scale_inv, f.status));
+            log_finish(w, slot, photon, 1, beta);
+            continue;
+        }
+        if (bounce + 1 >= J.max_bounce) {
+            tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
             log_finish(w, slot, photon, 2, beta);
             continue;
         }
@@ -1191,19 +1251,20 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(DevScene sc, DevC
         int qi = agg_inc(qout_count);
         qout[qi] = slot;
     }
-    block_tally(&f.tally[T_ABS], t_abs);
-    block_tally(&f.tally[T_ESC], t_esc);
-    block_tally(&f.tally[T_RES], t_res);
+    tally_finish(acc, jobs, multi);
 }
 
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
 template <bool COUNT>
-__global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(DevScene sc, Wave w, Frame f) {
+__global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const DevJob* __restrict__ jobs,
+                                                              int32_t n_jobs, Frame f) {
     int n = w.counts[2];
     if (n > w.S) n = w.S;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const DevJob& J = jobs[n_jobs > 1 ? w.sjob[i] : 0];
+        const DevScene& sc = J.sc;
         D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
         double max_dist = w.smax[i];
         RayCtx R = make_ray(o, d);
@@ -1211,10 +1272,10 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(DevScene sc, Wave
         if (traverse_any<COUNT>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         double lam = w.slam[i], c = w.sval[i];
         double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
-        long long* px = reinterpret_cast<long long*>(f.film) + 4 * (size_t)w.spix[i];
-        atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, f.film_scale_inv, f.status));
-        atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, f.film_scale_inv, f.status));
-        atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, f.film_scale_inv, f.status));
+        long long* px = reinterpret_cast<long long*>(J.film) + 4 * (size_t)w.spix[i];
+        atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, f.status));
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, J.film_scale_inv, f.status));
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, J.film_scale_inv, f.status));
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
     }
     if (COUNT) {
@@ -1236,6 +1297,7 @@ size_t wave_bytes(int32_t W, bool log) {
     b += align_up(4 * w) + align_up(8 * w * kStkCap);
     b += align_up(8 * w) + align_up(4 * w);   // hit
     b += 2 * align_up(4 * w) + align_up(64);  // queues + counts
+    b += align_up(4 * w) + align_up(4 * s) + align_up(sizeof(DevJob) * kWaveJobs);   // job ids + table
     b += 9 * align_up(8 * s) + align_up(4 * s);
     if (log) b += align_up(8 * w) + align_up(4 * w) + align_up(4 * w * 8);
     return b;
@@ -1259,6 +1321,8 @@ cudaError_t wave_alloc(Wave& w, int32_t W, bool log) {
     w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn);
     w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
     w.counts = (int32_t*)take(64);
+    w.job = (int32_t*)take(4 * wn); w.sjob = (int32_t*)take(4 * sn);
+    w.jobs = (DevJob*)take(sizeof(DevJob) * kWaveJobs);
     w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
     w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
     w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
@@ -1274,25 +1338,26 @@ void wave_free(Wave& w) {
     w.block = nullptr;
 }
 
-cudaError_t launch_wave(const DevScene& sc, const DevCam& cam, Wave& w, const Frame& f, uint64_t photon0,
-                        int32_t n, int32_t max_bounce, int32_t sms, cudaStream_t st, LaunchSink* sink) {
+cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_slots, int32_t max_bounce,
+                        const Frame& f, int32_t sms, cudaStream_t st, LaunchSink* sink) {
     const int T = 128;
-    int blocks_emit = (n + T - 1) / T;
+    int blocks_emit = (n_slots + T - 1) / T;
+    if (blocks_emit < 1) blocks_emit = 1;
     int grid = sms * 16;   // persistent-style grid for the queue-driven kernels
-    int gq = (n + T - 1) / T;
+    int gq = (n_slots + T - 1) / T;
     if (gq < grid) grid = gq < 1 ? 1 : gq;
     const bool count = f.stats != nullptr;
     auto mark = [&](int k, bool end) { if (sink) sink->mark(k, end, st); };
     auto shadow = [&]() {
         mark(K_SHADOW, false);
-        if (count) k_shadow<true><<<grid, T, 0, st>>>(sc, w, f);
-        else k_shadow<false><<<grid, T, 0, st>>>(sc, w, f);
+        if (count) k_shadow<true><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+        else k_shadow<false><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
         mark(K_SHADOW, true);
         cudaMemsetAsync(&w.counts[2], 0, 4, st);
     };
     cudaMemsetAsync(w.counts, 0, 64, st);
     mark(K_EMIT, false);
-    k_emit<<<blocks_emit, T, 0, st>>>(sc, cam, w, f, photon0, n, max_bounce);
+    k_emit<<<blocks_emit, T, 0, st>>>(w, jobs, n_jobs, n_slots, f);
     mark(K_EMIT, true);
     shadow();
     int32_t* qa = w.qa;
@@ -1301,12 +1366,12 @@ cudaError_t launch_wave(const DevScene& sc, const DevCam& cam, Wave& w, const Fr
     int32_t* cb = &w.counts[1];
     for (int b = 0; b < max_bounce; ++b) {
         mark(K_EXTEND, false);
-        if (count) k_extend<true><<<grid, T, 0, st>>>(sc, w, qa, ca, f);
-        else k_extend<false><<<grid, T, 0, st>>>(sc, w, qa, ca, f);
+        if (count) k_extend<true><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+        else k_extend<false><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
         mark(K_EXTEND, true);
         cudaMemsetAsync(cb, 0, 4, st);
         mark(K_SHADE, false);
-        k_shade<<<grid, T, 0, st>>>(sc, cam, w, f, qa, ca, qb, cb, photon0, b, max_bounce);
+        k_shade<<<grid, T, 0, st>>>(w, jobs, n_jobs, f, qa, ca, qb, cb, b);
         mark(K_SHADE, true);
         shadow();
         int32_t* tq = qa; qa = qb; qb = tq;

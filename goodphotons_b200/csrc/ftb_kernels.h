@@ -17,6 +17,21 @@ enum : int32_t {
 };
 
 constexpr int kStkCap = 4;
+constexpr int kWaveJobs = 256;   // jobs (frames / requests) one wave can carry
+
+// One job's share of a wave: its scene, camera and film, and the slots [slot0, slot0+n)
+// of the wave that trace its photons photon0, photon0+1, ...
+struct DevJob {
+    DevScene sc;
+    DevCam cam;
+    int64_t* film;             // 4 words per pixel
+    unsigned long long* tally; // 5 fixed-point energy tallies
+    double film_scale_inv;     // 2^frac / power_ref
+    double tally_scale_inv;    // 2^32 / power_ref
+    uint64_t photon0;
+    int32_t slot0, n;
+    int32_t max_bounce, pad;
+};
 
 // Per-wave path state, queues and shadow-ray records (structure of arrays, W slots).
 struct Wave {
@@ -31,6 +46,9 @@ struct Wave {
     int32_t* qa;               // active slot lists (ping-pong)
     int32_t* qb;
     int32_t* counts;           // [0] qa count, [1] qb count, [2] shadow count
+    int32_t* job;              // job of each slot (multi-job waves)
+    int32_t* sjob;             // job of each shadow record
+    DevJob* jobs;              // device job table, kWaveJobs entries
     double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
     int32_t* spix;
     // parity instrumentation (null unless logging)
@@ -44,15 +62,11 @@ struct Wave {
 };
 
 struct Frame {
-    int64_t* film;             // 4 words per pixel
-    unsigned long long* tally; // 5 fixed-point energy tallies
     unsigned long long* stats; // traversal counters (counting variant only, else null), 8:
                                // [0] closest-hit rays [1] their node visits [2] their record
                                // tests [3] any-hit rays [4] node visits [5] record tests
                                // [6] closest-hit / [7] any-hit exact (fp64) record tests
     int32_t* status;
-    double film_scale_inv;     // 2^frac / power_ref
-    double tally_scale_inv;    // 2^32 / power_ref
 };
 
 size_t wave_bytes(int32_t W, bool log);
@@ -69,11 +83,12 @@ struct LaunchSink {
     virtual ~LaunchSink() {}
 };
 
-// Trace photons [photon0, photon0+n) (n <= W) through all bounces on `stream`.  With
-// f.stats set, the counting variants of the traversal kernels run (slower; for traffic
-// accounting only).
-cudaError_t launch_wave(const DevScene& sc, const DevCam& cam, Wave& w, const Frame& f,
-                        uint64_t photon0, int32_t n, int32_t max_bounce, int32_t sms,
-                        cudaStream_t stream, LaunchSink* sink = nullptr);
+// Trace one wave on `stream`: jobs[0..n_jobs) is the device job table (already filled,
+// slot ranges consecutive from 0, n_slots = the sum of their n <= W), and every slot runs
+// through at most max_bounce bounces (the largest max_bounce of the jobs).  With f.stats set,
+// the counting variants of the traversal kernels run (slower; for traffic accounting only).
+cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_slots,
+                        int32_t max_bounce, const Frame& f, int32_t sms, cudaStream_t stream,
+                        LaunchSink* sink = nullptr);
 
 }  // namespace ftb

@@ -10,7 +10,7 @@
 //
 // Its scratch -- the path state, queues and shadow records of one wave of photons, plus the
 // energy tallies and the status word -- lives in one file-scope __device__ array of
-// kNoAllocBytes (about 9.5 MB for kNoAllocPhotons = 32768 slots), which every GPU that loads
+// kNoAllocBytes (about 10 MB for kNoAllocPhotons = 32768 slots), which every GPU that loads
 // the library holds until the process exits.  Host code cannot use the array's name as a
 // device address (it is a host-side stand-in), so the first call on each device, with that
 // device current, resolves it with cudaGetSymbolAddress; make that first call before any
@@ -40,7 +40,8 @@ constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 // Layout of one wave in the scratch array (same fields as ftb::wave_alloc).
 constexpr size_t wave_layout_bytes(size_t w) {
     return 2 * al(8 * w) + 8 * al(8 * w) + al(4 * w) + al(8 * w * ftb::kStkCap) + al(8 * w) + al(4 * w) +
-           2 * al(4 * w) + al(64) + 9 * al(8 * 2 * w) + al(4 * 2 * w);
+           2 * al(4 * w) + al(64) + al(4 * w) + al(4 * 2 * w) + al(sizeof(ftb::DevJob) * ftb::kWaveJobs) +
+           9 * al(8 * 2 * w) + al(4 * 2 * w);
 }
 constexpr size_t kWaveBytes = wave_layout_bytes(kNoAllocPhotons);
 constexpr size_t kNoAllocBytes = kWaveBytes + al(8 * sizeof(unsigned long long)) + al(64);
@@ -69,6 +70,8 @@ void carve(ftb::Wave& w, char* p, int32_t W) {
     w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn);
     w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
     w.counts = (int32_t*)take(64);
+    w.job = (int32_t*)take(4 * wn); w.sjob = (int32_t*)take(4 * sn);
+    w.jobs = (ftb::DevJob*)take(sizeof(ftb::DevJob) * ftb::kWaveJobs);
     w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
     w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
     w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
@@ -126,20 +129,29 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     int32_t* status = (int32_t*)(base + kWaveBytes + al(8 * sizeof(unsigned long long)));
     const int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
     ftb::Frame f;
-    f.film = d_film;
-    f.tally = tally;
     f.stats = nullptr;
     f.status = status;
-    f.film_scale_inv = std::ldexp(1.0, frac) / power;
-    f.tally_scale_inv = std::ldexp(1.0, 32) / power;
-    DevCam dc;
-    for (int i = 0; i < 3; ++i) { dc.eye[i] = cam->eye[i]; dc.u[i] = cam->u[i]; dc.v[i] = cam->v[i]; dc.w[i] = cam->w[i]; }
-    dc.thx = cam->tan_half_x; dc.thy = cam->tan_half_y; dc.rx = cam->res_x; dc.ry = cam->res_y;
+    ftb::DevJob J;   // the one-job table, staged from this pageable stack copy
+    std::memset(&J, 0, sizeof J);
+    J.sc = dev;
+    for (int i = 0; i < 3; ++i) {
+        J.cam.eye[i] = cam->eye[i]; J.cam.u[i] = cam->u[i]; J.cam.v[i] = cam->v[i]; J.cam.w[i] = cam->w[i];
+    }
+    J.cam.thx = cam->tan_half_x; J.cam.thy = cam->tan_half_y; J.cam.rx = cam->res_x; J.cam.ry = cam->res_y;
+    J.film = d_film;
+    J.tally = tally;
+    J.film_scale_inv = std::ldexp(1.0, frac) / power;
+    J.tally_scale_inv = std::ldexp(1.0, 32) / power;
+    J.photon0 = p->seed_base;
+    J.slot0 = 0;
+    J.n = (int32_t)p->n_photons;
+    J.max_bounce = p->max_bounce;
     ftb_status out = FTB_OK;
     cudaError_t e = cudaMemsetAsync(tally, 0, 8 * sizeof(unsigned long long), st);   // tallies start at zero
     if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w.jobs, &J, sizeof J, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && p->n_photons > 0)
-        e = ftb::launch_wave(dev, dc, w, f, p->seed_base, (int32_t)p->n_photons, p->max_bounce, sms, st, nullptr);
+        e = ftb::launch_wave(w, w.jobs, 1, (int32_t)p->n_photons, p->max_bounce, f, sms, st, nullptr);
     if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (out == FTB_OK && info) {
         info->frac_bits = frac;

@@ -71,6 +71,8 @@ def load(path=None):
     _sig(L, "ftb_render_forward_noalloc", st, PS, C.POINTER(abi.Camera),
          C.POINTER(abi.RenderParams), C.c_void_p, C.POINTER(abi.FilmInfo),
          C.POINTER(abi.Energy), C.c_void_p)
+    _sig(L, "ftb_render_batch", st, C.POINTER(abi.Job), C.c_int32, C.POINTER(abi.FilmInfo),
+         C.POINTER(abi.Energy), C.c_void_p)
     _sig(L, "ftb_scene_set_profiling", st, PS, C.c_int32)
     _sig(L, "ftb_scene_profile", st, PS, C.POINTER(abi.KernelProfile), C.c_int32)
     w = _Lib(L)
@@ -114,6 +116,24 @@ class _Lib:
                                            out.ctypes.data_as(C.POINTER(C.c_double)), cap,
                                            C.byref(n), C.byref(integral)))
         return out[: n.value + 1].copy(), integral.value
+
+    def render_batch(self, jobs, stream=None, want_energy=True):
+        """jobs: list of dicts(scene=Scene, cam=Camera, d_film=int ptr, n=..., seed_base=...,
+        max_bounce=..., frac_bits=0).  Returns (infos, energies or None)."""
+        n = len(jobs)
+        arr = (abi.Job * n)()
+        for i, j in enumerate(jobs):
+            arr[i].scene = j["scene"].h.value if hasattr(j["scene"].h, "value") else j["scene"].h
+            arr[i].cam = j["cam"]
+            arr[i].d_film = j["d_film"]
+            arr[i].n_photons = j["n"]
+            arr[i].seed_base = j.get("seed_base", 0)
+            arr[i].max_bounce = j.get("max_bounce", 8)
+            arr[i].frac_bits = j.get("frac_bits", 0)
+        infos = (abi.FilmInfo * n)()
+        ens = (abi.Energy * n)() if want_energy else None
+        self.check(self.L.ftb_render_batch(arr, n, infos, ens, C.c_void_p(stream or 0)))
+        return infos, ens
 
     def supported(self, desc):
         r = self.L.ftb_forward_supported(desc.ref())

@@ -255,6 +255,27 @@ ftb_status ftb_render_forward_device(ftb_scene* scene, const ftb_camera* cam,
                                      const ftb_render_params* params, int64_t* d_film,
                                      ftb_film_info* info, ftb_energy* energy, void* stream);
 
+/* Batched render (no counterpart in the reference, whose closest analogue is the
+ * multi-camera shared pass renderForwardSharedCuda, render_cuda.h:94-101): many jobs -- each
+ * with its own scene, camera, device film, photon range and bounce cap -- traced together in
+ * shared waves, so small jobs and the short tails of long ones fill the GPU together.  All
+ * scenes must live on one device.  A job's film and energy are bit-identical to rendering
+ * that job alone with ftb_render_forward_device (same frac_bits): photons are keyed by
+ * index and the film is fixed point.  Asynchronous on `stream` unless energies != NULL
+ * (then it synchronizes, checks the device status word and ACCUMULATES into energies[j]). */
+typedef struct ftb_job {
+    ftb_scene* scene;
+    ftb_camera cam;
+    int64_t* d_film;       /* device film, res_x*res_y*4 int64, accumulated */
+    int64_t n_photons;
+    uint64_t seed_base;
+    int32_t max_bounce;
+    int32_t frac_bits;     /* <= 0: the default for n_photons */
+} ftb_job;
+
+ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n_jobs, ftb_film_info* infos,
+                            ftb_energy* energies, void* stream);
+
 /* Resident session (replaces sharedForwardGpuBegin/Batch/Hits0/Download/End,
  * render_cuda.h:121-143).  Films and energy stay on the device between batches. */
 ftb_status ftb_session_begin(ftb_scene* scene, const ftb_camera* cams, int32_t n_cams,

@@ -59,6 +59,15 @@ _PD = C.POINTER(C.c_double)
 _PI32 = C.POINTER(C.c_int32)
 
 
+class BlasDesc(C.Structure):
+    _fields_ = [("n_tris", C.c_int64), ("tri_v", _PD), ("tri_n", _PD), ("tri_mat", _PI32),
+                ("handle", C.c_void_p)]
+
+
+class Instance(C.Structure):
+    _fields_ = [("blas", C.c_int32), ("mat_override", C.c_int32), ("to_world", C.c_double * 12)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [("n_tris", C.c_int64), ("tri_v", _PD), ("tri_n", _PD), ("tri_mat", _PI32),
                 ("n_spheres", C.c_int64), ("sph", _PD), ("sph_mat", _PI32),
@@ -68,7 +77,9 @@ class SceneDesc(C.Structure):
                 ("n_table", C.c_int64), ("table_w", _PD), ("table_v", _PD),
                 ("n_emitters", C.c_int32), ("n_media", C.c_int32),
                 ("emitters", C.POINTER(Emitter)), ("emitter_cdf", _PD),
-                ("media", C.POINTER(Medium))]
+                ("media", C.POINTER(Medium)), ("n_blas", C.c_int32), ("pad0", C.c_int32),
+                ("blas", C.POINTER(BlasDesc)), ("n_instances", C.c_int64),
+                ("instances", C.POINTER(Instance))]
 
 
 class Camera(C.Structure):
@@ -118,7 +129,8 @@ STRUCTS = {
     "ftb_medium": Medium, "ftb_scene_desc": SceneDesc, "ftb_camera": Camera,
     "ftb_render_params": RenderParams, "ftb_energy": Energy, "ftb_film_info": FilmInfo,
     "ftb_footprint": Footprint, "ftb_photon_log": PhotonLog,
-    "ftb_kernel_profile": KernelProfile, "ftb_job": Job,
+    "ftb_kernel_profile": KernelProfile, "ftb_job": Job, "ftb_blas_desc": BlasDesc,
+    "ftb_instance": Instance,
 }
 
 # every entry point declared in include/ftb200.h
@@ -129,6 +141,7 @@ EXPORTS = [
     "ftb_render_forward_device", "ftb_session_begin", "ftb_session_batch",
     "ftb_session_hits0", "ftb_session_download", "ftb_session_end", "ftb_trace_log",
     "ftb_scene_set_profiling", "ftb_scene_profile", "ftb_render_forward_noalloc",
-    "ftb_render_batch",
+    "ftb_render_batch", "ftb_blas_create", "ftb_blas_destroy", "ftb_scene_set_instance_transforms",
+    "ftb_scene_clone_instances",
 ]
 NOALLOC_MAX_PHOTONS = 32768

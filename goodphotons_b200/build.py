@@ -57,7 +57,7 @@ def build(verbose=False, force=False):
         ("ftb_kernels.cu", [*ARCH, "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
                             "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3"]),
         ("ftb_noalloc.cu", [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]),
-        ("ftb_api.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC"]),
+        ("ftb_api.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off"]),
         ("bvh_build.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC"]),
     ]
     for src, flags in units:

@@ -254,6 +254,48 @@ bool build_wide_bvh(const std::vector<Box>& boxes_in, double margin, WideBvh& ou
     return true;
 }
 
+bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, std::string& err) {
+    const size_t nn = b.nodes.size();
+    if (b.order.empty()) return true;
+    std::vector<Box> nb(nn);
+    // children always follow their parent, so a reverse sweep sees every child first
+    for (size_t i = nn; i-- > 0;) {
+        WNode& w = b.nodes[i];
+        double clo[3][8], chi[3][8];
+        int n = 0;
+        Box all;
+        for (int k = 0; k < FTB_WIDTH; ++k) {
+            uint32_t m = w.meta[k];
+            if (!m) break;   // the builder fills slots 0..n-1
+            Box c;
+            if ((w.imask >> k) & 1) {
+                c = nb[w.child_base + (m & 31)];
+            } else {
+                for (uint32_t r = 0; r < (m >> 5); ++r) {
+                    Box p = boxes[(size_t)b.order[w.prim_base + (m & 31) + r]];
+                    for (int a = 0; a < 3; ++a) { p.lo[a] -= margin; p.hi[a] += margin; }
+                    c.grow(p);
+                }
+            }
+            for (int a = 0; a < 3; ++a) { clo[a][k] = c.lo[a]; chi[a][k] = c.hi[a]; }
+            all.grow(c);
+            ++n;
+        }
+        nb[i] = all;
+        float p[3]; int e[3];
+        uint8_t* qlo[3] = {w.qlo_x, w.qlo_y, w.qlo_z};
+        uint8_t* qhi[3] = {w.qhi_x, w.qhi_y, w.qhi_z};
+        for (int a = 0; a < 3; ++a)
+            if (!quantize_axis(all.lo[a], all.hi[a], clo[a], chi[a], n, p[a], e[a], qlo[a], qhi[a])) {
+                err = "BVH quantization failed (scene extent out of float range)";
+                return false;
+            }
+        w.px = p[0]; w.py = p[1]; w.pz = p[2];
+        w.ex = (uint8_t)(e[0] + 127); w.ey = (uint8_t)(e[1] + 127); w.ez = (uint8_t)(e[2] + 127);
+    }
+    return true;
+}
+
 bool validate_wide_bvh(const WideBvh& b, int n_prims, std::string& err) {
     const size_t nn = b.nodes.size(), nr = b.order.size();
     if (nn == 0) { err = "BVH has no root"; return false; }

@@ -34,6 +34,11 @@ struct WideBvh {
 bool build_wide_bvh(const std::vector<Box>& boxes, double margin, WideBvh& out,
                     std::string& err);
 
+// Refit: the same topology over new primitive boxes (grown by `margin`).  Every node's
+// child boxes are recomputed bottom-up and quantized afresh, so the result is exactly as
+// conservative as a build; only the tree's shape may be worse for the new boxes.
+bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, std::string& err);
+
 // Structural check run on every bake: child and record indices in range, every node
 // reachable once, every primitive referenced exactly once, children after parents.
 bool validate_wide_bvh(const WideBvh& b, int n_prims, std::string& err);

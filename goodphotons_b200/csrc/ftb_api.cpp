@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -186,12 +187,76 @@ struct JobStage {
 };
 }  // namespace
 
+// ---- device blocks and BLAS assets ----------------------------------------------------
+namespace {
+// Device allocations released together, on their device.  Shared (std::shared_ptr) by the
+// objects that read them: a scene and its clones share their tables, scenes share a BLAS.
+struct DevBlock {
+    int device = 0;
+    std::vector<void*> ptrs;
+    uint64_t bytes = 0;
+    DevBlock() = default;
+    DevBlock(const DevBlock&) = delete;
+    DevBlock& operator=(const DevBlock&) = delete;
+    ~DevBlock() {
+        if (ptrs.empty()) return;
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(device);
+        for (void* p : ptrs) cudaFree(p);
+        cudaSetDevice(cur);
+    }
+};
+
+template <class T>
+ftb_status upload(DevBlock& blk, const T* host, size_t n, const T** out, const char* what) {
+    if (n == 0) { *out = nullptr; return FTB_OK; }
+    void* p = nullptr;
+    CK(cudaMalloc(&p, n * sizeof(T)), what);
+    blk.ptrs.push_back(p);
+    blk.bytes += n * sizeof(T);
+    CK(cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice), what);
+    *out = (const T*)p;
+    return FTB_OK;
+}
+
+// A baked BLAS (Blas, scene.h:996-1033): wide BVH and triangle records in local space.
+struct BlasDev {
+    DevBlock mem;
+    const WNode* nodes = nullptr;
+    const PrimRec* recs = nullptr;
+    const double* tri_n = nullptr;
+    int64_t n_tris = 0;
+    int32_t max_mat = -1;
+    double lo[3], hi[3];   // localBounds: union of the triangle boxes padded by 1e-6
+};
+
+// Host state kept for refitting the top-level hierarchy of a scene with instances.
+struct TlasHost {
+    ftb::WideBvh bvh;
+    std::vector<ftb::Box> boxes;     // unmargined primitive boxes, global order
+    double base_maxabs = 1.0;        // coordinate magnitude of everything but the instances
+    int64_t first_inst = 0;          // global index of instance 0
+    std::vector<int32_t> inst_blas;  // BLAS of each instance
+    std::vector<DevInst> inst;       // host copy of the device instance table
+};
+}  // namespace
+
+struct ftb_blas {
+    std::shared_ptr<BlasDev> p;
+};
+
 // ---- scene object ----------------------------------------------------------------------
 struct ftb_scene {
     int device = 0;
     int sms = 148;
     DevScene dev{};
-    std::vector<void*> allocs;
+    std::shared_ptr<DevBlock> tables;              // geometry, materials, emitters (shared with clones)
+    std::vector<std::shared_ptr<BlasDev>> blas;    // BLAS assets the instances place
+    std::unique_ptr<DevBlock> own;                 // this scene's TLAS nodes and instance table
+    TlasHost tlas;                                 // for refits (scenes with instances)
+    WNode* d_nodes = nullptr;                      // mutable TLAS nodes (in `own`)
+    DevInst* d_inst = nullptr;
     double power = 0.0;
     uint64_t scene_bytes = 0;
     std::mutex mu;   // one render at a time per scene
@@ -222,7 +287,6 @@ struct ftb_scene {
         if (stats) cudaFree(stats);
         if (batch_tally) cudaFree(batch_tally);
         delete prof;
-        for (void* p : allocs) cudaFree(p);
         cudaSetDevice(cur);
     }
 };
@@ -246,14 +310,7 @@ struct DeviceGuard {
 
 template <class T>
 ftb_status upload(ftb_scene* s, const T* host, size_t n, const T** out, const char* what) {
-    if (n == 0) { *out = nullptr; return FTB_OK; }
-    void* p = nullptr;
-    CK(cudaMalloc(&p, n * sizeof(T)), what);
-    s->allocs.push_back(p);
-    s->scene_bytes += n * sizeof(T);
-    CK(cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice), what);
-    *out = (const T*)p;
-    return FTB_OK;
+    return upload(*s->tables, host, n, out, what);
 }
 
 bool mat_type_supported(int t) {
@@ -272,8 +329,32 @@ ftb_status check_desc(const ftb_scene_desc* d) {
         (d->n_curves && (!d->curve || !d->curve_mat)) || (d->n_mats && !d->mats) ||
         (d->n_emitters && (!d->emitters || !d->emitter_cdf)) || (d->n_media && !d->media))
         return fail(FTB_ERR_INVALID, "null array for a nonzero count");
-    int64_t np = d->n_tris + d->n_spheres + d->n_curves;
+    if (d->n_blas < 0 || d->n_instances < 0) return fail(FTB_ERR_INVALID, "negative count in scene descriptor");
+    if ((d->n_blas && !d->blas) || (d->n_instances && !d->instances))
+        return fail(FTB_ERR_INVALID, "null array for a nonzero count");
+    int64_t np = d->n_tris + d->n_spheres + d->n_curves + d->n_instances;
     if (np > ((int64_t)1 << 29)) return fail(FTB_ERR_TOO_LARGE, "too many primitives (max 2^29)");
+    for (int b = 0; b < d->n_blas; ++b) {
+        const ftb_blas_desc& bd = d->blas[b];
+        if (bd.handle) {
+            if (!bd.handle->p || bd.handle->p->max_mat >= d->n_mats)
+                return fail(FTB_ERR_INVALID, "BLAS " + std::to_string(b) + ": material out of range for this scene");
+            continue;
+        }
+        if (bd.n_tris < 1 || bd.n_tris > ((int64_t)1 << 29) || !bd.tri_v || !bd.tri_mat)
+            return fail(FTB_ERR_INVALID, "BLAS " + std::to_string(b) + ": needs 1..2^29 triangles");
+        for (int64_t i = 0; i < bd.n_tris; ++i)
+            if (bd.tri_mat[i] < 0 || bd.tri_mat[i] >= d->n_mats)
+                return fail(FTB_ERR_INVALID, "BLAS " + std::to_string(b) + ": triangle material out of range");
+    }
+    for (int64_t k = 0; k < d->n_instances; ++k) {
+        const ftb_instance& in = d->instances[k];
+        if (in.blas < 0 || in.blas >= d->n_blas) return fail(FTB_ERR_INVALID, "instance BLAS index out of range");
+        if (in.mat_override < -1 || in.mat_override >= d->n_mats)
+            return fail(FTB_ERR_INVALID, "instance material override out of range");
+        for (int j = 0; j < 12; ++j)
+            if (!std::isfinite(in.to_world[j])) return fail(FTB_ERR_INVALID, "instance transform not finite");
+    }
     std::string why;
     for (int i = 0; i < d->n_spectra; ++i)
         if (!spec_valid(d, i, why)) return fail(FTB_ERR_INVALID, "spectrum " + std::to_string(i) + ": " + why);
@@ -313,6 +394,92 @@ ftb_status check_desc(const ftb_scene_desc* d) {
         if (m.bound < FTB_BOUND_NONE || m.bound > FTB_BOUND_SPHERE) return fail(FTB_ERR_INVALID, "bad medium bound");
     }
     for (int i = 0; i < d->n_spectra; ++i) (void)i;
+    return FTB_OK;
+}
+
+// Affine::inverse (linalg.h:129-144): 3x3 row-major then t; identity when singular.
+void affine_inverse(const double* x, double* r) {
+    for (int j = 0; j < 12; ++j) r[j] = 0.0;
+    r[0] = r[4] = r[8] = 1.0;
+    double a = x[0], b = x[1], c = x[2];
+    double d = x[3], e = x[4], f = x[5];
+    double g = x[6], h = x[7], i = x[8];
+    double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+    if (std::fabs(det) < 1e-30) return;
+    double id = 1.0 / det;
+    r[0] = (e * i - f * h) * id; r[1] = (c * h - b * i) * id; r[2] = (b * f - c * e) * id;
+    r[3] = (f * g - d * i) * id; r[4] = (a * i - c * g) * id; r[5] = (c * d - a * f) * id;
+    r[6] = (d * h - e * g) * id; r[7] = (b * g - a * h) * id; r[8] = (a * e - b * d) * id;
+    const double* t = x + 9;
+    r[9] = -(r[0] * t[0] + r[1] * t[1] + r[2] * t[2]);
+    r[10] = -(r[3] * t[0] + r[4] * t[1] + r[5] * t[2]);
+    r[11] = -(r[6] * t[0] + r[7] * t[1] + r[8] * t[2]);
+}
+
+// World box of an instance: the 8 corners of its BLAS's local bounds mapped by to_world
+// (Scene::collectPrimBoxes, scene.h:2030-2041).
+ftb::Box instance_box(const BlasDev& b, const double* xf) {
+    ftb::Box w;
+    for (int c = 0; c < 8; ++c) {
+        double q[3] = {(c & 1) ? b.hi[0] : b.lo[0], (c & 2) ? b.hi[1] : b.lo[1], (c & 4) ? b.hi[2] : b.lo[2]};
+        double p[3];
+        for (int r = 0; r < 3; ++r) p[r] = xf[3 * r] * q[0] + xf[3 * r + 1] * q[1] + xf[3 * r + 2] * q[2] + xf[9 + r];
+        w.grow_point(p);
+    }
+    return w;
+}
+
+double box_maxabs(const ftb::Box& b, double m) {
+    for (int a = 0; a < 3; ++a) m = std::max(m, std::max(std::fabs(b.lo[a]), std::fabs(b.hi[a])));
+    return m;
+}
+
+// Bake one BLAS on `device` (current): triangle boxes, wide BVH with a margin from the
+// local coordinate magnitude, records in leaf order (prim = the triangle's BLAS index).
+ftb_status bake_blas(const ftb_blas_desc& d, int device, std::shared_ptr<BlasDev>& out) {
+    auto b = std::make_shared<BlasDev>();
+    b->mem.device = device;
+    b->n_tris = d.n_tris;
+    const int64_t nt = d.n_tris;
+    std::vector<ftb::Box> boxes((size_t)nt);
+    double maxabs = 1.0;
+    const double pad = 1e-6;
+    for (int a = 0; a < 3; ++a) { b->lo[a] = DBL_MAX; b->hi[a] = -DBL_MAX; }
+    for (int64_t i = 0; i < nt; ++i) {
+        const double* v = d.tri_v + 9 * i;
+        ftb::Box x;
+        for (int k = 0; k < 3; ++k) x.grow_point(v + 3 * k);
+        boxes[(size_t)i] = x;
+        maxabs = box_maxabs(x, maxabs);
+        for (int a = 0; a < 3; ++a) {
+            b->lo[a] = std::min(b->lo[a], x.lo[a] - pad);
+            b->hi[a] = std::max(b->hi[a], x.hi[a] + pad);
+        }
+        b->max_mat = std::max(b->max_mat, d.tri_mat[i]);
+    }
+    ftb::WideBvh bvh;
+    std::string err;
+    if (!ftb::build_wide_bvh(boxes, std::ldexp(maxabs, -18), bvh, err)) return fail(FTB_ERR_INVALID, err);
+    if (!ftb::validate_wide_bvh(bvh, (int)nt, err)) return fail(FTB_ERR_INVALID, "BLAS BVH check: " + err);
+    std::vector<PrimRec> recs(bvh.order.size());
+    bool any_smooth = false;
+    for (size_t r = 0; r < bvh.order.size(); ++r) {
+        int p = bvh.order[r];
+        PrimRec& R = recs[r];
+        std::memset(&R, 0, sizeof R);
+        std::memcpy(R.d, d.tri_v + 9 * (size_t)p, 9 * sizeof(double));
+        R.prim = p;
+        int smooth = 0;
+        if (d.tri_n)
+            for (int k = 0; k < 9; ++k) if (d.tri_n[9 * (size_t)p + k] != 0.0) smooth = 1;
+        any_smooth |= smooth != 0;
+        R.info = d.tri_mat[p] | (REC_TRI << 24) | (smooth << 30);
+    }
+    ftb_status st = upload(b->mem, bvh.nodes.data(), bvh.nodes.size(), &b->nodes, "upload BLAS nodes");
+    if (st == FTB_OK) st = upload(b->mem, recs.data(), recs.size(), &b->recs, "upload BLAS records");
+    if (st == FTB_OK && any_smooth) st = upload(b->mem, d.tri_n, (size_t)nt * 9, &b->tri_n, "upload BLAS normals");
+    if (st != FTB_OK) return st;
+    out = std::move(b);
     return FTB_OK;
 }
 
@@ -407,6 +574,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
     while (j < base.size()) {
         table.clear();
         int32_t slots = 0, max_bounce = 0;
+        bool inst = false;
         while (j < base.size() && slots < W && (int)table.size() < ftb::kWaveJobs) {
             int64_t left = count[j] - done_in_job;
             if (left <= 0) { ++j; done_in_job = 0; continue; }
@@ -417,6 +585,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
             J.n = m;
             table.push_back(J);
             max_bounce = std::max(max_bounce, J.max_bounce);
+            inst |= J.sc.n_inst > 0;
             slots += m;
             done_in_job += m;
             if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
@@ -428,7 +597,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         w.log_base = log_base;
         cudaError_t e = s->stage[k & 1].push(table.data(), (int)table.size(), w.jobs, ws);
         if (e != cudaSuccess) return cuda_fail(e, "job table upload");
-        e = ftb::launch_wave(w, w.jobs, (int32_t)table.size(), slots, max_bounce, f, s->sms, ws,
+        e = ftb::launch_wave(w, w.jobs, (int32_t)table.size(), slots, max_bounce, inst, f, s->sms, ws,
                              s->prof_mode ? s->prof : nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         ++k;
@@ -604,11 +773,26 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     DeviceGuard guard(device);
     auto s = new ftb_scene();
     s->device = device;
+    s->tables = std::make_shared<DevBlock>();
+    s->tables->device = device;
     {
         cudaDeviceProp p;
         if (cudaGetDeviceProperties(&p, device) == cudaSuccess) s->sms = p.multiProcessorCount;
     }
-    const int64_t nt = d->n_tris, ns = d->n_spheres, nc = d->n_curves, np = nt + ns + nc;
+    // BLAS assets: shared handles or baked here
+    for (int b = 0; b < d->n_blas; ++b) {
+        std::shared_ptr<BlasDev> bp;
+        if (d->blas[b].handle) {
+            bp = d->blas[b].handle->p;
+            if (bp->mem.device != device) { delete s; return fail(FTB_ERR_INVALID, "BLAS handle lives on another device"); }
+        } else {
+            ftb_status bs = bake_blas(d->blas[b], device, bp);
+            if (bs != FTB_OK) { delete s; return bs; }
+        }
+        s->blas.push_back(std::move(bp));
+    }
+    const int64_t nt = d->n_tris, ns = d->n_spheres, nc = d->n_curves, ni = d->n_instances;
+    const int64_t np = nt + ns + nc + ni;
     // primitive boxes and the scene's coordinate magnitude (for the traversal margin)
     std::vector<ftb::Box> boxes((size_t)np);
     double maxabs = 1.0;
@@ -639,6 +823,24 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
         const ftb_emitter& e = d->emitters[i];
         for (int a = 0; a < 3; ++a) { see(e.origin[a] + std::fabs(e.u[a]) + std::fabs(e.v[a]) + e.radius); }
     }
+    // instances: world boxes, world -> local maps (MeshInstance::setToWorld, scene.h:1052-1062)
+    TlasHost& T = s->tlas;
+    T.base_maxabs = maxabs;
+    T.first_inst = nt + ns + nc;
+    for (int64_t k = 0; k < ni; ++k) {
+        const ftb_instance& in = d->instances[k];
+        const BlasDev& B = *s->blas[(size_t)in.blas];
+        ftb::Box b = instance_box(B, in.to_world);
+        boxes[(size_t)(nt + ns + nc + k)] = b;
+        maxabs = box_maxabs(b, maxabs);
+        DevInst I;
+        std::memset(&I, 0, sizeof I);
+        affine_inverse(in.to_world, I.xl);
+        I.nodes = B.nodes; I.recs = B.recs; I.tri_n = B.tri_n;
+        I.mat_override = in.mat_override;
+        T.inst.push_back(I);
+        T.inst_blas.push_back(in.blas);
+    }
     double margin = std::ldexp(maxabs, -18);
     ftb::WideBvh bvh;
     std::string err;
@@ -667,9 +869,13 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
         } else if (p < nt + ns) {
             std::memcpy(R.d, d->sph + 4 * (size_t)(p - nt), 4 * sizeof(double));
             ty = REC_SPHERE; mat = d->sph_mat[p - nt];
-        } else {
+        } else if (p < nt + ns + nc) {
             std::memcpy(R.d, d->curve + 10 * (size_t)(p - nt - ns), 8 * sizeof(double));
             ty = REC_CURVE; mat = d->curve_mat[p - nt - ns];
+        } else {
+            int64_t k = p - nt - ns - nc;
+            std::memcpy(&R.d[0], &k, sizeof k);
+            ty = REC_INST; mat = 0;
         }
         any_smooth |= smooth != 0;
         R.info = mat | (ty << 24) | (smooth << 30);
@@ -687,8 +893,23 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     DevScene& D = s->dev;
     const WNode* dn; const PrimRec* dr;
 #define UP(host, n, out, what) do { ftb_status u_ = upload(s, host, n, out, what); if (u_ != FTB_OK) { delete s; return u_; } } while (0)
-    UP(bvh.nodes.data(), bvh.nodes.size(), &dn, "upload nodes");
     UP(recs.data(), recs.size(), &dr, "upload records");
+    if (ni > 0) {   // the nodes and the instance table are this scene's own: refits rewrite them
+        s->own.reset(new DevBlock());
+        s->own->device = device;
+        const DevInst* di = nullptr;
+        ftb_status us = upload(*s->own, bvh.nodes.data(), bvh.nodes.size(), &dn, "upload nodes");
+        if (us == FTB_OK) us = upload(*s->own, T.inst.data(), T.inst.size(), &di, "upload instances");
+        if (us != FTB_OK) { delete s; return us; }
+        s->d_nodes = const_cast<WNode*>(dn);
+        s->d_inst = const_cast<DevInst*>(di);
+        D.inst = di;
+        D.n_inst = ni;
+        T.bvh = bvh;
+        T.boxes = std::move(boxes);
+    } else {
+        UP(bvh.nodes.data(), bvh.nodes.size(), &dn, "upload nodes");
+    }
     D.nodes = dn; D.recs = dr;
     if (any_smooth) UP(d->tri_n, (size_t)nt * 9, &D.tri_n, "upload normals");
     UP(spec.data(), spec.size(), &D.spec, "upload spectra");
@@ -734,12 +955,108 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     D.n_tris = nt;
     D.total_power = tp;
     s->power = tp;
+    s->scene_bytes = s->tables->bytes + (s->own ? s->own->bytes : 0);
+    for (auto& b : s->blas) s->scene_bytes += b->mem.bytes;
     *out = s;
     return FTB_OK;
 }
 
 ftb_status ftb_scene_destroy(ftb_scene* s) {
     delete s;
+    return FTB_OK;
+}
+
+ftb_status ftb_blas_create(const ftb_blas_desc* d, int32_t device, ftb_blas** out) {
+    if (!out || !d) return fail(FTB_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (d->handle) return fail(FTB_ERR_INVALID, "descriptor already names a baked BLAS");
+    if (d->n_tris < 1 || d->n_tris > ((int64_t)1 << 29) || !d->tri_v || !d->tri_mat)
+        return fail(FTB_ERR_INVALID, "a BLAS needs 1..2^29 triangles");
+    for (int64_t i = 0; i < d->n_tris; ++i)
+        if (d->tri_mat[i] < 0) return fail(FTB_ERR_INVALID, "negative triangle material");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return fail(FTB_ERR_NO_DEVICE, "no CUDA device"); }
+    if (device < 0 || device >= ndev) return fail(FTB_ERR_INVALID, "device index out of range");
+    DeviceGuard guard(device);
+    std::shared_ptr<BlasDev> b;
+    ftb_status st = bake_blas(*d, device, b);
+    if (st != FTB_OK) return st;
+    *out = new ftb_blas{std::move(b)};
+    return FTB_OK;
+}
+
+ftb_status ftb_blas_destroy(ftb_blas* b) {
+    delete b;   // scenes built on it keep their own reference
+    return FTB_OK;
+}
+
+namespace {
+// New world maps for instances [0, n): instance table, boxes, refit of the top level.
+ftb_status set_transforms(ftb_scene* s, const double* to_world, int64_t n) {
+    TlasHost& T = s->tlas;
+    for (int64_t k = 0; k < n; ++k) {
+        const double* xf = to_world + 12 * k;
+        for (int j = 0; j < 12; ++j)
+            if (!std::isfinite(xf[j])) return fail(FTB_ERR_INVALID, "instance transform not finite");
+    }
+    for (int64_t k = 0; k < n; ++k) {
+        const double* xf = to_world + 12 * k;
+        affine_inverse(xf, T.inst[(size_t)k].xl);
+        T.boxes[(size_t)(T.first_inst + k)] = instance_box(*s->blas[(size_t)T.inst_blas[(size_t)k]], xf);
+    }
+    double maxabs = T.base_maxabs;
+    for (size_t k = 0; k < T.inst.size(); ++k) maxabs = box_maxabs(T.boxes[(size_t)T.first_inst + k], maxabs);
+    std::string err;
+    if (!ftb::refit_wide_bvh(T.bvh, T.boxes, std::ldexp(maxabs, -18), err)) return fail(FTB_ERR_INVALID, err);
+    DeviceGuard guard(s->device);
+    CK(cudaMemcpy(s->d_nodes, T.bvh.nodes.data(), T.bvh.nodes.size() * sizeof(WNode), cudaMemcpyHostToDevice),
+       "upload refit nodes");
+    CK(cudaMemcpy(s->d_inst, T.inst.data(), T.inst.size() * sizeof(DevInst), cudaMemcpyHostToDevice),
+       "upload instances");
+    return FTB_OK;
+}
+}  // namespace
+
+ftb_status ftb_scene_set_instance_transforms(ftb_scene* s, const double* to_world, int64_t n) {
+    if (!s) return fail(FTB_ERR_INVALID, "null scene");
+    if (n < 0 || n > s->dev.n_inst || (n > 0 && !to_world)) return fail(FTB_ERR_INVALID, "bad instance range");
+    if (n == 0) return FTB_OK;
+    std::lock_guard<std::mutex> lk(s->mu);
+    return set_transforms(s, to_world, n);
+}
+
+ftb_status ftb_scene_clone_instances(const ftb_scene* src, const double* to_world, int64_t n, ftb_scene** out) {
+    if (!src || !out) return fail(FTB_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (n < 0 || n > src->dev.n_inst || (n > 0 && !to_world)) return fail(FTB_ERR_INVALID, "bad instance range");
+    DeviceGuard guard(src->device);
+    auto c = new ftb_scene();
+    c->device = src->device;
+    c->sms = src->sms;
+    c->dev = src->dev;
+    c->tables = src->tables;
+    c->blas = src->blas;
+    c->tlas = src->tlas;
+    c->power = src->power;
+    if (src->dev.n_inst > 0) {
+        c->own.reset(new DevBlock());
+        c->own->device = c->device;
+        const WNode* dn = nullptr;
+        const DevInst* di = nullptr;
+        ftb_status st = upload(*c->own, c->tlas.bvh.nodes.data(), c->tlas.bvh.nodes.size(), &dn, "upload nodes");
+        if (st == FTB_OK) st = upload(*c->own, c->tlas.inst.data(), c->tlas.inst.size(), &di, "upload instances");
+        if (st != FTB_OK) { delete c; return st; }
+        c->d_nodes = const_cast<WNode*>(dn);
+        c->d_inst = const_cast<DevInst*>(di);
+        c->dev.nodes = dn;
+        c->dev.inst = di;
+        if (n > 0) {
+            st = set_transforms(c, to_world, n);
+            if (st != FTB_OK) { delete c; return st; }
+        }
+    }
+    c->scene_bytes = src->scene_bytes;
+    *out = c;
     return FTB_OK;
 }
 

@@ -362,7 +362,7 @@ struct Hit {
     D3 p, n, ng;
     int mat, prim;
 };
-__device__ void hit_attributes(const DevScene& sc, const RayCtx& R, const PrimRec& r, Hit& h) {
+__device__ void hit_attributes(const double* __restrict__ tri_n, const RayCtx& R, const PrimRec& r, Hit& h) {
     int ty = rec_type(r);
     h.mat = rec_mat(r);
     h.prim = r.prim;
@@ -375,7 +375,7 @@ __device__ void hit_attributes(const DevScene& sc, const RayCtx& R, const PrimRe
         D3 tgn = normalize(cross(v1 - v0, v2 - v0));     // Tri::finalize (geometry.h:52)
         D3 n0 = tgn, n1 = tgn, n2 = tgn;
         if (rec_smooth(r)) {
-            const double* nn = sc.tri_n + 9 * (size_t)r.prim;
+            const double* nn = tri_n + 9 * (size_t)r.prim;
             D3 a = ld3(nn), b = ld3(nn + 3), c = ld3(nn + 6);
             if (!(dot(a, a) < 1e-12)) n0 = a;
             if (!(dot(b, b) < 1e-12)) n1 = b;
@@ -499,31 +499,17 @@ __device__ __forceinline__ uint32_t child_entry(uint32_t child_base, uint32_t pr
     return LEAF_BIT | ((prim_base + (m & 31u)) << 2) | ((m >> 5) - 1u);
 }
 
-// One record: the exact fp64 acceptance test.
-template <bool COUNT>
-__device__ __forceinline__ bool record_hit(const DevScene& sc, const RayCtx& R, int ri, double tmin, double tbest,
-                                           double& t, TravCount& cnt) {
-    if (COUNT) { cnt.recs++; cnt.exact++; }
-    PrimRec r;
-    load_rec(sc.recs, ri, r);
-    return rec_test(R, r, tmin, tbest, t);
-}
-
 #define CSWAP(a, b) { uint32_t lo_ = min(a, b); b = max(a, b); a = lo_; }
 
-// Closest hit: returns the record index (or -1) and t.  Children of a node are visited near
-// to far (leaves and inner nodes alike, keys sorted by an 8-input network in registers);
-// entries farther than the current hit are culled when popped.  The loop is "while-while":
-// a lane steps through inner nodes until it holds a leaf, so the lanes of a warp run the
-// expensive leaf tests together rather than interleaved with node steps.
-template <bool COUNT>
-__device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin, double& best_t,
-                                int32_t* status, TravCount& cnt) {
-    RayF F = make_rayf(R.o, R.d);
-    const float tmin_f = __double2float_rd(tmin);
-    best_t = DBL_MAX;
-    float tmax_f = FLT_MAX;
-    int best = -1;
+// Closest-hit walk of one wide BVH.  Children of a node are visited near to far (leaves and
+// inner nodes alike, keys sorted by an 8-input network in registers); entries farther than
+// the current hit are culled when popped.  The loop is "while-while": a lane steps through
+// inner nodes until it holds a leaf, so the lanes of a warp run the expensive leaf tests
+// together rather than interleaved with node steps.  leaf(first, count, tmax_f) tests a
+// leaf's records and returns the (possibly lowered) fp32 bound on t.
+template <bool COUNT, class Leaf>
+__device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, const RayF& F, float tmin_f,
+                                              float tmax_f, Leaf& leaf, int32_t* status, TravCount& cnt) {
     uint32_t st_e[FTB_STACK];
     float st_t[FTB_STACK];
     int sp = 0;
@@ -532,7 +518,7 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
     while (live) {
         while (!(cur & LEAF_BIT)) {
             uint4 n[5];
-            load_node(sc.nodes, cur, n);
+            load_node(nodes, cur, n);
             if (COUNT) cnt.nodes++;
             NodeRay N = node_setup(n, F);
             uint32_t k[8];
@@ -551,7 +537,7 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
 #pragma unroll
             for (int i = 7; i >= 1; --i) {
                 if (k[i] != 0xffffffffu) {
-                    if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return best; }
+                    if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return tmax_f; }
                     st_e[sp] = child_entry(child_base, prim_base, imask, N.meta, (int)(k[i] & 7u));
                     st_t[sp] = __uint_as_float(k[i] & ~7u);
                     ++sp;
@@ -569,15 +555,7 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
             if (!found) { live = false; break; }
         }
         if (!live) break;
-        {   // leaf phase
-            int first = (int)((cur & ~LEAF_BIT) >> 2), count = (int)(cur & 3u) + 1;
-            for (int k = 0; k < count; ++k) {
-                double t;
-                if (record_hit<COUNT>(sc, R, first + k, tmin, best_t, t, cnt)) {
-                    best_t = t; best = first + k; tmax_f = __double2float_ru(t);
-                }
-            }
-        }
+        tmax_f = leaf((int)((cur & ~LEAF_BIT) >> 2), (int)(cur & 3u) + 1, tmax_f);
         bool found = false;
         while (sp > 0) {
             --sp;
@@ -585,18 +563,14 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
         }
         if (!found) break;
     }
-    return best;
+    return tmax_f;
 }
 
-// Any hit with t in [tmin, seg) (Scene::occluded, scene.h:2249-2271).  Order does not
-// change the answer, so children are taken in slot order, leaves first; the loop is
-// while-while like traverse_closest.
-template <bool COUNT>
-__device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, double seg, int32_t* status,
-                             TravCount& cnt) {
-    RayF F = make_rayf(R.o, R.d);
-    const float tmin_f = __double2float_rd(tmin);
-    const float tmax_f = __double2float_ru(seg);
+// Any-hit walk: order does not change the answer, so children are taken in slot order,
+// leaves first; leaf(first, count) returns true on a hit, which ends the walk.
+template <bool COUNT, class Leaf>
+__device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const RayF& F, float tmin_f, float tmax_f,
+                                         Leaf& leaf, int32_t* status, TravCount& cnt) {
     uint32_t st_e[FTB_STACK];
     int sp = 0;
     uint32_t cur = 0;
@@ -604,7 +578,7 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
     while (live) {
         while (!(cur & LEAF_BIT)) {
             uint4 n[5];
-            load_node(sc.nodes, cur, n);
+            load_node(nodes, cur, n);
             if (COUNT) cnt.nodes++;
             NodeRay N = node_setup(n, F);
             uint32_t hit = 0;
@@ -628,15 +602,161 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
             cur = st_e[--sp];
         }
         if (!live) break;
-        int first = (int)((cur & ~LEAF_BIT) >> 2), count = (int)(cur & 3u) + 1;
-        for (int k = 0; k < count; ++k) {
-            double t;
-            if (record_hit<COUNT>(sc, R, first + k, tmin, seg, t, cnt)) return true;
-        }
+        if (leaf((int)((cur & ~LEAF_BIT) >> 2), (int)(cur & 3u) + 1)) return true;
         if (sp == 0) break;
         cur = st_e[--sp];
     }
     return false;
+}
+
+// Affine::apply / applyDir (linalg.h:105-114) of a 12-double map (3x3 row-major, then t)
+__device__ __forceinline__ D3 xf_point(const double* m, D3 p) {
+    return mk(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[9],
+              m[3] * p.x + m[4] * p.y + m[5] * p.z + m[10],
+              m[6] * p.x + m[7] * p.y + m[8] * p.z + m[11]);
+}
+__device__ __forceinline__ D3 xf_dir(const double* m, D3 v) {
+    return mk(m[0] * v.x + m[1] * v.y + m[2] * v.z,
+              m[3] * v.x + m[4] * v.y + m[5] * v.z,
+              m[6] * v.x + m[7] * v.y + m[8] * v.z);
+}
+// Affine::applyNormal of toWorld (linalg.h:161-167): toWorld.inverse() is toLocal, read
+// transposed.
+__device__ __forceinline__ D3 xf_normal(const double* il, D3 n) {
+    return mk(il[0] * n.x + il[3] * n.y + il[6] * n.z,
+              il[1] * n.x + il[4] * n.y + il[7] * n.z,
+              il[2] * n.x + il[5] * n.y + il[8] * n.z);
+}
+__device__ __forceinline__ int rec_inst(const PrimRec& r) { return (int)__double_as_longlong(r.d[0]); }
+
+// The world ray mapped into an instance's local space (Scene::closestHit instance leaf,
+// scene.h:2226-2228): local t equals world t, the direction is not renormalized.
+struct LocalRay { D3 o, d; };
+__device__ __forceinline__ LocalRay to_local(const DevInst& I, D3 o, D3 d) {
+    LocalRay L;
+    L.o = xf_point(I.xl, o);
+    L.d = xf_dir(I.xl, d);
+    return L;
+}
+
+// Blas::intersectLocal (scene.h:1017-1026): nearest BLAS triangle with t < best_t; updates
+// best_t / tmax_f and returns the BLAS record, or -1.
+template <bool COUNT>
+__device__ __noinline__ int blas_closest(const DevInst& I, D3 wo, D3 wd, double tmin, double& best_t,
+                                         float& tmax_f, int32_t* status, TravCount& cnt) {
+    const LocalRay L = to_local(I, wo, wd);
+    const Shear sh = make_shear(L.d);
+    const RayF F = make_rayf(L.o, L.d);
+    const PrimRec* __restrict__ recs = I.recs;
+    int best = -1;
+    auto leaf = [&](int first, int count, float tm) -> float {
+        for (int k = 0; k < count; ++k) {
+            if (COUNT) { cnt.recs++; cnt.exact++; }
+            PrimRec r;
+            load_rec(recs, first + k, r);
+            double t;
+            if (tri_test(sh, L.o, r.d, tmin, best_t, t, nullptr)) {
+                best_t = t; best = first + k; tm = __double2float_ru(t);
+            }
+        }
+        return tm;
+    };
+    tmax_f = walk_closest<COUNT>(I.nodes, F, __double2float_rd(tmin), tmax_f, leaf, status, cnt);
+    return best;
+}
+
+// Blas::occludedLocal (scene.h:1027-1033)
+template <bool COUNT>
+__device__ __noinline__ bool blas_any(const DevInst& I, D3 wo, D3 wd, double tmin, double seg, float tmax_f,
+                                      int32_t* status, TravCount& cnt) {
+    const LocalRay L = to_local(I, wo, wd);
+    const Shear sh = make_shear(L.d);
+    const RayF F = make_rayf(L.o, L.d);
+    const PrimRec* __restrict__ recs = I.recs;
+    auto leaf = [&](int first, int count) -> bool {
+        for (int k = 0; k < count; ++k) {
+            if (COUNT) { cnt.recs++; cnt.exact++; }
+            PrimRec r;
+            load_rec(recs, first + k, r);
+            double t;
+            if (tri_test(sh, L.o, r.d, tmin, seg, t, nullptr)) return true;
+        }
+        return false;
+    };
+    return walk_any<COUNT>(I.nodes, F, __double2float_rd(tmin), tmax_f, leaf, status, cnt);
+}
+
+// Closest hit (Scene::closestHit, scene.h:2194-2242): returns the world record (or -1) and
+// t; for an instance record, *sub receives the BLAS record.  INST selects the variant that
+// can meet instance records (scenes with instances); the plain variant has no such branch.
+template <bool COUNT, bool INST>
+__device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin, double& best_t, int* sub,
+                                int32_t* status, TravCount& cnt) {
+    const RayF F = make_rayf(R.o, R.d);
+    best_t = DBL_MAX;
+    int best = -1;
+    const PrimRec* __restrict__ recs = sc.recs;
+    auto leaf = [&](int first, int count, float tm) -> float {
+        for (int k = 0; k < count; ++k) {
+            if (COUNT) cnt.recs++;
+            PrimRec r;
+            load_rec(recs, first + k, r);
+            if (INST && rec_type(r) == REC_INST) {
+                int s = blas_closest<COUNT>(sc.inst[rec_inst(r)], R.o, R.d, tmin, best_t, tm, status, cnt);
+                if (s >= 0) { best = first + k; *sub = s; }
+                continue;
+            }
+            if (COUNT) cnt.exact++;
+            double t;
+            if (rec_test(R, r, tmin, best_t, t)) { best_t = t; best = first + k; tm = __double2float_ru(t); }
+        }
+        return tm;
+    };
+    walk_closest<COUNT>(sc.nodes, F, __double2float_rd(tmin), FLT_MAX, leaf, status, cnt);
+    return best;
+}
+
+// Any hit with t in [tmin, seg) (Scene::occluded, scene.h:2249-2271).
+template <bool COUNT, bool INST>
+__device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, double seg, int32_t* status,
+                             TravCount& cnt) {
+    const RayF F = make_rayf(R.o, R.d);
+    const float tmin_f = __double2float_rd(tmin), tmax_f = __double2float_ru(seg);
+    const PrimRec* __restrict__ recs = sc.recs;
+    auto leaf = [&](int first, int count) -> bool {
+        for (int k = 0; k < count; ++k) {
+            if (COUNT) cnt.recs++;
+            PrimRec r;
+            load_rec(recs, first + k, r);
+            if (INST && rec_type(r) == REC_INST) {
+                if (blas_any<COUNT>(sc.inst[rec_inst(r)], R.o, R.d, tmin, seg, tmax_f, status, cnt)) return true;
+                continue;
+            }
+            if (COUNT) cnt.exact++;
+            double t;
+            if (rec_test(R, r, tmin, seg, t)) return true;
+        }
+        return false;
+    };
+    return walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, leaf, status, cnt);
+}
+
+// Hit on BLAS record `sub` of instance I, in world terms: the local hit's attributes
+// (intersectTri on the local ray) mapped like Scene::instanceHitToWorld (scene.h:2139-2162).
+__device__ void instance_hit(const DevInst& I, int sub, D3 ro, D3 rd, Hit& h) {
+    const LocalRay L = to_local(I, ro, rd);
+    RayCtx R;
+    R.o = L.o; R.d = L.d;
+    R.sh = make_shear(L.d);
+    PrimRec br;
+    load_rec(I.recs, sub, br);
+    hit_attributes(I.tri_n, R, br, h);
+    h.p = ro + rd * h.t;                        // world t == local t
+    D3 wn = normalize(xf_normal(I.xl, h.n));
+    D3 wng = normalize(xf_normal(I.xl, h.ng));
+    h.ng = wng;
+    h.n = (dot(rd, wn) < 0.0) ? wn : neg(wn);
+    if (I.mat_override >= 0) h.mat = I.mat_override;
 }
 
 __device__ __forceinline__ RayCtx make_ray(D3 o, D3 d) {
@@ -999,7 +1119,7 @@ __device__ void block_add1(unsigned long long* dst, unsigned long long a) {
 #define FTB_SHADE_MINB 4
 #endif
 
-template <bool COUNT>
+template <bool COUNT, bool INST>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const DevJob* __restrict__ jobs,
                                                               int32_t n_jobs, const int32_t* q,
                                                               const int32_t* qcount, Frame f) {
@@ -1011,9 +1131,11 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const Dev
         const DevScene& sc = jobs[n_jobs > 1 ? w.job[slot] : 0].sc;
         RayCtx R = make_ray(mk(w.ox[slot], w.oy[slot], w.oz[slot]), mk(w.dx[slot], w.dy[slot], w.dz[slot]));
         double t;
-        int rec = traverse_closest<COUNT>(sc, R, EPS_RAY, t, f.status, cnt);
+        int sub = -1;
+        int rec = traverse_closest<COUNT, INST>(sc, R, EPS_RAY, t, &sub, f.status, cnt);
         w.hit_t[slot] = t;
         w.hit_rec[slot] = rec;
+        if (INST) w.hit_sub[slot] = sub;
         if (COUNT) rays++;
     }
     if (COUNT) {
@@ -1108,7 +1230,10 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         if (w.logs) {
             int nh = w.lnh[slot];
             int prim = rec >= 0 ? sc.recs[rec].prim : -1;
-            w.lhash[slot] = fnv_i32(w.lhash[slot], prim);
+            uint64_t hsh = fnv_i32(w.lhash[slot], prim);
+            if (rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)   // and the BLAS triangle
+                hsh = fnv_i32(hsh, sc.inst[rec_inst(sc.recs[rec])].recs[w.hit_sub[slot]].prim);
+            w.lhash[slot] = hsh;
             if (nh < 8) w.lprims[nh * w.W + slot] = prim;
             w.lnh[slot] = nh + 1;
         }
@@ -1141,9 +1266,14 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         } else {
             PrimRec r;
             load_rec(sc.recs, rec, r);
-            RayCtx R = make_ray(ro, rd);
             Hit h;
-            hit_attributes(sc, R, r, h);
+            if (rec_type(r) == REC_INST) {
+                instance_hit(sc.inst[rec_inst(r)], w.hit_sub[slot], ro, rd, h);
+                h.prim = r.prim;
+            } else {
+                RayCtx R = make_ray(ro, rd);
+                hit_attributes(sc.tri_n, R, r, h);
+            }
             const DevMat& m = sc.mats[h.mat];
             switch (m.type) {
             case FTB_MAT_DIELECTRIC: {   // render.h:1612-1660
@@ -1255,7 +1385,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
 }
 
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
-template <bool COUNT>
+template <bool COUNT, bool INST>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const DevJob* __restrict__ jobs,
                                                               int32_t n_jobs, Frame f) {
     int n = w.counts[2];
@@ -1269,7 +1399,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
         double max_dist = w.smax[i];
         RayCtx R = make_ray(o, d);
         if (COUNT) rays++;
-        if (traverse_any<COUNT>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
+        if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         double lam = w.slam[i], c = w.sval[i];
         double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
         long long* px = reinterpret_cast<long long*>(J.film) + 4 * (size_t)w.spix[i];
@@ -1285,40 +1415,21 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
 }
 
 // ------------------------------------------------------------------ host side ----------
-namespace {
-size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
-}
-
-size_t wave_bytes(int32_t W, bool log) {
-    size_t w = (size_t)W, s = 2 * (size_t)W;
-    size_t b = 0;
-    b += 2 * align_up(8 * w);                 // rng
-    b += 8 * align_up(8 * w);                 // ray + lam + beta
-    b += align_up(4 * w) + align_up(8 * w * kStkCap);
-    b += align_up(8 * w) + align_up(4 * w);   // hit
-    b += 2 * align_up(4 * w) + align_up(64);  // queues + counts
-    b += align_up(4 * w) + align_up(4 * s) + align_up(sizeof(DevJob) * kWaveJobs);   // job ids + table
-    b += 9 * align_up(8 * s) + align_up(4 * s);
-    if (log) b += align_up(8 * w) + align_up(4 * w) + align_up(4 * w * 8);
-    return b;
-}
-
-cudaError_t wave_alloc(Wave& w, int32_t W, bool log) {
+void wave_carve(Wave& w, void* block, int32_t W, bool log) {
     w = Wave{};
     w.W = W;
     w.S = 2 * W;
     w.bytes = wave_bytes(W, log);
-    cudaError_t e = cudaMalloc(&w.block, w.bytes);
-    if (e != cudaSuccess) { w.block = nullptr; return e; }
-    char* p = (char*)w.block;
-    auto take = [&](size_t n) { void* r = p; p += align_up(n); return r; };
+    w.block = block;
+    char* p = (char*)block;
+    auto take = [&](size_t n) { void* r = p; p += wave_align(n); return r; };
     size_t wn = (size_t)W, sn = (size_t)w.S;
     w.rng_s = (uint64_t*)take(8 * wn); w.rng_i = (uint64_t*)take(8 * wn);
     w.ox = (double*)take(8 * wn); w.oy = (double*)take(8 * wn); w.oz = (double*)take(8 * wn);
     w.dx = (double*)take(8 * wn); w.dy = (double*)take(8 * wn); w.dz = (double*)take(8 * wn);
     w.lam = (double*)take(8 * wn); w.beta = (double*)take(8 * wn);
     w.stk_n = (int32_t*)take(4 * wn); w.stk = (int2*)take(8 * wn * kStkCap);
-    w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn);
+    w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn); w.hit_sub = (int32_t*)take(4 * wn);
     w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
     w.counts = (int32_t*)take(64);
     w.job = (int32_t*)take(4 * wn); w.sjob = (int32_t*)take(4 * sn);
@@ -1330,6 +1441,13 @@ cudaError_t wave_alloc(Wave& w, int32_t W, bool log) {
     if (log) {
         w.lhash = (uint64_t*)take(8 * wn); w.lnh = (int32_t*)take(4 * wn); w.lprims = (int32_t*)take(4 * wn * 8);
     }
+}
+
+cudaError_t wave_alloc(Wave& w, int32_t W, bool log) {
+    void* block = nullptr;
+    cudaError_t e = cudaMalloc(&block, wave_bytes(W, log));
+    if (e != cudaSuccess) { w = Wave{}; return e; }
+    wave_carve(w, block, W, log);
     return cudaSuccess;
 }
 
@@ -1339,7 +1457,7 @@ void wave_free(Wave& w) {
 }
 
 cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_slots, int32_t max_bounce,
-                        const Frame& f, int32_t sms, cudaStream_t st, LaunchSink* sink) {
+                        bool inst, const Frame& f, int32_t sms, cudaStream_t st, LaunchSink* sink) {
     const int T = 128;
     int blocks_emit = (n_slots + T - 1) / T;
     if (blocks_emit < 1) blocks_emit = 1;
@@ -1350,8 +1468,13 @@ cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_s
     auto mark = [&](int k, bool end) { if (sink) sink->mark(k, end, st); };
     auto shadow = [&]() {
         mark(K_SHADOW, false);
-        if (count) k_shadow<true><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
-        else k_shadow<false><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+        if (count) {
+            if (inst) k_shadow<true, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+            else k_shadow<true, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+        } else {
+            if (inst) k_shadow<false, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+            else k_shadow<false, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+        }
         mark(K_SHADOW, true);
         cudaMemsetAsync(&w.counts[2], 0, 4, st);
     };
@@ -1366,8 +1489,13 @@ cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_s
     int32_t* cb = &w.counts[1];
     for (int b = 0; b < max_bounce; ++b) {
         mark(K_EXTEND, false);
-        if (count) k_extend<true><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
-        else k_extend<false><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+        if (count) {
+            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+        } else {
+            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+        }
         mark(K_EXTEND, true);
         cudaMemsetAsync(cb, 0, 4, st);
         mark(K_SHADE, false);

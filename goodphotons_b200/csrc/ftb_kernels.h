@@ -42,7 +42,8 @@ struct Wave {
     int32_t* stk_n;            // medium-stack depth per slot
     int2* stk;                 // [kStkCap][W] (material, priority)
     double* hit_t;
-    int32_t* hit_rec;
+    int32_t* hit_rec;          // world record of the closest hit, or -1
+    int32_t* hit_sub;          // BLAS record when hit_rec is an instance
     int32_t* qa;               // active slot lists (ping-pong)
     int32_t* qb;
     int32_t* counts;           // [0] qa count, [1] qb count, [2] shadow count
@@ -69,7 +70,24 @@ struct Frame {
     int32_t* status;
 };
 
-size_t wave_bytes(int32_t W, bool log);
+// Bytes of one wave of W slots: every array rounded up to 256 B, in the order wave_carve
+// lays them out.  constexpr so a fixed device array can hold a wave (ftb_noalloc.cu).
+constexpr size_t wave_align(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t wave_bytes(int32_t W, bool log) {
+    size_t w = (size_t)W, s = 2 * (size_t)W;
+    size_t b = 0;
+    b += 2 * wave_align(8 * w);                                     // rng
+    b += 8 * wave_align(8 * w);                                     // ray + lam + beta
+    b += wave_align(4 * w) + wave_align(8 * w * kStkCap);           // medium stack
+    b += wave_align(8 * w) + 2 * wave_align(4 * w);                 // hit t, record, sub-record
+    b += 2 * wave_align(4 * w) + wave_align(64);                    // queues + counts
+    b += wave_align(4 * w) + wave_align(4 * s) + wave_align(sizeof(DevJob) * kWaveJobs);   // job ids + table
+    b += 9 * wave_align(8 * s) + wave_align(4 * s);                 // shadow records
+    if (log) b += wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
+    return b;
+}
+// Point the arrays of `w` into `block` (wave_bytes(W, log) bytes, 256-B aligned).
+void wave_carve(Wave& w, void* block, int32_t W, bool log);
 cudaError_t wave_alloc(Wave& w, int32_t W, bool log);
 void wave_free(Wave& w);
 
@@ -85,10 +103,12 @@ struct LaunchSink {
 
 // Trace one wave on `stream`: jobs[0..n_jobs) is the device job table (already filled,
 // slot ranges consecutive from 0, n_slots = the sum of their n <= W), and every slot runs
-// through at most max_bounce bounces (the largest max_bounce of the jobs).  With f.stats set,
-// the counting variants of the traversal kernels run (slower; for traffic accounting only).
+// through at most max_bounce bounces (the largest max_bounce of the jobs).  `instances`
+// selects the traversal variants that meet instance records (set when any job's scene has
+// instances).  With f.stats set, the counting variants of the traversal kernels run
+// (slower; for traffic accounting only).
 cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_slots,
-                        int32_t max_bounce, const Frame& f, int32_t sms, cudaStream_t stream,
-                        LaunchSink* sink = nullptr);
+                        int32_t max_bounce, bool instances, const Frame& f, int32_t sms,
+                        cudaStream_t stream, LaunchSink* sink = nullptr);
 
 }  // namespace ftb

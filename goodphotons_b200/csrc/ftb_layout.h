@@ -11,6 +11,9 @@
 //             reads them); the last 8 B carry the global primitive index, material and
 //             type.  Leaf children of a node reference a contiguous run of records.
 //   tri_n   : optional per-triangle shading normals (9 doubles), by triangle index.
+//   inst    : DevInst[n_inst], 128 B each -- instances of shared BLAS assets.  The world
+//             hierarchy (TLAS) holds one REC_INST record per instance; a BLAS is a wide
+//             BVH and triangle records of its own, in its local space.
 //   spectra, tables, materials, emitters, media: small tables.
 #pragma once
 #include <stdint.h>
@@ -19,7 +22,7 @@
 #define FTB_LEAF_MAX 4
 #define FTB_STACK 64
 
-enum { REC_TRI = 0, REC_SPHERE = 1, REC_CURVE = 2 };
+enum { REC_TRI = 0, REC_SPHERE = 1, REC_CURVE = 2, REC_INST = 3 };
 
 // meta byte of a child slot: 0 = empty; otherwise count<<5 | offset.  For an internal child
 // (imask bit set) count is 1 and offset is the child's index relative to child_base; for a
@@ -36,7 +39,8 @@ struct alignas(16) WNode {
 static_assert(sizeof(WNode) == 80, "WNode must be 80 bytes");
 
 // 80-byte primitive record.  d[9] holds two int32: prim (global index) and
-// info = mat | type << 24 | smooth << 30.
+// info = mat | type << 24 | smooth << 30.  An instance record (REC_INST) keeps its instance
+// index in d[0] (as an int64 bit pattern); a BLAS triangle's prim is its index in the BLAS.
 struct alignas(16) PrimRec {
     double d[9];
     int32_t prim;
@@ -70,6 +74,16 @@ struct DevMed {
     double radius;
 };
 
+// One placement of a BLAS (MeshInstance, scene.h:1035-1063).
+struct DevInst {
+    double xl[12];            // world -> local map (toLocal): 3x3 row-major, then translation
+    const WNode* nodes;       // the BLAS hierarchy and triangle records
+    const PrimRec* recs;
+    const double* tri_n;      // 9 per BLAS triangle or null
+    int32_t mat_override, pad;
+};
+static_assert(sizeof(DevInst) == 128, "DevInst must be 128 bytes");
+
 struct DevScene {
     const WNode* nodes;
     const PrimRec* recs;
@@ -81,10 +95,11 @@ struct DevScene {
     const DevEmit* emit;
     const double* emit_cdf;   // selection CDF over emitters
     const DevMed* med;
+    const DevInst* inst;
     int32_t n_nodes, n_recs, n_mats, n_emit, n_med, n_spec;
     int64_t n_tris;
+    int64_t n_inst;
     double total_power;
-
 };
 
 struct DevCam {

@@ -37,13 +37,7 @@ constexpr int32_t kNoAllocPhotons = 1 << 15;
 
 constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Layout of one wave in the scratch array (same fields as ftb::wave_alloc).
-constexpr size_t wave_layout_bytes(size_t w) {
-    return 2 * al(8 * w) + 8 * al(8 * w) + al(4 * w) + al(8 * w * ftb::kStkCap) + al(8 * w) + al(4 * w) +
-           2 * al(4 * w) + al(64) + al(4 * w) + al(4 * 2 * w) + al(sizeof(ftb::DevJob) * ftb::kWaveJobs) +
-           9 * al(8 * 2 * w) + al(4 * 2 * w);
-}
-constexpr size_t kWaveBytes = wave_layout_bytes(kNoAllocPhotons);
+constexpr size_t kWaveBytes = ftb::wave_bytes(kNoAllocPhotons, false);
 constexpr size_t kNoAllocBytes = kWaveBytes + al(8 * sizeof(unsigned long long)) + al(64);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -54,28 +48,6 @@ void* g_scratch_addr[256] = {};   // per device, resolved once
 ftb_status na_fail(ftb_status s, const std::string& m) {
     ftb::set_last_error(m);
     return s;
-}
-
-void carve(ftb::Wave& w, char* p, int32_t W) {
-    auto take = [&](size_t n) { void* r = p; p += al(n); return r; };
-    size_t wn = (size_t)W, sn = 2 * (size_t)W;
-    w = ftb::Wave{};
-    w.W = W;
-    w.S = (int32_t)sn;
-    w.rng_s = (uint64_t*)take(8 * wn); w.rng_i = (uint64_t*)take(8 * wn);
-    w.ox = (double*)take(8 * wn); w.oy = (double*)take(8 * wn); w.oz = (double*)take(8 * wn);
-    w.dx = (double*)take(8 * wn); w.dy = (double*)take(8 * wn); w.dz = (double*)take(8 * wn);
-    w.lam = (double*)take(8 * wn); w.beta = (double*)take(8 * wn);
-    w.stk_n = (int32_t*)take(4 * wn); w.stk = (int2*)take(8 * wn * ftb::kStkCap);
-    w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn);
-    w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
-    w.counts = (int32_t*)take(64);
-    w.job = (int32_t*)take(4 * wn); w.sjob = (int32_t*)take(4 * sn);
-    w.jobs = (ftb::DevJob*)take(sizeof(ftb::DevJob) * ftb::kWaveJobs);
-    w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
-    w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
-    w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
-    w.spix = (int32_t*)take(4 * sn);
 }
 
 int default_frac_bits(int64_t n) {   // the same default as the other render entry points
@@ -124,7 +96,7 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     }
     cudaStream_t st = (cudaStream_t)stream;
     ftb::Wave w;
-    carve(w, base, kNoAllocPhotons);
+    ftb::wave_carve(w, base, kNoAllocPhotons, false);
     unsigned long long* tally = (unsigned long long*)(base + kWaveBytes);
     int32_t* status = (int32_t*)(base + kWaveBytes + al(8 * sizeof(unsigned long long)));
     const int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
@@ -151,7 +123,8 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 64, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(w.jobs, &J, sizeof J, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && p->n_photons > 0)
-        e = ftb::launch_wave(w, w.jobs, 1, (int32_t)p->n_photons, p->max_bounce, f, sms, st, nullptr);
+        e = ftb::launch_wave(w, w.jobs, 1, (int32_t)p->n_photons, p->max_bounce, dev.n_inst > 0, f, sms, st,
+                             nullptr);
     if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (out == FTB_OK && info) {
         info->frac_bits = frac;

@@ -73,6 +73,10 @@ def load(path=None):
          C.POINTER(abi.Energy), C.c_void_p)
     _sig(L, "ftb_render_batch", st, C.POINTER(abi.Job), C.c_int32, C.POINTER(abi.FilmInfo),
          C.POINTER(abi.Energy), C.c_void_p)
+    _sig(L, "ftb_blas_create", st, C.POINTER(abi.BlasDesc), C.c_int32, C.POINTER(PS))
+    _sig(L, "ftb_blas_destroy", st, PS)
+    _sig(L, "ftb_scene_set_instance_transforms", st, PS, C.POINTER(C.c_double), C.c_int64)
+    _sig(L, "ftb_scene_clone_instances", st, PS, C.POINTER(C.c_double), C.c_int64, C.POINTER(PS))
     _sig(L, "ftb_scene_set_profiling", st, PS, C.c_int32)
     _sig(L, "ftb_scene_profile", st, PS, C.POINTER(abi.KernelProfile), C.c_int32)
     w = _Lib(L)
@@ -140,15 +144,66 @@ class _Lib:
         return r, self.L.ftb_last_error().decode()
 
 
+class Blas:
+    """A baked, device-resident triangle asset (ftb_blas_create) that scenes can share:
+    pass it as `handle` to SceneBuilder.blas."""
+
+    def __init__(self, tri_v, tri_mat, normals=None, device=0, lib=None):
+        self.lib = lib or load()
+        self.tri_v = np.ascontiguousarray(tri_v, dtype=np.float64).reshape(-1, 9)
+        self.tri_mat = np.ascontiguousarray(np.broadcast_to(tri_mat, (len(self.tri_v),)), dtype=np.int32)
+        self.tri_n = None if normals is None else np.ascontiguousarray(normals, np.float64).reshape(-1, 9)
+        d = abi.BlasDesc()
+        d.n_tris = len(self.tri_v)
+        d.tri_v = self.tri_v.ctypes.data_as(C.POINTER(C.c_double))
+        d.tri_n = self.tri_n.ctypes.data_as(C.POINTER(C.c_double)) if self.tri_n is not None else None
+        d.tri_mat = self.tri_mat.ctypes.data_as(C.POINTER(C.c_int32))
+        h = C.c_void_p()
+        self.lib.check(self.lib.L.ftb_blas_create(C.byref(d), device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.L.ftb_blas_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _xf_array(to_world):
+    a = np.ascontiguousarray(to_world, dtype=np.float64).reshape(-1, 12)
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
 class Scene:
     """A baked, device-resident scene (ftb_scene_create)."""
 
-    def __init__(self, desc, device=0, lib=None):
+    def __init__(self, desc, device=0, lib=None, _handle=None):
         self.lib = lib or load()
         self.desc = desc
+        if _handle is not None:
+            self.h = _handle
+            return
         h = C.c_void_p()
         self.lib.check(self.lib.L.ftb_scene_create(desc.ref(), device, C.byref(h)))
         self.h = h
+
+    def set_instance_transforms(self, to_world):
+        """Refit: new to_world maps (n x 12: 3x3 row-major, then translation) for
+        instances 0..n-1."""
+        a, ptr = _xf_array(to_world)
+        self.lib.check(self.lib.L.ftb_scene_set_instance_transforms(self.h, ptr, len(a)))
+
+    def clone_instances(self, to_world):
+        """A scene sharing this one's device tables, with its own refit top level."""
+        a, ptr = _xf_array(to_world)
+        h = C.c_void_p()
+        self.lib.check(self.lib.L.ftb_scene_clone_instances(self.h, ptr, len(a), C.byref(h)))
+        return Scene(self.desc, lib=self.lib, _handle=h)
 
     def close(self):
         if self.h:

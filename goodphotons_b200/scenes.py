@@ -29,7 +29,8 @@ class SceneDesc:
     """Owns the numpy arrays behind an `ftb_scene_desc` and the struct itself."""
 
     def __init__(self, tri_v, tri_n, tri_mat, sph, sph_mat, curve, curve_mat, mats,
-                 spectra, table_w, table_v, emitters, emitter_cdf, media, meta=None):
+                 spectra, table_w, table_v, emitters, emitter_cdf, media, meta=None,
+                 blas=(), instances=()):
         self.tri_v = np.ascontiguousarray(tri_v, dtype=np.float64).reshape(-1, 9)
         self.tri_n = None if tri_n is None else np.ascontiguousarray(tri_n, np.float64).reshape(-1, 9)
         self.tri_mat = np.ascontiguousarray(tri_mat, dtype=np.int32)
@@ -49,6 +50,24 @@ class SceneDesc:
         self.media = (abi.Medium * max(1, len(media)))(*media)
         self.n_media = len(media)
         self.meta = dict(meta or {})
+        # BLAS assets: (tri_v, tri_n or None, tri_mat, handle or None)
+        self.blas_arrays = []
+        for tv, tn, tm, handle in blas:
+            tv = np.ascontiguousarray(tv, dtype=np.float64).reshape(-1, 9)
+            tn = None if tn is None else np.ascontiguousarray(tn, np.float64).reshape(-1, 9)
+            tm = np.ascontiguousarray(tm, dtype=np.int32)
+            self.blas_arrays.append((tv, tn, tm, handle))
+        self.blas = (abi.BlasDesc * max(1, len(self.blas_arrays)))()
+        for i, (tv, tn, tm, handle) in enumerate(self.blas_arrays):
+            b = self.blas[i]
+            b.n_tris = len(tv)
+            b.tri_v = _as_ptr(tv, C.c_double)
+            b.tri_n = _as_ptr(tn, C.c_double) if tn is not None else None
+            b.tri_mat = _as_ptr(tm, C.c_int32)
+            b.handle = handle.h.value if handle is not None else None
+        self.n_blas = len(self.blas_arrays)
+        self.instances = (abi.Instance * max(1, len(instances)))(*instances)
+        self.n_instances = len(instances)
         d = abi.SceneDesc()
         d.n_tris = len(self.tri_v)
         d.tri_v = _as_ptr(self.tri_v, C.c_double)
@@ -72,11 +91,15 @@ class SceneDesc:
         d.emitters = C.cast(self.emitters, C.POINTER(abi.Emitter))
         d.emitter_cdf = _as_ptr(self.emitter_cdf, C.c_double)
         d.media = C.cast(self.media, C.POINTER(abi.Medium))
+        d.n_blas = self.n_blas
+        d.blas = C.cast(self.blas, C.POINTER(abi.BlasDesc))
+        d.n_instances = self.n_instances
+        d.instances = C.cast(self.instances, C.POINTER(abi.Instance))
         self.desc = d
 
     @property
     def n_prims(self):
-        return len(self.tri_v) + len(self.sph) + len(self.curve)
+        return len(self.tri_v) + len(self.sph) + len(self.curve) + self.n_instances
 
     def ref(self):
         return C.byref(self.desc)
@@ -100,6 +123,8 @@ class SceneBuilder:
         self.media = []
         self.meta = {}
         self._smooth = False
+        self.blas_list = []     # (tri_v, tri_n, tri_mat, handle)
+        self.instance_list = []
 
     # -- spectra ----------------------------------------------------------------------
     def _spec(self, kind, p=(), n=0, offset=0):
@@ -170,6 +195,25 @@ class SceneBuilder:
         segs = np.asarray(segs, dtype=np.float64).reshape(-1, 10)
         self.curve.append(segs)
         self.curve_mat.append(np.full(len(segs), mat, dtype=np.int32))
+
+    def blas(self, v, mat, normals=None, handle=None):
+        """A triangle asset in its own local space (Blas, scene.h:996); returns its index.
+        `handle` (lib.Blas) shares an already baked device copy of the same triangles."""
+        v = np.asarray(v, dtype=np.float64).reshape(-1, 9)
+        m = np.ascontiguousarray(np.broadcast_to(np.asarray(mat, np.int32), (len(v),)))
+        self.blas_list.append((v, normals, m, handle))
+        return len(self.blas_list) - 1
+
+    def instance(self, blas, to_world, mat_override=-1):
+        """Place BLAS `blas` by the affine `to_world` (12 doubles: 3x3 row-major, then the
+        translation; MeshInstance, scene.h:1035); returns the instance index."""
+        inst = abi.Instance()
+        inst.blas = blas
+        inst.mat_override = mat_override
+        for i, x in enumerate(np.asarray(to_world, dtype=np.float64).reshape(12)):
+            inst.to_world[i] = float(x)
+        self.instance_list.append(inst)
+        return len(self.instance_list) - 1
 
     def box(self, center_xz, size, height, angle_deg, mat, y0=0.0):
         """Axis-aligned-in-y box (12 triangles) rotated about +y, outward winding."""
@@ -266,7 +310,21 @@ class SceneBuilder:
         cdf_all = np.concatenate(cdfs) if cdfs else np.zeros(0)
         return SceneDesc(tri_v, tri_n, tri_mat, sph, sph_mat, curve, curve_mat, self.mats,
                          self.spectra, self.table_w, self.table_v, emitters, cdf_all,
-                         self.media, self.meta)
+                         self.media, self.meta, blas=self.blas_list, instances=self.instance_list)
+
+
+def affine(axis=(0.0, 1.0, 0.0), angle_deg=0.0, translate=(0.0, 0.0, 0.0), scale=1.0):
+    """12-double to_world map: rotation by angle_deg about `axis` (Rodrigues), a uniform
+    scale, then the translation."""
+    a = np.asarray(axis, dtype=np.float64)
+    a = a / np.linalg.norm(a)
+    th = math.radians(angle_deg)
+    c, s = math.cos(th), math.sin(th)
+    x, y, z = a
+    R = np.array([[c + x * x * (1 - c), x * y * (1 - c) - z * s, x * z * (1 - c) + y * s],
+                  [y * x * (1 - c) + z * s, c + y * y * (1 - c), y * z * (1 - c) - x * s],
+                  [z * x * (1 - c) - y * s, z * y * (1 - c) + x * s, c + z * z * (1 - c)]]) * scale
+    return np.concatenate([R.reshape(9), np.asarray(translate, dtype=np.float64)])
 
 
 # ---------------------------------------------------------------------------------------
@@ -363,15 +421,27 @@ def value_noise3(p, seed, octaves=3, base_freq=4.0):
     return total / norm
 
 
-def glass_blob(sb: SceneBuilder, level=7, center=(1.0, 0.55, 1.0), radius=0.4, amp=0.05,
-               seed=0, mat=None):
+GLASS_CENTER = (1.0, 0.55, 1.0)
+
+
+def blob_tris(level=7, center=(0.0, 0.0, 0.0), radius=0.4, amp=0.05, seed=0):
+    """Triangles (n x 9) of a subdivided icosphere displaced radially by value noise."""
     v, f = icosphere(level)
     n = value_noise3(v, seed)
     r = radius + amp * (2.0 * n - 1.0)
     pos = np.asarray(center)[None, :] + v * r[:, None]
-    tv = pos[f].reshape(-1, 9)
+    return pos[f].reshape(-1, 9)
+
+
+def glass_material(sb: SceneBuilder):
+    return sb.material(abi.MAT_DIELECTRIC, ior=sb.cauchy(1.5, 0.0042), roughness=0.0)
+
+
+def glass_blob(sb: SceneBuilder, level=7, center=GLASS_CENTER, radius=0.4, amp=0.05,
+               seed=0, mat=None):
+    tv = blob_tris(level, center, radius, amp, seed)
     if mat is None:
-        mat = sb.material(abi.MAT_DIELECTRIC, ior=sb.cauchy(1.5, 0.0042), roughness=0.0)
+        mat = glass_material(sb)
     sb.tris(tv, mat)
     return mat
 
@@ -437,6 +507,20 @@ def make_glass(lib=None, level=7, seed=0):
     cornell_box(sb, boxes=False)
     glass_blob(sb, level=level, seed=seed)
     sb.meta.update(name="glass", level=level)
+    return sb.build(lib)
+
+
+def make_glass_instanced(lib=None, level=7, seed=0, to_world=None, handle=None):
+    """The glass scene with the blob as one instance of a BLAS authored about the origin
+    (to_world defaults to a translation to the blob's usual center).  `handle` (lib.Blas
+    of blob_tris(level, seed=seed) with material 5) shares a baked copy of the mesh."""
+    sb = SceneBuilder()
+    cornell_box(sb, boxes=False)
+    mat = glass_material(sb)
+    tv = None if handle is not None else blob_tris(level, seed=seed)
+    b = sb.blas(np.zeros((0, 9)) if tv is None else tv, mat, handle=handle)
+    sb.instance(b, affine(translate=GLASS_CENTER) if to_world is None else to_world)
+    sb.meta.update(name="glass_instanced", level=level)
     return sb.build(lib)
 
 

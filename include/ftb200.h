@@ -16,7 +16,7 @@
  *    order in which photons land, so renders are bit-reproducible across launches, stream
  *    counts and GPU counts.
  *  - Primitive indices are global, in the reference's order (scene.h:2194-2234):
- *    triangles, then spheres, then curve segments.
+ *    triangles, then spheres, then curve segments, then instances.
  */
 #ifndef FTB200_H
 #define FTB200_H
@@ -127,6 +127,32 @@ typedef struct ftb_medium {
     double radius;
 } ftb_medium;
 
+/* ---- instanced meshes --------------------------------------------------------------
+ * A BLAS is a triangle asset in its own (local) space; instances place it in the world by
+ * an affine map, like the reference's Blas / MeshInstance (scene.h:996-1063).  A ray meets
+ * an instance by being mapped into local space with the inverse map (toLocal, computed from
+ * to_world with the reference's Affine::inverse, linalg.h:129-144); local t equals world t.
+ * A BLAS may be baked once into a device-resident handle (ftb_blas_create) and shared by
+ * many scenes, e.g. the frames of an animation, which then only build their small
+ * top-level hierarchy. */
+typedef struct ftb_blas ftb_blas;
+
+typedef struct ftb_blas_desc {
+    int64_t n_tris;
+    const double* tri_v;    /* n_tris x 9, local space */
+    const double* tri_n;    /* optional per-vertex shading normals, n_tris x 9 */
+    const int32_t* tri_mat; /* indices into the scene's materials */
+    ftb_blas* handle;       /* optional: a baked copy of this BLAS (ftb_blas_create); the
+                               scene then shares it instead of baking its own, and the
+                               arrays above are not read. */
+} ftb_blas_desc;
+
+typedef struct ftb_instance {
+    int32_t blas;           /* index into ftb_scene_desc.blas */
+    int32_t mat_override;   /* >= 0 replaces the BLAS triangles' material */
+    double to_world[12];    /* 3x3 linear part row-major, then the translation */
+} ftb_instance;
+
 /* ---- scene --------------------------------------------------------------------------
  * tri_v:    n_tris x 9 doubles (v0 v1 v2), winding defines the geometric normal
  * tri_n:    optional n_tris x 9 doubles of per-vertex shading normals (NULL: flat);
@@ -156,6 +182,11 @@ typedef struct ftb_scene_desc {
     const ftb_emitter* emitters;
     const double* emitter_cdf;
     const ftb_medium* media;
+    int32_t n_blas;
+    int32_t pad0;
+    const ftb_blas_desc* blas;
+    int64_t n_instances;
+    const ftb_instance* instances;
 } ftb_scene_desc;
 
 /* ---- camera -------------------------------------------------------------------------
@@ -235,6 +266,32 @@ ftb_status ftb_emission_cdf(const ftb_spectrum* spd, const double* table_w,
  * render_cuda.cu:12692-13546).  The descriptor is only read during the call. */
 ftb_status ftb_scene_create(const ftb_scene_desc* desc, int32_t device, ftb_scene** out);
 ftb_status ftb_scene_destroy(ftb_scene* scene);
+
+/* Bake a BLAS (its wide BVH and records) once, for sharing by scenes (no counterpart in
+ * the reference, which rebuilds everything per scene load).  Triangle materials index the
+ * material table of each scene that uses it.  ftb_blas_destroy releases the caller's
+ * handle; scenes created on it hold their own reference, so the device copy lives until
+ * the last of them is destroyed. */
+ftb_status ftb_blas_create(const ftb_blas_desc* desc, int32_t device, ftb_blas** out);
+ftb_status ftb_blas_destroy(ftb_blas* blas);
+
+/* Move the scene's instances (TLAS refit; no counterpart in the reference): new to_world
+ * maps (12 doubles each) for instances [0, n), same BLAS and materials.  The top-level
+ * hierarchy keeps its topology and gets recomputed, re-quantized bounds, so a render after
+ * the refit traces the same paths as a scene created with the new maps (up to exact ties
+ * in t, which any two hierarchies may order differently).  No render of this scene may
+ * be in flight during the call (synchronize the streams of stream-ordered renders). */
+ftb_status ftb_scene_set_instance_transforms(ftb_scene* scene, const double* to_world,
+                                             int64_t n);
+
+/* A new scene that shares `src`'s device tables (geometry, materials, emitters, media,
+ * BLAS assets) and has its own top-level hierarchy, refit for new maps of instances
+ * [0, n) (no counterpart in the reference).  This is how the frames of an animation are
+ * made: one scene per frame costs one small top-level copy, and the frames can be
+ * rendered together in one ftb_render_batch.  Clones are destroyed with
+ * ftb_scene_destroy, in any order relative to `src`. */
+ftb_status ftb_scene_clone_instances(const ftb_scene* src, const double* to_world, int64_t n,
+                                     ftb_scene** out);
 ftb_status ftb_scene_footprint(const ftb_scene* scene, int32_t res_x, int32_t res_y,
                                ftb_footprint* out);
 /* Total emitted power the film and energy fixed point are relative to. */

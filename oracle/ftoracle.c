@@ -241,6 +241,25 @@ typedef struct {
     int left, right, first, count;   /* count>0: leaf over order[first..first+count) */
 } Node;
 
+/* Affine (linalg.h:99-182): m row-major 3x3, then t */
+typedef struct { double m[9]; V3 t; } Aff;
+
+/* a binary BVH over primitives order[] (the oracle's own culling structure) */
+typedef struct { Node* nodes; int n_nodes; int* order; } Tree;
+
+/* Blas (scene.h:996-1033): triangles in local space with their own tree */
+typedef struct {
+    int64_t nt;
+    Tri* tris;
+    Tree tree;
+    V3 lo, hi;          /* localBounds: union of the tri boxes padded by 1e-6 */
+} Blas;
+
+typedef struct {
+    int blas, mat_override;
+    Aff to_world, to_local;
+} Inst;
+
 typedef struct {
     int shape, collimated, n;
     double step, power;
@@ -257,6 +276,10 @@ typedef struct {
 } Med;
 
 struct fto_ctx {
+    int64_t ni;
+    int n_blas;
+    Blas* blas;
+    Inst* inst;
     SpecSet S;
     ftb_spectrum* spec;
     double *tw, *tv;
@@ -267,9 +290,7 @@ struct fto_ctx {
     double* sph;      /* 4 per sphere */
     int* sph_mat;
     Crv* crv;
-    Node* nodes;
-    int n_nodes;
-    int* order;
+    Tree world;       /* over tris, spheres, curves, instances */
     int n_emit;
     Emit* emit;
     double* cdf_store;
@@ -306,7 +327,7 @@ static double ld_diff(double a, double b, double c, double d) {
 
 typedef struct {
     double t;
-    int valid, prim, mat;
+    int valid, prim, mat, sub;
     V3 p, n, ng;
 } Hit;
 
@@ -496,29 +517,85 @@ static inline double shadow_terminator_g(V3 wi, V3 ns, V3 ng) {
     return g * g * (1.0 - g) + g;
 }
 
+/* ------------------------------------------------------------- Affine (linalg.h) --- */
+/* Affine::apply / applyDir (linalg.h:105-114) */
+static inline V3 aff_apply(const Aff* a, V3 p) {
+    return v3(a->m[0] * p.x + a->m[1] * p.y + a->m[2] * p.z + a->t.x,
+              a->m[3] * p.x + a->m[4] * p.y + a->m[5] * p.z + a->t.y,
+              a->m[6] * p.x + a->m[7] * p.y + a->m[8] * p.z + a->t.z);
+}
+static inline V3 aff_apply_dir(const Aff* a, V3 v) {
+    return v3(a->m[0] * v.x + a->m[1] * v.y + a->m[2] * v.z,
+              a->m[3] * v.x + a->m[4] * v.y + a->m[5] * v.z,
+              a->m[6] * v.x + a->m[7] * v.y + a->m[8] * v.z);
+}
+/* Affine::inverse (linalg.h:129-144) */
+static Aff aff_inverse(const Aff* x) {
+    Aff r;
+    memset(&r, 0, sizeof r);
+    r.m[0] = r.m[4] = r.m[8] = 1.0;
+    double a = x->m[0], b = x->m[1], c = x->m[2];
+    double d = x->m[3], e = x->m[4], f = x->m[5];
+    double g = x->m[6], h = x->m[7], i = x->m[8];
+    double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+    if (fabs(det) < 1e-30) return r;
+    double id = 1.0 / det;
+    r.m[0] = (e * i - f * h) * id; r.m[1] = (c * h - b * i) * id; r.m[2] = (b * f - c * e) * id;
+    r.m[3] = (f * g - d * i) * id; r.m[4] = (a * i - c * g) * id; r.m[5] = (c * d - a * f) * id;
+    r.m[6] = (d * h - e * g) * id; r.m[7] = (b * g - a * h) * id; r.m[8] = (a * e - b * d) * id;
+    r.t = v3(-(r.m[0] * x->t.x + r.m[1] * x->t.y + r.m[2] * x->t.z),
+             -(r.m[3] * x->t.x + r.m[4] * x->t.y + r.m[5] * x->t.z),
+             -(r.m[6] * x->t.x + r.m[7] * x->t.y + r.m[8] * x->t.z));
+    return r;
+}
+/* Affine::applyNormal (linalg.h:161-167): (M^-1)^T n with M^-1 = inverse() */
+static inline V3 aff_apply_normal(const Aff* inv, V3 n) {
+    return v3(inv->m[0] * n.x + inv->m[3] * n.y + inv->m[6] * n.z,
+              inv->m[1] * n.x + inv->m[4] * n.y + inv->m[7] * n.z,
+              inv->m[2] * n.x + inv->m[5] * n.y + inv->m[8] * n.z);
+}
+
 /* ------------------------------------------------------------- BVH (oracle only) ---- */
 /* A plain median-split binary BVH with boxes grown by a relative margin, so that its
  * culling never rejects a primitive the exact slab test would keep.  Closest-hit results
  * equal the reference's (bvh.h:181-224) except for exact ties in t. */
 typedef struct { V3 lo, hi, c; int idx; } BPrim;
 
+static void tri_box(const Tri* t, V3* lo, V3* hi) {
+    *lo = v3(fmin(t->v0.x, fmin(t->v1.x, t->v2.x)), fmin(t->v0.y, fmin(t->v1.y, t->v2.y)),
+             fmin(t->v0.z, fmin(t->v1.z, t->v2.z)));
+    *hi = v3(fmax(t->v0.x, fmax(t->v1.x, t->v2.x)), fmax(t->v0.y, fmax(t->v1.y, t->v2.y)),
+             fmax(t->v0.z, fmax(t->v1.z, t->v2.z)));
+}
+
 static void box_of(const fto_ctx* c, int p, V3* lo, V3* hi) {
     if (p < c->nt) {
-        const Tri* t = &c->tris[p];
-        *lo = v3(fmin(t->v0.x, fmin(t->v1.x, t->v2.x)), fmin(t->v0.y, fmin(t->v1.y, t->v2.y)),
-                 fmin(t->v0.z, fmin(t->v1.z, t->v2.z)));
-        *hi = v3(fmax(t->v0.x, fmax(t->v1.x, t->v2.x)), fmax(t->v0.y, fmax(t->v1.y, t->v2.y)),
-                 fmax(t->v0.z, fmax(t->v1.z, t->v2.z)));
+        tri_box(&c->tris[p], lo, hi);
     } else if (p < c->nt + c->ns) {
         const double* s = &c->sph[(p - c->nt) * 4];
         *lo = v3(s[0] - s[3], s[1] - s[3], s[2] - s[3]);
         *hi = v3(s[0] + s[3], s[1] + s[3], s[2] + s[3]);
-    } else {
+    } else if (p < c->nt + c->ns + c->nc) {
         const Crv* s = &c->crv[p - c->nt - c->ns];
         *lo = v3(fmin(s->p0.x - s->r0, s->p1.x - s->r1), fmin(s->p0.y - s->r0, s->p1.y - s->r1),
                  fmin(s->p0.z - s->r0, s->p1.z - s->r1));
         *hi = v3(fmax(s->p0.x + s->r0, s->p1.x + s->r1), fmax(s->p0.y + s->r0, s->p1.y + s->r1),
                  fmax(s->p0.z + s->r0, s->p1.z + s->r1));
+    } else {   /* instance: the 8 transformed corners of the BLAS bounds (scene.h:2033-2040) */
+        const Inst* in = &c->inst[p - c->nt - c->ns - c->nc];
+        const Blas* b = &c->blas[in->blas];
+        *lo = v3(DBL_MAX, DBL_MAX, DBL_MAX);
+        *hi = v3(-DBL_MAX, -DBL_MAX, -DBL_MAX);
+        for (int k = 0; k < 8; ++k) {
+            V3 q = v3((k & 1) ? b->hi.x : b->lo.x, (k & 2) ? b->hi.y : b->lo.y, (k & 4) ? b->hi.z : b->lo.z);
+            V3 w = aff_apply(&in->to_world, q);
+            *lo = v3(fmin(lo->x, w.x), fmin(lo->y, w.y), fmin(lo->z, w.z));
+            *hi = v3(fmax(hi->x, w.x), fmax(hi->y, w.y), fmax(hi->z, w.z));
+        }
+        double m = 1e-7 * (1.0 + fmax(fmax(fabs(lo->x), fabs(hi->x)),
+                                      fmax(fmax(fabs(lo->y), fabs(hi->y)), fmax(fabs(lo->z), fabs(hi->z)))));
+        *lo = v3(lo->x - m, lo->y - m, lo->z - m);
+        *hi = v3(hi->x + m, hi->y + m, hi->z + m);
     }
 }
 
@@ -528,9 +605,9 @@ static int cmp_prim(const void* a, const void* b) {
     return (x < y) ? -1 : (x > y) ? 1 : 0;
 }
 
-static int build_rec(fto_ctx* c, BPrim* bp, int start, int end) {
-    int ni = c->n_nodes++;
-    Node* nd = &c->nodes[ni];
+static int build_rec(Tree* T, BPrim* bp, int start, int end) {
+    int ni = T->n_nodes++;
+    Node* nd = &T->nodes[ni];
     V3 lo = v3(DBL_MAX, DBL_MAX, DBL_MAX), hi = v3(-DBL_MAX, -DBL_MAX, -DBL_MAX);
     V3 clo = lo, chi = hi;
     for (int i = start; i < end; ++i) {
@@ -554,11 +631,19 @@ static int build_rec(fto_ctx* c, BPrim* bp, int start, int end) {
     g_sort_axis = axis;
     qsort(bp + start, (size_t)count, sizeof(BPrim), cmp_prim);
     int mid = (start + end) / 2;
-    int l = build_rec(c, bp, start, mid);
-    int r = build_rec(c, bp, mid, end);
-    nd = &c->nodes[ni];
+    int l = build_rec(T, bp, start, mid);
+    int r = build_rec(T, bp, mid, end);
+    nd = &T->nodes[ni];
     nd->left = l; nd->right = r; nd->count = 0;
     return ni;
+}
+
+static void build_tree(Tree* T, BPrim* bp, int n) {
+    T->n_nodes = 0;
+    T->nodes = (Node*)malloc(sizeof(Node) * (size_t)(2 * n + 1));
+    T->order = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    if (n > 0) build_rec(T, bp, 0, n);
+    for (int i = 0; i < n; ++i) T->order[i] = bp[i].idx;
 }
 
 /* slab test in double against a grown box; NaN-safe like Aabb::hit (bvh.h:45-67) */
@@ -580,47 +665,32 @@ static inline int box_hit(const Node* n, V3 o, V3 inv, double tmin, double tmax,
     return 1;
 }
 
-/* prim test: returns 1 if accepted with t in [tmin, tbest) (fills hit if non-null) */
-static int prim_test(const fto_ctx* c, int p, const Shear* sh, const CurveRay* cr, V3 ro,
-                     V3 rd, double tmin, double tbest, Hit* hit, double* t_out) {
-    Hit h;
-    Hit* hp = hit ? hit : &h;
-    int ok;
-    if (p < c->nt) ok = intersect_tri(sh, ro, rd, &c->tris[p], tmin, tbest, hp);
-    else if (p < c->nt + c->ns)
-        ok = intersect_sphere(ro, rd, &c->sph[(p - c->nt) * 4], c->sph_mat[p - c->nt], tmin, tbest, hp);
-    else ok = intersect_curve(cr, ro, rd, &c->crv[p - c->nt - c->ns], tmin, tbest, hp);
-    if (ok && t_out) *t_out = hp->t;
-    return ok;
-}
-
-/* Scene::closestHit (scene.h:2194-2242): nearest accepted primitive; returns prim or -1 */
-static int closest_hit(const fto_ctx* c, V3 ro, V3 rd, double tmin, Hit* hit) {
-    hit->valid = 0; hit->t = DBL_MAX; hit->prim = -1;
-    if (c->n_nodes == 0) return -1;
-    Shear sh = make_shear(rd);
-    CurveRay cr = make_curve_ray(rd);
+/* Nearest primitive p of tree T with test(env, p, tbest, &t) accepted; returns p or -1. */
+typedef int (*PrimTest)(const void* env, int p, double tbest, double* t);
+static int tree_closest(const Tree* T, V3 ro, V3 rd, double tmin, double tbest, PrimTest test, const void* env,
+                        double* t_out) {
+    if (T->n_nodes == 0) return -1;
     V3 inv = v3(1.0 / rd.x, 1.0 / rd.y, 1.0 / rd.z);
-    double best = DBL_MAX;
+    double best = tbest;
     int bestp = -1;
     int stack[128]; double tst[128]; int sp = 0;
     double te;
-    if (!box_hit(&c->nodes[0], ro, inv, tmin, best, &te)) return -1;
+    if (!box_hit(&T->nodes[0], ro, inv, tmin, best, &te)) return -1;
     stack[sp] = 0; tst[sp] = te; ++sp;
     while (sp) {
         --sp;
         if (tst[sp] > best) continue;
-        const Node* n = &c->nodes[stack[sp]];
+        const Node* n = &T->nodes[stack[sp]];
         if (n->count > 0) {
             for (int i = 0; i < n->count; ++i) {
-                int p = c->order[n->first + i];
+                int p = T->order[n->first + i];
                 double t;
-                if (prim_test(c, p, &sh, &cr, ro, rd, tmin, best, NULL, &t)) { best = t; bestp = p; }
+                if (test(env, p, best, &t)) { best = t; bestp = p; }
             }
         } else {
             double tl = 0.0, tr = 0.0;
-            int hl = box_hit(&c->nodes[n->left], ro, inv, tmin, best, &tl);
-            int hr = box_hit(&c->nodes[n->right], ro, inv, tmin, best, &tr);
+            int hl = box_hit(&T->nodes[n->left], ro, inv, tmin, best, &tl);
+            int hr = box_hit(&T->nodes[n->right], ro, inv, tmin, best, &tr);
             if (sp + 2 > 128) { fail("oracle BVH stack overflow"); return -1; }
             if (hl && hr) {
                 if (tl <= tr) { stack[sp] = n->right; tst[sp++] = tr; stack[sp] = n->left; tst[sp++] = tl; }
@@ -629,35 +699,136 @@ static int closest_hit(const fto_ctx* c, V3 ro, V3 rd, double tmin, Hit* hit) {
             else if (hr) { stack[sp] = n->right; tst[sp++] = tr; }
         }
     }
-    if (bestp >= 0) {
-        prim_test(c, bestp, &sh, &cr, ro, rd, tmin, DBL_MAX, hit, NULL);
-        hit->prim = bestp;
+    if (bestp >= 0) *t_out = best;
+    return bestp;
+}
+
+/* Any primitive of tree T with test(env, p, seg, &t) accepted. */
+static int tree_any(const Tree* T, V3 o, V3 d, double tmin, double seg, PrimTest test, const void* env) {
+    if (T->n_nodes == 0) return 0;
+    V3 inv = v3(1.0 / d.x, 1.0 / d.y, 1.0 / d.z);
+    double te, t;
+    if (!box_hit(&T->nodes[0], o, inv, tmin, seg, &te)) return 0;
+    int stack[128]; int sp = 0; stack[sp++] = 0;
+    while (sp) {
+        const Node* n = &T->nodes[stack[--sp]];
+        if (n->count > 0) {
+            for (int i = 0; i < n->count; ++i)
+                if (test(env, T->order[n->first + i], seg, &t)) return 1;
+        } else {
+            if (sp + 2 > 128) { fail("oracle BVH stack overflow"); return 0; }
+            if (box_hit(&T->nodes[n->left], o, inv, tmin, seg, &te)) stack[sp++] = n->left;
+            if (box_hit(&T->nodes[n->right], o, inv, tmin, seg, &te)) stack[sp++] = n->right;
+        }
     }
+    return 0;
+}
+
+/* A ray as the leaf tests see it. */
+typedef struct {
+    const fto_ctx* c;
+    const Blas* b;     /* BLAS being walked (instance leaves) */
+    V3 ro, rd;
+    Shear sh;
+    CurveRay cr;
+    double tmin;
+} RayEnv;
+
+static int blas_test(const void* env, int p, double tbest, double* t) {
+    const RayEnv* E = (const RayEnv*)env;
+    Hit h;
+    if (!intersect_tri(&E->sh, E->ro, E->rd, &E->b->tris[p], E->tmin, tbest, &h)) return 0;
+    *t = h.t;
+    return 1;
+}
+
+/* Blas::intersectLocal / occludedLocal through an instance (scene.h:1017-1033, 2226-2231):
+ * the world ray mapped by toLocal; local t == world t. */
+static int inst_local_ray(const fto_ctx* c, int ii, V3 ro, V3 rd, double tmin, RayEnv* E) {
+    const Inst* in = &c->inst[ii];
+    E->c = c;
+    E->b = &c->blas[in->blas];
+    E->ro = aff_apply(&in->to_local, ro);
+    E->rd = aff_apply_dir(&in->to_local, rd);
+    E->sh = make_shear(E->rd);
+    E->tmin = tmin;
+    return 1;
+}
+
+static int world_test(const void* env, int p, double tbest, double* t) {
+    const RayEnv* E = (const RayEnv*)env;
+    const fto_ctx* c = E->c;
+    Hit h;
+    if (p < c->nt) {
+        if (!intersect_tri(&E->sh, E->ro, E->rd, &c->tris[p], E->tmin, tbest, &h)) return 0;
+    } else if (p < c->nt + c->ns) {
+        if (!intersect_sphere(E->ro, E->rd, &c->sph[(p - c->nt) * 4], c->sph_mat[p - c->nt], E->tmin, tbest, &h))
+            return 0;
+    } else if (p < c->nt + c->ns + c->nc) {
+        if (!intersect_curve(&E->cr, E->ro, E->rd, &c->crv[p - c->nt - c->ns], E->tmin, tbest, &h)) return 0;
+    } else {
+        RayEnv L;
+        inst_local_ray(c, (int)(p - c->nt - c->ns - c->nc), E->ro, E->rd, E->tmin, &L);
+        return tree_closest(&L.b->tree, L.ro, L.rd, E->tmin, tbest, blas_test, &L, t) >= 0;
+    }
+    *t = h.t;
+    return 1;
+}
+
+static int world_any(const void* env, int p, double seg, double* t) {
+    const RayEnv* E = (const RayEnv*)env;
+    const fto_ctx* c = E->c;
+    if (p >= c->nt + c->ns + c->nc) {
+        RayEnv L;
+        inst_local_ray(c, (int)(p - c->nt - c->ns - c->nc), E->ro, E->rd, E->tmin, &L);
+        return tree_any(&L.b->tree, L.ro, L.rd, E->tmin, seg, blas_test, &L);
+    }
+    return world_test(env, p, seg, t);
+}
+
+/* Scene::closestHit (scene.h:2194-2242): nearest accepted primitive, returns prim or -1.
+ * For an instance, hit->sub is the BLAS triangle and the hit is mapped to the world like
+ * Scene::instanceHitToWorld (scene.h:2107-2133). */
+static int closest_hit(const fto_ctx* c, V3 ro, V3 rd, double tmin, Hit* hit) {
+    hit->valid = 0; hit->t = DBL_MAX; hit->prim = -1; hit->sub = -1;
+    RayEnv E;
+    E.c = c; E.b = NULL; E.ro = ro; E.rd = rd; E.sh = make_shear(rd); E.cr = make_curve_ray(rd); E.tmin = tmin;
+    double t;
+    int bestp = tree_closest(&c->world, ro, rd, tmin, DBL_MAX, world_test, &E, &t);
+    if (bestp < 0) return -1;
+    if (bestp < c->nt) intersect_tri(&E.sh, ro, rd, &c->tris[bestp], tmin, DBL_MAX, hit);
+    else if (bestp < c->nt + c->ns)
+        intersect_sphere(ro, rd, &c->sph[(bestp - c->nt) * 4], c->sph_mat[bestp - c->nt], tmin, DBL_MAX, hit);
+    else if (bestp < c->nt + c->ns + c->nc)
+        intersect_curve(&E.cr, ro, rd, &c->crv[bestp - c->nt - c->ns], tmin, DBL_MAX, hit);
+    else {
+        int ii = (int)(bestp - c->nt - c->ns - c->nc);
+        const Inst* in = &c->inst[ii];
+        RayEnv L;
+        inst_local_ray(c, ii, ro, rd, tmin, &L);
+        double tl;
+        int tri = tree_closest(&L.b->tree, L.ro, L.rd, tmin, DBL_MAX, blas_test, &L, &tl);
+        Hit lh;
+        intersect_tri(&L.sh, L.ro, L.rd, &L.b->tris[tri], tmin, DBL_MAX, &lh);
+        lh.p = vadd(ro, vmul(rd, lh.t));
+        V3 wn = vnorm(aff_apply_normal(&in->to_local, lh.n));
+        V3 wng = vnorm(aff_apply_normal(&in->to_local, lh.ng));
+        lh.ng = wng;
+        lh.n = (vdot(rd, wn) < 0.0) ? wn : vneg(wn);
+        if (in->mat_override >= 0) lh.mat = in->mat_override;
+        *hit = lh;
+        hit->sub = tri;
+    }
+    hit->prim = bestp;
     return bestp;
 }
 
 /* Scene::occluded (scene.h:2249-2271): any primitive with t in [tmin, maxDist-tmin) */
 static int occluded(const fto_ctx* c, V3 o, V3 d, double max_dist, double tmin) {
     double seg = max_dist - tmin;
-    if (c->n_nodes == 0) return 0;
-    Shear sh = make_shear(d);
-    CurveRay cr = make_curve_ray(d);
-    V3 inv = v3(1.0 / d.x, 1.0 / d.y, 1.0 / d.z);
-    double te;
-    if (!box_hit(&c->nodes[0], o, inv, tmin, seg, &te)) return 0;
-    int stack[128]; int sp = 0; stack[sp++] = 0;
-    while (sp) {
-        const Node* n = &c->nodes[stack[--sp]];
-        if (n->count > 0) {
-            for (int i = 0; i < n->count; ++i)
-                if (prim_test(c, c->order[n->first + i], &sh, &cr, o, d, tmin, seg, NULL, NULL)) return 1;
-        } else {
-            if (sp + 2 > 128) { fail("oracle BVH stack overflow"); return 0; }
-            if (box_hit(&c->nodes[n->left], o, inv, tmin, seg, &te)) stack[sp++] = n->left;
-            if (box_hit(&c->nodes[n->right], o, inv, tmin, seg, &te)) stack[sp++] = n->right;
-        }
-    }
-    return 0;
+    RayEnv E;
+    E.c = c; E.b = NULL; E.ro = o; E.rd = d; E.sh = make_shear(d); E.cr = make_curve_ray(d); E.tmin = tmin;
+    return tree_any(&c->world, o, d, tmin, seg, world_any, &E);
 }
 
 int fto_closest_hit(const fto_ctx* c, const double o[3], const double d[3], double tmin,
@@ -1016,6 +1187,7 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
         T->rays++;
         int prim = closest_hit(c, ro, rd, 1e-6, &h);
         hash = fnv_i32(hash, prim);
+        if (prim >= c->nt + c->ns + c->nc) hash = fnv_i32(hash, h.sub);   /* BLAS triangle */
         if (nh < 8 && log) log->prims[nh] = prim;
         ++nh;
         double d_surf = h.valid ? h.t : 1e30;
@@ -1139,12 +1311,29 @@ done:
 void fto_release(fto_ctx* c) {
     if (!c) return;
     free(c->spec); free(c->tw); free(c->tv); free(c->mats); free(c->tris); free(c->sph);
-    free(c->sph_mat); free(c->crv); free(c->nodes); free(c->order); free(c->emit);
+    free(c->sph_mat); free(c->crv); free(c->world.nodes); free(c->world.order); free(c->emit);
     free(c->cdf_store); free(c->emitter_cdf); free(c->med);
+    for (int b = 0; b < c->n_blas; ++b) {
+        free(c->blas[b].tris); free(c->blas[b].tree.nodes); free(c->blas[b].tree.order);
+    }
+    free(c->blas); free(c->inst);
     free(c);
 }
 
 static V3 rd3(const double* p) { return v3(p[0], p[1], p[2]); }
+
+/* Tri::finalize (geometry.h:51-55): geometric normal; missing shading normals take it */
+static void finalize_tri(Tri* t, const double* v, const double* n, int mat) {
+    t->v0 = rd3(v); t->v1 = rd3(v + 3); t->v2 = rd3(v + 6);
+    t->mat = mat;
+    t->gn = vnorm(vcross(vsub(t->v1, t->v0), vsub(t->v2, t->v0)));
+    V3 z = v3(0, 0, 0);
+    t->n0 = z; t->n1 = z; t->n2 = z;
+    if (n) { t->n0 = rd3(n); t->n1 = rd3(n + 3); t->n2 = rd3(n + 6); }
+    if (vdot(t->n0, t->n0) < 1e-12) t->n0 = t->gn;
+    if (vdot(t->n1, t->n1) < 1e-12) t->n1 = t->gn;
+    if (vdot(t->n2, t->n2) < 1e-12) t->n2 = t->gn;
+}
 
 fto_ctx* fto_prepare(const ftb_scene_desc* d) {
     if (!d) { fail("null desc"); return NULL; }
@@ -1168,21 +1357,12 @@ fto_ctx* fto_prepare(const ftb_scene_desc* d) {
     memcpy(c->mats, d->mats, sizeof(ftb_material) * (size_t)d->n_mats);
     /* triangles: Tri::finalize (geometry.h:51-55) */
     c->nt = d->n_tris; c->ns = d->n_spheres; c->nc = d->n_curves;
-    c->np = c->nt + c->ns + c->nc;
     c->tris = (Tri*)malloc(sizeof(Tri) * (size_t)(c->nt > 0 ? c->nt : 1));
     for (int64_t i = 0; i < c->nt; ++i) {
-        Tri* t = &c->tris[i];
-        const double* v = d->tri_v + 9 * i;
-        t->v0 = rd3(v); t->v1 = rd3(v + 3); t->v2 = rd3(v + 6);
-        t->mat = d->tri_mat[i];
-        t->gn = vnorm(vcross(vsub(t->v1, t->v0), vsub(t->v2, t->v0)));
-        V3 z = v3(0, 0, 0);
-        t->n0 = z; t->n1 = z; t->n2 = z;
-        if (d->tri_n) { const double* n = d->tri_n + 9 * i; t->n0 = rd3(n); t->n1 = rd3(n + 3); t->n2 = rd3(n + 6); }
-        if (vdot(t->n0, t->n0) < 1e-12) t->n0 = t->gn;
-        if (vdot(t->n1, t->n1) < 1e-12) t->n1 = t->gn;
-        if (vdot(t->n2, t->n2) < 1e-12) t->n2 = t->gn;
-        if (t->mat < 0 || t->mat >= d->n_mats) { fail("tri material out of range"); fto_release(c); return NULL; }
+        finalize_tri(&c->tris[i], d->tri_v + 9 * i, d->tri_n ? d->tri_n + 9 * i : NULL, d->tri_mat[i]);
+        if (d->tri_mat[i] < 0 || d->tri_mat[i] >= d->n_mats) {
+            fail("tri material out of range"); fto_release(c); return NULL;
+        }
     }
     c->sph = (double*)malloc(sizeof(double) * 4 * (size_t)(c->ns > 0 ? c->ns : 1));
     c->sph_mat = (int*)malloc(sizeof(int) * (size_t)(c->ns > 0 ? c->ns : 1));
@@ -1196,7 +1376,49 @@ fto_ctx* fto_prepare(const ftb_scene_desc* d) {
         k->u0 = (double)(float)s[8]; k->u1 = (double)(float)s[9];
         k->mat = d->curve_mat[i];
     }
-    /* BVH */
+    /* BLAS assets (scene.h:996-1015) and instances (scene.h:1035-1063) */
+    c->n_blas = d->n_blas > 0 ? d->n_blas : 0;
+    c->ni = d->n_instances > 0 ? d->n_instances : 0;
+    c->blas = (Blas*)calloc((size_t)(c->n_blas > 0 ? c->n_blas : 1), sizeof(Blas));
+    c->inst = (Inst*)calloc((size_t)(c->ni > 0 ? c->ni : 1), sizeof(Inst));
+    for (int b = 0; b < c->n_blas; ++b) {
+        const ftb_blas_desc* bd = &d->blas[b];
+        Blas* B = &c->blas[b];
+        B->nt = bd->n_tris;
+        B->tris = (Tri*)malloc(sizeof(Tri) * (size_t)(B->nt > 0 ? B->nt : 1));
+        B->lo = v3(DBL_MAX, DBL_MAX, DBL_MAX);
+        B->hi = v3(-DBL_MAX, -DBL_MAX, -DBL_MAX);
+        BPrim* bp = (BPrim*)malloc(sizeof(BPrim) * (size_t)(B->nt > 0 ? B->nt : 1));
+        for (int64_t i = 0; i < B->nt; ++i) {
+            if (bd->tri_mat[i] < 0 || bd->tri_mat[i] >= d->n_mats) {
+                fail("blas tri material out of range"); free(bp); fto_release(c); return NULL;
+            }
+            finalize_tri(&B->tris[i], bd->tri_v + 9 * i, bd->tri_n ? bd->tri_n + 9 * i : NULL, bd->tri_mat[i]);
+            V3 lo, hi;
+            tri_box(&B->tris[i], &lo, &hi);
+            lo = v3(lo.x - 1e-6, lo.y - 1e-6, lo.z - 1e-6);
+            hi = v3(hi.x + 1e-6, hi.y + 1e-6, hi.z + 1e-6);
+            B->lo = v3(fmin(B->lo.x, lo.x), fmin(B->lo.y, lo.y), fmin(B->lo.z, lo.z));
+            B->hi = v3(fmax(B->hi.x, hi.x), fmax(B->hi.y, hi.y), fmax(B->hi.z, hi.z));
+            bp[i].lo = lo; bp[i].hi = hi; bp[i].c = vmul(vadd(lo, hi), 0.5); bp[i].idx = (int)i;
+        }
+        build_tree(&B->tree, bp, (int)B->nt);
+        free(bp);
+    }
+    for (int64_t k = 0; k < c->ni; ++k) {
+        const ftb_instance* id = &d->instances[k];
+        if (id->blas < 0 || id->blas >= c->n_blas || id->mat_override >= d->n_mats) {
+            fail("instance out of range"); fto_release(c); return NULL;
+        }
+        Inst* in = &c->inst[k];
+        in->blas = id->blas;
+        in->mat_override = id->mat_override;
+        memcpy(in->to_world.m, id->to_world, sizeof(double) * 9);
+        in->to_world.t = v3(id->to_world[9], id->to_world[10], id->to_world[11]);
+        in->to_local = aff_inverse(&in->to_world);
+    }
+    c->np = c->nt + c->ns + c->nc + c->ni;
+    /* world tree over tris, spheres, curves, instances */
     if (c->np > 0) {
         BPrim* bp = (BPrim*)malloc(sizeof(BPrim) * (size_t)c->np);
         for (int64_t i = 0; i < c->np; ++i) {
@@ -1204,11 +1426,7 @@ fto_ctx* fto_prepare(const ftb_scene_desc* d) {
             bp[i].c = vmul(vadd(bp[i].lo, bp[i].hi), 0.5);
             bp[i].idx = (int)i;
         }
-        c->nodes = (Node*)malloc(sizeof(Node) * (size_t)(2 * c->np + 1));
-        c->n_nodes = 0;
-        build_rec(c, bp, 0, (int)c->np);
-        c->order = (int*)malloc(sizeof(int) * (size_t)c->np);
-        for (int64_t i = 0; i < c->np; ++i) c->order[i] = bp[i].idx;
+        build_tree(&c->world, bp, (int)c->np);
         free(bp);
     }
     /* emitters + selection CDF (scene.h:1491-1513) */

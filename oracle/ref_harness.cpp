@@ -5,8 +5,8 @@
 // This file contains no reference code.  It is compiled against the reference's headers
 // where they lie (oracle/Makefile passes -I <reference>/src) and drives the reference's
 // public C++ API: it builds a `Scene` from the same POD description the C ABI takes
-// (Tri / Sphere / CurveSeg / Material / addAreaLight / addSphereLight / Medium, then
-// Scene::build, scene.h:1907), bakes the `Camera` fields, and runs
+// (Tri / Sphere / CurveSeg / Blas / MeshInstance / Material / addAreaLight /
+// addSphereLight / Medium, then Scene::build, scene.h:1907), bakes the `Camera` fields, and runs
 // Renderer::tracePhoton (render.h:1811) photon by photon with the reference's per-photon
 // seeding (seedUnit, main.cpp:11326) and std::thread banding (main.cpp:11305-11340).
 #include "render.h"
@@ -86,6 +86,32 @@ void* ftr_prepare(const ftb_scene_desc* d) {
         cs.p0 = v3(c); cs.p1 = v3(c + 3); cs.r0 = c[6]; cs.r1 = c[7];
         cs.u0 = (float)c[8]; cs.u1 = (float)c[9]; cs.matId = d->curve_mat[i];
         s.curveSegs.push_back(cs);
+    }
+    // shared BLAS assets and their placements (scene.h:996-1063)
+    for (int b = 0; b < d->n_blas; ++b) {
+        const ftb_blas_desc& bd = d->blas[b];
+        Blas bl;
+        for (int64_t i = 0; i < bd.n_tris; ++i) {
+            const double* v = bd.tri_v + 9 * i;
+            Tri t{v3(v), v3(v + 3), v3(v + 6), bd.tri_mat[i], -1, {}};
+            if (bd.tri_n) {
+                const double* n = bd.tri_n + 9 * i;
+                t.n0 = v3(n); t.n1 = v3(n + 3); t.n2 = v3(n + 6);
+            }
+            bl.tris.push_back(t);
+        }
+        s.blasList.push_back(std::move(bl));
+    }
+    for (int64_t k = 0; k < d->n_instances; ++k) {
+        const ftb_instance& in = d->instances[k];
+        MeshInstance mi;
+        mi.blasId = in.blas;
+        mi.matOverride = in.mat_override;
+        Affine xf;
+        for (int j = 0; j < 9; ++j) xf.m[j] = in.to_world[j];
+        xf.t = Vec3{in.to_world[9], in.to_world[10], in.to_world[11]};
+        mi.setToWorld(xf);
+        s.instances.push_back(mi);
     }
     for (int i = 0; i < d->n_emitters; ++i) {
         const ftb_emitter& e = d->emitters[i];

@@ -31,6 +31,30 @@ def make_materials(L):
     return sb.build(L)
 
 
+def make_instances(L):
+    """Instanced meshes (Blas / MeshInstance): a smooth-shaded dielectric blob placed twice
+    (a rotation with non-uniform scale, and a scaled copy with a glossy material override)
+    and a diffuse box asset rotated about y, beside the world triangles of the box."""
+    sb = scenes.SceneBuilder()
+    scenes.cornell_box(sb, boxes=False)
+    glass = sb.material(abi.MAT_DIELECTRIC, ior=sb.cauchy(1.5, 0.0042), roughness=0.0)
+    v, f = scenes.icosphere(2)
+    n = scenes.value_noise3(v, 5)
+    r = 0.25 + 0.03 * (2.0 * n - 1.0)
+    blob = sb.blas((v * r[:, None])[f].reshape(-1, 9), glass, normals=v[f].reshape(-1, 9))
+    box_sb = scenes.SceneBuilder()
+    white = sb.diffuse(sb.const(0.7))
+    box_sb.box((0.0, 0.0), (0.4, 0.4), 0.6, 0.0, 0, y0=-0.3)
+    box = sb.blas(np.concatenate(box_sb.tri_v), white)
+    xf = scenes.affine((1.0, 1.0, 0.0), 30.0, (0.6, 0.55, 1.0))
+    xf[:9] = (xf[:9].reshape(3, 3) @ np.diag([1.2, 0.8, 1.0])).reshape(9)
+    sb.instance(blob, xf)
+    glossy = sb.material(abi.MAT_GLOSSY, reflect=sb.const(0.8), roughness=0.25)
+    sb.instance(blob, scenes.affine((0.3, -1.0, 0.2), 75.0, (1.45, 0.45, 0.7), scale=0.8), mat_override=glossy)
+    sb.instance(box, scenes.affine((0.0, 1.0, 0.0), 20.0, (1.3, 0.31, 1.5)))
+    return sb.build(L)
+
+
 CASES = {
     # name: (builder, res, photons, max_bounce, seed_base)
     "cornell": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 0),
@@ -38,6 +62,7 @@ CASES = {
     "glass": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 0),
     "fog_strands": (lambda L: scenes.make_fog_strands(L, n_strands=500), 32, 8192, 32, 0),
     "materials": (make_materials, 32, 8192, 16, 7),
+    "instances": (make_instances, 32, 8192, 16, 11),
 }
 
 
@@ -55,4 +80,9 @@ def scene_hash(d):
     for arr, n in ((d.mats, d.n_mats), (d.spectra, d.n_spectra), (d.emitters, d.n_emitters),
                    (d.media, d.n_media)):
         h.update(C.string_at(C.addressof(arr), n * C.sizeof(arr._type_)))
+    for tv, tn, tm, _ in d.blas_arrays:
+        for a in (tv, tm) + (() if tn is None else (tn,)):
+            h.update(np.ascontiguousarray(a).tobytes())
+    if d.n_instances:
+        h.update(C.string_at(C.addressof(d.instances), d.n_instances * C.sizeof(abi.Instance)))
     return h.hexdigest()

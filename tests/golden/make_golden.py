@@ -2,7 +2,7 @@
 
 Run where the reference sources are available (they are read only at build time):
     make -C oracle            # builds oracle/_ref/libftref.so from the reference headers
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   # all cases when none is named
 
 For every case in tests/cases.py it stores, from Renderer::tracePhoton run single-threaded
 with the reference's per-photon seeding: the energy report, the film (XYZ sums and hits),
@@ -27,7 +27,10 @@ import cases  # noqa: E402
 def main():
     L = lib.load()
     R = Reference()
+    only = set(sys.argv[1:])
     for name, (mk, res, n, mb, seed) in cases.CASES.items():
+        if only and name not in only:
+            continue
         d = mk(L)
         cam = cases.camera(L, res)
         r = R.trace(d, cam, n, seed_base=seed, max_bounce=mb, per_photon=True)
@@ -36,6 +39,8 @@ def main():
             energy=r["energy"], xyz=r["xyz"], hits=r["hits"], rays=r["rays"].astype(np.int32),
             fate=r["fate"].astype(np.int8), beta=r["beta"], res=res, n=n, max_bounce=mb, seed_base=seed)
         print(name, r["energy"])
+    if only and "streams" not in only:
+        return
     ks = np.array([0, 1, 2, 3, 1000, 123456789, 2**40 + 5, 2**63 - 1], dtype=np.uint64)
     uni = np.stack([R.uniforms(int(k), 16) for k in ks])
     cam = R.look_at((1.0, 1.0, 5.4), (1.0, 1.0, 1.0), (0.0, 1.0, 0.0), 40.0, 256, 192)

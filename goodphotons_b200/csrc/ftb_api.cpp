@@ -246,6 +246,55 @@ struct ftb_blas {
     std::shared_ptr<BlasDev> p;
 };
 
+// ---- per-device render engine ------------------------------------------------------------
+namespace {
+// The wave buffers, streams and scratch every render on one device uses.  Shared by all
+// scenes of the device (a scene, its clones, the scenes of a batch), so their number does
+// not multiply the ~300 B per wave slot; renders on a device serialize on `mu`.
+struct Engine {
+    int device = 0;
+    std::mutex mu;
+    cudaStream_t streams[2] = {nullptr, nullptr};
+    ftb::Wave waves[2]{};
+    JobStage stage[2];
+    int32_t wave_W = 0;
+    bool wave_log = false;
+    int64_t* film = nullptr;          // film of the host-film entry points
+    size_t film_words = 0;
+    unsigned long long* tally = nullptr;
+    int32_t* status = nullptr;
+    unsigned long long* batch_tally = nullptr;   // 8 words per job of the last batch
+    size_t batch_cap = 0;
+    ~Engine() {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(device);
+        for (auto& w : waves) ftb::wave_free(w);
+        for (auto s : streams) if (s) cudaStreamDestroy(s);
+        if (film) cudaFree(film);
+        if (tally) cudaFree(tally);
+        if (status) cudaFree(status);
+        if (batch_tally) cudaFree(batch_tally);
+        cudaSetDevice(cur);
+    }
+};
+
+std::mutex g_engine_mu;
+std::weak_ptr<Engine> g_engines[256];
+
+// The device's engine, created on first use; it lives while any scene holds it.
+std::shared_ptr<Engine> engine_for(int device) {
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    auto e = g_engines[device].lock();
+    if (!e) {
+        e = std::make_shared<Engine>();
+        e->device = device;
+        g_engines[device] = e;
+    }
+    return e;
+}
+}  // namespace
+
 // ---- scene object ----------------------------------------------------------------------
 struct ftb_scene {
     int device = 0;
@@ -259,33 +308,15 @@ struct ftb_scene {
     DevInst* d_inst = nullptr;
     double power = 0.0;
     uint64_t scene_bytes = 0;
-    std::mutex mu;   // one render at a time per scene
-    // cached render resources
-    cudaStream_t streams[2] = {nullptr, nullptr};
-    ftb::Wave waves[2]{};
-    JobStage stage[2];
-    int32_t wave_W = 0;
-    bool wave_log = false;
-    int64_t* film = nullptr;
-    size_t film_words = 0;
-    unsigned long long* tally = nullptr;
-    int32_t* status = nullptr;
+    std::shared_ptr<Engine> eng;                   // render resources of the device
     int32_t prof_mode = 0;
     ProfSink* prof = nullptr;
-    unsigned long long* batch_tally = nullptr;   // 8 words per job of the last batch
-    size_t batch_cap = 0;
     unsigned long long* stats = nullptr;   // device counters for profiling mode 2
     ~ftb_scene() {
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(device);
-        for (auto& w : waves) ftb::wave_free(w);
-        for (auto s : streams) if (s) cudaStreamDestroy(s);
-        if (film) cudaFree(film);
-        if (tally) cudaFree(tally);
-        if (status) cudaFree(status);
         if (stats) cudaFree(stats);
-        if (batch_tally) cudaFree(batch_tally);
         delete prof;
         cudaSetDevice(cur);
     }
@@ -498,30 +529,30 @@ DevCam dev_cam(const ftb_camera* c) {
 }
 
 ftb_status ensure_waves(ftb_scene* s, int32_t W, bool log) {
-    if (s->wave_W >= W && s->wave_log == log && s->waves[0].block) return FTB_OK;
-    for (auto& w : s->waves) ftb::wave_free(w);
-    s->wave_W = 0;
-    for (auto& w : s->waves) {
+    if (s->eng->wave_W >= W && s->eng->wave_log == log && s->eng->waves[0].block) return FTB_OK;
+    for (auto& w : s->eng->waves) ftb::wave_free(w);
+    s->eng->wave_W = 0;
+    for (auto& w : s->eng->waves) {
         cudaError_t e = ftb::wave_alloc(w, W, log);
         if (e != cudaSuccess) return cuda_fail(e, "wave allocation");
     }
-    for (auto& st : s->streams)
+    for (auto& st : s->eng->streams)
         if (!st) CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream create");
-    for (auto& sg : s->stage) CK(sg.init(), "job staging");
-    s->wave_W = W;
-    s->wave_log = log;
+    for (auto& sg : s->eng->stage) CK(sg.init(), "job staging");
+    s->eng->wave_W = W;
+    s->eng->wave_log = log;
     return FTB_OK;
 }
 
 ftb_status ensure_frame(ftb_scene* s, size_t words) {
-    if (!s->tally) CK(cudaMalloc(&s->tally, 8 * sizeof(unsigned long long)), "tally alloc");
-    if (!s->status) CK(cudaMalloc(&s->status, 64), "status alloc");
-    if (s->film_words < words) {
-        if (s->film) cudaFree(s->film);
-        s->film = nullptr;
-        s->film_words = 0;
-        CK(cudaMalloc(&s->film, words * sizeof(int64_t)), "film alloc");
-        s->film_words = words;
+    if (!s->eng->tally) CK(cudaMalloc(&s->eng->tally, 8 * sizeof(unsigned long long)), "tally alloc");
+    if (!s->eng->status) CK(cudaMalloc(&s->eng->status, 64), "status alloc");
+    if (s->eng->film_words < words) {
+        if (s->eng->film) cudaFree(s->eng->film);
+        s->eng->film = nullptr;
+        s->eng->film_words = 0;
+        CK(cudaMalloc(&s->eng->film, words * sizeof(int64_t)), "film alloc");
+        s->eng->film_words = words;
     }
     return FTB_OK;
 }
@@ -559,14 +590,14 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
     int32_t W = pick_wave(total);
     ftb_status st = ensure_waves(s, W, log);
     if (st != FTB_OK) return st;
-    W = s->wave_W;
+    W = s->eng->wave_W;
     ftb::Frame f;
     f.stats = s->prof_mode == 2 ? s->stats : nullptr;
-    f.status = s->status;
+    f.status = s->eng->status;
     cudaEvent_t ready = nullptr;
     CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
     CK(cudaEventRecord(ready, user_stream), "event record");
-    for (auto st2 : s->streams) CK(cudaStreamWaitEvent(st2, ready, 0), "stream wait");
+    for (auto st2 : s->eng->streams) CK(cudaStreamWaitEvent(st2, ready, 0), "stream wait");
     size_t j = 0;
     int64_t done_in_job = 0;
     int k = 0;
@@ -591,18 +622,18 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
             if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
         }
         if (table.empty()) break;
-        ftb::Wave& w = s->waves[k & 1];
-        cudaStream_t ws = s->streams[k & 1];
+        ftb::Wave& w = s->eng->waves[k & 1];
+        cudaStream_t ws = s->eng->streams[k & 1];
         w.logs = d_logs;
         w.log_base = log_base;
-        cudaError_t e = s->stage[k & 1].push(table.data(), (int)table.size(), w.jobs, ws);
+        cudaError_t e = s->eng->stage[k & 1].push(table.data(), (int)table.size(), w.jobs, ws);
         if (e != cudaSuccess) return cuda_fail(e, "job table upload");
         e = ftb::launch_wave(w, w.jobs, (int32_t)table.size(), slots, max_bounce, inst, f, s->sms, ws,
                              s->prof_mode ? s->prof : nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         ++k;
     }
-    for (auto st2 : s->streams) {
+    for (auto st2 : s->eng->streams) {
         CK(cudaEventRecord(ready, st2), "event record");
         CK(cudaStreamWaitEvent(user_stream, ready, 0), "stream wait");
     }
@@ -620,7 +651,7 @@ ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t 
 
 ftb_status read_status(ftb_scene* s) {
     int32_t stv = 0;
-    CK(cudaMemcpy(&stv, s->status, 4, cudaMemcpyDeviceToHost), "status readback");
+    CK(cudaMemcpy(&stv, s->eng->status, 4, cudaMemcpyDeviceToHost), "status readback");
     if (stv) {
         std::string m = "device reported:";
         if (stv & ftb::ST_STACK_OVERFLOW) m += " traversal stack overflow;";
@@ -775,6 +806,7 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     s->device = device;
     s->tables = std::make_shared<DevBlock>();
     s->tables->device = device;
+    s->eng = engine_for(device);
     {
         cudaDeviceProp p;
         if (cudaGetDeviceProperties(&p, device) == cudaSuccess) s->sms = p.multiProcessorCount;
@@ -1021,7 +1053,7 @@ ftb_status ftb_scene_set_instance_transforms(ftb_scene* s, const double* to_worl
     if (!s) return fail(FTB_ERR_INVALID, "null scene");
     if (n < 0 || n > s->dev.n_inst || (n > 0 && !to_world)) return fail(FTB_ERR_INVALID, "bad instance range");
     if (n == 0) return FTB_OK;
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     return set_transforms(s, to_world, n);
 }
 
@@ -1035,6 +1067,7 @@ ftb_status ftb_scene_clone_instances(const ftb_scene* src, const double* to_worl
     c->sms = src->sms;
     c->dev = src->dev;
     c->tables = src->tables;
+    c->eng = src->eng;
     c->blas = src->blas;
     c->tlas = src->tlas;
     c->power = src->power;
@@ -1076,15 +1109,15 @@ ftb_status ftb_render_forward_device(ftb_scene* s, const ftb_camera* cam, const 
     ftb_status st = check_params(s, cam, p);
     if (st != FTB_OK) return st;
     if (!d_film) return fail(FTB_ERR_INVALID, "null film");
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     DeviceGuard guard(s->device);
     int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
     st = ensure_frame(s, 0);
     if (st != FTB_OK) return st;
     cudaStream_t us = (cudaStream_t)stream;
-    CK(cudaMemsetAsync(s->tally, 0, 8 * sizeof(unsigned long long), us), "memset");
-    CK(cudaMemsetAsync(s->status, 0, 64, us), "memset");
-    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, d_film, s->tally, nullptr, us);
+    CK(cudaMemsetAsync(s->eng->tally, 0, 8 * sizeof(unsigned long long), us), "memset");
+    CK(cudaMemsetAsync(s->eng->status, 0, 64, us), "memset");
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, d_film, s->eng->tally, nullptr, us);
     if (st != FTB_OK) return st;
     if (info) { info->frac_bits = frac; info->scale = s->power * std::ldexp(1.0, -frac); info->power_ref = s->power; }
     if (energy) {
@@ -1092,7 +1125,7 @@ ftb_status ftb_render_forward_device(ftb_scene* s, const ftb_camera* cam, const 
         st = read_status(s);
         if (st != FTB_OK) return st;
         unsigned long long fx[5];
-        CK(cudaMemcpy(fx, s->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally readback");
+        CK(cudaMemcpy(fx, s->eng->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally readback");
         tally_to_energy(fx, s->power, energy, true);
     }
     return FTB_OK;
@@ -1103,25 +1136,25 @@ ftb_status ftb_render_forward(ftb_scene* s, const ftb_camera* cam, const ftb_ren
     ftb_status st = check_params(s, cam, p);
     if (st != FTB_OK) return st;
     if (!film) return fail(FTB_ERR_INVALID, "null film");
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     DeviceGuard guard(s->device);
     size_t words = (size_t)cam->res_x * cam->res_y * 4;
     int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
     st = ensure_frame(s, words);
     if (st != FTB_OK) return st;
-    CK(cudaMemset(s->film, 0, words * sizeof(int64_t)), "memset film");
-    CK(cudaMemset(s->tally, 0, 8 * sizeof(unsigned long long)), "memset tally");
-    CK(cudaMemset(s->status, 0, 64), "memset status");
-    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->film, s->tally, nullptr, nullptr);
+    CK(cudaMemset(s->eng->film, 0, words * sizeof(int64_t)), "memset film");
+    CK(cudaMemset(s->eng->tally, 0, 8 * sizeof(unsigned long long)), "memset tally");
+    CK(cudaMemset(s->eng->status, 0, 64), "memset status");
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, nullptr, nullptr);
     if (st != FTB_OK) return st;
     CK(cudaDeviceSynchronize(), "render");
     st = read_status(s);
     if (st != FTB_OK) return st;
-    CK(cudaMemcpy(film, s->film, words * sizeof(int64_t), cudaMemcpyDeviceToHost), "film download");
+    CK(cudaMemcpy(film, s->eng->film, words * sizeof(int64_t), cudaMemcpyDeviceToHost), "film download");
     if (info) { info->frac_bits = frac; info->scale = s->power * std::ldexp(1.0, -frac); info->power_ref = s->power; }
     if (energy) {
         unsigned long long fx[5];
-        CK(cudaMemcpy(fx, s->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally readback");
+        CK(cudaMemcpy(fx, s->eng->tally, sizeof fx, cudaMemcpyDeviceToHost), "tally readback");
         tally_to_energy(fx, s->power, energy, true);
     }
     return FTB_OK;
@@ -1140,27 +1173,27 @@ ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n, ftb_film_info* infos
         ftb_status st = check_params(b.scene, &b.cam, &p);
         if (st != FTB_OK) return fail(st, "job " + std::to_string(j) + ": " + g_err);
     }
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     DeviceGuard guard(s->device);
     ftb_status st = ensure_frame(s, 0);
     if (st != FTB_OK) return st;
-    if (s->batch_cap < (size_t)n) {
-        if (s->batch_tally) cudaFree(s->batch_tally);
-        s->batch_tally = nullptr;
-        s->batch_cap = 0;
-        CK(cudaMalloc(&s->batch_tally, sizeof(unsigned long long) * 8 * (size_t)n), "batch tallies");
-        s->batch_cap = (size_t)n;
+    if (s->eng->batch_cap < (size_t)n) {
+        if (s->eng->batch_tally) cudaFree(s->eng->batch_tally);
+        s->eng->batch_tally = nullptr;
+        s->eng->batch_cap = 0;
+        CK(cudaMalloc(&s->eng->batch_tally, sizeof(unsigned long long) * 8 * (size_t)n), "batch tallies");
+        s->eng->batch_cap = (size_t)n;
     }
     cudaStream_t us = (cudaStream_t)stream;
-    CK(cudaMemsetAsync(s->batch_tally, 0, sizeof(unsigned long long) * 8 * (size_t)n, us), "memset");
-    CK(cudaMemsetAsync(s->status, 0, 64, us), "memset");
+    CK(cudaMemsetAsync(s->eng->batch_tally, 0, sizeof(unsigned long long) * 8 * (size_t)n, us), "memset");
+    CK(cudaMemsetAsync(s->eng->status, 0, 64, us), "memset");
     std::vector<ftb::DevJob> base;
     std::vector<int64_t> count;
     std::vector<uint64_t> seed;
     for (int j = 0; j < n; ++j) {
         const ftb_job& b = jobs[j];
         int frac = b.frac_bits > 0 ? b.frac_bits : default_frac_bits(b.n_photons);
-        base.push_back(make_job(b.scene, &b.cam, b.d_film, s->batch_tally + 8 * (size_t)j, frac, b.max_bounce));
+        base.push_back(make_job(b.scene, &b.cam, b.d_film, s->eng->batch_tally + 8 * (size_t)j, frac, b.max_bounce));
         count.push_back(b.n_photons);
         seed.push_back(b.seed_base);
         if (infos) {
@@ -1176,7 +1209,7 @@ ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n, ftb_film_info* infos
         st = read_status(s);
         if (st != FTB_OK) return st;
         std::vector<unsigned long long> fx(8 * (size_t)n);
-        CK(cudaMemcpy(fx.data(), s->batch_tally, fx.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+        CK(cudaMemcpy(fx.data(), s->eng->batch_tally, fx.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
            "tally readback");
         for (int j = 0; j < n; ++j) tally_to_energy(&fx[8 * (size_t)j], jobs[j].scene->power, &energies[j], true);
     }
@@ -1188,7 +1221,7 @@ ftb_status ftb_trace_log(ftb_scene* s, const ftb_camera* cam, const ftb_render_p
     if (st != FTB_OK) return st;
     if (!out) return fail(FTB_ERR_INVALID, "null log buffer");
     if (p->n_photons > ((int64_t)1 << 24)) return fail(FTB_ERR_TOO_LARGE, "ftb_trace_log: at most 2^24 photons per call");
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     DeviceGuard guard(s->device);
     size_t words = (size_t)cam->res_x * cam->res_y * 4;
     int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
@@ -1197,10 +1230,10 @@ ftb_status ftb_trace_log(ftb_scene* s, const ftb_camera* cam, const ftb_render_p
     ftb_photon_log* d_logs = nullptr;
     size_t lb = (size_t)std::max<int64_t>(p->n_photons, 1) * sizeof(ftb_photon_log);
     CK(cudaMalloc(&d_logs, lb), "log alloc");
-    cudaMemset(s->film, 0, words * sizeof(int64_t));
-    cudaMemset(s->tally, 0, 8 * sizeof(unsigned long long));
-    cudaMemset(s->status, 0, 64);
-    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->film, s->tally, d_logs, nullptr);
+    cudaMemset(s->eng->film, 0, words * sizeof(int64_t));
+    cudaMemset(s->eng->tally, 0, 8 * sizeof(unsigned long long));
+    cudaMemset(s->eng->status, 0, 64);
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, d_logs, nullptr);
     if (st == FTB_OK) {
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) st = cuda_fail(e, "trace_log");
@@ -1216,7 +1249,7 @@ ftb_status ftb_trace_log(ftb_scene* s, const ftb_camera* cam, const ftb_render_p
 
 ftb_status ftb_scene_set_profiling(ftb_scene* s, int32_t mode) {
     if (!s || mode < 0 || mode > 2) return fail(FTB_ERR_INVALID, "bad profiling arguments");
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     DeviceGuard guard(s->device);
     if (mode && !s->prof) s->prof = new ProfSink();
     if (mode == 2 && !s->stats) {
@@ -1229,7 +1262,7 @@ ftb_status ftb_scene_set_profiling(ftb_scene* s, int32_t mode) {
 
 ftb_status ftb_scene_profile(ftb_scene* s, ftb_kernel_profile* out, int32_t reset) {
     if (!s || !out) return fail(FTB_ERR_INVALID, "bad arguments");
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     DeviceGuard guard(s->device);
     std::memset(out, 0, sizeof *out);
     if (s->prof) {
@@ -1277,15 +1310,15 @@ ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cam
 ftb_status ftb_session_batch(ftb_session* ss, int64_t n, uint64_t seed_base) {
     if (!ss || n < 0) return fail(FTB_ERR_INVALID, "bad batch arguments");
     ftb_scene* s = ss->scene;
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
     DeviceGuard guard(s->device);
     ftb_status st = ensure_frame(s, 0);
     if (st != FTB_OK) return st;
-    CK(cudaMemset(s->status, 0, 64), "memset status");
+    CK(cudaMemset(s->eng->status, 0, 64), "memset status");
     // Model B connections draw no random numbers (render.h:272-275), so tracing the same
     // photon indices once per camera gives every camera exactly the film a shared pass would.
     for (size_t c = 0; c < ss->cams.size(); ++c) {
-        unsigned long long* tally = (c == 0) ? ss->tally : s->tally;
+        unsigned long long* tally = (c == 0) ? ss->tally : s->eng->tally;
         st = run_photons(s, &ss->cams[c], n, seed_base, ss->max_bounce, ss->frac_bits, ss->films[c], tally, nullptr,
                          nullptr);
         if (st != FTB_OK) return st;

@@ -370,7 +370,7 @@ def main():
         return
 
     import torch
-    from goodphotons_b200 import abi, lib, scenes
+    from goodphotons_b200 import abi, lib, multigpu, scenes
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -414,11 +414,12 @@ def main():
 
     def step(k):
         film.zero_()
-        seed = (k * world + rank) * n
-        sc.render_device(cam, n, film.data_ptr(), seed_base=seed, max_bounce=mb, frac_bits=frac,
-                         stream=stream.cuda_stream)
-        if dist is not None:
-            dist.reduce(film, dst=0, op=dist.ReduceOp.SUM)
+        if dist is None:
+            sc.render_device(cam, n, film.data_ptr(), seed_base=k * n, max_bounce=mb, frac_bits=frac,
+                             stream=stream.cuda_stream)
+        else:   # the frame is n photons per rank; each rank traces its index shard
+            multigpu.render_sharded(sc, cam, n * world, film, seed_base=k * n * world, max_bounce=mb,
+                                    dst=0, stream=stream.cuda_stream)
 
     for w in range(args.warmup):
         step(1000 + w)

@@ -347,13 +347,136 @@ def run_animation(args):
     blas.close()
 
 
+def run_serve(args):
+    """Served stream: Poisson arrivals of mixed jobs on resident scenes through the render
+    server (continuous batching), at 80% of the capacity the server measured on the same job
+    mix; p50/p99 latency, aggregate photons/s, and one-job-at-a-time rendering of a sample
+    of the jobs (resident scenes, and baking each job's scene like a scene load)."""
+    import torch
+    from goodphotons_b200 import lib, scenes, workloads
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    L = lib.load()
+    budget_hi = float(args.serve_budget_log2)
+    probe = workloads.served_jobs(args.jobs, 1.0, seed=0, budget_log2=(20.0, budget_hi))
+    keys = sorted({(j.family, j.size) for j in probe})
+    descs, cache, bake_ms = {}, {}, {}
+    for key in keys:
+        descs[key] = workloads.job_scene(L, *key)
+        t = time.perf_counter()
+        cache[key] = lib.Scene(descs[key], local, L)
+        bake_ms[key] = 1e3 * (time.perf_counter() - t)
+    cams = {}
+
+    def cam(res):
+        if res not in cams:
+            cams[res] = scenes.default_camera(L, res)
+        return cams[res]
+
+    def serve(jobs, paced):
+        srv = lib.Server(device=local, max_active=args.max_active, lib=L)
+        ids, films = [None] * len(jobs), [None] * len(jobs)
+        t0 = time.perf_counter()
+
+        def client():
+            for i, j in enumerate(jobs):
+                if paced:
+                    dt = j.arrival_s - (time.perf_counter() - t0)
+                    if dt > 0:
+                        time.sleep(dt)
+                films[i] = np.empty((j.res, j.res, 4), dtype=np.int64)
+                ids[i] = srv.submit(cache[(j.family, j.size)], cam(j.res), j.photons, seed_base=j.seed_base,
+                                    max_bounce=j.max_bounce, host_film=films[i])
+        th = threading.Thread(target=client)
+        th.start()
+        res = []
+        for i in range(len(jobs)):
+            while ids[i] is None:
+                time.sleep(0.0005)
+            res.append(srv.wait(ids[i]))
+            films[i] = None
+        th.join()
+        st = srv.stats()
+        srv.close()
+        bad = sum(1 for r in res if r.status != 0)
+        makespan = max(r.finish_s for r in res) - min(r.submit_s for r in res)
+        lat = np.array([r.finish_s - r.submit_s for r in res])
+        return {"res": res, "makespan": makespan, "lat": lat, "stats": st, "failed": bad}
+
+    # warm-up, then capacity: the whole mix submitted at once (closed loop)
+    serve(probe[: min(8, len(probe))], paced=False)
+    cap = serve(probe, paced=False)
+    photons = sum(j.photons for j in probe)
+    cap_jobs_s = len(probe) / cap["makespan"]
+    rate = 0.8 * cap_jobs_s
+    jobs = workloads.served_jobs(args.jobs, rate, seed=0, budget_log2=(20.0, budget_hi))
+    with ClockSampler(local) as clocks:
+        run = serve(jobs, paced=True)
+    lat = run["lat"]
+
+    # one job at a time on a sample: resident scenes, then the plain path (bake per job)
+    sample = jobs[: min(args.serve_sample, len(jobs))]
+    t = time.perf_counter()
+    for j in sample:
+        cache[(j.family, j.size)].render(cam(j.res), j.photons, seed_base=j.seed_base, max_bounce=j.max_bounce)
+    seq_s = time.perf_counter() - t
+    plain_s = 0.0
+    for j in sample:
+        t = time.perf_counter()
+        sc = lib.Scene(descs[(j.family, j.size)], local, L)
+        sc.render(cam(j.res), j.photons, seed_base=j.seed_base, max_bounce=j.max_bounce)
+        sc.close()
+        plain_s += time.perf_counter() - t
+    sample_ph = sum(j.photons for j in sample)
+    served_ph_s = sum(j.photons for j in jobs) / run["makespan"]
+    cap_ph_s = photons / cap["makespan"]
+    for s_ in cache.values():
+        s_.close()
+    line = {
+        "metric": "photon paths/s on 1 B200 (served stream)", "value": served_ph_s, "unit": "photon paths/s",
+        "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * run["makespan"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded job stream and scenes)",
+        "config": {"workload": "serve", "jobs": len(jobs), "arrivals": f"Poisson at {rate:.2f} jobs/s "
+                   "(80% of the measured capacity on the same mix)",
+                   "mix": "scene family uniform over cornell / glass / fog_strands; mesh 1k-2M tris log-uniform "
+                          "(glass snapped to icosphere levels, fog to strand counts); resolution 128^2-1024^2 and "
+                          f"photons 2^20-2^{budget_hi:g} log-uniform", "resident_scenes": len(cache),
+                   "scene_bake_ms_total": round(sum(bake_ms.values()), 1), "max_active": args.max_active},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "mean": float(lat.mean()), "max": float(lat.max())},
+        "utilization": round(run["stats"].busy_s / run["makespan"], 4),
+        "failed_jobs": run["failed"],
+        "capacity": {"value": cap_ph_s, "unit": "photon paths/s", "jobs_per_s": cap_jobs_s,
+                     "how": f"the {len(probe)}-job mix submitted at once"},
+        "one_at_a_time": {
+            "sample_jobs": len(sample),
+            "resident": {"value": sample_ph / seq_s, "unit": "photon paths/s", "call": "ftb_render_forward per job"},
+            "plain_bake_per_job": {"value": sample_ph / plain_s, "unit": "photon paths/s",
+                                   "call": "ftb_scene_create + ftb_render_forward + destroy per job"},
+        },
+        "capacity_vs_plain": round(cap_ph_s / (sample_ph / plain_s), 3),
+        "capacity_vs_resident_one_at_a_time": round(cap_ph_s / (sample_ph / seq_s), 3),
+        "e2e": {"value": served_ph_s, "unit": "photon paths/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(j.res * j.res * 32 for j in jobs)),
+                "call": "ftb_server_submit / ftb_server_wait, films to host"},
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="glass", choices=sorted(WORKLOADS) + ["animation"])
+    ap.add_argument("--workload", default="glass", choices=sorted(WORKLOADS) + ["animation", "serve"])
+    ap.add_argument("--jobs", type=int, default=2000, help="serve: jobs in the stream")
+    ap.add_argument("--serve-budget-log2", type=float, default=28.0, help="serve: largest photon budget, log2")
+    ap.add_argument("--serve-sample", type=int, default=40, help="serve: jobs rendered one at a time")
+    ap.add_argument("--max-active", type=int, default=64, help="serve: jobs admitted at once")
     ap.add_argument("--frames", type=int, default=64, help="animation: frames")
     ap.add_argument("--baseline-frames", type=int, default=64, help="animation: frames of the plain baseline")
     ap.add_argument("--level", type=int, default=7)
@@ -367,6 +490,9 @@ def main():
         return
     if args.workload == "animation":
         run_animation(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
         return
 
     import torch

@@ -9,6 +9,7 @@ FTB_OK = 0
 STATUS_NAMES = {
     0: "FTB_OK", 1: "FTB_ERR_INVALID", 2: "FTB_ERR_NO_DEVICE", 3: "FTB_ERR_UNSUPPORTED",
     4: "FTB_ERR_CUDA", 5: "FTB_ERR_OOM", 6: "FTB_ERR_DEVICE_LIMIT", 7: "FTB_ERR_TOO_LARGE",
+    8: "FTB_ERR_TIMEOUT",
 }
 
 SPEC_CONST, SPEC_TABLE, SPEC_CAUCHY, SPEC_SELLMEIER, SPEC_BLACKBODY = 0, 1, 2, 3, 4
@@ -124,13 +125,36 @@ class KernelProfile(C.Structure):
     _fields_ = [("ms", C.c_double * 4), ("launches", C.c_int64 * 4), ("counters", C.c_uint64 * 8)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_active", C.c_int32), ("film_budget", C.c_uint64),
+                ("wave_slots", C.c_int32), ("pad", C.c_int32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("cam", Camera), ("n_photons", C.c_int64),
+                ("seed_base", C.c_uint64), ("max_bounce", C.c_int32), ("frac_bits", C.c_int32),
+                ("host_film", C.POINTER(C.c_int64))]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("pad", C.c_int32), ("info", FilmInfo), ("energy", Energy),
+                ("submit_s", C.c_double), ("admit_s", C.c_double), ("finish_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("queued", C.c_int64), ("active", C.c_int64), ("photons_done", C.c_int64),
+                ("waves", C.c_int64), ("busy_s", C.c_double), ("film_bytes", C.c_uint64)]
+
+
 STRUCTS = {
     "ftb_spectrum": Spectrum, "ftb_material": Material, "ftb_emitter": Emitter,
     "ftb_medium": Medium, "ftb_scene_desc": SceneDesc, "ftb_camera": Camera,
     "ftb_render_params": RenderParams, "ftb_energy": Energy, "ftb_film_info": FilmInfo,
     "ftb_footprint": Footprint, "ftb_photon_log": PhotonLog,
     "ftb_kernel_profile": KernelProfile, "ftb_job": Job, "ftb_blas_desc": BlasDesc,
-    "ftb_instance": Instance,
+    "ftb_instance": Instance, "ftb_server_config": ServerConfig, "ftb_request": Request,
+    "ftb_job_result": JobResult, "ftb_server_stats": ServerStats,
 }
 
 # every entry point declared in include/ftb200.h
@@ -142,6 +166,7 @@ EXPORTS = [
     "ftb_session_hits0", "ftb_session_download", "ftb_session_end", "ftb_trace_log",
     "ftb_scene_set_profiling", "ftb_scene_profile", "ftb_render_forward_noalloc",
     "ftb_render_batch", "ftb_blas_create", "ftb_blas_destroy", "ftb_scene_set_instance_transforms",
-    "ftb_scene_clone_instances",
+    "ftb_scene_clone_instances", "ftb_server_create", "ftb_server_submit", "ftb_server_wait",
+    "ftb_server_get_stats", "ftb_server_destroy",
 ]
 NOALLOC_MAX_PHOTONS = 32768

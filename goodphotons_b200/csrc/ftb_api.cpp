@@ -20,6 +20,7 @@
 
 #include "../../include/ftb200.h"
 #include "bvh_build.h"
+#include "ftb_internal.h"
 #include "ftb_kernels.h"
 #include "ftb_layout.h"
 
@@ -689,9 +690,14 @@ ftb_status check_params(const ftb_scene* s, const ftb_camera* cam, const ftb_ren
 
 }  // namespace
 
-// ---- internal accessors (used by ftb_noalloc.cu) --------------------------------------
+// ---- internal accessors (ftb_internal.h) ------------------------------------------------
 namespace ftb {
 void set_last_error(const std::string& m) { g_err = m; }
+int default_frac_bits(int64_t n) { return ::default_frac_bits(n); }
+DevCam camera_to_dev(const ftb_camera* c) { return dev_cam(c); }
+void energy_from_tally(const unsigned long long* fx, double power, ftb_energy* e) {
+    tally_to_energy(fx, power, e, false);
+}
 
 bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power) {
     if (!s) return false;

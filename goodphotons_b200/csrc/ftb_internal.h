@@ -1,0 +1,22 @@
+// ftb_internal.h -- accessors shared by the library's translation units (not part of the
+// C ABI): the scene's device view, the error text and the fixed-point conventions.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/ftb200.h"
+#include "ftb_layout.h"
+
+namespace ftb {
+// The device view of a scene and where it lives; false for a null scene.
+bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power);
+// The text ftb_last_error() returns (thread-local).
+void set_last_error(const std::string& m);
+// The default film format for an n-photon render: 62 - ceil(log2 n) - 20 in [4, 40].
+int default_frac_bits(int64_t n);
+// The camera as the kernels read it.
+DevCam camera_to_dev(const ftb_camera* c);
+// Five fixed-point tallies (32 fraction bits per unit of `power`) as an energy report.
+void energy_from_tally(const unsigned long long* fx, double power, ftb_energy* e);
+}  // namespace ftb

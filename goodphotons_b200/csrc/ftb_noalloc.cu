@@ -23,13 +23,10 @@
 #include <string>
 
 #include "../../include/ftb200.h"
+#include "ftb_internal.h"
 #include "ftb_kernels.h"
 #include "ftb_layout.h"
 
-namespace ftb {
-bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power);
-void set_last_error(const std::string& m);   // the text ftb_last_error() returns
-}
 
 namespace {
 
@@ -50,12 +47,6 @@ ftb_status na_fail(ftb_status s, const std::string& m) {
     return s;
 }
 
-int default_frac_bits(int64_t n) {   // the same default as the other render entry points
-    int lg = 0;
-    while (lg < 62 && ((int64_t)1 << lg) < n) ++lg;
-    int f = 62 - lg - 20;
-    return f < 4 ? 4 : (f > 40 ? 40 : f);
-}
 
 }  // namespace
 
@@ -99,7 +90,7 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     ftb::wave_carve(w, base, kNoAllocPhotons, false);
     unsigned long long* tally = (unsigned long long*)(base + kWaveBytes);
     int32_t* status = (int32_t*)(base + kWaveBytes + al(8 * sizeof(unsigned long long)));
-    const int frac = p->frac_bits > 0 ? p->frac_bits : default_frac_bits(p->n_photons);
+    const int frac = p->frac_bits > 0 ? p->frac_bits : ftb::default_frac_bits(p->n_photons);
     ftb::Frame f;
     f.stats = nullptr;
     f.status = status;

@@ -77,6 +77,11 @@ def load(path=None):
     _sig(L, "ftb_blas_destroy", st, PS)
     _sig(L, "ftb_scene_set_instance_transforms", st, PS, C.POINTER(C.c_double), C.c_int64)
     _sig(L, "ftb_scene_clone_instances", st, PS, C.POINTER(C.c_double), C.c_int64, C.POINTER(PS))
+    _sig(L, "ftb_server_create", st, C.POINTER(abi.ServerConfig), C.POINTER(PS))
+    _sig(L, "ftb_server_submit", st, PS, C.POINTER(abi.Request), C.POINTER(C.c_uint64))
+    _sig(L, "ftb_server_wait", st, PS, C.c_uint64, C.c_double, C.POINTER(abi.JobResult))
+    _sig(L, "ftb_server_get_stats", st, PS, C.POINTER(abi.ServerStats))
+    _sig(L, "ftb_server_destroy", st, PS)
     _sig(L, "ftb_scene_set_profiling", st, PS, C.c_int32)
     _sig(L, "ftb_scene_profile", st, PS, C.POINTER(abi.KernelProfile), C.c_int32)
     w = _Lib(L)
@@ -260,6 +265,53 @@ class Scene:
         p = abi.RenderParams(n, seed_base, max_bounce, 0)
         self.lib.check(self.lib.L.ftb_trace_log(self.h, C.byref(cam), C.byref(p), logs))
         return logs_to_numpy(logs, n)
+
+
+class Server:
+    """Resident render server with continuous batching (ftb_server_*)."""
+
+    def __init__(self, device=0, max_active=64, film_budget=0, wave_slots=0, lib=None):
+        self.lib = lib or load()
+        cfg = abi.ServerConfig(device, max_active, film_budget, wave_slots, 0)
+        h = C.c_void_p()
+        self.lib.check(self.lib.L.ftb_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._films = {}
+
+    def submit(self, scene, cam, n, seed_base=0, max_bounce=8, frac_bits=0, host_film=None):
+        """Queue a job; host_film (int64 [res_y, res_x, 4], C-contiguous) receives the film."""
+        if host_film is not None:
+            assert host_film.dtype == np.int64 and host_film.flags.c_contiguous
+            assert host_film.size == cam.res_x * cam.res_y * 4
+        r = abi.Request(scene.h.value if hasattr(scene.h, "value") else scene.h, cam, n, seed_base, max_bounce,
+                        frac_bits, host_film.ctypes.data_as(C.POINTER(C.c_int64)) if host_film is not None else None)
+        jid = C.c_uint64()
+        self.lib.check(self.lib.L.ftb_server_submit(self.h, C.byref(r), C.byref(jid)))
+        self._films[jid.value] = host_film   # keep the buffer alive until the job is waited on
+        return jid.value
+
+    def wait(self, job_id, timeout=-1.0):
+        res = abi.JobResult()
+        self.lib.check(self.lib.L.ftb_server_wait(self.h, job_id, float(timeout), C.byref(res)))
+        self._films.pop(job_id, None)
+        return res
+
+    def stats(self):
+        st = abi.ServerStats()
+        self.lib.check(self.lib.L.ftb_server_get_stats(self.h, C.byref(st)))
+        return st
+
+    def close(self):
+        if self.h:
+            self.lib.L.ftb_server_destroy(self.h)
+            self.h = None
+            self._films.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def logs_to_numpy(logs, n):

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FTB_ABI_VERSION 1
+#define FTB_ABI_VERSION 2
 
 typedef enum ftb_status {
     FTB_OK = 0,
@@ -38,7 +38,8 @@ typedef enum ftb_status {
     FTB_ERR_CUDA = 4,         /* a CUDA runtime call failed */
     FTB_ERR_OOM = 5,          /* device allocation failed */
     FTB_ERR_DEVICE_LIMIT = 6, /* a bounded device loop gave up (stack/queue overflow) */
-    FTB_ERR_TOO_LARGE = 7     /* request exceeds a documented maximum */
+    FTB_ERR_TOO_LARGE = 7,    /* request exceeds a documented maximum */
+    FTB_ERR_TIMEOUT = 8       /* a wait ran out of time (the work goes on) */
 } ftb_status;
 
 /* ---- spectra ------------------------------------------------------------------------
@@ -399,6 +400,66 @@ typedef struct ftb_kernel_profile {
 ftb_status ftb_scene_set_profiling(ftb_scene* scene, int32_t mode);
 /* Waits for the recorded events, returns the totals since the last reset. */
 ftb_status ftb_scene_profile(ftb_scene* scene, ftb_kernel_profile* out, int32_t reset);
+
+/* ---- render server (continuous batching; no counterpart in the reference) ------------
+ * A server owns two wave buffers and streams on one device, a scheduler thread and a
+ * completion thread.  Jobs (a resident scene, a camera, a photon range) are submitted from
+ * any thread and admitted in arrival order while their film fits the film budget and a
+ * job slot is free.  The scheduler keeps packing the unscheduled photons of all admitted
+ * jobs into waves -- every job at least a fair share of each wave, the rest shortest
+ * remaining work first -- so a job that arrives while others are on the GPU joins the
+ * next wave and small jobs are not queued behind large ones.  A job's film and energy are
+ * exactly those of ftb_render_forward with the same arguments, whatever shares its waves
+ * (photons are keyed by index and the film is fixed point).  The scenes referenced by
+ * submitted jobs must stay alive until those jobs are done. */
+typedef struct ftb_server ftb_server;
+
+typedef struct ftb_server_config {
+    int32_t device;
+    int32_t max_active;        /* jobs admitted at once, 1..256 (0: 64) */
+    uint64_t film_budget;      /* bytes of device films admitted at once (0: a quarter of the
+                                  free device memory) */
+    int32_t wave_slots;        /* photon slots per wave, 1..2^22 (0: 2^22) */
+    int32_t pad;
+} ftb_server_config;
+
+typedef struct ftb_request {
+    const ftb_scene* scene;
+    ftb_camera cam;
+    int64_t n_photons;
+    uint64_t seed_base;
+    int32_t max_bounce;
+    int32_t frac_bits;         /* <= 0: the default for n_photons */
+    int64_t* host_film;        /* res_x*res_y*4 int64, written at completion (page-locked memory
+                                  copies fastest); NULL: the film is dropped */
+} ftb_request;
+
+typedef struct ftb_job_result {
+    ftb_status status;         /* of the render: FTB_OK or the error that failed it */
+    int32_t pad;
+    ftb_film_info info;
+    ftb_energy energy;
+    double submit_s, admit_s, finish_s;   /* server clock: seconds since ftb_server_create */
+} ftb_job_result;
+
+typedef struct ftb_server_stats {
+    int64_t submitted, completed, failed, queued, active;
+    int64_t photons_done;      /* photons of completed jobs */
+    int64_t waves;             /* waves launched */
+    double busy_s;             /* time with at least one wave in flight */
+    uint64_t film_bytes;       /* device film bytes of admitted jobs now */
+} ftb_server_stats;
+
+ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out);
+/* Queue a job; never blocks on the GPU.  A job whose film alone exceeds the budget fails
+ * here with FTB_ERR_TOO_LARGE. */
+ftb_status ftb_server_submit(ftb_server* s, const ftb_request* req, uint64_t* job_id);
+/* Wait for a job (timeout_s < 0: without limit).  FTB_OK: the job is finished, `out` holds
+ * its result and the server forgets it (wait once per job); FTB_ERR_TIMEOUT: still running. */
+ftb_status ftb_server_wait(ftb_server* s, uint64_t job_id, double timeout_s, ftb_job_result* out);
+ftb_status ftb_server_get_stats(ftb_server* s, ftb_server_stats* out);
+/* Finish every submitted job, then stop and release the server. */
+ftb_status ftb_server_destroy(ftb_server* s);
 
 #ifdef __cplusplus
 }

@@ -119,19 +119,25 @@ void admit_locked(ftb_server* s) {
         s->queue.pop_front();
         j->slot = s->free_slots.back();
         s->free_slots.pop_back();
-        void* p = nullptr;
-        cudaError_t e = cudaMallocFromPoolAsync(&p, j->film_bytes, s->pool, s->admit_stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, j->film_bytes, s->admit_stream);
-        if (e == cudaSuccess)
-            e = cudaMemsetAsync(s->d_tally + 8 * (size_t)j->slot, 0, 8 * sizeof(unsigned long long), s->admit_stream);
-        j->d_film = (int64_t*)p;
+        cudaError_t e = cudaSuccess;
+        if (j->req.n_photons > 0) {   // an empty job needs no device film: its film is zero
+            void* p = nullptr;
+            e = cudaMallocFromPoolAsync(&p, j->film_bytes, s->pool, s->admit_stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, j->film_bytes, s->admit_stream);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(s->d_tally + 8 * (size_t)j->slot, 0, 8 * sizeof(unsigned long long),
+                                    s->admit_stream);
+            j->d_film = (int64_t*)p;
+            s->admitted_since_launch = true;
+        }
         j->t_admit = s->now();
         s->film_bytes += j->film_bytes;
         s->st.queued--;
         s->st.active++;
-        s->admitted_since_launch = true;
         if (e != cudaSuccess) {
             cudaGetLastError();
+            if (j->d_film) cudaFreeAsync(j->d_film, s->admit_stream);
+            j->d_film = nullptr;
             j->error = e == cudaErrorMemoryAllocation ? FTB_ERR_OOM : FTB_ERR_CUDA;
             j->next = j->req.n_photons;   // nothing to trace
         }

@@ -35,7 +35,15 @@ namespace {
 
 constexpr double kTableStep = 0.5;   // nm
 
+struct BakedBlas {
+    std::vector<double> tri_v, tri_n;
+    std::vector<int32_t> tri_mat;
+};
+
 struct Baked {
+    std::vector<BakedBlas> blas;
+    std::vector<ftb_blas_desc> blas_desc;
+    std::vector<ftb_instance> instances;
     std::vector<double> tri_v, tri_n, sph, curve, table_w, table_v, cdf;
     std::vector<int32_t> tri_mat, sph_mat, curve_mat;
     std::vector<ftb_material> mats;
@@ -105,10 +113,32 @@ void bake(const Scene& sc, Baked& b) {
                                        (double)c.u0, (double)c.u1});
         b.curve_mat.push_back(c.matId);
     }
-    if (!sc.implicits.empty() || !sc.instances.empty() || !sc.emissiveVolumes.empty() ||
+    // shared mesh assets and their placements (Scene::blasList / instances, scene.h:1089-1090)
+    for (const Blas& bl : sc.blasList) {
+        BakedBlas bb;
+        for (const Tri& t : bl.tris) {
+            const Vec3 v[3] = {t.v0, t.v1, t.v2};
+            const Vec3 n[3] = {t.n0, t.n1, t.n2};
+            for (int k = 0; k < 3; ++k) {
+                bb.tri_v.insert(bb.tri_v.end(), {v[k].x, v[k].y, v[k].z});
+                bb.tri_n.insert(bb.tri_n.end(), {n[k].x, n[k].y, n[k].z});
+            }
+            bb.tri_mat.push_back(t.matId);
+        }
+        b.blas.push_back(std::move(bb));
+    }
+    for (const MeshInstance& mi : sc.instances) {
+        ftb_instance o{};
+        o.blas = mi.blasId;
+        o.mat_override = mi.matOverride;
+        for (int k = 0; k < 9; ++k) o.to_world[k] = mi.toWorld.m[k];
+        o.to_world[9] = mi.toWorld.t.x; o.to_world[10] = mi.toWorld.t.y; o.to_world[11] = mi.toWorld.t.z;
+        b.instances.push_back(o);
+    }
+    if (!sc.implicits.empty() || !sc.emissiveVolumes.empty() ||
         sc.envMap || !sc.mirrorPlanes.empty() || !sc.dielSphereIdx.empty() || !sc.mirrorSphereIdx.empty()) {
         b.supported = false;
-        b.why = "implicits, instances, emissive volumes, environment maps and specular connectors are not on this path";
+        b.why = "implicits, emissive volumes, environment maps and specular connectors are not on this path";
     }
     for (const Emitter& e : sc.emitters) {
         ftb_emitter o{};
@@ -170,6 +200,18 @@ void bake(const Scene& sc, Baked& b) {
     d.emitter_cdf = b.cdf.data();
     d.n_media = (int32_t)b.media.size();
     d.media = b.media.data();
+    for (BakedBlas& bb : b.blas) {
+        ftb_blas_desc o{};
+        o.n_tris = (int64_t)bb.tri_mat.size();
+        o.tri_v = bb.tri_v.data();
+        o.tri_n = bb.tri_n.data();
+        o.tri_mat = bb.tri_mat.data();
+        b.blas_desc.push_back(o);
+    }
+    d.n_blas = (int32_t)b.blas_desc.size();
+    d.blas = b.blas_desc.data();
+    d.n_instances = (int64_t)b.instances.size();
+    d.instances = b.instances.data();
 }
 
 ftb_camera bake_camera(const Camera& c, int resX, int resY) {

@@ -31,13 +31,13 @@ def make_materials(L):
     return sb.build(L)
 
 
-def make_instances(L):
+def make_instances(L, ramp=0.01, cauchy=True):
     """Instanced meshes (Blas / MeshInstance): a smooth-shaded dielectric blob placed twice
     (a rotation with non-uniform scale, and a scaled copy with a glossy material override)
     and a diffuse box asset rotated about y, beside the world triangles of the box."""
     sb = scenes.SceneBuilder()
-    scenes.cornell_box(sb, boxes=False)
-    glass = sb.material(abi.MAT_DIELECTRIC, ior=sb.cauchy(1.5, 0.0042), roughness=0.0)
+    scenes.cornell_box(sb, boxes=False, ramp=ramp)
+    glass = sb.material(abi.MAT_DIELECTRIC, ior=sb.cauchy(1.5, 0.0042) if cauchy else sb.const(1.5), roughness=0.0)
     v, f = scenes.icosphere(2)
     n = scenes.value_noise3(v, 5)
     r = 0.25 + 0.03 * (2.0 * n - 1.0)

@@ -138,3 +138,41 @@ def test_energy_conservation_full_size_cornell(gpu):
     assert abs(fx[0] - (fx[1] + fx[2] + fx[3] + fx[4])) <= n
     assert film[..., 3].sum() > 0
     sc.close()
+
+
+@pytest.mark.parametrize("name,level", [("cornell", 0), ("glass", 5)])
+def test_film_statistics_independent_photons(name, level, gpu, oracle):
+    """The statistical film criterion with independent photons: the GPU renders indices
+    [0, N), the oracle [N, 2N), each as K = 32 batches.  Per pixel, the two batch means of Y
+    are compared in units of their combined standard error; the number of lit pixels beyond
+    3 sigma must be consistent with chance (binomial tail 1e-4 at the Student-t rate for
+    K - 1 degrees of freedom), and the mean luminance of the two films must agree within
+    0.5%.  A systematic error shows up as many pixels beyond 3 sigma."""
+    stats = pytest.importorskip("scipy.stats")
+    d = scenes.make_cornell(gpu) if name == "cornell" else scenes.make_glass(gpu, level=level)
+    mb = 8 if name == "cornell" else 16
+    res, K, per = 32, 32, (1 << 16 if name == "cornell" else 1 << 18)
+    cam = scenes.default_camera(gpu, res)
+    sc = lib.Scene(d, 0, gpu)
+    ctx = oracle.prepare(d)
+    g, c = [], []
+    try:
+        for k in range(K):
+            film, info, _ = sc.render(cam, per, seed_base=k * per, max_bounce=mb)
+            g.append(lib.film_to_xyz(film, info)[0][..., 1])
+            o = oracle.trace(d, cam, per, seed_base=(K + k) * per, max_bounce=mb, threads=os.cpu_count() or 4,
+                             ctx=ctx)
+            c.append(o["xyz"][..., 1])
+    finally:
+        oracle.L.fto_release(ctx)
+        sc.close()
+    g, c = np.array(g), np.array(c)
+    mg, mc = g.mean(0), c.mean(0)
+    se = np.sqrt(g.var(0, ddof=1) / K + c.var(0, ddof=1) / K)
+    lit = se > 0
+    bad = int((np.abs(mg - mc)[lit] > 3.0 * se[lit]).sum())
+    p = 2.0 * stats.t.sf(3.0, K - 1)
+    limit = stats.binom.isf(1e-4, int(lit.sum()), p)
+    assert bad <= limit, f"{bad} of {lit.sum()} pixels beyond 3 sigma (chance allows {limit:.0f})"
+    rel = mg.sum() / mc.sum() - 1.0
+    assert abs(rel) < 0.005, f"mean luminance differs by {rel:.4%}"

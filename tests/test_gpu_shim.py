@@ -13,6 +13,7 @@ import os
 import numpy as np
 import pytest
 
+import cases
 from goodphotons_b200 import abi, lib, scenes
 
 pytestmark = pytest.mark.gpu
@@ -37,12 +38,20 @@ def shim(gpu):
     return L
 
 
-def test_render_forward_cuda_through_shim(shim, gpu):
+def cornell_on_grid(gpu):
     sb = scenes.SceneBuilder()
     scenes.cornell_box(sb, boxes=True, ramp=0.5)
-    d = sb.build(gpu)
+    return sb.build(gpu)
+
+
+@pytest.mark.parametrize("scene", ["cornell", "instances"])
+def test_render_forward_cuda_through_shim(shim, gpu, scene):
+    """`instances`: the reference Scene's blasList / MeshInstances go through the shim's bake
+    (with a constant IOR: the shim tabulates non-constant spectra every 0.5 nm, exact only for
+    piecewise-linear ones)."""
+    d = cornell_on_grid(gpu) if scene == "cornell" else cases.make_instances(gpu, ramp=0.5, cauchy=False)
     cam = scenes.default_camera(gpu, 48)
-    n, mb, seed = 60_000, 8, 77
+    n, mb, seed = 60_000, (8 if scene == "cornell" else 16), 77
     ref = shim.ftr_prepare(d.ref())
     try:
         npix = 48 * 48

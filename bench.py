@@ -76,6 +76,8 @@ class ClockSampler:
         self.lines = []
 
     def __enter__(self):
+        if self.index < 0:   # sampling off
+            return self
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -256,12 +258,12 @@ def run_animation(args):
         return [dict(scene=c, cam=cams[f.res], d_film=fl.data_ptr(), n=max(1, f.photons // scale),
                      seed_base=f.seed_base, max_bounce=16, frac_bits=0) for c, f, fl in zip(clones, frames, films)]
 
+    t = time.perf_counter()   # autotuner on frame 0 (untimed)
+    tuning = L.autotune(clones[0], cams[frames[0].res], 1 << 23, 16)
+    tune_s = time.perf_counter() - t
     for w in range(args.warmup):   # warm-up at 1/16 of every budget (same wave sizes)
         L.render_batch(jobs(16), stream=stream.cuda_stream, want_energy=False)
     torch.cuda.synchronize(dev)
-    base.set_profiling(1)
-    for c in clones:
-        c.set_profiling(1)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
@@ -273,8 +275,11 @@ def run_animation(args):
             ev[k][1].record(stream)
         torch.cuda.synchronize(dev)
     batch_s = sum(a.elapsed_time(b) for a, b in ev) / 1e3
-    prof = clones[0].profile(reset=True)
     value = total * args.steps / batch_s
+    # photons are packed contiguously into waves; a wave launches emit, shadow and, per
+    # bounce, extend, shade and shadow
+    waves = -(-total // tuning.wave_slots)
+    launches = waves * (2 + 3 * 16)
 
     # end to end: per-frame TLAS refit + the batch + every film to pinned host memory
     t = time.perf_counter()
@@ -320,7 +325,9 @@ def run_animation(args):
                "transforms": "seeded rotation about a random axis 0-360 deg, translation +-0.2 m",
                "warmup": f"{args.warmup} batches at 1/16 of every budget",
                "l2": "flushed between timed steps (256 MiB write)", "blas_bake_ms": round(blas_ms, 1),
-               "clone_refit_ms_per_frame": round(clone_ms / len(frames), 3)}
+               "clone_refit_ms_per_frame": round(clone_ms / len(frames), 3),
+               "tuning": {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
+                          "graph_replay": bool(tuning.use_graphs), "autotune_s": round(tune_s, 2)}}
         line = {
             "metric": "photon paths/s on 1 B200 (batched animation)", "value": value, "unit": "photon paths/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * batch_s / args.steps,
@@ -337,7 +344,7 @@ def run_animation(args):
                                          "call": "ftb_scene_create + ftb_render_forward + destroy per frame"},
             },
             "speedup_e2e_vs_plain": round((total / e2e_s) / (plain_ph / plain_s), 3),
-            "gpu_launches": int(sum(prof.launches)),
+            "gpu_launches": int(launches),
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -547,25 +554,38 @@ def main():
             multigpu.render_sharded(sc, cam, n * world, film, seed_base=k * n * world, max_bounce=mb,
                                     dst=0, stream=stream.cuda_stream)
 
+    # autotuner (untimed): grid size, wave size and graph replay for this workload
+    t = time.perf_counter()
+    tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)
+    cfg["tuning"] = {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
+                     "graph_replay": bool(tuning.use_graphs), "autotune_s": round(time.perf_counter() - t, 2)}
+
     for w in range(args.warmup):
         step(1000 + w)
     torch.cuda.synchronize(dev)
+
+    def timed(first_step, clocks_on):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        with ClockSampler(local if clocks_on else -1) as clk:
+            for k in range(args.steps):
+                flush.fill_(k & 0xff)
+                ev[k][0].record(stream)
+                step(first_step + k)
+                ev[k][1].record(stream)
+            torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        return [a.elapsed_time(b) for a, b in ev], clk
+
+    # the timed steps: the product's own launch path (graph replay when tuned so)
+    step_ms, clocks = timed(0, True)
+    # the same steps again with per-kernel CUDA events (direct launches), for the roofline
     sc.set_profiling(1)
     sc.profile(reset=True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    with ClockSampler(local) as clocks:
-        for k in range(args.steps):
-            flush.fill_(k & 0xff)
-            ev[k][0].record(stream)
-            step(k)
-            ev[k][1].record(stream)
-        torch.cuda.synchronize(dev)
-    if dist is not None:
-        dist.barrier()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
+    prof_ms, _ = timed(args.steps, False)
     prof = sc.profile(reset=True)
     sc.set_profiling(0)
     total_s = sum(step_ms) / 1e3
@@ -581,7 +601,7 @@ def main():
     kms = list(prof.ms)
     dom = int(np.argmax(kms))
     peak, peak_kind = measured_peak()
-    rays_timed = rays_per_photon * n * args.steps
+    rays_timed = rays_per_photon * n * args.steps   # of the profiled steps
     extend_launches = max(1, prof.launches[1])
     bytes_launch = rays_timed * bytes_per_ray / extend_launches
     avg_launch_s = kms[1] / 1e3 / extend_launches
@@ -599,6 +619,8 @@ def main():
         "shadow_rays_per_photon": round(cp.counters[3] / n_count, 4),
         "kernel_share": {nm: round(x / max(1e-9, sum(kms)), 4) for nm, x in zip(names, kms)},
         "dominant_kernel": names[dom],
+        "kernel_times": "CUDA events on the launching streams over a second set of the same timed steps "
+                        f"(direct launches, {sum(prof_ms) / len(prof_ms):.2f} ms per step)",
     }
     gpu_launches = int(sum(prof.launches))
 

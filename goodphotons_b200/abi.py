@@ -125,6 +125,11 @@ class KernelProfile(C.Structure):
     _fields_ = [("ms", C.c_double * 4), ("launches", C.c_int64 * 4), ("counters", C.c_uint64 * 8)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("wave_slots", C.c_int32), ("grid_mult", C.c_int32), ("use_graphs", C.c_int32),
+                ("pad", C.c_int32)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_active", C.c_int32), ("film_budget", C.c_uint64),
                 ("wave_slots", C.c_int32), ("pad", C.c_int32)]
@@ -154,7 +159,7 @@ STRUCTS = {
     "ftb_footprint": Footprint, "ftb_photon_log": PhotonLog,
     "ftb_kernel_profile": KernelProfile, "ftb_job": Job, "ftb_blas_desc": BlasDesc,
     "ftb_instance": Instance, "ftb_server_config": ServerConfig, "ftb_request": Request,
-    "ftb_job_result": JobResult, "ftb_server_stats": ServerStats,
+    "ftb_job_result": JobResult, "ftb_server_stats": ServerStats, "ftb_tuning": Tuning,
 }
 
 # every entry point declared in include/ftb200.h
@@ -167,6 +172,6 @@ EXPORTS = [
     "ftb_scene_set_profiling", "ftb_scene_profile", "ftb_render_forward_noalloc",
     "ftb_render_batch", "ftb_blas_create", "ftb_blas_destroy", "ftb_scene_set_instance_transforms",
     "ftb_scene_clone_instances", "ftb_server_create", "ftb_server_submit", "ftb_server_wait",
-    "ftb_server_get_stats", "ftb_server_destroy",
+    "ftb_server_get_stats", "ftb_server_destroy", "ftb_get_tuning", "ftb_set_tuning", "ftb_autotune",
 ]
 NOALLOC_MAX_PHOTONS = 32768

@@ -162,7 +162,8 @@ struct JobStage {
     int next = 0;
     cudaError_t init() {
         if (host) return cudaSuccess;
-        cudaError_t e = cudaHostAlloc((void**)&host, sizeof(ftb::DevJob) * ftb::kWaveJobs * kRing, cudaHostAllocDefault);
+        cudaError_t e = cudaHostAlloc((void**)&host, sizeof(ftb::DevJob) * (ftb::kWaveJobs + 1) * kRing,
+                                      cudaHostAllocDefault);
         if (e != cudaSuccess) { host = nullptr; return e; }
         for (auto& v : ev) {
             e = cudaEventCreateWithFlags(&v, cudaEventDisableTiming);
@@ -170,14 +171,19 @@ struct JobStage {
         }
         return cudaSuccess;
     }
-    cudaError_t push(const ftb::DevJob* jobs, int n, ftb::DevJob* dst, cudaStream_t st) {
+    // The table and its parameters {jobs, slots} into the wave (w.jobs, w.params).
+    cudaError_t push(const ftb::DevJob* jobs, int n, int32_t slots, ftb::Wave& w, cudaStream_t st) {
         int e = next;
         next = (next + 1) % kRing;
         cudaError_t r = cudaEventSynchronize(ev[e]);
         if (r != cudaSuccess) return r;
-        ftb::DevJob* h = host + (size_t)e * ftb::kWaveJobs;
+        ftb::DevJob* h = host + (size_t)e * (ftb::kWaveJobs + 1);
         std::memcpy(h, jobs, sizeof(ftb::DevJob) * (size_t)n);
-        r = cudaMemcpyAsync(dst, h, sizeof(ftb::DevJob) * (size_t)n, cudaMemcpyHostToDevice, st);
+        int32_t* par = reinterpret_cast<int32_t*>(h + ftb::kWaveJobs);
+        par[0] = n;
+        par[1] = slots;
+        r = cudaMemcpyAsync(w.jobs, h, sizeof(ftb::DevJob) * (size_t)n, cudaMemcpyHostToDevice, st);
+        if (r == cudaSuccess) r = cudaMemcpyAsync(w.params, par, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, st);
         if (r != cudaSuccess) return r;
         return cudaEventRecord(ev[e], st);
     }
@@ -266,10 +272,14 @@ struct Engine {
     int32_t* status = nullptr;
     unsigned long long* batch_tally = nullptr;   // 8 words per job of the last batch
     size_t batch_cap = 0;
+    ftb::WaveGraphs* graphs[2] = {nullptr, nullptr};
+    ftb::LaunchShape shape;                      // grid and graph choice (autotuned)
+    int32_t wave_cap = 1 << 22;                  // largest wave (autotuned)
     ~Engine() {
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(device);
+        for (auto g : graphs) ftb::wave_graphs_destroy(g);
         for (auto& w : waves) ftb::wave_free(w);
         for (auto s : streams) if (s) cudaStreamDestroy(s);
         if (film) cudaFree(film);
@@ -282,6 +292,10 @@ struct Engine {
 
 std::mutex g_engine_mu;
 std::weak_ptr<Engine> g_engines[256];
+ftb_tuning g_tuning[256];          // per device; a new engine starts from it
+bool g_tuning_set[256] = {};
+
+ftb_tuning default_tuning() { return ftb_tuning{1 << 22, 16, 1, 0}; }
 
 // The device's engine, created on first use; it lives while any scene holds it.
 std::shared_ptr<Engine> engine_for(int device) {
@@ -290,6 +304,10 @@ std::shared_ptr<Engine> engine_for(int device) {
     if (!e) {
         e = std::make_shared<Engine>();
         e->device = device;
+        const ftb_tuning t = g_tuning_set[device] ? g_tuning[device] : default_tuning();
+        e->wave_cap = t.wave_slots;
+        e->shape.grid_mult = t.grid_mult;
+        e->shape.graph = t.use_graphs != 0;
         g_engines[device] = e;
     }
     return e;
@@ -532,6 +550,10 @@ DevCam dev_cam(const ftb_camera* c) {
 ftb_status ensure_waves(ftb_scene* s, int32_t W, bool log) {
     if (s->eng->wave_W >= W && s->eng->wave_log == log && s->eng->waves[0].block) return FTB_OK;
     for (auto& w : s->eng->waves) ftb::wave_free(w);
+    for (auto& g : s->eng->graphs) {   // captured graphs hold the old buffers' addresses
+        ftb::wave_graphs_destroy(g);
+        g = ftb::wave_graphs_create();
+    }
     s->eng->wave_W = 0;
     for (auto& w : s->eng->waves) {
         cudaError_t e = ftb::wave_alloc(w, W, log);
@@ -558,8 +580,8 @@ ftb_status ensure_frame(ftb_scene* s, size_t words) {
     return FTB_OK;
 }
 
-int32_t pick_wave(int64_t n) {
-    int64_t W = std::min<int64_t>(n, (int64_t)1 << 22);
+int32_t pick_wave(int64_t n, int32_t cap) {
+    int64_t W = std::min<int64_t>(n, (int64_t)cap);
     return (int32_t)std::max<int64_t>(W, 1);
 }
 
@@ -588,10 +610,9 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
                     cudaStream_t user_stream) {
     int64_t total = 0;
     for (auto c : count) total += c;
-    int32_t W = pick_wave(total);
-    ftb_status st = ensure_waves(s, W, log);
+    int32_t W = pick_wave(total, s->eng->wave_cap);
+    ftb_status st = ensure_waves(s, W, log);   // may keep larger buffers; waves use W slots
     if (st != FTB_OK) return st;
-    W = s->eng->wave_W;
     ftb::Frame f;
     f.stats = s->prof_mode == 2 ? s->stats : nullptr;
     f.status = s->eng->status;
@@ -627,10 +648,10 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         cudaStream_t ws = s->eng->streams[k & 1];
         w.logs = d_logs;
         w.log_base = log_base;
-        cudaError_t e = s->eng->stage[k & 1].push(table.data(), (int)table.size(), w.jobs, ws);
+        cudaError_t e = s->eng->stage[k & 1].push(table.data(), (int)table.size(), slots, w, ws);
         if (e != cudaSuccess) return cuda_fail(e, "job table upload");
-        e = ftb::launch_wave(w, w.jobs, (int32_t)table.size(), slots, max_bounce, inst, f, s->sms, ws,
-                             s->prof_mode ? s->prof : nullptr);
+        e = ftb::launch_wave(w, max_bounce, inst, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
+                             s->eng->graphs[k & 1]);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         ++k;
     }
@@ -1287,6 +1308,95 @@ ftb_status ftb_scene_profile(ftb_scene* s, ftb_kernel_profile* out, int32_t rese
 }
 
 // ---- sessions ---------------------------------------------------------------------------
+ftb_status ftb_get_tuning(int32_t device, ftb_tuning* out) {
+    if (!out || device < 0 || device >= 256) return fail(FTB_ERR_INVALID, "bad arguments");
+    std::lock_guard<std::mutex> lk(g_engine_mu);
+    *out = g_tuning_set[device] ? g_tuning[device] : default_tuning();
+    return FTB_OK;
+}
+
+ftb_status ftb_set_tuning(int32_t device, const ftb_tuning* t) {
+    if (!t || device < 0 || device >= 256) return fail(FTB_ERR_INVALID, "bad arguments");
+    if (t->wave_slots < 1 || t->wave_slots > (1 << 22) || t->grid_mult < 1 || t->grid_mult > 64)
+        return fail(FTB_ERR_INVALID, "tuning out of range");
+    std::shared_ptr<Engine> e;
+    {
+        std::lock_guard<std::mutex> lk(g_engine_mu);
+        g_tuning[device] = *t;
+        g_tuning_set[device] = true;
+        e = g_engines[device].lock();
+    }
+    if (e) {
+        std::lock_guard<std::mutex> lk(e->mu);
+        e->wave_cap = t->wave_slots;
+        e->shape.grid_mult = t->grid_mult;
+        e->shape.graph = t->use_graphs != 0;
+    }
+    return FTB_OK;
+}
+
+ftb_status ftb_autotune(ftb_scene* s, const ftb_camera* cam, int64_t n, int32_t max_bounce, ftb_tuning* out) {
+    ftb_render_params p{n, (uint64_t)1 << 60, max_bounce, 0};
+    ftb_status st = check_params(s, cam, &p);
+    if (st != FTB_OK) return st;
+    if (n < 1) return fail(FTB_ERR_INVALID, "autotune needs photons");
+    DeviceGuard guard(s->device);
+    int64_t* film = nullptr;
+    const size_t words = (size_t)cam->res_x * cam->res_y * 4;
+    CK(cudaMalloc(&film, words * sizeof(int64_t)), "autotune film");
+    cudaStream_t us = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t ce = cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&a);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&b);
+    ftb_tuning best;
+    ftb_get_tuning(s->device, &best);
+    double best_ms = 1e300;
+    auto trial = [&](const ftb_tuning& t, double& ms) -> ftb_status {
+        ftb_status r = ftb_set_tuning(s->device, &t);
+        if (r != FTB_OK) return r;
+        float v = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {   // the first run warms (allocations, graph capture)
+            if (cudaMemsetAsync(film, 0, words * sizeof(int64_t), us) != cudaSuccess) return fail(FTB_ERR_CUDA, "memset");
+            if (cudaEventRecord(a, us) != cudaSuccess) return fail(FTB_ERR_CUDA, "event");
+            r = ftb_render_forward_device(s, cam, &p, film, nullptr, nullptr, us);
+            if (r != FTB_OK) return r;
+            if (cudaEventRecord(b, us) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess)
+                return fail(FTB_ERR_CUDA, "event");
+            cudaEventElapsedTime(&v, a, b);
+        }
+        r = read_status(s);
+        ms = v;
+        return r;
+    };
+    if (ce == cudaSuccess) {
+        // one knob at a time from the current setting: grid, then wave size, then graphs
+        const int grids[] = {4, 8, 16, 32};
+        const int waves[] = {1 << 20, 1 << 21, 1 << 22};
+        for (int pass = 0; pass < 3 && st == FTB_OK; ++pass) {
+            std::vector<ftb_tuning> cand;
+            if (pass == 0) for (int g : grids) { ftb_tuning t = best; t.grid_mult = g; cand.push_back(t); }
+            if (pass == 1) for (int w : waves) { ftb_tuning t = best; t.wave_slots = w; cand.push_back(t); }
+            if (pass == 2) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.use_graphs = u; cand.push_back(t); }
+            for (const ftb_tuning& t : cand) {
+                double ms = 0;
+                st = trial(t, ms);
+                if (st != FTB_OK) break;
+                if (ms < best_ms) { best_ms = ms; best = t; }
+            }
+        }
+    } else {
+        st = cuda_fail(ce, "autotune setup");
+    }
+    ftb_set_tuning(s->device, &best);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (us) cudaStreamDestroy(us);
+    cudaFree(film);
+    if (st == FTB_OK && out) *out = best;
+    return st;
+}
+
 ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cams, int32_t max_bounce,
                              int32_t frac_bits, ftb_session** out) {
     if (!s || !cams || n_cams < 1 || !out) return fail(FTB_ERR_INVALID, "bad session arguments");

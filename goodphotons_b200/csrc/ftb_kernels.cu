@@ -21,6 +21,8 @@
 // tracer photon for photon; the remaining differences are last-bit ones from CUDA's
 // exp/log/sin/cos/pow, and exact ties in t.
 #include <cooperative_groups.h>
+#include <algorithm>
+#include <vector>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <stdint.h>
@@ -1018,8 +1020,8 @@ __device__ __forceinline__ void log_finish(const Wave& w, int slot, uint64_t pho
 }
 
 // ------------------------------------------------------------------ kernels ------------
-__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, int32_t n_jobs,
-                                              int32_t n_slots, Frame f) {
+__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f) {
+    const int32_t n_jobs = w.params[0], n_slots = w.params[1];
     const bool multi = n_jobs > 1;
     TallyAcc acc;
     tally_init(acc);
@@ -1121,8 +1123,8 @@ __device__ void block_add1(unsigned long long* dst, unsigned long long a) {
 
 template <bool COUNT, bool INST>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const DevJob* __restrict__ jobs,
-                                                              int32_t n_jobs, const int32_t* q,
-                                                              const int32_t* qcount, Frame f) {
+                                                              const int32_t* q, const int32_t* qcount, Frame f) {
+    const int32_t n_jobs = w.params[0];
     int nq = *qcount;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
@@ -1207,10 +1209,10 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
-                                                               int32_t n_jobs, Frame f, const int32_t* qin,
+                                                               Frame f, const int32_t* qin,
                                                                const int32_t* qin_count, int32_t* qout,
                                                                int32_t* qout_count, int32_t bounce) {
-    const bool multi = n_jobs > 1;
+    const bool multi = w.params[0] > 1;
     TallyAcc acc;
     tally_init(acc);
     int nq = *qin_count;
@@ -1387,7 +1389,8 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
 template <bool COUNT, bool INST>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const DevJob* __restrict__ jobs,
-                                                              int32_t n_jobs, Frame f) {
+                                                              Frame f) {
+    const int32_t n_jobs = w.params[0];
     int n = w.counts[2];
     if (n > w.S) n = w.S;
     TravCount cnt{0, 0, 0};
@@ -1434,6 +1437,7 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log) {
     w.counts = (int32_t*)take(64);
     w.job = (int32_t*)take(4 * wn); w.sjob = (int32_t*)take(4 * sn);
     w.jobs = (DevJob*)take(sizeof(DevJob) * kWaveJobs);
+    w.params = (int32_t*)take(64);
     w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
     w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
     w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
@@ -1456,31 +1460,32 @@ void wave_free(Wave& w) {
     w.block = nullptr;
 }
 
-cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_slots, int32_t max_bounce,
-                        bool inst, const Frame& f, int32_t sms, cudaStream_t st, LaunchSink* sink) {
+namespace {
+// The launch sequence of one wave: emit, its connections, then per bounce closest hit,
+// shading and the connections it queued.  Every launch reads the wave's job count and
+// slot count from w.params, so the same sequence serves any table (and one captured graph
+// serves every wave of its shape).
+void issue_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int grid, cudaStream_t st,
+                LaunchSink* sink) {
     const int T = 128;
-    int blocks_emit = (n_slots + T - 1) / T;
-    if (blocks_emit < 1) blocks_emit = 1;
-    int grid = sms * 16;   // persistent-style grid for the queue-driven kernels
-    int gq = (n_slots + T - 1) / T;
-    if (gq < grid) grid = gq < 1 ? 1 : gq;
+    const DevJob* jobs = w.jobs;
     const bool count = f.stats != nullptr;
     auto mark = [&](int k, bool end) { if (sink) sink->mark(k, end, st); };
     auto shadow = [&]() {
         mark(K_SHADOW, false);
         if (count) {
-            if (inst) k_shadow<true, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
-            else k_shadow<true, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+            if (inst) k_shadow<true, true><<<grid, T, 0, st>>>(w, jobs, f);
+            else k_shadow<true, false><<<grid, T, 0, st>>>(w, jobs, f);
         } else {
-            if (inst) k_shadow<false, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
-            else k_shadow<false, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, f);
+            if (inst) k_shadow<false, true><<<grid, T, 0, st>>>(w, jobs, f);
+            else k_shadow<false, false><<<grid, T, 0, st>>>(w, jobs, f);
         }
         mark(K_SHADOW, true);
         cudaMemsetAsync(&w.counts[2], 0, 4, st);
     };
     cudaMemsetAsync(w.counts, 0, 64, st);
     mark(K_EMIT, false);
-    k_emit<<<blocks_emit, T, 0, st>>>(w, jobs, n_jobs, n_slots, f);
+    k_emit<<<grid, T, 0, st>>>(w, jobs, f);
     mark(K_EMIT, true);
     shadow();
     int32_t* qa = w.qa;
@@ -1490,22 +1495,67 @@ cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_s
     for (int b = 0; b < max_bounce; ++b) {
         mark(K_EXTEND, false);
         if (count) {
-            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
-            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
+            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
         } else {
-            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
-            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, n_jobs, qa, ca, f);
+            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
+            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
         }
         mark(K_EXTEND, true);
         cudaMemsetAsync(cb, 0, 4, st);
         mark(K_SHADE, false);
-        k_shade<<<grid, T, 0, st>>>(w, jobs, n_jobs, f, qa, ca, qb, cb, b);
+        k_shade<<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
         mark(K_SHADE, true);
         shadow();
         int32_t* tq = qa; qa = qb; qb = tq;
         int32_t* tc = ca; ca = cb; cb = tc;
     }
-    return cudaGetLastError();
+}
+}  // namespace
+
+struct WaveGraphs {
+    struct Entry {
+        int32_t max_bounce, grid;
+        bool inst;
+        int32_t* status;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Entry> entries;
+    ~WaveGraphs() {
+        for (auto& e : entries) cudaGraphExecDestroy(e.exec);
+    }
+};
+
+WaveGraphs* wave_graphs_create() { return new WaveGraphs(); }
+void wave_graphs_destroy(WaveGraphs* g) { delete g; }
+
+cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int32_t sms,
+                        const LaunchShape& shape, cudaStream_t st, LaunchSink* sink, WaveGraphs* graphs) {
+    const int T = 128;
+    int grid = sms * std::max(1, shape.grid_mult);
+    const int gw = (w.W + T - 1) / T;   // enough blocks to give every slot a thread
+    if (gw < grid) grid = gw < 1 ? 1 : gw;
+    // A graph bakes the kernel arguments: the wave's buffers and status word are fixed for the
+    // life of its cache, but a log buffer changes per call, so logging waves launch directly.
+    if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
+        issue_wave(w, max_bounce, inst, f, grid, st, sink);
+        return cudaGetLastError();
+    }
+    for (auto& e : graphs->entries)
+        if (e.max_bounce == max_bounce && e.grid == grid && e.inst == inst && e.status == f.status)
+            return cudaGraphLaunch(e.exec, st);
+    cudaGraph_t g = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) return err;
+    issue_wave(w, max_bounce, inst, f, grid, st, nullptr);
+    err = cudaStreamEndCapture(st, &g);
+    if (err != cudaSuccess) return err;
+    WaveGraphs::Entry e{max_bounce, grid, inst, f.status, nullptr};
+    err = cudaGraphInstantiate(&e.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (err != cudaSuccess) return err;
+    graphs->entries.push_back(e);
+    return cudaGraphLaunch(e.exec, st);
 }
 
 }  // namespace ftb

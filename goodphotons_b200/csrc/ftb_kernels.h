@@ -50,6 +50,7 @@ struct Wave {
     int32_t* job;              // job of each slot (multi-job waves)
     int32_t* sjob;             // job of each shadow record
     DevJob* jobs;              // device job table, kWaveJobs entries
+    int32_t* params;           // [0] jobs in the table, [1] slots in use (written with the table)
     double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
     int32_t* spix;
     // parity instrumentation (null unless logging)
@@ -82,6 +83,7 @@ constexpr size_t wave_bytes(int32_t W, bool log) {
     b += wave_align(8 * w) + 2 * wave_align(4 * w);                 // hit t, record, sub-record
     b += 2 * wave_align(4 * w) + wave_align(64);                    // queues + counts
     b += wave_align(4 * w) + wave_align(4 * s) + wave_align(sizeof(DevJob) * kWaveJobs);   // job ids + table
+    b += wave_align(64);                                            // table parameters
     b += 9 * wave_align(8 * s) + wave_align(4 * s);                 // shadow records
     if (log) b += wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
     return b;
@@ -101,14 +103,29 @@ struct LaunchSink {
     virtual ~LaunchSink() {}
 };
 
-// Trace one wave on `stream`: jobs[0..n_jobs) is the device job table (already filled,
-// slot ranges consecutive from 0, n_slots = the sum of their n <= W), and every slot runs
-// through at most max_bounce bounces (the largest max_bounce of the jobs).  `instances`
-// selects the traversal variants that meet instance records (set when any job's scene has
-// instances).  With f.stats set, the counting variants of the traversal kernels run
-// (slower; for traffic accounting only).
-cudaError_t launch_wave(Wave& w, const DevJob* jobs, int32_t n_jobs, int32_t n_slots,
-                        int32_t max_bounce, bool instances, const Frame& f, int32_t sms,
-                        cudaStream_t stream, LaunchSink* sink = nullptr);
+// Launch shape chosen by the autotuner: blocks per SM of the queue-driven kernels, and
+// whether a wave is replayed from a captured CUDA graph.
+struct LaunchShape {
+    int32_t grid_mult = 16;
+    bool graph = true;
+};
+
+// Instantiated graphs of one wave buffer, by (bounce cap, grid, instance variant, status
+// word): captured on first use, replayed after.
+struct WaveGraphs;
+WaveGraphs* wave_graphs_create();
+void wave_graphs_destroy(WaveGraphs* g);
+
+// Trace one wave on `stream`.  The caller has written, stream-ordered before this call, the
+// job table to w.jobs (slot ranges consecutive from 0) and w.params = {jobs, slots} (slots
+// <= W); every slot runs through at most max_bounce bounces (the largest of its jobs).
+// `instances` selects the traversal variants that meet instance records (any job's scene has
+// instances).  With `graphs` and shape.graph the sequence is replayed from a CUDA graph;
+// profiling (sink), counting (f.stats) and logging (w.logs) launches are issued directly.
+// A cache's graphs hold the addresses of its wave buffer and status word: destroy the cache
+// when either changes.
+cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool instances, const Frame& f, int32_t sms,
+                        const LaunchShape& shape, cudaStream_t stream, LaunchSink* sink = nullptr,
+                        WaveGraphs* graphs = nullptr);
 
 }  // namespace ftb

@@ -112,10 +112,13 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     ftb_status out = FTB_OK;
     cudaError_t e = cudaMemsetAsync(tally, 0, 8 * sizeof(unsigned long long), st);   // tallies start at zero
     if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 64, st);
+    const int32_t params[2] = {1, (int32_t)p->n_photons};   // one job, its photons' slots
     if (e == cudaSuccess) e = cudaMemcpyAsync(w.jobs, &J, sizeof J, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w.params, params, sizeof params, cudaMemcpyHostToDevice, st);
+    ftb::LaunchShape shape;
+    shape.graph = false;
     if (e == cudaSuccess && p->n_photons > 0)
-        e = ftb::launch_wave(w, w.jobs, 1, (int32_t)p->n_photons, p->max_bounce, dev.n_inst > 0, f, sms, st,
-                             nullptr);
+        e = ftb::launch_wave(w, p->max_bounce, dev.n_inst > 0, f, sms, shape, st);
     if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (out == FTB_OK && info) {
         info->frac_bits = frac;

@@ -62,6 +62,7 @@ struct Job {
 
 struct WaveSlot {
     ftb::Wave wave{};
+    ftb::WaveGraphs* graphs = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     ftb::DevJob* table = nullptr;   // pinned staging of this buffer's job table
@@ -76,6 +77,7 @@ struct ftb_server {
     int sms = 148;
     int max_active = 64;
     int32_t W = 1 << 22;
+    ftb::LaunchShape shape;
     uint64_t budget = 0;
     Clock::time_point t0;
 
@@ -260,15 +262,20 @@ void scheduler(ftb_server* s) {
         retire(s, b);   // the buffer's previous wave
         WaveSlot& w = s->ws[b];
         std::memcpy(w.table, table.data(), sizeof(ftb::DevJob) * table.size());
+        int32_t* par = reinterpret_cast<int32_t*>(w.table + ftb::kWaveJobs);
+        par[0] = (int32_t)table.size();
+        par[1] = slots;
         cudaError_t e = cudaMemcpyAsync(w.wave.jobs, w.table, sizeof(ftb::DevJob) * table.size(),
                                         cudaMemcpyHostToDevice, w.stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(w.wave.params, par, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, w.stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_status + 16 * b, 0, 64, w.stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(w.stream, s->admit_ev, 0);
         ftb::Frame f;
         f.stats = nullptr;
         f.status = s->d_status + 16 * b;
         if (e == cudaSuccess)
-            e = ftb::launch_wave(w.wave, w.wave.jobs, (int32_t)table.size(), slots, mb, inst, f, s->sms, w.stream);
+            e = ftb::launch_wave(w.wave, mb, inst, f, s->sms, s->shape, w.stream, nullptr, w.graphs);
         if (e == cudaSuccess) e = cudaEventRecord(w.done, w.stream);
         {
             std::lock_guard<std::mutex> lk(s->mu);
@@ -332,6 +339,7 @@ void completer(ftb_server* s) {
 void release(ftb_server* s) {
     set_device(s);
     for (auto& w : s->ws) {
+        ftb::wave_graphs_destroy(w.graphs);
         ftb::wave_free(w.wave);
         if (w.stream) cudaStreamDestroy(w.stream);
         if (w.done) cudaEventDestroy(w.done);
@@ -384,8 +392,10 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
         if ((e = ftb::wave_alloc(w.wave, s->W, false)) != cudaSuccess) return bad(e, "wave allocation");
         if ((e = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
         if ((e = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) != cudaSuccess) return bad(e, "event");
-        if ((e = cudaHostAlloc((void**)&w.table, sizeof(ftb::DevJob) * ftb::kWaveJobs, cudaHostAllocDefault)) != cudaSuccess)
+        if ((e = cudaHostAlloc((void**)&w.table, sizeof(ftb::DevJob) * (ftb::kWaveJobs + 1), cudaHostAllocDefault)) !=
+            cudaSuccess)
             return bad(e, "job table staging");
+        w.graphs = ftb::wave_graphs_create();
     }
     if ((e = cudaStreamCreateWithFlags(&s->admit_stream, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
     if ((e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");

@@ -77,6 +77,9 @@ def load(path=None):
     _sig(L, "ftb_blas_destroy", st, PS)
     _sig(L, "ftb_scene_set_instance_transforms", st, PS, C.POINTER(C.c_double), C.c_int64)
     _sig(L, "ftb_scene_clone_instances", st, PS, C.POINTER(C.c_double), C.c_int64, C.POINTER(PS))
+    _sig(L, "ftb_get_tuning", st, C.c_int32, C.POINTER(abi.Tuning))
+    _sig(L, "ftb_set_tuning", st, C.c_int32, C.POINTER(abi.Tuning))
+    _sig(L, "ftb_autotune", st, PS, C.POINTER(abi.Camera), C.c_int64, C.c_int32, C.POINTER(abi.Tuning))
     _sig(L, "ftb_server_create", st, C.POINTER(abi.ServerConfig), C.POINTER(PS))
     _sig(L, "ftb_server_submit", st, PS, C.POINTER(abi.Request), C.POINTER(C.c_uint64))
     _sig(L, "ftb_server_wait", st, PS, C.c_uint64, C.c_double, C.POINTER(abi.JobResult))
@@ -143,6 +146,27 @@ class _Lib:
         ens = (abi.Energy * n)() if want_energy else None
         self.check(self.L.ftb_render_batch(arr, n, infos, ens, C.c_void_p(stream or 0)))
         return infos, ens
+
+    def get_tuning(self, device=0):
+        t = abi.Tuning()
+        self.check(self.L.ftb_get_tuning(device, C.byref(t)))
+        return t
+
+    def set_tuning(self, device=0, wave_slots=None, grid_mult=None, use_graphs=None):
+        t = self.get_tuning(device)
+        if wave_slots is not None:
+            t.wave_slots = wave_slots
+        if grid_mult is not None:
+            t.grid_mult = grid_mult
+        if use_graphs is not None:
+            t.use_graphs = int(bool(use_graphs))
+        self.check(self.L.ftb_set_tuning(device, C.byref(t)))
+        return t
+
+    def autotune(self, scene, cam, n, max_bounce):
+        t = abi.Tuning()
+        self.check(self.L.ftb_autotune(scene.h, C.byref(cam), n, max_bounce, C.byref(t)))
+        return t
 
     def supported(self, desc):
         r = self.L.ftb_forward_supported(desc.ref())

@@ -401,6 +401,29 @@ ftb_status ftb_scene_set_profiling(ftb_scene* scene, int32_t mode);
 /* Waits for the recorded events, returns the totals since the last reset. */
 ftb_status ftb_scene_profile(ftb_scene* scene, ftb_kernel_profile* out, int32_t reset);
 
+/* ---- launch tuning (no counterpart in the reference) ---------------------------------
+ * How a device's renders are launched: photon slots per wave (path state is ~300 B per
+ * slot, two waves in flight), blocks per SM of the queue-driven kernels, and whether each
+ * wave's bounce loop (about 5 launches per bounce) is replayed from a captured CUDA graph.
+ * Renders on the device use the setting current when they start; results do not depend on
+ * it (photons are keyed by index, films are fixed point). */
+typedef struct ftb_tuning {
+    int32_t wave_slots;   /* 1 .. 2^22 */
+    int32_t grid_mult;    /* 1 .. 64 */
+    int32_t use_graphs;   /* 0 / 1 */
+    int32_t pad;
+} ftb_tuning;
+
+ftb_status ftb_get_tuning(int32_t device, ftb_tuning* out);
+ftb_status ftb_set_tuning(int32_t device, const ftb_tuning* t);
+/* Autotuner: render n_photons of `scene` through `cam` (into a scratch film) under
+ * candidate tunings -- grid sizes, wave sizes, graphs on and off, one knob at a time from the
+ * current setting -- timing each with CUDA events after a warm-up, then keep the fastest
+ * for the scene's device and return it.  n_photons of at least a few waves (>= 2^23) gives
+ * stable timings. */
+ftb_status ftb_autotune(ftb_scene* scene, const ftb_camera* cam, int64_t n_photons, int32_t max_bounce,
+                        ftb_tuning* out);
+
 /* ---- render server (continuous batching; no counterpart in the reference) ------------
  * A server owns two wave buffers and streams on one device, a scheduler thread and a
  * completion thread.  Jobs (a resident scene, a camera, a photon range) are submitted from

@@ -2,6 +2,8 @@
 photon ranges and bounce caps share waves.  Each job's film and energy report must be
 bit-identical to rendering that job alone -- photons are keyed by index and the film is
 fixed point, so the mix cannot change a result."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -45,4 +47,31 @@ def test_batch_results_equal_solo_renders(gpu):
         assert list(ens[i].fx) == list(en.fx), f"job {i} energy"
         assert infos[i].frac_bits == 28
     for sc in (sc_c, sc_g, sc_m, sc_f):
+        sc.close()
+
+
+def test_tuning_and_graph_replay_do_not_change_results(gpu):
+    """Wave size, grid size and graph replay change only how waves are launched: films and
+    energy tallies stay bit-identical; the autotuner returns a setting in range."""
+    L = gpu
+    sc = lib.Scene(scenes.make_glass(L, level=3), 0, L)
+    cam = scenes.default_camera(L, 40)
+    saved = L.get_tuning(0)
+    try:
+        ref = None
+        for slots, grid, graphs in [(1 << 22, 16, 0), (1 << 20, 4, 1), (1 << 19, 32, 1), (3 << 18, 8, 0),
+                                    (1 << 22, 16, 1)]:
+            L.set_tuning(0, wave_slots=slots, grid_mult=grid, use_graphs=graphs)
+            for _ in range(2):   # the second render replays a captured graph
+                film, _, en = sc.render(cam, 1_500_000, seed_base=42, max_bounce=16, frac_bits=30)
+                if ref is None:
+                    ref = (film, list(en.fx))
+                np.testing.assert_array_equal(film, ref[0], err_msg=f"{slots} {grid} {graphs}")
+                assert list(en.fx) == ref[1]
+        t = L.autotune(sc, cam, 1 << 21, 16)
+        assert 1 <= t.wave_slots <= 1 << 22 and 1 <= t.grid_mult <= 64 and t.use_graphs in (0, 1)
+        film, _, _ = sc.render(cam, 1_500_000, seed_base=42, max_bounce=16, frac_bits=30)
+        np.testing.assert_array_equal(film, ref[0])
+    finally:
+        L.L.ftb_set_tuning(0, C.byref(saved))
         sc.close()

@@ -523,6 +523,10 @@ def main():
     cfg["l2"] = "flushed between timed steps (256 MiB write)"
     L = lib.load()
     desc = make_scene(args.workload, args.level, L)
+    lib.Scene(desc, local, L, build=abi.BUILD_DEVICE).close()   # first use loads the builder's kernels
+    t = time.perf_counter()
+    sc_fast = lib.Scene(desc, local, L, build=abi.BUILD_DEVICE)   # the GPU-built BVH, for comparison
+    bake_fast_ms = 1e3 * (time.perf_counter() - t)
     t = time.perf_counter()
     sc = lib.Scene(desc, local, L)
     bake_ms = 1e3 * (time.perf_counter() - t)
@@ -624,6 +628,17 @@ def main():
     }
     gpu_launches = int(sum(prof.launches))
 
+    # the same frame on the GPU-built BVH (device LBVH: faster bake, looser tree)
+    fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    film.zero_()
+    fa.record(stream)
+    sc_fast.render_device(cam, n, film.data_ptr(), seed_base=(1 << 51), max_bounce=mb, stream=stream.cuda_stream)
+    fb.record(stream)
+    torch.cuda.synchronize(dev)
+    device_build = {"bake_ms": round(bake_fast_ms, 1), "bake_ms_host_sah": round(bake_ms, 1),
+                    "photons_per_s": n / (fa.elapsed_time(fb) / 1e3)}
+    sc_fast.close()
+
     # end to end through the C ABI call with a pinned host film
     e2e = None
     host = torch.empty((res, res, 4), dtype=torch.int64, pin_memory=True)
@@ -660,6 +675,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded scene generator; no dataset)", "config": cfg,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": gpu_launches,
+            "device_bvh_build": device_build,
             "clocks": clocks.summary(),
             "notes": "fp64 path arithmetic (reference order), fp32 conservative BVH culling, int64 fixed-point film",
         }

@@ -6,6 +6,8 @@ sizes and field offsets against the compiled library.
 import ctypes as C
 
 FTB_OK = 0
+BUILD_SAH, BUILD_DEVICE = 0, 1
+
 STATUS_NAMES = {
     0: "FTB_OK", 1: "FTB_ERR_INVALID", 2: "FTB_ERR_NO_DEVICE", 3: "FTB_ERR_UNSUPPORTED",
     4: "FTB_ERR_CUDA", 5: "FTB_ERR_OOM", 6: "FTB_ERR_DEVICE_LIMIT", 7: "FTB_ERR_TOO_LARGE",
@@ -78,7 +80,7 @@ class SceneDesc(C.Structure):
                 ("n_table", C.c_int64), ("table_w", _PD), ("table_v", _PD),
                 ("n_emitters", C.c_int32), ("n_media", C.c_int32),
                 ("emitters", C.POINTER(Emitter)), ("emitter_cdf", _PD),
-                ("media", C.POINTER(Medium)), ("n_blas", C.c_int32), ("pad0", C.c_int32),
+                ("media", C.POINTER(Medium)), ("n_blas", C.c_int32), ("build", C.c_int32),
                 ("blas", C.POINTER(BlasDesc)), ("n_instances", C.c_int64),
                 ("instances", C.POINTER(Instance))]
 

@@ -59,6 +59,7 @@ def build(verbose=False, force=False):
         ("ftb_noalloc.cu", [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]),
         ("ftb_api.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off"]),
         ("bvh_build.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC"]),
+        ("bvh_device.cu", [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]),
         ("ftb_server.cpp", ["-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread"]),
     ]
     for src, flags in units:

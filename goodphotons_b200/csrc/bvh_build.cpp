@@ -26,10 +26,13 @@ namespace {
 #endif
 constexpr int kLeafSize = FTB_BUILD_LEAF;
 
-struct BNode {
-    Box box;
-    int left = -1, right = -1, first = 0, count = 0;
-};
+using BNode = BinNode;
+
+double area(const Box& b) {
+    double dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    if (dx < 0 || dy < 0 || dz < 0) return 0.0;
+    return 2.0 * (dx * dy + dy * dz + dz * dx);
+}
 
 struct Builder {
     const std::vector<Box>& boxes;
@@ -38,11 +41,6 @@ struct Builder {
     std::vector<BNode> nodes;
     explicit Builder(const std::vector<Box>& b) : boxes(b) {}
 
-    static double area(const Box& b) {
-        double dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
-        if (dx < 0 || dy < 0 || dz < 0) return 0.0;
-        return 2.0 * (dx * dy + dy * dz + dz * dx);
-    }
     double cent(int p, int a) const { return a == 0 ? cx[p] : (a == 1 ? cy[p] : cz[p]); }
 
     int build(int start, int end) {
@@ -166,7 +164,7 @@ bool quantize_axis(double nlo, double nhi, const double* clo, const double* chi,
 }  // namespace
 
 bool build_wide_bvh(const std::vector<Box>& boxes_in, double margin, WideBvh& out,
-                    std::string& err) {
+                    std::string& err, BuildMethod method, int device) {
     out.nodes.clear();
     out.order.clear();
     const int n = (int)boxes_in.size();
@@ -174,18 +172,36 @@ bool build_wide_bvh(const std::vector<Box>& boxes_in, double margin, WideBvh& ou
     std::vector<Box> boxes(boxes_in);
     for (auto& b : boxes)
         for (int a = 0; a < 3; ++a) { b.lo[a] -= margin; b.hi[a] += margin; }
-    Builder B(boxes);
-    B.idx.resize(n);
-    B.cx.resize(n); B.cy.resize(n); B.cz.resize(n);
-    for (int i = 0; i < n; ++i) {
-        B.idx[i] = i;
-        B.cx[i] = 0.5 * (boxes[i].lo[0] + boxes[i].hi[0]);
-        B.cy[i] = 0.5 * (boxes[i].lo[1] + boxes[i].hi[1]);
-        B.cz[i] = 0.5 * (boxes[i].lo[2] + boxes[i].hi[2]);
+    if (method == BuildMethod::kDeviceLbvh) return build_wide_lbvh_device(boxes, kLeafSize, device, out, err);
+    std::vector<BinNode> nodes;
+    std::vector<int> idx;
+    {
+        Builder B(boxes);
+        B.idx.resize(n);
+        B.cx.resize(n); B.cy.resize(n); B.cz.resize(n);
+        for (int i = 0; i < n; ++i) {
+            B.idx[i] = i;
+            B.cx[i] = 0.5 * (boxes[i].lo[0] + boxes[i].hi[0]);
+            B.cy[i] = 0.5 * (boxes[i].lo[1] + boxes[i].hi[1]);
+            B.cz[i] = 0.5 * (boxes[i].lo[2] + boxes[i].hi[2]);
+        }
+        B.nodes.reserve(2 * (size_t)n / FTB_LEAF_MAX + 16);
+        B.build(0, n);
+        nodes.swap(B.nodes);
+        idx.swap(B.idx);
     }
-    B.nodes.reserve(2 * (size_t)n / FTB_LEAF_MAX + 16);
-    B.build(0, n);
+    return collapse_to_wide(nodes, idx, out, err);
+}
 
+bool collapse_to_wide(const std::vector<BinNode>& bnodes, const std::vector<int>& bidx, WideBvh& out,
+                      std::string& err) {
+    struct {
+        const std::vector<BinNode>& nodes;
+        const std::vector<int>& idx;
+    } B{bnodes, bidx};
+    out.nodes.clear();
+    out.order.clear();
+    if (bnodes.empty()) return true;
     // Collapse.  A wide node is described by the binary node ids of its (<= 8) children.
     struct Pending { int bnode; int wide; };
     std::vector<Pending> queue;
@@ -204,7 +220,7 @@ bool build_wide_bvh(const std::vector<Box>& boxes_in, double margin, WideBvh& ou
             for (int k = 0; k < (int)kids.size(); ++k) {
                 const BNode& c = B.nodes[kids[k]];
                 if (c.count > 0) continue;
-                double a = Builder::area(c.box);
+                double a = area(c.box);
                 if (a > ba) { ba = a; best = k; }
             }
             if (best < 0) break;

@@ -30,9 +30,32 @@ struct WideBvh {
     std::vector<int> order;     // record i holds primitive order[i]
 };
 
-// Build over primitive boxes grown by `margin` (absolute, in scene units).
+// A binary tree: root 0; a node with count > 0 is a leaf over idx[first, first + count).
+struct BinNode {
+    Box box;
+    int left = -1, right = -1, first = 0, count = 0;
+};
+
+enum class BuildMethod {
+    kHostSah,      // binned SAH (32 bins, 3 axes) on the host: the better tree
+    kDeviceLbvh    // Morton-ordered radix tree on the GPU: a faster build, a looser tree
+};
+
+// Build over primitive boxes grown by `margin` (absolute, in scene units): a binary tree by
+// `method`, collapsed to 8-wide nodes with conservative 8-bit child planes.
 bool build_wide_bvh(const std::vector<Box>& boxes, double margin, WideBvh& out,
-                    std::string& err);
+                    std::string& err, BuildMethod method = BuildMethod::kHostSah, int device = 0);
+
+// The collapse: each wide node opens the binary child of largest surface area until it has
+// 8 children; leaf children become runs of records laid out per wide node.
+bool collapse_to_wide(const std::vector<BinNode>& nodes, const std::vector<int>& idx, WideBvh& out,
+                      std::string& err);
+
+// Linear BVH on `device` (bvh_device.cu): 63-bit Morton codes of the box centres, a radix
+// sort, the Karras radix tree and bottom-up boxes (subtrees of at most leaf_size primitives
+// become leaves), collapsed to 8-wide nodes on the device as well.  Boxes are grown already.
+bool build_wide_lbvh_device(const std::vector<Box>& boxes, int leaf_size, int device, WideBvh& out,
+                            std::string& err);
 
 // Refit: the same topology over new primitive boxes (grown by `margin`).  Every node's
 // child boxes are recomputed bottom-up and quantized afresh, so the result is exactly as

@@ -380,6 +380,7 @@ ftb_status check_desc(const ftb_scene_desc* d) {
         (d->n_emitters && (!d->emitters || !d->emitter_cdf)) || (d->n_media && !d->media))
         return fail(FTB_ERR_INVALID, "null array for a nonzero count");
     if (d->n_blas < 0 || d->n_instances < 0) return fail(FTB_ERR_INVALID, "negative count in scene descriptor");
+    if (d->build != FTB_BUILD_SAH && d->build != FTB_BUILD_DEVICE) return fail(FTB_ERR_INVALID, "unknown BVH build");
     if ((d->n_blas && !d->blas) || (d->n_instances && !d->instances))
         return fail(FTB_ERR_INVALID, "null array for a nonzero count");
     int64_t np = d->n_tris + d->n_spheres + d->n_curves + d->n_instances;
@@ -486,7 +487,7 @@ double box_maxabs(const ftb::Box& b, double m) {
 
 // Bake one BLAS on `device` (current): triangle boxes, wide BVH with a margin from the
 // local coordinate magnitude, records in leaf order (prim = the triangle's BLAS index).
-ftb_status bake_blas(const ftb_blas_desc& d, int device, std::shared_ptr<BlasDev>& out) {
+ftb_status bake_blas(const ftb_blas_desc& d, int device, ftb::BuildMethod method, std::shared_ptr<BlasDev>& out) {
     auto b = std::make_shared<BlasDev>();
     b->mem.device = device;
     b->n_tris = d.n_tris;
@@ -509,7 +510,8 @@ ftb_status bake_blas(const ftb_blas_desc& d, int device, std::shared_ptr<BlasDev
     }
     ftb::WideBvh bvh;
     std::string err;
-    if (!ftb::build_wide_bvh(boxes, std::ldexp(maxabs, -18), bvh, err)) return fail(FTB_ERR_INVALID, err);
+    if (!ftb::build_wide_bvh(boxes, std::ldexp(maxabs, -18), bvh, err, method, device))
+        return fail(FTB_ERR_INVALID, err);
     if (!ftb::validate_wide_bvh(bvh, (int)nt, err)) return fail(FTB_ERR_INVALID, "BLAS BVH check: " + err);
     std::vector<PrimRec> recs(bvh.order.size());
     bool any_smooth = false;
@@ -845,7 +847,9 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
             bp = d->blas[b].handle->p;
             if (bp->mem.device != device) { delete s; return fail(FTB_ERR_INVALID, "BLAS handle lives on another device"); }
         } else {
-            ftb_status bs = bake_blas(d->blas[b], device, bp);
+            ftb_status bs = bake_blas(d->blas[b], device,
+                                      d->build == FTB_BUILD_DEVICE ? ftb::BuildMethod::kDeviceLbvh
+                                                                   : ftb::BuildMethod::kHostSah, bp);
             if (bs != FTB_OK) { delete s; return bs; }
         }
         s->blas.push_back(std::move(bp));
@@ -903,7 +907,12 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     double margin = std::ldexp(maxabs, -18);
     ftb::WideBvh bvh;
     std::string err;
-    if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err)) { delete s; return fail(FTB_ERR_INVALID, err); }
+    const ftb::BuildMethod method = d->build == FTB_BUILD_DEVICE ? ftb::BuildMethod::kDeviceLbvh
+                                                                 : ftb::BuildMethod::kHostSah;
+    if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err, method, device)) {
+        delete s;
+        return fail(FTB_ERR_INVALID, err);
+    }
     if (np > 0 && !ftb::validate_wide_bvh(bvh, (int)np, err)) { delete s; return fail(FTB_ERR_INVALID, "BVH check: " + err); }
     if (np == 0) {   // an empty root with no children
         bvh.nodes.resize(1);
@@ -1038,7 +1047,7 @@ ftb_status ftb_blas_create(const ftb_blas_desc* d, int32_t device, ftb_blas** ou
     if (device < 0 || device >= ndev) return fail(FTB_ERR_INVALID, "device index out of range");
     DeviceGuard guard(device);
     std::shared_ptr<BlasDev> b;
-    ftb_status st = bake_blas(*d, device, b);
+    ftb_status st = bake_blas(*d, device, ftb::BuildMethod::kHostSah, b);
     if (st != FTB_OK) return st;
     *out = new ftb_blas{std::move(b)};
     return FTB_OK;

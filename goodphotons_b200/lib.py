@@ -211,14 +211,19 @@ def _xf_array(to_world):
 class Scene:
     """A baked, device-resident scene (ftb_scene_create)."""
 
-    def __init__(self, desc, device=0, lib=None, _handle=None):
+    def __init__(self, desc, device=0, lib=None, _handle=None, build=abi.BUILD_SAH):
+        """build: abi.BUILD_SAH (host binned SAH) or abi.BUILD_DEVICE (GPU linear BVH)."""
         self.lib = lib or load()
         self.desc = desc
         if _handle is not None:
             self.h = _handle
             return
         h = C.c_void_p()
-        self.lib.check(self.lib.L.ftb_scene_create(desc.ref(), device, C.byref(h)))
+        desc.desc.build = build
+        try:
+            self.lib.check(self.lib.L.ftb_scene_create(desc.ref(), device, C.byref(h)))
+        finally:
+            desc.desc.build = abi.BUILD_SAH
         self.h = h
 
     def set_instance_transforms(self, to_world):

@@ -128,6 +128,14 @@ typedef struct ftb_medium {
     double radius;
 } ftb_medium;
 
+/* BVH builds (no counterpart in the reference, which builds with binned SAH on the host at
+ * scene load, bvh.h:89-176).  Either tree gives the same hits: only culling efficiency
+ * differs. */
+typedef enum ftb_build {
+    FTB_BUILD_SAH = 0,      /* binned SAH on the host: the tighter tree (default) */
+    FTB_BUILD_DEVICE = 1    /* linear BVH on the GPU: a much faster bake, a looser tree */
+} ftb_build;
+
 /* ---- instanced meshes --------------------------------------------------------------
  * A BLAS is a triangle asset in its own (local) space; instances place it in the world by
  * an affine map, like the reference's Blas / MeshInstance (scene.h:996-1063).  A ray meets
@@ -184,7 +192,7 @@ typedef struct ftb_scene_desc {
     const double* emitter_cdf;
     const ftb_medium* media;
     int32_t n_blas;
-    int32_t pad0;
+    int32_t build;          /* ftb_build: how ftb_scene_create builds the scene's BVH */
     const ftb_blas_desc* blas;
     int64_t n_instances;
     const ftb_instance* instances;

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 import cases
-from goodphotons_b200 import lib, scenes
+from goodphotons_b200 import abi, lib, scenes
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -72,6 +72,22 @@ def test_per_photon_paths_match_oracle(name, scenes_cache, gpu, oracle):
     assert (~same).sum() <= allowed, f"{(~same).sum()} of {n} photon paths differ; first {np.nonzero(~same)[0][:5]}"
     np.testing.assert_allclose(gl["beta"][same], ol["beta"][same], rtol=1e-12, atol=0)
     np.testing.assert_array_equal(gl["prims"][same], ol["prims"][same])
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_device_build_paths_match_oracle(name, gpu, oracle):
+    """The GPU-built linear BVH culls differently but must find the same hits: per-photon
+    paths equal the oracle's under the same allowance as the host-built tree."""
+    mk, res, _, mb, seed = cases.CASES[name]
+    d = mk(gpu)
+    sc = lib.Scene(d, 0, gpu, build=abi.BUILD_DEVICE)
+    n = 1 << 14
+    cam = cases.camera(gpu, res)
+    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=mb)
+    sc.close()
+    ol = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, threads=4)["logs"]
+    same = (gl["n_hits"] == ol["n_hits"]) & (gl["prim_hash"] == ol["prim_hash"]) & (gl["fate"] == ol["fate"])
+    assert (~same).sum() <= max(1, int(1e-5 * n)), f"{(~same).sum()} of {n} photon paths differ"
 
 
 def test_film_is_order_independent_and_linear(scenes_cache, gpu):

@@ -490,6 +490,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--photons", type=int, default=0, help="photons per step (default: the workload's frame)")
+    ap.add_argument("--tuning", default="", help="wave_slots,blocks_per_sm,graphs instead of the autotuner")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -560,7 +561,11 @@ def main():
 
     # autotuner (untimed): grid size, wave size and graph replay for this workload
     t = time.perf_counter()
-    tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)
+    if args.tuning:   # a fixed setting instead (reproducible launch sequences for profiling)
+        slots, grid, graphs = (int(x) for x in args.tuning.split(","))
+        tuning = L.set_tuning(local, wave_slots=slots, grid_mult=grid, use_graphs=graphs)
+    else:
+        tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)
     cfg["tuning"] = {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
                      "graph_replay": bool(tuning.use_graphs), "autotune_s": round(time.perf_counter() - t, 2)}
 

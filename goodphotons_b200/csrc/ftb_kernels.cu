@@ -503,17 +503,24 @@ __device__ __forceinline__ uint32_t child_entry(uint32_t child_base, uint32_t pr
 
 #define CSWAP(a, b) { uint32_t lo_ = min(a, b); b = max(a, b); a = lo_; }
 
+// A traversal stack in local memory.  (Keeping the top entries in shared memory measured
+// slower on B200: the L1 serves this stack well, and shared memory takes L1 capacity.)
+template <class E>
+struct LocalStack {
+    E loc[FTB_STACK];
+    __device__ __forceinline__ void put(int i, E v) { loc[i] = v; }
+    __device__ __forceinline__ E get(int i) const { return loc[i]; }
+};
+
 // Closest-hit walk of one wide BVH.  Children of a node are visited near to far (leaves and
 // inner nodes alike, keys sorted by an 8-input network in registers); entries farther than
 // the current hit are culled when popped.  The loop is "while-while": a lane steps through
 // inner nodes until it holds a leaf, so the lanes of a warp run the expensive leaf tests
 // together rather than interleaved with node steps.  leaf(first, count, tmax_f) tests a
 // leaf's records and returns the (possibly lowered) fp32 bound on t.
-template <bool COUNT, class Leaf>
+template <bool COUNT, class Stack, class Leaf>
 __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, const RayF& F, float tmin_f,
-                                              float tmax_f, Leaf& leaf, int32_t* status, TravCount& cnt) {
-    uint32_t st_e[FTB_STACK];
-    float st_t[FTB_STACK];
+                                              float tmax_f, Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt) {
     int sp = 0;
     uint32_t cur = 0;
     bool live = true;
@@ -540,8 +547,8 @@ __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, c
             for (int i = 7; i >= 1; --i) {
                 if (k[i] != 0xffffffffu) {
                     if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return tmax_f; }
-                    st_e[sp] = child_entry(child_base, prim_base, imask, N.meta, (int)(k[i] & 7u));
-                    st_t[sp] = __uint_as_float(k[i] & ~7u);
+                    st.put(sp, make_uint2(child_entry(child_base, prim_base, imask, N.meta, (int)(k[i] & 7u)),
+                                          k[i] & ~7u));
                     ++sp;
                 }
             }
@@ -552,7 +559,8 @@ __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, c
             bool found = false;
             while (sp > 0) {
                 --sp;
-                if (st_t[sp] <= tmax_f * T_CULL) { cur = st_e[sp]; found = true; break; }
+                const uint2 v = st.get(sp);
+                if (__uint_as_float(v.y) <= tmax_f * T_CULL) { cur = v.x; found = true; break; }
             }
             if (!found) { live = false; break; }
         }
@@ -561,7 +569,8 @@ __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, c
         bool found = false;
         while (sp > 0) {
             --sp;
-            if (st_t[sp] <= tmax_f * T_CULL) { cur = st_e[sp]; found = true; break; }
+            const uint2 v = st.get(sp);
+            if (__uint_as_float(v.y) <= tmax_f * T_CULL) { cur = v.x; found = true; break; }
         }
         if (!found) break;
     }
@@ -570,10 +579,9 @@ __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, c
 
 // Any-hit walk: order does not change the answer, so children are taken in slot order,
 // leaves first; leaf(first, count) returns true on a hit, which ends the walk.
-template <bool COUNT, class Leaf>
+template <bool COUNT, class Stack, class Leaf>
 __device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const RayF& F, float tmin_f, float tmax_f,
-                                         Leaf& leaf, int32_t* status, TravCount& cnt) {
-    uint32_t st_e[FTB_STACK];
+                                         Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt) {
     int sp = 0;
     uint32_t cur = 0;
     bool live = true;
@@ -597,16 +605,16 @@ __device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const 
                 uint32_t e = child_entry(child_base, prim_base, imask, N.meta, b & 7);
                 if (!have_next) { next = e; have_next = true; continue; }
                 if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return false; }
-                st_e[sp++] = e;
+                st.put(sp++, e);
             }
             if (have_next) { cur = next; continue; }
             if (sp == 0) { live = false; break; }
-            cur = st_e[--sp];
+            cur = st.get(--sp);
         }
         if (!live) break;
         if (leaf((int)((cur & ~LEAF_BIT) >> 2), (int)(cur & 3u) + 1)) return true;
         if (sp == 0) break;
-        cur = st_e[--sp];
+        cur = st.get(--sp);
     }
     return false;
 }
@@ -663,7 +671,8 @@ __device__ __noinline__ int blas_closest(const DevInst& I, D3 wo, D3 wd, double 
         }
         return tm;
     };
-    tmax_f = walk_closest<COUNT>(I.nodes, F, __double2float_rd(tmin), tmax_f, leaf, status, cnt);
+    LocalStack<uint2> st;
+    tmax_f = walk_closest<COUNT>(I.nodes, F, __double2float_rd(tmin), tmax_f, st, leaf, status, cnt);
     return best;
 }
 
@@ -685,7 +694,8 @@ __device__ __noinline__ bool blas_any(const DevInst& I, D3 wo, D3 wd, double tmi
         }
         return false;
     };
-    return walk_any<COUNT>(I.nodes, F, __double2float_rd(tmin), tmax_f, leaf, status, cnt);
+    LocalStack<uint32_t> st;
+    return walk_any<COUNT>(I.nodes, F, __double2float_rd(tmin), tmax_f, st, leaf, status, cnt);
 }
 
 // Closest hit (Scene::closestHit, scene.h:2194-2242): returns the world record (or -1) and
@@ -714,7 +724,8 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
         }
         return tm;
     };
-    walk_closest<COUNT>(sc.nodes, F, __double2float_rd(tmin), FLT_MAX, leaf, status, cnt);
+    LocalStack<uint2> st;
+    walk_closest<COUNT>(sc.nodes, F, __double2float_rd(tmin), FLT_MAX, st, leaf, status, cnt);
     return best;
 }
 
@@ -740,7 +751,8 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
         }
         return false;
     };
-    return walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, leaf, status, cnt);
+    LocalStack<uint32_t> st;
+    return walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt);
 }
 
 // Hit on BLAS record `sub` of instance I, in world terms: the local hit's attributes

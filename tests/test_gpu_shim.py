@@ -62,7 +62,10 @@ def test_render_forward_cuda_through_shim(shim, gpu, scene):
         assert shim.ftr_trace(ref, C.byref(cam), n, seed, mb, 1, P(cx), P(ch), P(ce), None, None, None) == 0
     finally:
         shim.ftr_release(ref)
-    sc = lib.Scene(d, 0, gpu)
+    # the shim bakes per call with the GPU-built tree unless the budget exceeds 4096 photons per
+    # primitive; the direct render uses the same tree, so hits (ties included) are the same
+    build = abi.BUILD_SAH if n > 4096 * d.n_prims else abi.BUILD_DEVICE
+    sc = lib.Scene(d, 0, gpu, build=build)
     film, info, e2 = sc.render(cam, n, seed_base=seed, max_bounce=mb)
     sc.close()
     dx, dh = lib.film_to_xyz(film, info)

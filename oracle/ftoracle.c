@@ -1465,6 +1465,255 @@ fto_ctx* fto_prepare(const ftb_scene_desc* d) {
     return c;
 }
 
+/* ------------------------------------------------------------- hero wavelengths ----- */
+#define HERO_MAX 8
+
+/* connectHero (render.h:564-577): one connectGeom (render.h:499-536), then every live
+ * wavelength splats with its own beta and reflectance.  Hero bundles never run with media. */
+static void connect_surface_hero(Tr* T, V3 p, V3 n, V3 ng, V3 wi, const double* lam, const double* beta,
+                                 const double* rho, int nup) {
+    const Cam* cam = T->cam;
+    V3 to_cam = vsub(cam->eye, p);
+    double dist = vlen(to_cam);
+    V3 wdir = vdiv(to_cam, dist);
+    double cos_surf = vdot(n, wdir);
+    if (cos_surf <= 0) return;
+    double stg = shadow_terminator_g(wdir, n, ng);
+    if (stg <= 0.0) return;
+    int px, py; double cos_cam, dist2;
+    if (!cam_project(cam, p, &px, &py, &cos_cam, &dist2)) return;
+    T->rays++;
+    if (occluded(T->c, vadd(p, vmul(ng, 1e-6)), wdir, dist - 2e-6, 1e-6)) return;
+    double omega = cam_pixel_solid_angle(cam, cos_cam);
+    double corr = shading_adjoint_corr(wi, wdir, n, ng);
+    double denom = dist2 * omega;
+    for (int i = 0; i < nup; ++i) {
+        double f = rho[i] / PI_D;
+        double contrib = beta[i] * f * cos_surf * corr / denom * stg;
+        film_add(T->film, px, py, cie_x(lam[i]) * contrib, cie_y(lam[i]) * contrib, cie_z(lam[i]) * contrib);
+    }
+}
+
+/* the energy of the live wavelengths (activeSum, render.h:2324-2325) */
+static inline double active_sum(const double* beta, int n) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += beta[i];
+    return s;
+}
+
+static inline double max_of(const double* a, int n) {   /* hero::maxOf (hero.h:120-126) */
+    double m = a[0];
+    for (int i = 1; i < n; ++i) if (a[i] > m) m = a[i];
+    return m;
+}
+
+/* Renderer::tracePhotonHero + tracePhotonHeroLoop (render.h:2252-2631) for the materials on
+ * this path: C wavelengths per photon (hero.h sampleBundle), geometry decided by the hero,
+ * analog RR on the max over live wavelengths with bounded reweights booked as absorption,
+ * and a dielectric de-heroes (the hero continues alone, boosted x C). */
+static void trace_photon_hero(Tr* T, Pcg* rng, int max_bounce, int C, double* e, ftb_photon_log* log) {
+    const fto_ctx* c = T->c;
+    uint64_t hash = FNV_BASIS;
+    int nh = 0;
+    if (log) { memset(log, 0, sizeof *log); log->fate = 4; for (int i = 0; i < 8; ++i) log->prims[i] = -2; }
+    if (c->total_power <= 0.0 || c->n_emit == 0) return;
+    int ei = 0;
+    if (c->n_emit > 1) {
+        double u = pcg_uniform(rng);
+        int lo = 0, hi = c->n_emit - 1;
+        while (lo < hi) { int mid = (lo + hi) / 2; if (c->emitter_cdf[mid] < u) lo = mid + 1; else hi = mid; }
+        ei = lo;
+    }
+    const Emit* em = &c->emit[ei];
+    double u1 = pcg_uniform(rng), u2 = pcg_uniform(rng);
+    V3 origin, emit_n, dir;
+    if (em->shape == FTB_EMIT_SPHERE) {
+        double z = 1.0 - 2.0 * u1;
+        double s = 1.0 - z * z;
+        double r = sqrt(s > 0.0 ? s : 0.0);
+        double phi = 2.0 * PI_D * u2;
+        V3 d = v3(r * cos(phi), r * sin(phi), z);
+        emit_n = d;
+        origin = vadd(em->origin, vmul(d, em->radius));
+    } else {
+        origin = vadd(vadd(em->origin, vmul(em->u, u1)), vmul(em->v, u2));
+        emit_n = em->normal;
+    }
+    dir = em->collimated ? em->beam : cosine_hemisphere(emit_n, rng);
+    /* hero::sampleBundle (hero.h:100-113): one variate, strata u + i/C wrapped */
+    double lam[HERO_MAX], pdf[HERO_MAX], beta[HERO_MAX];
+    double u = pcg_uniform(rng);
+    pdf[0] = 0.0;
+    lam[0] = emission_sample_at(em->cdf, em->n, em->step, u, &pdf[0]);
+    if (pdf[0] <= 0.0) return;
+    for (int i = 1; i < C; ++i) {
+        double uu = u + (double)i / (double)C;
+        if (uu >= 1.0) uu -= 1.0;
+        pdf[i] = 0.0;
+        lam[i] = emission_sample_at(em->cdf, em->n, em->step, uu, &pdf[i]);
+    }
+    double base = (c->n_emit == 1) ? em->power : c->total_power;
+    base *= 1.0;   /* spotW */
+    for (int i = 0; i < C; ++i) beta[i] = base / C;
+    int sec_alive = C > 1;
+    e[E_EMIT] += active_sum(beta, sec_alive ? C : 1);
+    {
+        double one[HERO_MAX];
+        for (int i = 0; i < C; ++i) one[i] = 1.0;
+        connect_surface_hero(T, origin, emit_n, emit_n, emit_n, lam, beta, one, C);
+    }
+    V3 ro = vadd(origin, vmul(dir, 1e-6)), rd = dir;
+    Stack stk; stk.n = 0;
+    int fate = 2;
+    for (int bounce = 0; bounce < max_bounce; ++bounce) {
+        int nup = sec_alive ? C : 1;
+        Hit h;
+        T->rays++;
+        int prim = closest_hit(c, ro, rd, 1e-6, &h);
+        hash = fnv_i32(hash, prim);
+        if (prim >= c->nt + c->ns + c->nc) hash = fnv_i32(hash, h.sub);
+        if (nh < 8 && log) log->prims[nh] = prim;
+        ++nh;
+        double d_event = h.valid ? h.t : 1e30;
+        {   /* Beer-Lambert per live wavelength (render.h:2389-2398) */
+            int mi = stk_top_mat(&stk);
+            if (mi >= 0)
+                for (int i = 0; i < nup; ++i) {
+                    double a = slot(c, c->mats[mi].absorb, lam[i], 0.0);
+                    if (a > 0.0) beta[i] *= exp(-a * d_event);
+                }
+        }
+        if (!h.valid) { e[E_ESC] += active_sum(beta, sec_alive ? C : 1); fate = 1; goto done; }
+        const ftb_material* m = &c->mats[h.mat];
+        switch (m->type) {
+        case FTB_MAT_DIFFUSE_TRANSMIT: {   /* render.h:2454-2503 */
+            double rho_r[HERO_MAX] = {0}, rho_t[HERO_MAX] = {0};
+            for (int i = 0; i < nup; ++i) {
+                double rr = clamp01(slot(c, m->reflect, lam[i], 0.5));
+                double rt = clamp01(slot(c, m->transmit, lam[i], 0.0));
+                double s = rr + rt;
+                if (s > 1.0) { rr /= s; rt /= s; }
+                rho_r[i] = rr; rho_t[i] = rt;
+            }
+            V3 ngo = oriented_geo_n(&h);
+            V3 wi = v3(-rd.x, -rd.y, -rd.z);
+            connect_surface_hero(T, h.p, h.n, ngo, wi, lam, beta, rho_r, nup);
+            connect_surface_hero(T, h.p, vneg(h.n), vneg(ngo), wi, lam, beta, rho_t, nup);
+            double q_r = max_of(rho_r, nup), q_t = max_of(rho_t, nup);
+            double sum_h = q_r + q_t;
+            if (nup > 1 && sum_h > 1.0) { q_r /= sum_h; q_t /= sum_h; sum_h = q_r + q_t; }
+            double uu = pcg_uniform(rng);
+            if (uu < q_r) {
+                for (int i = 0; i < nup; ++i) {
+                    double w = rho_r[i] / q_r;
+                    e[E_ABS] += beta[i] * (1.0 - w);
+                    beta[i] *= w;
+                }
+                V3 wo = cosine_hemisphere(h.n, rng);
+                double corr = shading_adjoint_corr(wi, wo, h.n, ngo);
+                for (int i = 0; i < nup; ++i) beta[i] *= corr;
+                ro = vadd(h.p, vmul(h.n, 1e-6)); rd = wo;
+                continue;
+            } else if (uu < sum_h) {
+                for (int i = 0; i < nup; ++i) {
+                    double w = rho_t[i] / q_t;
+                    e[E_ABS] += beta[i] * (1.0 - w);
+                    beta[i] *= w;
+                }
+                V3 wo = cosine_hemisphere(v3(-h.n.x, -h.n.y, -h.n.z), rng);
+                double corr = shading_adjoint_corr(wi, wo, h.n, ngo);
+                for (int i = 0; i < nup; ++i) beta[i] *= corr;
+                ro = vsub(h.p, vmul(h.n, 1e-6)); rd = wo;
+                continue;
+            }
+            e[E_ABS] += active_sum(beta, sec_alive ? C : 1); fate = 0; goto done;
+        }
+        case FTB_MAT_FILTER:
+        case FTB_MAT_GLOSSY: {   /* achromatic lobes (render.h:2505-2537) */
+            double cc[HERO_MAX] = {0};
+            for (int i = 0; i < nup; ++i)
+                cc[i] = (m->type == FTB_MAT_FILTER) ? clamp01(slot(c, m->transmit, lam[i], 0.0))
+                                                     : clamp01(slot(c, m->reflect, lam[i], 0.5));
+            double q = max_of(cc, nup);
+            if (pcg_uniform(rng) >= q) { e[E_ABS] += active_sum(beta, sec_alive ? C : 1); fate = 0; goto done; }
+            for (int i = 0; i < nup; ++i) {
+                double w = cc[i] / q;
+                e[E_ABS] += beta[i] * (1.0 - w);
+                beta[i] *= w;
+            }
+            if (m->type == FTB_MAT_FILTER) {
+                ro = vadd(h.p, vmul(rd, 1e-6));
+            } else {
+                V3 o = sample_glossy(vreflect(rd, h.n), m->roughness, rng);
+                if (vdot(o, h.n) <= 0) { e[E_ABS] += active_sum(beta, sec_alive ? C : 1); fate = 0; goto done; }
+                ro = vadd(h.p, vmul(h.n, 1e-6)); rd = o;
+            }
+            continue;
+        }
+        case FTB_MAT_DIELECTRIC: {   /* de-hero, then the scalar interaction (render.h:2539-2589) */
+            if (sec_alive) { beta[0] *= (double)C; sec_alive = 0; }
+            const double lam0 = lam[0];
+            int entering = vdot(rd, h.ng) < 0.0;
+            int mi = h.mat, pr = m->priority;
+            int has_pri = pr != INT_MIN;
+            V3 no, nd; int transmitted = 0;
+            if (entering) {
+                int out_mat = stk_top_mat(&stk), out_pri = stk_top_pri(&stk);
+                int ranked = has_pri && (stk.n == 0 || (out_mat >= 0 && c->mats[out_mat].priority != INT_MIN));
+                if (ranked && stk.n != 0 && pr <= out_pri) {
+                    stk_push(&stk, mi, pr);
+                    ro = vadd(h.p, vmul(rd, 1e-6));
+                    continue;
+                }
+                double ext = (ranked && out_mat >= 0) ? mat_ior(c, &c->mats[out_mat], lam0) : 1.0;
+                refract_or_reflect(c, m, &h, rd, lam0, rng, &transmitted, ext, &no, &nd);
+                ro = no; rd = nd;
+                if (transmitted) stk_push(&stk, mi, pr);
+            } else {
+                Stack after = stk;
+                stk_pop_mat(&after, mi);
+                int new_mat = stk_top_mat(&after), new_pri = stk_top_pri(&after);
+                int ranked = has_pri && (after.n == 0 || (new_mat >= 0 && c->mats[new_mat].priority != INT_MIN));
+                if (ranked && new_mat >= 0 && pr <= new_pri) {
+                    stk_pop_mat(&stk, mi);
+                    ro = vadd(h.p, vmul(rd, 1e-6));
+                    continue;
+                }
+                double ext = (ranked && new_mat >= 0) ? mat_ior(c, &c->mats[new_mat], lam0) : 1.0;
+                refract_or_reflect(c, m, &h, rd, lam0, rng, &transmitted, ext, &no, &nd);
+                ro = no; rd = nd;
+                if (transmitted) stk_pop_mat(&stk, mi);
+            }
+            continue;
+        }
+        case FTB_MAT_DIFFUSE:
+        default: {   /* render.h:2591-2625 */
+            double rho[HERO_MAX] = {0};
+            for (int i = 0; i < nup; ++i) rho[i] = clamp01(slot(c, m->reflect, lam[i], 0.5));
+            V3 ngo = oriented_geo_n(&h);
+            V3 wi = v3(-rd.x, -rd.y, -rd.z);
+            connect_surface_hero(T, h.p, h.n, ngo, wi, lam, beta, rho, nup);
+            double q = max_of(rho, nup);
+            if (pcg_uniform(rng) >= q) { e[E_ABS] += active_sum(beta, sec_alive ? C : 1); fate = 0; goto done; }
+            for (int i = 0; i < nup; ++i) {
+                double w = rho[i] / q;
+                e[E_ABS] += beta[i] * (1.0 - w);
+                beta[i] *= w;
+            }
+            V3 wo = cosine_hemisphere(h.n, rng);
+            double corr = shading_adjoint_corr(wi, wo, h.n, ngo);
+            for (int i = 0; i < nup; ++i) beta[i] *= corr;
+            ro = vadd(h.p, vmul(h.n, 1e-6)); rd = wo;
+            continue;
+        }
+        }
+    }
+    e[E_RES] += active_sum(beta, sec_alive ? C : 1);
+    fate = 2;
+done:
+    if (log) { log->n_hits = nh; log->fate = fate; log->prim_hash = hash; log->beta = beta[0]; }
+}
+
 /* ------------------------------------------------------------- driver --------------- */
 typedef struct {
     const fto_ctx* c;
@@ -1472,6 +1721,7 @@ typedef struct {
     int64_t lo, hi;
     uint64_t seed_base;
     int max_bounce;
+    int hero_c;   /* wavelengths per photon; 1 = the scalar tracer */
     double* xyz;
     double* hits;
     double e[5];
@@ -1487,16 +1737,22 @@ static void* worker(void* arg) {
     for (int64_t i = j->lo; i < j->hi; ++i) {
         seed_unit(&rng, j->seed_base + (uint64_t)i, PHOTON_SALT);
         T.rays = 0;
-        trace_photon(&T, &rng, j->max_bounce, j->e, j->logs ? &j->logs[i] : NULL);
+        if (j->hero_c > 1) trace_photon_hero(&T, &rng, j->max_bounce, j->hero_c, j->e, j->logs ? &j->logs[i] : NULL);
+        else trace_photon(&T, &rng, j->max_bounce, j->e, j->logs ? &j->logs[i] : NULL);
         if (j->rays) j->rays[i] = T.rays;
     }
     return NULL;
 }
 
 int fto_trace(const fto_ctx* c, const ftb_camera* cam, int64_t n, uint64_t seed_base,
-              int max_bounce, int threads, double* film_xyz, double* film_hits,
+              int max_bounce, int hero_c, int threads, double* film_xyz, double* film_hits,
               double* energy, ftb_photon_log* logs, int64_t* rays) {
     if (!c || !cam || n < 0 || !film_xyz || !film_hits || !energy) return fail("fto_trace: bad input");
+    /* -heroc is clamped to [1, kHeroMax] and hero sampling is off in scenes with media
+     * (hero.h:81-86, main.cpp:11309-11312) */
+    if (hero_c < 1) hero_c = 1;
+    if (hero_c > HERO_MAX) hero_c = HERO_MAX;
+    if (c->n_med > 0) hero_c = 1;
     if (threads < 1) threads = 1;
     Cam cm;
     cm.eye = rd3(cam->eye); cm.u = rd3(cam->u); cm.v = rd3(cam->v); cm.w = rd3(cam->w);
@@ -1506,7 +1762,7 @@ int fto_trace(const fto_ctx* c, const ftb_camera* cam, int64_t n, uint64_t seed_
     pthread_t* th = (pthread_t*)calloc((size_t)threads, sizeof(pthread_t));
     for (int t = 0; t < threads; ++t) {
         Job* j = &jobs[t];
-        j->c = c; j->cam = &cm; j->seed_base = seed_base; j->max_bounce = max_bounce;
+        j->c = c; j->cam = &cm; j->seed_base = seed_base; j->max_bounce = max_bounce; j->hero_c = hero_c;
         j->lo = n * t / threads; j->hi = n * (t + 1) / threads;
         j->logs = logs; j->rays = rays;
         if (threads == 1) { j->xyz = film_xyz; j->hits = film_hits; }

@@ -39,9 +39,11 @@ void fto_release(fto_ctx* ctx);
  *   energy: 5 doubles emitted/absorbed/sensor/escaped/residual (accumulated)
  *   logs: optional, n records (see ftb_photon_log)
  *   rays: optional, n per-photon counts of closest-hit + occlusion queries
+ *   hero_c: wavelengths per photon (Renderer::tracePhotonHero when > 1; clamped to 1..8;
+ *           1 in scenes with media, as the reference gates it)
  * Returns 0, or -1 on invalid input (message in fto_last_error()). */
 int fto_trace(const fto_ctx* ctx, const ftb_camera* cam, int64_t n, uint64_t seed_base,
-              int max_bounce, int threads, double* film_xyz, double* film_hits,
+              int max_bounce, int hero_c, int threads, double* film_xyz, double* film_hits,
               double* energy, ftb_photon_log* logs, int64_t* rays);
 
 /* Total emitted power (Scene::totalPower, scene.h:1509-1511). */

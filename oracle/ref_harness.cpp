@@ -197,7 +197,7 @@ int ftr_occluded(void* h, const double* o, const double* d, double max_dist) {
 /* Trace photons [seed_base, seed_base+n) like renderForward's CPU branch.  With logs
  * (threads must be 1) each photon gets its own EnergyReport so its fate and final beta
  * are exact: fate[i] = 0 absorbed, 1 escaped, 2 residual, 3 sensor, 4 nothing booked. */
-int ftr_trace(void* h, const ftb_camera* cam, int64_t n, uint64_t seed_base, int max_bounce,
+int ftr_trace(void* h, const ftb_camera* cam, int64_t n, uint64_t seed_base, int max_bounce, int hero_c,
               int threads, double* film_xyz, double* film_hits, double* energy,
               int64_t* rays, int32_t* fate, double* beta) {
     const Scene& scene = static_cast<Ref*>(h)->scene;
@@ -214,7 +214,10 @@ int ftr_trace(void* h, const ftb_camera* cam, int64_t n, uint64_t seed_base, int
     for (auto& f : films) { f.resX = rx; f.resY = ry; f.alloc(); }
     auto worker = [&](int tid) {
         Renderer r;
-        r.useHero = false; r.heroC = 1; r.maxBounce = max_bounce;
+        // hero sampling as renderForward sets it (main.cpp:11309-11315): -heroc clamped to
+        // [1, kHeroMax], on only without media
+        const int hc = hero_c < 1 ? 1 : (hero_c > hero::kHeroMax ? hero::kHeroMax : hero_c);
+        r.useHero = hc > 1 && scene.media.empty(); r.heroC = hc; r.maxBounce = max_bounce;
         Pcg32 rng;
         long long lo = n * tid / threads, hi = n * (tid + 1) / threads;
         for (long long i = lo; i < hi; ++i) {

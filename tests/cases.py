@@ -56,13 +56,17 @@ def make_instances(L, ramp=0.01, cauchy=True):
 
 
 CASES = {
-    # name: (builder, res, photons, max_bounce, seed_base)
-    "cornell": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 0),
-    "cornell_seed": (lambda L: scenes.make_cornell(L), 32, 4096, 8, 123456789),
-    "glass": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 0),
-    "fog_strands": (lambda L: scenes.make_fog_strands(L, n_strands=500), 32, 8192, 32, 0),
-    "materials": (make_materials, 32, 8192, 16, 7),
-    "instances": (make_instances, 32, 8192, 16, 11),
+    # name: (builder, res, photons, max_bounce, seed_base, wavelengths per photon)
+    "cornell": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 0, 1),
+    "cornell_seed": (lambda L: scenes.make_cornell(L), 32, 4096, 8, 123456789, 1),
+    "glass": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 0, 1),
+    "fog_strands": (lambda L: scenes.make_fog_strands(L, n_strands=500), 32, 8192, 32, 0, 1),
+    "materials": (make_materials, 32, 8192, 16, 7, 1),
+    "instances": (make_instances, 32, 8192, 16, 11, 1),
+    # hero-wavelength bundles (Renderer::tracePhotonHero): C wavelengths per photon
+    "cornell_hero4": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 3, 4),
+    "glass_hero4": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 5, 4),
+    "materials_hero3": (make_materials, 32, 8192, 16, 9, 3),
 }
 
 

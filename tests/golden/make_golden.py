@@ -5,8 +5,9 @@ Run where the reference sources are available (they are read only at build time)
     python tests/golden/make_golden.py [case ...]   # all cases when none is named
 
 For every case in tests/cases.py it stores, from Renderer::tracePhoton run single-threaded
-with the reference's per-photon seeding: the energy report, the film (XYZ sums and hits),
-and per photon the number of ray queries, the termination and the final beta.  It also
+with the reference's per-photon seeding (hero-wavelength cases through tracePhotonHero):
+the energy report, the film (XYZ sums and hits), and per photon the number of ray queries,
+the termination and the final beta (the last two meaningful for one wavelength per photon).  It also
 stores the PCG32 streams of a few photon indices, a baked camera and an emission CDF.
 The scene's content hash is stored so that drift in the scene generator is detected.
 """
@@ -28,16 +29,21 @@ def main():
     L = lib.load()
     R = Reference()
     only = set(sys.argv[1:])
-    for name, (mk, res, n, mb, seed) in cases.CASES.items():
+    for name, (mk, res, n, mb, seed, hero) in cases.CASES.items():
         if only and name not in only:
             continue
         d = mk(L)
         cam = cases.camera(L, res)
-        r = R.trace(d, cam, n, seed_base=seed, max_bounce=mb, per_photon=True)
+        # film and energy accumulated like renderForward; per-photon ray counts (and, for one
+        # wavelength per photon, the termination and final beta) from a photon-by-photon run
+        r = R.trace(d, cam, n, seed_base=seed, max_bounce=mb, hero_c=hero)
+        r.update({k: v for k, v in R.trace(d, cam, n, seed_base=seed, max_bounce=mb, per_photon=True,
+                                           hero_c=hero).items() if k in ("rays", "fate", "beta")})
         np.savez_compressed(
             os.path.join(HERE, f"trace_{name}.npz"), scene_hash=np.array(cases.scene_hash(d)),
             energy=r["energy"], xyz=r["xyz"], hits=r["hits"], rays=r["rays"].astype(np.int32),
-            fate=r["fate"].astype(np.int8), beta=r["beta"], res=res, n=n, max_bounce=mb, seed_base=seed)
+            fate=r["fate"].astype(np.int8), beta=r["beta"], res=res, n=n, max_bounce=mb, seed_base=seed,
+            hero_c=hero)
         print(name, r["energy"])
     if only and "streams" not in only:
         return

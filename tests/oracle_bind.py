@@ -37,7 +37,7 @@ class Oracle:
         L.fto_release.argtypes = [C.c_void_p]
         L.fto_trace.restype = C.c_int
         L.fto_trace.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int64, C.c_uint64, C.c_int,
-                                C.c_int, _PD, _PD, _PD, C.POINTER(abi.PhotonLog), _PI64]
+                                C.c_int, C.c_int, _PD, _PD, _PD, C.POINTER(abi.PhotonLog), _PI64]
         L.fto_total_power.restype = C.c_double
         L.fto_total_power.argtypes = [C.c_void_p]
         L.fto_emission_cdf.restype = C.c_int
@@ -59,7 +59,8 @@ class Oracle:
             raise RuntimeError(self.L.fto_last_error().decode())
         return h
 
-    def trace(self, desc, cam, n, seed_base=0, max_bounce=8, threads=1, logs=False, rays=False, ctx=None):
+    def trace(self, desc, cam, n, seed_base=0, max_bounce=8, threads=1, logs=False, rays=False, ctx=None,
+              hero_c=1):
         h = ctx or self.prepare(desc)
         npix = cam.res_x * cam.res_y
         xyz = np.zeros((npix, 3))
@@ -68,7 +69,7 @@ class Oracle:
         lg = (abi.PhotonLog * max(1, n))() if logs else None
         ry = np.zeros(max(1, n), dtype=np.int64) if rays else None
         try:
-            r = self.L.fto_trace(h, C.byref(cam), n, seed_base, max_bounce, threads, _ptr(xyz), _ptr(hits),
+            r = self.L.fto_trace(h, C.byref(cam), n, seed_base, max_bounce, hero_c, threads, _ptr(xyz), _ptr(hits),
                                  _ptr(en), lg, _ptr(ry, C.c_int64) if rays else None)
             if r != 0:
                 raise RuntimeError(self.L.fto_last_error().decode())
@@ -121,7 +122,7 @@ class Reference:
         L.ftr_look_at.argtypes = [_PD, _PD, _PD, C.c_double, C.c_int, C.c_int, C.POINTER(abi.Camera)]
         L.ftr_trace.restype = C.c_int
         L.ftr_trace.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int64, C.c_uint64, C.c_int, C.c_int,
-                                _PD, _PD, _PD, _PI64, C.POINTER(C.c_int32), _PD]
+                                C.c_int, _PD, _PD, _PD, _PI64, C.POINTER(C.c_int32), _PD]
         self.L = L
 
     @staticmethod
@@ -131,7 +132,7 @@ class Reference:
     def prepare(self, desc):
         return self.L.ftr_prepare(desc.ref())
 
-    def trace(self, desc, cam, n, seed_base=0, max_bounce=8, threads=1, per_photon=False, ctx=None):
+    def trace(self, desc, cam, n, seed_base=0, max_bounce=8, threads=1, per_photon=False, ctx=None, hero_c=1):
         h = ctx or self.prepare(desc)
         npix = cam.res_x * cam.res_y
         xyz = np.zeros((npix, 3))
@@ -143,7 +144,7 @@ class Reference:
             fate = np.zeros(max(1, n), dtype=np.int32)
             beta = np.zeros(max(1, n))
         try:
-            r = self.L.ftr_trace(h, C.byref(cam), n, seed_base, max_bounce, threads, _ptr(xyz), _ptr(hits),
+            r = self.L.ftr_trace(h, C.byref(cam), n, seed_base, max_bounce, hero_c, threads, _ptr(xyz), _ptr(hits),
                                  _ptr(en), _ptr(rays, C.c_int64) if per_photon else None,
                                  _ptr(fate, C.c_int32) if per_photon else None,
                                  _ptr(beta) if per_photon else None)

@@ -30,7 +30,7 @@ def golden(name):
 @pytest.fixture(scope="module")
 def scenes_cache(gpu):
     out = {}
-    for name, (mk, res, n, mb, seed) in cases.CASES.items():
+    for name, (mk, res, n, mb, seed, hero) in cases.CASES.items():
         d = mk(gpu)
         out[name] = (d, lib.Scene(d, 0, gpu))
     yield out
@@ -48,7 +48,7 @@ def assert_film_close(film, info, xyz_ref, hits_ref):
 
 @pytest.mark.parametrize("name", sorted(cases.CASES))
 def test_film_and_energy_match_reference_golden(name, scenes_cache, gpu):
-    mk, res, n, mb, seed = cases.CASES[name]
+    mk, res, n, mb, seed, hero = cases.CASES[name]
     d, sc = scenes_cache[name]
     g = golden(f"trace_{name}.npz")
     assert cases.scene_hash(d) == str(g["scene_hash"])
@@ -60,7 +60,7 @@ def test_film_and_energy_match_reference_golden(name, scenes_cache, gpu):
 
 @pytest.mark.parametrize("name", sorted(cases.CASES))
 def test_per_photon_paths_match_oracle(name, scenes_cache, gpu, oracle):
-    mk, res, _, mb, seed = cases.CASES[name]
+    mk, res, _, mb, seed, hero = cases.CASES[name]
     d, sc = scenes_cache[name]
     n = 1 << 15
     cam = cases.camera(gpu, res)
@@ -78,7 +78,7 @@ def test_per_photon_paths_match_oracle(name, scenes_cache, gpu, oracle):
 def test_device_build_paths_match_oracle(name, gpu, oracle):
     """The GPU-built linear BVH culls differently but must find the same hits: per-photon
     paths equal the oracle's under the same allowance as the host-built tree."""
-    mk, res, _, mb, seed = cases.CASES[name]
+    mk, res, _, mb, seed, hero = cases.CASES[name]
     d = mk(gpu)
     sc = lib.Scene(d, 0, gpu, build=abi.BUILD_DEVICE)
     n = 1 << 14

@@ -33,7 +33,7 @@ def shim(gpu):
     L.ftshim_render.restype = C.c_int
     L.ftshim_render.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int64, C.c_uint64, C.c_int, PD, PD, PD]
     L.ftr_trace.restype = C.c_int
-    L.ftr_trace.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int64, C.c_uint64, C.c_int, C.c_int,
+    L.ftr_trace.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int64, C.c_uint64, C.c_int, C.c_int, C.c_int,
                             PD, PD, PD, C.POINTER(C.c_int64), C.POINTER(C.c_int32), PD]
     return L
 
@@ -59,7 +59,7 @@ def test_render_forward_cuda_through_shim(shim, gpu, scene):
         P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
         assert shim.ftshim_render(ref, C.byref(cam), n, seed, mb, P(xyz), P(hits), P(en)) == 0
         cx, ch, ce = np.zeros(npix * 3), np.zeros(npix), np.zeros(5)
-        assert shim.ftr_trace(ref, C.byref(cam), n, seed, mb, 1, P(cx), P(ch), P(ce), None, None, None) == 0
+        assert shim.ftr_trace(ref, C.byref(cam), n, seed, mb, 1, 1, P(cx), P(ch), P(ce), None, None, None) == 0
     finally:
         shim.ftr_release(ref)
     # the shim bakes per call with the GPU-built tree unless the budget exceeds 4096 photons per

@@ -51,28 +51,30 @@ def test_emission_cdf_and_power(oracle, L):
 
 @pytest.mark.parametrize("name", sorted(cases.CASES))
 def test_trace_matches_golden(name, oracle, L):
-    mk, res, n, mb, seed = cases.CASES[name]
+    mk, res, n, mb, seed, hero = cases.CASES[name]
     g = golden(f"trace_{name}.npz")
     d = mk(L)
     assert cases.scene_hash(d) == str(g["scene_hash"]), "scene generator drifted from the golden scene"
     cam = cases.camera(L, res)
-    o = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, rays=True)
+    o = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, rays=True, hero_c=hero)
     np.testing.assert_array_equal(o["energy"], g["energy"])
     np.testing.assert_array_equal(o["xyz"], g["xyz"])
     np.testing.assert_array_equal(o["hits"], g["hits"])
     np.testing.assert_array_equal(o["rays"], g["rays"])
-    np.testing.assert_array_equal(o["logs"]["fate"], g["fate"])
-    np.testing.assert_array_equal(o["logs"]["beta"], g["beta"])
+    if hero == 1:   # with a bundle, absorption is booked along the way: no single fate
+        np.testing.assert_array_equal(o["logs"]["fate"], g["fate"])
+        np.testing.assert_array_equal(o["logs"]["beta"], g["beta"])
 
 
-@pytest.mark.parametrize("name", ["cornell", "materials", "fog_strands"])
-def test_trace_matches_reference_live(name, oracle, reference, L):
-    mk, res, n, mb, _ = cases.CASES[name]
+@pytest.mark.parametrize("name,hero", [("cornell", 1), ("materials", 1), ("fog_strands", 1), ("materials", 4),
+                                       ("instances", 8), ("fog_strands", 4)])
+def test_trace_matches_reference_live(name, hero, oracle, reference, L):
+    mk, res, n, mb, _, _ = cases.CASES[name]
     d = mk(L)
     cam = cases.camera(L, 48)
     for seed, threads, count in ((555, 1, 6000), (10**9, 4, 20000)):
-        o = oracle.trace(d, cam, count, seed_base=seed, max_bounce=mb, threads=threads)
-        r = reference.trace(d, cam, count, seed_base=seed, max_bounce=mb, threads=threads)
+        o = oracle.trace(d, cam, count, seed_base=seed, max_bounce=mb, threads=threads, hero_c=hero)
+        r = reference.trace(d, cam, count, seed_base=seed, max_bounce=mb, threads=threads, hero_c=hero)
         np.testing.assert_array_equal(o["energy"], r["energy"])
         np.testing.assert_array_equal(o["xyz"], r["xyz"])
         np.testing.assert_array_equal(o["hits"], r["hits"])

@@ -491,6 +491,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--photons", type=int, default=0, help="photons per step (default: the workload's frame)")
     ap.add_argument("--tuning", default="", help="wave_slots,blocks_per_sm,graphs instead of the autotuner")
+    ap.add_argument("--hero", type=int, default=1, help="wavelengths per photon (hero bundles when > 1)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -521,6 +522,8 @@ def main():
         n = args.photons
         cfg["photons_per_frame"] = n
     cfg["parallelism"] = f"photon-index shards x{world} (weak), NCCL int64 film sum at frame end" if world > 1 else "single GPU"
+    if args.hero > 1:
+        cfg["wavelengths_per_photon"] = f"{args.hero} (hero bundles)"
     cfg["l2"] = "flushed between timed steps (256 MiB write)"
     L = lib.load()
     desc = make_scene(args.workload, args.level, L)
@@ -554,9 +557,9 @@ def main():
         film.zero_()
         if dist is None:
             sc.render_device(cam, n, film.data_ptr(), seed_base=k * n, max_bounce=mb, frac_bits=frac,
-                             stream=stream.cuda_stream)
+                             stream=stream.cuda_stream, hero_c=args.hero)
         else:   # the frame is n photons per rank; each rank traces its index shard
-            multigpu.render_sharded(sc, cam, n * world, film, seed_base=k * n * world, max_bounce=mb,
+            multigpu.render_sharded(sc, cam, n * world, film, seed_base=k * n * world, max_bounce=mb, hero_c=args.hero,
                                     dst=0, stream=stream.cuda_stream)
 
     # autotuner (untimed): grid size, wave size and graph replay for this workload
@@ -565,7 +568,7 @@ def main():
         slots, grid, graphs = (int(x) for x in args.tuning.split(","))
         tuning = L.set_tuning(local, wave_slots=slots, grid_mult=grid, use_graphs=graphs)
     else:
-        tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)
+        tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)   # (one wavelength per photon)
     cfg["tuning"] = {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
                      "graph_replay": bool(tuning.use_graphs), "autotune_s": round(time.perf_counter() - t, 2)}
 
@@ -657,7 +660,7 @@ def main():
         flush.fill_(k & 0xff)
         torch.cuda.synchronize(dev)
         t = time.perf_counter()
-        sc.render(cam, n, seed_base=(1 << 53) + (k * world + rank) * n, max_bounce=mb, out=host_np)
+        sc.render(cam, n, seed_base=(1 << 53) + (k * world + rank) * n, max_bounce=mb, out=host_np, hero_c=args.hero)
         e_times.append(time.perf_counter() - t)
     e_total = sum(e_times)
     if dist is not None:

@@ -92,7 +92,8 @@ class Camera(C.Structure):
 
 class RenderParams(C.Structure):
     _fields_ = [("n_photons", C.c_int64), ("seed_base", C.c_uint64),
-                ("max_bounce", C.c_int32), ("frac_bits", C.c_int32)]
+                ("max_bounce", C.c_int32), ("frac_bits", C.c_int32), ("hero_c", C.c_int32),
+                ("pad", C.c_int32)]
 
 
 class Energy(C.Structure):
@@ -120,7 +121,8 @@ class PhotonLog(C.Structure):
 
 class Job(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("cam", Camera), ("d_film", C.c_void_p), ("n_photons", C.c_int64),
-                ("seed_base", C.c_uint64), ("max_bounce", C.c_int32), ("frac_bits", C.c_int32)]
+                ("seed_base", C.c_uint64), ("max_bounce", C.c_int32), ("frac_bits", C.c_int32),
+                ("hero_c", C.c_int32), ("pad", C.c_int32)]
 
 
 class KernelProfile(C.Structure):
@@ -134,13 +136,13 @@ class Tuning(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_active", C.c_int32), ("film_budget", C.c_uint64),
-                ("wave_slots", C.c_int32), ("pad", C.c_int32)]
+                ("wave_slots", C.c_int32), ("hero_max", C.c_int32)]
 
 
 class Request(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("cam", Camera), ("n_photons", C.c_int64),
                 ("seed_base", C.c_uint64), ("max_bounce", C.c_int32), ("frac_bits", C.c_int32),
-                ("host_film", C.POINTER(C.c_int64))]
+                ("hero_c", C.c_int32), ("pad", C.c_int32), ("host_film", C.POINTER(C.c_int64))]
 
 
 class JobResult(C.Structure):

@@ -549,8 +549,11 @@ DevCam dev_cam(const ftb_camera* c) {
     return d;
 }
 
-ftb_status ensure_waves(ftb_scene* s, int32_t W, bool log) {
-    if (s->eng->wave_W >= W && s->eng->wave_log == log && s->eng->waves[0].block) return FTB_OK;
+ftb_status ensure_waves(ftb_scene* s, int32_t W, bool log, int32_t hero = 1) {
+    if (s->eng->wave_W >= W && s->eng->wave_log == log && s->eng->waves[0].block && s->eng->waves[0].hero >= hero)
+        return FTB_OK;
+    hero = std::max(hero, s->eng->waves[0].block ? s->eng->waves[0].hero : 1);   // keep the bundle room
+    if (s->eng->wave_log == log) W = std::max(W, s->eng->wave_W);
     for (auto& w : s->eng->waves) ftb::wave_free(w);
     for (auto& g : s->eng->graphs) {   // captured graphs hold the old buffers' addresses
         ftb::wave_graphs_destroy(g);
@@ -558,7 +561,7 @@ ftb_status ensure_waves(ftb_scene* s, int32_t W, bool log) {
     }
     s->eng->wave_W = 0;
     for (auto& w : s->eng->waves) {
-        cudaError_t e = ftb::wave_alloc(w, W, log);
+        cudaError_t e = ftb::wave_alloc(w, W, log, hero);
         if (e != cudaSuccess) return cuda_fail(e, "wave allocation");
     }
     for (auto& st : s->eng->streams)
@@ -587,8 +590,15 @@ int32_t pick_wave(int64_t n, int32_t cap) {
     return (int32_t)std::max<int64_t>(W, 1);
 }
 
+// Wavelengths a photon of this scene carries for a requested -heroc: clamped to
+// [1, kHeroMax], and 1 in scenes with media (main.cpp:11309-11312, hero.h:81-86).
+int32_t effective_hero(const ftb_scene* s, int32_t hero_c) {
+    if (hero_c <= 1 || s->dev.n_med > 0) return 1;
+    return hero_c > ftb::kHeroMax ? ftb::kHeroMax : hero_c;
+}
+
 ftb::DevJob make_job(const ftb_scene* s, const ftb_camera* cam, int64_t* d_film, unsigned long long* d_tally,
-                     int32_t frac_bits, int32_t max_bounce) {
+                     int32_t frac_bits, int32_t max_bounce, int32_t hero_c = 1) {
     ftb::DevJob J;
     std::memset(&J, 0, sizeof J);
     J.sc = s->dev;
@@ -598,6 +608,7 @@ ftb::DevJob make_job(const ftb_scene* s, const ftb_camera* cam, int64_t* d_film,
     J.film_scale_inv = std::ldexp(1.0, frac_bits) / s->power;
     J.tally_scale_inv = std::ldexp(1.0, 32) / s->power;
     J.max_bounce = max_bounce;
+    J.hero_c = effective_hero(s, hero_c);
     return J;
 }
 
@@ -611,9 +622,13 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
                     const std::vector<uint64_t>& seed, bool log, ftb_photon_log* d_logs, int64_t log_base,
                     cudaStream_t user_stream) {
     int64_t total = 0;
-    for (auto c : count) total += c;
+    int32_t hero = 1;
+    for (size_t i = 0; i < count.size(); ++i) {
+        total += count[i];
+        hero = std::max(hero, base[i].hero_c);
+    }
     int32_t W = pick_wave(total, s->eng->wave_cap);
-    ftb_status st = ensure_waves(s, W, log);   // may keep larger buffers; waves use W slots
+    ftb_status st = ensure_waves(s, W, log, hero);   // may keep larger buffers; waves use W slots
     if (st != FTB_OK) return st;
     ftb::Frame f;
     f.stats = s->prof_mode == 2 ? s->stats : nullptr;
@@ -630,9 +645,13 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         table.clear();
         int32_t slots = 0, max_bounce = 0;
         bool inst = false;
+        int bundles = -1;   // a wave holds either one-wavelength jobs or bundles, not both
         while (j < base.size() && slots < W && (int)table.size() < ftb::kWaveJobs) {
             int64_t left = count[j] - done_in_job;
             if (left <= 0) { ++j; done_in_job = 0; continue; }
+            const int is_bundle = base[j].hero_c > 1 ? 1 : 0;
+            if (bundles >= 0 && is_bundle != bundles) break;
+            bundles = is_bundle;
             int32_t m = (int32_t)std::min<int64_t>(left, (int64_t)(W - slots));
             ftb::DevJob J = base[j];
             J.photon0 = seed[j] + (uint64_t)done_in_job;
@@ -652,8 +671,8 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         w.log_base = log_base;
         cudaError_t e = s->eng->stage[k & 1].push(table.data(), (int)table.size(), slots, w, ws);
         if (e != cudaSuccess) return cuda_fail(e, "job table upload");
-        e = ftb::launch_wave(w, max_bounce, inst, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
-                             s->eng->graphs[k & 1]);
+        e = ftb::launch_wave(w, max_bounce, inst, bundles == 1, f, s->sms, s->eng->shape, ws,
+                             s->prof_mode ? s->prof : nullptr, s->eng->graphs[k & 1]);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         ++k;
     }
@@ -668,8 +687,8 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
 // Trace n photons from seed_base into d_film / tally, on the scene's streams.
 ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t seed_base, int32_t max_bounce,
                        int32_t frac_bits, int64_t* d_film, unsigned long long* d_tally, ftb_photon_log* d_logs,
-                       cudaStream_t user_stream) {
-    std::vector<ftb::DevJob> base{make_job(s, cam, d_film, d_tally, frac_bits, max_bounce)};
+                       cudaStream_t user_stream, int32_t hero_c = 1) {
+    std::vector<ftb::DevJob> base{make_job(s, cam, d_film, d_tally, frac_bits, max_bounce, hero_c)};
     return run_jobs(s, base, {n}, {seed_base}, d_logs != nullptr, d_logs, (int64_t)seed_base, user_stream);
 }
 
@@ -1153,7 +1172,8 @@ ftb_status ftb_render_forward_device(ftb_scene* s, const ftb_camera* cam, const 
     cudaStream_t us = (cudaStream_t)stream;
     CK(cudaMemsetAsync(s->eng->tally, 0, 8 * sizeof(unsigned long long), us), "memset");
     CK(cudaMemsetAsync(s->eng->status, 0, 64, us), "memset");
-    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, d_film, s->eng->tally, nullptr, us);
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, d_film, s->eng->tally, nullptr, us,
+                     p->hero_c);
     if (st != FTB_OK) return st;
     if (info) { info->frac_bits = frac; info->scale = s->power * std::ldexp(1.0, -frac); info->power_ref = s->power; }
     if (energy) {
@@ -1181,7 +1201,8 @@ ftb_status ftb_render_forward(ftb_scene* s, const ftb_camera* cam, const ftb_ren
     CK(cudaMemset(s->eng->film, 0, words * sizeof(int64_t)), "memset film");
     CK(cudaMemset(s->eng->tally, 0, 8 * sizeof(unsigned long long)), "memset tally");
     CK(cudaMemset(s->eng->status, 0, 64), "memset status");
-    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, nullptr, nullptr);
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, nullptr,
+                     nullptr, p->hero_c);
     if (st != FTB_OK) return st;
     CK(cudaDeviceSynchronize(), "render");
     st = read_status(s);
@@ -1229,7 +1250,8 @@ ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n, ftb_film_info* infos
     for (int j = 0; j < n; ++j) {
         const ftb_job& b = jobs[j];
         int frac = b.frac_bits > 0 ? b.frac_bits : default_frac_bits(b.n_photons);
-        base.push_back(make_job(b.scene, &b.cam, b.d_film, s->eng->batch_tally + 8 * (size_t)j, frac, b.max_bounce));
+        base.push_back(make_job(b.scene, &b.cam, b.d_film, s->eng->batch_tally + 8 * (size_t)j, frac, b.max_bounce,
+                                b.hero_c));
         count.push_back(b.n_photons);
         seed.push_back(b.seed_base);
         if (infos) {
@@ -1269,7 +1291,8 @@ ftb_status ftb_trace_log(ftb_scene* s, const ftb_camera* cam, const ftb_render_p
     cudaMemset(s->eng->film, 0, words * sizeof(int64_t));
     cudaMemset(s->eng->tally, 0, 8 * sizeof(unsigned long long));
     cudaMemset(s->eng->status, 0, 64);
-    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, d_logs, nullptr);
+    st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, d_logs,
+                     nullptr, p->hero_c);
     if (st == FTB_OK) {
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) st = cuda_fail(e, "trace_log");

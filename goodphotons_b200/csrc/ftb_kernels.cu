@@ -1031,6 +1031,42 @@ __device__ __forceinline__ void log_finish(const Wave& w, int slot, uint64_t pho
     for (int k = 0; k < 8; ++k) L.prims[k] = w.lprims[k * w.W + slot];
 }
 
+// ------------------------------------------------------------------ emission -----------
+// Scene::selectEmitter (scene.h:1851-1857): no draw with one emitter.
+__device__ __forceinline__ int select_emitter(const DevScene& sc, Pcg& rng) {
+    if (sc.n_emit <= 1) return 0;
+    double u = uniform(rng);
+    int lo = 0, hi = sc.n_emit - 1;
+    while (lo < hi) { int mid = (lo + hi) / 2; if (sc.emit_cdf[mid] < u) lo = mid + 1; else hi = mid; }
+    return lo;
+}
+// Emitter::samplePoint (scene.h:815-880) and the emission direction (render.h:1938-1941)
+__device__ __forceinline__ void emit_sample(const DevEmit& em, Pcg& rng, D3& origin, D3& emit_n, D3& dir) {
+    double u1 = uniform(rng), u2 = uniform(rng);
+    if (em.shape == FTB_EMIT_SPHERE) {
+        double z = 1.0 - 2.0 * u1;
+        double s = 1.0 - z * z;
+        double r = sqrt(s > 0.0 ? s : 0.0);
+        double phi = 2.0 * PI_D * u2;
+        D3 d = mk(r * cos(phi), r * sin(phi), z);
+        emit_n = d;
+        origin = ld3(em.origin) + d * em.radius;
+    } else {
+        origin = ld3(em.origin) + ld3(em.u) * u1 + ld3(em.v) * u2;
+        emit_n = ld3(em.normal);
+    }
+    dir = em.collimated ? ld3(em.beam) : cosine_hemisphere(emit_n, rng);
+}
+// EmissionSampler::sampleAt (spectrum.h:374-383)
+__device__ __forceinline__ double sample_at(const DevEmit& em, double u, double& pdf) {
+    int lo = 0, hi = em.n;
+    while (lo + 1 < hi) { int mid = (lo + hi) / 2; if (em.cdf[mid] <= u) lo = mid; else hi = mid; }
+    double c0 = em.cdf[lo], c1 = em.cdf[lo + 1];
+    double frac = (c1 > c0) ? (u - c0) / (c1 - c0) : 0.5;
+    pdf = (c1 - c0) / em.step;
+    return LAMBDA_MIN + (lo + frac) * em.step;
+}
+
 // ------------------------------------------------------------------ kernels ------------
 __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f) {
     const int32_t n_jobs = w.params[0], n_slots = w.params[1];
@@ -1054,37 +1090,12 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
             for (int q = 0; q < 8; ++q) w.lprims[q * w.W + slot] = -2;
         }
         if (sc.total_power <= 0.0 || sc.n_emit == 0) { log_finish(w, slot, k, 4, 0.0); continue; }
-        int ei = 0;
-        if (sc.n_emit > 1) {   // Scene::selectEmitter (scene.h:1851-1857)
-            double u = uniform(rng);
-            int lo = 0, hi = sc.n_emit - 1;
-            while (lo < hi) { int mid = (lo + hi) / 2; if (sc.emit_cdf[mid] < u) lo = mid + 1; else hi = mid; }
-            ei = lo;
-        }
+        const int ei = select_emitter(sc, rng);
         const DevEmit& em = sc.emit[ei];
-        double u1 = uniform(rng), u2 = uniform(rng);
-        D3 origin, emit_n;
-        if (em.shape == FTB_EMIT_SPHERE) {   // Emitter::samplePoint (scene.h:815-880)
-            double z = 1.0 - 2.0 * u1;
-            double s = 1.0 - z * z;
-            double r = sqrt(s > 0.0 ? s : 0.0);
-            double phi = 2.0 * PI_D * u2;
-            D3 d = mk(r * cos(phi), r * sin(phi), z);
-            emit_n = d;
-            origin = ld3(em.origin) + d * em.radius;
-        } else {
-            origin = ld3(em.origin) + ld3(em.u) * u1 + ld3(em.v) * u2;
-            emit_n = ld3(em.normal);
-        }
-        D3 dir = em.collimated ? ld3(em.beam) : cosine_hemisphere(emit_n, rng);
-        // EmissionSampler::sampleAt (spectrum.h:374-383)
-        double u = uniform(rng);
-        int lo = 0, hi = em.n;
-        while (lo + 1 < hi) { int mid = (lo + hi) / 2; if (em.cdf[mid] <= u) lo = mid; else hi = mid; }
-        double c0 = em.cdf[lo], c1 = em.cdf[lo + 1];
-        double frac = (c1 > c0) ? (u - c0) / (c1 - c0) : 0.5;
-        double lam = LAMBDA_MIN + (lo + frac) * em.step;
-        double pdf = (c1 - c0) / em.step;
+        D3 origin, emit_n, dir;
+        emit_sample(em, rng, origin, emit_n, dir);
+        double pdf;
+        double lam = sample_at(em, uniform(rng), pdf);
         if (pdf <= 0) { log_finish(w, slot, k, 4, 0.0); continue; }
         double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
         beta *= 1.0;
@@ -1429,12 +1440,373 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
     }
 }
 
+// ------------------------------------------------------------------ hero bundles -------
+// Hero-wavelength sampling (Renderer::tracePhotonHero / tracePhotonHeroLoop, render.h:
+// 2252-2631; the policies of hero.h:28-70): a photon carries C wavelengths drawn from one
+// stratified variate; the hero decides the geometry, analog Russian roulette uses the
+// maximum over the live wavelengths with the bounded reweights booked as absorption, and a
+// dielectric de-heroes (the hero goes on alone, its beta times C).  A camera connection
+// tests occlusion once and splats every live wavelength.  The reference runs bundles only
+// in scenes without media, and so does this path (the host sends such jobs to the scalar
+// kernels).
+
+__device__ __forceinline__ void push_shadow_hero(const Wave& w, const Frame& f, int job, D3 o, D3 d, double tmax,
+                                                 int nup, const double* lam, const double* val, int pix) {
+    int i = agg_inc(&w.counts[2]);
+    if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
+    w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
+    w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
+    w.smax[i] = tmax; w.spix[i] = pix; w.sjob[i] = job;
+    w.slam[i] = lam[0]; w.sval[i] = val[0];
+    for (int k = 1; k < nup; ++k) {
+        w.xlam[(size_t)(k - 1) * w.S + i] = lam[k];
+        w.xval[(size_t)(k - 1) * w.S + i] = val[k];
+    }
+    w.snup[i] = nup;
+}
+
+// connectHero (render.h:564-577): one connectGeom, a contribution per live wavelength
+__device__ void connect_surface_hero(const DevCam& cam, const Wave& w, const Frame& f, int job, D3 p, D3 n,
+                                     D3 ng, D3 wi, const double* lam, const double* beta, const double* rho,
+                                     int nup) {
+    D3 to_cam = ld3(cam.eye) - p;
+    double dist = len(to_cam);
+    D3 wdir = to_cam / dist;
+    double cos_surf = dot(n, wdir);
+    if (cos_surf <= 0) return;
+    double stg = shadow_terminator_g(wdir, n, ng);
+    if (stg <= 0.0) return;
+    int px, py; double cos_cam, dist2;
+    if (!cam_project(cam, p, px, py, cos_cam, dist2)) return;
+    double omega = cam_pixel_solid_angle(cam, cos_cam);
+    double corr = shading_adjoint_corr(wi, wdir, n, ng);
+    double denom = dist2 * omega;
+    double val[kHeroMax];
+    for (int i = 0; i < nup; ++i) {
+        double fr = rho[i] / PI_D;
+        val[i] = beta[i] * fr * cos_surf * corr / denom * stg;
+    }
+    push_shadow_hero(w, f, job, p + ng * 1e-6, wdir, dist - 2e-6, nup, lam, val, py * cam.rx + px);
+}
+
+__device__ __forceinline__ double sum_of(const double* a, int n) {   // activeSum (render.h:2324)
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += a[i];
+    return s;
+}
+__device__ __forceinline__ double max_of(const double* a, int n) {   // hero::maxOf (hero.h:120-126)
+    double m = a[0];
+    for (int i = 1; i < n; ++i) if (a[i] > m) m = a[i];
+    return m;
+}
+
+__global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f) {
+    const int32_t n_jobs = w.params[0], n_slots = w.params[1];
+    const bool multi = n_jobs > 1;
+    TallyAcc acc;
+    tally_init(acc);
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n_slots; slot += gridDim.x * blockDim.x) {
+        int j = 0;
+        if (multi) {
+            int lo = 0, hi = n_jobs - 1;
+            while (lo < hi) { int mid = (lo + hi + 1) / 2; if (jobs[mid].slot0 <= slot) lo = mid; else hi = mid - 1; }
+            j = lo;
+            w.job[slot] = j;
+        }
+        const DevJob& J = jobs[j];
+        const DevScene& sc = J.sc;
+        const int C = J.hero_c;
+        uint64_t k = J.photon0 + (uint64_t)(slot - J.slot0);
+        Pcg rng = seed_photon(k);
+        if (w.logs) {
+            w.lhash[slot] = 1469598103934665603ULL; w.lnh[slot] = 0;
+            for (int q = 0; q < 8; ++q) w.lprims[q * w.W + slot] = -2;
+        }
+        if (sc.total_power <= 0.0 || sc.n_emit == 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        const DevEmit& em = sc.emit[select_emitter(sc, rng)];
+        D3 origin, emit_n, dir;
+        emit_sample(em, rng, origin, emit_n, dir);
+        // hero::sampleBundle (hero.h:100-113): one variate, strata u + i/C wrapped into [0,1)
+        double lam[kHeroMax], beta[kHeroMax], one[kHeroMax];
+        double u = uniform(rng), pdf;
+        lam[0] = sample_at(em, u, pdf);
+        if (pdf <= 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        for (int i = 1; i < C; ++i) {
+            double uu = u + (double)i / (double)C;
+            if (uu >= 1.0) uu -= 1.0;
+            double p2;
+            lam[i] = sample_at(em, uu, p2);
+        }
+        double base = (sc.n_emit == 1) ? em.power : sc.total_power;
+        base *= 1.0;   // spotW
+        for (int i = 0; i < C; ++i) { beta[i] = base / C; one[i] = 1.0; }
+        tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
+        connect_surface_hero(J.cam, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, one, C);
+        D3 ro = origin + dir * 1e-6;
+        if (J.max_bounce <= 0) {
+            tally_add(acc, jobs, multi, j, T_RES, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
+            log_finish(w, slot, k, 2, beta[0]);
+            continue;
+        }
+        w.rng_s[slot] = rng.s; w.rng_i[slot] = rng.inc;
+        w.ox[slot] = ro.x; w.oy[slot] = ro.y; w.oz[slot] = ro.z;
+        w.dx[slot] = dir.x; w.dy[slot] = dir.y; w.dz[slot] = dir.z;
+        for (int i = 0; i < C; ++i) {
+            w.hlam[(size_t)i * w.W + slot] = lam[i];
+            w.hbeta[(size_t)i * w.W + slot] = beta[i];
+        }
+        w.hlive[slot] = C;
+        w.stk_n[slot] = 0;
+        int q = agg_inc(&w.counts[0]);
+        w.qa[q] = slot;
+    }
+    tally_finish(acc, jobs, multi);
+}
+
+__global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, const DevJob* __restrict__ jobs,
+                                                                    Frame f, const int32_t* qin,
+                                                                    const int32_t* qin_count, int32_t* qout,
+                                                                    int32_t* qout_count, int32_t bounce) {
+    const bool multi = w.params[0] > 1;
+    TallyAcc acc;
+    tally_init(acc);
+    int nq = *qin_count;
+    for (int qi0 = blockIdx.x * blockDim.x + threadIdx.x; qi0 < nq; qi0 += gridDim.x * blockDim.x) {
+        int slot = qin[qi0];
+        const int j = multi ? w.job[slot] : 0;
+        const DevJob& J = jobs[j];
+        const DevScene& sc = J.sc;
+        const DevCam& cam = J.cam;
+        const int C = J.hero_c;
+        Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
+        D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
+        int nup = w.hlive[slot];
+        double lam[kHeroMax], beta[kHeroMax];
+        for (int i = 0; i < nup; ++i) {
+            lam[i] = w.hlam[(size_t)i * w.W + slot];
+            beta[i] = w.hbeta[(size_t)i * w.W + slot];
+        }
+        double ht = w.hit_t[slot];
+        int rec = w.hit_rec[slot];
+        Stk stk; stk.n = w.stk_n[slot];
+        for (int k = 0; k < stk.n; ++k) stk.e[k] = w.stk[k * w.W + slot];
+        if (w.logs) {
+            int nh = w.lnh[slot];
+            int prim = rec >= 0 ? sc.recs[rec].prim : -1;
+            uint64_t hsh = fnv_i32(w.lhash[slot], prim);
+            if (rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)
+                hsh = fnv_i32(hsh, sc.inst[rec_inst(sc.recs[rec])].recs[w.hit_sub[slot]].prim);
+            w.lhash[slot] = hsh;
+            if (nh < 8) w.lprims[nh * w.W + slot] = prim;
+            w.lnh[slot] = nh + 1;
+        }
+        const bool valid = rec >= 0;
+        const double d_event = valid ? ht : 1e30;
+        {   // Beer-Lambert per live wavelength (render.h:2389-2398)
+            int mi = stk_top_mat(stk);
+            if (mi >= 0)
+                for (int i = 0; i < nup; ++i) {
+                    double a = spec_slot(sc, sc.mats[mi].absorb, lam[i], 0.0);
+                    if (a > 0.0) beta[i] *= exp(-a * d_event);
+                }
+        }
+        int fate = -1;   // -1 continue, 0 absorbed, 1 escaped
+        D3 no = ro, nd = rd;
+        long long absorbed = 0;   // reweights booked as absorption (fixed point, per add)
+        if (!valid) {
+            fate = 1;
+        } else {
+            PrimRec r;
+            load_rec(sc.recs, rec, r);
+            Hit h;
+            if (rec_type(r) == REC_INST) {
+                instance_hit(sc.inst[rec_inst(r)], w.hit_sub[slot], ro, rd, h);
+                h.prim = r.prim;
+            } else {
+                RayCtx R = make_ray(ro, rd);
+                hit_attributes(sc.tri_n, R, r, h);
+            }
+            const DevMat& m = sc.mats[h.mat];
+            switch (m.type) {
+            case FTB_MAT_DIFFUSE_TRANSMIT: {   // render.h:2454-2503
+                double rr[kHeroMax], rt[kHeroMax];
+                for (int i = 0; i < nup; ++i) {
+                    double a = clamp01(spec_slot(sc, m.reflect, lam[i], 0.5));
+                    double b = clamp01(spec_slot(sc, m.transmit, lam[i], 0.0));
+                    double s = a + b;
+                    if (s > 1.0) { a /= s; b /= s; }
+                    rr[i] = a; rt[i] = b;
+                }
+                D3 ngo = oriented_geo_n(h);
+                D3 wi = mk(-rd.x, -rd.y, -rd.z);
+                connect_surface_hero(cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr, nup);
+                connect_surface_hero(cam, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt, nup);
+                double q_r = max_of(rr, nup), q_t = max_of(rt, nup);
+                double sum_h = q_r + q_t;
+                if (nup > 1 && sum_h > 1.0) { q_r /= sum_h; q_t /= sum_h; sum_h = q_r + q_t; }
+                double uu = uniform(rng);
+                if (uu < q_r || uu < sum_h) {
+                    const bool front = uu < q_r;
+                    for (int i = 0; i < nup; ++i) {
+                        double wgt = (front ? rr[i] : rt[i]) / (front ? q_r : q_t);
+                        absorbed += to_fixed(beta[i] * (1.0 - wgt), J.tally_scale_inv, f.status);
+                        beta[i] *= wgt;
+                    }
+                    D3 wo = cosine_hemisphere(front ? h.n : mk(-h.n.x, -h.n.y, -h.n.z), rng);
+                    double corr = shading_adjoint_corr(wi, wo, h.n, ngo);
+                    for (int i = 0; i < nup; ++i) beta[i] *= corr;
+                    no = front ? h.p + h.n * 1e-6 : h.p - h.n * 1e-6;
+                    nd = wo;
+                } else {
+                    fate = 0;
+                }
+                break;
+            }
+            case FTB_MAT_FILTER:
+            case FTB_MAT_GLOSSY: {   // achromatic lobes (render.h:2505-2537)
+                double cc[kHeroMax];
+                for (int i = 0; i < nup; ++i)
+                    cc[i] = (m.type == FTB_MAT_FILTER) ? clamp01(spec_slot(sc, m.transmit, lam[i], 0.0))
+                                                       : clamp01(spec_slot(sc, m.reflect, lam[i], 0.5));
+                double q = max_of(cc, nup);
+                if (uniform(rng) >= q) { fate = 0; break; }
+                for (int i = 0; i < nup; ++i) {
+                    double wgt = cc[i] / q;
+                    absorbed += to_fixed(beta[i] * (1.0 - wgt), J.tally_scale_inv, f.status);
+                    beta[i] *= wgt;
+                }
+                if (m.type == FTB_MAT_FILTER) {
+                    no = h.p + rd * 1e-6;
+                } else {
+                    D3 o = sample_glossy(reflect(rd, h.n), m.roughness, rng);
+                    if (dot(o, h.n) <= 0) { fate = 0; break; }
+                    no = h.p + h.n * 1e-6; nd = o;
+                }
+                break;
+            }
+            case FTB_MAT_DIELECTRIC: {   // de-hero, then the scalar interaction (render.h:2539-2589)
+                if (nup > 1) { beta[0] *= (double)C; nup = 1; }
+                const double lam0 = lam[0];
+                bool entering = dot(rd, h.ng) < 0.0;
+                int mi = h.mat, pr = m.priority;
+                bool has_pri = pr != INT_MIN;
+                bool transmitted = false;
+                if (entering) {
+                    int out_mat = stk_top_mat(stk), out_pri = stk_top_pri(stk);
+                    bool ranked = has_pri && (stk.n == 0 || (out_mat >= 0 && sc.mats[out_mat].priority != INT_MIN));
+                    if (ranked && stk.n != 0 && pr <= out_pri) {
+                        stk_push(stk, mi, pr, f.status);
+                        no = h.p + rd * 1e-6;
+                    } else {
+                        double ext = (ranked && out_mat >= 0) ? mat_ior(sc, sc.mats[out_mat], lam0) : 1.0;
+                        refract_or_reflect(sc, m, h, rd, lam0, rng, transmitted, ext, no, nd);
+                        if (transmitted) stk_push(stk, mi, pr, f.status);
+                    }
+                } else {
+                    Stk after = stk;
+                    stk_pop_mat(after, mi);
+                    int new_mat = stk_top_mat(after), new_pri = stk_top_pri(after);
+                    bool ranked = has_pri && (after.n == 0 || (new_mat >= 0 && sc.mats[new_mat].priority != INT_MIN));
+                    if (ranked && new_mat >= 0 && pr <= new_pri) {
+                        stk_pop_mat(stk, mi);
+                        no = h.p + rd * 1e-6;
+                    } else {
+                        double ext = (ranked && new_mat >= 0) ? mat_ior(sc, sc.mats[new_mat], lam0) : 1.0;
+                        refract_or_reflect(sc, m, h, rd, lam0, rng, transmitted, ext, no, nd);
+                        if (transmitted) stk_pop_mat(stk, mi);
+                    }
+                }
+                break;
+            }
+            default: {   // Diffuse (render.h:2591-2625)
+                double rho[kHeroMax];
+                for (int i = 0; i < nup; ++i) rho[i] = clamp01(spec_slot(sc, m.reflect, lam[i], 0.5));
+                D3 ngo = oriented_geo_n(h);
+                D3 wi = mk(-rd.x, -rd.y, -rd.z);
+                connect_surface_hero(cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho, nup);
+                double q = max_of(rho, nup);
+                if (uniform(rng) >= q) { fate = 0; break; }
+                for (int i = 0; i < nup; ++i) {
+                    double wgt = rho[i] / q;
+                    absorbed += to_fixed(beta[i] * (1.0 - wgt), J.tally_scale_inv, f.status);
+                    beta[i] *= wgt;
+                }
+                D3 wo = cosine_hemisphere(h.n, rng);
+                double corr = shading_adjoint_corr(wi, wo, h.n, ngo);
+                for (int i = 0; i < nup; ++i) beta[i] *= corr;
+                no = h.p + h.n * 1e-6; nd = wo;
+                break;
+            }
+            }
+        }
+        if (absorbed) tally_add(acc, jobs, multi, j, T_ABS, absorbed);
+        uint64_t photon = J.photon0 + (uint64_t)(slot - J.slot0);
+        if (fate >= 0) {
+            tally_add(acc, jobs, multi, j, fate == 0 ? T_ABS : T_ESC,
+                      to_fixed(sum_of(beta, nup), J.tally_scale_inv, f.status));
+            log_finish(w, slot, photon, fate, beta[0]);
+            continue;
+        }
+        if (bounce + 1 >= J.max_bounce) {
+            tally_add(acc, jobs, multi, j, T_RES, to_fixed(sum_of(beta, nup), J.tally_scale_inv, f.status));
+            log_finish(w, slot, photon, 2, beta[0]);
+            continue;
+        }
+        w.rng_s[slot] = rng.s;
+        w.ox[slot] = no.x; w.oy[slot] = no.y; w.oz[slot] = no.z;
+        w.dx[slot] = nd.x; w.dy[slot] = nd.y; w.dz[slot] = nd.z;
+        for (int i = 0; i < nup; ++i) w.hbeta[(size_t)i * w.W + slot] = beta[i];
+        w.hlive[slot] = nup;
+        w.stk_n[slot] = stk.n;
+        for (int k = 0; k < stk.n; ++k) w.stk[k * w.W + slot] = stk.e[k];
+        int qo = agg_inc(qout_count);
+        qout[qo] = slot;
+    }
+    tally_finish(acc, jobs, multi);
+}
+
+// Connections of bundles: one occlusion test, then a splat per wavelength.
+template <bool COUNT, bool INST>
+__global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, const DevJob* __restrict__ jobs,
+                                                                   Frame f) {
+    const int32_t n_jobs = w.params[0];
+    int n = w.counts[2];
+    if (n > w.S) n = w.S;
+    TravCount cnt{0, 0, 0};
+    unsigned long long rays = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const DevJob& J = jobs[n_jobs > 1 ? w.sjob[i] : 0];
+        const DevScene& sc = J.sc;
+        D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
+        double max_dist = w.smax[i];
+        RayCtx R = make_ray(o, d);
+        if (COUNT) rays++;
+        if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
+        long long* px = reinterpret_cast<long long*>(J.film) + 4 * (size_t)w.spix[i];
+        const int nup = w.snup[i];
+        for (int k = 0; k < nup; ++k) {
+            double lam = k == 0 ? w.slam[i] : w.xlam[(size_t)(k - 1) * w.S + i];
+            double c = k == 0 ? w.sval[i] : w.xval[(size_t)(k - 1) * w.S + i];
+            double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
+            atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, f.status));
+            atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, J.film_scale_inv, f.status));
+            atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, J.film_scale_inv, f.status));
+            atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
+        }
+    }
+    if (COUNT) {
+        block_add3(f.stats + 3, rays, cnt.nodes, cnt.recs);
+        block_add1(f.stats + 7, cnt.exact);
+    }
+}
+
 // ------------------------------------------------------------------ host side ----------
-void wave_carve(Wave& w, void* block, int32_t W, bool log) {
+void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     w = Wave{};
     w.W = W;
     w.S = 2 * W;
-    w.bytes = wave_bytes(W, log);
+    w.hero = hero > 1 ? hero : 1;
+    w.bytes = wave_bytes(W, log, hero);
     w.block = block;
     char* p = (char*)block;
     auto take = [&](size_t n) { void* r = p; p += wave_align(n); return r; };
@@ -1457,13 +1829,19 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log) {
     if (log) {
         w.lhash = (uint64_t*)take(8 * wn); w.lnh = (int32_t*)take(4 * wn); w.lprims = (int32_t*)take(4 * wn * 8);
     }
+    if (hero > 1) {
+        const size_t h = (size_t)hero;
+        w.hlam = (double*)take(8 * wn * h); w.hbeta = (double*)take(8 * wn * h); w.hlive = (int32_t*)take(4 * wn);
+        w.xlam = (double*)take(8 * sn * (h - 1)); w.xval = (double*)take(8 * sn * (h - 1));
+        w.snup = (int32_t*)take(4 * sn);
+    }
 }
 
-cudaError_t wave_alloc(Wave& w, int32_t W, bool log) {
+cudaError_t wave_alloc(Wave& w, int32_t W, bool log, int32_t hero) {
     void* block = nullptr;
-    cudaError_t e = cudaMalloc(&block, wave_bytes(W, log));
+    cudaError_t e = cudaMalloc(&block, wave_bytes(W, log, hero));
     if (e != cudaSuccess) { w = Wave{}; return e; }
-    wave_carve(w, block, W, log);
+    wave_carve(w, block, W, log, hero);
     return cudaSuccess;
 }
 
@@ -1477,7 +1855,7 @@ namespace {
 // shading and the connections it queued.  Every launch reads the wave's job count and
 // slot count from w.params, so the same sequence serves any table (and one captured graph
 // serves every wave of its shape).
-void issue_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int grid, cudaStream_t st,
+void issue_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const Frame& f, int grid, cudaStream_t st,
                 LaunchSink* sink) {
     const int T = 128;
     const DevJob* jobs = w.jobs;
@@ -1485,7 +1863,15 @@ void issue_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int grid
     auto mark = [&](int k, bool end) { if (sink) sink->mark(k, end, st); };
     auto shadow = [&]() {
         mark(K_SHADOW, false);
-        if (count) {
+        if (hero) {
+            if (count) {
+                if (inst) k_shadow_hero<true, true><<<grid, T, 0, st>>>(w, jobs, f);
+                else k_shadow_hero<true, false><<<grid, T, 0, st>>>(w, jobs, f);
+            } else {
+                if (inst) k_shadow_hero<false, true><<<grid, T, 0, st>>>(w, jobs, f);
+                else k_shadow_hero<false, false><<<grid, T, 0, st>>>(w, jobs, f);
+            }
+        } else if (count) {
             if (inst) k_shadow<true, true><<<grid, T, 0, st>>>(w, jobs, f);
             else k_shadow<true, false><<<grid, T, 0, st>>>(w, jobs, f);
         } else {
@@ -1497,7 +1883,8 @@ void issue_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int grid
     };
     cudaMemsetAsync(w.counts, 0, 64, st);
     mark(K_EMIT, false);
-    k_emit<<<grid, T, 0, st>>>(w, jobs, f);
+    if (hero) k_emit_hero<<<grid, T, 0, st>>>(w, jobs, f);
+    else k_emit<<<grid, T, 0, st>>>(w, jobs, f);
     mark(K_EMIT, true);
     shadow();
     int32_t* qa = w.qa;
@@ -1516,7 +1903,8 @@ void issue_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int grid
         mark(K_EXTEND, true);
         cudaMemsetAsync(cb, 0, 4, st);
         mark(K_SHADE, false);
-        k_shade<<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+        if (hero) k_shade_hero<<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+        else k_shade<<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
         mark(K_SHADE, true);
         shadow();
         int32_t* tq = qa; qa = qb; qb = tq;
@@ -1528,7 +1916,7 @@ void issue_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int grid
 struct WaveGraphs {
     struct Entry {
         int32_t max_bounce, grid;
-        bool inst;
+        bool inst, hero;
         int32_t* status;
         cudaGraphExec_t exec;
     };
@@ -1541,8 +1929,9 @@ struct WaveGraphs {
 WaveGraphs* wave_graphs_create() { return new WaveGraphs(); }
 void wave_graphs_destroy(WaveGraphs* g) { delete g; }
 
-cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, int32_t sms,
+cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const Frame& f, int32_t sms,
                         const LaunchShape& shape, cudaStream_t st, LaunchSink* sink, WaveGraphs* graphs) {
+    if (hero && w.hero < 2) return cudaErrorInvalidValue;   // the buffer carries no bundles
     const int T = 128;
     int grid = sms * std::max(1, shape.grid_mult);
     const int gw = (w.W + T - 1) / T;   // enough blocks to give every slot a thread
@@ -1550,19 +1939,19 @@ cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool inst, const Frame& f, 
     // A graph bakes the kernel arguments: the wave's buffers and status word are fixed for the
     // life of its cache, but a log buffer changes per call, so logging waves launch directly.
     if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
-        issue_wave(w, max_bounce, inst, f, grid, st, sink);
+        issue_wave(w, max_bounce, inst, hero, f, grid, st, sink);
         return cudaGetLastError();
     }
     for (auto& e : graphs->entries)
-        if (e.max_bounce == max_bounce && e.grid == grid && e.inst == inst && e.status == f.status)
+        if (e.max_bounce == max_bounce && e.grid == grid && e.inst == inst && e.hero == hero && e.status == f.status)
             return cudaGraphLaunch(e.exec, st);
     cudaGraph_t g = nullptr;
     cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) return err;
-    issue_wave(w, max_bounce, inst, f, grid, st, nullptr);
+    issue_wave(w, max_bounce, inst, hero, f, grid, st, nullptr);
     err = cudaStreamEndCapture(st, &g);
     if (err != cudaSuccess) return err;
-    WaveGraphs::Entry e{max_bounce, grid, inst, f.status, nullptr};
+    WaveGraphs::Entry e{max_bounce, grid, inst, hero, f.status, nullptr};
     err = cudaGraphInstantiate(&e.exec, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) return err;

@@ -17,6 +17,7 @@ enum : int32_t {
 };
 
 constexpr int kStkCap = 4;
+constexpr int kHeroMax = 8;      // wavelengths a hero bundle can carry (hero::kHeroMax)
 constexpr int kWaveJobs = 256;   // jobs (frames / requests) one wave can carry
 
 // One job's share of a wave: its scene, camera and film, and the slots [slot0, slot0+n)
@@ -30,7 +31,8 @@ struct DevJob {
     double tally_scale_inv;    // 2^32 / power_ref
     uint64_t photon0;
     int32_t slot0, n;
-    int32_t max_bounce, pad;
+    int32_t max_bounce;
+    int32_t hero_c;            // wavelengths per photon (1: the scalar tracer)
 };
 
 // Per-wave path state, queues and shadow-ray records (structure of arrays, W slots).
@@ -53,6 +55,14 @@ struct Wave {
     int32_t* params;           // [0] jobs in the table, [1] slots in use (written with the table)
     double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
     int32_t* spix;
+    // hero-wavelength bundles (hero > 1 only; null otherwise)
+    int32_t hero;              // wavelengths a path of this buffer can carry
+    double* hlam;              // [hero][W] wavelengths, index 0 the hero
+    double* hbeta;             // [hero][W] per-wavelength throughput
+    int32_t* hlive;            // [W] live wavelengths (hero_c, 1 after a dielectric)
+    double* xlam;              // [hero-1][S] further wavelengths of a connection
+    double* xval;              // [hero-1][S] and their contributions
+    int32_t* snup;             // [S] wavelengths in each connection
     // parity instrumentation (null unless logging)
     uint64_t* lhash;
     int32_t* lnh;
@@ -74,7 +84,7 @@ struct Frame {
 // Bytes of one wave of W slots: every array rounded up to 256 B, in the order wave_carve
 // lays them out.  constexpr so a fixed device array can hold a wave (ftb_noalloc.cu).
 constexpr size_t wave_align(size_t x) { return (x + 255) & ~(size_t)255; }
-constexpr size_t wave_bytes(int32_t W, bool log) {
+constexpr size_t wave_bytes(int32_t W, bool log, int32_t hero = 1) {
     size_t w = (size_t)W, s = 2 * (size_t)W;
     size_t b = 0;
     b += 2 * wave_align(8 * w);                                     // rng
@@ -86,11 +96,14 @@ constexpr size_t wave_bytes(int32_t W, bool log) {
     b += wave_align(64);                                            // table parameters
     b += 9 * wave_align(8 * s) + wave_align(4 * s);                 // shadow records
     if (log) b += wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
+    if (hero > 1)                                                   // bundles
+        b += 2 * wave_align(8 * w * hero) + wave_align(4 * w) + 2 * wave_align(8 * s * (hero - 1)) +
+             wave_align(4 * s);
     return b;
 }
-// Point the arrays of `w` into `block` (wave_bytes(W, log) bytes, 256-B aligned).
-void wave_carve(Wave& w, void* block, int32_t W, bool log);
-cudaError_t wave_alloc(Wave& w, int32_t W, bool log);
+// Point the arrays of `w` into `block` (wave_bytes(W, log, hero) bytes, 256-B aligned).
+void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero = 1);
+cudaError_t wave_alloc(Wave& w, int32_t W, bool log, int32_t hero = 1);
 void wave_free(Wave& w);
 
 // Kernel ids for profiling.
@@ -124,7 +137,9 @@ void wave_graphs_destroy(WaveGraphs* g);
 // profiling (sink), counting (f.stats) and logging (w.logs) launches are issued directly.
 // A cache's graphs hold the addresses of its wave buffer and status word: destroy the cache
 // when either changes.
-cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool instances, const Frame& f, int32_t sms,
+// `bundles` runs the hero-wavelength kernels (every job of the table has hero_c > 1 and the
+// buffer was allocated with hero >= the largest of them).
+cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool instances, bool bundles, const Frame& f, int32_t sms,
                         const LaunchShape& shape, cudaStream_t stream, LaunchSink* sink = nullptr,
                         WaveGraphs* graphs = nullptr);
 

@@ -62,6 +62,9 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     if (p->n_photons < 0 || p->max_bounce < 0 || p->max_bounce > 1024 || p->frac_bits > 56 ||
         cam->res_x <= 0 || cam->res_y <= 0)
         return na_fail(FTB_ERR_INVALID, "bad render parameters");
+    if (p->hero_c > 1 && dev.n_med == 0)
+        return na_fail(FTB_ERR_UNSUPPORTED, "ftb_render_forward_noalloc traces one wavelength per photon "
+                                            "(its scratch holds no bundles); use hero_c <= 1");
     if (p->n_photons > kNoAllocPhotons)
         return na_fail(FTB_ERR_TOO_LARGE, "ftb_render_forward_noalloc: at most " + std::to_string(kNoAllocPhotons) +
                                               " photons per call (its scratch is a fixed device array); "
@@ -118,7 +121,7 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     ftb::LaunchShape shape;
     shape.graph = false;
     if (e == cudaSuccess && p->n_photons > 0)
-        e = ftb::launch_wave(w, p->max_bounce, dev.n_inst > 0, f, sms, shape, st);
+        e = ftb::launch_wave(w, p->max_bounce, dev.n_inst > 0, false, f, sms, shape, st);
     if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (out == FTB_OK && info) {
         info->frac_bits = frac;

@@ -49,6 +49,7 @@ struct Job {
     DevScene sc{};
     double power = 0.0;
     int frac = 0;
+    int hero = 1;               // wavelengths per photon (1 or a bundle)
     uint64_t film_bytes = 0;
     int64_t next = 0;           // photons handed to waves so far
     int32_t pending = 0;        // launched waves holding this job's photons, not yet retired
@@ -77,6 +78,7 @@ struct ftb_server {
     int sms = 148;
     int max_active = 64;
     int32_t W = 1 << 22;
+    int32_t hero_max = 4;              // largest bundle the wave buffers hold
     ftb::LaunchShape shape;
     uint64_t budget = 0;
     Clock::time_point t0;
@@ -158,7 +160,7 @@ void admit_locked(ftb_server* s) {
 // Wave table: every job with photons left gets min(left, W / (4 * jobs)) slots, then the
 // remaining capacity goes to the jobs with the least work left.  One entry per job (mu held).
 int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::vector<Job*>& members,
-                           int32_t& max_bounce, bool& inst) {
+                           int32_t& max_bounce, bool& inst, bool& bundle_wave) {
     std::vector<Job*> c;
     for (Job* j : s->active)
         if (j->next < j->req.n_photons) c.push_back(j);
@@ -166,6 +168,10 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
     std::stable_sort(c.begin(), c.end(), [](const Job* a, const Job* b) {
         return a->req.n_photons - a->next < b->req.n_photons - b->next;
     });
+    // a wave holds one-wavelength jobs or bundles, not both: the class of the job with the
+    // least work left goes first
+    const bool bundles = c[0]->hero > 1;
+    c.erase(std::remove_if(c.begin(), c.end(), [&](const Job* j) { return (j->hero > 1) != bundles; }), c.end());
     if ((int)c.size() > ftb::kWaveJobs) c.resize(ftb::kWaveJobs);
     std::vector<int64_t> give(c.size(), 0);
     int64_t cap = s->W;
@@ -182,6 +188,7 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
     int32_t slots = 0;
     max_bounce = 0;
     inst = false;
+    bundle_wave = bundles;
     for (size_t i = 0; i < c.size(); ++i) {
         if (give[i] <= 0) continue;
         Job* j = c[i];
@@ -196,7 +203,8 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
         J.photon0 = j->req.seed_base + (uint64_t)j->next;
         J.slot0 = slots;
         J.n = (int32_t)give[i];
-        J.max_bounce = j->req.max_bounce;
+            J.max_bounce = j->req.max_bounce;
+        J.hero_c = j->hero;
         table.push_back(J);
         members.push_back(j);
         j->next += give[i];
@@ -240,11 +248,11 @@ void scheduler(ftb_server* s) {
         table.clear();
         members.clear();
         int32_t slots = 0, mb = 0;
-        bool inst = false;
+        bool inst = false, bundles = false;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             admit_locked(s);
-            slots = build_table_locked(s, table, members, mb, inst);
+            slots = build_table_locked(s, table, members, mb, inst, bundles);
             if (slots == 0) {
                 bool busy = s->ws[0].busy || s->ws[1].busy;
                 if (!busy) {
@@ -275,7 +283,7 @@ void scheduler(ftb_server* s) {
         f.stats = nullptr;
         f.status = s->d_status + 16 * b;
         if (e == cudaSuccess)
-            e = ftb::launch_wave(w.wave, mb, inst, f, s->sms, s->shape, w.stream, nullptr, w.graphs);
+            e = ftb::launch_wave(w.wave, mb, inst, bundles, f, s->sms, s->shape, w.stream, nullptr, w.graphs);
         if (e == cudaSuccess) e = cudaEventRecord(w.done, w.stream);
         {
             std::lock_guard<std::mutex> lk(s->mu);
@@ -374,6 +382,7 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
     s->device = cfg->device;
     s->max_active = cfg->max_active ? cfg->max_active : 64;
     s->W = cfg->wave_slots ? cfg->wave_slots : (1 << 22);
+    s->hero_max = cfg->hero_max > 0 ? (cfg->hero_max > ftb::kHeroMax ? ftb::kHeroMax : cfg->hero_max) : 4;
     s->t0 = Clock::now();
     set_device(s);
     cudaDeviceProp p;
@@ -389,7 +398,7 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
     };
     cudaError_t e;
     for (auto& w : s->ws) {
-        if ((e = ftb::wave_alloc(w.wave, s->W, false)) != cudaSuccess) return bad(e, "wave allocation");
+        if ((e = ftb::wave_alloc(w.wave, s->W, false, s->hero_max)) != cudaSuccess) return bad(e, "wave allocation");
         if ((e = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
         if ((e = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) != cudaSuccess) return bad(e, "event");
         if ((e = cudaHostAlloc((void**)&w.table, sizeof(ftb::DevJob) * (ftb::kWaveJobs + 1), cudaHostAllocDefault)) !=
@@ -439,6 +448,12 @@ ftb_status ftb_server_submit(ftb_server* s, const ftb_request* r, uint64_t* job_
     if (!(j->power > 0.0)) { delete j; return fail(FTB_ERR_UNSUPPORTED, "scene emits no power"); }
     j->req = *r;
     j->frac = r->frac_bits > 0 ? r->frac_bits : ftb::default_frac_bits(r->n_photons);
+    // bundles as the reference gates them: clamped to kHeroMax, none in scenes with media
+    j->hero = (r->hero_c <= 1 || j->sc.n_med > 0) ? 1 : (r->hero_c > ftb::kHeroMax ? ftb::kHeroMax : r->hero_c);
+    if (j->hero > s->hero_max) {
+        delete j;
+        return fail(FTB_ERR_TOO_LARGE, "bundle larger than the server's hero_max");
+    }
     j->film_bytes = (uint64_t)c.res_x * (uint64_t)c.res_y * 4 * sizeof(int64_t);
     if (j->film_bytes > s->budget) { delete j; return fail(FTB_ERR_TOO_LARGE, "film exceeds the server's film budget"); }
     std::lock_guard<std::mutex> lk(s->mu);

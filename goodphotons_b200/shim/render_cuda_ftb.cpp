@@ -271,14 +271,15 @@ bool cudaForwardSupported(const Scene& scene) {
     return b.supported && ftb_forward_supported(&b.desc) == 1;
 }
 
-// camMode 'B' (pinhole) with heroC 1 and the megakernel/wavefront choice folded into the
-// one wavefront backend; other camera models are not on this path and return empty films.
+// camMode 'B' (pinhole), any heroC (bundles as tracePhotonHero), and the megakernel/wavefront
+// choice folded into the one wavefront backend; other camera models are not on this path and
+// return empty films.
 Film renderForwardCuda(const Scene& scene, const Camera& cam, int resX, int resY, long long N,
                        EnergyReport& eOut, bool /*diffraction*/, char camMode,
                        unsigned long long seedBase, bool /*wavefront*/, int heroC) {
     Film out;
     out.resX = resX; out.resY = resY; out.alloc();
-    if (camMode != 'B' || heroC > 1) return out;
+    if (camMode != 'B') return out;
     Baked b;
     bake(scene, b);
     if (!b.supported) return out;
@@ -286,7 +287,7 @@ Film renderForwardCuda(const Scene& scene, const Camera& cam, int resX, int resY
     b.desc.build = pick_build(b.desc, N);
     if (!report(ftb_scene_create(&b.desc, 0, &s), "scene bake")) return out;
     ftb_camera c = bake_camera(cam, resX, resY);
-    ftb_render_params p{N, seedBase, g_ftbMaxBounce, 0};
+    ftb_render_params p{N, seedBase, g_ftbMaxBounce, 0, heroC, 0};   // bundles when heroC > 1 (no media)
     std::vector<int64_t> fx((size_t)resX * resY * 4);
     ftb_film_info info{};
     ftb_energy en{};

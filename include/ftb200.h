@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FTB_ABI_VERSION 2
+#define FTB_ABI_VERSION 3
 
 typedef enum ftb_status {
     FTB_OK = 0,
@@ -213,6 +213,11 @@ typedef struct ftb_render_params {
     uint64_t seed_base;   /* absolute index of the first photon (render_cuda.h:65-68) */
     int32_t max_bounce;   /* bounce cap (reference Renderer::maxBounce, render.h:301) */
     int32_t frac_bits;    /* film fixed-point fraction bits; <=0 picks a safe default */
+    int32_t hero_c;       /* wavelengths per photon (-heroc, render_cuda.h:74-82): <= 1 one
+                             wavelength; 2..8 hero bundles (Renderer::tracePhotonHero), used
+                             only in scenes without media, as the reference does; larger
+                             values are clamped to 8 */
+    int32_t pad;
 } ftb_render_params;
 
 /* Energy report (reference EnergyReport, render.h:29-31).  Each tally is the sum of the
@@ -337,6 +342,8 @@ typedef struct ftb_job {
     uint64_t seed_base;
     int32_t max_bounce;
     int32_t frac_bits;     /* <= 0: the default for n_photons */
+    int32_t hero_c;        /* wavelengths per photon, as ftb_render_params.hero_c */
+    int32_t pad;
 } ftb_job;
 
 ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n_jobs, ftb_film_info* infos,
@@ -451,7 +458,8 @@ typedef struct ftb_server_config {
     uint64_t film_budget;      /* bytes of device films admitted at once (0: a quarter of the
                                   free device memory) */
     int32_t wave_slots;        /* photon slots per wave, 1..2^22 (0: 2^22) */
-    int32_t pad;
+    int32_t hero_max;          /* largest hero_c a request may carry, 1..8 (0: 4); the wave
+                                  buffers grow by ~260 B per slot at 4 */
 } ftb_server_config;
 
 typedef struct ftb_request {
@@ -461,6 +469,8 @@ typedef struct ftb_request {
     uint64_t seed_base;
     int32_t max_bounce;
     int32_t frac_bits;         /* <= 0: the default for n_photons */
+    int32_t hero_c;            /* wavelengths per photon, as ftb_render_params.hero_c */
+    int32_t pad;
     int64_t* host_film;        /* res_x*res_y*4 int64, written at completion (page-locked memory
                                   copies fastest); NULL: the film is dropped */
 } ftb_request;

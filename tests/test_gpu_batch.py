@@ -75,3 +75,29 @@ def test_tuning_and_graph_replay_do_not_change_results(gpu):
     finally:
         L.L.ftb_set_tuning(0, C.byref(saved))
         sc.close()
+
+
+def test_bundles_and_single_wavelength_jobs_in_one_batch(gpu):
+    """A batch mixing hero bundles (C = 4, 3) with one-wavelength jobs: waves hold one kind,
+    and every job equals its solo render."""
+    torch = pytest.importorskip("torch")
+    L = gpu
+    sc_g = lib.Scene(scenes.make_glass(L, level=3), 0, L)
+    sc_c = lib.Scene(scenes.make_cornell(L), 0, L)
+    specs = [(sc_g, 40, 700_000, 4), (sc_c, 32, 300_000, 1), (sc_c, 24, 900_000, 3), (sc_g, 48, 200_000, 1)]
+    jobs, films = [], []
+    for k, (sc, res, n, hero) in enumerate(specs):
+        film = torch.zeros((res, res, 4), dtype=torch.int64, device="cuda:0")
+        films.append(film)
+        jobs.append(dict(scene=sc, cam=scenes.default_camera(L, res), d_film=film.data_ptr(), n=n,
+                         seed_base=10_000 * k, max_bounce=16, frac_bits=30, hero_c=hero))
+    stream = torch.cuda.current_stream().cuda_stream
+    _, ens = L.render_batch(jobs, stream=stream)
+    torch.cuda.synchronize()
+    for k, (j, film) in enumerate(zip(jobs, films)):
+        solo, _, en = j["scene"].render(j["cam"], j["n"], seed_base=j["seed_base"], max_bounce=16, frac_bits=30,
+                                        hero_c=j["hero_c"])
+        np.testing.assert_array_equal(film.cpu().numpy(), solo, err_msg=f"job {k}")
+        assert list(ens[k].fx) == list(en.fx)
+    sc_g.close()
+    sc_c.close()

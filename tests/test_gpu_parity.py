@@ -53,7 +53,7 @@ def test_film_and_energy_match_reference_golden(name, scenes_cache, gpu):
     g = golden(f"trace_{name}.npz")
     assert cases.scene_hash(d) == str(g["scene_hash"])
     cam = cases.camera(gpu, res)
-    film, info, en = sc.render(cam, n, seed_base=seed, max_bounce=mb)
+    film, info, en = sc.render(cam, n, seed_base=seed, max_bounce=mb, hero_c=hero)
     assert_film_close(film, info, g["xyz"], g["hits"])
     np.testing.assert_allclose(en.as_list(), g["energy"], rtol=1e-9, atol=0)
 
@@ -64,8 +64,8 @@ def test_per_photon_paths_match_oracle(name, scenes_cache, gpu, oracle):
     d, sc = scenes_cache[name]
     n = 1 << 15
     cam = cases.camera(gpu, res)
-    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=mb)
-    ol = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, threads=4)["logs"]
+    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=mb, hero_c=hero)
+    ol = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, threads=4, hero_c=hero)["logs"]
     # multi-threaded oracle logs are per photon, so order is by photon index either way
     same = (gl["n_hits"] == ol["n_hits"]) & (gl["prim_hash"] == ol["prim_hash"]) & (gl["fate"] == ol["fate"])
     allowed = max(1, int(1e-5 * n))
@@ -83,9 +83,9 @@ def test_device_build_paths_match_oracle(name, gpu, oracle):
     sc = lib.Scene(d, 0, gpu, build=abi.BUILD_DEVICE)
     n = 1 << 14
     cam = cases.camera(gpu, res)
-    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=mb)
+    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=mb, hero_c=hero)
     sc.close()
-    ol = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, threads=4)["logs"]
+    ol = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, threads=4, hero_c=hero)["logs"]
     same = (gl["n_hits"] == ol["n_hits"]) & (gl["prim_hash"] == ol["prim_hash"]) & (gl["fate"] == ol["fate"])
     assert (~same).sum() <= max(1, int(1e-5 * n)), f"{(~same).sum()} of {n} photon paths differ"
 

@@ -559,8 +559,8 @@ def main():
             sc.render_device(cam, n, film.data_ptr(), seed_base=k * n, max_bounce=mb, frac_bits=frac,
                              stream=stream.cuda_stream, hero_c=args.hero)
         else:   # the frame is n photons per rank; each rank traces its index shard
-            multigpu.render_sharded(sc, cam, n * world, film, seed_base=k * n * world, max_bounce=mb, hero_c=args.hero,
-                                    dst=0, stream=stream.cuda_stream)
+            multigpu.render_sharded(sc, cam, n * world, film, seed_base=k * n * world, max_bounce=mb,
+                                    hero_c=args.hero, dst=0, stream=stream.cuda_stream)
 
     # autotuner (untimed): grid size, wave size and graph replay for this workload
     t = time.perf_counter()

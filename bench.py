@@ -545,7 +545,7 @@ def main():
     sc.set_profiling(2)
     n_count = min(n, 1 << 22)
     sc.render_device(cam, n_count, film.data_ptr(), seed_base=1 << 50, max_bounce=mb,
-                     stream=stream.cuda_stream)
+                     stream=stream.cuda_stream, hero_c=args.hero)
     torch.cuda.synchronize(dev)
     cp = sc.profile(reset=True)
     rays_c, nodes_c, recs_c = cp.counters[0], cp.counters[1], cp.counters[2]

@@ -1784,15 +1784,21 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, cons
         if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         long long* px = reinterpret_cast<long long*>(J.film) + 4 * (size_t)w.spix[i];
         const int nup = w.snup[i];
+        // every wavelength is one Film::add, each rounded to fixed point on its own; their
+        // integer sum goes to the pixel in one atomic per channel (integer sums are exact)
+        long long sx = 0, sy = 0, sz = 0;
         for (int k = 0; k < nup; ++k) {
             double lam = k == 0 ? w.slam[i] : w.xlam[(size_t)(k - 1) * w.S + i];
             double c = k == 0 ? w.sval[i] : w.xval[(size_t)(k - 1) * w.S + i];
             double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
-            atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, f.status));
-            atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, J.film_scale_inv, f.status));
-            atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, J.film_scale_inv, f.status));
-            atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
+            sx += to_fixed(X, J.film_scale_inv, f.status);
+            sy += to_fixed(Y, J.film_scale_inv, f.status);
+            sz += to_fixed(Z, J.film_scale_inv, f.status);
         }
+        atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)sx);
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)sy);
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)sz);
+        atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), (unsigned long long)nup);
     }
     if (COUNT) {
         block_add3(f.stats + 3, rays, cnt.nodes, cnt.recs);

@@ -345,6 +345,7 @@ struct ftb_session {
     ftb_scene* scene = nullptr;
     std::vector<ftb_camera> cams;
     std::vector<int64_t*> films;
+    ftb::DevView* views = nullptr;   // device: every camera with its film (one shared pass)
     unsigned long long* tally = nullptr;
     int32_t max_bounce = 32;
     int32_t frac_bits = 0;
@@ -646,13 +647,19 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         int32_t slots = 0, max_bounce = 0;
         bool inst = false;
         int bundles = -1;   // a wave holds either one-wavelength jobs or bundles, not both
-        while (j < base.size() && slots < W && (int)table.size() < ftb::kWaveJobs) {
+        // A path queues at most 2 connections per view per bounce and the shadow queue holds
+        // 2W records, so a wave of multi-camera jobs carries W / views slots.
+        int32_t cap = W;
+        while (j < base.size() && slots < cap && (int)table.size() < ftb::kWaveJobs) {
             int64_t left = count[j] - done_in_job;
             if (left <= 0) { ++j; done_in_job = 0; continue; }
             const int is_bundle = base[j].hero_c > 1 ? 1 : 0;
             if (bundles >= 0 && is_bundle != bundles) break;
+            const int32_t jcap = std::max(1, W / std::max(1, base[j].n_views));
+            if (jcap < cap && slots >= jcap) break;   // this job needs a roomier wave of its own
+            cap = std::min(cap, jcap);
             bundles = is_bundle;
-            int32_t m = (int32_t)std::min<int64_t>(left, (int64_t)(W - slots));
+            int32_t m = (int32_t)std::min<int64_t>(left, (int64_t)(cap - slots));
             ftb::DevJob J = base[j];
             J.photon0 = seed[j] + (uint64_t)done_in_job;
             J.slot0 = slots;
@@ -1448,9 +1455,19 @@ ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cam
         if (e != cudaSuccess) { for (auto p : ss->films) cudaFree(p); delete ss; return cuda_fail(e, "session film"); }
         ss->films.push_back(f);
     }
+    std::vector<ftb::DevView> hv((size_t)n_cams);
+    for (int c = 0; c < n_cams; ++c) { hv[c].cam = dev_cam(&cams[c]); hv[c].film = ss->films[c]; }
     cudaError_t e = cudaMalloc(&ss->tally, 8 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(ss->tally, 0, 8 * sizeof(unsigned long long));
-    if (e != cudaSuccess) { for (auto p : ss->films) cudaFree(p); delete ss; return cuda_fail(e, "session tally"); }
+    if (e == cudaSuccess) e = cudaMalloc(&ss->views, sizeof(ftb::DevView) * hv.size());
+    if (e == cudaSuccess) e = cudaMemcpy(ss->views, hv.data(), sizeof(ftb::DevView) * hv.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        for (auto p : ss->films) cudaFree(p);
+        if (ss->tally) cudaFree(ss->tally);
+        if (ss->views) cudaFree(ss->views);
+        delete ss;
+        return cuda_fail(e, "session setup");
+    }
     *out = ss;
     return FTB_OK;
 }
@@ -1463,14 +1480,13 @@ ftb_status ftb_session_batch(ftb_session* ss, int64_t n, uint64_t seed_base) {
     ftb_status st = ensure_frame(s, 0);
     if (st != FTB_OK) return st;
     CK(cudaMemset(s->eng->status, 0, 64), "memset status");
-    // Model B connections draw no random numbers (render.h:272-275), so tracing the same
-    // photon indices once per camera gives every camera exactly the film a shared pass would.
-    for (size_t c = 0; c < ss->cams.size(); ++c) {
-        unsigned long long* tally = (c == 0) ? ss->tally : s->eng->tally;
-        st = run_photons(s, &ss->cams[c], n, seed_base, ss->max_bounce, ss->frac_bits, ss->films[c], tally, nullptr,
-                         nullptr);
-        if (st != FTB_OK) return st;
-    }
+    // One shared pass (the multi-camera shared splat, render_cuda.cu:13873-13895): every
+    // path vertex connects to each camera; the paths are traced once.
+    ftb::DevJob J = make_job(s, &ss->cams[0], ss->films[0], ss->tally, ss->frac_bits, ss->max_bounce);
+    J.views = ss->views;
+    J.n_views = (int32_t)ss->cams.size();
+    st = run_jobs(s, {J}, {n}, {seed_base}, false, nullptr, 0, nullptr);
+    if (st != FTB_OK) return st;
     CK(cudaDeviceSynchronize(), "session batch");
     return read_status(s);
 }
@@ -1510,6 +1526,7 @@ ftb_status ftb_session_end(ftb_session* ss) {
     DeviceGuard guard(ss->scene->device);
     for (auto p : ss->films) cudaFree(p);
     if (ss->tally) cudaFree(ss->tally);
+    if (ss->views) cudaFree(ss->views);
     delete ss;
     return FTB_OK;
 }

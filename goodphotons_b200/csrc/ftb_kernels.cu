@@ -906,51 +906,66 @@ __device__ __forceinline__ int agg_inc(int32_t* ctr) {
     return g.shfl(base, 0) + (int)g.thread_rank();
 }
 
-__device__ __forceinline__ void push_shadow(const Wave& w, const Frame& f, int job, D3 o, D3 d, double tmax,
-                                            double val, double lam, int pix) {
+__device__ __forceinline__ void push_shadow(const Wave& w, const Frame& f, int job, int view, D3 o, D3 d,
+                                            double tmax, double val, double lam, int pix) {
     int i = agg_inc(&w.counts[2]);
     if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
     w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
     w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
     w.smax[i] = tmax; w.sval[i] = val; w.slam[i] = lam; w.spix[i] = pix;
-    w.sjob[i] = job;
+    w.sjob[i] = job; w.sview[i] = view;
+}
+
+// The views a job's vertices connect to: its own camera, or every view of a multi-camera job.
+__device__ __forceinline__ int view_count(const DevJob& J) { return J.n_views > 1 ? J.n_views : 1; }
+__device__ __forceinline__ const DevCam& view_cam(const DevJob& J, int v) {
+    return J.n_views > 1 ? J.views[v].cam : J.cam;
+}
+__device__ __forceinline__ int64_t* view_film(const DevJob& J, int v) {
+    return J.n_views > 1 ? J.views[v].film : J.film;
 }
 
 // connectGeom + connect, model B (render.h:499-559); the occlusion test is deferred to
 // k_shadow, the rest of the contribution is formed here in the reference's order.
-__device__ void connect_surface(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f, int job,
+__device__ void connect_surface(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f, int job,
                                 D3 p, D3 n, D3 ng, D3 wi, double lam, double beta, double rho) {
-    D3 to_cam = ld3(cam.eye) - p;
-    double dist = len(to_cam);
-    D3 wdir = to_cam / dist;
-    double cos_surf = dot(n, wdir);
-    if (cos_surf <= 0) return;
-    double stg = shadow_terminator_g(wdir, n, ng);
-    if (stg <= 0.0) return;
-    int px, py; double cos_cam, dist2;
-    if (!cam_project(cam, p, px, py, cos_cam, dist2)) return;
-    double omega = cam_pixel_solid_angle(cam, cos_cam);
-    double corr = shading_adjoint_corr(wi, wdir, n, ng);
-    double denom = dist2 * omega;
-    double fr = rho / PI_D;
-    double contrib = beta * fr * cos_surf * corr / denom * stg;
-    if (sc.n_med > 0) contrib *= media_transmittance(sc, p, wdir, dist, lam);
-    push_shadow(w, f, job, p + ng * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+    for (int v = 0; v < view_count(J); ++v) {
+        const DevCam& cam = view_cam(J, v);
+        D3 to_cam = ld3(cam.eye) - p;
+        double dist = len(to_cam);
+        D3 wdir = to_cam / dist;
+        double cos_surf = dot(n, wdir);
+        if (cos_surf <= 0) continue;
+        double stg = shadow_terminator_g(wdir, n, ng);
+        if (stg <= 0.0) continue;
+        int px, py; double cos_cam, dist2;
+        if (!cam_project(cam, p, px, py, cos_cam, dist2)) continue;
+        double omega = cam_pixel_solid_angle(cam, cos_cam);
+        double corr = shading_adjoint_corr(wi, wdir, n, ng);
+        double denom = dist2 * omega;
+        double fr = rho / PI_D;
+        double contrib = beta * fr * cos_surf * corr / denom * stg;
+        if (sc.n_med > 0) contrib *= media_transmittance(sc, p, wdir, dist, lam);
+        push_shadow(w, f, job, v, p + ng * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+    }
 }
 // connectVolume (render.h:584-600)
-__device__ void connect_volume(const DevScene& sc, const DevCam& cam, const Wave& w, const Frame& f, int job,
+__device__ void connect_volume(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f, int job,
                                const DevMed& m, D3 p, D3 win, double lam, double beta) {
-    D3 to_cam = ld3(cam.eye) - p;
-    double dist = len(to_cam);
-    D3 wdir = to_cam / dist;
-    int px, py; double cos_cam, dist2;
-    if (!cam_project(cam, p, px, py, cos_cam, dist2)) return;
-    double ph = hg_phase(dot(win, wdir), m.g);
-    double alb = med_albedo(sc, m, lam);
-    double omega = cam_pixel_solid_angle(cam, cos_cam);
-    double contrib = beta * alb * ph / (dist2 * omega);
-    contrib *= media_transmittance(sc, p, wdir, dist, lam);
-    push_shadow(w, f, job, p + wdir * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+    for (int v = 0; v < view_count(J); ++v) {
+        const DevCam& cam = view_cam(J, v);
+        D3 to_cam = ld3(cam.eye) - p;
+        double dist = len(to_cam);
+        D3 wdir = to_cam / dist;
+        int px, py; double cos_cam, dist2;
+        if (!cam_project(cam, p, px, py, cos_cam, dist2)) continue;
+        double ph = hg_phase(dot(win, wdir), m.g);
+        double alb = med_albedo(sc, m, lam);
+        double omega = cam_pixel_solid_angle(cam, cos_cam);
+        double contrib = beta * alb * ph / (dist2 * omega);
+        contrib *= media_transmittance(sc, p, wdir, dist, lam);
+        push_shadow(w, f, job, v, p + wdir * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+    }
 }
 
 // ------------------------------------------------------------------ tallies ------------
@@ -1100,7 +1115,7 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
         double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
         beta *= 1.0;
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(beta, J.tally_scale_inv, f.status));
-        connect_surface(sc, J.cam, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
+        connect_surface(sc, J, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
@@ -1244,7 +1259,6 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         const int j = multi ? w.job[slot] : 0;
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
-        const DevCam& cam = J.cam;
         Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
         D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
         double lam = w.lam[slot], beta = w.beta[slot];
@@ -1283,7 +1297,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         D3 no = ro, nd = rd;
         if (medium_event) {   // render.h:2105-2115
             const DevMed& sm = sc.med[scatter_med];
-            connect_volume(sc, cam, w, f, j, sm, mp, rd, lam, beta);
+            connect_volume(sc, J, w, f, j, sm, mp, rd, lam, beta);
             if (uniform(rng) >= med_albedo(sc, sm, lam)) fate = 0;
             else { nd = sample_hg(rd, sm.g, rng); no = mp; }
         } else if (!valid) {
@@ -1354,8 +1368,8 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
                 if (sum > 1.0) { rr /= sum; rt /= sum; sum = 1.0; }
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface(sc, cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr);
-                connect_surface(sc, cam, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
+                connect_surface(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr);
+                connect_surface(sc, J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
                 double u = uniform(rng);
                 if (u < rr) {
                     D3 wo = cosine_hemisphere(h.n, rng);
@@ -1372,7 +1386,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
                 double rho = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface(sc, cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho);
+                connect_surface(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho);
                 if (uniform(rng) >= rho) { fate = 0; break; }
                 D3 wo = cosine_hemisphere(h.n, rng);
                 beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
@@ -1428,7 +1442,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
         if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         double lam = w.slam[i], c = w.sval[i];
         double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
-        long long* px = reinterpret_cast<long long*>(J.film) + 4 * (size_t)w.spix[i];
+        long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i])) + 4 * (size_t)w.spix[i];
         atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, f.status));
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, J.film_scale_inv, f.status));
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, J.film_scale_inv, f.status));
@@ -1450,13 +1464,13 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
 // in scenes without media, and so does this path (the host sends such jobs to the scalar
 // kernels).
 
-__device__ __forceinline__ void push_shadow_hero(const Wave& w, const Frame& f, int job, D3 o, D3 d, double tmax,
-                                                 int nup, const double* lam, const double* val, int pix) {
+__device__ __forceinline__ void push_shadow_hero(const Wave& w, const Frame& f, int job, int view, D3 o, D3 d,
+                                                 double tmax, int nup, const double* lam, const double* val, int pix) {
     int i = agg_inc(&w.counts[2]);
     if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
     w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
     w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
-    w.smax[i] = tmax; w.spix[i] = pix; w.sjob[i] = job;
+    w.smax[i] = tmax; w.spix[i] = pix; w.sjob[i] = job; w.sview[i] = view;
     w.slam[i] = lam[0]; w.sval[i] = val[0];
     for (int k = 1; k < nup; ++k) {
         w.xlam[(size_t)(k - 1) * w.S + i] = lam[k];
@@ -1466,27 +1480,30 @@ __device__ __forceinline__ void push_shadow_hero(const Wave& w, const Frame& f, 
 }
 
 // connectHero (render.h:564-577): one connectGeom, a contribution per live wavelength
-__device__ void connect_surface_hero(const DevCam& cam, const Wave& w, const Frame& f, int job, D3 p, D3 n,
+__device__ void connect_surface_hero(const DevJob& J, const Wave& w, const Frame& f, int job, D3 p, D3 n,
                                      D3 ng, D3 wi, const double* lam, const double* beta, const double* rho,
                                      int nup) {
-    D3 to_cam = ld3(cam.eye) - p;
-    double dist = len(to_cam);
-    D3 wdir = to_cam / dist;
-    double cos_surf = dot(n, wdir);
-    if (cos_surf <= 0) return;
-    double stg = shadow_terminator_g(wdir, n, ng);
-    if (stg <= 0.0) return;
-    int px, py; double cos_cam, dist2;
-    if (!cam_project(cam, p, px, py, cos_cam, dist2)) return;
-    double omega = cam_pixel_solid_angle(cam, cos_cam);
-    double corr = shading_adjoint_corr(wi, wdir, n, ng);
-    double denom = dist2 * omega;
-    double val[kHeroMax];
-    for (int i = 0; i < nup; ++i) {
-        double fr = rho[i] / PI_D;
-        val[i] = beta[i] * fr * cos_surf * corr / denom * stg;
+    for (int v = 0; v < view_count(J); ++v) {
+        const DevCam& cam = view_cam(J, v);
+        D3 to_cam = ld3(cam.eye) - p;
+        double dist = len(to_cam);
+        D3 wdir = to_cam / dist;
+        double cos_surf = dot(n, wdir);
+        if (cos_surf <= 0) continue;
+        double stg = shadow_terminator_g(wdir, n, ng);
+        if (stg <= 0.0) continue;
+        int px, py; double cos_cam, dist2;
+        if (!cam_project(cam, p, px, py, cos_cam, dist2)) continue;
+        double omega = cam_pixel_solid_angle(cam, cos_cam);
+        double corr = shading_adjoint_corr(wi, wdir, n, ng);
+        double denom = dist2 * omega;
+        double val[kHeroMax];
+        for (int i = 0; i < nup; ++i) {
+            double fr = rho[i] / PI_D;
+            val[i] = beta[i] * fr * cos_surf * corr / denom * stg;
+        }
+        push_shadow_hero(w, f, job, v, p + ng * 1e-6, wdir, dist - 2e-6, nup, lam, val, py * cam.rx + px);
     }
-    push_shadow_hero(w, f, job, p + ng * 1e-6, wdir, dist - 2e-6, nup, lam, val, py * cam.rx + px);
 }
 
 __device__ __forceinline__ double sum_of(const double* a, int n) {   // activeSum (render.h:2324)
@@ -1541,7 +1558,7 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
         base *= 1.0;   // spotW
         for (int i = 0; i < C; ++i) { beta[i] = base / C; one[i] = 1.0; }
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
-        connect_surface_hero(J.cam, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, one, C);
+        connect_surface_hero(J, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, one, C);
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
@@ -1576,7 +1593,6 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
         const int j = multi ? w.job[slot] : 0;
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
-        const DevCam& cam = J.cam;
         const int C = J.hero_c;
         Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
         D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
@@ -1639,8 +1655,8 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                 }
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface_hero(cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr, nup);
-                connect_surface_hero(cam, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt, nup);
+                connect_surface_hero(J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr, nup);
+                connect_surface_hero(J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt, nup);
                 double q_r = max_of(rr, nup), q_t = max_of(rt, nup);
                 double sum_h = q_r + q_t;
                 if (nup > 1 && sum_h > 1.0) { q_r /= sum_h; q_t /= sum_h; sum_h = q_r + q_t; }
@@ -1723,7 +1739,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                 for (int i = 0; i < nup; ++i) rho[i] = clamp01(spec_slot(sc, m.reflect, lam[i], 0.5));
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface_hero(cam, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho, nup);
+                connect_surface_hero(J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho, nup);
                 double q = max_of(rho, nup);
                 if (uniform(rng) >= q) { fate = 0; break; }
                 for (int i = 0; i < nup; ++i) {
@@ -1782,7 +1798,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, cons
         RayCtx R = make_ray(o, d);
         if (COUNT) rays++;
         if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
-        long long* px = reinterpret_cast<long long*>(J.film) + 4 * (size_t)w.spix[i];
+        long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i])) + 4 * (size_t)w.spix[i];
         const int nup = w.snup[i];
         // every wavelength is one Film::add, each rounded to fixed point on its own; their
         // integer sum goes to the pixel in one atomic per channel (integer sums are exact)
@@ -1832,6 +1848,7 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
     w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
     w.spix = (int32_t*)take(4 * sn);
+    w.sview = (int32_t*)take(4 * sn);
     if (log) {
         w.lhash = (uint64_t*)take(8 * wn); w.lnh = (int32_t*)take(4 * wn); w.lprims = (int32_t*)take(4 * wn * 8);
     }

@@ -20,12 +20,20 @@ constexpr int kStkCap = 4;
 constexpr int kHeroMax = 8;      // wavelengths a hero bundle can carry (hero::kHeroMax)
 constexpr int kWaveJobs = 256;   // jobs (frames / requests) one wave can carry
 
-// One job's share of a wave: its scene, camera and film, and the slots [slot0, slot0+n)
-// of the wave that trace its photons photon0, photon0+1, ...
+// A camera and its film (one view of a multi-camera job).
+struct DevView {
+    DevCam cam;
+    int64_t* film;
+};
+
+// One job's share of a wave: its scene, camera(s) and film(s), and the slots
+// [slot0, slot0+n) of the wave that trace its photons photon0, photon0+1, ...
 struct DevJob {
     DevScene sc;
     DevCam cam;
     int64_t* film;             // 4 words per pixel
+    const DevView* views;      // n_views > 1: every vertex connects to each view (shared splat)
+    int32_t n_views, pad;
     unsigned long long* tally; // 5 fixed-point energy tallies
     double film_scale_inv;     // 2^frac / power_ref
     double tally_scale_inv;    // 2^32 / power_ref
@@ -55,6 +63,7 @@ struct Wave {
     int32_t* params;           // [0] jobs in the table, [1] slots in use (written with the table)
     double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
     int32_t* spix;
+    int32_t* sview;            // view of each connection (multi-camera jobs)
     // hero-wavelength bundles (hero > 1 only; null otherwise)
     int32_t hero;              // wavelengths a path of this buffer can carry
     double* hlam;              // [hero][W] wavelengths, index 0 the hero
@@ -94,7 +103,7 @@ constexpr size_t wave_bytes(int32_t W, bool log, int32_t hero = 1) {
     b += 2 * wave_align(4 * w) + wave_align(64);                    // queues + counts
     b += wave_align(4 * w) + wave_align(4 * s) + wave_align(sizeof(DevJob) * kWaveJobs);   // job ids + table
     b += wave_align(64);                                            // table parameters
-    b += 9 * wave_align(8 * s) + wave_align(4 * s);                 // shadow records
+    b += 9 * wave_align(8 * s) + 2 * wave_align(4 * s);             // shadow records
     if (log) b += wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
     if (hero > 1)                                                   // bundles
         b += 2 * wave_align(8 * w * hero) + wave_align(4 * w) + 2 * wave_align(8 * s * (hero - 1)) +

@@ -645,7 +645,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
     while (j < base.size()) {
         table.clear();
         int32_t slots = 0, max_bounce = 0;
-        bool inst = false;
+        bool inst = false, media = false;
         int bundles = -1;   // a wave holds either one-wavelength jobs or bundles, not both
         // A path queues at most 2 connections per view per bounce and the shadow queue holds
         // 2W records, so a wave of multi-camera jobs carries W / views slots.
@@ -667,6 +667,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
             table.push_back(J);
             max_bounce = std::max(max_bounce, J.max_bounce);
             inst |= J.sc.n_inst > 0;
+            media |= J.sc.n_med > 0;
             slots += m;
             done_in_job += m;
             if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
@@ -678,8 +679,12 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         w.log_base = log_base;
         cudaError_t e = s->eng->stage[k & 1].push(table.data(), (int)table.size(), slots, w, ws);
         if (e != cudaSuccess) return cuda_fail(e, "job table upload");
-        e = ftb::launch_wave(w, max_bounce, inst, bundles == 1, f, s->sms, s->eng->shape, ws,
-                             s->prof_mode ? s->prof : nullptr, s->eng->graphs[k & 1]);
+        ftb::WaveKind kind;
+        kind.instances = inst;
+        kind.bundles = bundles == 1;
+        kind.media = media;
+        e = ftb::launch_wave(w, max_bounce, kind, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
+                             s->eng->graphs[k & 1]);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         ++k;
     }

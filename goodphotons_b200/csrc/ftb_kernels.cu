@@ -927,6 +927,7 @@ __device__ __forceinline__ int64_t* view_film(const DevJob& J, int v) {
 
 // connectGeom + connect, model B (render.h:499-559); the occlusion test is deferred to
 // k_shadow, the rest of the contribution is formed here in the reference's order.
+template <bool MEDIA>
 __device__ void connect_surface(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f, int job,
                                 D3 p, D3 n, D3 ng, D3 wi, double lam, double beta, double rho) {
     for (int v = 0; v < view_count(J); ++v) {
@@ -945,7 +946,7 @@ __device__ void connect_surface(const DevScene& sc, const DevJob& J, const Wave&
         double denom = dist2 * omega;
         double fr = rho / PI_D;
         double contrib = beta * fr * cos_surf * corr / denom * stg;
-        if (sc.n_med > 0) contrib *= media_transmittance(sc, p, wdir, dist, lam);
+        if (MEDIA && sc.n_med > 0) contrib *= media_transmittance(sc, p, wdir, dist, lam);
         push_shadow(w, f, job, v, p + ng * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
     }
 }
@@ -1083,6 +1084,7 @@ __device__ __forceinline__ double sample_at(const DevEmit& em, double u, double&
 }
 
 // ------------------------------------------------------------------ kernels ------------
+template <bool MEDIA>
 __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f) {
     const int32_t n_jobs = w.params[0], n_slots = w.params[1];
     const bool multi = n_jobs > 1;
@@ -1115,7 +1117,7 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
         double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
         beta *= 1.0;
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(beta, J.tally_scale_inv, f.status));
-        connect_surface(sc, J, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
+        connect_surface<MEDIA>(sc, J, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
@@ -1246,6 +1248,7 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 }
 
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
+template <bool MEDIA, bool INST>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
                                                                Frame f, const int32_t* qin,
                                                                const int32_t* qin_count, int32_t* qout,
@@ -1270,7 +1273,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
             int nh = w.lnh[slot];
             int prim = rec >= 0 ? sc.recs[rec].prim : -1;
             uint64_t hsh = fnv_i32(w.lhash[slot], prim);
-            if (rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)   // and the BLAS triangle
+            if (INST && rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)   // and the BLAS triangle
                 hsh = fnv_i32(hsh, sc.inst[rec_inst(sc.recs[rec])].recs[w.hit_sub[slot]].prim);
             w.lhash[slot] = hsh;
             if (nh < 8) w.lprims[nh * w.W + slot] = prim;
@@ -1283,7 +1286,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         bool medium_event = false;
         int scatter_med = -1;
         D3 mp = mk(0, 0, 0);
-        if (sc.n_med > 0) {
+        if (MEDIA && sc.n_med > 0) {
             double tm; int which;
             if (sample_media_collision(sc, ro, rd, d_surf, lam, rng, tm, which)) {
                 d_event = tm; medium_event = true; scatter_med = which; mp = ro + rd * tm;
@@ -1306,7 +1309,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
             PrimRec r;
             load_rec(sc.recs, rec, r);
             Hit h;
-            if (rec_type(r) == REC_INST) {
+            if (INST && rec_type(r) == REC_INST) {
                 instance_hit(sc.inst[rec_inst(r)], w.hit_sub[slot], ro, rd, h);
                 h.prim = r.prim;
             } else {
@@ -1368,8 +1371,8 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
                 if (sum > 1.0) { rr /= sum; rt /= sum; sum = 1.0; }
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr);
-                connect_surface(sc, J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
+                connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr);
+                connect_surface<MEDIA>(sc, J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
                 double u = uniform(rng);
                 if (u < rr) {
                     D3 wo = cosine_hemisphere(h.n, rng);
@@ -1386,7 +1389,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
                 double rho = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho);
+                connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho);
                 if (uniform(rng) >= rho) { fate = 0; break; }
                 D3 wo = cosine_hemisphere(h.n, rng);
                 beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
@@ -1580,6 +1583,7 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
     tally_finish(acc, jobs, multi);
 }
 
+template <bool INST>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, const DevJob* __restrict__ jobs,
                                                                     Frame f, const int32_t* qin,
                                                                     const int32_t* qin_count, int32_t* qout,
@@ -1610,7 +1614,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
             int nh = w.lnh[slot];
             int prim = rec >= 0 ? sc.recs[rec].prim : -1;
             uint64_t hsh = fnv_i32(w.lhash[slot], prim);
-            if (rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)
+            if (INST && rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)
                 hsh = fnv_i32(hsh, sc.inst[rec_inst(sc.recs[rec])].recs[w.hit_sub[slot]].prim);
             w.lhash[slot] = hsh;
             if (nh < 8) w.lprims[nh * w.W + slot] = prim;
@@ -1635,7 +1639,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
             PrimRec r;
             load_rec(sc.recs, rec, r);
             Hit h;
-            if (rec_type(r) == REC_INST) {
+            if (INST && rec_type(r) == REC_INST) {
                 instance_hit(sc.inst[rec_inst(r)], w.hit_sub[slot], ro, rd, h);
                 h.prim = r.prim;
             } else {
@@ -1878,8 +1882,9 @@ namespace {
 // shading and the connections it queued.  Every launch reads the wave's job count and
 // slot count from w.params, so the same sequence serves any table (and one captured graph
 // serves every wave of its shape).
-void issue_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const Frame& f, int grid, cudaStream_t st,
+void issue_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int grid, cudaStream_t st,
                 LaunchSink* sink) {
+    const bool inst = kind.instances, hero = kind.bundles, media = kind.media;
     const int T = 128;
     const DevJob* jobs = w.jobs;
     const bool count = f.stats != nullptr;
@@ -1907,7 +1912,8 @@ void issue_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const Frame& 
     cudaMemsetAsync(w.counts, 0, 64, st);
     mark(K_EMIT, false);
     if (hero) k_emit_hero<<<grid, T, 0, st>>>(w, jobs, f);
-    else k_emit<<<grid, T, 0, st>>>(w, jobs, f);
+    else if (media) k_emit<true><<<grid, T, 0, st>>>(w, jobs, f);
+    else k_emit<false><<<grid, T, 0, st>>>(w, jobs, f);
     mark(K_EMIT, true);
     shadow();
     int32_t* qa = w.qa;
@@ -1926,8 +1932,16 @@ void issue_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const Frame& 
         mark(K_EXTEND, true);
         cudaMemsetAsync(cb, 0, 4, st);
         mark(K_SHADE, false);
-        if (hero) k_shade_hero<<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
-        else k_shade<<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+        if (hero) {
+            if (inst) k_shade_hero<true><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+            else k_shade_hero<false><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+        } else if (media) {
+            if (inst) k_shade<true, true><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+            else k_shade<true, false><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+        } else {
+            if (inst) k_shade<false, true><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+            else k_shade<false, false><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
+        }
         mark(K_SHADE, true);
         shadow();
         int32_t* tq = qa; qa = qb; qb = tq;
@@ -1939,7 +1953,7 @@ void issue_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const Frame& 
 struct WaveGraphs {
     struct Entry {
         int32_t max_bounce, grid;
-        bool inst, hero;
+        bool inst, hero, media;
         int32_t* status;
         cudaGraphExec_t exec;
     };
@@ -1952,9 +1966,9 @@ struct WaveGraphs {
 WaveGraphs* wave_graphs_create() { return new WaveGraphs(); }
 void wave_graphs_destroy(WaveGraphs* g) { delete g; }
 
-cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const Frame& f, int32_t sms,
+cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int32_t sms,
                         const LaunchShape& shape, cudaStream_t st, LaunchSink* sink, WaveGraphs* graphs) {
-    if (hero && w.hero < 2) return cudaErrorInvalidValue;   // the buffer carries no bundles
+    if (kind.bundles && w.hero < 2) return cudaErrorInvalidValue;   // the buffer carries no bundles
     const int T = 128;
     int grid = sms * std::max(1, shape.grid_mult);
     const int gw = (w.W + T - 1) / T;   // enough blocks to give every slot a thread
@@ -1962,19 +1976,20 @@ cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool inst, bool hero, const
     // A graph bakes the kernel arguments: the wave's buffers and status word are fixed for the
     // life of its cache, but a log buffer changes per call, so logging waves launch directly.
     if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
-        issue_wave(w, max_bounce, inst, hero, f, grid, st, sink);
+        issue_wave(w, max_bounce, kind, f, grid, st, sink);
         return cudaGetLastError();
     }
     for (auto& e : graphs->entries)
-        if (e.max_bounce == max_bounce && e.grid == grid && e.inst == inst && e.hero == hero && e.status == f.status)
+        if (e.max_bounce == max_bounce && e.grid == grid && e.inst == kind.instances && e.hero == kind.bundles &&
+            e.media == kind.media && e.status == f.status)
             return cudaGraphLaunch(e.exec, st);
     cudaGraph_t g = nullptr;
     cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) return err;
-    issue_wave(w, max_bounce, inst, hero, f, grid, st, nullptr);
+    issue_wave(w, max_bounce, kind, f, grid, st, nullptr);
     err = cudaStreamEndCapture(st, &g);
     if (err != cudaSuccess) return err;
-    WaveGraphs::Entry e{max_bounce, grid, inst, hero, f.status, nullptr};
+    WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, f.status, nullptr};
     err = cudaGraphInstantiate(&e.exec, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) return err;

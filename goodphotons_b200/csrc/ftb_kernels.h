@@ -138,17 +138,22 @@ struct WaveGraphs;
 WaveGraphs* wave_graphs_create();
 void wave_graphs_destroy(WaveGraphs* g);
 
+// Which kernel variants a wave needs, from the jobs of its table.
+struct WaveKind {
+    bool instances = false;   // some scene has instance records (two-level traversal)
+    bool bundles = false;     // hero-wavelength jobs (every job of the table has hero_c > 1)
+    bool media = false;       // some scene has participating media
+};
+
 // Trace one wave on `stream`.  The caller has written, stream-ordered before this call, the
 // job table to w.jobs (slot ranges consecutive from 0) and w.params = {jobs, slots} (slots
 // <= W); every slot runs through at most max_bounce bounces (the largest of its jobs).
-// `instances` selects the traversal variants that meet instance records (any job's scene has
-// instances).  With `graphs` and shape.graph the sequence is replayed from a CUDA graph;
-// profiling (sink), counting (f.stats) and logging (w.logs) launches are issued directly.
-// A cache's graphs hold the addresses of its wave buffer and status word: destroy the cache
-// when either changes.
-// `bundles` runs the hero-wavelength kernels (every job of the table has hero_c > 1 and the
-// buffer was allocated with hero >= the largest of them).
-cudaError_t launch_wave(Wave& w, int32_t max_bounce, bool instances, bool bundles, const Frame& f, int32_t sms,
+// Bundles need a buffer allocated with hero >= the largest hero_c of the table.  With
+// `graphs` and shape.graph the sequence is replayed from a CUDA graph; profiling (sink),
+// counting (f.stats) and logging (w.logs) launches are issued directly.  A cache's graphs
+// hold the addresses of its wave buffer and status word: destroy the cache when either
+// changes.
+cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int32_t sms,
                         const LaunchShape& shape, cudaStream_t stream, LaunchSink* sink = nullptr,
                         WaveGraphs* graphs = nullptr);
 

@@ -120,8 +120,10 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     if (e == cudaSuccess) e = cudaMemcpyAsync(w.params, params, sizeof params, cudaMemcpyHostToDevice, st);
     ftb::LaunchShape shape;
     shape.graph = false;
-    if (e == cudaSuccess && p->n_photons > 0)
-        e = ftb::launch_wave(w, p->max_bounce, dev.n_inst > 0, false, f, sms, shape, st);
+    ftb::WaveKind kind;
+    kind.instances = dev.n_inst > 0;
+    kind.media = dev.n_med > 0;
+    if (e == cudaSuccess && p->n_photons > 0) e = ftb::launch_wave(w, p->max_bounce, kind, f, sms, shape, st);
     if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (out == FTB_OK && info) {
         info->frac_bits = frac;

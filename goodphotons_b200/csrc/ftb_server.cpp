@@ -160,7 +160,7 @@ void admit_locked(ftb_server* s) {
 // Wave table: every job with photons left gets min(left, W / (4 * jobs)) slots, then the
 // remaining capacity goes to the jobs with the least work left.  One entry per job (mu held).
 int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::vector<Job*>& members,
-                           int32_t& max_bounce, bool& inst, bool& bundle_wave) {
+                           int32_t& max_bounce, ftb::WaveKind& kind) {
     std::vector<Job*> c;
     for (Job* j : s->active)
         if (j->next < j->req.n_photons) c.push_back(j);
@@ -187,8 +187,8 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
     }
     int32_t slots = 0;
     max_bounce = 0;
-    inst = false;
-    bundle_wave = bundles;
+    kind = ftb::WaveKind{};
+    kind.bundles = bundles;
     for (size_t i = 0; i < c.size(); ++i) {
         if (give[i] <= 0) continue;
         Job* j = c[i];
@@ -211,7 +211,8 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
         j->pending++;
         slots += J.n;
         max_bounce = std::max(max_bounce, J.max_bounce);
-        inst |= J.sc.n_inst > 0;
+        kind.instances |= J.sc.n_inst > 0;
+        kind.media |= J.sc.n_med > 0;
     }
     return slots;
 }
@@ -248,11 +249,11 @@ void scheduler(ftb_server* s) {
         table.clear();
         members.clear();
         int32_t slots = 0, mb = 0;
-        bool inst = false, bundles = false;
+        ftb::WaveKind kind;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             admit_locked(s);
-            slots = build_table_locked(s, table, members, mb, inst, bundles);
+            slots = build_table_locked(s, table, members, mb, kind);
             if (slots == 0) {
                 bool busy = s->ws[0].busy || s->ws[1].busy;
                 if (!busy) {
@@ -283,7 +284,7 @@ void scheduler(ftb_server* s) {
         f.stats = nullptr;
         f.status = s->d_status + 16 * b;
         if (e == cudaSuccess)
-            e = ftb::launch_wave(w.wave, mb, inst, bundles, f, s->sms, s->shape, w.stream, nullptr, w.graphs);
+            e = ftb::launch_wave(w.wave, mb, kind, f, s->sms, s->shape, w.stream, nullptr, w.graphs);
         if (e == cudaSuccess) e = cudaEventRecord(w.done, w.stream);
         {
             std::lock_guard<std::mutex> lk(s->mu);

@@ -906,13 +906,17 @@ __device__ __forceinline__ int agg_inc(int32_t* ctr) {
     return g.shfl(base, 0) + (int)g.thread_rank();
 }
 
+// A one-wavelength connection: the film increments cieX/Y/Z(lambda) * contribution in the
+// order Film::add forms them (scene_film.h:12), from the matching functions evaluated once
+// per path at emission.
 __device__ __forceinline__ void push_shadow(const Wave& w, const Frame& f, int job, int view, D3 o, D3 d,
-                                            double tmax, double val, double lam, int pix) {
+                                            double tmax, double val, const double* cie, int pix) {
     int i = agg_inc(&w.counts[2]);
     if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
     w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
     w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
-    w.smax[i] = tmax; w.sval[i] = val; w.slam[i] = lam; w.spix[i] = pix;
+    w.smax[i] = tmax; w.spix[i] = pix;
+    w.sxyz[i] = cie[0] * val; w.sxyz[w.S + i] = cie[1] * val; w.sxyz[2 * (size_t)w.S + i] = cie[2] * val;
     w.sjob[i] = job; w.sview[i] = view;
 }
 
@@ -929,7 +933,7 @@ __device__ __forceinline__ int64_t* view_film(const DevJob& J, int v) {
 // k_shadow, the rest of the contribution is formed here in the reference's order.
 template <bool MEDIA>
 __device__ void connect_surface(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f, int job,
-                                D3 p, D3 n, D3 ng, D3 wi, double lam, double beta, double rho) {
+                                D3 p, D3 n, D3 ng, D3 wi, double lam, const double* cie, double beta, double rho) {
     for (int v = 0; v < view_count(J); ++v) {
         const DevCam& cam = view_cam(J, v);
         D3 to_cam = ld3(cam.eye) - p;
@@ -947,12 +951,12 @@ __device__ void connect_surface(const DevScene& sc, const DevJob& J, const Wave&
         double fr = rho / PI_D;
         double contrib = beta * fr * cos_surf * corr / denom * stg;
         if (MEDIA && sc.n_med > 0) contrib *= media_transmittance(sc, p, wdir, dist, lam);
-        push_shadow(w, f, job, v, p + ng * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+        push_shadow(w, f, job, v, p + ng * 1e-6, wdir, dist - 2e-6, contrib, cie, py * cam.rx + px);
     }
 }
 // connectVolume (render.h:584-600)
 __device__ void connect_volume(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f, int job,
-                               const DevMed& m, D3 p, D3 win, double lam, double beta) {
+                               const DevMed& m, D3 p, D3 win, double lam, const double* cie, double beta) {
     for (int v = 0; v < view_count(J); ++v) {
         const DevCam& cam = view_cam(J, v);
         D3 to_cam = ld3(cam.eye) - p;
@@ -965,7 +969,7 @@ __device__ void connect_volume(const DevScene& sc, const DevJob& J, const Wave& 
         double omega = cam_pixel_solid_angle(cam, cos_cam);
         double contrib = beta * alb * ph / (dist2 * omega);
         contrib *= media_transmittance(sc, p, wdir, dist, lam);
-        push_shadow(w, f, job, v, p + wdir * 1e-6, wdir, dist - 2e-6, contrib, lam, py * cam.rx + px);
+        push_shadow(w, f, job, v, p + wdir * 1e-6, wdir, dist - 2e-6, contrib, cie, py * cam.rx + px);
     }
 }
 
@@ -1117,7 +1121,8 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
         double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
         beta *= 1.0;
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(beta, J.tally_scale_inv, f.status));
-        connect_surface<MEDIA>(sc, J, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
+        const double cie[3] = {cie_x(lam), cie_y(lam), cie_z(lam)};
+        connect_surface<MEDIA>(sc, J, w, f, j, origin, emit_n, emit_n, emit_n, lam, cie, beta, 1.0);
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
@@ -1128,6 +1133,7 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
         w.ox[slot] = ro.x; w.oy[slot] = ro.y; w.oz[slot] = ro.z;
         w.dx[slot] = dir.x; w.dy[slot] = dir.y; w.dz[slot] = dir.z;
         w.lam[slot] = lam; w.beta[slot] = beta;
+        w.cie[slot] = cie[0]; w.cie[w.W + slot] = cie[1]; w.cie[2 * (size_t)w.W + slot] = cie[2];
         w.stk_n[slot] = 0;
         int q = agg_inc(&w.counts[0]);
         w.qa[q] = slot;
@@ -1265,6 +1271,10 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
         D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
         double lam = w.lam[slot], beta = w.beta[slot];
+        double cie[3];   // read only by the paths that connect
+        auto load_cie = [&]() {
+            cie[0] = w.cie[slot]; cie[1] = w.cie[w.W + slot]; cie[2] = w.cie[2 * (size_t)w.W + slot];
+        };
         double ht = w.hit_t[slot];
         int rec = w.hit_rec[slot];
         Stk stk; stk.n = w.stk_n[slot];
@@ -1300,7 +1310,8 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         D3 no = ro, nd = rd;
         if (medium_event) {   // render.h:2105-2115
             const DevMed& sm = sc.med[scatter_med];
-            connect_volume(sc, J, w, f, j, sm, mp, rd, lam, beta);
+            load_cie();
+            connect_volume(sc, J, w, f, j, sm, mp, rd, lam, cie, beta);
             if (uniform(rng) >= med_albedo(sc, sm, lam)) fate = 0;
             else { nd = sample_hg(rd, sm.g, rng); no = mp; }
         } else if (!valid) {
@@ -1371,8 +1382,9 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
                 if (sum > 1.0) { rr /= sum; rt /= sum; sum = 1.0; }
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr);
-                connect_surface<MEDIA>(sc, J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt);
+                load_cie();
+                connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, cie, beta, rr);
+                connect_surface<MEDIA>(sc, J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, cie, beta, rt);
                 double u = uniform(rng);
                 if (u < rr) {
                     D3 wo = cosine_hemisphere(h.n, rng);
@@ -1389,7 +1401,8 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
                 double rho = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
-                connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho);
+                load_cie();
+                connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, cie, beta, rho);
                 if (uniform(rng) >= rho) { fate = 0; break; }
                 D3 wo = cosine_hemisphere(h.n, rng);
                 beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
@@ -1443,8 +1456,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
         RayCtx R = make_ray(o, d);
         if (COUNT) rays++;
         if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
-        double lam = w.slam[i], c = w.sval[i];
-        double X = cie_x(lam) * c, Y = cie_y(lam) * c, Z = cie_z(lam) * c;
+        const double X = w.sxyz[i], Y = w.sxyz[w.S + i], Z = w.sxyz[2 * (size_t)w.S + i];
         long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i])) + 4 * (size_t)w.spix[i];
         atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, f.status));
         atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, J.film_scale_inv, f.status));
@@ -1840,7 +1852,7 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     w.rng_s = (uint64_t*)take(8 * wn); w.rng_i = (uint64_t*)take(8 * wn);
     w.ox = (double*)take(8 * wn); w.oy = (double*)take(8 * wn); w.oz = (double*)take(8 * wn);
     w.dx = (double*)take(8 * wn); w.dy = (double*)take(8 * wn); w.dz = (double*)take(8 * wn);
-    w.lam = (double*)take(8 * wn); w.beta = (double*)take(8 * wn);
+    w.lam = (double*)take(8 * wn); w.beta = (double*)take(8 * wn); w.cie = (double*)take(24 * wn);
     w.stk_n = (int32_t*)take(4 * wn); w.stk = (int2*)take(8 * wn * kStkCap);
     w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn); w.hit_sub = (int32_t*)take(4 * wn);
     w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
@@ -1851,6 +1863,7 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
     w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
     w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
+    w.sxyz = (double*)take(24 * sn);
     w.spix = (int32_t*)take(4 * sn);
     w.sview = (int32_t*)take(4 * sn);
     if (log) {

@@ -49,6 +49,7 @@ struct Wave {
     int32_t S;                 // shadow-record capacity
     uint64_t* rng_s; uint64_t* rng_i;
     double *ox, *oy, *oz, *dx, *dy, *dz, *lam, *beta;
+    double* cie;               // [3][W] the CIE matching functions at the path's wavelength
     int32_t* stk_n;            // medium-stack depth per slot
     int2* stk;                 // [kStkCap][W] (material, priority)
     double* hit_t;
@@ -62,6 +63,7 @@ struct Wave {
     DevJob* jobs;              // device job table, kWaveJobs entries
     int32_t* params;           // [0] jobs in the table, [1] slots in use (written with the table)
     double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
+    double* sxyz;              // [3][S] film increments (X, Y, Z) of one-wavelength connections
     int32_t* spix;
     int32_t* sview;            // view of each connection (multi-camera jobs)
     // hero-wavelength bundles (hero > 1 only; null otherwise)
@@ -97,13 +99,13 @@ constexpr size_t wave_bytes(int32_t W, bool log, int32_t hero = 1) {
     size_t w = (size_t)W, s = 2 * (size_t)W;
     size_t b = 0;
     b += 2 * wave_align(8 * w);                                     // rng
-    b += 8 * wave_align(8 * w);                                     // ray + lam + beta
+    b += 8 * wave_align(8 * w) + wave_align(24 * w);                // ray + lam + beta + cie
     b += wave_align(4 * w) + wave_align(8 * w * kStkCap);           // medium stack
     b += wave_align(8 * w) + 2 * wave_align(4 * w);                 // hit t, record, sub-record
     b += 2 * wave_align(4 * w) + wave_align(64);                    // queues + counts
     b += wave_align(4 * w) + wave_align(4 * s) + wave_align(sizeof(DevJob) * kWaveJobs);   // job ids + table
     b += wave_align(64);                                            // table parameters
-    b += 9 * wave_align(8 * s) + 2 * wave_align(4 * s);             // shadow records
+    b += 9 * wave_align(8 * s) + wave_align(24 * s) + 2 * wave_align(4 * s);   // shadow records
     if (log) b += wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
     if (hero > 1)                                                   // bundles
         b += 2 * wave_align(8 * w * hero) + wave_align(4 * w) + 2 * wave_align(8 * s * (hero - 1)) +

@@ -386,7 +386,7 @@ ftb_status ftb_trace_log(ftb_scene* scene, const ftb_camera* cam,
  * start-up (ftb_scene_create allocates); then this call only launches kernels and async
  * memsets on `stream`, accumulating into the caller's DEVICE film like
  * ftb_render_forward_device.  Its scratch (one wave of path state, queues, shadow records,
- * tallies and status: ~9.5 MB) is a fixed device array in the library, held by every GPU
+ * tallies and status: ~12.7 MB) is a fixed device array in the library, held by every GPU
  * that loads the library until exit.  Limit: n_photons <= FTB_NOALLOC_MAX_PHOTONS per call
  * (larger requests return FTB_ERR_TOO_LARGE; render more with consecutive seed_base).  The
  * first call on a device resolves the array's device address (cudaGetSymbolAddress) with

@@ -490,7 +490,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--photons", type=int, default=0, help="photons per step (default: the workload's frame)")
-    ap.add_argument("--tuning", default="", help="wave_slots,blocks_per_sm,graphs instead of the autotuner")
+    ap.add_argument("--tuning", default="", help="wave_slots,blocks_per_sm,graphs[,sort_rays] instead of the autotuner")
     ap.add_argument("--hero", type=int, default=1, help="wavelengths per photon (hero bundles when > 1)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -565,12 +565,13 @@ def main():
     # autotuner (untimed): grid size, wave size and graph replay for this workload
     t = time.perf_counter()
     if args.tuning:   # a fixed setting instead (reproducible launch sequences for profiling)
-        slots, grid, graphs = (int(x) for x in args.tuning.split(","))
-        tuning = L.set_tuning(local, wave_slots=slots, grid_mult=grid, use_graphs=graphs)
+        v = [int(x) for x in args.tuning.split(",")] + [0]
+        tuning = L.set_tuning(local, wave_slots=v[0], grid_mult=v[1], use_graphs=v[2], sort_rays=v[3])
     else:
         tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)   # (one wavelength per photon)
     cfg["tuning"] = {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
-                     "graph_replay": bool(tuning.use_graphs), "autotune_s": round(time.perf_counter() - t, 2)}
+                     "graph_replay": bool(tuning.use_graphs), "sort_rays": bool(tuning.sort_rays),
+                     "autotune_s": round(time.perf_counter() - t, 2)}
 
     for w in range(args.warmup):
         step(1000 + w)

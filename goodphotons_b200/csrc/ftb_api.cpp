@@ -297,6 +297,13 @@ bool g_tuning_set[256] = {};
 
 ftb_tuning default_tuning() { return ftb_tuning{1 << 22, 16, 1, 0}; }
 
+void apply_tuning(Engine& e, const ftb_tuning& t) {
+    e.wave_cap = t.wave_slots;
+    e.shape.grid_mult = t.grid_mult;
+    e.shape.graph = t.use_graphs != 0;
+    e.shape.sort_rays = t.sort_rays != 0;
+}
+
 // The device's engine, created on first use; it lives while any scene holds it.
 std::shared_ptr<Engine> engine_for(int device) {
     std::lock_guard<std::mutex> lk(g_engine_mu);
@@ -304,10 +311,7 @@ std::shared_ptr<Engine> engine_for(int device) {
     if (!e) {
         e = std::make_shared<Engine>();
         e->device = device;
-        const ftb_tuning t = g_tuning_set[device] ? g_tuning[device] : default_tuning();
-        e->wave_cap = t.wave_slots;
-        e->shape.grid_mult = t.grid_mult;
-        e->shape.graph = t.use_graphs != 0;
+        apply_tuning(*e, g_tuning_set[device] ? g_tuning[device] : default_tuning());
         g_engines[device] = e;
     }
     return e;
@@ -1372,9 +1376,7 @@ ftb_status ftb_set_tuning(int32_t device, const ftb_tuning* t) {
     }
     if (e) {
         std::lock_guard<std::mutex> lk(e->mu);
-        e->wave_cap = t->wave_slots;
-        e->shape.grid_mult = t->grid_mult;
-        e->shape.graph = t->use_graphs != 0;
+        apply_tuning(*e, *t);
     }
     return FTB_OK;
 }
@@ -1414,14 +1416,15 @@ ftb_status ftb_autotune(ftb_scene* s, const ftb_camera* cam, int64_t n, int32_t 
         return r;
     };
     if (ce == cudaSuccess) {
-        // one knob at a time from the current setting: grid, then wave size, then graphs
+        // one knob at a time from the current setting: grid, wave size, graphs, ray reordering
         const int grids[] = {4, 8, 16, 32};
         const int waves[] = {1 << 20, 1 << 21, 1 << 22};
-        for (int pass = 0; pass < 3 && st == FTB_OK; ++pass) {
+        for (int pass = 0; pass < 4 && st == FTB_OK; ++pass) {
             std::vector<ftb_tuning> cand;
             if (pass == 0) for (int g : grids) { ftb_tuning t = best; t.grid_mult = g; cand.push_back(t); }
             if (pass == 1) for (int w : waves) { ftb_tuning t = best; t.wave_slots = w; cand.push_back(t); }
             if (pass == 2) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.use_graphs = u; cand.push_back(t); }
+            if (pass == 3) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.sort_rays = u; cand.push_back(t); }
             for (const ftb_tuning& t : cand) {
                 double ms = 0;
                 st = trial(t, ms);

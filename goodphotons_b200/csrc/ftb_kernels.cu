@@ -1192,6 +1192,68 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const Dev
     }
 }
 
+// Optional reordering of a closest-hit queue by ray direction: pieces of kSortChunk entries
+// are bucketed by an 8-bit direction key (an octahedral 16 x 16 grid in Morton order), so
+// the lanes of a warp head the same way.  The order of rays does not change any result.
+constexpr int kSortChunk = 1024;
+
+__device__ __forceinline__ uint32_t direction_key(D3 d) {
+    float x = (float)d.x, y = (float)d.y, z = (float)d.z;
+    const float s = fabsf(x) + fabsf(y) + fabsf(z);
+    x /= s; y /= s; z /= s;
+    if (z < 0.0f) {   // fold the lower hemisphere onto the octahedron's outer triangles
+        const float fx = (1.0f - fabsf(y)) * copysignf(1.0f, x);
+        const float fy = (1.0f - fabsf(x)) * copysignf(1.0f, y);
+        x = fx; y = fy;
+    }
+    uint32_t u = (uint32_t)min(15, max(0, (int)((x * 0.5f + 0.5f) * 16.0f)));
+    uint32_t v = (uint32_t)min(15, max(0, (int)((y * 0.5f + 0.5f) * 16.0f)));
+    u = (u | (u << 2)) & 0x33u; u = (u | (u << 1)) & 0x55u;   // 4-bit Morton interleave
+    v = (v | (v << 2)) & 0x33u; v = (v | (v << 1)) & 0x55u;
+    return u | (v << 1);
+}
+
+// Reorders each kSortChunk-entry piece of a queue by direction key, in place (one block per
+// piece, counting sort in shared memory).  The closest-hit kernel then reads the queue as
+// usual: a warp's 32 lanes take 32 consecutive entries.
+__global__ void __launch_bounds__(128) k_sort_queue(Wave w, int32_t* q, const int32_t* qcount) {
+    __shared__ int32_t hist[256];
+    const int nq = *qcount;
+    constexpr int kPer = kSortChunk / 128;
+    for (int base = blockIdx.x * kSortChunk; base < nq; base += gridDim.x * kSortChunk) {
+        for (int t = threadIdx.x; t < 256; t += 128) hist[t] = 0;
+        __syncthreads();
+        int slot[kPer], key[kPer], off[kPer];
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) {
+            const int i = base + r * 128 + threadIdx.x;
+            slot[r] = i < nq ? q[i] : -1;
+            key[r] = slot[r] >= 0 ? (int)direction_key(mk(w.dx[slot[r]], w.dy[slot[r]], w.dz[slot[r]])) : 255;
+            off[r] = slot[r] >= 0 ? atomicAdd(&hist[key[r]], 1) : 0;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {   // exclusive scan of the 256 bucket counts by one warp
+            int v[8], run = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) { v[k] = hist[threadIdx.x * 8 + k]; run += v[k]; }
+            int incl = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((int)threadIdx.x >= o) incl += y;
+            }
+            int acc = incl - run;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) { hist[threadIdx.x * 8 + k] = acc; acc += v[k]; }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kPer; ++r)
+            if (slot[r] >= 0) q[base + hist[key[r]] + off[r]] = slot[r];
+        __syncthreads();   // before the next piece reuses the histogram
+    }
+}
+
 // medium stack (medium_stack.h:17-47), kStkCap entries per slot
 struct Stk { int n; int2 e[kStkCap]; };
 __device__ __forceinline__ int stk_top_pri(const Stk& s) {
@@ -1895,8 +1957,8 @@ namespace {
 // shading and the connections it queued.  Every launch reads the wave's job count and
 // slot count from w.params, so the same sequence serves any table (and one captured graph
 // serves every wave of its shape).
-void issue_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int grid, cudaStream_t st,
-                LaunchSink* sink) {
+void issue_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int grid, bool sorted,
+                cudaStream_t st, LaunchSink* sink) {
     const bool inst = kind.instances, hero = kind.bundles, media = kind.media;
     const int T = 128;
     const DevJob* jobs = w.jobs;
@@ -1935,6 +1997,10 @@ void issue_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& 
     int32_t* cb = &w.counts[1];
     for (int b = 0; b < max_bounce; ++b) {
         mark(K_EXTEND, false);
+        if (sorted) {
+            const int gs = std::max(1, std::min(grid, (w.W + kSortChunk - 1) / kSortChunk));
+            k_sort_queue<<<gs, T, 0, st>>>(w, qa, ca);
+        }
         if (count) {
             if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
             else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
@@ -1966,7 +2032,7 @@ void issue_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& 
 struct WaveGraphs {
     struct Entry {
         int32_t max_bounce, grid;
-        bool inst, hero, media;
+        bool inst, hero, media, sorted;
         int32_t* status;
         cudaGraphExec_t exec;
     };
@@ -1989,20 +2055,21 @@ cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const
     // A graph bakes the kernel arguments: the wave's buffers and status word are fixed for the
     // life of its cache, but a log buffer changes per call, so logging waves launch directly.
     if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
-        issue_wave(w, max_bounce, kind, f, grid, st, sink);
+        issue_wave(w, max_bounce, kind, f, grid, shape.sort_rays, st, sink);
         return cudaGetLastError();
     }
     for (auto& e : graphs->entries)
         if (e.max_bounce == max_bounce && e.grid == grid && e.inst == kind.instances && e.hero == kind.bundles &&
-            e.media == kind.media && e.status == f.status)
+            e.media == kind.media && e.sorted == shape.sort_rays && e.status == f.status)
             return cudaGraphLaunch(e.exec, st);
     cudaGraph_t g = nullptr;
     cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) return err;
-    issue_wave(w, max_bounce, kind, f, grid, st, nullptr);
+    issue_wave(w, max_bounce, kind, f, grid, shape.sort_rays, st, nullptr);
     err = cudaStreamEndCapture(st, &g);
     if (err != cudaSuccess) return err;
-    WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, f.status, nullptr};
+    WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, shape.sort_rays, f.status,
+                        nullptr};
     err = cudaGraphInstantiate(&e.exec, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) return err;

@@ -127,11 +127,13 @@ struct LaunchSink {
     virtual ~LaunchSink() {}
 };
 
-// Launch shape chosen by the autotuner: blocks per SM of the queue-driven kernels, and
-// whether a wave is replayed from a captured CUDA graph.
+// Launch shape chosen by the autotuner: blocks per SM of the queue-driven kernels, whether a
+// wave is replayed from a captured CUDA graph, and whether closest-hit rays are reordered by
+// direction within each block.
 struct LaunchShape {
     int32_t grid_mult = 16;
     bool graph = true;
+    bool sort_rays = false;   // reorder each block's closest-hit rays by direction first
 };
 
 // Instantiated graphs of one wave buffer, by (bounce cap, grid, instance variant, status

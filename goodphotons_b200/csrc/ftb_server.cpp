@@ -384,6 +384,14 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
     s->max_active = cfg->max_active ? cfg->max_active : 64;
     s->W = cfg->wave_slots ? cfg->wave_slots : (1 << 22);
     s->hero_max = cfg->hero_max > 0 ? (cfg->hero_max > ftb::kHeroMax ? ftb::kHeroMax : cfg->hero_max) : 4;
+    {   // launch shape: the device's current tuning (ftb_set_tuning / ftb_autotune)
+        ftb_tuning t;
+        if (ftb_get_tuning(cfg->device, &t) == FTB_OK) {
+            s->shape.grid_mult = t.grid_mult;
+            s->shape.graph = t.use_graphs != 0;
+            s->shape.sort_rays = t.sort_rays != 0;
+        }
+    }
     s->t0 = Clock::now();
     set_device(s);
     cudaDeviceProp p;

@@ -417,16 +417,17 @@ ftb_status ftb_scene_set_profiling(ftb_scene* scene, int32_t mode);
 ftb_status ftb_scene_profile(ftb_scene* scene, ftb_kernel_profile* out, int32_t reset);
 
 /* ---- launch tuning (no counterpart in the reference) ---------------------------------
- * How a device's renders are launched: photon slots per wave (path state is ~300 B per
- * slot, two waves in flight), blocks per SM of the queue-driven kernels, and whether each
- * wave's bounce loop (about 5 launches per bounce) is replayed from a captured CUDA graph.
+ * How a device's renders are launched: photon slots per wave (path state is ~400 B per
+ * slot, two waves in flight), blocks per SM of the queue-driven kernels, whether each
+ * wave's bounce loop (about 5 launches per bounce) is replayed from a captured CUDA graph,
+ * and whether closest-hit rays are bucketed by direction before traversal.
  * Renders on the device use the setting current when they start; results do not depend on
  * it (photons are keyed by index, films are fixed point). */
 typedef struct ftb_tuning {
     int32_t wave_slots;   /* 1 .. 2^22 */
     int32_t grid_mult;    /* 1 .. 64 */
     int32_t use_graphs;   /* 0 / 1 */
-    int32_t pad;
+    int32_t sort_rays;    /* 0 / 1: reorder closest-hit rays by direction within each block */
 } ftb_tuning;
 
 ftb_status ftb_get_tuning(int32_t device, ftb_tuning* out);

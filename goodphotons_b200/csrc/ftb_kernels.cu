@@ -12,6 +12,12 @@
 //   k_shadow  any-hit test of the queued connections (Scene::occluded, scene.h:2249) and
 //             the splat into the 64-bit fixed-point film (Film::add, scene_film.h:12)
 //
+// Variants: k_emit_hero / k_shade_hero / k_shadow_hero trace hero-wavelength bundles (one
+// path carries up to kHeroMax wavelengths), and the kernels are templated on whether the
+// wave's scenes have instances or participating media, so a wave launches only the code
+// its scenes need.  k_sort_queue optionally buckets a closest-hit queue by ray direction.
+// A wave's launch sequence is captured once as a CUDA graph and replayed (launch_wave).
+//
 // Numerics.  Everything that decides a path -- triangle/sphere/curve tests, hit points,
 // normals, BSDF sampling, Russian roulette, the camera projection -- is computed in fp64
 // in the reference's operation order, and this file is compiled with -fmad=false so no

@@ -490,7 +490,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--photons", type=int, default=0, help="photons per step (default: the workload's frame)")
-    ap.add_argument("--tuning", default="", help="wave_slots,blocks_per_sm,graphs[,sort_rays] instead of the autotuner")
+    ap.add_argument("--tuning", default="",
+                    help="wave_slots,blocks_per_sm,graphs[,sort_rays[,regenerate]] instead of the autotuner")
     ap.add_argument("--hero", type=int, default=1, help="wavelengths per photon (hero bundles when > 1)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -565,12 +566,15 @@ def main():
     # autotuner (untimed): grid size, wave size and graph replay for this workload
     t = time.perf_counter()
     if args.tuning:   # a fixed setting instead (reproducible launch sequences for profiling)
-        v = [int(x) for x in args.tuning.split(",")] + [0]
-        tuning = L.set_tuning(local, wave_slots=v[0], grid_mult=v[1], use_graphs=v[2], sort_rays=v[3])
+        v = [int(x) for x in args.tuning.split(",")]
+        v += [0, 1][len(v) - 3:]
+        tuning = L.set_tuning(local, wave_slots=v[0], grid_mult=v[1], use_graphs=v[2], sort_rays=v[3],
+                              regenerate=v[4])
     else:
         tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)   # (one wavelength per photon)
     cfg["tuning"] = {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
                      "graph_replay": bool(tuning.use_graphs), "sort_rays": bool(tuning.sort_rays),
+                     "regenerate": bool(tuning.regenerate),
                      "autotune_s": round(time.perf_counter() - t, 2)}
 
     for w in range(args.warmup):

@@ -131,7 +131,7 @@ class KernelProfile(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("wave_slots", C.c_int32), ("grid_mult", C.c_int32), ("use_graphs", C.c_int32),
-                ("sort_rays", C.c_int32)]
+                ("sort_rays", C.c_int32), ("regenerate", C.c_int32)]
 
 
 class ServerConfig(C.Structure):

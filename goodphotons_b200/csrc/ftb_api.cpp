@@ -171,8 +171,10 @@ struct JobStage {
         }
         return cudaSuccess;
     }
-    // The table and its parameters {jobs, slots} into the wave (w.jobs, w.params).
-    cudaError_t push(const ftb::DevJob* jobs, int n, int32_t slots, ftb::Wave& w, cudaStream_t st) {
+    // The table and its parameters {jobs, slots} into the wave (w.jobs, w.params); a
+    // streaming pass adds its photon count and half-iteration cap (int64 at [1], [2]).
+    cudaError_t push(const ftb::DevJob* jobs, int n, int32_t slots, ftb::Wave& w, cudaStream_t st,
+                     int64_t photons = 0, int64_t half_cap = 0) {
         int e = next;
         next = (next + 1) % kRing;
         cudaError_t r = cudaEventSynchronize(ev[e]);
@@ -182,8 +184,10 @@ struct JobStage {
         int32_t* par = reinterpret_cast<int32_t*>(h + ftb::kWaveJobs);
         par[0] = n;
         par[1] = slots;
+        reinterpret_cast<int64_t*>(par)[1] = photons;
+        reinterpret_cast<int64_t*>(par)[2] = half_cap;
         r = cudaMemcpyAsync(w.jobs, h, sizeof(ftb::DevJob) * (size_t)n, cudaMemcpyHostToDevice, st);
-        if (r == cudaSuccess) r = cudaMemcpyAsync(w.params, par, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, st);
+        if (r == cudaSuccess) r = cudaMemcpyAsync(w.params, par, 6 * sizeof(int32_t), cudaMemcpyHostToDevice, st);
         if (r != cudaSuccess) return r;
         return cudaEventRecord(ev[e], st);
     }
@@ -295,13 +299,14 @@ std::weak_ptr<Engine> g_engines[256];
 ftb_tuning g_tuning[256];          // per device; a new engine starts from it
 bool g_tuning_set[256] = {};
 
-ftb_tuning default_tuning() { return ftb_tuning{1 << 22, 16, 1, 0}; }
+ftb_tuning default_tuning() { return ftb_tuning{1 << 22, 16, 1, 0, 0}; }
 
 void apply_tuning(Engine& e, const ftb_tuning& t) {
     e.wave_cap = t.wave_slots;
     e.shape.grid_mult = t.grid_mult;
     e.shape.graph = t.use_graphs != 0;
     e.shape.sort_rays = t.sort_rays != 0;
+    e.shape.regenerate = t.regenerate != 0;
 }
 
 // The device's engine, created on first use; it lives while any scene holds it.
@@ -646,6 +651,58 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
     int64_t done_in_job = 0;
     int k = 0;
     std::vector<ftb::DevJob> table;
+    // Streaming passes: up to kWaveJobs photon ranges of one class (bundles or not) and one
+    // view count, traced with every freed slot refilled, so the device stays full until the
+    // pass's last photons.
+    while (s->eng->shape.regenerate && j < base.size()) {
+        table.clear();
+        int64_t g = 0;
+        int32_t max_bounce = 0, slots = W;
+        bool inst = false, media = false;
+        int bundles = -1, views = -1;
+        while (j < base.size() && (int)table.size() < ftb::kWaveJobs) {
+            const int64_t left = count[j] - done_in_job;
+            if (left <= 0) { ++j; done_in_job = 0; continue; }
+            const int is_bundle = base[j].hero_c > 1 ? 1 : 0;
+            const int nv = std::max(1, base[j].n_views);
+            if ((bundles >= 0 && is_bundle != bundles) || (views >= 0 && nv != views)) break;
+            bundles = is_bundle;
+            views = nv;
+            // a path queues at most 2 connections per view per bounce and a refilled slot one
+            // more per view; the shadow queue holds 3W records, so V views get W / V slots
+            slots = std::max(1, W / nv);
+            const int64_t m = std::min<int64_t>(left, (int64_t)1 << 30);
+            ftb::DevJob J = base[j];
+            J.photon0 = seed[j] + (uint64_t)done_in_job;
+            J.g0 = g;
+            J.slot0 = 0;
+            J.n = (int32_t)m;
+            table.push_back(J);
+            max_bounce = std::max(max_bounce, J.max_bounce);
+            inst |= J.sc.n_inst > 0;
+            media |= J.sc.n_med > 0;
+            g += m;
+            done_in_job += m;
+            if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
+        }
+        if (table.empty()) break;
+        slots = (int32_t)std::min<int64_t>(slots, std::max<int64_t>(1, g));
+        ftb::Wave& w = s->eng->waves[k & 1];
+        cudaStream_t ws = s->eng->streams[k & 1];
+        w.logs = d_logs;
+        w.log_base = log_base;
+        cudaError_t e = s->eng->stage[k & 1].push(table.data(), (int)table.size(), slots, w, ws, g,
+                                                  ftb::stream_half_cap(g, slots, max_bounce));
+        if (e != cudaSuccess) return cuda_fail(e, "job table upload");
+        ftb::WaveKind kind;
+        kind.instances = inst;
+        kind.bundles = bundles == 1;
+        kind.media = media;
+        e = ftb::launch_stream(w, kind, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
+                               s->eng->graphs[k & 1]);
+        if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+        ++k;
+    }
     while (j < base.size()) {
         table.clear();
         int32_t slots = 0, max_bounce = 0;
@@ -717,6 +774,7 @@ ftb_status read_status(ftb_scene* s) {
         if (stv & ftb::ST_FILM_SATURATED) m += " film fixed-point saturation (lower frac_bits);";
         if (stv & ftb::ST_MEDIUM_STACK) m += " nested dielectrics deeper than 4;";
         if (stv & ftb::ST_QUEUE_OVERFLOW) m += " shadow queue overflow;";
+        if (stv & ftb::ST_LOOP_CAP) m += " streaming pass iteration cap reached with work left;";
         return fail(FTB_ERR_DEVICE_LIMIT, m);
     }
     return FTB_OK;
@@ -1416,15 +1474,17 @@ ftb_status ftb_autotune(ftb_scene* s, const ftb_camera* cam, int64_t n, int32_t 
         return r;
     };
     if (ce == cudaSuccess) {
-        // one knob at a time from the current setting: grid, wave size, graphs, ray reordering
+        // one knob at a time from the current setting: slot refill, grid, wave size, graphs,
+        // ray reordering
         const int grids[] = {4, 8, 16, 32};
         const int waves[] = {1 << 20, 1 << 21, 1 << 22};
-        for (int pass = 0; pass < 4 && st == FTB_OK; ++pass) {
+        for (int pass = 0; pass < 5 && st == FTB_OK; ++pass) {
             std::vector<ftb_tuning> cand;
-            if (pass == 0) for (int g : grids) { ftb_tuning t = best; t.grid_mult = g; cand.push_back(t); }
-            if (pass == 1) for (int w : waves) { ftb_tuning t = best; t.wave_slots = w; cand.push_back(t); }
-            if (pass == 2) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.use_graphs = u; cand.push_back(t); }
-            if (pass == 3) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.sort_rays = u; cand.push_back(t); }
+            if (pass == 0) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.regenerate = u; cand.push_back(t); }
+            if (pass == 1) for (int g : grids) { ftb_tuning t = best; t.grid_mult = g; cand.push_back(t); }
+            if (pass == 2) for (int w : waves) { ftb_tuning t = best; t.wave_slots = w; cand.push_back(t); }
+            if (pass == 3) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.use_graphs = u; cand.push_back(t); }
+            if (pass == 4) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.sort_rays = u; cand.push_back(t); }
             for (const ftb_tuning& t : cand) {
                 double ms = 0;
                 st = trial(t, ms);

@@ -1047,14 +1047,99 @@ __device__ __forceinline__ uint64_t fnv_i32(uint64_t h, int32_t v) {
 }
 
 // Per-slot instrumentation (parity tests only).
-__device__ __forceinline__ void log_finish(const Wave& w, int slot, uint64_t photon, int fate, double beta) {
+__device__ __forceinline__ void log_finish(const Wave& w, int slot, int fate, double beta) {
     if (!w.logs) return;
-    ftb_photon_log& L = w.logs[photon - (uint64_t)w.log_base];
+    ftb_photon_log& L = w.logs[w.pid[slot] - (uint64_t)w.log_base];
     L.n_hits = w.lnh[slot];
     L.fate = fate;
     L.prim_hash = w.lhash[slot];
     L.beta = beta;
     for (int k = 0; k < 8; ++k) L.prims[k] = w.lprims[k * w.W + slot];
+}
+// The log of a photon that ends at emission (it never holds a slot).
+__device__ __forceinline__ void log_emitted(const Wave& w, uint64_t photon, int fate, double beta) {
+    if (!w.logs) return;
+    ftb_photon_log& L = w.logs[photon - (uint64_t)w.log_base];
+    L.n_hits = 0;
+    L.fate = fate;
+    L.prim_hash = 1469598103934665603ULL;
+    L.beta = beta;
+    for (int k = 0; k < 8; ++k) L.prims[k] = -2;
+}
+__device__ __forceinline__ void log_start(const Wave& w, int slot, uint64_t photon) {
+    if (!w.logs) return;
+    w.pid[slot] = photon;
+    w.lhash[slot] = 1469598103934665603ULL; w.lnh[slot] = 0;
+    for (int q = 0; q < 8; ++q) w.lprims[q * w.W + slot] = -2;
+}
+
+// Photon sources of the emission kernels.  A wave gives slot s of its table's range the
+// photon photon0 + (s - slot0); a streaming pass hands out stream indices next .. next+F-1
+// (F = free slots, at most the photons left), maps each to its range's photon, and a photon
+// that survives emission takes a slot off the free stack.
+struct PhotonSource {
+    int64_t n;           // photons this launch emits
+    int64_t next;        // streaming: first stream index
+    int32_t free_n;      // streaming: free-stack height
+};
+template <bool STREAM>
+__device__ __forceinline__ PhotonSource photon_source(const Wave& w) {
+    PhotonSource p;
+    if (STREAM) {
+        const int64_t total = reinterpret_cast<const int64_t*>(w.params)[1];
+        p.next = w.ctl->next;
+        p.free_n = w.ctl->free_n;
+        const int64_t left = total - p.next;
+        p.n = left < (int64_t)p.free_n ? left : (int64_t)p.free_n;
+    } else {
+        p.n = w.params[1];
+        p.next = 0;
+        p.free_n = 0;
+    }
+    return p;
+}
+// Job and photon index of the t-th photon of this launch.
+template <bool STREAM>
+__device__ __forceinline__ int photon_job(const Wave& w, const DevJob* __restrict__ jobs, int n_jobs,
+                                          const PhotonSource& p, int64_t t, uint64_t& photon) {
+    int j = 0;
+    if (STREAM) {
+        const int64_t g = p.next + t;
+        if (n_jobs > 1) {
+            int lo = 0, hi = n_jobs - 1;
+            while (lo < hi) { int mid = (lo + hi + 1) / 2; if (jobs[mid].g0 <= g) lo = mid; else hi = mid - 1; }
+            j = lo;
+        }
+        photon = jobs[j].photon0 + (uint64_t)(g - jobs[j].g0);
+    } else {
+        const int slot = (int)t;
+        if (n_jobs > 1) {
+            int lo = 0, hi = n_jobs - 1;
+            while (lo < hi) { int mid = (lo + hi + 1) / 2; if (jobs[mid].slot0 <= slot) lo = mid; else hi = mid - 1; }
+            j = lo;
+        }
+        photon = jobs[j].photon0 + (uint64_t)(slot - jobs[j].slot0);
+    }
+    return j;
+}
+// The slot a surviving photon is traced in, with its job and log set up.
+template <bool STREAM>
+__device__ __forceinline__ int photon_slot(const Wave& w, const PhotonSource& p, int64_t t, int j, bool multi,
+                                           uint64_t photon) {
+    int slot;
+    if (STREAM) {
+        slot = w.freel[p.free_n - 1 - agg_inc(&w.ctl->taken)];
+        w.nbounce[slot] = 0;
+    } else {
+        slot = (int)t;
+    }
+    if (multi) w.job[slot] = j;
+    log_start(w, slot, photon);
+    return slot;
+}
+// A path that ends: a streaming pass returns its slot to the free stack.
+__device__ __forceinline__ void retire_slot(const Wave& w, int32_t bounce, int slot) {
+    if (bounce < 0) w.freel[agg_inc(&w.ctl->free_n)] = slot;
 }
 
 // ------------------------------------------------------------------ emission -----------
@@ -1094,36 +1179,28 @@ __device__ __forceinline__ double sample_at(const DevEmit& em, double u, double&
 }
 
 // ------------------------------------------------------------------ kernels ------------
-template <bool MEDIA>
-__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f) {
-    const int32_t n_jobs = w.params[0], n_slots = w.params[1];
+template <bool MEDIA, bool STREAM>
+__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f, int32_t* qout,
+                                              int32_t* qout_count) {
+    const int32_t n_jobs = w.params[0];
     const bool multi = n_jobs > 1;
+    const PhotonSource src = photon_source<STREAM>(w);
     TallyAcc acc;
     tally_init(acc);
-    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n_slots; slot += gridDim.x * blockDim.x) {
-        int j = 0;
-        if (multi) {   // the job whose slot range holds this slot
-            int lo = 0, hi = n_jobs - 1;
-            while (lo < hi) { int mid = (lo + hi + 1) / 2; if (jobs[mid].slot0 <= slot) lo = mid; else hi = mid - 1; }
-            j = lo;
-            w.job[slot] = j;
-        }
+    for (int64_t t = blockIdx.x * blockDim.x + threadIdx.x; t < src.n; t += gridDim.x * blockDim.x) {
+        uint64_t k;
+        const int j = photon_job<STREAM>(w, jobs, n_jobs, src, t, k);
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
-        uint64_t k = J.photon0 + (uint64_t)(slot - J.slot0);
         Pcg rng = seed_photon(k);
-        if (w.logs) {
-            w.lhash[slot] = 1469598103934665603ULL; w.lnh[slot] = 0;
-            for (int q = 0; q < 8; ++q) w.lprims[q * w.W + slot] = -2;
-        }
-        if (sc.total_power <= 0.0 || sc.n_emit == 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        if (sc.total_power <= 0.0 || sc.n_emit == 0) { log_emitted(w, k, 4, 0.0); continue; }
         const int ei = select_emitter(sc, rng);
         const DevEmit& em = sc.emit[ei];
         D3 origin, emit_n, dir;
         emit_sample(em, rng, origin, emit_n, dir);
         double pdf;
         double lam = sample_at(em, uniform(rng), pdf);
-        if (pdf <= 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        if (pdf <= 0) { log_emitted(w, k, 4, 0.0); continue; }
         double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
         beta *= 1.0;
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(beta, J.tally_scale_inv, f.status));
@@ -1132,17 +1209,17 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
-            log_finish(w, slot, k, 2, beta);
+            log_emitted(w, k, 2, beta);
             continue;
         }
+        const int slot = photon_slot<STREAM>(w, src, t, j, multi, k);
         w.rng_s[slot] = rng.s; w.rng_i[slot] = rng.inc;
         w.ox[slot] = ro.x; w.oy[slot] = ro.y; w.oz[slot] = ro.z;
         w.dx[slot] = dir.x; w.dy[slot] = dir.y; w.dz[slot] = dir.z;
         w.lam[slot] = lam; w.beta[slot] = beta;
         w.cie[slot] = cie[0]; w.cie[w.W + slot] = cie[1]; w.cie[2 * (size_t)w.W + slot] = cie[2];
         w.stk_n[slot] = 0;
-        int q = agg_inc(&w.counts[0]);
-        w.qa[q] = slot;
+        qout[agg_inc(qout_count)] = slot;
     }
     tally_finish(acc, jobs, multi);
 }
@@ -1479,22 +1556,26 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
             }
             }
         }
-        uint64_t photon = J.photon0 + (uint64_t)(slot - J.slot0);
+        const int32_t b = bounce >= 0 ? bounce : w.nbounce[slot];
         if (fate == 0) {
             tally_add(acc, jobs, multi, j, T_ABS, to_fixed(beta, J.tally_scale_inv, f.status));
-            log_finish(w, slot, photon, 0, beta);
+            log_finish(w, slot, 0, beta);
+            retire_slot(w, bounce, slot);
             continue;
         }
         if (fate == 1) {
             tally_add(acc, jobs, multi, j, T_ESC, to_fixed(beta, J.tally_scale_inv, f.status));
-            log_finish(w, slot, photon, 1, beta);
+            log_finish(w, slot, 1, beta);
+            retire_slot(w, bounce, slot);
             continue;
         }
-        if (bounce + 1 >= J.max_bounce) {
+        if (b + 1 >= J.max_bounce) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
-            log_finish(w, slot, photon, 2, beta);
+            log_finish(w, slot, 2, beta);
+            retire_slot(w, bounce, slot);
             continue;
         }
+        if (bounce < 0) w.nbounce[slot] = b + 1;
         w.rng_s[slot] = rng.s;
         w.ox[slot] = no.x; w.oy[slot] = no.y; w.oz[slot] = no.z;
         w.dx[slot] = nd.x; w.dy[slot] = nd.y; w.dz[slot] = nd.z;
@@ -1600,29 +1681,22 @@ __device__ __forceinline__ double max_of(const double* a, int n) {   // hero::ma
     return m;
 }
 
-__global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f) {
-    const int32_t n_jobs = w.params[0], n_slots = w.params[1];
+template <bool STREAM>
+__global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f, int32_t* qout,
+                                                   int32_t* qout_count) {
+    const int32_t n_jobs = w.params[0];
     const bool multi = n_jobs > 1;
+    const PhotonSource src = photon_source<STREAM>(w);
     TallyAcc acc;
     tally_init(acc);
-    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n_slots; slot += gridDim.x * blockDim.x) {
-        int j = 0;
-        if (multi) {
-            int lo = 0, hi = n_jobs - 1;
-            while (lo < hi) { int mid = (lo + hi + 1) / 2; if (jobs[mid].slot0 <= slot) lo = mid; else hi = mid - 1; }
-            j = lo;
-            w.job[slot] = j;
-        }
+    for (int64_t t = blockIdx.x * blockDim.x + threadIdx.x; t < src.n; t += gridDim.x * blockDim.x) {
+        uint64_t k;
+        const int j = photon_job<STREAM>(w, jobs, n_jobs, src, t, k);
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
         const int C = J.hero_c;
-        uint64_t k = J.photon0 + (uint64_t)(slot - J.slot0);
         Pcg rng = seed_photon(k);
-        if (w.logs) {
-            w.lhash[slot] = 1469598103934665603ULL; w.lnh[slot] = 0;
-            for (int q = 0; q < 8; ++q) w.lprims[q * w.W + slot] = -2;
-        }
-        if (sc.total_power <= 0.0 || sc.n_emit == 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        if (sc.total_power <= 0.0 || sc.n_emit == 0) { log_emitted(w, k, 4, 0.0); continue; }
         const DevEmit& em = sc.emit[select_emitter(sc, rng)];
         D3 origin, emit_n, dir;
         emit_sample(em, rng, origin, emit_n, dir);
@@ -1630,7 +1704,7 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
         double lam[kHeroMax], beta[kHeroMax], one[kHeroMax];
         double u = uniform(rng), pdf;
         lam[0] = sample_at(em, u, pdf);
-        if (pdf <= 0) { log_finish(w, slot, k, 4, 0.0); continue; }
+        if (pdf <= 0) { log_emitted(w, k, 4, 0.0); continue; }
         for (int i = 1; i < C; ++i) {
             double uu = u + (double)i / (double)C;
             if (uu >= 1.0) uu -= 1.0;
@@ -1645,9 +1719,10 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
-            log_finish(w, slot, k, 2, beta[0]);
+            log_emitted(w, k, 2, beta[0]);
             continue;
         }
+        const int slot = photon_slot<STREAM>(w, src, t, j, multi, k);
         w.rng_s[slot] = rng.s; w.rng_i[slot] = rng.inc;
         w.ox[slot] = ro.x; w.oy[slot] = ro.y; w.oz[slot] = ro.z;
         w.dx[slot] = dir.x; w.dy[slot] = dir.y; w.dz[slot] = dir.z;
@@ -1657,8 +1732,7 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
         }
         w.hlive[slot] = C;
         w.stk_n[slot] = 0;
-        int q = agg_inc(&w.counts[0]);
-        w.qa[q] = slot;
+        qout[agg_inc(qout_count)] = slot;
     }
     tally_finish(acc, jobs, multi);
 }
@@ -1840,18 +1914,21 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
             }
         }
         if (absorbed) tally_add(acc, jobs, multi, j, T_ABS, absorbed);
-        uint64_t photon = J.photon0 + (uint64_t)(slot - J.slot0);
+        const int32_t b = bounce >= 0 ? bounce : w.nbounce[slot];
         if (fate >= 0) {
             tally_add(acc, jobs, multi, j, fate == 0 ? T_ABS : T_ESC,
                       to_fixed(sum_of(beta, nup), J.tally_scale_inv, f.status));
-            log_finish(w, slot, photon, fate, beta[0]);
+            log_finish(w, slot, fate, beta[0]);
+            retire_slot(w, bounce, slot);
             continue;
         }
-        if (bounce + 1 >= J.max_bounce) {
+        if (b + 1 >= J.max_bounce) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(sum_of(beta, nup), J.tally_scale_inv, f.status));
-            log_finish(w, slot, photon, 2, beta[0]);
+            log_finish(w, slot, 2, beta[0]);
+            retire_slot(w, bounce, slot);
             continue;
         }
+        if (bounce < 0) w.nbounce[slot] = b + 1;
         w.rng_s[slot] = rng.s;
         w.ox[slot] = no.x; w.oy[slot] = no.y; w.oz[slot] = no.z;
         w.dx[slot] = nd.x; w.dy[slot] = nd.y; w.dz[slot] = nd.z;
@@ -1910,7 +1987,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, cons
 void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     w = Wave{};
     w.W = W;
-    w.S = 2 * W;
+    w.S = kShadowPerSlot * W;
     w.hero = hero > 1 ? hero : 1;
     w.bytes = wave_bytes(W, log, hero);
     w.block = block;
@@ -1928,6 +2005,7 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     w.job = (int32_t*)take(4 * wn); w.sjob = (int32_t*)take(4 * sn);
     w.jobs = (DevJob*)take(sizeof(DevJob) * kWaveJobs);
     w.params = (int32_t*)take(64);
+    w.nbounce = (int32_t*)take(4 * wn); w.freel = (int32_t*)take(4 * wn); w.ctl = (StreamCtl*)take(64);
     w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
     w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
     w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
@@ -1935,6 +2013,7 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     w.spix = (int32_t*)take(4 * sn);
     w.sview = (int32_t*)take(4 * sn);
     if (log) {
+        w.pid = (uint64_t*)take(8 * wn);
         w.lhash = (uint64_t*)take(8 * wn); w.lnh = (int32_t*)take(4 * wn); w.lprims = (int32_t*)take(4 * wn * 8);
     }
     if (hero > 1) {
@@ -1958,21 +2037,78 @@ void wave_free(Wave& w) {
     w.block = nullptr;
 }
 
+// Streaming-pass bookkeeping: the free-slot stack holds every slot (popped in slot order),
+// the queues are empty and nothing has been handed out.
+__global__ void __launch_bounds__(128) k_stream_init(Wave w) {
+    const int32_t slots = w.params[1];
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int i = tid; i < slots; i += gridDim.x * blockDim.x) w.freel[i] = slots - 1 - i;
+    if (tid == 0) {
+        StreamCtl& c = *w.ctl;
+        c.next = 0; c.free_n = slots; c.taken = 0; c.half = 0; c.more = 1;
+        for (int k = 0; k < 16; ++k) w.counts[k] = 0;
+    }
+}
+
+// End of a half-iteration (one thread): the refill's photons and claimed slots are booked,
+// the consumed queue and the connection queue are emptied, and whether work is left --
+// paths queued for the next half-iteration or photons not yet handed out -- goes to the
+// progress word and, inside a graph, to the loop condition.  A pass that reaches its
+// half-iteration cap with work left stops with ST_LOOP_CAP.
+__global__ void k_stream_advance(Wave w, Frame f, int32_t* consumed, const int32_t* next_q,
+                                 cudaGraphConditionalHandle loop, int32_t set_loop) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    StreamCtl& c = *w.ctl;
+    const int64_t total = reinterpret_cast<const int64_t*>(w.params)[1];
+    const int64_t cap = reinterpret_cast<const int64_t*>(w.params)[2];
+    const int64_t left = total - c.next;
+    c.next += left < (int64_t)c.free_n ? left : (int64_t)c.free_n;
+    c.free_n -= c.taken;
+    c.taken = 0;
+    c.half += 1;
+    *consumed = 0;
+    w.counts[2] = 0;
+    int32_t more = (*next_q > 0 || c.next < total) ? 1 : 0;
+    if (more && c.half >= cap) {
+        atomicOr(f.status, ST_LOOP_CAP);
+        more = 0;
+    }
+    c.more = more;
+    if (set_loop) cudaGraphSetConditional(loop, (unsigned)more);
+}
+
 namespace {
-// The launch sequence of one wave: emit, its connections, then per bounce closest hit,
-// shading and the connections it queued.  Every launch reads the wave's job count and
-// slot count from w.params, so the same sequence serves any table (and one captured graph
-// serves every wave of its shape).
-void issue_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int grid, bool sorted,
-                cudaStream_t st, LaunchSink* sink) {
-    const bool inst = kind.instances, hero = kind.bundles, media = kind.media;
-    const int T = 128;
-    const DevJob* jobs = w.jobs;
-    const bool count = f.stats != nullptr;
-    auto mark = [&](int k, bool end) { if (sink) sink->mark(k, end, st); };
-    auto shadow = [&]() {
+// Kernel launches of one wave buffer with the variants its WaveKind selects.
+struct Issue {
+    Wave& w;
+    const WaveKind& kind;
+    const Frame& f;
+    int grid;
+    bool sorted;
+    cudaStream_t st;
+    LaunchSink* sink;
+    static constexpr int T = 128;
+
+    void mark(int k, bool end) { if (sink) sink->mark(k, end, st); }
+    void emit(bool stream, int32_t* qo, int32_t* co) {
+        mark(K_EMIT, false);
+        const DevJob* jobs = w.jobs;
+        if (stream) {
+            if (kind.bundles) k_emit_hero<true><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+            else if (kind.media) k_emit<true, true><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+            else k_emit<false, true><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+        } else {
+            if (kind.bundles) k_emit_hero<false><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+            else if (kind.media) k_emit<true, false><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+            else k_emit<false, false><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+        }
+        mark(K_EMIT, true);
+    }
+    void shadow() {
+        const bool inst = kind.instances, count = f.stats != nullptr;
+        const DevJob* jobs = w.jobs;
         mark(K_SHADOW, false);
-        if (hero) {
+        if (kind.bundles) {
             if (count) {
                 if (inst) k_shadow_hero<true, true><<<grid, T, 0, st>>>(w, jobs, f);
                 else k_shadow_hero<true, false><<<grid, T, 0, st>>>(w, jobs, f);
@@ -1988,56 +2124,92 @@ void issue_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& 
             else k_shadow<false, false><<<grid, T, 0, st>>>(w, jobs, f);
         }
         mark(K_SHADOW, true);
-        cudaMemsetAsync(&w.counts[2], 0, 4, st);
-    };
+    }
+    void extend(int32_t* q, int32_t* c) {
+        const bool inst = kind.instances, count = f.stats != nullptr;
+        const DevJob* jobs = w.jobs;
+        mark(K_EXTEND, false);
+        if (sorted) {
+            const int gs = std::max(1, std::min(grid, (w.W + kSortChunk - 1) / kSortChunk));
+            k_sort_queue<<<gs, T, 0, st>>>(w, q, c);
+        }
+        if (count) {
+            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, q, c, f);
+            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, q, c, f);
+        } else {
+            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, q, c, f);
+            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, q, c, f);
+        }
+        mark(K_EXTEND, true);
+    }
+    void shade(const int32_t* qi, const int32_t* ci, int32_t* qo, int32_t* co, int32_t bounce) {
+        const bool inst = kind.instances;
+        const DevJob* jobs = w.jobs;
+        mark(K_SHADE, false);
+        if (kind.bundles) {
+            if (inst) k_shade_hero<true><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+            else k_shade_hero<false><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+        } else if (kind.media) {
+            if (inst) k_shade<true, true><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+            else k_shade<true, false><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+        } else {
+            if (inst) k_shade<false, true><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+            else k_shade<false, false><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+        }
+        mark(K_SHADE, true);
+    }
+};
+
+// The launch sequence of one wave: emit, its connections, then per bounce closest hit,
+// shading and the connections it queued.  Every launch reads the wave's job count and
+// slot count from w.params, so the same sequence serves any table (and one captured graph
+// serves every wave of its shape).
+void issue_wave(Issue& I, int32_t max_bounce) {
+    Wave& w = I.w;
+    cudaStream_t st = I.st;
     cudaMemsetAsync(w.counts, 0, 64, st);
-    mark(K_EMIT, false);
-    if (hero) k_emit_hero<<<grid, T, 0, st>>>(w, jobs, f);
-    else if (media) k_emit<true><<<grid, T, 0, st>>>(w, jobs, f);
-    else k_emit<false><<<grid, T, 0, st>>>(w, jobs, f);
-    mark(K_EMIT, true);
-    shadow();
+    I.emit(false, w.qa, &w.counts[0]);
+    I.shadow();
+    cudaMemsetAsync(&w.counts[2], 0, 4, st);
     int32_t* qa = w.qa;
     int32_t* qb = w.qb;
     int32_t* ca = &w.counts[0];
     int32_t* cb = &w.counts[1];
     for (int b = 0; b < max_bounce; ++b) {
-        mark(K_EXTEND, false);
-        if (sorted) {
-            const int gs = std::max(1, std::min(grid, (w.W + kSortChunk - 1) / kSortChunk));
-            k_sort_queue<<<gs, T, 0, st>>>(w, qa, ca);
-        }
-        if (count) {
-            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
-            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
-        } else {
-            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
-            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, qa, ca, f);
-        }
-        mark(K_EXTEND, true);
+        I.extend(qa, ca);
         cudaMemsetAsync(cb, 0, 4, st);
-        mark(K_SHADE, false);
-        if (hero) {
-            if (inst) k_shade_hero<true><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
-            else k_shade_hero<false><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
-        } else if (media) {
-            if (inst) k_shade<true, true><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
-            else k_shade<true, false><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
-        } else {
-            if (inst) k_shade<false, true><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
-            else k_shade<false, false><<<grid, T, 0, st>>>(w, jobs, f, qa, ca, qb, cb, b);
-        }
-        mark(K_SHADE, true);
-        shadow();
+        I.shade(qa, ca, qb, cb, b);
+        I.shadow();
+        cudaMemsetAsync(&w.counts[2], 0, 4, st);
         int32_t* tq = qa; qa = qb; qb = tq;
         int32_t* tc = ca; ca = cb; cb = tc;
     }
+}
+
+// A streaming pass: the prologue fills the slots from the free stack (refill into qa) and
+// traces the emission connections; a half-iteration traces the queue `qi` and leaves the
+// next one in `qo` (survivors of shading, then the refill).
+void stream_prologue(Issue& I) {
+    Wave& w = I.w;
+    const int gi = std::max(1, std::min(I.grid, (w.W + Issue::T - 1) / Issue::T));
+    k_stream_init<<<gi, Issue::T, 0, I.st>>>(w);
+    I.emit(true, w.qa, &w.counts[0]);
+    I.shadow();
+    k_stream_advance<<<1, 32, 0, I.st>>>(w, I.f, &w.counts[1], &w.counts[0], 0, 0);
+}
+void stream_half(Issue& I, int32_t* qi, int32_t* ci, int32_t* qo, int32_t* co, cudaGraphConditionalHandle loop,
+                 int32_t set_loop) {
+    I.extend(qi, ci);
+    I.shade(qi, ci, qo, co, -1);
+    I.emit(true, qo, co);
+    I.shadow();
+    k_stream_advance<<<1, 32, 0, I.st>>>(I.w, I.f, ci, co, loop, set_loop);
 }
 }  // namespace
 
 struct WaveGraphs {
     struct Entry {
-        int32_t max_bounce, grid;
+        int32_t max_bounce, grid;   // max_bounce -1: a streaming pass
         bool inst, hero, media, sorted;
         int32_t* status;
         cudaGraphExec_t exec;
@@ -2046,38 +2218,122 @@ struct WaveGraphs {
     ~WaveGraphs() {
         for (auto& e : entries) cudaGraphExecDestroy(e.exec);
     }
+    cudaGraphExec_t find(int32_t max_bounce, int32_t grid, const WaveKind& kind, bool sorted, int32_t* status) const {
+        for (auto& e : entries)
+            if (e.max_bounce == max_bounce && e.grid == grid && e.inst == kind.instances && e.hero == kind.bundles &&
+                e.media == kind.media && e.sorted == sorted && e.status == status)
+                return e.exec;
+        return nullptr;
+    }
 };
 
 WaveGraphs* wave_graphs_create() { return new WaveGraphs(); }
 void wave_graphs_destroy(WaveGraphs* g) { delete g; }
 
-cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int32_t sms,
-                        const LaunchShape& shape, cudaStream_t st, LaunchSink* sink, WaveGraphs* graphs) {
-    if (kind.bundles && w.hero < 2) return cudaErrorInvalidValue;   // the buffer carries no bundles
-    const int T = 128;
+namespace {
+int launch_grid(const Wave& w, int32_t sms, const LaunchShape& shape) {
+    const int T = Issue::T;
     int grid = sms * std::max(1, shape.grid_mult);
     const int gw = (w.W + T - 1) / T;   // enough blocks to give every slot a thread
     if (gw < grid) grid = gw < 1 ? 1 : gw;
+    return grid;
+}
+}  // namespace
+
+cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int32_t sms,
+                        const LaunchShape& shape, cudaStream_t st, LaunchSink* sink, WaveGraphs* graphs) {
+    if (kind.bundles && w.hero < 2) return cudaErrorInvalidValue;   // the buffer carries no bundles
+    const int grid = launch_grid(w, sms, shape);
     // A graph bakes the kernel arguments: the wave's buffers and status word are fixed for the
     // life of its cache, but a log buffer changes per call, so logging waves launch directly.
     if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
-        issue_wave(w, max_bounce, kind, f, grid, shape.sort_rays, st, sink);
+        Issue I{w, kind, f, grid, shape.sort_rays, st, sink};
+        issue_wave(I, max_bounce);
         return cudaGetLastError();
     }
-    for (auto& e : graphs->entries)
-        if (e.max_bounce == max_bounce && e.grid == grid && e.inst == kind.instances && e.hero == kind.bundles &&
-            e.media == kind.media && e.sorted == shape.sort_rays && e.status == f.status)
-            return cudaGraphLaunch(e.exec, st);
+    if (cudaGraphExec_t ex = graphs->find(max_bounce, grid, kind, shape.sort_rays, f.status))
+        return cudaGraphLaunch(ex, st);
     cudaGraph_t g = nullptr;
     cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) return err;
-    issue_wave(w, max_bounce, kind, f, grid, shape.sort_rays, st, nullptr);
+    Issue I{w, kind, f, grid, shape.sort_rays, st, nullptr};
+    issue_wave(I, max_bounce);
     err = cudaStreamEndCapture(st, &g);
     if (err != cudaSuccess) return err;
     WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, shape.sort_rays, f.status,
                         nullptr};
     err = cudaGraphInstantiate(&e.exec, g, 0);
     cudaGraphDestroy(g);
+    if (err != cudaSuccess) return err;
+    graphs->entries.push_back(e);
+    return cudaGraphLaunch(e.exec, st);
+}
+
+cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t sms, const LaunchShape& shape,
+                          cudaStream_t st, LaunchSink* sink, WaveGraphs* graphs) {
+    if (kind.bundles && w.hero < 2) return cudaErrorInvalidValue;
+    const int grid = launch_grid(w, sms, shape);
+    int32_t* ca = &w.counts[0];
+    int32_t* cb = &w.counts[1];
+    if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
+        // host-driven: groups of half-iterations, the progress word read between groups
+        Issue I{w, kind, f, grid, shape.sort_rays, st, sink};
+        stream_prologue(I);
+        for (;;) {
+            for (int r = 0; r < 4; ++r) {
+                stream_half(I, w.qa, ca, w.qb, cb, 0, 0);
+                stream_half(I, w.qb, cb, w.qa, ca, 0, 0);
+            }
+            cudaError_t e = cudaGetLastError();
+            int32_t more = 0;
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&more, &w.ctl->more, sizeof more, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return e;
+            if (!more) return cudaSuccess;
+        }
+    }
+    if (cudaGraphExec_t ex = graphs->find(-1, grid, kind, shape.sort_rays, f.status)) return cudaGraphLaunch(ex, st);
+    // prologue, then a conditional while node whose body is two half-iterations (the queues
+    // swap roles between them); the last advance of the body sets the loop condition
+    Issue I{w, kind, f, grid, shape.sort_rays, st, nullptr};
+    cudaGraph_t g = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) return err;
+    stream_prologue(I);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t n_deps = 0;
+    cudaGraphConditionalHandle loop = 0;
+    cudaGraphNode_t node = nullptr;
+    cudaGraphNodeParams p{};
+    err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &n_deps);
+    if (err == cudaSuccess) err = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+    if (err == cudaSuccess) {
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = loop;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        err = cudaGraphAddNode(&node, g, deps, n_deps, &p);
+    }
+    if (err == cudaSuccess) err = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    cudaGraph_t captured = nullptr;
+    cudaError_t end = cudaStreamEndCapture(st, &captured);
+    if (err == cudaSuccess) err = end;
+    if (err != cudaSuccess) {
+        if (captured) cudaGraphDestroy(captured);
+        return err;
+    }
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    err = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+        stream_half(I, w.qa, ca, w.qb, cb, loop, 0);
+        stream_half(I, w.qb, cb, w.qa, ca, loop, 1);
+        cudaGraph_t b2 = nullptr;
+        err = cudaStreamEndCapture(st, &b2);
+    }
+    WaveGraphs::Entry e{-1, grid, kind.instances, kind.bundles, kind.media, shape.sort_rays, f.status, nullptr};
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&e.exec, captured, 0);
+    cudaGraphDestroy(captured);
     if (err != cudaSuccess) return err;
     graphs->entries.push_back(e);
     return cudaGraphLaunch(e.exec, st);

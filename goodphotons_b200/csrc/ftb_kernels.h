@@ -13,7 +13,8 @@ enum : int32_t {
     ST_STACK_OVERFLOW = 1,    // traversal stack exhausted
     ST_FILM_SATURATED = 2,    // a splat exceeded the fixed-point range
     ST_MEDIUM_STACK = 4,      // nested-dielectric stack deeper than kStkCap
-    ST_QUEUE_OVERFLOW = 8     // shadow queue capacity exceeded
+    ST_QUEUE_OVERFLOW = 8,    // shadow queue capacity exceeded
+    ST_LOOP_CAP = 16          // a streaming pass ran out of iterations with work left
 };
 
 constexpr int kStkCap = 4;
@@ -27,7 +28,9 @@ struct DevView {
 };
 
 // One job's share of a wave: its scene, camera(s) and film(s), and the slots
-// [slot0, slot0+n) of the wave that trace its photons photon0, photon0+1, ...
+// [slot0, slot0+n) of the wave that trace its photons photon0, photon0+1, ...  In a
+// streaming pass the table is a list of photon ranges instead: the pass hands out photons
+// g = 0, 1, ... in order, and g in [g0, g0+n) is this job's photon photon0 + (g - g0).
 struct DevJob {
     DevScene sc;
     DevCam cam;
@@ -38,9 +41,19 @@ struct DevJob {
     double film_scale_inv;     // 2^frac / power_ref
     double tally_scale_inv;    // 2^32 / power_ref
     uint64_t photon0;
+    int64_t g0;                // streaming pass: first stream index of this range
     int32_t slot0, n;
     int32_t max_bounce;
     int32_t hero_c;            // wavelengths per photon (1: the scalar tracer)
+};
+
+// Progress of a streaming pass (device memory, updated by k_stream_advance).
+struct StreamCtl {
+    long long next;            // photons of the pass handed out so far
+    int32_t free_n;            // entries on the free-slot stack (Wave::freel)
+    int32_t taken;             // slots claimed by the current refill
+    int32_t half;              // half-iterations (extend / shade / refill / shadow) run
+    int32_t more;              // work left after the last half-iteration (0 / 1)
 };
 
 // Per-wave path state, queues and shadow-ray records (structure of arrays, W slots).
@@ -61,7 +74,11 @@ struct Wave {
     int32_t* job;              // job of each slot (multi-job waves)
     int32_t* sjob;             // job of each shadow record
     DevJob* jobs;              // device job table, kWaveJobs entries
-    int32_t* params;           // [0] jobs in the table, [1] slots in use (written with the table)
+    int32_t* params;           // [0] jobs in the table, [1] slots in use (written with the table);
+                               // streaming pass: int64 [1] photons of the pass, [2] half-iteration cap
+    int32_t* nbounce;          // bounces done per slot (streaming pass)
+    int32_t* freel;            // free-slot stack (streaming pass)
+    StreamCtl* ctl;
     double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
     double* sxyz;              // [3][S] film increments (X, Y, Z) of one-wavelength connections
     int32_t* spix;
@@ -75,6 +92,7 @@ struct Wave {
     double* xval;              // [hero-1][S] and their contributions
     int32_t* snup;             // [S] wavelengths in each connection
     // parity instrumentation (null unless logging)
+    uint64_t* pid;             // photon index per slot
     uint64_t* lhash;
     int32_t* lnh;
     int32_t* lprims;           // [8][W]
@@ -92,11 +110,15 @@ struct Frame {
     int32_t* status;
 };
 
+// Shadow records per slot: a path queues at most 2 connections per view per bounce, and in
+// a streaming pass a refilled slot's emission adds one more in the same half-iteration.
+constexpr int kShadowPerSlot = 3;
+
 // Bytes of one wave of W slots: every array rounded up to 256 B, in the order wave_carve
 // lays them out.  constexpr so a fixed device array can hold a wave (ftb_noalloc.cu).
 constexpr size_t wave_align(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t wave_bytes(int32_t W, bool log, int32_t hero = 1) {
-    size_t w = (size_t)W, s = 2 * (size_t)W;
+    size_t w = (size_t)W, s = kShadowPerSlot * (size_t)W;
     size_t b = 0;
     b += 2 * wave_align(8 * w);                                     // rng
     b += 8 * wave_align(8 * w) + wave_align(24 * w);                // ray + lam + beta + cie
@@ -105,8 +127,9 @@ constexpr size_t wave_bytes(int32_t W, bool log, int32_t hero = 1) {
     b += 2 * wave_align(4 * w) + wave_align(64);                    // queues + counts
     b += wave_align(4 * w) + wave_align(4 * s) + wave_align(sizeof(DevJob) * kWaveJobs);   // job ids + table
     b += wave_align(64);                                            // table parameters
+    b += 2 * wave_align(4 * w) + wave_align(64);                    // streaming: bounces, free stack, ctl
     b += 9 * wave_align(8 * s) + wave_align(24 * s) + 2 * wave_align(4 * s);   // shadow records
-    if (log) b += wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
+    if (log) b += 2 * wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
     if (hero > 1)                                                   // bundles
         b += 2 * wave_align(8 * w * hero) + wave_align(4 * w) + 2 * wave_align(8 * s * (hero - 1)) +
              wave_align(4 * s);
@@ -134,6 +157,7 @@ struct LaunchShape {
     int32_t grid_mult = 16;
     bool graph = true;
     bool sort_rays = false;   // reorder each block's closest-hit rays by direction first
+    bool regenerate = true;   // streaming passes: freed slots are refilled with new photons
 };
 
 // Instantiated graphs of one wave buffer, by (bounce cap, grid, instance variant, status
@@ -160,5 +184,23 @@ struct WaveKind {
 cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const Frame& f, int32_t sms,
                         const LaunchShape& shape, cudaStream_t stream, LaunchSink* sink = nullptr,
                         WaveGraphs* graphs = nullptr);
+
+// Trace a streaming pass on `stream`: the caller has written the table of photon ranges to
+// w.jobs (g0 consecutive from 0) and w.params = {ranges, slots, photons (int64 at [1]),
+// half-iteration cap (int64 at [2])}.  The pass keeps `slots` paths in flight: every
+// half-iteration runs closest hit, shading (dead paths push their slot on the free stack),
+// a refill that emits the next photons of the pass into the free slots, and the queued
+// connections, until every photon is done.  With `graphs` and shape.graph the loop is one
+// graph launch (a conditional while node whose condition the device sets); otherwise the
+// host issues half-iterations in groups and reads the progress word between groups.
+cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t sms, const LaunchShape& shape,
+                          cudaStream_t stream, LaunchSink* sink = nullptr, WaveGraphs* graphs = nullptr);
+
+// Half-iterations a streaming pass of `photons` over `slots` slots can need: every slot
+// consumes a photon at least once per max_bounce + 1 half-iterations while photons remain.
+inline int64_t stream_half_cap(int64_t photons, int64_t slots, int32_t max_bounce) {
+    const int64_t per = slots > 0 ? (photons + slots - 1) / slots : 0;
+    return (per + 2) * ((int64_t)(max_bounce > 0 ? max_bounce : 0) + 2) + 4;
+}
 
 }  // namespace ftb

@@ -153,10 +153,13 @@ class _Lib:
         self.check(self.L.ftb_get_tuning(device, C.byref(t)))
         return t
 
-    def set_tuning(self, device=0, wave_slots=None, grid_mult=None, use_graphs=None, sort_rays=None):
+    def set_tuning(self, device=0, wave_slots=None, grid_mult=None, use_graphs=None, sort_rays=None,
+                   regenerate=None):
         t = self.get_tuning(device)
         if sort_rays is not None:
             t.sort_rays = int(bool(sort_rays))
+        if regenerate is not None:
+            t.regenerate = int(bool(regenerate))
         if wave_slots is not None:
             t.wave_slots = wave_slots
         if grid_mult is not None:

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FTB_ABI_VERSION 3
+#define FTB_ABI_VERSION 4
 
 typedef enum ftb_status {
     FTB_OK = 0,
@@ -386,7 +386,7 @@ ftb_status ftb_trace_log(ftb_scene* scene, const ftb_camera* cam,
  * start-up (ftb_scene_create allocates); then this call only launches kernels and async
  * memsets on `stream`, accumulating into the caller's DEVICE film like
  * ftb_render_forward_device.  Its scratch (one wave of path state, queues, shadow records,
- * tallies and status: ~12.7 MB) is a fixed device array in the library, held by every GPU
+ * tallies and status: ~16.5 MB) is a fixed device array in the library, held by every GPU
  * that loads the library until exit.  Limit: n_photons <= FTB_NOALLOC_MAX_PHOTONS per call
  * (larger requests return FTB_ERR_TOO_LARGE; render more with consecutive seed_base).  The
  * first call on a device resolves the array's device address (cudaGetSymbolAddress) with
@@ -428,6 +428,10 @@ typedef struct ftb_tuning {
     int32_t grid_mult;    /* 1 .. 64 */
     int32_t use_graphs;   /* 0 / 1 */
     int32_t sort_rays;    /* 0 / 1: reorder closest-hit rays by direction within each block */
+    int32_t regenerate;   /* 0 / 1: streaming passes -- a slot freed by a finished path is
+                             refilled with the next photon at once, so the device stays full
+                             until the last photons (1), or waves traced to their last bounce
+                             one after another (0) */
 } ftb_tuning;
 
 ftb_status ftb_get_tuning(int32_t device, ftb_tuning* out);

@@ -13,7 +13,16 @@ from goodphotons_b200 import lib, scenes
 pytestmark = pytest.mark.gpu
 
 
-def test_batch_results_equal_solo_renders(gpu):
+@pytest.fixture(params=[1, 0], ids=["streaming", "waves"])
+def launch_mode(request, gpu):
+    """Streaming passes (freed slots refilled at once) or waves traced to their last bounce."""
+    saved = gpu.get_tuning(0)
+    gpu.set_tuning(0, regenerate=request.param)
+    yield request.param
+    gpu.L.ftb_set_tuning(0, C.byref(saved))
+
+
+def test_batch_results_equal_solo_renders(gpu, launch_mode):
     torch = pytest.importorskip("torch")
     L = gpu
     sc_c = lib.Scene(scenes.make_cornell(L), 0, L)
@@ -51,26 +60,28 @@ def test_batch_results_equal_solo_renders(gpu):
 
 
 def test_tuning_and_graph_replay_do_not_change_results(gpu):
-    """Wave size, grid size and graph replay change only how waves are launched: films and
-    energy tallies stay bit-identical; the autotuner returns a setting in range."""
+    """Slot refill, wave size, grid size and graph replay change only how paths are launched:
+    films and energy tallies stay bit-identical; the autotuner returns a setting in range."""
     L = gpu
     sc = lib.Scene(scenes.make_glass(L, level=3), 0, L)
     cam = scenes.default_camera(L, 40)
     saved = L.get_tuning(0)
     try:
         ref = None
-        for slots, grid, graphs, srt in [(1 << 22, 16, 0, 0), (1 << 20, 4, 1, 1), (1 << 19, 32, 1, 0),
-                                         (3 << 18, 8, 0, 1), (1 << 22, 16, 1, 1)]:
-            L.set_tuning(0, wave_slots=slots, grid_mult=grid, use_graphs=graphs, sort_rays=srt)
+        for slots, grid, graphs, srt, regen in [(1 << 22, 16, 0, 0, 0), (1 << 20, 4, 1, 1, 0),
+                                                (1 << 19, 32, 1, 0, 1), (3 << 18, 8, 0, 1, 1),
+                                                (1 << 22, 16, 1, 1, 1), (1 << 22, 16, 1, 0, 0),
+                                                (40_000, 16, 1, 0, 1), (1_000, 4, 0, 0, 1)]:
+            L.set_tuning(0, wave_slots=slots, grid_mult=grid, use_graphs=graphs, sort_rays=srt, regenerate=regen)
             for _ in range(2):   # the second render replays a captured graph
                 film, _, en = sc.render(cam, 1_500_000, seed_base=42, max_bounce=16, frac_bits=30)
                 if ref is None:
                     ref = (film, list(en.fx))
-                np.testing.assert_array_equal(film, ref[0], err_msg=f"{slots} {grid} {graphs} {srt}")
+                np.testing.assert_array_equal(film, ref[0], err_msg=f"{slots} {grid} {graphs} {srt} {regen}")
                 assert list(en.fx) == ref[1]
         t = L.autotune(sc, cam, 1 << 21, 16)
         assert 1 <= t.wave_slots <= 1 << 22 and 1 <= t.grid_mult <= 64 and t.use_graphs in (0, 1)
-        assert t.sort_rays in (0, 1)
+        assert t.sort_rays in (0, 1) and t.regenerate in (0, 1)
         film, _, _ = sc.render(cam, 1_500_000, seed_base=42, max_bounce=16, frac_bits=30)
         np.testing.assert_array_equal(film, ref[0])
     finally:

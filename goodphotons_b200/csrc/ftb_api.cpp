@@ -299,7 +299,7 @@ std::weak_ptr<Engine> g_engines[256];
 ftb_tuning g_tuning[256];          // per device; a new engine starts from it
 bool g_tuning_set[256] = {};
 
-ftb_tuning default_tuning() { return ftb_tuning{1 << 22, 16, 1, 0, 0}; }
+ftb_tuning default_tuning() { return ftb_tuning{1 << 22, 16, 1, 0, 1}; }
 
 void apply_tuning(Engine& e, const ftb_tuning& t) {
     e.wave_cap = t.wave_slots;

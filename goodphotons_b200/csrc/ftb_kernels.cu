@@ -1046,17 +1046,17 @@ __device__ __forceinline__ uint64_t fnv_i32(uint64_t h, int32_t v) {
     return h;
 }
 
-// Per-slot instrumentation (parity tests only).
-__device__ __forceinline__ void log_finish(const Wave& w, int slot, int fate, double beta) {
+// Per-path instrumentation (parity tests only).
+__device__ __forceinline__ void log_finish(const Wave& w, const PathState& ps, int i, int fate, double beta) {
     if (!w.logs) return;
-    ftb_photon_log& L = w.logs[w.pid[slot] - (uint64_t)w.log_base];
-    L.n_hits = w.lnh[slot];
+    ftb_photon_log& L = w.logs[ps.pid[i] - (uint64_t)w.log_base];
+    L.n_hits = ps.lnh[i];
     L.fate = fate;
-    L.prim_hash = w.lhash[slot];
+    L.prim_hash = ps.lhash[i];
     L.beta = beta;
-    for (int k = 0; k < 8; ++k) L.prims[k] = w.lprims[k * w.W + slot];
+    for (int k = 0; k < 8; ++k) L.prims[k] = ps.lprims[k * w.W + i];
 }
-// The log of a photon that ends at emission (it never holds a slot).
+// The log of a photon that ends at emission (it never enters a queue).
 __device__ __forceinline__ void log_emitted(const Wave& w, uint64_t photon, int fate, double beta) {
     if (!w.logs) return;
     ftb_photon_log& L = w.logs[photon - (uint64_t)w.log_base];
@@ -1066,42 +1066,63 @@ __device__ __forceinline__ void log_emitted(const Wave& w, uint64_t photon, int 
     L.beta = beta;
     for (int k = 0; k < 8; ++k) L.prims[k] = -2;
 }
-__device__ __forceinline__ void log_start(const Wave& w, int slot, uint64_t photon) {
+__device__ __forceinline__ void log_start(const Wave& w, const PathState& ps, int i, uint64_t photon) {
     if (!w.logs) return;
-    w.pid[slot] = photon;
-    w.lhash[slot] = 1469598103934665603ULL; w.lnh[slot] = 0;
-    for (int q = 0; q < 8; ++q) w.lprims[q * w.W + slot] = -2;
+    ps.pid[i] = photon;
+    ps.lhash[i] = 1469598103934665603ULL; ps.lnh[i] = 0;
+    for (int q = 0; q < 8; ++q) ps.lprims[q * w.W + i] = -2;
+}
+// A hit joins the log of path i (in place), before shading decides its fate.
+template <bool INST>
+__device__ __forceinline__ void log_hit(const Wave& w, const PathState& ps, int i, const DevScene& sc, int rec) {
+    if (!w.logs) return;
+    const int nh = ps.lnh[i];
+    const int prim = rec >= 0 ? sc.recs[rec].prim : -1;
+    uint64_t hsh = fnv_i32(ps.lhash[i], prim);
+    if (INST && rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)   // and the BLAS triangle
+        hsh = fnv_i32(hsh, sc.inst[rec_inst(sc.recs[rec])].recs[w.hit_sub[i]].prim);
+    ps.lhash[i] = hsh;
+    if (nh < 8) ps.lprims[nh * w.W + i] = prim;
+    ps.lnh[i] = nh + 1;
+}
+// A surviving path's log moves with it.
+__device__ __forceinline__ void log_move(const Wave& w, const PathState& in, int i, const PathState& out, int o) {
+    if (!w.logs) return;
+    out.pid[o] = in.pid[i];
+    out.lhash[o] = in.lhash[i];
+    out.lnh[o] = in.lnh[i];
+    for (int q = 0; q < 8; ++q) out.lprims[q * w.W + o] = in.lprims[q * w.W + i];
 }
 
-// Photon sources of the emission kernels.  A wave gives slot s of its table's range the
-// photon photon0 + (s - slot0); a streaming pass hands out stream indices next .. next+F-1
-// (F = free slots, at most the photons left), maps each to its range's photon, and a photon
-// that survives emission takes a slot off the free stack.
+// Photon sources of the emission kernels.  A wave emits photon photon0 + (t - slot0) of the
+// table range holding t, for t < params[1]; a streaming pass's refill emits stream indices
+// next .. next+F-1, F = the free places (slots less the survivors already queued, at most the
+// photons left), each mapped to its range's photon.
 struct PhotonSource {
     int64_t n;           // photons this launch emits
     int64_t next;        // streaming: first stream index
-    int32_t free_n;      // streaming: free-stack height
+    int32_t have;        // streaming: survivors already in the output queue
 };
 template <bool STREAM>
-__device__ __forceinline__ PhotonSource photon_source(const Wave& w) {
+__device__ __forceinline__ PhotonSource photon_source(const Wave& w, const int32_t* out_count) {
     PhotonSource p;
     if (STREAM) {
         const int64_t total = reinterpret_cast<const int64_t*>(w.params)[1];
         p.next = w.ctl->next;
-        p.free_n = w.ctl->free_n;
-        const int64_t left = total - p.next;
-        p.n = left < (int64_t)p.free_n ? left : (int64_t)p.free_n;
+        p.have = *out_count;   // the refill appends through ctl->taken, so this stays put
+        const int64_t room = (int64_t)w.params[1] - p.have, left = total - p.next;
+        p.n = left < room ? left : room;
     } else {
         p.n = w.params[1];
         p.next = 0;
-        p.free_n = 0;
+        p.have = 0;
     }
     return p;
 }
 // Job and photon index of the t-th photon of this launch.
 template <bool STREAM>
-__device__ __forceinline__ int photon_job(const Wave& w, const DevJob* __restrict__ jobs, int n_jobs,
-                                          const PhotonSource& p, int64_t t, uint64_t& photon) {
+__device__ __forceinline__ int photon_job(const DevJob* __restrict__ jobs, int n_jobs, const PhotonSource& p,
+                                          int64_t t, uint64_t& photon) {
     int j = 0;
     if (STREAM) {
         const int64_t g = p.next + t;
@@ -1122,24 +1143,15 @@ __device__ __forceinline__ int photon_job(const Wave& w, const DevJob* __restric
     }
     return j;
 }
-// The slot a surviving photon is traced in, with its job and log set up.
+// Queue position of a photon that survives emission, with its job, bounce count and log set.
 template <bool STREAM>
-__device__ __forceinline__ int photon_slot(const Wave& w, const PhotonSource& p, int64_t t, int j, bool multi,
-                                           uint64_t photon) {
-    int slot;
-    if (STREAM) {
-        slot = w.freel[p.free_n - 1 - agg_inc(&w.ctl->taken)];
-        w.nbounce[slot] = 0;
-    } else {
-        slot = (int)t;
-    }
-    if (multi) w.job[slot] = j;
-    log_start(w, slot, photon);
-    return slot;
-}
-// A path that ends: a streaming pass returns its slot to the free stack.
-__device__ __forceinline__ void retire_slot(const Wave& w, int32_t bounce, int slot) {
-    if (bounce < 0) w.freel[agg_inc(&w.ctl->free_n)] = slot;
+__device__ __forceinline__ int photon_enqueue(const Wave& w, const PathState& out, int32_t* out_count,
+                                              const PhotonSource& p, int j, bool multi, uint64_t photon) {
+    const int o = STREAM ? p.have + agg_inc(&w.ctl->taken) : agg_inc(out_count);
+    out.nbounce[o] = 0;
+    if (multi) out.job[o] = j;
+    log_start(w, out, o, photon);
+    return o;
 }
 
 // ------------------------------------------------------------------ emission -----------
@@ -1180,16 +1192,16 @@ __device__ __forceinline__ double sample_at(const DevEmit& em, double u, double&
 
 // ------------------------------------------------------------------ kernels ------------
 template <bool MEDIA, bool STREAM>
-__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f, int32_t* qout,
-                                              int32_t* qout_count) {
+__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
+                                              int32_t* out_count) {
     const int32_t n_jobs = w.params[0];
     const bool multi = n_jobs > 1;
-    const PhotonSource src = photon_source<STREAM>(w);
+    const PhotonSource src = photon_source<STREAM>(w, out_count);
     TallyAcc acc;
     tally_init(acc);
     for (int64_t t = blockIdx.x * blockDim.x + threadIdx.x; t < src.n; t += gridDim.x * blockDim.x) {
         uint64_t k;
-        const int j = photon_job<STREAM>(w, jobs, n_jobs, src, t, k);
+        const int j = photon_job<STREAM>(jobs, n_jobs, src, t, k);
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
         Pcg rng = seed_photon(k);
@@ -1212,14 +1224,13 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
             log_emitted(w, k, 2, beta);
             continue;
         }
-        const int slot = photon_slot<STREAM>(w, src, t, j, multi, k);
-        w.rng_s[slot] = rng.s; w.rng_i[slot] = rng.inc;
-        w.ox[slot] = ro.x; w.oy[slot] = ro.y; w.oz[slot] = ro.z;
-        w.dx[slot] = dir.x; w.dy[slot] = dir.y; w.dz[slot] = dir.z;
-        w.lam[slot] = lam; w.beta[slot] = beta;
-        w.cie[slot] = cie[0]; w.cie[w.W + slot] = cie[1]; w.cie[2 * (size_t)w.W + slot] = cie[2];
-        w.stk_n[slot] = 0;
-        qout[agg_inc(qout_count)] = slot;
+        const int o = photon_enqueue<STREAM>(w, out, out_count, src, j, multi, k);
+        out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
+        out.ox[o] = ro.x; out.oy[o] = ro.y; out.oz[o] = ro.z;
+        out.dx[o] = dir.x; out.dy[o] = dir.y; out.dz[o] = dir.z;
+        out.lam[o] = lam; out.beta[o] = beta;
+        out.cie[o] = cie[0]; out.cie[w.W + o] = cie[1]; out.cie[2 * (size_t)w.W + o] = cie[2];
+        out.stk_n[o] = 0;
     }
     tally_finish(acc, jobs, multi);
 }
@@ -1252,21 +1263,22 @@ __device__ void block_add1(unsigned long long* dst, unsigned long long a) {
 
 template <bool COUNT, bool INST>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const DevJob* __restrict__ jobs,
-                                                              const int32_t* q, const int32_t* qcount, Frame f) {
+                                                              PathState in, const int32_t* qcount,
+                                                              const int32_t* __restrict__ order, Frame f) {
     const int32_t n_jobs = w.params[0];
     int nq = *qcount;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
-        int slot = q[i];
-        const DevScene& sc = jobs[n_jobs > 1 ? w.job[slot] : 0].sc;
-        RayCtx R = make_ray(mk(w.ox[slot], w.oy[slot], w.oz[slot]), mk(w.dx[slot], w.dy[slot], w.dz[slot]));
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const int i = order ? order[q] : q;
+        const DevScene& sc = jobs[n_jobs > 1 ? in.job[i] : 0].sc;
+        RayCtx R = make_ray(mk(in.ox[i], in.oy[i], in.oz[i]), mk(in.dx[i], in.dy[i], in.dz[i]));
         double t;
         int sub = -1;
         int rec = traverse_closest<COUNT, INST>(sc, R, EPS_RAY, t, &sub, f.status, cnt);
-        w.hit_t[slot] = t;
-        w.hit_rec[slot] = rec;
-        if (INST) w.hit_sub[slot] = sub;
+        w.hit_t[i] = t;
+        w.hit_rec[i] = rec;
+        if (INST) w.hit_sub[i] = sub;
         if (COUNT) rays++;
     }
     if (COUNT) {
@@ -1296,23 +1308,24 @@ __device__ __forceinline__ uint32_t direction_key(D3 d) {
     return u | (v << 1);
 }
 
-// Reorders each kSortChunk-entry piece of a queue by direction key, in place (one block per
-// piece, counting sort in shared memory).  The closest-hit kernel then reads the queue as
-// usual: a warp's 32 lanes take 32 consecutive entries.
-__global__ void __launch_bounds__(128) k_sort_queue(Wave w, int32_t* q, const int32_t* qcount) {
+// Traversal order of a queue, each kSortChunk-entry piece bucketed by direction key (one
+// block per piece, counting sort in shared memory): order[q] is the path the closest-hit
+// kernel's q-th lane takes, so a warp's 32 lanes head the same way.
+__global__ void __launch_bounds__(128) k_sort_queue(Wave w, PathState in, const int32_t* qcount,
+                                                    int32_t* order) {
     __shared__ int32_t hist[256];
     const int nq = *qcount;
     constexpr int kPer = kSortChunk / 128;
     for (int base = blockIdx.x * kSortChunk; base < nq; base += gridDim.x * kSortChunk) {
         for (int t = threadIdx.x; t < 256; t += 128) hist[t] = 0;
         __syncthreads();
-        int slot[kPer], key[kPer], off[kPer];
+        int pos[kPer], key[kPer], off[kPer];
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
             const int i = base + r * 128 + threadIdx.x;
-            slot[r] = i < nq ? q[i] : -1;
-            key[r] = slot[r] >= 0 ? (int)direction_key(mk(w.dx[slot[r]], w.dy[slot[r]], w.dz[slot[r]])) : 255;
-            off[r] = slot[r] >= 0 ? atomicAdd(&hist[key[r]], 1) : 0;
+            pos[r] = i < nq ? i : -1;
+            key[r] = pos[r] >= 0 ? (int)direction_key(mk(in.dx[i], in.dy[i], in.dz[i])) : 255;
+            off[r] = pos[r] >= 0 ? atomicAdd(&hist[key[r]], 1) : 0;
         }
         __syncthreads();
         if (threadIdx.x < 32) {   // exclusive scan of the 256 bucket counts by one warp
@@ -1332,12 +1345,11 @@ __global__ void __launch_bounds__(128) k_sort_queue(Wave w, int32_t* q, const in
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < kPer; ++r)
-            if (slot[r] >= 0) q[base + hist[key[r]] + off[r]] = slot[r];
+            if (pos[r] >= 0) order[base + hist[key[r]] + off[r]] = pos[r];
         __syncthreads();   // before the next piece reuses the histogram
     }
 }
 
-// medium stack (medium_stack.h:17-47), kStkCap entries per slot
 struct Stk { int n; int2 e[kStkCap]; };
 __device__ __forceinline__ int stk_top_pri(const Stk& s) {
     int bp = INT_MIN;
@@ -1401,39 +1413,31 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
 template <bool MEDIA, bool INST>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
-                                                               Frame f, const int32_t* qin,
-                                                               const int32_t* qin_count, int32_t* qout,
-                                                               int32_t* qout_count, int32_t bounce) {
+                                                               Frame f, PathState in, const int32_t* in_count,
+                                                               PathState out, int32_t* out_count) {
     const bool multi = w.params[0] > 1;
     TallyAcc acc;
     tally_init(acc);
-    int nq = *qin_count;
+    int nq = *in_count;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
-        int slot = qin[i];
-        const int j = multi ? w.job[slot] : 0;
+        const int j = multi ? in.job[i] : 0;
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
-        Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
-        D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
-        double lam = w.lam[slot], beta = w.beta[slot];
-        double cie[3];   // read only by the paths that connect
+        Pcg rng; rng.s = in.rng_s[i]; rng.inc = in.rng_i[i];
+        D3 ro = mk(in.ox[i], in.oy[i], in.oz[i]), rd = mk(in.dx[i], in.dy[i], in.dz[i]);
+        double lam = in.lam[i], beta = in.beta[i];
+        double cie[3];   // read by the paths that connect or survive
+        bool have_cie = false;
         auto load_cie = [&]() {
-            cie[0] = w.cie[slot]; cie[1] = w.cie[w.W + slot]; cie[2] = w.cie[2 * (size_t)w.W + slot];
+            if (have_cie) return;
+            cie[0] = in.cie[i]; cie[1] = in.cie[w.W + i]; cie[2] = in.cie[2 * (size_t)w.W + i];
+            have_cie = true;
         };
-        double ht = w.hit_t[slot];
-        int rec = w.hit_rec[slot];
-        Stk stk; stk.n = w.stk_n[slot];
-        for (int k = 0; k < stk.n; ++k) stk.e[k] = w.stk[k * w.W + slot];
-        if (w.logs) {
-            int nh = w.lnh[slot];
-            int prim = rec >= 0 ? sc.recs[rec].prim : -1;
-            uint64_t hsh = fnv_i32(w.lhash[slot], prim);
-            if (INST && rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)   // and the BLAS triangle
-                hsh = fnv_i32(hsh, sc.inst[rec_inst(sc.recs[rec])].recs[w.hit_sub[slot]].prim);
-            w.lhash[slot] = hsh;
-            if (nh < 8) w.lprims[nh * w.W + slot] = prim;
-            w.lnh[slot] = nh + 1;
-        }
+        double ht = w.hit_t[i];
+        int rec = w.hit_rec[i];
+        Stk stk; stk.n = in.stk_n[i];
+        for (int k = 0; k < stk.n; ++k) stk.e[k] = in.stk[k * w.W + i];
+        log_hit<INST>(w, in, i, sc, rec);
         int fate = -1;   // -1 continue, 0 absorbed, 1 escaped
         bool valid = rec >= 0;
         double d_surf = valid ? ht : 1e30;
@@ -1466,7 +1470,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
             load_rec(sc.recs, rec, r);
             Hit h;
             if (INST && rec_type(r) == REC_INST) {
-                instance_hit(sc.inst[rec_inst(r)], w.hit_sub[slot], ro, rd, h);
+                instance_hit(sc.inst[rec_inst(r)], w.hit_sub[i], ro, rd, h);
                 h.prim = r.prim;
             } else {
                 RayCtx R = make_ray(ro, rd);
@@ -1556,34 +1560,34 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
             }
             }
         }
-        const int32_t b = bounce >= 0 ? bounce : w.nbounce[slot];
         if (fate == 0) {
             tally_add(acc, jobs, multi, j, T_ABS, to_fixed(beta, J.tally_scale_inv, f.status));
-            log_finish(w, slot, 0, beta);
-            retire_slot(w, bounce, slot);
+            log_finish(w, in, i, 0, beta);
             continue;
         }
         if (fate == 1) {
             tally_add(acc, jobs, multi, j, T_ESC, to_fixed(beta, J.tally_scale_inv, f.status));
-            log_finish(w, slot, 1, beta);
-            retire_slot(w, bounce, slot);
+            log_finish(w, in, i, 1, beta);
             continue;
         }
+        const int32_t b = in.nbounce[i];
         if (b + 1 >= J.max_bounce) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
-            log_finish(w, slot, 2, beta);
-            retire_slot(w, bounce, slot);
+            log_finish(w, in, i, 2, beta);
             continue;
         }
-        if (bounce < 0) w.nbounce[slot] = b + 1;
-        w.rng_s[slot] = rng.s;
-        w.ox[slot] = no.x; w.oy[slot] = no.y; w.oz[slot] = no.z;
-        w.dx[slot] = nd.x; w.dy[slot] = nd.y; w.dz[slot] = nd.z;
-        w.beta[slot] = beta;
-        w.stk_n[slot] = stk.n;
-        for (int k = 0; k < stk.n; ++k) w.stk[k * w.W + slot] = stk.e[k];
-        int qi = agg_inc(qout_count);
-        qout[qi] = slot;
+        load_cie();
+        const int o = agg_inc(out_count);
+        out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
+        out.ox[o] = no.x; out.oy[o] = no.y; out.oz[o] = no.z;
+        out.dx[o] = nd.x; out.dy[o] = nd.y; out.dz[o] = nd.z;
+        out.lam[o] = lam; out.beta[o] = beta;
+        out.cie[o] = cie[0]; out.cie[w.W + o] = cie[1]; out.cie[2 * (size_t)w.W + o] = cie[2];
+        out.stk_n[o] = stk.n;
+        for (int k = 0; k < stk.n; ++k) out.stk[k * w.W + o] = stk.e[k];
+        out.nbounce[o] = b + 1;
+        if (multi) out.job[o] = j;
+        log_move(w, in, i, out, o);
     }
     tally_finish(acc, jobs, multi);
 }
@@ -1682,16 +1686,16 @@ __device__ __forceinline__ double max_of(const double* a, int n) {   // hero::ma
 }
 
 template <bool STREAM>
-__global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f, int32_t* qout,
-                                                   int32_t* qout_count) {
+__global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
+                                                   int32_t* out_count) {
     const int32_t n_jobs = w.params[0];
     const bool multi = n_jobs > 1;
-    const PhotonSource src = photon_source<STREAM>(w);
+    const PhotonSource src = photon_source<STREAM>(w, out_count);
     TallyAcc acc;
     tally_init(acc);
     for (int64_t t = blockIdx.x * blockDim.x + threadIdx.x; t < src.n; t += gridDim.x * blockDim.x) {
         uint64_t k;
-        const int j = photon_job<STREAM>(w, jobs, n_jobs, src, t, k);
+        const int j = photon_job<STREAM>(jobs, n_jobs, src, t, k);
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
         const int C = J.hero_c;
@@ -1722,58 +1726,46 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
             log_emitted(w, k, 2, beta[0]);
             continue;
         }
-        const int slot = photon_slot<STREAM>(w, src, t, j, multi, k);
-        w.rng_s[slot] = rng.s; w.rng_i[slot] = rng.inc;
-        w.ox[slot] = ro.x; w.oy[slot] = ro.y; w.oz[slot] = ro.z;
-        w.dx[slot] = dir.x; w.dy[slot] = dir.y; w.dz[slot] = dir.z;
+        const int o = photon_enqueue<STREAM>(w, out, out_count, src, j, multi, k);
+        out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
+        out.ox[o] = ro.x; out.oy[o] = ro.y; out.oz[o] = ro.z;
+        out.dx[o] = dir.x; out.dy[o] = dir.y; out.dz[o] = dir.z;
         for (int i = 0; i < C; ++i) {
-            w.hlam[(size_t)i * w.W + slot] = lam[i];
-            w.hbeta[(size_t)i * w.W + slot] = beta[i];
+            out.hlam[(size_t)i * w.W + o] = lam[i];
+            out.hbeta[(size_t)i * w.W + o] = beta[i];
         }
-        w.hlive[slot] = C;
-        w.stk_n[slot] = 0;
-        qout[agg_inc(qout_count)] = slot;
+        out.hlive[o] = C;
+        out.stk_n[o] = 0;
     }
     tally_finish(acc, jobs, multi);
 }
 
 template <bool INST>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, const DevJob* __restrict__ jobs,
-                                                                    Frame f, const int32_t* qin,
-                                                                    const int32_t* qin_count, int32_t* qout,
-                                                                    int32_t* qout_count, int32_t bounce) {
+                                                                    Frame f, PathState in, const int32_t* in_count,
+                                                                    PathState out, int32_t* out_count) {
     const bool multi = w.params[0] > 1;
     TallyAcc acc;
     tally_init(acc);
-    int nq = *qin_count;
-    for (int qi0 = blockIdx.x * blockDim.x + threadIdx.x; qi0 < nq; qi0 += gridDim.x * blockDim.x) {
-        int slot = qin[qi0];
-        const int j = multi ? w.job[slot] : 0;
+    int nq = *in_count;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
+        const int j = multi ? in.job[p] : 0;
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
         const int C = J.hero_c;
-        Pcg rng; rng.s = w.rng_s[slot]; rng.inc = w.rng_i[slot];
-        D3 ro = mk(w.ox[slot], w.oy[slot], w.oz[slot]), rd = mk(w.dx[slot], w.dy[slot], w.dz[slot]);
-        int nup = w.hlive[slot];
+        Pcg rng; rng.s = in.rng_s[p]; rng.inc = in.rng_i[p];
+        D3 ro = mk(in.ox[p], in.oy[p], in.oz[p]), rd = mk(in.dx[p], in.dy[p], in.dz[p]);
+        int nup = in.hlive[p];
         double lam[kHeroMax], beta[kHeroMax];
-        for (int i = 0; i < nup; ++i) {
-            lam[i] = w.hlam[(size_t)i * w.W + slot];
-            beta[i] = w.hbeta[(size_t)i * w.W + slot];
+        for (int k = 0; k < nup; ++k) {
+            lam[k] = in.hlam[(size_t)k * w.W + p];
+            beta[k] = in.hbeta[(size_t)k * w.W + p];
         }
-        double ht = w.hit_t[slot];
-        int rec = w.hit_rec[slot];
-        Stk stk; stk.n = w.stk_n[slot];
-        for (int k = 0; k < stk.n; ++k) stk.e[k] = w.stk[k * w.W + slot];
-        if (w.logs) {
-            int nh = w.lnh[slot];
-            int prim = rec >= 0 ? sc.recs[rec].prim : -1;
-            uint64_t hsh = fnv_i32(w.lhash[slot], prim);
-            if (INST && rec >= 0 && rec_type(sc.recs[rec]) == REC_INST)
-                hsh = fnv_i32(hsh, sc.inst[rec_inst(sc.recs[rec])].recs[w.hit_sub[slot]].prim);
-            w.lhash[slot] = hsh;
-            if (nh < 8) w.lprims[nh * w.W + slot] = prim;
-            w.lnh[slot] = nh + 1;
-        }
+        double ht = w.hit_t[p];
+        int rec = w.hit_rec[p];
+        Stk stk; stk.n = in.stk_n[p];
+        for (int k = 0; k < stk.n; ++k) stk.e[k] = in.stk[k * w.W + p];
+        log_hit<INST>(w, in, p, sc, rec);
         const bool valid = rec >= 0;
         const double d_event = valid ? ht : 1e30;
         {   // Beer-Lambert per live wavelength (render.h:2389-2398)
@@ -1794,7 +1786,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
             load_rec(sc.recs, rec, r);
             Hit h;
             if (INST && rec_type(r) == REC_INST) {
-                instance_hit(sc.inst[rec_inst(r)], w.hit_sub[slot], ro, rd, h);
+                instance_hit(sc.inst[rec_inst(r)], w.hit_sub[p], ro, rd, h);
                 h.prim = r.prim;
             } else {
                 RayCtx R = make_ray(ro, rd);
@@ -1914,30 +1906,32 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
             }
         }
         if (absorbed) tally_add(acc, jobs, multi, j, T_ABS, absorbed);
-        const int32_t b = bounce >= 0 ? bounce : w.nbounce[slot];
         if (fate >= 0) {
             tally_add(acc, jobs, multi, j, fate == 0 ? T_ABS : T_ESC,
                       to_fixed(sum_of(beta, nup), J.tally_scale_inv, f.status));
-            log_finish(w, slot, fate, beta[0]);
-            retire_slot(w, bounce, slot);
+            log_finish(w, in, p, fate, beta[0]);
             continue;
         }
+        const int32_t b = in.nbounce[p];
         if (b + 1 >= J.max_bounce) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(sum_of(beta, nup), J.tally_scale_inv, f.status));
-            log_finish(w, slot, 2, beta[0]);
-            retire_slot(w, bounce, slot);
+            log_finish(w, in, p, 2, beta[0]);
             continue;
         }
-        if (bounce < 0) w.nbounce[slot] = b + 1;
-        w.rng_s[slot] = rng.s;
-        w.ox[slot] = no.x; w.oy[slot] = no.y; w.oz[slot] = no.z;
-        w.dx[slot] = nd.x; w.dy[slot] = nd.y; w.dz[slot] = nd.z;
-        for (int i = 0; i < nup; ++i) w.hbeta[(size_t)i * w.W + slot] = beta[i];
-        w.hlive[slot] = nup;
-        w.stk_n[slot] = stk.n;
-        for (int k = 0; k < stk.n; ++k) w.stk[k * w.W + slot] = stk.e[k];
-        int qo = agg_inc(qout_count);
-        qout[qo] = slot;
+        const int o = agg_inc(out_count);
+        out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
+        out.ox[o] = no.x; out.oy[o] = no.y; out.oz[o] = no.z;
+        out.dx[o] = nd.x; out.dy[o] = nd.y; out.dz[o] = nd.z;
+        for (int k = 0; k < nup; ++k) {
+            out.hlam[(size_t)k * w.W + o] = lam[k];
+            out.hbeta[(size_t)k * w.W + o] = beta[k];
+        }
+        out.hlive[o] = nup;
+        out.stk_n[o] = stk.n;
+        for (int k = 0; k < stk.n; ++k) out.stk[k * w.W + o] = stk.e[k];
+        out.nbounce[o] = b + 1;
+        if (multi) out.job[o] = j;
+        log_move(w, in, p, out, o);
     }
     tally_finish(acc, jobs, multi);
 }
@@ -1994,31 +1988,37 @@ void wave_carve(Wave& w, void* block, int32_t W, bool log, int32_t hero) {
     char* p = (char*)block;
     auto take = [&](size_t n) { void* r = p; p += wave_align(n); return r; };
     size_t wn = (size_t)W, sn = (size_t)w.S;
-    w.rng_s = (uint64_t*)take(8 * wn); w.rng_i = (uint64_t*)take(8 * wn);
-    w.ox = (double*)take(8 * wn); w.oy = (double*)take(8 * wn); w.oz = (double*)take(8 * wn);
-    w.dx = (double*)take(8 * wn); w.dy = (double*)take(8 * wn); w.dz = (double*)take(8 * wn);
-    w.lam = (double*)take(8 * wn); w.beta = (double*)take(8 * wn); w.cie = (double*)take(24 * wn);
-    w.stk_n = (int32_t*)take(4 * wn); w.stk = (int2*)take(8 * wn * kStkCap);
+    for (PathState& ps : w.ps) {   // path_state_bytes order
+        ps.rng_s = (uint64_t*)take(8 * wn); ps.rng_i = (uint64_t*)take(8 * wn);
+        ps.ox = (double*)take(8 * wn); ps.oy = (double*)take(8 * wn); ps.oz = (double*)take(8 * wn);
+        ps.dx = (double*)take(8 * wn); ps.dy = (double*)take(8 * wn); ps.dz = (double*)take(8 * wn);
+        ps.lam = (double*)take(8 * wn); ps.beta = (double*)take(8 * wn); ps.cie = (double*)take(24 * wn);
+        ps.stk_n = (int32_t*)take(4 * wn); ps.stk = (int2*)take(8 * wn * kStkCap);
+        ps.nbounce = (int32_t*)take(4 * wn); ps.job = (int32_t*)take(4 * wn);
+        if (hero > 1) {
+            const size_t h = (size_t)hero;
+            ps.hlam = (double*)take(8 * wn * h); ps.hbeta = (double*)take(8 * wn * h); ps.hlive = (int32_t*)take(4 * wn);
+        }
+        if (log) {
+            ps.pid = (uint64_t*)take(8 * wn); ps.lhash = (uint64_t*)take(8 * wn);
+            ps.lnh = (int32_t*)take(4 * wn); ps.lprims = (int32_t*)take(4 * wn * 8);
+        }
+    }
     w.hit_t = (double*)take(8 * wn); w.hit_rec = (int32_t*)take(4 * wn); w.hit_sub = (int32_t*)take(4 * wn);
-    w.qa = (int32_t*)take(4 * wn); w.qb = (int32_t*)take(4 * wn);
+    w.perm = (int32_t*)take(4 * wn);
     w.counts = (int32_t*)take(64);
-    w.job = (int32_t*)take(4 * wn); w.sjob = (int32_t*)take(4 * sn);
+    w.sjob = (int32_t*)take(4 * sn);
     w.jobs = (DevJob*)take(sizeof(DevJob) * kWaveJobs);
     w.params = (int32_t*)take(64);
-    w.nbounce = (int32_t*)take(4 * wn); w.freel = (int32_t*)take(4 * wn); w.ctl = (StreamCtl*)take(64);
+    w.ctl = (StreamCtl*)take(64);
     w.sox = (double*)take(8 * sn); w.soy = (double*)take(8 * sn); w.soz = (double*)take(8 * sn);
     w.sdx = (double*)take(8 * sn); w.sdy = (double*)take(8 * sn); w.sdz = (double*)take(8 * sn);
     w.smax = (double*)take(8 * sn); w.sval = (double*)take(8 * sn); w.slam = (double*)take(8 * sn);
     w.sxyz = (double*)take(24 * sn);
     w.spix = (int32_t*)take(4 * sn);
     w.sview = (int32_t*)take(4 * sn);
-    if (log) {
-        w.pid = (uint64_t*)take(8 * wn);
-        w.lhash = (uint64_t*)take(8 * wn); w.lnh = (int32_t*)take(4 * wn); w.lprims = (int32_t*)take(4 * wn * 8);
-    }
     if (hero > 1) {
         const size_t h = (size_t)hero;
-        w.hlam = (double*)take(8 * wn * h); w.hbeta = (double*)take(8 * wn * h); w.hlive = (int32_t*)take(4 * wn);
         w.xlam = (double*)take(8 * sn * (h - 1)); w.xval = (double*)take(8 * sn * (h - 1));
         w.snup = (int32_t*)take(4 * sn);
     }
@@ -2037,33 +2037,29 @@ void wave_free(Wave& w) {
     w.block = nullptr;
 }
 
-// Streaming-pass bookkeeping: the free-slot stack holds every slot (popped in slot order),
-// the queues are empty and nothing has been handed out.
-__global__ void __launch_bounds__(128) k_stream_init(Wave w) {
-    const int32_t slots = w.params[1];
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int i = tid; i < slots; i += gridDim.x * blockDim.x) w.freel[i] = slots - 1 - i;
-    if (tid == 0) {
-        StreamCtl& c = *w.ctl;
-        c.next = 0; c.free_n = slots; c.taken = 0; c.half = 0; c.more = 1;
-        for (int k = 0; k < 16; ++k) w.counts[k] = 0;
-    }
+// Streaming-pass bookkeeping: both queues and the connection queue empty, nothing handed out.
+__global__ void k_stream_init(Wave w) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    StreamCtl& c = *w.ctl;
+    c.next = 0; c.taken = 0; c.half = 0; c.more = 1;
+    for (int k = 0; k < 16; ++k) w.counts[k] = 0;
 }
 
-// End of a half-iteration (one thread): the refill's photons and claimed slots are booked,
-// the consumed queue and the connection queue are emptied, and whether work is left --
-// paths queued for the next half-iteration or photons not yet handed out -- goes to the
-// progress word and, inside a graph, to the loop condition.  A pass that reaches its
+// End of a half-iteration (one thread): the refill's photons are booked and its paths join
+// the queue for the next half-iteration, the consumed queue and the connection queue are
+// emptied, and whether work is left -- paths queued or photons not yet handed out -- goes to
+// the progress word and, inside a graph, to the loop condition.  A pass that reaches its
 // half-iteration cap with work left stops with ST_LOOP_CAP.
-__global__ void k_stream_advance(Wave w, Frame f, int32_t* consumed, const int32_t* next_q,
+__global__ void k_stream_advance(Wave w, Frame f, int32_t* consumed, int32_t* next_q,
                                  cudaGraphConditionalHandle loop, int32_t set_loop) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     StreamCtl& c = *w.ctl;
     const int64_t total = reinterpret_cast<const int64_t*>(w.params)[1];
     const int64_t cap = reinterpret_cast<const int64_t*>(w.params)[2];
-    const int64_t left = total - c.next;
-    c.next += left < (int64_t)c.free_n ? left : (int64_t)c.free_n;
-    c.free_n -= c.taken;
+    const int32_t have = *next_q;   // survivors; the refill filled the room above them
+    const int64_t room = (int64_t)w.params[1] - have, left = total - c.next;
+    c.next += left < room ? left : room;
+    *next_q = have + c.taken;
     c.taken = 0;
     c.half += 1;
     *consumed = 0;
@@ -2090,17 +2086,17 @@ struct Issue {
     static constexpr int T = 128;
 
     void mark(int k, bool end) { if (sink) sink->mark(k, end, st); }
-    void emit(bool stream, int32_t* qo, int32_t* co) {
+    void emit(bool stream, const PathState& out, int32_t* co) {
         mark(K_EMIT, false);
         const DevJob* jobs = w.jobs;
         if (stream) {
-            if (kind.bundles) k_emit_hero<true><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
-            else if (kind.media) k_emit<true, true><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
-            else k_emit<false, true><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+            if (kind.bundles) k_emit_hero<true><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            else if (kind.media) k_emit<true, true><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            else k_emit<false, true><<<grid, T, 0, st>>>(w, jobs, f, out, co);
         } else {
-            if (kind.bundles) k_emit_hero<false><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
-            else if (kind.media) k_emit<true, false><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
-            else k_emit<false, false><<<grid, T, 0, st>>>(w, jobs, f, qo, co);
+            if (kind.bundles) k_emit_hero<false><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            else if (kind.media) k_emit<true, false><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            else k_emit<false, false><<<grid, T, 0, st>>>(w, jobs, f, out, co);
         }
         mark(K_EMIT, true);
     }
@@ -2125,85 +2121,81 @@ struct Issue {
         }
         mark(K_SHADOW, true);
     }
-    void extend(int32_t* q, int32_t* c) {
+    void extend(const PathState& in, int32_t* c) {
         const bool inst = kind.instances, count = f.stats != nullptr;
         const DevJob* jobs = w.jobs;
         mark(K_EXTEND, false);
+        const int32_t* order = nullptr;
         if (sorted) {
             const int gs = std::max(1, std::min(grid, (w.W + kSortChunk - 1) / kSortChunk));
-            k_sort_queue<<<gs, T, 0, st>>>(w, q, c);
+            k_sort_queue<<<gs, T, 0, st>>>(w, in, c, w.perm);
+            order = w.perm;
         }
         if (count) {
-            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, q, c, f);
-            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, q, c, f);
+            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
+            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
         } else {
-            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, q, c, f);
-            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, q, c, f);
+            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
+            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
         }
         mark(K_EXTEND, true);
     }
-    void shade(const int32_t* qi, const int32_t* ci, int32_t* qo, int32_t* co, int32_t bounce) {
+    void shade(const PathState& in, const int32_t* ci, const PathState& out, int32_t* co) {
         const bool inst = kind.instances;
         const DevJob* jobs = w.jobs;
         mark(K_SHADE, false);
         if (kind.bundles) {
-            if (inst) k_shade_hero<true><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
-            else k_shade_hero<false><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+            if (inst) k_shade_hero<true><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
+            else k_shade_hero<false><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
         } else if (kind.media) {
-            if (inst) k_shade<true, true><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
-            else k_shade<true, false><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+            if (inst) k_shade<true, true><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
+            else k_shade<true, false><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
         } else {
-            if (inst) k_shade<false, true><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
-            else k_shade<false, false><<<grid, T, 0, st>>>(w, jobs, f, qi, ci, qo, co, bounce);
+            if (inst) k_shade<false, true><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
+            else k_shade<false, false><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
         }
         mark(K_SHADE, true);
     }
 };
 
 // The launch sequence of one wave: emit, its connections, then per bounce closest hit,
-// shading and the connections it queued.  Every launch reads the wave's job count and
-// slot count from w.params, so the same sequence serves any table (and one captured graph
-// serves every wave of its shape).
+// shading (survivors compacted into the other path buffer) and the connections it queued.
+// Every launch reads the wave's job count and slot count from w.params, so the same
+// sequence serves any table (and one captured graph serves every wave of its shape).
 void issue_wave(Issue& I, int32_t max_bounce) {
     Wave& w = I.w;
     cudaStream_t st = I.st;
     cudaMemsetAsync(w.counts, 0, 64, st);
-    I.emit(false, w.qa, &w.counts[0]);
+    I.emit(false, w.ps[0], &w.counts[0]);
     I.shadow();
     cudaMemsetAsync(&w.counts[2], 0, 4, st);
-    int32_t* qa = w.qa;
-    int32_t* qb = w.qb;
-    int32_t* ca = &w.counts[0];
-    int32_t* cb = &w.counts[1];
     for (int b = 0; b < max_bounce; ++b) {
-        I.extend(qa, ca);
-        cudaMemsetAsync(cb, 0, 4, st);
-        I.shade(qa, ca, qb, cb, b);
+        const int a = b & 1;
+        I.extend(w.ps[a], &w.counts[a]);
+        cudaMemsetAsync(&w.counts[a ^ 1], 0, 4, st);
+        I.shade(w.ps[a], &w.counts[a], w.ps[a ^ 1], &w.counts[a ^ 1]);
         I.shadow();
         cudaMemsetAsync(&w.counts[2], 0, 4, st);
-        int32_t* tq = qa; qa = qb; qb = tq;
-        int32_t* tc = ca; ca = cb; cb = tc;
     }
 }
 
-// A streaming pass: the prologue fills the slots from the free stack (refill into qa) and
-// traces the emission connections; a half-iteration traces the queue `qi` and leaves the
-// next one in `qo` (survivors of shading, then the refill).
+// A streaming pass: the prologue fills the first queue (ps[0]) and traces its emission
+// connections; a half-iteration traces queue `a` and leaves the next one in queue a ^ 1
+// (the survivors of shading, then the refill).
 void stream_prologue(Issue& I) {
     Wave& w = I.w;
-    const int gi = std::max(1, std::min(I.grid, (w.W + Issue::T - 1) / Issue::T));
-    k_stream_init<<<gi, Issue::T, 0, I.st>>>(w);
-    I.emit(true, w.qa, &w.counts[0]);
+    k_stream_init<<<1, 32, 0, I.st>>>(w);
+    I.emit(true, w.ps[0], &w.counts[0]);
     I.shadow();
     k_stream_advance<<<1, 32, 0, I.st>>>(w, I.f, &w.counts[1], &w.counts[0], 0, 0);
 }
-void stream_half(Issue& I, int32_t* qi, int32_t* ci, int32_t* qo, int32_t* co, cudaGraphConditionalHandle loop,
-                 int32_t set_loop) {
-    I.extend(qi, ci);
-    I.shade(qi, ci, qo, co, -1);
-    I.emit(true, qo, co);
+void stream_half(Issue& I, int a, cudaGraphConditionalHandle loop, int32_t set_loop) {
+    Wave& w = I.w;
+    I.extend(w.ps[a], &w.counts[a]);
+    I.shade(w.ps[a], &w.counts[a], w.ps[a ^ 1], &w.counts[a ^ 1]);
+    I.emit(true, w.ps[a ^ 1], &w.counts[a ^ 1]);
     I.shadow();
-    k_stream_advance<<<1, 32, 0, I.st>>>(I.w, I.f, ci, co, loop, set_loop);
+    k_stream_advance<<<1, 32, 0, I.st>>>(w, I.f, &w.counts[a], &w.counts[a ^ 1], loop, set_loop);
 }
 }  // namespace
 
@@ -2273,16 +2265,14 @@ cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t
                           cudaStream_t st, LaunchSink* sink, WaveGraphs* graphs) {
     if (kind.bundles && w.hero < 2) return cudaErrorInvalidValue;
     const int grid = launch_grid(w, sms, shape);
-    int32_t* ca = &w.counts[0];
-    int32_t* cb = &w.counts[1];
     if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
         // host-driven: groups of half-iterations, the progress word read between groups
         Issue I{w, kind, f, grid, shape.sort_rays, st, sink};
         stream_prologue(I);
         for (;;) {
             for (int r = 0; r < 4; ++r) {
-                stream_half(I, w.qa, ca, w.qb, cb, 0, 0);
-                stream_half(I, w.qb, cb, w.qa, ca, 0, 0);
+                stream_half(I, 0, 0, 0);
+                stream_half(I, 1, 0, 0);
             }
             cudaError_t e = cudaGetLastError();
             int32_t more = 0;
@@ -2326,8 +2316,8 @@ cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t
     cudaGraph_t body = p.conditional.phGraph_out[0];
     err = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (err == cudaSuccess) {
-        stream_half(I, w.qa, ca, w.qb, cb, loop, 0);
-        stream_half(I, w.qb, cb, w.qa, ca, loop, 1);
+        stream_half(I, 0, loop, 0);
+        stream_half(I, 1, loop, 1);
         cudaGraph_t b2 = nullptr;
         err = cudaStreamEndCapture(st, &b2);
     }

@@ -50,53 +50,59 @@ struct DevJob {
 // Progress of a streaming pass (device memory, updated by k_stream_advance).
 struct StreamCtl {
     long long next;            // photons of the pass handed out so far
-    int32_t free_n;            // entries on the free-slot stack (Wave::freel)
-    int32_t taken;             // slots claimed by the current refill
+    int32_t taken;             // paths the current refill appended
     int32_t half;              // half-iterations (extend / shade / refill / shadow) run
     int32_t more;              // work left after the last half-iteration (0 / 1)
+    int32_t pad;
 };
 
-// Per-wave path state, queues and shadow-ray records (structure of arrays, W slots).
-struct Wave {
-    int32_t W;                 // slots
-    int32_t S;                 // shadow-record capacity
+// The state of the paths in flight, compacted: path i of a queue of n lives at index i of
+// every array (structure of arrays, W entries each), so every kernel reads and writes it
+// with consecutive lanes on consecutive entries.  A wave holds two, and shading copies the
+// surviving paths from one to the other.
+struct PathState {
     uint64_t* rng_s; uint64_t* rng_i;
     double *ox, *oy, *oz, *dx, *dy, *dz, *lam, *beta;
     double* cie;               // [3][W] the CIE matching functions at the path's wavelength
-    int32_t* stk_n;            // medium-stack depth per slot
+    int32_t* stk_n;            // medium-stack depth
     int2* stk;                 // [kStkCap][W] (material, priority)
-    double* hit_t;
+    int32_t* nbounce;          // bounces traced so far
+    int32_t* job;              // job of each path (multi-job tables)
+    // hero-wavelength bundles (null unless the buffer carries bundles)
+    double* hlam;              // [hero][W] wavelengths, index 0 the hero
+    double* hbeta;             // [hero][W] per-wavelength throughput
+    int32_t* hlive;            // live wavelengths (hero_c, 1 after a dielectric)
+    // parity instrumentation (null unless logging)
+    uint64_t* pid;             // photon index
+    uint64_t* lhash;
+    int32_t* lnh;
+    int32_t* lprims;           // [8][W]
+};
+
+// Per-wave path state, hits, queues and shadow-ray records (structure of arrays).
+struct Wave {
+    int32_t W;                 // paths
+    int32_t S;                 // shadow-record capacity
+    PathState ps[2];           // the paths to trace and the survivors of shading (ping-pong)
+    double* hit_t;             // closest hit of path i (indexed like the queue being traced)
     int32_t* hit_rec;          // world record of the closest hit, or -1
     int32_t* hit_sub;          // BLAS record when hit_rec is an instance
-    int32_t* qa;               // active slot lists (ping-pong)
-    int32_t* qb;
-    int32_t* counts;           // [0] qa count, [1] qb count, [2] shadow count
-    int32_t* job;              // job of each slot (multi-job waves)
+    int32_t* perm;             // optional traversal order of a queue (bucketed by direction)
+    int32_t* counts;           // [0] paths in ps[0], [1] in ps[1], [2] shadow records
     int32_t* sjob;             // job of each shadow record
     DevJob* jobs;              // device job table, kWaveJobs entries
-    int32_t* params;           // [0] jobs in the table, [1] slots in use (written with the table);
-                               // streaming pass: int64 [1] photons of the pass, [2] half-iteration cap
-    int32_t* nbounce;          // bounces done per slot (streaming pass)
-    int32_t* freel;            // free-slot stack (streaming pass)
+    int32_t* params;           // [0] jobs in the table, [1] paths in flight at most (written with
+                               // the table); streaming pass: int64 [1] photons, [2] half-iteration cap
     StreamCtl* ctl;
     double *sox, *soy, *soz, *sdx, *sdy, *sdz, *smax, *sval, *slam;
     double* sxyz;              // [3][S] film increments (X, Y, Z) of one-wavelength connections
     int32_t* spix;
     int32_t* sview;            // view of each connection (multi-camera jobs)
-    // hero-wavelength bundles (hero > 1 only; null otherwise)
     int32_t hero;              // wavelengths a path of this buffer can carry
-    double* hlam;              // [hero][W] wavelengths, index 0 the hero
-    double* hbeta;             // [hero][W] per-wavelength throughput
-    int32_t* hlive;            // [W] live wavelengths (hero_c, 1 after a dielectric)
     double* xlam;              // [hero-1][S] further wavelengths of a connection
     double* xval;              // [hero-1][S] and their contributions
     int32_t* snup;             // [S] wavelengths in each connection
-    // parity instrumentation (null unless logging)
-    uint64_t* pid;             // photon index per slot
-    uint64_t* lhash;
-    int32_t* lnh;
-    int32_t* lprims;           // [8][W]
-    ftb_photon_log* logs;      // output, indexed by photon - log_base
+    ftb_photon_log* logs;      // output, indexed by photon - log_base (null unless logging)
     int64_t log_base;
     void* block;               // the single allocation backing everything above
     size_t bytes;
@@ -110,29 +116,30 @@ struct Frame {
     int32_t* status;
 };
 
-// Shadow records per slot: a path queues at most 2 connections per view per bounce, and in
-// a streaming pass a refilled slot's emission adds one more in the same half-iteration.
+// Shadow records per path: a path queues at most 2 connections per view per bounce, and in
+// a streaming pass a refilled path's emission adds one more in the same half-iteration.
 constexpr int kShadowPerSlot = 3;
 
-// Bytes of one wave of W slots: every array rounded up to 256 B, in the order wave_carve
+// Bytes of one wave of W paths: every array rounded up to 256 B, in the order wave_carve
 // lays them out.  constexpr so a fixed device array can hold a wave (ftb_noalloc.cu).
 constexpr size_t wave_align(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t path_state_bytes(size_t w, bool log, int32_t hero) {
+    size_t b = 2 * wave_align(8 * w);                                   // rng
+    b += 8 * wave_align(8 * w) + wave_align(24 * w);                    // ray + lam + beta + cie
+    b += wave_align(4 * w) + wave_align(8 * w * kStkCap);               // medium stack
+    b += 2 * wave_align(4 * w);                                         // bounces, job
+    if (hero > 1) b += 2 * wave_align(8 * w * (size_t)hero) + wave_align(4 * w);
+    if (log) b += 2 * wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
+    return b;
+}
 constexpr size_t wave_bytes(int32_t W, bool log, int32_t hero = 1) {
     size_t w = (size_t)W, s = kShadowPerSlot * (size_t)W;
-    size_t b = 0;
-    b += 2 * wave_align(8 * w);                                     // rng
-    b += 8 * wave_align(8 * w) + wave_align(24 * w);                // ray + lam + beta + cie
-    b += wave_align(4 * w) + wave_align(8 * w * kStkCap);           // medium stack
-    b += wave_align(8 * w) + 2 * wave_align(4 * w);                 // hit t, record, sub-record
-    b += 2 * wave_align(4 * w) + wave_align(64);                    // queues + counts
-    b += wave_align(4 * w) + wave_align(4 * s) + wave_align(sizeof(DevJob) * kWaveJobs);   // job ids + table
-    b += wave_align(64);                                            // table parameters
-    b += 2 * wave_align(4 * w) + wave_align(64);                    // streaming: bounces, free stack, ctl
+    size_t b = 2 * path_state_bytes(w, log, hero);
+    b += wave_align(8 * w) + 3 * wave_align(4 * w);                     // hit t, record, sub-record, perm
+    b += wave_align(64) + wave_align(4 * s) + wave_align(sizeof(DevJob) * kWaveJobs);   // counts, sjob, table
+    b += 2 * wave_align(64);                                            // table parameters, ctl
     b += 9 * wave_align(8 * s) + wave_align(24 * s) + 2 * wave_align(4 * s);   // shadow records
-    if (log) b += 2 * wave_align(8 * w) + wave_align(4 * w) + wave_align(4 * w * 8);
-    if (hero > 1)                                                   // bundles
-        b += 2 * wave_align(8 * w * hero) + wave_align(4 * w) + 2 * wave_align(8 * s * (hero - 1)) +
-             wave_align(4 * s);
+    if (hero > 1) b += 2 * wave_align(8 * s * (hero - 1)) + wave_align(4 * s);
     return b;
 }
 // Point the arrays of `w` into `block` (wave_bytes(W, log, hero) bytes, 256-B aligned).
@@ -187,17 +194,18 @@ cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const
 
 // Trace a streaming pass on `stream`: the caller has written the table of photon ranges to
 // w.jobs (g0 consecutive from 0) and w.params = {ranges, slots, photons (int64 at [1]),
-// half-iteration cap (int64 at [2])}.  The pass keeps `slots` paths in flight: every
-// half-iteration runs closest hit, shading (dead paths push their slot on the free stack),
-// a refill that emits the next photons of the pass into the free slots, and the queued
-// connections, until every photon is done.  With `graphs` and shape.graph the loop is one
+// half-iteration cap (int64 at [2])}.  The pass keeps up to `slots` paths in flight: every
+// half-iteration runs closest hit, shading (the survivors are compacted into the other
+// path buffer), a refill that appends the next photons of the pass up to `slots` paths,
+// and the queued connections, until every photon is done.  With `graphs` and shape.graph the loop is one
 // graph launch (a conditional while node whose condition the device sets); otherwise the
 // host issues half-iterations in groups and reads the progress word between groups.
 cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t sms, const LaunchShape& shape,
                           cudaStream_t stream, LaunchSink* sink = nullptr, WaveGraphs* graphs = nullptr);
 
-// Half-iterations a streaming pass of `photons` over `slots` slots can need: every slot
-// consumes a photon at least once per max_bounce + 1 half-iterations while photons remain.
+// Half-iterations a streaming pass of `photons` with `slots` paths in flight can need: a
+// path ends within max_bounce half-iterations and its place is refilled in the one it ends
+// in, so while photons remain every max_bounce + 1 half-iterations hand out >= slots.
 inline int64_t stream_half_cap(int64_t photons, int64_t slots, int32_t max_bounce) {
     const int64_t per = slots > 0 ? (photons + slots - 1) / slots : 0;
     return (per + 2) * ((int64_t)(max_bounce > 0 ? max_bounce : 0) + 2) + 4;

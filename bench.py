@@ -276,10 +276,15 @@ def run_animation(args):
         torch.cuda.synchronize(dev)
     batch_s = sum(a.elapsed_time(b) for a, b in ev) / 1e3
     value = total * args.steps / batch_s
-    # photons are packed contiguously into waves; a wave launches emit, shadow and, per
-    # bounce, extend, shade and shadow
-    waves = -(-total // tuning.wave_slots)
-    launches = waves * (2 + 3 * 16)
+    # launches of one batch, counted by the profiler on an untimed copy of it (direct
+    # launches, the same sequence a graph replay makes; progress kernels as in main())
+    clones[0].set_profiling(1)
+    clones[0].profile(reset=True)
+    L.render_batch(jobs(), stream=stream.cuda_stream, want_energy=False)
+    torch.cuda.synchronize(dev)
+    pl = clones[0].profile(reset=True).launches
+    clones[0].set_profiling(0)
+    launches = int(sum(pl)) + (int(pl[1]) + 2 if tuning.regenerate else 0)
 
     # end to end: per-frame TLAS refit + the batch + every film to pinned host memory
     t = time.perf_counter()
@@ -327,7 +332,8 @@ def run_animation(args):
                "l2": "flushed between timed steps (256 MiB write)", "blas_bake_ms": round(blas_ms, 1),
                "clone_refit_ms_per_frame": round(clone_ms / len(frames), 3),
                "tuning": {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
-                          "graph_replay": bool(tuning.use_graphs), "autotune_s": round(tune_s, 2)}}
+                          "graph_replay": bool(tuning.use_graphs), "regenerate": bool(tuning.regenerate),
+                          "autotune_s": round(tune_s, 2)}}
         line = {
             "metric": "photon paths/s on 1 B200 (batched animation)", "value": value, "unit": "photon paths/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * batch_s / args.steps,
@@ -639,7 +645,14 @@ def main():
         "kernel_times": "CUDA events on the launching streams over a second set of the same timed steps "
                         f"(direct launches, {sum(prof_ms) / len(prof_ms):.2f} ms per step)",
     }
+    # kernels the profiled steps launched: the four traced kernels (counted by the profiler),
+    # plus, in streaming passes, the progress kernel after every half-iteration (one per
+    # closest-hit launch) and a pass's set-up and first progress launch, and the queue sort
     gpu_launches = int(sum(prof.launches))
+    if tuning.regenerate:
+        gpu_launches += int(prof.launches[1]) + 2 * args.steps
+    if tuning.sort_rays:
+        gpu_launches += int(prof.launches[1])
 
     # the same frame on the GPU-built BVH (device LBVH: faster bake, looser tree)
     fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -2266,14 +2266,13 @@ cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t
     if (kind.bundles && w.hero < 2) return cudaErrorInvalidValue;
     const int grid = launch_grid(w, sms, shape);
     if (!(shape.graph && graphs) || sink || f.stats || w.logs) {
-        // host-driven: groups of half-iterations, the progress word read between groups
+        // host-driven: the graph's loop body (two half-iterations) at a time, the progress
+        // word read after each, so the launches are the ones a graph replay makes
         Issue I{w, kind, f, grid, shape.sort_rays, st, sink};
         stream_prologue(I);
         for (;;) {
-            for (int r = 0; r < 4; ++r) {
-                stream_half(I, 0, 0, 0);
-                stream_half(I, 1, 0, 0);
-            }
+            stream_half(I, 0, 0, 0);
+            stream_half(I, 1, 0, 0);
             cudaError_t e = cudaGetLastError();
             int32_t more = 0;
             if (e == cudaSuccess) e = cudaMemcpyAsync(&more, &w.ctl->more, sizeof more, cudaMemcpyDeviceToHost, st);

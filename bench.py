@@ -577,7 +577,7 @@ def main():
         tuning = L.set_tuning(local, wave_slots=v[0], grid_mult=v[1], use_graphs=v[2], sort_rays=v[3],
                               regenerate=v[4])
     else:
-        tuning = L.autotune(sc, cam, min(n, 1 << 24), mb)   # (one wavelength per photon)
+        tuning = L.autotune(sc, cam, min(n, 1 << 26), mb)   # (one wavelength per photon)
     cfg["tuning"] = {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
                      "graph_replay": bool(tuning.use_graphs), "sort_rays": bool(tuning.sort_rays),
                      "regenerate": bool(tuning.regenerate),

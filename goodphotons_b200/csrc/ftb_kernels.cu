@@ -1007,33 +1007,55 @@ __device__ void block_tally(unsigned long long* dst, long long v) {
 
 enum { T_EMIT = 0, T_ABS = 1, T_SENSOR = 2, T_ESC = 3, T_RES = 4 };
 
-// Per-thread energy tallies.  A single-job wave reduces them over the block once at the
-// end of the kernel; in a multi-job wave a thread flushes its sums to the job's tallies
-// whenever the job of the path it books changes (slots of one job are contiguous, so
-// this is rare) and at the end.
+// Per-thread energy tallies.  A single-job launch reduces them over the block once at the
+// end of the kernel.  In a multi-job launch a thread moves its sums into a per-block table
+// in shared memory (one row of five per job of the table) whenever the job of the path it
+// books changes -- often, in a streaming pass, where the paths of neighbouring jobs share
+// the queues -- and the block adds the table's nonzero entries to the jobs' tallies once
+// at the end, so the global atomics per launch do not grow with the job changes.
 struct TallyAcc {
     int job;
+    bool multi;
     long long v[5];
 };
-__device__ __forceinline__ void tally_init(TallyAcc& a) {
+__device__ __forceinline__ unsigned long long* tally_table() {
+    __shared__ unsigned long long tab[kWaveJobs * 5];
+    return tab;
+}
+// Called by every thread of the block at the start of the kernel.
+__device__ __forceinline__ void tally_init(TallyAcc& a, bool multi, int n_jobs) {
     a.job = 0;
+    a.multi = multi;
 #pragma unroll
     for (int k = 0; k < 5; ++k) a.v[k] = 0;
+    if (multi) {
+        unsigned long long* tab = tally_table();
+        for (int e = threadIdx.x; e < n_jobs * 5; e += blockDim.x) tab[e] = 0ull;
+        __syncthreads();
+    }
 }
-__device__ __forceinline__ void tally_flush(TallyAcc& a, const DevJob* jobs) {
-    unsigned long long* t = jobs[a.job].tally;
+__device__ __forceinline__ void tally_flush(TallyAcc& a) {
+    unsigned long long* row = tally_table() + 5 * a.job;
 #pragma unroll
     for (int k = 0; k < 5; ++k)
-        if (a.v[k]) { atomicAdd(t + k, (unsigned long long)a.v[k]); a.v[k] = 0; }
+        if (a.v[k]) { atomicAdd(row + k, (unsigned long long)a.v[k]); a.v[k] = 0; }
 }
 __device__ __forceinline__ void tally_add(TallyAcc& a, const DevJob* jobs, bool multi, int job, int k,
                                           long long x) {
-    if (multi && job != a.job) { tally_flush(a, jobs); a.job = job; }
+    if (multi && job != a.job) { tally_flush(a); a.job = job; }
     a.v[k] += x;
 }
 __device__ void block_tally(unsigned long long* dst, long long v);
-__device__ __forceinline__ void tally_finish(TallyAcc& a, const DevJob* jobs, bool multi) {
-    if (multi) { tally_flush(a, jobs); return; }
+// Called by every thread of the block at the end of the kernel.
+__device__ __forceinline__ void tally_finish(TallyAcc& a, const DevJob* jobs, bool multi, int n_jobs = 1) {
+    if (multi) {
+        tally_flush(a);
+        __syncthreads();
+        const unsigned long long* tab = tally_table();
+        for (int e = threadIdx.x; e < n_jobs * 5; e += blockDim.x)
+            if (tab[e]) atomicAdd(jobs[e / 5].tally + e % 5, tab[e]);
+        return;
+    }
     unsigned long long* t = jobs[0].tally;
 #pragma unroll
     for (int k = 0; k < 5; ++k) block_tally(t + k, a.v[k]);
@@ -1198,7 +1220,7 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
     const bool multi = n_jobs > 1;
     const PhotonSource src = photon_source<STREAM>(w, out_count);
     TallyAcc acc;
-    tally_init(acc);
+    tally_init(acc, multi, n_jobs);
     for (int64_t t = blockIdx.x * blockDim.x + threadIdx.x; t < src.n; t += gridDim.x * blockDim.x) {
         uint64_t k;
         const int j = photon_job<STREAM>(jobs, n_jobs, src, t, k);
@@ -1232,7 +1254,7 @@ __global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__
         out.cie[o] = cie[0]; out.cie[w.W + o] = cie[1]; out.cie[2 * (size_t)w.W + o] = cie[2];
         out.stk_n[o] = 0;
     }
-    tally_finish(acc, jobs, multi);
+    tally_finish(acc, jobs, multi, n_jobs);
 }
 
 __device__ void block_add3(unsigned long long* dst, unsigned long long a, unsigned long long b,
@@ -1415,9 +1437,10 @@ template <bool MEDIA, bool INST>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
                                                                Frame f, PathState in, const int32_t* in_count,
                                                                PathState out, int32_t* out_count) {
-    const bool multi = w.params[0] > 1;
+    const int32_t n_jobs = w.params[0];
+    const bool multi = n_jobs > 1;
     TallyAcc acc;
-    tally_init(acc);
+    tally_init(acc, multi, n_jobs);
     int nq = *in_count;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
         const int j = multi ? in.job[i] : 0;
@@ -1589,7 +1612,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
         if (multi) out.job[o] = j;
         log_move(w, in, i, out, o);
     }
-    tally_finish(acc, jobs, multi);
+    tally_finish(acc, jobs, multi, n_jobs);
 }
 
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
@@ -1692,7 +1715,7 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
     const bool multi = n_jobs > 1;
     const PhotonSource src = photon_source<STREAM>(w, out_count);
     TallyAcc acc;
-    tally_init(acc);
+    tally_init(acc, multi, n_jobs);
     for (int64_t t = blockIdx.x * blockDim.x + threadIdx.x; t < src.n; t += gridDim.x * blockDim.x) {
         uint64_t k;
         const int j = photon_job<STREAM>(jobs, n_jobs, src, t, k);
@@ -1737,16 +1760,17 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
         out.hlive[o] = C;
         out.stk_n[o] = 0;
     }
-    tally_finish(acc, jobs, multi);
+    tally_finish(acc, jobs, multi, n_jobs);
 }
 
 template <bool INST>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, const DevJob* __restrict__ jobs,
                                                                     Frame f, PathState in, const int32_t* in_count,
                                                                     PathState out, int32_t* out_count) {
-    const bool multi = w.params[0] > 1;
+    const int32_t n_jobs = w.params[0];
+    const bool multi = n_jobs > 1;
     TallyAcc acc;
-    tally_init(acc);
+    tally_init(acc, multi, n_jobs);
     int nq = *in_count;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
         const int j = multi ? in.job[p] : 0;
@@ -1933,7 +1957,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
         if (multi) out.job[o] = j;
         log_move(w, in, p, out, o);
     }
-    tally_finish(acc, jobs, multi);
+    tally_finish(acc, jobs, multi, n_jobs);
 }
 
 // Connections of bundles: one occlusion test, then a splat per wavelength.

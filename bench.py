@@ -593,12 +593,14 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
         with ClockSampler(local if clocks_on else -1) as clk:
+            torch.cuda.nvtx.range_push("timed")   # ncu --nvtx --nvtx-include "timed/" selects these steps
             for k in range(args.steps):
                 flush.fill_(k & 0xff)
                 ev[k][0].record(stream)
                 step(first_step + k)
                 ev[k][1].record(stream)
             torch.cuda.synchronize(dev)
+            torch.cuda.nvtx.range_pop()
         if dist is not None:
             dist.barrier()
         return [a.elapsed_time(b) for a, b in ev], clk

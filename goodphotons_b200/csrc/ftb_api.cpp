@@ -658,7 +658,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         table.clear();
         int64_t g = 0;
         int32_t max_bounce = 0, slots = W;
-        bool inst = false, media = false;
+        bool inst = false, media = false, shapes = false;
         int bundles = -1, views = -1;
         while (j < base.size() && (int)table.size() < ftb::kWaveJobs) {
             const int64_t left = count[j] - done_in_job;
@@ -681,6 +681,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
             max_bounce = std::max(max_bounce, J.max_bounce);
             inst |= J.sc.n_inst > 0;
             media |= J.sc.n_med > 0;
+            shapes |= ftb::scene_has_shapes(J.sc);
             g += m;
             done_in_job += m;
             if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
@@ -698,6 +699,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         kind.instances = inst;
         kind.bundles = bundles == 1;
         kind.media = media;
+        kind.shapes = shapes;
         e = ftb::launch_stream(w, kind, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
                                s->eng->graphs[k & 1]);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
@@ -706,7 +708,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
     while (j < base.size()) {
         table.clear();
         int32_t slots = 0, max_bounce = 0;
-        bool inst = false, media = false;
+        bool inst = false, media = false, shapes = false;
         int bundles = -1;   // a wave holds either one-wavelength jobs or bundles, not both
         // A path queues at most 2 connections per view per bounce and the shadow queue holds
         // 2W records, so a wave of multi-camera jobs carries W / views slots.
@@ -729,6 +731,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
             max_bounce = std::max(max_bounce, J.max_bounce);
             inst |= J.sc.n_inst > 0;
             media |= J.sc.n_med > 0;
+            shapes |= ftb::scene_has_shapes(J.sc);
             slots += m;
             done_in_job += m;
             if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
@@ -744,6 +747,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         kind.instances = inst;
         kind.bundles = bundles == 1;
         kind.media = media;
+        kind.shapes = shapes;
         e = ftb::launch_wave(w, max_bounce, kind, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
                              s->eng->graphs[k & 1]);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");

@@ -356,8 +356,12 @@ struct RayCtx {
     CurveRay cr;
 };
 
+// SHAPES: the scene has spheres or curves besides triangles; without them the record test
+// is the triangle test alone (a smaller traversal kernel with fewer spills).
+template <bool SHAPES>
 __device__ __forceinline__ bool rec_test(const RayCtx& R, const PrimRec& r, double tmin, double tbest,
                                          double& t) {
+    if (!SHAPES) return tri_test(R.sh, R.o, r.d, tmin, tbest, t, nullptr);
     int ty = rec_type(r);
     if (ty == REC_TRI) return tri_test(R.sh, R.o, r.d, tmin, tbest, t, nullptr);
     if (ty == REC_SPHERE) return sphere_test(R.o, R.d, r.d, tmin, tbest, t);
@@ -370,8 +374,9 @@ struct Hit {
     D3 p, n, ng;
     int mat, prim;
 };
+template <bool SHAPES>
 __device__ void hit_attributes(const double* __restrict__ tri_n, const RayCtx& R, const PrimRec& r, Hit& h) {
-    int ty = rec_type(r);
+    int ty = SHAPES ? rec_type(r) : REC_TRI;
     h.mat = rec_mat(r);
     h.prim = r.prim;
     double t = 0.0;
@@ -707,7 +712,7 @@ __device__ __noinline__ bool blas_any(const DevInst& I, D3 wo, D3 wd, double tmi
 // Closest hit (Scene::closestHit, scene.h:2194-2242): returns the world record (or -1) and
 // t; for an instance record, *sub receives the BLAS record.  INST selects the variant that
 // can meet instance records (scenes with instances); the plain variant has no such branch.
-template <bool COUNT, bool INST>
+template <bool COUNT, bool INST, bool SHAPES>
 __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin, double& best_t, int* sub,
                                 int32_t* status, TravCount& cnt) {
     const RayF F = make_rayf(R.o, R.d);
@@ -726,7 +731,7 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
             }
             if (COUNT) cnt.exact++;
             double t;
-            if (rec_test(R, r, tmin, best_t, t)) { best_t = t; best = first + k; tm = __double2float_ru(t); }
+            if (rec_test<SHAPES>(R, r, tmin, best_t, t)) { best_t = t; best = first + k; tm = __double2float_ru(t); }
         }
         return tm;
     };
@@ -736,7 +741,7 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
 }
 
 // Any hit with t in [tmin, seg) (Scene::occluded, scene.h:2249-2271).
-template <bool COUNT, bool INST>
+template <bool COUNT, bool INST, bool SHAPES>
 __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, double seg, int32_t* status,
                              TravCount& cnt) {
     const RayF F = make_rayf(R.o, R.d);
@@ -753,7 +758,7 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
             }
             if (COUNT) cnt.exact++;
             double t;
-            if (rec_test(R, r, tmin, seg, t)) return true;
+            if (rec_test<SHAPES>(R, r, tmin, seg, t)) return true;
         }
         return false;
     };
@@ -770,7 +775,7 @@ __device__ void instance_hit(const DevInst& I, int sub, D3 ro, D3 rd, Hit& h) {
     R.sh = make_shear(L.d);
     PrimRec br;
     load_rec(I.recs, sub, br);
-    hit_attributes(I.tri_n, R, br, h);
+    hit_attributes<false>(I.tri_n, R, br, h);   // BLAS records are triangles
     h.p = ro + rd * h.t;                        // world t == local t
     D3 wn = normalize(xf_normal(I.xl, h.n));
     D3 wng = normalize(xf_normal(I.xl, h.ng));
@@ -1283,7 +1288,7 @@ __device__ void block_add1(unsigned long long* dst, unsigned long long a) {
 #define FTB_SHADE_MINB 4
 #endif
 
-template <bool COUNT, bool INST>
+template <bool COUNT, bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const DevJob* __restrict__ jobs,
                                                               PathState in, const int32_t* qcount,
                                                               const int32_t* __restrict__ order, Frame f) {
@@ -1297,7 +1302,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const Dev
         RayCtx R = make_ray(mk(in.ox[i], in.oy[i], in.oz[i]), mk(in.dx[i], in.dy[i], in.dz[i]));
         double t;
         int sub = -1;
-        int rec = traverse_closest<COUNT, INST>(sc, R, EPS_RAY, t, &sub, f.status, cnt);
+        int rec = traverse_closest<COUNT, INST, SHAPES>(sc, R, EPS_RAY, t, &sub, f.status, cnt);
         w.hit_t[i] = t;
         w.hit_rec[i] = rec;
         if (INST) w.hit_sub[i] = sub;
@@ -1433,7 +1438,7 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 }
 
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
-template <bool MEDIA, bool INST>
+template <bool MEDIA, bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
                                                                Frame f, PathState in, const int32_t* in_count,
                                                                PathState out, int32_t* out_count) {
@@ -1497,7 +1502,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
                 h.prim = r.prim;
             } else {
                 RayCtx R = make_ray(ro, rd);
-                hit_attributes(sc.tri_n, R, r, h);
+                hit_attributes<SHAPES>(sc.tri_n, R, r, h);
             }
             const DevMat& m = sc.mats[h.mat];
             switch (m.type) {
@@ -1616,7 +1621,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const Dev
 }
 
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
-template <bool COUNT, bool INST>
+template <bool COUNT, bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const DevJob* __restrict__ jobs,
                                                               Frame f) {
     const int32_t n_jobs = w.params[0];
@@ -1631,7 +1636,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
         double max_dist = w.smax[i];
         RayCtx R = make_ray(o, d);
         if (COUNT) rays++;
-        if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
+        if (traverse_any<COUNT, INST, SHAPES>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         const double X = w.sxyz[i], Y = w.sxyz[w.S + i], Z = w.sxyz[2 * (size_t)w.S + i];
         long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i])) + 4 * (size_t)w.spix[i];
         atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, f.status));
@@ -1763,7 +1768,7 @@ __global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restr
     tally_finish(acc, jobs, multi, n_jobs);
 }
 
-template <bool INST>
+template <bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, const DevJob* __restrict__ jobs,
                                                                     Frame f, PathState in, const int32_t* in_count,
                                                                     PathState out, int32_t* out_count) {
@@ -1814,7 +1819,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                 h.prim = r.prim;
             } else {
                 RayCtx R = make_ray(ro, rd);
-                hit_attributes(sc.tri_n, R, r, h);
+                hit_attributes<SHAPES>(sc.tri_n, R, r, h);
             }
             const DevMat& m = sc.mats[h.mat];
             switch (m.type) {
@@ -1961,7 +1966,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
 }
 
 // Connections of bundles: one occlusion test, then a splat per wavelength.
-template <bool COUNT, bool INST>
+template <bool COUNT, bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, const DevJob* __restrict__ jobs,
                                                                    Frame f) {
     const int32_t n_jobs = w.params[0];
@@ -1976,7 +1981,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, cons
         double max_dist = w.smax[i];
         RayCtx R = make_ray(o, d);
         if (COUNT) rays++;
-        if (traverse_any<COUNT, INST>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
+        if (traverse_any<COUNT, INST, SHAPES>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i])) + 4 * (size_t)w.spix[i];
         const int nup = w.snup[i];
         // every wavelength is one Film::add, each rounded to fixed point on its own; their
@@ -2097,6 +2102,27 @@ __global__ void k_stream_advance(Wave w, Frame f, int32_t* consumed, int32_t* ne
     if (set_loop) cudaGraphSetConditional(loop, (unsigned)more);
 }
 
+// Launchers of the traversal kernels' variants (template template arguments of Issue::trav).
+template <bool C, bool I, bool S>
+struct LaunchExtend {
+    static void go(int grid, cudaStream_t st, Wave w, const DevJob* jobs, PathState in, const int32_t* c,
+                   const int32_t* order, Frame f) {
+        k_extend<C, I, S><<<grid, 128, 0, st>>>(w, jobs, in, c, order, f);
+    }
+};
+template <bool C, bool I, bool S>
+struct LaunchShadow {
+    static void go(int grid, cudaStream_t st, Wave w, const DevJob* jobs, Frame f) {
+        k_shadow<C, I, S><<<grid, 128, 0, st>>>(w, jobs, f);
+    }
+};
+template <bool C, bool I, bool S>
+struct LaunchShadowHero {
+    static void go(int grid, cudaStream_t st, Wave w, const DevJob* jobs, Frame f) {
+        k_shadow_hero<C, I, S><<<grid, 128, 0, st>>>(w, jobs, f);
+    }
+};
+
 namespace {
 // Kernel launches of one wave buffer with the variants its WaveKind selects.
 struct Issue {
@@ -2124,30 +2150,24 @@ struct Issue {
         }
         mark(K_EMIT, true);
     }
-    void shadow() {
-        const bool inst = kind.instances, count = f.stats != nullptr;
-        const DevJob* jobs = w.jobs;
-        mark(K_SHADOW, false);
-        if (kind.bundles) {
-            if (count) {
-                if (inst) k_shadow_hero<true, true><<<grid, T, 0, st>>>(w, jobs, f);
-                else k_shadow_hero<true, false><<<grid, T, 0, st>>>(w, jobs, f);
-            } else {
-                if (inst) k_shadow_hero<false, true><<<grid, T, 0, st>>>(w, jobs, f);
-                else k_shadow_hero<false, false><<<grid, T, 0, st>>>(w, jobs, f);
-            }
-        } else if (count) {
-            if (inst) k_shadow<true, true><<<grid, T, 0, st>>>(w, jobs, f);
-            else k_shadow<true, false><<<grid, T, 0, st>>>(w, jobs, f);
+    template <template <bool, bool, bool> class K, class... A>
+    void trav(A... args) {   // a traversal kernel with the counting / instance / shape variant
+        const bool count = f.stats != nullptr, inst = kind.instances, shp = kind.shapes;
+        if (count) {
+            if (inst) { if (shp) K<true, true, true>::go(grid, st, args...); else K<true, true, false>::go(grid, st, args...); }
+            else { if (shp) K<true, false, true>::go(grid, st, args...); else K<true, false, false>::go(grid, st, args...); }
         } else {
-            if (inst) k_shadow<false, true><<<grid, T, 0, st>>>(w, jobs, f);
-            else k_shadow<false, false><<<grid, T, 0, st>>>(w, jobs, f);
+            if (inst) { if (shp) K<false, true, true>::go(grid, st, args...); else K<false, true, false>::go(grid, st, args...); }
+            else { if (shp) K<false, false, true>::go(grid, st, args...); else K<false, false, false>::go(grid, st, args...); }
         }
+    }
+    void shadow() {
+        mark(K_SHADOW, false);
+        if (kind.bundles) trav<LaunchShadowHero>(w, (const DevJob*)w.jobs, f);
+        else trav<LaunchShadow>(w, (const DevJob*)w.jobs, f);
         mark(K_SHADOW, true);
     }
     void extend(const PathState& in, int32_t* c) {
-        const bool inst = kind.instances, count = f.stats != nullptr;
-        const DevJob* jobs = w.jobs;
         mark(K_EXTEND, false);
         const int32_t* order = nullptr;
         if (sorted) {
@@ -2155,29 +2175,25 @@ struct Issue {
             k_sort_queue<<<gs, T, 0, st>>>(w, in, c, w.perm);
             order = w.perm;
         }
-        if (count) {
-            if (inst) k_extend<true, true><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
-            else k_extend<true, false><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
-        } else {
-            if (inst) k_extend<false, true><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
-            else k_extend<false, false><<<grid, T, 0, st>>>(w, jobs, in, c, order, f);
-        }
+        trav<LaunchExtend>(w, (const DevJob*)w.jobs, in, (const int32_t*)c, order, f);
         mark(K_EXTEND, true);
     }
     void shade(const PathState& in, const int32_t* ci, const PathState& out, int32_t* co) {
-        const bool inst = kind.instances;
+        const bool inst = kind.instances, shp = kind.shapes;
         const DevJob* jobs = w.jobs;
         mark(K_SHADE, false);
+#define FTB_SHADE(...) __VA_ARGS__<<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co)
         if (kind.bundles) {
-            if (inst) k_shade_hero<true><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
-            else k_shade_hero<false><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
+            if (inst) { if (shp) FTB_SHADE(k_shade_hero<true, true>); else FTB_SHADE(k_shade_hero<true, false>); }
+            else { if (shp) FTB_SHADE(k_shade_hero<false, true>); else FTB_SHADE(k_shade_hero<false, false>); }
         } else if (kind.media) {
-            if (inst) k_shade<true, true><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
-            else k_shade<true, false><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
+            if (inst) { if (shp) FTB_SHADE(k_shade<true, true, true>); else FTB_SHADE(k_shade<true, true, false>); }
+            else { if (shp) FTB_SHADE(k_shade<true, false, true>); else FTB_SHADE(k_shade<true, false, false>); }
         } else {
-            if (inst) k_shade<false, true><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
-            else k_shade<false, false><<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co);
+            if (inst) { if (shp) FTB_SHADE(k_shade<false, true, true>); else FTB_SHADE(k_shade<false, true, false>); }
+            else { if (shp) FTB_SHADE(k_shade<false, false, true>); else FTB_SHADE(k_shade<false, false, false>); }
         }
+#undef FTB_SHADE
         mark(K_SHADE, true);
     }
 };
@@ -2226,7 +2242,7 @@ void stream_half(Issue& I, int a, cudaGraphConditionalHandle loop, int32_t set_l
 struct WaveGraphs {
     struct Entry {
         int32_t max_bounce, grid;   // max_bounce -1: a streaming pass
-        bool inst, hero, media, sorted;
+        bool inst, hero, media, shapes, sorted;
         int32_t* status;
         cudaGraphExec_t exec;
     };
@@ -2237,7 +2253,7 @@ struct WaveGraphs {
     cudaGraphExec_t find(int32_t max_bounce, int32_t grid, const WaveKind& kind, bool sorted, int32_t* status) const {
         for (auto& e : entries)
             if (e.max_bounce == max_bounce && e.grid == grid && e.inst == kind.instances && e.hero == kind.bundles &&
-                e.media == kind.media && e.sorted == sorted && e.status == status)
+                e.media == kind.media && e.shapes == kind.shapes && e.sorted == sorted && e.status == status)
                 return e.exec;
         return nullptr;
     }
@@ -2276,8 +2292,8 @@ cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const
     issue_wave(I, max_bounce);
     err = cudaStreamEndCapture(st, &g);
     if (err != cudaSuccess) return err;
-    WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, shape.sort_rays, f.status,
-                        nullptr};
+    WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, kind.shapes, shape.sort_rays,
+                        f.status, nullptr};
     err = cudaGraphInstantiate(&e.exec, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) return err;
@@ -2344,7 +2360,8 @@ cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t
         cudaGraph_t b2 = nullptr;
         err = cudaStreamEndCapture(st, &b2);
     }
-    WaveGraphs::Entry e{-1, grid, kind.instances, kind.bundles, kind.media, shape.sort_rays, f.status, nullptr};
+    WaveGraphs::Entry e{-1, grid, kind.instances, kind.bundles, kind.media, kind.shapes, shape.sort_rays, f.status,
+                        nullptr};
     if (err == cudaSuccess) err = cudaGraphInstantiate(&e.exec, captured, 0);
     cudaGraphDestroy(captured);
     if (err != cudaSuccess) return err;

@@ -178,7 +178,10 @@ struct WaveKind {
     bool instances = false;   // some scene has instance records (two-level traversal)
     bool bundles = false;     // hero-wavelength jobs (every job of the table has hero_c > 1)
     bool media = false;       // some scene has participating media
+    bool shapes = false;      // some scene has spheres or curves (not only triangles)
 };
+// Whether a scene's world records include spheres or curves.
+inline bool scene_has_shapes(const DevScene& sc) { return (int64_t)sc.n_recs > sc.n_tris + sc.n_inst; }
 
 // Trace one wave on `stream`.  The caller has written, stream-ordered before this call, the
 // job table to w.jobs (slot ranges consecutive from 0) and w.params = {jobs, slots} (slots

@@ -123,6 +123,7 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     ftb::WaveKind kind;
     kind.instances = dev.n_inst > 0;
     kind.media = dev.n_med > 0;
+    kind.shapes = ftb::scene_has_shapes(dev);
     if (e == cudaSuccess && p->n_photons > 0) e = ftb::launch_wave(w, p->max_bounce, kind, f, sms, shape, st);
     if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (out == FTB_OK && info) {

@@ -6,9 +6,11 @@
 // by one caller.  Here many jobs on many resident scenes share the device:
 //
 //   submit (any thread) -> queue -> admission (FIFO; film budget and job slots) -> active
-//   scheduler thread: packs unscheduled photons of the active jobs into waves of W slots
-//                     and launches them alternately on two streams / wave buffers; before a
-//                     buffer is reused, its previous wave is retired (event sync, status)
+//   scheduler thread: packs unscheduled photons of the active jobs of one kernel class into
+//                     a streaming pass of up to 4 W photons (W paths in flight; or a wave of
+//                     W slots when the device's tuning turns slot refill off) and launches the
+//                     passes alternately on two streams / wave buffers; before a buffer is
+//                     reused, its previous pass is retired (event sync, status)
 //   completion thread: copies a finished job's film and tallies out, frees its film
 //
 // Photons are keyed by index (seed_base + i) and the film is int64 fixed point, so how a
@@ -50,6 +52,7 @@ struct Job {
     double power = 0.0;
     int frac = 0;
     int hero = 1;               // wavelengths per photon (1 or a bundle)
+    int klass = 0;              // kernel variant class: bundles, media, spheres/curves, instances
     uint64_t film_bytes = 0;
     int64_t next = 0;           // photons handed to waves so far
     int32_t pending = 0;        // launched waves holding this job's photons, not yet retired
@@ -94,6 +97,7 @@ struct ftb_server {
     uint64_t next_id = 1;
     uint64_t film_bytes = 0;
     std::vector<int> free_slots;
+    int skipped[16] = {};              // passes since each kernel class was last served
     ftb_server_stats st{};
     int inflight = 0;
     Clock::time_point busy_since;
@@ -157,9 +161,14 @@ void admit_locked(ftb_server* s) {
     if (s->admitted_since_launch) cudaEventRecord(s->admit_ev, s->admit_stream);
 }
 
-// Wave table: every job with photons left gets min(left, W / (4 * jobs)) slots, then the
-// remaining capacity goes to the jobs with the least work left.  One entry per job (mu held).
-int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::vector<Job*>& members,
+// The table of the next pass (or wave).  Its jobs share one kernel class -- bundles or not,
+// media, spheres/curves, instances -- so the pass runs the leanest kernel variants that
+// serve them: the class of the job with the least work left, unless another class has
+// waited two passes (then the longest-waiting one).  Within the class every job with
+// photons left gets min(left, cap / (4 * jobs)) photons, then the remaining capacity goes
+// to the jobs with the least work left.  cap = the pass's photon budget (4 W in a
+// streaming pass, W in a wave).  One entry per job (mu held).
+int64_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::vector<Job*>& members,
                            int32_t& max_bounce, ftb::WaveKind& kind) {
     std::vector<Job*> c;
     for (Job* j : s->active)
@@ -168,14 +177,18 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
     std::stable_sort(c.begin(), c.end(), [](const Job* a, const Job* b) {
         return a->req.n_photons - a->next < b->req.n_photons - b->next;
     });
-    // a wave holds one-wavelength jobs or bundles, not both: the class of the job with the
-    // least work left goes first
-    const bool bundles = c[0]->hero > 1;
-    c.erase(std::remove_if(c.begin(), c.end(), [&](const Job* j) { return (j->hero > 1) != bundles; }), c.end());
+    bool present[16] = {};
+    for (Job* j : c) present[j->klass] = true;
+    int klass = c[0]->klass;
+    for (int k = 0; k < 16; ++k)
+        if (present[k] && s->skipped[k] >= 2 && (klass == c[0]->klass || s->skipped[k] > s->skipped[klass])) klass = k;
+    for (int k = 0; k < 16; ++k) s->skipped[k] = (present[k] && k != klass) ? s->skipped[k] + 1 : 0;
+    c.erase(std::remove_if(c.begin(), c.end(), [&](const Job* j) { return j->klass != klass; }), c.end());
     if ((int)c.size() > ftb::kWaveJobs) c.resize(ftb::kWaveJobs);
     std::vector<int64_t> give(c.size(), 0);
-    int64_t cap = s->W;
-    const int64_t fair = std::max<int64_t>(1, s->W / (4 * (int64_t)c.size()));
+    const int64_t budget = s->shape.regenerate ? 4 * (int64_t)s->W : (int64_t)s->W;
+    int64_t cap = budget;
+    const int64_t fair = std::max<int64_t>(1, budget / (4 * (int64_t)c.size()));
     for (size_t i = 0; i < c.size() && cap > 0; ++i) {
         give[i] = std::min<int64_t>({c[i]->req.n_photons - c[i]->next, fair, cap});
         cap -= give[i];
@@ -185,10 +198,9 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
         give[i] += more;
         cap -= more;
     }
-    int32_t slots = 0;
+    int64_t photons = 0;
     max_bounce = 0;
     kind = ftb::WaveKind{};
-    kind.bundles = bundles;
     for (size_t i = 0; i < c.size(); ++i) {
         if (give[i] <= 0) continue;
         Job* j = c[i];
@@ -201,20 +213,23 @@ int32_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
         J.film_scale_inv = std::ldexp(1.0, j->frac) / j->power;
         J.tally_scale_inv = std::ldexp(1.0, 32) / j->power;
         J.photon0 = j->req.seed_base + (uint64_t)j->next;
-        J.slot0 = slots;
+        J.g0 = photons;                // stream index of a streaming pass
+        J.slot0 = (int32_t)photons;    // first slot of a wave
         J.n = (int32_t)give[i];
-            J.max_bounce = j->req.max_bounce;
+        J.max_bounce = j->req.max_bounce;
         J.hero_c = j->hero;
         table.push_back(J);
         members.push_back(j);
         j->next += give[i];
         j->pending++;
-        slots += J.n;
+        photons += give[i];
         max_bounce = std::max(max_bounce, J.max_bounce);
+        kind.bundles |= j->hero > 1;
         kind.instances |= J.sc.n_inst > 0;
         kind.media |= J.sc.n_med > 0;
+        kind.shapes |= ftb::scene_has_shapes(J.sc);
     }
-    return slots;
+    return photons;
 }
 
 // Wait for buffer b's wave, read its status word, release its jobs.
@@ -248,13 +263,14 @@ void scheduler(ftb_server* s) {
     for (;;) {
         table.clear();
         members.clear();
-        int32_t slots = 0, mb = 0;
+        int64_t photons = 0;
+        int32_t mb = 0;
         ftb::WaveKind kind;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             admit_locked(s);
-            slots = build_table_locked(s, table, members, mb, kind);
-            if (slots == 0) {
+            photons = build_table_locked(s, table, members, mb, kind);
+            if (photons == 0) {
                 bool busy = s->ws[0].busy || s->ws[1].busy;
                 if (!busy) {
                     if (s->stopping && s->queue.empty() && s->active.empty()) break;
@@ -264,27 +280,34 @@ void scheduler(ftb_server* s) {
             }
         }
         const int b = k & 1;
-        if (slots == 0) {   // nothing new to launch: retire the older wave in flight
+        if (photons == 0) {   // nothing new to launch: retire the older wave in flight
             retire(s, s->ws[b].busy ? b : 1 - b);
             continue;
         }
         retire(s, b);   // the buffer's previous wave
         WaveSlot& w = s->ws[b];
         std::memcpy(w.table, table.data(), sizeof(ftb::DevJob) * table.size());
+        // streaming pass: {ranges, paths in flight, photons (int64), half-iteration cap (int64)};
+        // wave: {jobs, slots}
+        const bool stream = s->shape.regenerate;
+        const int32_t slots = (int32_t)std::min<int64_t>(photons, s->W);
         int32_t* par = reinterpret_cast<int32_t*>(w.table + ftb::kWaveJobs);
         par[0] = (int32_t)table.size();
         par[1] = slots;
+        reinterpret_cast<int64_t*>(par)[1] = photons;
+        reinterpret_cast<int64_t*>(par)[2] = ftb::stream_half_cap(photons, slots, mb);
         cudaError_t e = cudaMemcpyAsync(w.wave.jobs, w.table, sizeof(ftb::DevJob) * table.size(),
                                         cudaMemcpyHostToDevice, w.stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(w.wave.params, par, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, w.stream);
+            e = cudaMemcpyAsync(w.wave.params, par, 6 * sizeof(int32_t), cudaMemcpyHostToDevice, w.stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_status + 16 * b, 0, 64, w.stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(w.stream, s->admit_ev, 0);
         ftb::Frame f;
         f.stats = nullptr;
         f.status = s->d_status + 16 * b;
         if (e == cudaSuccess)
-            e = ftb::launch_wave(w.wave, mb, kind, f, s->sms, s->shape, w.stream, nullptr, w.graphs);
+            e = stream ? ftb::launch_stream(w.wave, kind, f, s->sms, s->shape, w.stream, nullptr, w.graphs)
+                       : ftb::launch_wave(w.wave, mb, kind, f, s->sms, s->shape, w.stream, nullptr, w.graphs);
         if (e == cudaSuccess) e = cudaEventRecord(w.done, w.stream);
         {
             std::lock_guard<std::mutex> lk(s->mu);
@@ -390,6 +413,7 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
             s->shape.grid_mult = t.grid_mult;
             s->shape.graph = t.use_graphs != 0;
             s->shape.sort_rays = t.sort_rays != 0;
+            s->shape.regenerate = t.regenerate != 0;
         }
     }
     s->t0 = Clock::now();
@@ -459,6 +483,8 @@ ftb_status ftb_server_submit(ftb_server* s, const ftb_request* r, uint64_t* job_
     j->frac = r->frac_bits > 0 ? r->frac_bits : ftb::default_frac_bits(r->n_photons);
     // bundles as the reference gates them: clamped to kHeroMax, none in scenes with media
     j->hero = (r->hero_c <= 1 || j->sc.n_med > 0) ? 1 : (r->hero_c > ftb::kHeroMax ? ftb::kHeroMax : r->hero_c);
+    j->klass = (j->hero > 1 ? 1 : 0) | (j->sc.n_med > 0 ? 2 : 0) | (ftb::scene_has_shapes(j->sc) ? 4 : 0) |
+               (j->sc.n_inst > 0 ? 8 : 0);
     if (j->hero > s->hero_max) {
         delete j;
         return fail(FTB_ERR_TOO_LARGE, "bundle larger than the server's hero_max");

@@ -448,12 +448,16 @@ ftb_status ftb_autotune(ftb_scene* scene, const ftb_camera* cam, int64_t n_photo
  * A server owns two wave buffers and streams on one device, a scheduler thread and a
  * completion thread.  Jobs (a resident scene, a camera, a photon range) are submitted from
  * any thread and admitted in arrival order while their film fits the film budget and a
- * job slot is free.  The scheduler keeps packing the unscheduled photons of all admitted
- * jobs into waves -- every job at least a fair share of each wave, the rest shortest
- * remaining work first -- so a job that arrives while others are on the GPU joins the
- * next wave and small jobs are not queued behind large ones.  A job's film and energy are
- * exactly those of ftb_render_forward with the same arguments, whatever shares its waves
- * (photons are keyed by index and the film is fixed point).  The scenes referenced by
+ * job slot is free.  The scheduler keeps packing the unscheduled photons of the admitted
+ * jobs into passes of up to 4 x wave_slots photons (wave_slots paths in flight, freed paths
+ * refilled at once; a wave of wave_slots photons when the device's tuning turns refill off)
+ * -- the jobs of one kernel class per pass (bundles or not, media, spheres/curves,
+ * instances: the class of the job with the least work left, a class that waited two passes
+ * first), every job of the class at least a fair share, the rest shortest remaining work
+ * first -- so a job that arrives while others are on the GPU joins the next pass and small
+ * jobs are not queued behind large ones.  A job's film and energy are exactly those of
+ * ftb_render_forward with the same arguments, whatever shares its passes (photons are
+ * keyed by index and the film is fixed point).  The scenes referenced by
  * submitted jobs must stay alive until those jobs are done. */
 typedef struct ftb_server ftb_server;
 
@@ -462,7 +466,7 @@ typedef struct ftb_server_config {
     int32_t max_active;        /* jobs admitted at once, 1..256 (0: 64) */
     uint64_t film_budget;      /* bytes of device films admitted at once (0: a quarter of the
                                   free device memory) */
-    int32_t wave_slots;        /* photon slots per wave, 1..2^22 (0: 2^22) */
+    int32_t wave_slots;        /* paths in flight per pass, 1..2^22 (0: 2^22) */
     int32_t hero_max;          /* largest hero_c a request may carry, 1..8 (0: 4); the wave
                                   buffers grow by ~260 B per slot at 4 */
 } ftb_server_config;

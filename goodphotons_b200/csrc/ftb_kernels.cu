@@ -37,6 +37,21 @@
 
 namespace cg = cooperative_groups;
 
+// Resident blocks per SM each kernel is compiled for (register budget 65536 / (128 x minB)),
+// chosen by measurement on B200: latency hiding beats the spills the smaller budget costs.
+#ifndef FTB_EMIT_MINB
+#define FTB_EMIT_MINB 8
+#endif
+#ifndef FTB_TRAV_MINB
+#define FTB_TRAV_MINB 8
+#endif
+#ifndef FTB_SHADE_MINB
+#define FTB_SHADE_MINB 8
+#endif
+#ifndef FTB_SHADE_MEDIA_MINB   // shading with participating media: more registers pay off
+#define FTB_SHADE_MEDIA_MINB 4
+#endif
+
 namespace ftb {
 
 #define PI_D 3.141592653589793
@@ -1219,7 +1234,7 @@ __device__ __forceinline__ double sample_at(const DevEmit& em, double u, double&
 
 // ------------------------------------------------------------------ kernels ------------
 template <bool MEDIA, bool STREAM>
-__global__ void __launch_bounds__(128) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
+__global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
                                               int32_t* out_count) {
     const int32_t n_jobs = w.params[0];
     const bool multi = n_jobs > 1;
@@ -1279,14 +1294,6 @@ __device__ void block_add1(unsigned long long* dst, unsigned long long a) {
     if ((threadIdx.x & 31) == 0 && a) atomicAdd(dst, a);
 }
 
-// Resident blocks per SM the traversal and shading kernels are compiled for (register
-// budget 65536 / (128 x minB)); chosen by measurement on B200.
-#ifndef FTB_TRAV_MINB
-#define FTB_TRAV_MINB 8
-#endif
-#ifndef FTB_SHADE_MINB
-#define FTB_SHADE_MINB 4
-#endif
 
 template <bool COUNT, bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const DevJob* __restrict__ jobs,
@@ -1439,7 +1446,7 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
 template <bool MEDIA, bool INST, bool SHAPES>
-__global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
+__global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
                                                                Frame f, PathState in, const int32_t* in_count,
                                                                PathState out, int32_t* out_count) {
     const int32_t n_jobs = w.params[0];
@@ -1714,7 +1721,7 @@ __device__ __forceinline__ double max_of(const double* a, int n) {   // hero::ma
 }
 
 template <bool STREAM>
-__global__ void __launch_bounds__(128) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
+__global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
                                                    int32_t* out_count) {
     const int32_t n_jobs = w.params[0];
     const bool multi = n_jobs > 1;

@@ -932,12 +932,22 @@ __device__ __forceinline__ int agg_inc(int32_t* ctr) {
     return g.shfl(base, 0) + (int)g.thread_rank();
 }
 
+// A queue of paths is two-ended: paths outside every dielectric grow from entry 0 up
+// (count q[0]), paths inside one grow from entry W-1 down (count q[1]), so each end holds
+// paths of similar traversal cost (inside a closed mesh a ray crosses it; outside most rays
+// meet a wall after a few nodes) and warps diverge less.  Queue position p < q[0] is entry
+// p; position q[0] + k is entry W-1-k.
+__device__ __forceinline__ int queue_len(const int32_t* q) { return q[0] + q[1]; }
+__device__ __forceinline__ int queue_entry(const Wave& w, int front, int p) {
+    return p < front ? p : w.W - 1 - (p - front);
+}
+
 // A one-wavelength connection: the film increments cieX/Y/Z(lambda) * contribution in the
 // order Film::add forms them (scene_film.h:12), from the matching functions evaluated once
 // per path at emission.
 __device__ __forceinline__ void push_shadow(const Wave& w, const Frame& f, int job, int view, D3 o, D3 d,
                                             double tmax, double val, const double* cie, int pix) {
-    int i = agg_inc(&w.counts[2]);
+    int i = agg_inc(&w.counts[kShadowCount]);
     if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
     w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
     w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
@@ -1151,8 +1161,8 @@ __device__ __forceinline__ PhotonSource photon_source(const Wave& w, const int32
     if (STREAM) {
         const int64_t total = reinterpret_cast<const int64_t*>(w.params)[1];
         p.next = w.ctl->next;
-        p.have = *out_count;   // the refill appends through ctl->taken, so this stays put
-        const int64_t room = (int64_t)w.params[1] - p.have, left = total - p.next;
+        p.have = out_count[0];   // the refill appends through ctl->taken, so this stays put
+        const int64_t room = (int64_t)w.params[1] - p.have - out_count[1], left = total - p.next;
         p.n = left < room ? left : room;
     } else {
         p.n = w.params[1];
@@ -1300,11 +1310,11 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const Dev
                                                               PathState in, const int32_t* qcount,
                                                               const int32_t* __restrict__ order, Frame f) {
     const int32_t n_jobs = w.params[0];
-    int nq = *qcount;
+    const int front = qcount[0], nq = queue_len(qcount);
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
-        const int i = order ? order[q] : q;
+        const int i = order ? order[q] : queue_entry(w, front, q);
         const DevScene& sc = jobs[n_jobs > 1 ? in.job[i] : 0].sc;
         RayCtx R = make_ray(mk(in.ox[i], in.oy[i], in.oz[i]), mk(in.dx[i], in.dy[i], in.dz[i]));
         double t;
@@ -1342,13 +1352,13 @@ __device__ __forceinline__ uint32_t direction_key(D3 d) {
     return u | (v << 1);
 }
 
-// Traversal order of a queue, each kSortChunk-entry piece bucketed by direction key (one
-// block per piece, counting sort in shared memory): order[q] is the path the closest-hit
-// kernel's q-th lane takes, so a warp's 32 lanes head the same way.
+// Traversal order of a queue, each kSortChunk-position piece bucketed by direction key (one
+// block per piece, counting sort in shared memory): order[q] is the entry of the path the
+// closest-hit kernel's q-th lane takes, so a warp's 32 lanes head the same way.
 __global__ void __launch_bounds__(128) k_sort_queue(Wave w, PathState in, const int32_t* qcount,
                                                     int32_t* order) {
     __shared__ int32_t hist[256];
-    const int nq = *qcount;
+    const int front = qcount[0], nq = queue_len(qcount);
     constexpr int kPer = kSortChunk / 128;
     for (int base = blockIdx.x * kSortChunk; base < nq; base += gridDim.x * kSortChunk) {
         for (int t = threadIdx.x; t < 256; t += 128) hist[t] = 0;
@@ -1356,8 +1366,9 @@ __global__ void __launch_bounds__(128) k_sort_queue(Wave w, PathState in, const 
         int pos[kPer], key[kPer], off[kPer];
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
-            const int i = base + r * 128 + threadIdx.x;
-            pos[r] = i < nq ? i : -1;
+            const int p = base + r * 128 + threadIdx.x;
+            const int i = p < nq ? queue_entry(w, front, p) : 0;
+            pos[r] = p < nq ? i : -1;
             key[r] = pos[r] >= 0 ? (int)direction_key(mk(in.dx[i], in.dy[i], in.dz[i])) : 255;
             off[r] = pos[r] >= 0 ? atomicAdd(&hist[key[r]], 1) : 0;
         }
@@ -1453,8 +1464,9 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
     const bool multi = n_jobs > 1;
     TallyAcc acc;
     tally_init(acc, multi, n_jobs);
-    int nq = *in_count;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+    const int front = in_count[0], nq = queue_len(in_count);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const int i = queue_entry(w, front, q);
         const int j = multi ? in.job[i] : 0;
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
@@ -1612,7 +1624,7 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
             continue;
         }
         load_cie();
-        const int o = agg_inc(out_count);
+        const int o = stk.n > 0 ? w.W - 1 - agg_inc(out_count + 1) : agg_inc(out_count);
         out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
         out.ox[o] = no.x; out.oy[o] = no.y; out.oz[o] = no.z;
         out.dx[o] = nd.x; out.dy[o] = nd.y; out.dz[o] = nd.z;
@@ -1632,7 +1644,7 @@ template <bool COUNT, bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const DevJob* __restrict__ jobs,
                                                               Frame f) {
     const int32_t n_jobs = w.params[0];
-    int n = w.counts[2];
+    int n = w.counts[kShadowCount];
     if (n > w.S) n = w.S;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
@@ -1669,7 +1681,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
 
 __device__ __forceinline__ void push_shadow_hero(const Wave& w, const Frame& f, int job, int view, D3 o, D3 d,
                                                  double tmax, int nup, const double* lam, const double* val, int pix) {
-    int i = agg_inc(&w.counts[2]);
+    int i = agg_inc(&w.counts[kShadowCount]);
     if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
     w.sox[i] = o.x; w.soy[i] = o.y; w.soz[i] = o.z;
     w.sdx[i] = d.x; w.sdy[i] = d.y; w.sdz[i] = d.z;
@@ -1783,8 +1795,9 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
     const bool multi = n_jobs > 1;
     TallyAcc acc;
     tally_init(acc, multi, n_jobs);
-    int nq = *in_count;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nq; p += gridDim.x * blockDim.x) {
+    const int front = in_count[0], nq = queue_len(in_count);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const int p = queue_entry(w, front, q);
         const int j = multi ? in.job[p] : 0;
         const DevJob& J = jobs[j];
         const DevScene& sc = J.sc;
@@ -1954,7 +1967,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
             log_finish(w, in, p, 2, beta[0]);
             continue;
         }
-        const int o = agg_inc(out_count);
+        const int o = stk.n > 0 ? w.W - 1 - agg_inc(out_count + 1) : agg_inc(out_count);
         out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
         out.ox[o] = no.x; out.oy[o] = no.y; out.oz[o] = no.z;
         out.dx[o] = nd.x; out.dy[o] = nd.y; out.dz[o] = nd.z;
@@ -1977,7 +1990,7 @@ template <bool COUNT, bool INST, bool SHAPES>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, const DevJob* __restrict__ jobs,
                                                                    Frame f) {
     const int32_t n_jobs = w.params[0];
-    int n = w.counts[2];
+    int n = w.counts[kShadowCount];
     if (n > w.S) n = w.S;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
@@ -2092,15 +2105,16 @@ __global__ void k_stream_advance(Wave w, Frame f, int32_t* consumed, int32_t* ne
     StreamCtl& c = *w.ctl;
     const int64_t total = reinterpret_cast<const int64_t*>(w.params)[1];
     const int64_t cap = reinterpret_cast<const int64_t*>(w.params)[2];
-    const int32_t have = *next_q;   // survivors; the refill filled the room above them
-    const int64_t room = (int64_t)w.params[1] - have, left = total - c.next;
+    const int32_t have = next_q[0];   // survivors at the front; the refill filled the room above them
+    const int64_t room = (int64_t)w.params[1] - have - next_q[1], left = total - c.next;
     c.next += left < room ? left : room;
-    *next_q = have + c.taken;
+    next_q[0] = have + c.taken;
     c.taken = 0;
     c.half += 1;
-    *consumed = 0;
-    w.counts[2] = 0;
-    int32_t more = (*next_q > 0 || c.next < total) ? 1 : 0;
+    consumed[0] = 0;
+    consumed[1] = 0;
+    w.counts[kShadowCount] = 0;
+    int32_t more = (queue_len(next_q) > 0 || c.next < total) ? 1 : 0;
     if (more && c.half >= cap) {
         atomicOr(f.status, ST_LOOP_CAP);
         more = 0;
@@ -2213,16 +2227,16 @@ void issue_wave(Issue& I, int32_t max_bounce) {
     Wave& w = I.w;
     cudaStream_t st = I.st;
     cudaMemsetAsync(w.counts, 0, 64, st);
-    I.emit(false, w.ps[0], &w.counts[0]);
+    I.emit(false, w.ps[0], queue_counts(w, 0));
     I.shadow();
-    cudaMemsetAsync(&w.counts[2], 0, 4, st);
+    cudaMemsetAsync(&w.counts[kShadowCount], 0, 4, st);
     for (int b = 0; b < max_bounce; ++b) {
         const int a = b & 1;
-        I.extend(w.ps[a], &w.counts[a]);
-        cudaMemsetAsync(&w.counts[a ^ 1], 0, 4, st);
-        I.shade(w.ps[a], &w.counts[a], w.ps[a ^ 1], &w.counts[a ^ 1]);
+        I.extend(w.ps[a], queue_counts(w, a));
+        cudaMemsetAsync(queue_counts(w, a ^ 1), 0, 8, st);
+        I.shade(w.ps[a], queue_counts(w, a), w.ps[a ^ 1], queue_counts(w, a ^ 1));
         I.shadow();
-        cudaMemsetAsync(&w.counts[2], 0, 4, st);
+        cudaMemsetAsync(&w.counts[kShadowCount], 0, 4, st);
     }
 }
 
@@ -2232,17 +2246,17 @@ void issue_wave(Issue& I, int32_t max_bounce) {
 void stream_prologue(Issue& I) {
     Wave& w = I.w;
     k_stream_init<<<1, 32, 0, I.st>>>(w);
-    I.emit(true, w.ps[0], &w.counts[0]);
+    I.emit(true, w.ps[0], queue_counts(w, 0));
     I.shadow();
-    k_stream_advance<<<1, 32, 0, I.st>>>(w, I.f, &w.counts[1], &w.counts[0], 0, 0);
+    k_stream_advance<<<1, 32, 0, I.st>>>(w, I.f, queue_counts(w, 1), queue_counts(w, 0), 0, 0);
 }
 void stream_half(Issue& I, int a, cudaGraphConditionalHandle loop, int32_t set_loop) {
     Wave& w = I.w;
-    I.extend(w.ps[a], &w.counts[a]);
-    I.shade(w.ps[a], &w.counts[a], w.ps[a ^ 1], &w.counts[a ^ 1]);
-    I.emit(true, w.ps[a ^ 1], &w.counts[a ^ 1]);
+    I.extend(w.ps[a], queue_counts(w, a));
+    I.shade(w.ps[a], queue_counts(w, a), w.ps[a ^ 1], queue_counts(w, a ^ 1));
+    I.emit(true, w.ps[a ^ 1], queue_counts(w, a ^ 1));
     I.shadow();
-    k_stream_advance<<<1, 32, 0, I.st>>>(w, I.f, &w.counts[a], &w.counts[a ^ 1], loop, set_loop);
+    k_stream_advance<<<1, 32, 0, I.st>>>(w, I.f, queue_counts(w, a), queue_counts(w, a ^ 1), loop, set_loop);
 }
 }  // namespace
 

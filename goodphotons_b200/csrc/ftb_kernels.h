@@ -88,7 +88,7 @@ struct Wave {
     int32_t* hit_rec;          // world record of the closest hit, or -1
     int32_t* hit_sub;          // BLAS record when hit_rec is an instance
     int32_t* perm;             // optional traversal order of a queue (bucketed by direction)
-    int32_t* counts;           // [0] paths in ps[0], [1] in ps[1], [2] shadow records
+    int32_t* counts;           // [2a], [2a+1]: the two ends of the queue in ps[a]; [4] shadow records
     int32_t* sjob;             // job of each shadow record
     DevJob* jobs;              // device job table, kWaveJobs entries
     int32_t* params;           // [0] jobs in the table, [1] paths in flight at most (written with
@@ -115,6 +115,10 @@ struct Frame {
                                // [6] closest-hit / [7] any-hit exact (fp64) record tests
     int32_t* status;
 };
+
+// Queue counts of path buffer a (front and back end) and the shadow-record count in Wave::counts.
+constexpr int kShadowCount = 4;
+inline int32_t* queue_counts(const Wave& w, int a) { return w.counts + 2 * a; }
 
 // Shadow records per path: a path queues at most 2 connections per view per bounce, and in
 // a streaming pass a refilled path's emission adds one more in the same half-iteration.

@@ -1427,7 +1427,7 @@ ftb_status ftb_get_tuning(int32_t device, ftb_tuning* out) {
 
 ftb_status ftb_set_tuning(int32_t device, const ftb_tuning* t) {
     if (!t || device < 0 || device >= 256) return fail(FTB_ERR_INVALID, "bad arguments");
-    if (t->wave_slots < 1 || t->wave_slots > (1 << 22) || t->grid_mult < 1 || t->grid_mult > 64)
+    if (t->wave_slots < 1 || t->wave_slots > (1 << 24) || t->grid_mult < 1 || t->grid_mult > 64)
         return fail(FTB_ERR_INVALID, "tuning out of range");
     std::shared_ptr<Engine> e;
     {
@@ -1481,7 +1481,7 @@ ftb_status ftb_autotune(ftb_scene* s, const ftb_camera* cam, int64_t n, int32_t 
         // one knob at a time from the current setting: slot refill, grid, wave size, graphs,
         // ray reordering
         const int grids[] = {4, 8, 16, 32};
-        const int waves[] = {1 << 20, 1 << 21, 1 << 22};
+        const int waves[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24};
         for (int pass = 0; pass < 5 && st == FTB_OK; ++pass) {
             std::vector<ftb_tuning> cand;
             if (pass == 0) for (int u = 0; u < 2; ++u) { ftb_tuning t = best; t.regenerate = u; cand.push_back(t); }

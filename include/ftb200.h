@@ -424,7 +424,7 @@ ftb_status ftb_scene_profile(ftb_scene* scene, ftb_kernel_profile* out, int32_t 
  * Renders on the device use the setting current when they start; results do not depend on
  * it (photons are keyed by index, films are fixed point). */
 typedef struct ftb_tuning {
-    int32_t wave_slots;   /* 1 .. 2^22 */
+    int32_t wave_slots;   /* paths in flight per wave buffer, 1 .. 2^24 */
     int32_t grid_mult;    /* 1 .. 64 */
     int32_t use_graphs;   /* 0 / 1 */
     int32_t sort_rays;    /* 0 / 1: reorder closest-hit rays by direction within each block */

@@ -938,6 +938,19 @@ __device__ __forceinline__ int agg_inc(int32_t* ctr) {
 // meet a wall after a few nodes) and warps diverge less.  Queue position p < q[0] is entry
 // p; position q[0] + k is entry W-1-k.
 __device__ __forceinline__ int queue_len(const int32_t* q) { return q[0] + q[1]; }
+
+// Dynamic work distribution over a queue: a warp takes the next 32 positions from a
+// per-launch counter in Wave::counts whenever it is done, so warps that drew short paths
+// take more and a launch ends with fewer idle SMs than a fixed grid-stride split.  Every
+// lane of the warp calls warp_fetch; the loop ends for the whole warp at once.
+__device__ __forceinline__ int warp_fetch(int32_t* ctr) {
+    int base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(ctr, 32);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+#define FTB_FOR_WARP_CHUNKS(var, n, ctr)                                                      \
+    for (int var##_base = warp_fetch(ctr); var##_base < (n); var##_base = warp_fetch(ctr))   \
+        if (const int var = var##_base + (int)(threadIdx.x & 31); var < (n))
 __device__ __forceinline__ int queue_entry(const Wave& w, int front, int p) {
     return p < front ? p : w.W - 1 - (p - front);
 }
@@ -1313,7 +1326,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_extend(Wave w, const Dev
     const int front = qcount[0], nq = queue_len(qcount);
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    FTB_FOR_WARP_CHUNKS(q, nq, &w.counts[kFetchExtend]) {
         const int i = order ? order[q] : queue_entry(w, front, q);
         const DevScene& sc = jobs[n_jobs > 1 ? in.job[i] : 0].sc;
         RayCtx R = make_ray(mk(in.ox[i], in.oy[i], in.oz[i]), mk(in.dx[i], in.dy[i], in.dz[i]));
@@ -1465,7 +1478,7 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
     TallyAcc acc;
     tally_init(acc, multi, n_jobs);
     const int front = in_count[0], nq = queue_len(in_count);
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    FTB_FOR_WARP_CHUNKS(q, nq, &w.counts[kFetchShade]) {
         const int i = queue_entry(w, front, q);
         const int j = multi ? in.job[i] : 0;
         const DevJob& J = jobs[j];
@@ -1648,7 +1661,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
     if (n > w.S) n = w.S;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    FTB_FOR_WARP_CHUNKS(i, n, &w.counts[kFetchShadow]) {
         const DevJob& J = jobs[n_jobs > 1 ? w.sjob[i] : 0];
         const DevScene& sc = J.sc;
         D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
@@ -1796,7 +1809,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
     TallyAcc acc;
     tally_init(acc, multi, n_jobs);
     const int front = in_count[0], nq = queue_len(in_count);
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    FTB_FOR_WARP_CHUNKS(q, nq, &w.counts[kFetchShade]) {
         const int p = queue_entry(w, front, q);
         const int j = multi ? in.job[p] : 0;
         const DevJob& J = jobs[j];
@@ -1994,7 +2007,7 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, cons
     if (n > w.S) n = w.S;
     TravCount cnt{0, 0, 0};
     unsigned long long rays = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    FTB_FOR_WARP_CHUNKS(i, n, &w.counts[kFetchShadow]) {
         const DevJob& J = jobs[n_jobs > 1 ? w.sjob[i] : 0];
         const DevScene& sc = J.sc;
         D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
@@ -2114,6 +2127,9 @@ __global__ void k_stream_advance(Wave w, Frame f, int32_t* consumed, int32_t* ne
     consumed[0] = 0;
     consumed[1] = 0;
     w.counts[kShadowCount] = 0;
+    w.counts[kFetchExtend] = 0;
+    w.counts[kFetchShade] = 0;
+    w.counts[kFetchShadow] = 0;
     int32_t more = (queue_len(next_q) > 0 || c.next < total) ? 1 : 0;
     if (more && c.half >= cap) {
         atomicOr(f.status, ST_LOOP_CAP);
@@ -2229,14 +2245,14 @@ void issue_wave(Issue& I, int32_t max_bounce) {
     cudaMemsetAsync(w.counts, 0, 64, st);
     I.emit(false, w.ps[0], queue_counts(w, 0));
     I.shadow();
-    cudaMemsetAsync(&w.counts[kShadowCount], 0, 4, st);
+    cudaMemsetAsync(&w.counts[kShadowCount], 0, 4 * kCountWords, st);
     for (int b = 0; b < max_bounce; ++b) {
         const int a = b & 1;
         I.extend(w.ps[a], queue_counts(w, a));
         cudaMemsetAsync(queue_counts(w, a ^ 1), 0, 8, st);
         I.shade(w.ps[a], queue_counts(w, a), w.ps[a ^ 1], queue_counts(w, a ^ 1));
         I.shadow();
-        cudaMemsetAsync(&w.counts[kShadowCount], 0, 4, st);
+        cudaMemsetAsync(&w.counts[kShadowCount], 0, 4 * kCountWords, st);
     }
 }
 

@@ -88,7 +88,8 @@ struct Wave {
     int32_t* hit_rec;          // world record of the closest hit, or -1
     int32_t* hit_sub;          // BLAS record when hit_rec is an instance
     int32_t* perm;             // optional traversal order of a queue (bucketed by direction)
-    int32_t* counts;           // [2a], [2a+1]: the two ends of the queue in ps[a]; [4] shadow records
+    int32_t* counts;           // [2a], [2a+1]: the two ends of the queue in ps[a]; [4] shadow records;
+                               // [5..7] per-launch work counters
     int32_t* sjob;             // job of each shadow record
     DevJob* jobs;              // device job table, kWaveJobs entries
     int32_t* params;           // [0] jobs in the table, [1] paths in flight at most (written with
@@ -116,8 +117,12 @@ struct Frame {
     int32_t* status;
 };
 
-// Queue counts of path buffer a (front and back end) and the shadow-record count in Wave::counts.
+// Queue counts of path buffer a (front and back end), the shadow-record count and the
+// per-launch work counters of the closest-hit, shading and shadow kernels in Wave::counts
+// ([4] .. [4 + kCountWords - 1] are cleared together after every connection launch).
 constexpr int kShadowCount = 4;
+constexpr int kFetchExtend = 5, kFetchShade = 6, kFetchShadow = 7;
+constexpr int kCountWords = 4;
 inline int32_t* queue_counts(const Wave& w, int a) { return w.counts + 2 * a; }
 
 // Shadow records per path: a path queues at most 2 connections per view per bounce, and in

@@ -387,6 +387,13 @@ def run_serve(args):
             cams[res] = scenes.default_camera(L, res)
         return cams[res]
 
+    # deployment step: autotune the device's launch shape on a mid-size glass scene of the
+    # mix (the server and the one-at-a-time renders below both use it)
+    glass = sorted(k for k in keys if k[0] == "glass") or keys
+    t = time.perf_counter()
+    tuning = L.autotune(cache[glass[len(glass) // 2]], cam(1024), 1 << 26, 16)
+    tune_s = time.perf_counter() - t
+
     def serve(jobs, paced):
         srv = lib.Server(device=local, max_active=args.max_active, lib=L)
         ids, films = [None] * len(jobs), [None] * len(jobs)
@@ -455,7 +462,11 @@ def run_serve(args):
                    "mix": "scene family uniform over cornell / glass / fog_strands; mesh 1k-2M tris log-uniform "
                           "(glass snapped to icosphere levels, fog to strand counts); resolution 128^2-1024^2 and "
                           f"photons 2^20-2^{budget_hi:g} log-uniform", "resident_scenes": len(cache),
-                   "scene_bake_ms_total": round(sum(bake_ms.values()), 1), "max_active": args.max_active},
+                   "scene_bake_ms_total": round(sum(bake_ms.values()), 1), "max_active": args.max_active,
+                   "tuning": {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
+                              "graph_replay": bool(tuning.use_graphs), "sort_rays": bool(tuning.sort_rays),
+                              "regenerate": bool(tuning.regenerate), "autotune_s": round(tune_s, 2),
+                              "on": f"{glass[len(glass) // 2][0]} size {glass[len(glass) // 2][1]}"}},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "mean": float(lat.mean()), "max": float(lat.max())},
         "utilization": round(run["stats"].busy_s / run["makespan"], 4),

@@ -399,7 +399,7 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return fail(FTB_ERR_NO_DEVICE, "no CUDA device"); }
     if (cfg->device < 0 || cfg->device >= ndev) return fail(FTB_ERR_INVALID, "device index out of range");
     if (cfg->max_active < 0 || cfg->max_active > ftb::kWaveJobs) return fail(FTB_ERR_INVALID, "max_active out of range");
-    if (cfg->wave_slots < 0 || cfg->wave_slots > (1 << 22)) return fail(FTB_ERR_INVALID, "wave_slots out of range");
+    if (cfg->wave_slots < 0 || cfg->wave_slots > (1 << 24)) return fail(FTB_ERR_INVALID, "wave_slots out of range");
     int prev = 0;
     cudaGetDevice(&prev);
     auto s = new ftb_server();
@@ -410,6 +410,7 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
     {   // launch shape: the device's current tuning (ftb_set_tuning / ftb_autotune)
         ftb_tuning t;
         if (ftb_get_tuning(cfg->device, &t) == FTB_OK) {
+            if (!cfg->wave_slots) s->W = t.wave_slots;
             s->shape.grid_mult = t.grid_mult;
             s->shape.graph = t.use_graphs != 0;
             s->shape.sort_rays = t.sort_rays != 0;

@@ -466,7 +466,8 @@ typedef struct ftb_server_config {
     int32_t max_active;        /* jobs admitted at once, 1..256 (0: 64) */
     uint64_t film_budget;      /* bytes of device films admitted at once (0: a quarter of the
                                   free device memory) */
-    int32_t wave_slots;        /* paths in flight per pass, 1..2^22 (0: 2^22) */
+    int32_t wave_slots;        /* paths in flight per pass, 1..2^24 (0: the device's tuning,
+                                  ftb_get_tuning) */
     int32_t hero_max;          /* largest hero_c a request may carry, 1..8 (0: 4); the wave
                                   buffers grow by ~260 B per slot at 4 */
 } ftb_server_config;

@@ -1,22 +1,29 @@
 // ftb_kernels.cu -- sm_100a wavefront kernels of the forward pinhole light tracer.
 //
-// One wave of W photon paths is traced with four kernels:
+// Up to W photon paths are in flight at once, traced with four kernels:
 //   k_emit    seed the per-photon PCG32 stream, pick emitter / point / direction /
 //             wavelength, book `emitted`, queue the emitter's direct camera connection
 //             (reference: Renderer::tracePhoton emission, render.h:1827-1984)
-//   k_extend  closest hit of every active path over the 8-wide BVH (Scene::closestHit,
+//   k_extend  closest hit of every queued path over the 8-wide BVH (Scene::closestHit,
 //             scene.h:2194-2242)
 //   k_shade   media, interior absorption and the material interaction of one bounce;
-//             queues camera connections and compacts the surviving paths into the next
-//             active list (render.h:2013-2238)
+//             queues camera connections and copies the surviving paths into the other
+//             path buffer (render.h:2013-2238)
 //   k_shadow  any-hit test of the queued connections (Scene::occluded, scene.h:2249) and
 //             the splat into the 64-bit fixed-point film (Film::add, scene_film.h:12)
 //
+// Path state is compacted (a queue of n paths is entries 0..n-1 of structure-of-arrays
+// buffers, no index lists) and two-ended (paths inside a dielectric grow from the top
+// entry down, so each end holds paths of similar traversal cost).  The queue kernels hand
+// out work to warps 32 entries at a time from a per-launch counter.  A streaming pass
+// (launch_stream) refills the room freed by finished paths with the next photons every
+// half-iteration and runs as one CUDA graph with a device-driven while loop; a wave
+// (launch_wave) traces W photons to their last bounce.
+//
 // Variants: k_emit_hero / k_shade_hero / k_shadow_hero trace hero-wavelength bundles (one
 // path carries up to kHeroMax wavelengths), and the kernels are templated on whether the
-// wave's scenes have instances or participating media, so a wave launches only the code
-// its scenes need.  k_sort_queue optionally buckets a closest-hit queue by ray direction.
-// A wave's launch sequence is captured once as a CUDA graph and replayed (launch_wave).
+// scenes have instances, participating media or spheres/curves, so a launch runs only the
+// code its scenes need.  k_sort_queue optionally orders a closest-hit queue by direction.
 //
 // Numerics.  Everything that decides a path -- triangle/sphere/curve tests, hit points,
 // normals, BSDF sampling, Russian roulette, the camera projection -- is computed in fp64

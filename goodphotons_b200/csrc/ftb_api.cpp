@@ -1232,7 +1232,12 @@ ftb_status ftb_scene_footprint(const ftb_scene* s, int32_t rx, int32_t ry, ftb_f
     if (!s || !out || rx <= 0 || ry <= 0) return fail(FTB_ERR_INVALID, "bad arguments");
     out->scene_bytes = s->scene_bytes;
     out->film_bytes = (uint64_t)rx * (uint64_t)ry * 4 * sizeof(int64_t);
-    out->wave_bytes = 2 * (uint64_t)ftb::wave_bytes(1 << 22, false);
+    int32_t W = 1 << 22;
+    {
+        std::lock_guard<std::mutex> lk(s->eng->mu);
+        W = s->eng->wave_cap;   // the device's current tuning
+    }
+    out->wave_bytes = 2 * (uint64_t)ftb::wave_bytes(W, false);
     out->total_bytes = out->scene_bytes + out->film_bytes + out->wave_bytes;
     return FTB_OK;
 }

@@ -246,7 +246,8 @@ typedef struct ftb_session ftb_session;   /* resident film(s) + scene */
 typedef struct ftb_footprint {
     uint64_t scene_bytes;     /* BVH + primitive records + tables */
     uint64_t film_bytes;      /* per camera film */
-    uint64_t wave_bytes;      /* path state + queues for one in-flight wave */
+    uint64_t wave_bytes;      /* path state, queues and connection records of the device's
+                                 two wave buffers at its current tuning (wave_slots) */
     uint64_t total_bytes;
 } ftb_footprint;
 

@@ -71,7 +71,8 @@ def test_tuning_and_graph_replay_do_not_change_results(gpu):
         for slots, grid, graphs, srt, regen in [(1 << 22, 16, 0, 0, 0), (1 << 20, 4, 1, 1, 0),
                                                 (1 << 19, 32, 1, 0, 1), (3 << 18, 8, 0, 1, 1),
                                                 (1 << 22, 16, 1, 1, 1), (1 << 22, 16, 1, 0, 0),
-                                                (40_000, 16, 1, 0, 1), (1_000, 4, 0, 0, 1)]:
+                                                (40_000, 16, 1, 0, 1), (1_000, 4, 0, 0, 1),
+                                                (1 << 23, 8, 1, 1, 1)]:
             L.set_tuning(0, wave_slots=slots, grid_mult=grid, use_graphs=graphs, sort_rays=srt, regenerate=regen)
             for _ in range(2):   # the second render replays a captured graph
                 film, _, en = sc.render(cam, 1_500_000, seed_base=42, max_bounce=16, frac_bits=30)
@@ -80,7 +81,7 @@ def test_tuning_and_graph_replay_do_not_change_results(gpu):
                 np.testing.assert_array_equal(film, ref[0], err_msg=f"{slots} {grid} {graphs} {srt} {regen}")
                 assert list(en.fx) == ref[1]
         t = L.autotune(sc, cam, 1 << 21, 16)
-        assert 1 <= t.wave_slots <= 1 << 22 and 1 <= t.grid_mult <= 64 and t.use_graphs in (0, 1)
+        assert 1 <= t.wave_slots <= 1 << 24 and 1 <= t.grid_mult <= 64 and t.use_graphs in (0, 1)
         assert t.sort_rays in (0, 1) and t.regenerate in (0, 1)
         film, _, _ = sc.render(cam, 1_500_000, seed_base=42, max_bounce=16, frac_bits=30)
         np.testing.assert_array_equal(film, ref[0])

@@ -101,3 +101,26 @@ def test_oversized_film_and_timeouts(gpu, resident):
     with pytest.raises(lib.FtbError):
         srv.wait(jid)   # already collected
     srv.close()
+
+
+def test_bundles_and_classes_in_the_mix(gpu, resident):
+    """Hero bundles (C = 4, 3) among one-wavelength jobs of every kernel class: passes hold
+    one class at a time, and each job still equals its solo render."""
+    specs = [("glass", 32, 400_000, 4), ("cornell", 24, 300_000, 1), ("fog", 16, 50_000, 1),
+             ("cornell", 40, 900_000, 3), ("instances", 24, 200_000, 4), ("materials", 32, 250_000, 1)]
+    srv = lib.Server(device=0, lib=gpu, wave_slots=1 << 19)
+    films, ids = [], []
+    for k, (name, res, n, hero) in enumerate(specs):
+        films.append(np.full((res, res, 4), -1, dtype=np.int64))
+        mb = {"cornell": 8, "fog": 32}.get(name, 16)
+        ids.append(srv.submit(resident[name], scenes.default_camera(gpu, res), n, seed_base=777 * k,
+                              max_bounce=mb, host_film=films[k], hero_c=hero))
+    results = [srv.wait(i) for i in ids]
+    srv.close()
+    for k, ((name, res, n, hero), film, r) in enumerate(zip(specs, films, results)):
+        assert r.status == 0, name
+        mb = {"cornell": 8, "fog": 32}.get(name, 16)
+        solo, _, en = resident[name].render(scenes.default_camera(gpu, res), n, seed_base=777 * k, max_bounce=mb,
+                                            hero_c=hero)
+        np.testing.assert_array_equal(film, solo, err_msg=f"{name} hero {hero}")
+        assert list(r.energy.fx) == list(en.fx), f"{name} hero {hero} energy"

@@ -57,10 +57,18 @@ def make_scene(name, level, lib_):
     return scenes.make_fog_strands(lib_)
 
 
+def lambda_mode(args):
+    from goodphotons_b200 import abi
+    band = args.lambda_policy == "band" or (args.lambda_policy == "auto" and args.workload == "cornell")
+    return abi.LAMBDA_UNIFORM_380_780 if band else abi.LAMBDA_SPD
+
+
 def workload_config(args):
     res, n, mb = WORKLOADS[args.workload]
+    lam = ("uniform over 380-780 nm, power weighted by the SPD pdf (FTB_LAMBDA_UNIFORM_380_780)"
+           if lambda_mode(args) else "sampled from the emitter SPD over 360-830 nm")
     cfg = {"workload": args.workload, "film": f"{res}x{res}", "photons_per_frame": n,
-           "max_bounce": mb, "seed": 0, "lambda": "sampled from the emitter SPD over 360-830 nm"}
+           "max_bounce": mb, "seed": 0, "lambda": lam}
     if args.workload == "glass":
         cfg.update(mesh=f"level-{args.level} icosphere r=0.4 m, 3-octave value noise 0.05 m",
                    triangles=20 * 4 ** args.level, ior="Cauchy 1.5 + 0.0042/um^2")
@@ -510,6 +518,9 @@ def main():
     ap.add_argument("--tuning", default="",
                     help="wave_slots,blocks_per_sm,graphs[,sort_rays[,regenerate]] instead of the autotuner")
     ap.add_argument("--hero", type=int, default=1, help="wavelengths per photon (hero bundles when > 1)")
+    ap.add_argument("--lambda-policy", default="auto", choices=["auto", "spd", "band"],
+                    help="wavelength draw: the emitter SPD (the reference's), uniform 380-780 nm, or auto "
+                         "(uniform for the Cornell configuration, which specifies it; SPD otherwise)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -562,8 +573,9 @@ def main():
     # counting pass (untimed): traversal work per closest-hit ray and per photon
     sc.set_profiling(2)
     n_count = min(n, 1 << 22)
+    lam = lambda_mode(args)
     sc.render_device(cam, n_count, film.data_ptr(), seed_base=1 << 50, max_bounce=mb,
-                     stream=stream.cuda_stream, hero_c=args.hero)
+                     stream=stream.cuda_stream, hero_c=args.hero, lambda_mode=lam)
     torch.cuda.synchronize(dev)
     cp = sc.profile(reset=True)
     rays_c, nodes_c, recs_c = cp.counters[0], cp.counters[1], cp.counters[2]
@@ -575,10 +587,10 @@ def main():
         film.zero_()
         if dist is None:
             sc.render_device(cam, n, film.data_ptr(), seed_base=k * n, max_bounce=mb, frac_bits=frac,
-                             stream=stream.cuda_stream, hero_c=args.hero)
+                             stream=stream.cuda_stream, hero_c=args.hero, lambda_mode=lam)
         else:   # the frame is n photons per rank; each rank traces its index shard
             multigpu.render_sharded(sc, cam, n * world, film, seed_base=k * n * world, max_bounce=mb,
-                                    hero_c=args.hero, dst=0, stream=stream.cuda_stream)
+                                    hero_c=args.hero, lambda_mode=lam, dst=0, stream=stream.cuda_stream)
 
     # autotuner (untimed): grid size, wave size and graph replay for this workload
     t = time.perf_counter()
@@ -671,7 +683,8 @@ def main():
     fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     film.zero_()
     fa.record(stream)
-    sc_fast.render_device(cam, n, film.data_ptr(), seed_base=(1 << 51), max_bounce=mb, stream=stream.cuda_stream)
+    sc_fast.render_device(cam, n, film.data_ptr(), seed_base=(1 << 51), max_bounce=mb, stream=stream.cuda_stream,
+                          hero_c=args.hero, lambda_mode=lam)
     fb.record(stream)
     torch.cuda.synchronize(dev)
     device_build = {"bake_ms": round(bake_fast_ms, 1), "bake_ms_host_sah": round(bake_ms, 1),
@@ -684,14 +697,15 @@ def main():
     e2e_steps = 0 if args.no_e2e else max(2, min(args.steps, 3))
     host_np = host.numpy()
     if e2e_steps:
-        sc.render(cam, 1 << 20, seed_base=1 << 52, max_bounce=mb, out=host_np)
+        sc.render(cam, 1 << 20, seed_base=1 << 52, max_bounce=mb, out=host_np, lambda_mode=lam)
     torch.cuda.synchronize(dev)
     e_times = []
     for k in range(e2e_steps):
         flush.fill_(k & 0xff)
         torch.cuda.synchronize(dev)
         t = time.perf_counter()
-        sc.render(cam, n, seed_base=(1 << 53) + (k * world + rank) * n, max_bounce=mb, out=host_np, hero_c=args.hero)
+        sc.render(cam, n, seed_base=(1 << 53) + (k * world + rank) * n, max_bounce=mb, out=host_np, hero_c=args.hero,
+                  lambda_mode=lam)
         e_times.append(time.perf_counter() - t)
     e_total = sum(e_times)
     if dist is not None:
@@ -706,6 +720,8 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(desc, cam, mb)
+        if cpu and lam:
+            cpu["lambda"] = "drawn from the emitter SPD: the reference has no uniform-band policy"
 
     if rank == 0:
         line = {

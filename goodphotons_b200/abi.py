@@ -6,6 +6,8 @@ sizes and field offsets against the compiled library.
 import ctypes as C
 
 FTB_OK = 0
+LAMBDA_SPD = 0
+LAMBDA_UNIFORM_380_780 = 1
 BUILD_SAH, BUILD_DEVICE = 0, 1
 
 STATUS_NAMES = {
@@ -93,7 +95,7 @@ class Camera(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("n_photons", C.c_int64), ("seed_base", C.c_uint64),
                 ("max_bounce", C.c_int32), ("frac_bits", C.c_int32), ("hero_c", C.c_int32),
-                ("pad", C.c_int32)]
+                ("lambda_mode", C.c_int32)]
 
 
 class Energy(C.Structure):
@@ -122,7 +124,7 @@ class PhotonLog(C.Structure):
 class Job(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("cam", Camera), ("d_film", C.c_void_p), ("n_photons", C.c_int64),
                 ("seed_base", C.c_uint64), ("max_bounce", C.c_int32), ("frac_bits", C.c_int32),
-                ("hero_c", C.c_int32), ("pad", C.c_int32)]
+                ("hero_c", C.c_int32), ("lambda_mode", C.c_int32)]
 
 
 class KernelProfile(C.Structure):
@@ -142,7 +144,7 @@ class ServerConfig(C.Structure):
 class Request(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("cam", Camera), ("n_photons", C.c_int64),
                 ("seed_base", C.c_uint64), ("max_bounce", C.c_int32), ("frac_bits", C.c_int32),
-                ("hero_c", C.c_int32), ("pad", C.c_int32), ("host_film", C.POINTER(C.c_int64))]
+                ("hero_c", C.c_int32), ("lambda_mode", C.c_int32), ("host_film", C.POINTER(C.c_int64))]
 
 
 class JobResult(C.Structure):

@@ -608,7 +608,7 @@ int32_t effective_hero(const ftb_scene* s, int32_t hero_c) {
 }
 
 ftb::DevJob make_job(const ftb_scene* s, const ftb_camera* cam, int64_t* d_film, unsigned long long* d_tally,
-                     int32_t frac_bits, int32_t max_bounce, int32_t hero_c = 1) {
+                     int32_t frac_bits, int32_t max_bounce, int32_t hero_c = 1, int32_t lambda_mode = 0) {
     ftb::DevJob J;
     std::memset(&J, 0, sizeof J);
     J.sc = s->dev;
@@ -619,6 +619,7 @@ ftb::DevJob make_job(const ftb_scene* s, const ftb_camera* cam, int64_t* d_film,
     J.tally_scale_inv = std::ldexp(1.0, 32) / s->power;
     J.max_bounce = max_bounce;
     J.hero_c = effective_hero(s, hero_c);
+    J.lambda_mode = lambda_mode;
     return J;
 }
 
@@ -764,8 +765,8 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
 // Trace n photons from seed_base into d_film / tally, on the scene's streams.
 ftb_status run_photons(ftb_scene* s, const ftb_camera* cam, int64_t n, uint64_t seed_base, int32_t max_bounce,
                        int32_t frac_bits, int64_t* d_film, unsigned long long* d_tally, ftb_photon_log* d_logs,
-                       cudaStream_t user_stream, int32_t hero_c = 1) {
-    std::vector<ftb::DevJob> base{make_job(s, cam, d_film, d_tally, frac_bits, max_bounce, hero_c)};
+                       cudaStream_t user_stream, int32_t hero_c = 1, int32_t lambda_mode = 0) {
+    std::vector<ftb::DevJob> base{make_job(s, cam, d_film, d_tally, frac_bits, max_bounce, hero_c, lambda_mode)};
     return run_jobs(s, base, {n}, {seed_base}, d_logs != nullptr, d_logs, (int64_t)seed_base, user_stream);
 }
 
@@ -804,6 +805,8 @@ ftb_status check_params(const ftb_scene* s, const ftb_camera* cam, const ftb_ren
     if (p->n_photons < 0) return fail(FTB_ERR_INVALID, "negative photon count");
     if (p->max_bounce < 0 || p->max_bounce > 1024) return fail(FTB_ERR_INVALID, "max_bounce out of range [0, 1024]");
     if (p->frac_bits > 56) return fail(FTB_ERR_INVALID, "frac_bits too large");
+    if (p->lambda_mode != FTB_LAMBDA_SPD && p->lambda_mode != FTB_LAMBDA_UNIFORM_380_780)
+        return fail(FTB_ERR_INVALID, "unknown lambda_mode");
     if (!(s->power > 0.0)) return fail(FTB_ERR_UNSUPPORTED, "scene emits no power");
     return FTB_OK;
 }
@@ -1256,7 +1259,7 @@ ftb_status ftb_render_forward_device(ftb_scene* s, const ftb_camera* cam, const 
     CK(cudaMemsetAsync(s->eng->tally, 0, 8 * sizeof(unsigned long long), us), "memset");
     CK(cudaMemsetAsync(s->eng->status, 0, 64, us), "memset");
     st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, d_film, s->eng->tally, nullptr, us,
-                     p->hero_c);
+                     p->hero_c, p->lambda_mode);
     if (st != FTB_OK) return st;
     if (info) { info->frac_bits = frac; info->scale = s->power * std::ldexp(1.0, -frac); info->power_ref = s->power; }
     if (energy) {
@@ -1285,7 +1288,7 @@ ftb_status ftb_render_forward(ftb_scene* s, const ftb_camera* cam, const ftb_ren
     CK(cudaMemset(s->eng->tally, 0, 8 * sizeof(unsigned long long)), "memset tally");
     CK(cudaMemset(s->eng->status, 0, 64), "memset status");
     st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, nullptr,
-                     nullptr, p->hero_c);
+                     nullptr, p->hero_c, p->lambda_mode);
     if (st != FTB_OK) return st;
     CK(cudaDeviceSynchronize(), "render");
     st = read_status(s);
@@ -1309,7 +1312,7 @@ ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n, ftb_film_info* infos
         const ftb_job& b = jobs[j];
         if (!b.scene || !b.d_film) return fail(FTB_ERR_INVALID, "job " + std::to_string(j) + ": null scene or film");
         if (b.scene->device != s->device) return fail(FTB_ERR_INVALID, "batch jobs must share one device");
-        ftb_render_params p{b.n_photons, b.seed_base, b.max_bounce, b.frac_bits};
+        ftb_render_params p{b.n_photons, b.seed_base, b.max_bounce, b.frac_bits, b.hero_c, b.lambda_mode};
         ftb_status st = check_params(b.scene, &b.cam, &p);
         if (st != FTB_OK) return fail(st, "job " + std::to_string(j) + ": " + g_err);
     }
@@ -1334,7 +1337,7 @@ ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n, ftb_film_info* infos
         const ftb_job& b = jobs[j];
         int frac = b.frac_bits > 0 ? b.frac_bits : default_frac_bits(b.n_photons);
         base.push_back(make_job(b.scene, &b.cam, b.d_film, s->eng->batch_tally + 8 * (size_t)j, frac, b.max_bounce,
-                                b.hero_c));
+                                b.hero_c, b.lambda_mode));
         count.push_back(b.n_photons);
         seed.push_back(b.seed_base);
         if (infos) {
@@ -1375,7 +1378,7 @@ ftb_status ftb_trace_log(ftb_scene* s, const ftb_camera* cam, const ftb_render_p
     cudaMemset(s->eng->tally, 0, 8 * sizeof(unsigned long long));
     cudaMemset(s->eng->status, 0, 64);
     st = run_photons(s, cam, p->n_photons, p->seed_base, p->max_bounce, frac, s->eng->film, s->eng->tally, d_logs,
-                     nullptr, p->hero_c);
+                     nullptr, p->hero_c, p->lambda_mode);
     if (st == FTB_OK) {
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) st = cuda_fail(e, "trace_log");

@@ -1262,6 +1262,18 @@ __device__ __forceinline__ double sample_at(const DevEmit& em, double u, double&
     return LAMBDA_MIN + (lo + frac) * em.step;
 }
 
+// FTB_LAMBDA_UNIFORM_380_780 (no counterpart in the reference): lambda uniform over
+// [380, 780) nm from the variate u, and the weight pdf_SPD(lambda) / (1/400 nm) with the
+// emitter's binned SPD pdf, so the photon's power times the weight is unbiased for the band.
+__device__ __forceinline__ double sample_uniform_band(const DevEmit& em, double u, double& weight) {
+    const double lam = 380.0 + 400.0 * u;
+    int b = (int)((lam - LAMBDA_MIN) / em.step);
+    if (b < 0) b = 0;
+    if (b > em.n - 1) b = em.n - 1;
+    weight = (em.cdf[b + 1] - em.cdf[b]) / em.step * 400.0;
+    return lam;
+}
+
 // ------------------------------------------------------------------ kernels ------------
 template <bool MEDIA, bool STREAM>
 __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
@@ -1282,11 +1294,19 @@ __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit(Wave w, const DevJo
         const DevEmit& em = sc.emit[ei];
         D3 origin, emit_n, dir;
         emit_sample(em, rng, origin, emit_n, dir);
-        double pdf;
-        double lam = sample_at(em, uniform(rng), pdf);
+        double pdf = 0.0, wl = 1.0;
+        const double ul = uniform(rng);
+        double lam;
+        if (J.lambda_mode == FTB_LAMBDA_UNIFORM_380_780) {
+            lam = sample_uniform_band(em, ul, wl);
+            pdf = wl;
+        } else {
+            lam = sample_at(em, ul, pdf);
+        }
         if (pdf <= 0) { log_emitted(w, k, 4, 0.0); continue; }
         double beta = (sc.n_emit == 1) ? em.power : sc.total_power;
         beta *= 1.0;
+        if (J.lambda_mode == FTB_LAMBDA_UNIFORM_380_780) beta *= wl;
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(beta, J.tally_scale_inv, f.status));
         const double cie[3] = {cie_x(lam), cie_y(lam), cie_z(lam)};
         connect_surface<MEDIA>(sc, J, w, f, j, origin, emit_n, emit_n, emit_n, lam, cie, beta, 1.0);
@@ -1772,19 +1792,26 @@ __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit_hero(Wave w, const 
         D3 origin, emit_n, dir;
         emit_sample(em, rng, origin, emit_n, dir);
         // hero::sampleBundle (hero.h:100-113): one variate, strata u + i/C wrapped into [0,1)
-        double lam[kHeroMax], beta[kHeroMax], one[kHeroMax];
+        double lam[kHeroMax], beta[kHeroMax], one[kHeroMax], wl[kHeroMax];
+        const bool band = J.lambda_mode == FTB_LAMBDA_UNIFORM_380_780;
         double u = uniform(rng), pdf;
-        lam[0] = sample_at(em, u, pdf);
+        if (band) { lam[0] = sample_uniform_band(em, u, wl[0]); pdf = wl[0]; }
+        else lam[0] = sample_at(em, u, pdf);
         if (pdf <= 0) { log_emitted(w, k, 4, 0.0); continue; }
         for (int i = 1; i < C; ++i) {
             double uu = u + (double)i / (double)C;
             if (uu >= 1.0) uu -= 1.0;
             double p2;
-            lam[i] = sample_at(em, uu, p2);
+            if (band) lam[i] = sample_uniform_band(em, uu, wl[i]);
+            else lam[i] = sample_at(em, uu, p2);
         }
         double base = (sc.n_emit == 1) ? em.power : sc.total_power;
         base *= 1.0;   // spotW
-        for (int i = 0; i < C; ++i) { beta[i] = base / C; one[i] = 1.0; }
+        for (int i = 0; i < C; ++i) {
+            beta[i] = base / C;
+            if (band) beta[i] *= wl[i];
+            one[i] = 1.0;
+        }
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
         connect_surface_hero(J, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, one, C);
         D3 ro = origin + dir * 1e-6;

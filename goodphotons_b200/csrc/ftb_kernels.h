@@ -36,7 +36,8 @@ struct DevJob {
     DevCam cam;
     int64_t* film;             // 4 words per pixel
     const DevView* views;      // n_views > 1: every vertex connects to each view (shared splat)
-    int32_t n_views, pad;
+    int32_t n_views;
+    int32_t lambda_mode;       // ftb_lambda_mode of the job's photons
     unsigned long long* tally; // 5 fixed-point energy tallies
     double film_scale_inv;     // 2^frac / power_ref
     double tally_scale_inv;    // 2^32 / power_ref

@@ -60,7 +60,8 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     if (!scene || !cam || !p || !d_film) return na_fail(FTB_ERR_INVALID, "null argument");
     if (!ftb::scene_internals(scene, &dev, &device, &sms, &power)) return na_fail(FTB_ERR_INVALID, "bad scene");
     if (p->n_photons < 0 || p->max_bounce < 0 || p->max_bounce > 1024 || p->frac_bits > 56 ||
-        cam->res_x <= 0 || cam->res_y <= 0)
+        cam->res_x <= 0 || cam->res_y <= 0 ||
+        (p->lambda_mode != FTB_LAMBDA_SPD && p->lambda_mode != FTB_LAMBDA_UNIFORM_380_780))
         return na_fail(FTB_ERR_INVALID, "bad render parameters");
     if (p->hero_c > 1 && dev.n_med == 0)
         return na_fail(FTB_ERR_UNSUPPORTED, "ftb_render_forward_noalloc traces one wavelength per photon "
@@ -112,6 +113,7 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     J.slot0 = 0;
     J.n = (int32_t)p->n_photons;
     J.max_bounce = p->max_bounce;
+    J.lambda_mode = p->lambda_mode;
     ftb_status out = FTB_OK;
     cudaError_t e = cudaMemsetAsync(tally, 0, 8 * sizeof(unsigned long long), st);   // tallies start at zero
     if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 64, st);

@@ -218,6 +218,7 @@ int64_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
         J.n = (int32_t)give[i];
         J.max_bounce = j->req.max_bounce;
         J.hero_c = j->hero;
+        J.lambda_mode = j->req.lambda_mode;
         table.push_back(J);
         members.push_back(j);
         j->next += give[i];
@@ -475,7 +476,8 @@ ftb_status ftb_server_submit(ftb_server* s, const ftb_request* r, uint64_t* job_
     if (dev != s->device) { delete j; return fail(FTB_ERR_INVALID, "scene lives on another device"); }
     const ftb_camera& c = r->cam;
     if (c.res_x <= 0 || c.res_y <= 0 || (int64_t)c.res_x * c.res_y > ((int64_t)1 << 28) || r->n_photons < 0 ||
-        r->max_bounce < 0 || r->max_bounce > 1024 || r->frac_bits > 56) {
+        r->max_bounce < 0 || r->max_bounce > 1024 || r->frac_bits > 56 ||
+        (r->lambda_mode != FTB_LAMBDA_SPD && r->lambda_mode != FTB_LAMBDA_UNIFORM_380_780)) {
         delete j;
         return fail(FTB_ERR_INVALID, "bad request");
     }

@@ -143,6 +143,7 @@ class _Lib:
             arr[i].max_bounce = j.get("max_bounce", 8)
             arr[i].frac_bits = j.get("frac_bits", 0)
             arr[i].hero_c = j.get("hero_c", 1)
+            arr[i].lambda_mode = j.get("lambda_mode", abi.LAMBDA_SPD)
         infos = (abi.FilmInfo * n)()
         ens = (abi.Energy * n)() if want_energy else None
         self.check(self.L.ftb_render_batch(arr, n, infos, ens, C.c_void_p(stream or 0)))
@@ -265,12 +266,12 @@ class Scene:
         self.lib.check(self.lib.L.ftb_scene_footprint(self.h, rx, ry, C.byref(fp)))
         return fp
 
-    def render(self, cam, n, seed_base=0, max_bounce=8, frac_bits=0, out=None, hero_c=1):
+    def render(self, cam, n, seed_base=0, max_bounce=8, frac_bits=0, out=None, hero_c=1, lambda_mode=0):
         """One-shot render into a host film: returns (film int64 [ry, rx, 4], info, energy).
         `out` may be a preallocated (e.g. pinned) int64 array of that shape."""
         film = out if out is not None else np.zeros((cam.res_y, cam.res_x, 4), dtype=np.int64)
         assert film.dtype == np.int64 and film.shape == (cam.res_y, cam.res_x, 4) and film.flags.c_contiguous
-        p = abi.RenderParams(n, seed_base, max_bounce, frac_bits, hero_c)
+        p = abi.RenderParams(n, seed_base, max_bounce, frac_bits, hero_c, lambda_mode)
         info, en = abi.FilmInfo(), abi.Energy()
         self.lib.check(self.lib.L.ftb_render_forward(
             self.h, C.byref(cam), C.byref(p), film.ctypes.data_as(C.POINTER(C.c_int64)),
@@ -278,8 +279,8 @@ class Scene:
         return film, info, en
 
     def render_device(self, cam, n, d_film_ptr, seed_base=0, max_bounce=8, frac_bits=0,
-                      stream=None, want_energy=False, hero_c=1):
-        p = abi.RenderParams(n, seed_base, max_bounce, frac_bits, hero_c)
+                      stream=None, want_energy=False, hero_c=1, lambda_mode=0):
+        p = abi.RenderParams(n, seed_base, max_bounce, frac_bits, hero_c, lambda_mode)
         info = abi.FilmInfo()
         en = abi.Energy() if want_energy else None
         self.lib.check(self.lib.L.ftb_render_forward_device(
@@ -295,9 +296,9 @@ class Scene:
         self.lib.check(self.lib.L.ftb_scene_profile(self.h, C.byref(kp), 1 if reset else 0))
         return kp
 
-    def trace_log(self, cam, n, seed_base=0, max_bounce=8, hero_c=1):
+    def trace_log(self, cam, n, seed_base=0, max_bounce=8, hero_c=1, lambda_mode=0):
         logs = (abi.PhotonLog * max(1, n))()
-        p = abi.RenderParams(n, seed_base, max_bounce, 0, hero_c)
+        p = abi.RenderParams(n, seed_base, max_bounce, 0, hero_c, lambda_mode)
         self.lib.check(self.lib.L.ftb_trace_log(self.h, C.byref(cam), C.byref(p), logs))
         return logs_to_numpy(logs, n)
 
@@ -313,13 +314,14 @@ class Server:
         self.h = h
         self._films = {}
 
-    def submit(self, scene, cam, n, seed_base=0, max_bounce=8, frac_bits=0, host_film=None, hero_c=1):
+    def submit(self, scene, cam, n, seed_base=0, max_bounce=8, frac_bits=0, host_film=None, hero_c=1,
+               lambda_mode=0):
         """Queue a job; host_film (int64 [res_y, res_x, 4], C-contiguous) receives the film."""
         if host_film is not None:
             assert host_film.dtype == np.int64 and host_film.flags.c_contiguous
             assert host_film.size == cam.res_x * cam.res_y * 4
         r = abi.Request(scene.h.value if hasattr(scene.h, "value") else scene.h, cam, n, seed_base, max_bounce,
-                        frac_bits, hero_c, 0,
+                        frac_bits, hero_c, lambda_mode,
                         host_film.ctypes.data_as(C.POINTER(C.c_int64)) if host_film is not None else None)
         jid = C.c_uint64()
         self.lib.check(self.lib.L.ftb_server_submit(self.h, C.byref(r), C.byref(jid)))

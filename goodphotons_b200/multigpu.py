@@ -44,7 +44,7 @@ def reduce_film(film, tally=None, dst=None, group=None):
 
 
 def render_sharded(scene, cam, n, film, seed_base=0, max_bounce=8, frac_bits=0, dst=None,
-                   group=None, stream=None, hero_c=1):
+                   group=None, stream=None, hero_c=1, lambda_mode=0):
     """This rank's share of an n-photon frame into the device film `film` (int64 tensor of
     shape [res_y, res_x, 4]), then the frame-end sum over ranks.  Returns the frame's
     energy tallies (int64 tensor of 5, fixed point with 32 fraction bits per unit of the
@@ -56,7 +56,7 @@ def render_sharded(scene, cam, n, film, seed_base=0, max_bounce=8, frac_bits=0, 
     frac = frac_bits or default_frac_bits(n)
     _, en = scene.render_device(cam, count, film.data_ptr(), seed_base=seed_base + first,
                                 max_bounce=max_bounce, frac_bits=frac, stream=stream, want_energy=True,
-                                hero_c=hero_c)
+                                hero_c=hero_c, lambda_mode=lambda_mode)
     tally = torch.tensor([int(x) - (1 << 64) if x >= (1 << 63) else int(x) for x in en.fx],
                          dtype=torch.int64, device=film.device)
     reduce_film(film, tally, dst=dst, group=group)

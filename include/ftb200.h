@@ -217,8 +217,18 @@ typedef struct ftb_render_params {
                              wavelength; 2..8 hero bundles (Renderer::tracePhotonHero), used
                              only in scenes without media, as the reference does; larger
                              values are clamped to 8 */
-    int32_t pad;
+    int32_t lambda_mode;  /* ftb_lambda_mode: how the photon's wavelength is drawn */
 } ftb_render_params;
+
+/* Wavelength policy of emission.  FTB_LAMBDA_SPD is the reference's: lambda drawn from the
+ * emitter's SPD over 360-830 nm (EmissionSampler::sampleAt, spectrum.h:374-383), the photon
+ * carrying the emitter's power.  FTB_LAMBDA_UNIFORM_380_780 has no counterpart in the
+ * reference: lambda = 380 + 400 u from the same variate u, the photon's power times
+ * pdf_SPD(lambda) / (1/400 nm) with the same binned SPD pdf, so the estimate of the light in
+ * 380-780 nm is unbiased (light outside the band is not emitted); a photon whose bin has zero
+ * SPD is not emitted, like a zero-pdf draw.  Hero bundles stratify u as before and weight
+ * each wavelength the same way. */
+typedef enum ftb_lambda_mode { FTB_LAMBDA_SPD = 0, FTB_LAMBDA_UNIFORM_380_780 = 1 } ftb_lambda_mode;
 
 /* Energy report (reference EnergyReport, render.h:29-31).  Each tally is the sum of the
  * photons' carried beta, kept in 64-bit fixed point with 32 fraction bits relative to the
@@ -344,7 +354,7 @@ typedef struct ftb_job {
     int32_t max_bounce;
     int32_t frac_bits;     /* <= 0: the default for n_photons */
     int32_t hero_c;        /* wavelengths per photon, as ftb_render_params.hero_c */
-    int32_t pad;
+    int32_t lambda_mode;   /* as ftb_render_params.lambda_mode */
 } ftb_job;
 
 ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n_jobs, ftb_film_info* infos,
@@ -481,7 +491,7 @@ typedef struct ftb_request {
     int32_t max_bounce;
     int32_t frac_bits;         /* <= 0: the default for n_photons */
     int32_t hero_c;            /* wavelengths per photon, as ftb_render_params.hero_c */
-    int32_t pad;
+    int32_t lambda_mode;       /* as ftb_render_params.lambda_mode */
     int64_t* host_film;        /* res_x*res_y*4 int64, written at completion (page-locked memory
                                   copies fastest); NULL: the film is dropped */
 } ftb_request;

@@ -187,6 +187,18 @@ int fto_emission_cdf(const ftb_scene_desc* d, int spec, double step, double* cdf
     return emission_build(&S, spec, step, cdf, cap, integral);
 }
 
+/* FTB_LAMBDA_UNIFORM_380_780 (no counterpart in the reference; the build's uniform-band
+ * policy, restated here so the oracle checks it): lambda = 380 + 400 u, weight =
+ * pdf_SPD(lambda) / (1/400 nm) from the emitter's binned CDF. */
+static double emission_sample_band(const double* cdf, int n, double step, double u, double* weight) {
+    double lam = 380.0 + 400.0 * u;
+    int b = (int)((lam - LAMBDA_MIN) / step);
+    if (b < 0) b = 0;
+    if (b > n - 1) b = n - 1;
+    *weight = (cdf[b + 1] - cdf[b]) / step * 400.0;
+    return lam;
+}
+
 /* EmissionSampler::sampleAt (spectrum.h:374-383) */
 static double emission_sample_at(const double* cdf, int n, double step, double u,
                                  double* pdf) {
@@ -276,6 +288,7 @@ typedef struct {
 } Med;
 
 struct fto_ctx {
+    int lambda_mode;   /* ftb_lambda_mode; set by fto_set_lambda_mode */
     int64_t ni;
     int n_blas;
     Blas* blas;
@@ -301,6 +314,12 @@ struct fto_ctx {
 };
 
 double fto_total_power(const fto_ctx* c) { return c ? c->total_power : 0.0; }
+
+int fto_set_lambda_mode(fto_ctx* c, int mode) {
+    if (!c || (mode != FTB_LAMBDA_SPD && mode != FTB_LAMBDA_UNIFORM_380_780)) return fail("fto_set_lambda_mode: bad input");
+    c->lambda_mode = mode;
+    return 0;
+}
 
 /* ------------------------------------------------------------- geometry.h ----------- */
 typedef struct { int kx, ky, kz; double Sx, Sy, Sz; } Shear;
@@ -1172,11 +1191,18 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
         emit_n = em->normal;
     }
     dir = em->collimated ? em->beam : cosine_hemisphere(emit_n, rng);
-    double pdf_l = 0.0;
-    double lam = emission_sample_at(em->cdf, em->n, em->step, pcg_uniform(rng), &pdf_l);
+    double pdf_l = 0.0, wl = 1.0;
+    double ul = pcg_uniform(rng), lam;
+    if (c->lambda_mode == FTB_LAMBDA_UNIFORM_380_780) {
+        lam = emission_sample_band(em->cdf, em->n, em->step, ul, &wl);
+        pdf_l = wl;
+    } else {
+        lam = emission_sample_at(em->cdf, em->n, em->step, ul, &pdf_l);
+    }
     if (pdf_l <= 0) return;
     double beta = (c->n_emit == 1) ? em->power : c->total_power;
     beta *= 1.0;   /* spotW */
+    if (c->lambda_mode == FTB_LAMBDA_UNIFORM_380_780) beta *= wl;
     e[E_EMIT] += beta;
     connect_surface(T, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
     V3 ro = vadd(origin, vmul(dir, 1e-6)), rd = dir;
@@ -1541,20 +1567,26 @@ static void trace_photon_hero(Tr* T, Pcg* rng, int max_bounce, int C, double* e,
     }
     dir = em->collimated ? em->beam : cosine_hemisphere(emit_n, rng);
     /* hero::sampleBundle (hero.h:100-113): one variate, strata u + i/C wrapped */
-    double lam[HERO_MAX], pdf[HERO_MAX], beta[HERO_MAX];
+    double lam[HERO_MAX], pdf[HERO_MAX], beta[HERO_MAX], wl[HERO_MAX];
+    const int band = c->lambda_mode == FTB_LAMBDA_UNIFORM_380_780;
     double u = pcg_uniform(rng);
     pdf[0] = 0.0;
-    lam[0] = emission_sample_at(em->cdf, em->n, em->step, u, &pdf[0]);
+    if (band) { lam[0] = emission_sample_band(em->cdf, em->n, em->step, u, &wl[0]); pdf[0] = wl[0]; }
+    else lam[0] = emission_sample_at(em->cdf, em->n, em->step, u, &pdf[0]);
     if (pdf[0] <= 0.0) return;
     for (int i = 1; i < C; ++i) {
         double uu = u + (double)i / (double)C;
         if (uu >= 1.0) uu -= 1.0;
         pdf[i] = 0.0;
-        lam[i] = emission_sample_at(em->cdf, em->n, em->step, uu, &pdf[i]);
+        if (band) lam[i] = emission_sample_band(em->cdf, em->n, em->step, uu, &wl[i]);
+        else lam[i] = emission_sample_at(em->cdf, em->n, em->step, uu, &pdf[i]);
     }
     double base = (c->n_emit == 1) ? em->power : c->total_power;
     base *= 1.0;   /* spotW */
-    for (int i = 0; i < C; ++i) beta[i] = base / C;
+    for (int i = 0; i < C; ++i) {
+        beta[i] = base / C;
+        if (band) beta[i] *= wl[i];
+    }
     int sec_alive = C > 1;
     e[E_EMIT] += active_sum(beta, sec_alive ? C : 1);
     {

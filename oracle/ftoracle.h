@@ -49,6 +49,10 @@ int fto_trace(const fto_ctx* ctx, const ftb_camera* cam, int64_t n, uint64_t see
 /* Total emitted power (Scene::totalPower, scene.h:1509-1511). */
 double fto_total_power(const fto_ctx* ctx);
 
+/* Wavelength policy of later fto_trace calls (ftb_lambda_mode; FTB_LAMBDA_SPD, the
+ * reference's, by default).  Returns 0, or -1 on invalid input. */
+int fto_set_lambda_mode(fto_ctx* ctx, int mode);
+
 /* EmissionSampler::build (spectrum.h:357-369) for spectrum `spec` of the descriptor;
  * returns the bin count (cdf has count+1 entries) or -1. */
 int fto_emission_cdf(const ftb_scene_desc* desc, int spec, double step, double* cdf,

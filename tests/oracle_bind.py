@@ -40,6 +40,8 @@ class Oracle:
                                 C.c_int, C.c_int, _PD, _PD, _PD, C.POINTER(abi.PhotonLog), _PI64]
         L.fto_total_power.restype = C.c_double
         L.fto_total_power.argtypes = [C.c_void_p]
+        L.fto_set_lambda_mode.restype = C.c_int
+        L.fto_set_lambda_mode.argtypes = [C.c_void_p, C.c_int]
         L.fto_emission_cdf.restype = C.c_int
         L.fto_emission_cdf.argtypes = [C.POINTER(abi.SceneDesc), C.c_int, C.c_double, _PD, C.c_int, _PD]
         L.fto_spectrum_eval.restype = C.c_double
@@ -60,8 +62,10 @@ class Oracle:
         return h
 
     def trace(self, desc, cam, n, seed_base=0, max_bounce=8, threads=1, logs=False, rays=False, ctx=None,
-              hero_c=1):
+              hero_c=1, lambda_mode=0):
         h = ctx or self.prepare(desc)
+        if self.L.fto_set_lambda_mode(h, lambda_mode) != 0:
+            raise RuntimeError(self.L.fto_last_error().decode())
         npix = cam.res_x * cam.res_y
         xyz = np.zeros((npix, 3))
         hits = np.zeros(npix)

@@ -192,3 +192,27 @@ def test_film_statistics_independent_photons(name, level, gpu, oracle):
     assert bad <= limit, f"{bad} of {lit.sum()} pixels beyond 3 sigma (chance allows {limit:.0f})"
     rel = mg.sum() / mc.sum() - 1.0
     assert abs(rel) < 0.005, f"mean luminance differs by {rel:.4%}"
+
+
+@pytest.mark.parametrize("name,hero", [("cornell", 1), ("glass", 4), ("fog_strands", 1), ("instances", 1)])
+def test_uniform_band_policy_matches_oracle(name, hero, scenes_cache, gpu, oracle):
+    """FTB_LAMBDA_UNIFORM_380_780 (the build's uniform-band wavelength policy) against the
+    oracle's restatement of it: per-photon paths, then film and energy."""
+    mk, res, _, mb, seed, _ = cases.CASES[name]
+    d, sc = scenes_cache[name]
+    n = 1 << 14
+    band = abi.LAMBDA_UNIFORM_380_780
+    cam = cases.camera(gpu, res)
+    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=mb, hero_c=hero, lambda_mode=band)
+    ol = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, logs=True, threads=4, hero_c=hero,
+                      lambda_mode=band)["logs"]
+    same = (gl["n_hits"] == ol["n_hits"]) & (gl["prim_hash"] == ol["prim_hash"]) & (gl["fate"] == ol["fate"])
+    assert (~same).sum() <= max(1, int(1e-5 * n)), f"{(~same).sum()} of {n} photon paths differ"
+    np.testing.assert_allclose(gl["beta"][same], ol["beta"][same], rtol=1e-12, atol=0)
+    film, info, en = sc.render(cam, n, seed_base=seed, max_bounce=mb, hero_c=hero, lambda_mode=band)
+    o = oracle.trace(d, cam, n, seed_base=seed, max_bounce=mb, threads=1, hero_c=hero, lambda_mode=band)
+    assert_film_close(film, info, o["xyz"], o["hits"])
+    np.testing.assert_allclose(en.as_list(), o["energy"], rtol=1e-9, atol=0)
+    # the policy changes the film: the SPD-sampled render of the same photons differs
+    film_spd, _, _ = sc.render(cam, n, seed_base=seed, max_bounce=mb, hero_c=hero)
+    assert not np.array_equal(film_spd, film)

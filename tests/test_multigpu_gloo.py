@@ -35,7 +35,7 @@ class FakeScene:
         self.calls = []
 
     def render_device(self, cam, n, d_film_ptr, seed_base=0, max_bounce=8, frac_bits=0, stream=None,
-                      want_energy=False, hero_c=1):
+                      want_energy=False, hero_c=1, lambda_mode=0):
         import torch
         assert d_film_ptr == self.film.data_ptr()
         self.calls.append((n, seed_base, frac_bits))

@@ -46,6 +46,8 @@ METRIC = "photon paths/s on 1 B200"
 NODE_BYTES = 80     # WNode
 REC_BYTES = 80      # PrimRec
 RAY_IO_BYTES = 64   # extend: queue index 4 + ray 48 read, hit t 8 + record 4 written
+SHADOW_IO_BYTES = 140   # shadow: record read (origin 24, direction 24, max 8, XYZ 24, pixel, job,
+                        # view 12) + 4 film words of 8 B updated (read + write)
 
 
 def make_scene(name, level, lib_):
@@ -644,22 +646,33 @@ def main():
     photons = n * args.steps * world
     value = photons / total_s
 
-    # roofline of the dominant kernel (closest-hit traversal unless another dominates)
+    # roofline of the dominant traversal kernel: closest hit, or the shadow rays' any-hit walk
+    # where that takes more of the frame (the Cornell and fog workloads)
     names = ["k_emit", "k_extend", "k_shade", "k_shadow"]
     kms = list(prof.ms)
     dom = int(np.argmax(kms))
     peak, peak_kind = measured_peak()
-    rays_timed = rays_per_photon * n * args.steps   # of the profiled steps
-    extend_launches = max(1, prof.launches[1])
-    bytes_launch = rays_timed * bytes_per_ray / extend_launches
-    avg_launch_s = kms[1] / 1e3 / extend_launches
+    traffic_ray = None
+    if kms[3] > kms[1]:
+        ki, kname = 3, "k_shadow (any-hit traversal of the camera connections + splat)"
+        srays_c = max(1, cp.counters[3])
+        unit_bytes = (cp.counters[4] * NODE_BYTES + cp.counters[5] * REC_BYTES) / srays_c + SHADOW_IO_BYTES
+        units_timed = cp.counters[3] / n_count * n * args.steps
+    else:
+        ki, kname = 1, "k_extend (closest-hit traversal)"
+        unit_bytes = bytes_per_ray
+        units_timed = rays_per_photon * n * args.steps   # of the profiled steps
+        traffic_ray = ncu_traffic_per_ray(args.workload)
+    launches_k = max(1, prof.launches[ki])
+    bytes_launch = units_timed * unit_bytes / launches_k
+    avg_launch_s = kms[ki] / 1e3 / launches_k
     achieved = bytes_launch / avg_launch_s / 1e9
-    traffic_ray = ncu_traffic_per_ray(args.workload)
     roofline = {
-        "bound": "hbm", "kernel": "k_extend (closest-hit traversal)", "achieved": round(achieved, 1),
+        "bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-        "traffic": (round(traffic_ray * rays_timed / extend_launches) if traffic_ray else None),
+        "traffic": (round(traffic_ray * units_timed / launches_k) if traffic_ray else None),
         "peak_source": f"{peak_kind} hbm_gbs (copy)",
+        "algorithmic_bytes_per_unit": round(unit_bytes, 1),
         "algorithmic_bytes_per_ray": round(bytes_per_ray, 1),
         "node_visits_per_ray": round(nodes_c / max(1, rays_c), 3),
         "record_tests_per_ray": round(recs_c / max(1, rays_c), 3),

@@ -940,9 +940,10 @@ __device__ __forceinline__ int agg_inc(int32_t* ctr) {
 }
 
 // A queue of paths is two-ended: paths outside every dielectric grow from entry 0 up
-// (count q[0]), paths inside one grow from entry W-1 down (count q[1]), so each end holds
-// paths of similar traversal cost (inside a closed mesh a ray crosses it; outside most rays
-// meet a wall after a few nodes) and warps diverge less.  Queue position p < q[0] is entry
+// (count q[0]), paths inside one -- or leaving a curve, among the strands -- grow from entry
+// W-1 down (count q[1]), so each end holds paths of similar traversal cost (inside a closed
+// mesh a ray crosses it; outside most rays meet a wall after a few nodes) and warps diverge
+// less.  Queue position p < q[0] is entry
 // p; position q[0] + k is entry W-1-k.
 __device__ __forceinline__ int queue_len(const int32_t* q) { return q[0] + q[1]; }
 
@@ -1526,6 +1527,7 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
         for (int k = 0; k < stk.n; ++k) stk.e[k] = in.stk[k * w.W + i];
         log_hit<INST>(w, in, i, sc, rec);
         int fate = -1;   // -1 continue, 0 absorbed, 1 escaped
+        bool costly = false;   // the next ray starts among curves: back end of the queue
         bool valid = rec >= 0;
         double d_surf = valid ? ht : 1e30;
         double d_event = d_surf;
@@ -1555,6 +1557,7 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
         } else {
             PrimRec r;
             load_rec(sc.recs, rec, r);
+            if (SHAPES && rec_type(r) == REC_CURVE) costly = true;
             Hit h;
             if (INST && rec_type(r) == REC_INST) {
                 instance_hit(sc.inst[rec_inst(r)], w.hit_sub[i], ro, rd, h);
@@ -1664,7 +1667,7 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
             continue;
         }
         load_cie();
-        const int o = stk.n > 0 ? w.W - 1 - agg_inc(out_count + 1) : agg_inc(out_count);
+        const int o = (stk.n > 0 || costly) ? w.W - 1 - agg_inc(out_count + 1) : agg_inc(out_count);
         out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
         out.ox[o] = no.x; out.oy[o] = no.y; out.oz[o] = no.z;
         out.dx[o] = nd.x; out.dy[o] = nd.y; out.dz[o] = nd.z;
@@ -1873,6 +1876,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                 }
         }
         int fate = -1;   // -1 continue, 0 absorbed, 1 escaped
+        bool costly = false;   // the next ray starts among curves: back end of the queue
         D3 no = ro, nd = rd;
         long long absorbed = 0;   // reweights booked as absorption (fixed point, per add)
         if (!valid) {
@@ -1880,6 +1884,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
         } else {
             PrimRec r;
             load_rec(sc.recs, rec, r);
+            if (SHAPES && rec_type(r) == REC_CURVE) costly = true;
             Hit h;
             if (INST && rec_type(r) == REC_INST) {
                 instance_hit(sc.inst[rec_inst(r)], w.hit_sub[p], ro, rd, h);
@@ -2014,7 +2019,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
             log_finish(w, in, p, 2, beta[0]);
             continue;
         }
-        const int o = stk.n > 0 ? w.W - 1 - agg_inc(out_count + 1) : agg_inc(out_count);
+        const int o = (stk.n > 0 || costly) ? w.W - 1 - agg_inc(out_count + 1) : agg_inc(out_count);
         out.rng_s[o] = rng.s; out.rng_i[o] = rng.inc;
         out.ox[o] = no.x; out.oy[o] = no.y; out.oz[o] = no.z;
         out.dx[o] = nd.x; out.dy[o] = nd.y; out.dz[o] = nd.z;

@@ -63,3 +63,38 @@ def test_band_policy_changes_only_the_wavelength_draw(L, oracle):
     first_a = a["logs"]["prims"][:, 0]
     first_b = b["logs"]["prims"][:, 0]
     np.testing.assert_array_equal(first_a, first_b)
+
+
+def test_hero_bundle_band_weights(L, oracle):
+    """Hero bundles under the band policy: C wavelengths from one variate, stratified as
+    hero.h:100-113 does (u + i/C wrapped into [0, 1)), each carrying power/C times its own
+    band weight; with no bounces the emitted tally is their sum, photon by photon."""
+    desc = scenes.make_cornell(L)
+    cam = cases.camera(L, 32)
+    n, first, C = 1000, 999, 4
+    out = oracle.trace(desc, cam, n, seed_base=first, max_bounce=0, threads=1, hero_c=C,
+                       lambda_mode=abi.LAMBDA_UNIFORM_380_780)
+    em = desc.emitters[0]
+    cdf = desc.emitter_cdf[em.cdf_offset: em.cdf_offset + em.cdf_n + 1]
+
+    def weight(u):
+        lam = 380.0 + 400.0 * u
+        b = min(max(int((lam - 360.0) / em.step), 0), em.cdf_n - 1)
+        return (cdf[b + 1] - cdf[b]) / em.step * 400.0
+
+    expect = 0.0
+    for k in range(first, first + n):
+        u = oracle.uniforms(k, 5)[4]
+        w = [weight(u)]
+        for i in range(1, C):
+            uu = u + i / C
+            if uu >= 1.0:
+                uu -= 1.0
+            w.append(weight(uu))
+        if not w[0] > 0.0:
+            continue
+        s = 0.0
+        for wi in w:
+            s += em.power * 1.0 / C * wi
+        expect += s
+    assert out["energy"][0] == expect

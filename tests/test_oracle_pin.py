@@ -106,3 +106,55 @@ def test_closest_hit_known_answers(oracle, reference, L):
     finally:
         oracle.L.fto_release(octx)
         reference.L.ftr_release(rctx)
+
+
+def test_curve_and_occlusion_known_answers(oracle, reference, L):
+    """Modelled on the reference's -checkcurve (main.cpp:565-903) and -checkfog
+    (main.cpp:2730): rays aimed into the strand ball of the fog + strands scene (round cones
+    among the box's triangles); the closest hit's distance and material, and occlusion of
+    random segments, must agree with the reference's own Scene::closestHit / occluded."""
+    import ctypes as C
+    d = scenes.make_fog_strands(L, n_strands=3000)
+    nt, ns = len(d.tri_mat), len(d.sph_mat)
+
+    def mat_of(p):
+        if p < nt:
+            return int(d.tri_mat[p])
+        if p < nt + ns:
+            return int(d.sph_mat[p - nt])
+        return int(d.curve_mat[p - nt - ns])
+
+    octx = oracle.prepare(d)
+    rctx = reference.prepare(d)
+    rng = np.random.default_rng(11)
+    roots = d.curve[:, :3]
+    curve_hits = 0
+    try:
+        for i in range(2000):
+            o = rng.uniform(0.05, 1.95, 3)
+            target = roots[rng.integers(len(roots))] + rng.normal(scale=0.002, size=3)
+            dv = target - o
+            dv /= np.linalg.norm(dv)
+            m, t = reference.closest_hit(rctx, o, dv)
+            to = np.zeros(1)
+            p = oracle.L.fto_closest_hit(octx, o.ctypes.data_as(C.POINTER(C.c_double)),
+                                         dv.ctypes.data_as(C.POINTER(C.c_double)), 1e-6,
+                                         to.ctypes.data_as(C.POINTER(C.c_double)))
+            if m < 0:
+                assert p < 0
+                continue
+            assert to[0] == t, (i, to[0], t)
+            assert mat_of(p) == m
+            curve_hits += p >= nt + ns
+            # occlusion of the segment up to just before / after the hit
+            for frac, expect in ((0.5, 0), (1.5, 1)):
+                dist = t * frac
+                occ_ref = reference.L.ftr_occluded(rctx, o.ctypes.data_as(C.POINTER(C.c_double)),
+                                                   dv.ctypes.data_as(C.POINTER(C.c_double)), dist)
+                occ_or = oracle.L.fto_occluded(octx, o.ctypes.data_as(C.POINTER(C.c_double)),
+                                               dv.ctypes.data_as(C.POINTER(C.c_double)), dist, 1e-6)
+                assert occ_ref == occ_or == expect, (i, frac, occ_ref, occ_or)
+        assert curve_hits > 300
+    finally:
+        oracle.L.fto_release(octx)
+        reference.L.ftr_release(rctx)

@@ -197,6 +197,8 @@ def run_reference_arm(args):
         return
     from goodphotons_b200 import lib, scenes
     cfg, res, _, mb = workload_config(args)
+    if lambda_mode(args):   # the reference can only draw from the SPD
+        cfg["lambda"] = "sampled from the emitter SPD over 360-830 nm (the reference has no uniform-band policy)"
     L = lib.load()
     desc = make_scene(args.workload, args.level, L)
     cam = scenes.default_camera(L, res)

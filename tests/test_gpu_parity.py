@@ -216,3 +216,19 @@ def test_uniform_band_policy_matches_oracle(name, hero, scenes_cache, gpu, oracl
     # the policy changes the film: the SPD-sampled render of the same photons differs
     film_spd, _, _ = sc.render(cam, n, seed_base=seed, max_bounce=mb, hero_c=hero)
     assert not np.array_equal(film_spd, film)
+
+
+@pytest.mark.parametrize("rx,ry,n,mb", [(37, 23, 20_000, 8), (1, 1, 5_000, 8), (64, 48, 20_000, 0),
+                                        (24, 24, 1, 8), (24, 24, 0, 8)])
+def test_ragged_and_tiny_renders_match_oracle(rx, ry, n, mb, scenes_cache, gpu, oracle):
+    """Odd, non-square and one-pixel films, a one-photon and an empty render, and no
+    bounces (emission splats only): film and energy equal the oracle's."""
+    d, sc = scenes_cache["cornell"]
+    cam = gpu.look_at((1.0, 1.0, 5.4), (1.0, 1.0, 1.0), (0.0, 1.0, 0.0), 40.0, rx, ry)
+    film, info, en = sc.render(cam, n, seed_base=4242, max_bounce=mb)
+    o = oracle.trace(d, cam, n, seed_base=4242, max_bounce=mb, threads=1)
+    assert film.shape == (ry, rx, 4)
+    assert_film_close(film, info, o["xyz"], o["hits"])
+    np.testing.assert_allclose(en.as_list(), o["energy"], rtol=1e-9, atol=0)
+    if n == 0:
+        assert not film.any() and not any(en.as_list())

@@ -98,3 +98,20 @@ def test_hero_bundle_band_weights(L, oracle):
             s += em.power * 1.0 / C * wi
         expect += s
     assert out["energy"][0] == expect
+
+
+@pytest.mark.parametrize("hero", [1, 4])
+def test_band_policy_conserves_energy(L, oracle, hero):
+    """Under the band policy every photon's weight flows through its path like the power it
+    replaces: absorbed + sensor + escaped + residual equals emitted (EnergyReport's
+    sum/emitted == 1 check, main.cpp:13693-13696) -- photon by photon for one wavelength;
+    for bundles only in expectation, as under the SPD policy, because a dielectric drops the
+    secondary wavelengths and scales the hero by C (hero.h:28-70)."""
+    desc = scenes.make_glass(L, level=2)
+    cam = cases.camera(L, 32)
+    out = oracle.trace(desc, cam, 20_000, seed_base=3, max_bounce=16, threads=2, hero_c=hero,
+                       lambda_mode=abi.LAMBDA_UNIFORM_380_780)
+    emitted, absorbed, sensor, escaped, residual = out["energy"]
+    assert emitted > 0
+    tol = 1e-9 if hero == 1 else 1e-2
+    assert abs(absorbed + sensor + escaped + residual - emitted) <= tol * emitted

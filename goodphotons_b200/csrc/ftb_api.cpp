@@ -1009,11 +1009,42 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     std::string err;
     const ftb::BuildMethod method = d->build == FTB_BUILD_DEVICE ? ftb::BuildMethod::kDeviceLbvh
                                                                  : ftb::BuildMethod::kHostSah;
-    if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err, method, device)) {
-        delete s;
-        return fail(FTB_ERR_INVALID, err);
+    // Scenes with both curves and other primitives (and no instances) get two hierarchies,
+    // one over the curves and one over the rest, stored one after the other; a closest-hit
+    // or occlusion walk covers both with the shared t bound, so each walk tests one kind of
+    // record and the lanes of a warp stay on one code path.
+    const int64_t n_other = nt + ns;
+    const bool split = nc > 0 && n_other > 0 && ni == 0;
+    int32_t root2 = -1;
+    if (split) {
+        ftb::WideBvh a, b;
+        std::vector<ftb::Box> ba(boxes.begin(), boxes.begin() + n_other), bb(boxes.begin() + n_other, boxes.end());
+        if (!ftb::build_wide_bvh(ba, margin, a, err, method, device) ||
+            !ftb::build_wide_bvh(bb, margin, b, err, method, device)) {
+            delete s;
+            return fail(FTB_ERR_INVALID, err);
+        }
+        if (!ftb::validate_wide_bvh(a, (int)n_other, err) || !ftb::validate_wide_bvh(b, (int)nc, err)) {
+            delete s;
+            return fail(FTB_ERR_INVALID, "BVH check: " + err);
+        }
+        const uint32_t node_shift = (uint32_t)a.nodes.size(), rec_shift = (uint32_t)a.order.size();
+        root2 = (int32_t)node_shift;
+        bvh.nodes = std::move(a.nodes);
+        bvh.order = std::move(a.order);
+        for (WNode nd : b.nodes) {   // child and record indices of the second tree move up
+            nd.child_base += node_shift;
+            nd.prim_base += rec_shift;
+            bvh.nodes.push_back(nd);
+        }
+        for (int p : b.order) bvh.order.push_back(p + (int)n_other);
+    } else {
+        if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err, method, device)) {
+            delete s;
+            return fail(FTB_ERR_INVALID, err);
+        }
+        if (np > 0 && !ftb::validate_wide_bvh(bvh, (int)np, err)) { delete s; return fail(FTB_ERR_INVALID, "BVH check: " + err); }
     }
-    if (np > 0 && !ftb::validate_wide_bvh(bvh, (int)np, err)) { delete s; return fail(FTB_ERR_INVALID, "BVH check: " + err); }
     if (np == 0) {   // an empty root with no children
         bvh.nodes.resize(1);
         std::memset(&bvh.nodes[0], 0, sizeof(WNode));
@@ -1079,6 +1110,7 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
         UP(bvh.nodes.data(), bvh.nodes.size(), &dn, "upload nodes");
     }
     D.nodes = dn; D.recs = dr;
+    D.root2 = root2;
     if (any_smooth) UP(d->tri_n, (size_t)nt * 9, &D.tri_n, "upload normals");
     UP(spec.data(), spec.size(), &D.spec, "upload spectra");
     UP(d->table_w, (size_t)d->n_table, &D.tw, "upload tables");

@@ -553,9 +553,10 @@ struct LocalStack {
 // leaf's records and returns the (possibly lowered) fp32 bound on t.
 template <bool COUNT, class Stack, class Leaf>
 __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, const RayF& F, float tmin_f,
-                                              float tmax_f, Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt) {
+                                              float tmax_f, Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt,
+                                              uint32_t root = 0) {
     int sp = 0;
-    uint32_t cur = 0;
+    uint32_t cur = root;
     bool live = true;
     while (live) {
         while (!(cur & LEAF_BIT)) {
@@ -614,9 +615,10 @@ __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, c
 // leaves first; leaf(first, count) returns true on a hit, which ends the walk.
 template <bool COUNT, class Stack, class Leaf>
 __device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const RayF& F, float tmin_f, float tmax_f,
-                                         Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt) {
+                                         Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt,
+                                         uint32_t root = 0) {
     int sp = 0;
-    uint32_t cur = 0;
+    uint32_t cur = root;
     bool live = true;
     while (live) {
         while (!(cur & LEAF_BIT)) {
@@ -758,7 +760,9 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
         return tm;
     };
     LocalStack<uint2> st;
-    walk_closest<COUNT>(sc.nodes, F, __double2float_rd(tmin), FLT_MAX, st, leaf, status, cnt);
+    const float tm = walk_closest<COUNT>(sc.nodes, F, __double2float_rd(tmin), FLT_MAX, st, leaf, status, cnt);
+    if (SHAPES && sc.root2 > 0)   // the curves' hierarchy, under the bound the first walk left
+        walk_closest<COUNT>(sc.nodes, F, __double2float_rd(tmin), tm, st, leaf, status, cnt, (uint32_t)sc.root2);
     return best;
 }
 
@@ -785,7 +789,9 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
         return false;
     };
     LocalStack<uint32_t> st;
-    return walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt);
+    if (walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt)) return true;
+    return SHAPES && sc.root2 > 0 &&
+           walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt, (uint32_t)sc.root2);
 }
 
 // Hit on BLAS record `sub` of instance I, in world terms: the local hit's attributes

@@ -97,6 +97,8 @@ struct DevScene {
     const DevMed* med;
     const DevInst* inst;
     int32_t n_nodes, n_recs, n_mats, n_emit, n_med, n_spec;
+    int32_t root2;            // second hierarchy (the curves') in nodes, or -1
+    int32_t pad2;
     int64_t n_tris;
     int64_t n_inst;
     double total_power;

@@ -673,6 +673,9 @@ def main():
         "bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
         "traffic": (round(traffic_ray * units_timed / launches_k) if traffic_ray else None),
+        "traffic_source": (f"transcribed, not measured in this run: ncu dram bytes per ray from "
+                           f"profiles/k_extend_{args.workload}.md (a smaller capture of the same kernel) "
+                           f"x this run's rays per launch" if traffic_ray else None),
         "peak_source": f"{peak_kind} hbm_gbs (copy)",
         "algorithmic_bytes_per_unit": round(unit_bytes, 1),
         "algorithmic_bytes_per_ray": round(bytes_per_ray, 1),

@@ -181,3 +181,4 @@ EXPORTS = [
     "ftb_server_get_stats", "ftb_server_destroy", "ftb_get_tuning", "ftb_set_tuning", "ftb_autotune",
 ]
 NOALLOC_MAX_PHOTONS = 32768
+NOALLOC_SCRATCH_BYTES = 21060864

@@ -73,10 +73,17 @@ def build(verbose=False, force=False):
     return LIB
 
 
-def build_oracle(verbose=False):
-    """The CPU checkers under oracle/ (test infrastructure)."""
+def build_oracle(verbose=False, reference=None):
+    """The CPU checkers under oracle/ (test infrastructure).  `reference` (or the
+    FTB_REFERENCE environment variable) names a checkout of the reference, whose headers
+    the reference-built checkers under oracle/_ref are compiled from; without one only the
+    plain-C restatement is built."""
     root = os.path.dirname(PKG)
-    _run(["make", "-s", "-C", os.path.join(root, "oracle")], verbose)
+    ref = reference or os.environ.get("FTB_REFERENCE", "")
+    cmd = ["make", "-s", "-C", os.path.join(root, "oracle")]
+    if ref:
+        cmd.append(f"REF={ref}")
+    _run(cmd, verbose)
 
 
 if __name__ == "__main__":

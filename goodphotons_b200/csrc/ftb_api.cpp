@@ -822,6 +822,11 @@ void energy_from_tally(const unsigned long long* fx, double power, ftb_energy* e
     tally_to_energy(fx, power, e, false);
 }
 
+ftb_status check_render_params(const ftb_scene* s, const ftb_camera* cam, const ftb_render_params* p) {
+    return check_params(s, cam, p);
+}
+std::mutex& scene_mutex(const ftb_scene* s) { return s->eng->mu; }
+
 bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power) {
     if (!s) return false;
     *dev = s->dev;

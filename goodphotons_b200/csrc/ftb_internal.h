@@ -3,6 +3,7 @@
 #pragma once
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 
 #include "../../include/ftb200.h"
@@ -11,6 +12,12 @@
 namespace ftb {
 // The device view of a scene and where it lives; false for a null scene.
 bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power);
+// The checks every render entry point applies to its arguments (null pointers, camera
+// resolution, photon count, bounce cap, film format, wavelength policy, emitted power);
+// FTB_OK or the error, with its text set.
+ftb_status check_render_params(const ftb_scene* s, const ftb_camera* cam, const ftb_render_params* p);
+// The mutex the scene's device engine holds while a render of it is being issued.
+std::mutex& scene_mutex(const ftb_scene* s);
 // The text ftb_last_error() returns (thread-local).
 void set_last_error(const std::string& m);
 // The default film format for an n-photon render: 62 - ceil(log2 n) - 20 in [4, 40].

@@ -9,12 +9,18 @@
 // only launches kernels and issues async memsets on the caller's stream.
 //
 // Its scratch -- the path state, queues and shadow records of one wave of photons, plus the
-// energy tallies and the status word -- lives in one file-scope __device__ array of
-// kNoAllocBytes (about 10 MB for kNoAllocPhotons = 32768 slots), which every GPU that loads
-// the library holds until the process exits.  Host code cannot use the array's name as a
-// device address (it is a host-side stand-in), so the first call on each device, with that
-// device current, resolves it with cudaGetSymbolAddress; make that first call before any
-// stream capture.
+// energy tallies and the status word -- lives in one file-scope __device__ array of exactly
+// FTB_NOALLOC_SCRATCH_BYTES (21,060,864 B, 20.1 MiB, for FTB_NOALLOC_MAX_PHOTONS = 32768
+// slots), which every GPU that loads the library holds until the process exits.  Host code
+// cannot use the array's name as a device address (it is a host-side stand-in), so the
+// first call on each device, with that device current, resolves it with
+// cudaGetSymbolAddress; make that first call before any stream capture.
+//
+// A call issues one staging kernel (the job table, launch parameters, zeroed tallies and
+// status word, all passed as kernel arguments) and the wave's kernels on the caller's
+// stream; it copies nothing from host memory.  Every call shares the one array and leaves
+// its contents behind, so the staging kernel clears what must start at zero, and calls that
+// overlap on the GPU race.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -36,6 +42,8 @@ constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
 constexpr size_t kWaveBytes = ftb::wave_bytes(kNoAllocPhotons, false);
 constexpr size_t kNoAllocBytes = kWaveBytes + al(8 * sizeof(unsigned long long)) + al(64);
+static_assert(kNoAllocPhotons == FTB_NOALLOC_MAX_PHOTONS, "photon limit out of step with ftb200.h");
+static_assert(kNoAllocBytes == FTB_NOALLOC_SCRATCH_BYTES, "scratch size out of step with ftb200.h");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -45,6 +53,21 @@ void* g_scratch_addr[256] = {};   // per device, resolved once
 ftb_status na_fail(ftb_status s, const std::string& m) {
     ftb::set_last_error(m);
     return s;
+}
+
+// Stream-ordered staging of one call: the one-job table and the wave parameters {jobs,
+// slots} arrive as kernel arguments (no host memory is read), the five energy tallies and
+// the status word are cleared.  One block of 32 threads.
+__global__ void k_noalloc_stage(ftb::DevJob job, ftb::DevJob* jobs, int32_t* params, unsigned long long* tally,
+                                int32_t* status) {
+    const int t = threadIdx.x;
+    if (t == 0) {
+        jobs[0] = job;
+        params[0] = 1;
+        params[1] = job.n;
+    }
+    if (t < 8) tally[t] = 0;
+    if (t < 16) status[t] = 0;
 }
 
 
@@ -57,21 +80,24 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     DevScene dev;
     int device = 0, sms = 0;
     double power = 0.0;
-    if (!scene || !cam || !p || !d_film) return na_fail(FTB_ERR_INVALID, "null argument");
+    if (!d_film) return na_fail(FTB_ERR_INVALID, "null film");
+    ftb_status chk = ftb::check_render_params(scene, cam, p);   // the same checks as every render call
+    if (chk != FTB_OK) return chk;
     if (!ftb::scene_internals(scene, &dev, &device, &sms, &power)) return na_fail(FTB_ERR_INVALID, "bad scene");
-    if (p->n_photons < 0 || p->max_bounce < 0 || p->max_bounce > 1024 || p->frac_bits > 56 ||
-        cam->res_x <= 0 || cam->res_y <= 0 ||
-        (p->lambda_mode != FTB_LAMBDA_SPD && p->lambda_mode != FTB_LAMBDA_UNIFORM_380_780))
-        return na_fail(FTB_ERR_INVALID, "bad render parameters");
+    // Bundles: the scratch holds one wavelength per path, so hero_c > 1 is refused -- except
+    // in scenes with media, where every render path traces one wavelength per photon
+    // whatever hero_c says (the reference's tracer ignores -heroc there too), so the call
+    // goes ahead as hero_c = 1.
     if (p->hero_c > 1 && dev.n_med == 0)
         return na_fail(FTB_ERR_UNSUPPORTED, "ftb_render_forward_noalloc traces one wavelength per photon "
                                             "(its scratch holds no bundles); use hero_c <= 1");
     if (p->n_photons > kNoAllocPhotons)
         return na_fail(FTB_ERR_TOO_LARGE, "ftb_render_forward_noalloc: at most " + std::to_string(kNoAllocPhotons) +
                                               " photons per call (its scratch is a fixed device array); "
-                                              "split the render into calls with consecutive seed_base");
-    if (!(power > 0.0)) return na_fail(FTB_ERR_UNSUPPORTED, "scene emits no power");
+                                              "split the render into calls with consecutive seed_base and one "
+                                              "explicit frac_bits");
     if (device < 0 || device >= 256) return na_fail(FTB_ERR_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> scene_lock(ftb::scene_mutex(scene));
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != device) cudaSetDevice(device);
@@ -98,7 +124,7 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     ftb::Frame f;
     f.stats = nullptr;
     f.status = status;
-    ftb::DevJob J;   // the one-job table, staged from this pageable stack copy
+    ftb::DevJob J;   // the one-job table, passed to the staging kernel by value
     std::memset(&J, 0, sizeof J);
     J.sc = dev;
     for (int i = 0; i < 3; ++i) {
@@ -115,11 +141,8 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     J.max_bounce = p->max_bounce;
     J.lambda_mode = p->lambda_mode;
     ftb_status out = FTB_OK;
-    cudaError_t e = cudaMemsetAsync(tally, 0, 8 * sizeof(unsigned long long), st);   // tallies start at zero
-    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 64, st);
-    const int32_t params[2] = {1, (int32_t)p->n_photons};   // one job, its photons' slots
-    if (e == cudaSuccess) e = cudaMemcpyAsync(w.jobs, &J, sizeof J, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(w.params, params, sizeof params, cudaMemcpyHostToDevice, st);
+    k_noalloc_stage<<<1, 32, 0, st>>>(J, w.jobs, w.params, tally, status);
+    cudaError_t e = cudaGetLastError();
     ftb::LaunchShape shape;
     shape.graph = false;
     ftb::WaveKind kind;

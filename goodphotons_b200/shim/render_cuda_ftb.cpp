@@ -3,8 +3,8 @@
 //
 // Compile this file inside the reference tree (it includes the reference's scene.h,
 // camera.h, render.h and render_cuda.h) and link libftb200.so; the reference's own
-// definitions of the same functions in render_cuda.cu are then excluded (see
-// INTEGRATION.md).  The signatures are the reference's; the behaviour differs only where
+// definitions of the same functions in render_cuda.cu are then excluded (the build
+// compiles this file in place of render_cuda.cu).  The signatures are the reference's; the behaviour differs only where
 // the reference calls exit(): here a failed CUDA call prints the C ABI's error and returns
 // an empty film, like the reference's "unsupported scene" path.
 //

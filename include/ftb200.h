@@ -394,17 +394,27 @@ ftb_status ftb_trace_log(ftb_scene* scene, const ftb_camera* cam,
  * allocation inside their render callbacks (engine / DCC plug-in hosts with their own
  * allocator), frame loops that must not allocate once running, and code for which a
  * cudaMalloc or cudaFree would synchronize the device mid-stream.  Create the scene once at
- * start-up (ftb_scene_create allocates); then this call only launches kernels and async
- * memsets on `stream`, accumulating into the caller's DEVICE film like
- * ftb_render_forward_device.  Its scratch (one wave of path state, queues, shadow records,
- * tallies and status: ~16.5 MB) is a fixed device array in the library, held by every GPU
- * that loads the library until exit.  Limit: n_photons <= FTB_NOALLOC_MAX_PHOTONS per call
- * (larger requests return FTB_ERR_TOO_LARGE; render more with consecutive seed_base).  The
- * first call on a device resolves the array's device address (cudaGetSymbolAddress) with
- * that device current: make it before any stream capture.  All calls share the one array,
- * so calls that overlap on the GPU (other streams, other threads) race; serialize them.
- * energy != NULL synchronizes `stream` and also checks the device status word. */
+ * start-up (ftb_scene_create allocates); then this call only launches kernels on `stream`
+ * (a staging kernel that takes the job as kernel arguments, then the wave's kernels),
+ * accumulating into the caller's DEVICE film like ftb_render_forward_device.  Its scratch
+ * (one wave of path state, queues, shadow records, tallies and status) is a fixed device
+ * array of exactly FTB_NOALLOC_SCRATCH_BYTES in the library, held by every GPU that loads
+ * the library until exit.
+ *  - Limit: n_photons <= FTB_NOALLOC_MAX_PHOTONS per call; larger requests return
+ *    FTB_ERR_TOO_LARGE.  Render more with calls of consecutive seed_base, all passing one
+ *    explicit frac_bits (e.g. the default for the total photon count): with frac_bits <= 0
+ *    each call picks the default for its own n_photons, and calls of different sizes would
+ *    add to the film at different scales.
+ *  - The first call on a device resolves the array's device address (cudaGetSymbolAddress)
+ *    with that device current: make it before any stream capture.
+ *  - All calls share the one array, which keeps the last call's contents (the call clears
+ *    what must start at zero), so calls that overlap on the GPU (other streams, other
+ *    threads) race; serialize them.
+ *  - hero_c > 1 is refused (FTB_ERR_UNSUPPORTED) in scenes without media; in scenes with
+ *    media every entry point traces one wavelength per photon and so does this one.
+ *  - energy != NULL synchronizes `stream` and also checks the device status word. */
 #define FTB_NOALLOC_MAX_PHOTONS 32768
+#define FTB_NOALLOC_SCRATCH_BYTES 21060864
 ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_camera* cam,
                                       const ftb_render_params* params, int64_t* d_film,
                                       ftb_film_info* info, ftb_energy* energy, void* stream);

@@ -93,3 +93,12 @@ def test_invalid_arguments_are_reported_not_fatal(L):
     st = L.L.ftb_emission_cdf(C.byref(s), None, None, 1.0, cdf.ctypes.data_as(C.POINTER(C.c_double)), 4,
                               C.byref(n), C.byref(integ))
     assert st == 1 and "small" in L.L.ftb_last_error().decode()
+
+
+def test_header_constants_match_binding():
+    """The no-allocation limits the header states are the binding's (the library itself
+    checks its scratch array against the header's size at compile time)."""
+    src = open(HEADER).read()
+    get = lambda name: int(re.search(rf"#define {name} (\d+)", src).group(1))
+    assert get("FTB_NOALLOC_MAX_PHOTONS") == abi.NOALLOC_MAX_PHOTONS
+    assert get("FTB_NOALLOC_SCRATCH_BYTES") == abi.NOALLOC_SCRATCH_BYTES

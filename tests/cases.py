@@ -70,6 +70,19 @@ CASES = {
 }
 
 
+# The benchmark configurations at their own size: scene, film, bounce cap.  The photon
+# count is the golden vectors' (the per-photon tests trace 2^15).
+CONFIG_CASES = {
+    # dispersive caustics: level-7 (327,680 triangles) and level-8 (1,310,720) glass, 1024^2
+    "cfg_glass_l7": (lambda L: scenes.make_glass(L, level=7), 1024, 2048, 16, 0, 1),
+    "cfg_glass_l8": (lambda L: scenes.make_glass(L, level=8), 1024, 2048, 16, 1 << 40, 1),
+    # fog + 250k strands (1M round cones), 512^2, 32 bounces
+    "cfg_fog_strands": (lambda L: scenes.make_fog_strands(L, n_strands=250_000), 512, 2048, 32, 77, 1),
+    # the Cornell box at 256^2, 8 bounces
+    "cfg_cornell": (lambda L: scenes.make_cornell(L), 256, 4096, 8, 5, 1),
+}
+
+
 def camera(L, res):
     return scenes.default_camera(L, res)
 

@@ -4,7 +4,8 @@ Run where the reference sources are available (they are read only at build time)
     make -C oracle            # builds oracle/_ref/libftref.so from the reference headers
     python tests/golden/make_golden.py [case ...]   # all cases when none is named
 
-For every case in tests/cases.py it stores, from Renderer::tracePhoton run single-threaded
+For every case in tests/cases.py (the small cases and the benchmark configurations at their
+own scene and film size) it stores, from Renderer::tracePhoton run single-threaded
 with the reference's per-photon seeding (hero-wavelength cases through tracePhotonHero):
 the energy report, the film (XYZ sums and hits), and per photon the number of ray queries,
 the termination and the final beta (the last two meaningful for one wavelength per photon).  It also
@@ -29,7 +30,7 @@ def main():
     L = lib.load()
     R = Reference()
     only = set(sys.argv[1:])
-    for name, (mk, res, n, mb, seed, hero) in cases.CASES.items():
+    for name, (mk, res, n, mb, seed, hero) in {**cases.CASES, **cases.CONFIG_CASES}.items():
         if only and name not in only:
             continue
         d = mk(L)

@@ -49,9 +49,13 @@ def test_emission_cdf_and_power(oracle, L):
     assert ointeg == float(g["bb_integral"])
 
 
-@pytest.mark.parametrize("name", sorted(cases.CASES))
+ALL_CASES = {**cases.CASES, **cases.CONFIG_CASES}
+
+
+@pytest.mark.parametrize("name", sorted(ALL_CASES))
 def test_trace_matches_golden(name, oracle, L):
-    mk, res, n, mb, seed, hero = cases.CASES[name]
+    """Small cases and the benchmark configurations at their own scene and film size."""
+    mk, res, n, mb, seed, hero = ALL_CASES[name]
     g = golden(f"trace_{name}.npz")
     d = mk(L)
     assert cases.scene_hash(d) == str(g["scene_hash"]), "scene generator drifted from the golden scene"

@@ -358,6 +358,7 @@ struct ftb_session {
     unsigned long long* tally = nullptr;
     int32_t max_bounce = 32;
     int32_t frac_bits = 0;
+    int32_t hero_c = 1;              // wavelengths per photon (bundles of every camera's paths)
 };
 
 namespace {
@@ -1554,7 +1555,7 @@ ftb_status ftb_autotune(ftb_scene* s, const ftb_camera* cam, int64_t n, int32_t 
 }
 
 ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cams, int32_t max_bounce,
-                             int32_t frac_bits, ftb_session** out) {
+                             int32_t frac_bits, int32_t hero_c, ftb_session** out) {
     if (!s || !cams || n_cams < 1 || !out) return fail(FTB_ERR_INVALID, "bad session arguments");
     if (max_bounce < 0 || max_bounce > 1024) return fail(FTB_ERR_INVALID, "max_bounce out of range");
     DeviceGuard guard(s->device);
@@ -1562,6 +1563,7 @@ ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cam
     ss->scene = s;
     ss->max_bounce = max_bounce;
     ss->frac_bits = frac_bits > 0 ? frac_bits : default_frac_bits((int64_t)1 << 36);
+    ss->hero_c = effective_hero(s, hero_c);
     for (int c = 0; c < n_cams; ++c) {
         if (cams[c].res_x <= 0 || cams[c].res_y <= 0) { delete ss; return fail(FTB_ERR_INVALID, "bad camera"); }
         ss->cams.push_back(cams[c]);
@@ -1599,7 +1601,7 @@ ftb_status ftb_session_batch(ftb_session* ss, int64_t n, uint64_t seed_base) {
     CK(cudaMemset(s->eng->status, 0, 64), "memset status");
     // One shared pass (the multi-camera shared splat, render_cuda.cu:13873-13895): every
     // path vertex connects to each camera; the paths are traced once.
-    ftb::DevJob J = make_job(s, &ss->cams[0], ss->films[0], ss->tally, ss->frac_bits, ss->max_bounce);
+    ftb::DevJob J = make_job(s, &ss->cams[0], ss->films[0], ss->tally, ss->frac_bits, ss->max_bounce, ss->hero_c);
     J.views = ss->views;
     J.n_views = (int32_t)ss->cams.size();
     st = run_jobs(s, {J}, {n}, {seed_base}, false, nullptr, 0, nullptr);

@@ -38,6 +38,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include <float.h>
+#include <limits.h>
 #include <stdint.h>
 
 #include "ftb_kernels.h"
@@ -684,11 +685,23 @@ __device__ __forceinline__ LocalRay to_local(const DevInst& I, D3 o, D3 d) {
     return L;
 }
 
-// Blas::intersectLocal (scene.h:1017-1026): nearest BLAS triangle with t < best_t; updates
-// best_t / tmax_f and returns the BLAS record, or -1.
+// The next double above a positive t (DBL_MAX -> +inf): record tests given this bound accept
+// t <= best, so that an exact tie can be settled by primitive index.
+__device__ __forceinline__ double next_up(double t) { return __longlong_as_double(__double_as_longlong(t) + 1); }
+
+// Exact ties in t go to the lower primitive index (world index first, then the index within
+// the BLAS).  The reference takes the first tied primitive its own hierarchy happens to
+// test; with the index rule a closest hit does not depend on the hierarchy at all, and the
+// oracle applies the same rule.
+struct BestHit { int prim, sub_prim; };
+
+// Blas::intersectLocal (scene.h:1017-1026): nearest BLAS triangle with t <= best_t that wins
+// against the current best (ties by index); updates best_t / tmax_f / bh and returns the BLAS
+// record, or -1.  `inst_prim` is the instance's world primitive index.
 template <bool COUNT>
 __device__ __noinline__ int blas_closest(const DevInst& I, D3 wo, D3 wd, double tmin, double& best_t,
-                                         float& tmax_f, int32_t* status, TravCount& cnt) {
+                                         float& tmax_f, int inst_prim, BestHit& bh, int32_t* status,
+                                         TravCount& cnt) {
     const LocalRay L = to_local(I, wo, wd);
     const Shear sh = make_shear(L.d);
     const RayF F = make_rayf(L.o, L.d);
@@ -700,8 +713,10 @@ __device__ __noinline__ int blas_closest(const DevInst& I, D3 wo, D3 wd, double 
             PrimRec r;
             load_rec(recs, first + k, r);
             double t;
-            if (tri_test(sh, L.o, r.d, tmin, best_t, t, nullptr)) {
+            if (tri_test(sh, L.o, r.d, tmin, next_up(best_t), t, nullptr) &&
+                (t < best_t || inst_prim < bh.prim || (inst_prim == bh.prim && r.prim < bh.sub_prim))) {
                 best_t = t; best = first + k; tm = __double2float_ru(t);
+                bh.prim = inst_prim; bh.sub_prim = r.prim;
             }
         }
         return tm;
@@ -742,6 +757,7 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
     const RayF F = make_rayf(R.o, R.d);
     best_t = DBL_MAX;
     int best = -1;
+    BestHit bh{INT_MAX, INT_MAX};
     const PrimRec* __restrict__ recs = sc.recs;
     auto leaf = [&](int first, int count, float tm) -> float {
         for (int k = 0; k < count; ++k) {
@@ -749,13 +765,17 @@ __device__ int traverse_closest(const DevScene& sc, const RayCtx& R, double tmin
             PrimRec r;
             load_rec(recs, first + k, r);
             if (INST && rec_type(r) == REC_INST) {
-                int s = blas_closest<COUNT>(sc.inst[rec_inst(r)], R.o, R.d, tmin, best_t, tm, status, cnt);
+                int s = blas_closest<COUNT>(sc.inst[rec_inst(r)], R.o, R.d, tmin, best_t, tm, r.prim, bh, status, cnt);
                 if (s >= 0) { best = first + k; *sub = s; }
                 continue;
             }
             if (COUNT) cnt.exact++;
             double t;
-            if (rec_test<SHAPES>(R, r, tmin, best_t, t)) { best_t = t; best = first + k; tm = __double2float_ru(t); }
+            // t <= best_t from the test; a tie goes to the lower index
+            if (rec_test<SHAPES>(R, r, tmin, next_up(best_t), t) && (t < best_t || r.prim < bh.prim)) {
+                best_t = t; best = first + k; tm = __double2float_ru(t);
+                bh.prim = r.prim; bh.sub_prim = INT_MAX;
+            }
         }
         return tm;
     };

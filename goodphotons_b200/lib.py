@@ -60,7 +60,7 @@ def load(path=None):
          C.POINTER(abi.RenderParams), C.c_void_p, C.POINTER(abi.FilmInfo),
          C.POINTER(abi.Energy), C.c_void_p)
     _sig(L, "ftb_session_begin", st, PS, C.POINTER(abi.Camera), C.c_int32, C.c_int32,
-         C.c_int32, C.POINTER(PS))
+         C.c_int32, C.c_int32, C.POINTER(PS))
     _sig(L, "ftb_session_batch", st, PS, C.c_int64, C.c_uint64)
     _sig(L, "ftb_session_hits0", st, PS, C.POINTER(C.c_double))
     _sig(L, "ftb_session_download", st, PS, C.c_int32, C.POINTER(C.c_int64),

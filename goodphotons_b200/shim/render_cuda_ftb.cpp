@@ -13,15 +13,24 @@
 //  - triangles, spheres and curve segments are copied verbatim (double precision);
 //  - emitters pass their own EmissionSampler CDF and power, so wavelength sampling is
 //    bit-identical to the CPU tracer;
-//  - material / medium spectra are std::function values that cannot be inspected: a
-//    spectrum that is constant over [360, 830] nm becomes FTB_SPEC_CONST (exact), any
-//    other is tabulated at kTableStep nm and interpolated linearly (exact only for
-//    piecewise-linear spectra with breakpoints on that grid).
+//  - material / medium spectra arrive as std::function values.  A spectrum made by one of
+//    the reference's closed-form builders -- cauchy, sellmeier, tabulatedSpectrum
+//    (spectrum.h:128-175) -- is baked as that form with the builder's own parameters
+//    (FTB_SPEC_CAUCHY / SELLMEIER / TABLE), so the device evaluates it with the same
+//    arithmetic at every wavelength; a spectrum constant over [360, 830] nm becomes
+//    FTB_SPEC_CONST.  Every such bake is checked against the original, bit for bit, at
+//    ~3000 wavelengths before it is used.  Any other spectrum (or one whose check fails)
+//    is tabulated at kTableStep nm and interpolated linearly, which is exact only for
+//    piecewise-linear spectra with breakpoints on that grid.
 //  - maxBounce: the reference's GPU path ignores -max-bounce and uses 32
 //    (render_cuda.cu:13702); g_ftbMaxBounce keeps that default and can be set by the
 //    caller to honour the CLI value like the CPU path does.
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <typeinfo>
+#include <utility>
 #include <vector>
 
 #include "render.h"
@@ -66,16 +75,159 @@ struct Baked {
     std::string why;
 };
 
+// ---- exact spectra -------------------------------------------------------------------
+// The device's evaluation of each form (spec_eval in the kernels: the reference's own
+// expressions, spectrum.h:128-175), restated here so a candidate can be checked on the host.
+double eval_form(const ftb_spectrum& f, const std::vector<double>& tw, const std::vector<double>& tv, double w) {
+    switch (f.kind) {
+    case FTB_SPEC_CONST: return f.p[0];
+    case FTB_SPEC_CAUCHY: { double um = w * 1e-3; return f.p[0] + f.p[1] / (um * um); }
+    case FTB_SPEC_SELLMEIER: {
+        double l2 = (w * 1e-3) * (w * 1e-3);
+        double n2 = 1.0 + f.p[0] * l2 / (l2 - f.p[3]) + f.p[1] * l2 / (l2 - f.p[4]) + f.p[2] * l2 / (l2 - f.p[5]);
+        return std::sqrt(n2 > 1.0 ? n2 : 1.0);
+    }
+    case FTB_SPEC_TABLE: {
+        const double* x = tw.data() + f.offset;
+        const double* y = tv.data() + f.offset;
+        const int n = f.n;
+        if (w <= x[0]) return y[0];
+        if (w >= x[n - 1]) return y[n - 1];
+        int lo = 0, hi = n - 1;
+        while (lo + 1 < hi) { int mid = (lo + hi) / 2; if (x[mid] <= w) lo = mid; else hi = mid; }
+        double w0 = x[lo], w1 = x[lo + 1], v0 = y[lo], v1 = y[lo + 1];
+        double fr = (w1 > w0) ? (w - w0) / (w1 - w0) : 0.0;
+        return v0 + (v1 - v0) * fr;
+    }
+    default: return 0.0;
+    }
+}
+
+bool same_bits(double a, double b) {
+    uint64_t x, y;
+    std::memcpy(&x, &a, 8);
+    std::memcpy(&y, &b, 8);
+    return x == y || (a != a && b != b);
+}
+
+// Wavelengths a baked form is checked at: the 0.5 nm grid over [360, 830], 2048 seeded
+// pseudo-random wavelengths in that band, and (tables) every breakpoint and its
+// floating-point neighbours.
+std::vector<double> check_wavelengths(const std::vector<double>& breaks) {
+    std::vector<double> w;
+    for (double x = LAMBDA_MIN; x <= LAMBDA_MAX + 1e-9; x += kTableStep) w.push_back(x);
+    uint64_t st = 0x9E3779B97F4A7C15ull;
+    for (int i = 0; i < 2048; ++i) {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        w.push_back(LAMBDA_MIN + (LAMBDA_MAX - LAMBDA_MIN) * ((double)(st >> 11) * 0x1.0p-53));
+    }
+    for (double x : breaks) {
+        w.push_back(x);
+        w.push_back(std::nextafter(x, -1e300));
+        w.push_back(std::nextafter(x, 1e300));
+    }
+    return w;
+}
+
+bool form_matches(const Spectrum& s, const ftb_spectrum& f, const std::vector<double>& tw,
+                  const std::vector<double>& tv, const std::vector<double>& ws) {
+    for (double w : ws)
+        if (!same_bits(eval_form(f, tw, tv, w), s(w))) return false;
+    return true;
+}
+
+// The closure object inside a Spectrum made by a known builder (libstdc++ only): the
+// target type identifies the builder -- every call of e.g. cauchy() yields the same closure
+// type -- and libstdc++ keeps a closure of at most 16 trivially copyable bytes inside the
+// function object itself, any other behind a pointer at its start.  Only closures whose
+// type was matched are read, and only as the builder captured them: Cauchy 2 doubles
+// (stored inside), Sellmeier 6 doubles and tabulatedSpectrum one vector of (w, v) pairs
+// (both stored behind the pointer).  The order of the captured doubles is not fixed by
+// the language, so every order is tried, and each candidate must pass form_matches.
+#if defined(__GLIBCXX__)
+static_assert(sizeof(Spectrum) == 32, "unexpected std::function layout");
+const std::type_info& cauchy_type() { static const Spectrum p = cauchy(1.0, 1.0); return p.target_type(); }
+const std::type_info& sellmeier_type() {
+    static const Spectrum p = sellmeier(1.0, 1.0, 1.0, 1.0, 1.0, 1.0);
+    return p.target_type();
+}
+const std::type_info& table_type() {
+    static const Spectrum p = tabulatedSpectrum({{400.0, 0.0}, {500.0, 1.0}});
+    return p.target_type();
+}
+const void* heap_closure(const Spectrum& s) {
+    const void* p;
+    std::memcpy(&p, &s, sizeof p);
+    return p;
+}
+#endif
+
+bool exact_form(Baked& b, const Spectrum& s, ftb_spectrum& out) {
+#if defined(__GLIBCXX__)
+    if (!s) return false;
+    const std::type_info& t = s.target_type();
+    if (t == cauchy_type()) {
+        double c[2];
+        std::memcpy(c, &s, sizeof c);
+        static const std::vector<double> ws = check_wavelengths({});
+        for (int order = 0; order < 2; ++order) {
+            ftb_spectrum f{};
+            f.kind = FTB_SPEC_CAUCHY;
+            f.p[0] = c[order];
+            f.p[1] = c[1 - order];
+            if (form_matches(s, f, b.table_w, b.table_v, ws)) { out = f; return true; }
+        }
+        return false;
+    }
+    if (t == sellmeier_type()) {
+        double c[6];
+        std::memcpy(c, heap_closure(s), sizeof c);
+        static const std::vector<double> ws = check_wavelengths({});
+        int idx[6] = {0, 1, 2, 3, 4, 5};
+        do {
+            ftb_spectrum f{};
+            f.kind = FTB_SPEC_SELLMEIER;
+            for (int k = 0; k < 6; ++k) f.p[k] = c[idx[k]];
+            if (form_matches(s, f, b.table_w, b.table_v, ws)) { out = f; return true; }
+        } while (std::next_permutation(idx, idx + 6));
+        return false;
+    }
+    if (t == table_type()) {
+        const auto* pairs = static_cast<const std::vector<std::pair<double, double>>*>(heap_closure(s));
+        if (pairs->empty()) return false;
+        ftb_spectrum f{};
+        f.kind = FTB_SPEC_TABLE;
+        f.offset = (int64_t)b.table_w.size();
+        f.n = (int32_t)pairs->size();
+        std::vector<double> breaks;
+        for (const auto& pr : *pairs) {
+            b.table_w.push_back(pr.first);
+            b.table_v.push_back(pr.second);
+            breaks.push_back(pr.first);
+        }
+        bool distinct = true;
+        for (size_t i = 1; i < breaks.size(); ++i) distinct = distinct && breaks[i] > breaks[i - 1];
+        if (distinct && form_matches(s, f, b.table_w, b.table_v, check_wavelengths(breaks))) { out = f; return true; }
+        b.table_w.resize((size_t)f.offset);   // not usable: drop the candidate's pairs
+        b.table_v.resize((size_t)f.offset);
+        return false;
+    }
+#else
+    (void)b; (void)s; (void)out;
+#endif
+    return false;
+}
+
 int bake_spectrum(Baked& b, const Spectrum& s) {
     ftb_spectrum out{};
     double v0 = s(LAMBDA_MIN);
     bool constant = true;
     for (double w = LAMBDA_MIN; w <= LAMBDA_MAX; w += kTableStep)
-        if (s(w) != v0) { constant = false; break; }
+        if (!same_bits(s(w), v0)) { constant = false; break; }
     if (constant) {
         out.kind = FTB_SPEC_CONST;
         out.p[0] = v0;
-    } else {
+    } else if (!exact_form(b, s, out)) {
         out.kind = FTB_SPEC_TABLE;
         out.offset = (int64_t)b.table_w.size();
         int n = 0;
@@ -259,6 +411,21 @@ bool report(ftb_status s, const char* what) {
 
 }  // namespace
 
+// What the bake makes of a scene's material and medium spectra, in bake order (reflect,
+// ior, absorb, transmit of each material, then sigma_a, sigma_s of each medium), with the
+// table pairs the TABLE entries index: an integrator can check that the scene's spectra
+// bake in closed form (CAUCHY, SELLMEIER, or TABLE with the authored breakpoints) and not
+// as a 0.5 nm sampled table.  Not part of render_cuda.h.
+int ftbShimBakedSpectra(const Scene& scene, std::vector<ftb_spectrum>& spectra, std::vector<double>& table_w,
+                        std::vector<double>& table_v) {
+    Baked b;
+    bake(scene, b);
+    spectra = b.spectra;
+    table_w = b.table_w;
+    table_v = b.table_v;
+    return (int)spectra.size();
+}
+
 bool cudaAvailable() { return ftb_available() != 0; }
 
 const char* cudaDeviceName() { return ftb_device_name(); }
@@ -312,7 +479,7 @@ SharedGpuSession* sharedForwardGpuBegin(const Scene& scene, const std::vector<Ca
                                         const std::vector<int>& resX, const std::vector<int>& resY,
                                         char camMode, bool /*wavefront*/, int heroC, bool beamGather,
                                         const std::vector<Film>* seedFilms, const EnergyReport* seedEnergy) {
-    if (camMode != 'B' || heroC > 1 || beamGather || cams.empty()) return nullptr;
+    if (camMode != 'B' || beamGather || cams.empty()) return nullptr;
     Baked b;
     bake(scene, b);
     if (!b.supported) return nullptr;
@@ -320,7 +487,8 @@ SharedGpuSession* sharedForwardGpuBegin(const Scene& scene, const std::vector<Ca
     if (!report(ftb_scene_create(&b.desc, 0, &g->scene), "scene bake")) { delete g; return nullptr; }
     std::vector<ftb_camera> cs;
     for (size_t i = 0; i < cams.size(); ++i) cs.push_back(bake_camera(cams[i], resX[i], resY[i]));
-    if (!report(ftb_session_begin(g->scene, cs.data(), (int32_t)cs.size(), g_ftbMaxBounce, 0, &g->session),
+    if (!report(ftb_session_begin(g->scene, cs.data(), (int32_t)cs.size(), g_ftbMaxBounce, 0, heroC,
+                                  &g->session),
                 "session")) {
         ftb_scene_destroy(g->scene);
         delete g;

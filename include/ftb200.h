@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FTB_ABI_VERSION 4
+#define FTB_ABI_VERSION 5
 
 typedef enum ftb_status {
     FTB_OK = 0,
@@ -361,9 +361,13 @@ ftb_status ftb_render_batch(const ftb_job* jobs, int32_t n_jobs, ftb_film_info* 
                             ftb_energy* energies, void* stream);
 
 /* Resident session (replaces sharedForwardGpuBegin/Batch/Hits0/Download/End,
- * render_cuda.h:121-143).  Films and energy stay on the device between batches. */
+ * render_cuda.h:121-143).  Films and energy stay on the device between batches.  Every
+ * batch traces its photons once and connects each path vertex to every camera (the
+ * multi-camera shared splat); hero_c is the wavelengths per photon, as in
+ * ftb_render_params (the reference's session takes heroC too, render_cuda.h:122-128). */
 ftb_status ftb_session_begin(ftb_scene* scene, const ftb_camera* cams, int32_t n_cams,
-                             int32_t max_bounce, int32_t frac_bits, ftb_session** out);
+                             int32_t max_bounce, int32_t frac_bits, int32_t hero_c,
+                             ftb_session** out);
 ftb_status ftb_session_batch(ftb_session* s, int64_t n_photons, uint64_t seed_base);
 /* hits of camera 0 as doubles (reference sharedForwardGpuHits0) */
 ftb_status ftb_session_hits0(ftb_session* s, double* hits);

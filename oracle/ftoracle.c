@@ -684,7 +684,13 @@ static inline int box_hit(const Node* n, V3 o, V3 inv, double tmin, double tmax,
     return 1;
 }
 
-/* Nearest primitive p of tree T with test(env, p, tbest, &t) accepted; returns p or -1. */
+/* Nearest primitive p of tree T with test(env, p, tbest, &t) accepted; returns p or -1.
+ * Exact ties in t go to the lower primitive index.  The reference takes the first of the
+ * tied primitives its own hierarchy happens to test (bvh.h:181-224, strict t < tBest), an
+ * order no other hierarchy reproduces; with the index rule the result does not depend on
+ * the hierarchy at all, so the oracle and the device (which applies the same rule) agree on
+ * every tie, and differ from the reference only where the reference's order picked the
+ * higher index. */
 typedef int (*PrimTest)(const void* env, int p, double tbest, double* t);
 static int tree_closest(const Tree* T, V3 ro, V3 rd, double tmin, double tbest, PrimTest test, const void* env,
                         double* t_out) {
@@ -704,7 +710,11 @@ static int tree_closest(const Tree* T, V3 ro, V3 rd, double tmin, double tbest, 
             for (int i = 0; i < n->count; ++i) {
                 int p = T->order[n->first + i];
                 double t;
-                if (test(env, p, best, &t)) { best = t; bestp = p; }
+                /* accept t <= best, then keep the lower index on a tie */
+                if (test(env, p, nextafter(best, INFINITY), &t) && (t < best || bestp < 0 || p < bestp)) {
+                    best = t;
+                    bestp = p;
+                }
             }
         } else {
             double tl = 0.0, tr = 0.0;

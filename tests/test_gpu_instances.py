@@ -113,3 +113,83 @@ def test_bad_instance_arguments_fail_cleanly(gpu):
     with pytest.raises(lib.FtbError):
         sc.set_instance_transforms([bad])
     sc.close()
+
+
+# ---- anchored to the oracle and the reference ------------------------------------------
+# The tests above show that a refit TLAS, a clone and a batched frame render what a fresh
+# scene renders.  These show that what they render is the reference's light transport for
+# the moved instance: per-photon paths against the oracle built from a descriptor with the
+# new transform (MeshInstance::setToWorld, scene.h:1052-1062), films and energy against
+# the oracle and against the reference's own tracer, within the parity tolerances of
+# test_gpu_parity.py.
+def assert_film_close(film, info, xyz_ref, hits_ref):
+    xyz, hits = lib.film_to_xyz(film, info)
+    np.testing.assert_array_equal(hits, hits_ref)
+    tol = hits_ref[..., None] * info.scale + 1e-10 * np.abs(xyz_ref)
+    bad = np.abs(xyz - xyz_ref) > tol
+    assert not bad.any(), f"{bad.sum()} film values differ"
+
+
+def check_against_oracle(sc, desc, oracle, reference, res=40, n=1 << 14, seed=9):
+    cam = scenes.default_camera(sc.lib, res)
+    gl = sc.trace_log(cam, n, seed_base=seed, max_bounce=16)
+    ol = oracle.trace(desc, cam, n, seed_base=seed, max_bounce=16, logs=True, threads=4)["logs"]
+    same = (gl["n_hits"] == ol["n_hits"]) & (gl["prim_hash"] == ol["prim_hash"]) & (gl["fate"] == ol["fate"])
+    assert (~same).sum() <= max(1, int(1e-5 * n)), f"{(~same).sum()} of {n} photon paths differ"
+    np.testing.assert_allclose(gl["beta"][same], ol["beta"][same], rtol=1e-12, atol=0)
+    film, info, en = sc.render(cam, n, seed_base=seed, max_bounce=16)
+    o = oracle.trace(desc, cam, n, seed_base=seed, max_bounce=16, threads=1)
+    assert_film_close(film, info, o["xyz"], o["hits"])
+    np.testing.assert_allclose(en.as_list(), o["energy"], rtol=1e-9, atol=0)
+    r = reference.trace(desc, cam, n, seed_base=seed, max_bounce=16, threads=1)
+    assert_film_close(film, info, r["xyz"], r["hits"])
+    np.testing.assert_allclose(en.as_list(), r["energy"], rtol=1e-9, atol=0)
+
+
+def test_refit_and_clone_match_oracle_and_reference(gpu, oracle, reference):
+    a = lib.Scene(scenes.make_glass_instanced(gpu, LEVEL, to_world=XF_A), 0, gpu)
+    try:
+        a.set_instance_transforms([XF_B])                   # refit
+        check_against_oracle(a, scenes.make_glass_instanced(gpu, LEVEL, to_world=XF_B), oracle, reference)
+        xf_c = scenes.affine((0.7, -0.2, 0.4), 290.0, (1.1, 0.45, 0.9), scale=0.9)
+        c = a.clone_instances([xf_c])                       # clone with a third transform
+        try:
+            check_against_oracle(c, scenes.make_glass_instanced(gpu, LEVEL, to_world=xf_c), oracle, reference)
+        finally:
+            c.close()
+    finally:
+        a.close()
+
+
+def test_batched_frames_match_oracle(gpu, oracle):
+    """Four animation frames (clones with seeded rigid transforms, uneven films and
+    budgets) in one ftb_render_batch: each frame's film and energy against the oracle's
+    render of a descriptor with that frame's transform."""
+    torch = pytest.importorskip("torch")
+    base = lib.Scene(scenes.make_glass_instanced(gpu, LEVEL, to_world=XF_A), 0, gpu)
+    rng = np.random.default_rng(17)
+    frames, jobs, films, xfs = [], [], [], []
+    try:
+        for k in range(4):
+            xf = scenes.affine(rng.normal(size=3), rng.uniform(0, 360),
+                               np.asarray(scenes.GLASS_CENTER) + rng.uniform(-0.2, 0.2, 3))
+            xfs.append(xf)
+            fr = base.clone_instances([xf])
+            frames.append(fr)
+            res = (24, 40, 32, 48)[k]
+            film = torch.zeros((res, res, 4), dtype=torch.int64, device="cuda:0")
+            films.append(film)
+            jobs.append(dict(scene=fr, cam=scenes.default_camera(gpu, res), d_film=film.data_ptr(),
+                             n=(9000, 30000, 15000, 22000)[k], seed_base=50_000 * k, max_bounce=16,
+                             frac_bits=30))
+        infos, ens = gpu.render_batch(jobs, stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        for k, j in enumerate(jobs):
+            desc = scenes.make_glass_instanced(gpu, LEVEL, to_world=xfs[k])
+            o = oracle.trace(desc, j["cam"], j["n"], seed_base=j["seed_base"], max_bounce=16, threads=1)
+            assert_film_close(films[k].cpu().numpy(), infos[k], o["xyz"], o["hits"])
+            np.testing.assert_allclose(ens[k].as_list(), o["energy"], rtol=1e-9, atol=0)
+    finally:
+        for fr in frames:
+            fr.close()
+        base.close()

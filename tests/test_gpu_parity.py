@@ -104,12 +104,16 @@ def test_film_is_order_independent_and_linear(scenes_cache, gpu):
     assert [x + y for x, y in zip(e1.fx, e2.fx)] == list(ea.fx)
 
 
-def test_session_accumulates_like_one_render(scenes_cache, gpu):
-    d, sc = scenes_cache["cornell"]
+@pytest.mark.parametrize("name,mb,hero", [("cornell", 8, 1), ("glass", 16, 4)])
+def test_session_accumulates_like_one_render(name, mb, hero, scenes_cache, gpu):
+    """Two cameras in one session (the shared splat), two batches: each camera's film equals
+    a one-shot render of all the photons through that camera alone, with one wavelength per
+    photon and with hero bundles."""
+    d, sc = scenes_cache[name]
     cams = [cases.camera(gpu, 48), gpu.look_at((1.2, 1.1, 5.0), (1.0, 1.0, 1.0), (0, 1, 0), 35.0, 40, 32)]
     arr = (type(cams[0]) * 2)(*cams)
     h = C.c_void_p()
-    gpu.check(gpu.L.ftb_session_begin(sc.h, arr, 2, 8, 28, C.byref(h)))
+    gpu.check(gpu.L.ftb_session_begin(sc.h, arr, 2, mb, 28, hero, C.byref(h)))
     try:
         gpu.check(gpu.L.ftb_session_batch(h, 50_000, 0))
         gpu.check(gpu.L.ftb_session_batch(h, 70_000, 50_000))
@@ -117,7 +121,7 @@ def test_session_accumulates_like_one_render(scenes_cache, gpu):
         for c, cam in enumerate(cams):
             film = np.zeros((cam.res_y, cam.res_x, 4), dtype=np.int64)
             gpu.check(gpu.L.ftb_session_download(h, c, film.ctypes.data_as(C.POINTER(C.c_int64)), None, None))
-            whole, _, _ = sc.render(cam, 120_000, seed_base=0, max_bounce=8, frac_bits=28)
+            whole, _, _ = sc.render(cam, 120_000, seed_base=0, max_bounce=mb, frac_bits=28, hero_c=hero)
             np.testing.assert_array_equal(film, whole)
             films.append(film)
         hits = np.zeros(48 * 48)

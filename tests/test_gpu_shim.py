@@ -2,10 +2,13 @@
 main.cpp: a reference Scene and Camera in, renderForwardCuda(...) with the reference's own
 signature (render_cuda.h:79-82), a reference Film out.
 
-The scene's step spectra have their breakpoints on the shim's 0.5 nm sampling grid, so the
-shim's baked tables equal the originals and the film through the shim must equal, bit for
-bit, the film through the C ABI directly -- and match the reference CPU tracer on the same
-photons within the parity tolerances of test_gpu_parity.py.
+The shim bakes spectra made by the reference's builders (Cauchy, Sellmeier, tables) in
+closed form, so the film through the shim must equal, bit for bit, the film through the C
+ABI directly -- and match the reference CPU tracer on the same photons within the parity
+tolerances of test_gpu_parity.py -- on the benchmarked dispersive glass (Cauchy IOR, step
+spectra with breakpoints off any sampling grid) and on every material branch.  The
+resident session (sharedForwardGpu*) is driven the same way, with one wavelength per
+photon and with hero bundles (the reference CLI's default heroC is 4).
 """
 import ctypes as C
 import os
@@ -32,6 +35,9 @@ def shim(gpu):
     PD = C.POINTER(C.c_double)
     L.ftshim_render.restype = C.c_int
     L.ftshim_render.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int64, C.c_uint64, C.c_int, PD, PD, PD]
+    L.ftshim_session.restype = C.c_int
+    L.ftshim_session.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int, C.c_int64, C.c_int64, C.c_int,
+                                 C.c_int, C.c_int, PD, PD, PD]
     L.ftr_trace.restype = C.c_int
     L.ftr_trace.argtypes = [C.c_void_p, C.POINTER(abi.Camera), C.c_int64, C.c_uint64, C.c_int, C.c_int, C.c_int,
                             PD, PD, PD, C.POINTER(C.c_int64), C.POINTER(C.c_int32), PD]
@@ -44,14 +50,23 @@ def cornell_on_grid(gpu):
     return sb.build(gpu)
 
 
-@pytest.mark.parametrize("scene", ["cornell", "instances"])
+SHIM_SCENES = {
+    "cornell": (cornell_on_grid, 8),
+    "glass": (lambda L: scenes.make_glass(L, level=3), 16),
+    "materials": (cases.make_materials, 16),
+    "instances": (cases.make_instances, 16),
+}
+
+
+@pytest.mark.parametrize("scene", sorted(SHIM_SCENES))
 def test_render_forward_cuda_through_shim(shim, gpu, scene):
-    """`instances`: the reference Scene's blasList / MeshInstances go through the shim's bake
-    (with a constant IOR: the shim tabulates non-constant spectra every 0.5 nm, exact only for
-    piecewise-linear ones)."""
-    d = cornell_on_grid(gpu) if scene == "cornell" else cases.make_instances(gpu, ramp=0.5, cauchy=False)
+    """`glass`: the benchmarked material (Cauchy IOR; wall steps with 0.01 nm ramps);
+    `materials`: Sellmeier, nested priorities, filters, glossy; `instances`: the reference
+    Scene's blasList / MeshInstances go through the shim's bake."""
+    mk, mb = SHIM_SCENES[scene]
+    d = mk(gpu)
     cam = scenes.default_camera(gpu, 48)
-    n, mb, seed = 60_000, (8 if scene == "cornell" else 16), 77
+    n, seed = 60_000, 77
     ref = shim.ftr_prepare(d.ref())
     try:
         npix = 48 * 48
@@ -75,5 +90,37 @@ def test_render_forward_cuda_through_shim(shim, gpu, scene):
     # against the reference CPU tracer on the same photons
     np.testing.assert_array_equal(hits, ch)
     tol = ch[:, None] * info.scale + 1e-10 * np.abs(cx.reshape(-1, 3))
+    assert (np.abs(xyz.reshape(-1, 3) - cx.reshape(-1, 3)) <= tol).all()
+    np.testing.assert_allclose(en, ce, rtol=1e-9)
+
+
+@pytest.mark.parametrize("scene,hero", [("glass", 1), ("glass", 4), ("cornell", 4)])
+def test_shared_session_through_shim(shim, gpu, oracle, scene, hero):
+    """sharedForwardGpuBegin with two cameras and heroC, two batches with the cumulative
+    seedBase: camera 0's running total equals the reference CPU tracer's film of the same
+    photons through that camera alone (the shared splat draws no random numbers)."""
+    mk, mb = SHIM_SCENES[scene]
+    d = mk(gpu)
+    cams = (abi.Camera * 2)(scenes.default_camera(gpu, 40),
+                            gpu.look_at((1.3, 1.2, 4.8), (1.0, 0.9, 1.0), (0, 1, 0), 38.0, 32, 24))
+    n0, n1 = 30_000, 45_000
+    ref = shim.ftr_prepare(d.ref())
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    try:
+        npix = 40 * 40
+        xyz, hits, en = np.zeros(npix * 3), np.zeros(npix), np.zeros(5)
+        assert shim.ftshim_session(ref, cams, 2, n0, n1, mb, hero, 0, P(xyz), P(hits), P(en)) == 0
+        cx, ch, ce = np.zeros(npix * 3), np.zeros(npix), np.zeros(5)
+        assert shim.ftr_trace(ref, C.byref(cams[0]), n0 + n1, 0, mb, hero, 4, P(cx), P(ch), P(ce),
+                              None, None, None) == 0
+    finally:
+        shim.ftr_release(ref)
+    assert hits.sum() > 0
+    np.testing.assert_array_equal(hits, ch)
+    # the session's film format: the default for 2^36 photons (ftb_session_begin, frac_bits 0)
+    sc = lib.Scene(d, 0, gpu)
+    q = sc.power * 2.0 ** -(62 - 36 - 20)
+    sc.close()
+    tol = ch[:, None] * q + 1e-10 * np.abs(cx.reshape(-1, 3))
     assert (np.abs(xyz.reshape(-1, 3) - cx.reshape(-1, 3)) <= tol).all()
     np.testing.assert_allclose(en, ce, rtol=1e-9)

@@ -83,6 +83,39 @@ CONFIG_CASES = {
 }
 
 
+def joint_ties(d, gl, ol, idx):
+    """Of the photons `idx` whose logged paths differ between two tracers, those that differ
+    only in which of two consecutive segments of one strand was hit at their shared joint
+    (the segment of one strand ends where the next begins, so a ray meeting the joint meets
+    both round cones at the same point, with distances equal to within ~1e-16 m; a last-bit
+    difference in the ray -- CUDA's sin/cos/log against glibc's -- can decide which is
+    nearer).  Such photons have the same bounce count, termination and final beta, and the
+    same hit sequence up to those swaps.  Only paths of at most 8 hits (all logged) count."""
+    base = len(d.tri_v) + len(d.sph)
+    curve = d.curve
+    nc = len(curve)
+
+    def joint(a, b):
+        ia, ib = a - base, b - base
+        if not (0 <= ia < nc and 0 <= ib < nc):
+            return False
+        pa, pb = curve[ia], curve[ib]
+        return bool(np.array_equal(pa[3:6], pb[0:3]) or np.array_equal(pb[3:6], pa[0:3]))
+
+    out = []
+    for i in idx:
+        nh = int(gl["n_hits"][i])
+        if nh != int(ol["n_hits"][i]) or gl["fate"][i] != ol["fate"][i] or nh > 8:
+            continue
+        if not np.isclose(gl["beta"][i], ol["beta"][i], rtol=1e-12, atol=0):
+            continue
+        ga, oa = gl["prims"][i][:nh], ol["prims"][i][:nh]
+        diff = np.nonzero(ga != oa)[0]
+        if len(diff) and all(joint(int(ga[k]), int(oa[k])) for k in diff):
+            out.append(int(i))
+    return out
+
+
 def camera(L, res):
     return scenes.default_camera(L, res)
 

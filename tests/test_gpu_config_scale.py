@@ -11,8 +11,13 @@ traversal stack depth are stressed.  So here, at those sizes:
     tracer from these exact scenes, tests/golden/make_golden.py);
   * every photon's hit-primitive sequence, bounce count and termination equal the oracle's
     on 2^15 photons, with the host-built and the GPU-built hierarchies, allowing
-    max(1, 1e-5 n) mismatches (grazing hits / exact ties) and 1e-12 relative on the final
-    beta;
+    max(1, 1e-5 n) mismatches (grazing hits) and 1e-12 relative on the final beta.  Among
+    the strands, a ray can meet the joint of two consecutive segments of a strand, where
+    both round cones pass through the same point and their distances agree to ~1e-16 m; a
+    last-bit difference in the ray (CUDA's sin/cos/log against glibc's) can then decide
+    which segment is reported, with the same path afterwards.  Those photons are counted
+    apart (cases.joint_ties) and bounded by 1e-4 n; measured: 4 of 131072 photons of the
+    fog + 250k strands configuration, none elsewhere;
   * the statistical film criterion on the configurations' full films: independent photons
     on each side (GPU indices [0, N), oracle [N, 2N)), K = 32 batches, per-pixel means of Y
     compared in units of their combined standard error -- the count of lit pixels beyond
@@ -88,8 +93,12 @@ def test_config_per_photon_paths_match_oracle(name, build, config_scenes, gpu, o
     ol = oracle.trace(d, cam, n, seed_base=seed + 12345, max_bounce=mb, logs=True, threads=os.cpu_count() or 4,
                       hero_c=hero)["logs"]
     same = same_paths(gl, ol)
+    bad = np.nonzero(~same)[0]
+    ties = cases.joint_ties(d, gl, ol, bad)
+    other = [int(i) for i in bad if int(i) not in set(ties)]
     allowed = max(1, int(1e-5 * n))
-    assert (~same).sum() <= allowed, f"{(~same).sum()} of {n} photon paths differ; first {np.nonzero(~same)[0][:5]}"
+    assert len(other) <= allowed, f"{len(other)} of {n} photon paths differ (besides joint ties); first {other[:5]}"
+    assert len(ties) <= max(1, int(1e-4 * n)), f"{len(ties)} strand-joint ties of {n}"
     np.testing.assert_allclose(gl["beta"][same], ol["beta"][same], rtol=1e-12, atol=0)
     np.testing.assert_array_equal(gl["prims"][same], ol["prims"][same])
     assert gl["n_hits"].mean() > 1.0   # the photons do bounce in these scenes

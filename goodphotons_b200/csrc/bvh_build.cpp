@@ -228,57 +228,41 @@ bool collapse_to_wide(const std::vector<BinNode>& bnodes, const std::vector<int>
             kids[best] = B.nodes[id].left;
             kids.push_back(B.nodes[id].right);
         }
-        // slots by direction (octant_slots); then, in slot order, internal children get
-        // consecutive wide nodes (child k of a node is child_base + its rank among the
-        // internal slots) and leaves consecutive record runs.
+        // assign: internal children get consecutive wide-node slots, leaves consecutive
+        // record runs.
         WNode w;
         std::memset(&w, 0, sizeof w);
         w.child_base = (uint32_t)out.nodes.size();
         w.prim_base = (uint32_t)out.order.size();
-        const int nk = (int)kids.size();
+        int n_int = 0, prim_off = 0;
+        double clo[3][8], chi[3][8];
         Box nb;
-        double cen[8][3];
-        for (int k = 0; k < nk; ++k) {
+        for (int k = 0; k < (int)kids.size(); ++k) {
             const BNode& c = B.nodes[kids[k]];
             nb.grow(c.box);
-            for (int a = 0; a < 3; ++a) cen[k][a] = 0.5 * (c.box.lo[a] + c.box.hi[a]);
-        }
-        double nc[3];
-        for (int a = 0; a < 3; ++a) nc[a] = 0.5 * (nb.lo[a] + nb.hi[a]);
-        int slot_of[8], kid_at[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
-        octant_slots(cen, nk, nc, slot_of);
-        for (int k = 0; k < nk; ++k) kid_at[slot_of[k]] = k;
-        int n_int = 0, prim_off = 0, nq = 0, qslot[8];
-        double clo[3][8], chi[3][8];
-        for (int s = 0; s < FTB_WIDTH; ++s) {
-            if (kid_at[s] < 0) continue;
-            const BNode& c = B.nodes[kids[kid_at[s]]];
-            for (int a = 0; a < 3; ++a) { clo[a][nq] = c.box.lo[a]; chi[a][nq] = c.box.hi[a]; }
-            qslot[nq++] = s;
+            for (int a = 0; a < 3; ++a) { clo[a][k] = c.box.lo[a]; chi[a][k] = c.box.hi[a]; }
             if (c.count > 0) {
                 if (prim_off > 31) { err = "leaf record offset exceeds 5 bits"; return false; }
-                w.meta[s] = (uint8_t)((c.count << 5) | prim_off);
+                w.meta[k] = (uint8_t)((c.count << 5) | prim_off);
                 for (int i = 0; i < c.count; ++i) out.order.push_back(B.idx[c.first + i]);
                 prim_off += c.count;
             } else {
-                w.meta[s] = (uint8_t)((1 << 5) | n_int);
-                w.imask |= (uint8_t)(1u << s);
+                w.meta[k] = (uint8_t)((1 << 5) | n_int);
+                w.imask |= (uint8_t)(1u << k);
                 out.nodes.push_back(WNode{});
-                queue.push_back({kids[kid_at[s]], (int)w.child_base + n_int});
+                queue.push_back({kids[k], (int)w.child_base + n_int});
                 ++n_int;
             }
         }
         float p[3]; int e[3];
         uint8_t* qlo[3] = {w.qlo_x, w.qlo_y, w.qlo_z};
         uint8_t* qhi[3] = {w.qhi_x, w.qhi_y, w.qhi_z};
-        for (int a = 0; a < 3; ++a) {
-            uint8_t lo8[8], hi8[8];
-            if (!quantize_axis(nb.lo[a], nb.hi[a], clo[a], chi[a], nq, p[a], e[a], lo8, hi8)) {
+        for (int a = 0; a < 3; ++a)
+            if (!quantize_axis(nb.lo[a], nb.hi[a], clo[a], chi[a], (int)kids.size(), p[a], e[a],
+                               qlo[a], qhi[a])) {
                 err = "BVH quantization failed (scene extent out of float range)";
                 return false;
             }
-            for (int i = 0; i < nq; ++i) { qlo[a][qslot[i]] = lo8[i]; qhi[a][qslot[i]] = hi8[i]; }
-        }
         w.px = p[0]; w.py = p[1]; w.pz = p[2];
         w.ex = (uint8_t)(e[0] + 127); w.ey = (uint8_t)(e[1] + 127); w.ez = (uint8_t)(e[2] + 127);
         out.nodes[pd.wide] = w;
@@ -294,11 +278,11 @@ bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, st
     for (size_t i = nn; i-- > 0;) {
         WNode& w = b.nodes[i];
         double clo[3][8], chi[3][8];
-        int n = 0, qslot[8];
+        int n = 0;
         Box all;
         for (int k = 0; k < FTB_WIDTH; ++k) {
             uint32_t m = w.meta[k];
-            if (!m) continue;   // an empty slot
+            if (!m) break;   // the builder fills slots 0..n-1
             Box c;
             if ((w.imask >> k) & 1) {
                 c = nb[w.child_base + (m & 31)];
@@ -309,8 +293,7 @@ bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, st
                     c.grow(p);
                 }
             }
-            for (int a = 0; a < 3; ++a) { clo[a][n] = c.lo[a]; chi[a][n] = c.hi[a]; }
-            qslot[n] = k;
+            for (int a = 0; a < 3; ++a) { clo[a][k] = c.lo[a]; chi[a][k] = c.hi[a]; }
             all.grow(c);
             ++n;
         }
@@ -318,14 +301,11 @@ bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, st
         float p[3]; int e[3];
         uint8_t* qlo[3] = {w.qlo_x, w.qlo_y, w.qlo_z};
         uint8_t* qhi[3] = {w.qhi_x, w.qhi_y, w.qhi_z};
-        for (int a = 0; a < 3; ++a) {
-            uint8_t lo8[8], hi8[8];
-            if (!quantize_axis(all.lo[a], all.hi[a], clo[a], chi[a], n, p[a], e[a], lo8, hi8)) {
+        for (int a = 0; a < 3; ++a)
+            if (!quantize_axis(all.lo[a], all.hi[a], clo[a], chi[a], n, p[a], e[a], qlo[a], qhi[a])) {
                 err = "BVH quantization failed (scene extent out of float range)";
                 return false;
             }
-            for (int j = 0; j < n; ++j) { qlo[a][qslot[j]] = lo8[j]; qhi[a][qslot[j]] = hi8[j]; }
-        }
         w.px = p[0]; w.py = p[1]; w.pz = p[2];
         w.ex = (uint8_t)(e[0] + 127); w.ey = (uint8_t)(e[1] + 127); w.ez = (uint8_t)(e[2] + 127);
     }
@@ -340,14 +320,11 @@ bool validate_wide_bvh(const WideBvh& b, int n_prims, std::string& err) {
     seen_node[0] = 1;
     for (size_t i = 0; i < nn; ++i) {
         const WNode& w = b.nodes[i];
-        uint32_t rank = 0;
         for (int k = 0; k < FTB_WIDTH; ++k) {
             uint32_t m = w.meta[k];
             if (!m) { if ((w.imask >> k) & 1) { err = "internal bit on an empty slot"; return false; } continue; }
             uint32_t cnt = m >> 5, off = m & 31;
             if ((w.imask >> k) & 1) {
-                // the traversal finds internal child k at child_base + (internal slots below k)
-                if (off != rank++) { err = "internal children out of slot order"; return false; }
                 uint64_t c = (uint64_t)w.child_base + off;
                 if (cnt != 1 || c >= nn || c <= i || seen_node[c]) { err = "bad child node index"; return false; }
                 seen_node[c] = 1;

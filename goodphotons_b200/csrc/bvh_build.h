@@ -25,44 +25,6 @@ struct Box {
     }
 };
 
-#ifdef __CUDACC__
-#define FTB_HD __host__ __device__
-#else
-#define FTB_HD
-#endif
-
-// Child slots of a wide node by direction.  Slot s stands for the octant direction v_s
-// whose component a is -1 where bit a of s is set and +1 where it is clear; the children
-// (box centres cen[k], k < nk) are placed greedily, the (child, slot) pair with the largest
-// projection of (centre - node centre) on v_s first.  A ray whose direction has its
-// positive components where the bits of s are set then meets slot s's child first, the
-// slots one bit away next, and so on: traversal visits children in slot order s ^ x for a
-// per-ray x, an approximate near-to-far order that needs no sorting.
-FTB_HD inline void octant_slots(const double (*cen)[3], int nk, const double* node_c, int* slot_of) {
-    double cost[8][8];
-    for (int k = 0; k < nk; ++k)
-        for (int s = 0; s < 8; ++s) {
-            double c = 0.0;
-            for (int a = 0; a < 3; ++a) c += ((s >> a) & 1) ? node_c[a] - cen[k][a] : cen[k][a] - node_c[a];
-            cost[k][s] = c;
-        }
-    unsigned used = 0, placed = 0;
-    for (int it = 0; it < nk; ++it) {
-        int bk = -1, bs = -1;
-        double bc = 0.0;
-        for (int k = 0; k < nk; ++k) {
-            if ((placed >> k) & 1) continue;
-            for (int s = 0; s < 8; ++s) {
-                if ((used >> s) & 1) continue;
-                if (bk < 0 || cost[k][s] > bc) { bk = k; bs = s; bc = cost[k][s]; }
-            }
-        }
-        slot_of[bk] = bs;
-        placed |= 1u << bk;
-        used |= 1u << bs;
-    }
-}
-
 struct WideBvh {
     std::vector<WNode> nodes;   // root at 0
     std::vector<int> order;     // record i holds primitive order[i]

@@ -222,38 +222,23 @@ __global__ void k_collapse_level(const DBin* __restrict__ bins, const int* __res
     memset(&o, 0, sizeof o);
     o.child_base = (uint32_t)child_base;
     o.prim_base = (uint32_t)prim_base;
-    // slots by direction (octant_slots, as the host collapse), then in slot order internal
-    // children get consecutive wide nodes and leaves consecutive record runs
-    double nlo[3] = {1e300, 1e300, 1e300}, nhi[3] = {-1e300, -1e300, -1e300}, cen[FTB_WIDTH][3];
+    double clo[3][FTB_WIDTH], chi[3][FTB_WIDTH], nlo[3] = {1e300, 1e300, 1e300}, nhi[3] = {-1e300, -1e300, -1e300};
+    int ii = 0, off = 0;
     for (int k = 0; k < nk; ++k) {
         const DBin& c = bins[kids[k]];
         for (int a = 0; a < 3; ++a) {
-            cen[k][a] = 0.5 * (c.lo[a] + c.hi[a]);
+            clo[a][k] = c.lo[a]; chi[a][k] = c.hi[a];
             nlo[a] = c.lo[a] < nlo[a] ? c.lo[a] : nlo[a];
             nhi[a] = c.hi[a] > nhi[a] ? c.hi[a] : nhi[a];
         }
-    }
-    double nc[3];
-    for (int a = 0; a < 3; ++a) nc[a] = 0.5 * (nlo[a] + nhi[a]);
-    int slot_of[FTB_WIDTH], kid_at[FTB_WIDTH];
-    for (int s = 0; s < FTB_WIDTH; ++s) kid_at[s] = -1;
-    octant_slots(cen, nk, nc, slot_of);
-    for (int k = 0; k < nk; ++k) kid_at[slot_of[k]] = k;
-    double clo[3][FTB_WIDTH], chi[3][FTB_WIDTH];
-    int ii = 0, off = 0, nq = 0, qslot[FTB_WIDTH];
-    for (int s = 0; s < FTB_WIDTH; ++s) {
-        if (kid_at[s] < 0) continue;
-        const DBin& c = bins[kids[kid_at[s]]];
-        for (int a = 0; a < 3; ++a) { clo[a][nq] = c.lo[a]; chi[a][nq] = c.hi[a]; }
-        qslot[nq++] = s;
         if (c.count > 0) {
-            o.meta[s] = (uint8_t)((c.count << 5) | off);
+            o.meta[k] = (uint8_t)((c.count << 5) | off);
             for (int r = 0; r < c.count; ++r) order[prim_base + off + r] = idx[c.first + r];
             off += c.count;
         } else {
-            o.meta[s] = (uint8_t)((1 << 5) | ii);
-            o.imask |= (uint8_t)(1u << s);
-            src[child_base + ii] = kids[kid_at[s]];
+            o.meta[k] = (uint8_t)((1 << 5) | ii);
+            o.imask |= (uint8_t)(1u << k);
+            src[child_base + ii] = kids[k];
             ++ii;
         }
     }
@@ -261,15 +246,11 @@ __global__ void k_collapse_level(const DBin* __restrict__ bins, const int* __res
     int e[3];
     uint8_t* qlo[3] = {o.qlo_x, o.qlo_y, o.qlo_z};
     uint8_t* qhi[3] = {o.qhi_x, o.qhi_y, o.qhi_z};
-    for (int a = 0; a < 3; ++a) {
-        uint8_t lo8[FTB_WIDTH], hi8[FTB_WIDTH];
-        if (!quantize_axis_dev(nlo[a], nhi[a], clo[a], chi[a], nq, p[a], e[a], lo8, hi8)) {
+    for (int a = 0; a < 3; ++a)
+        if (!quantize_axis_dev(nlo[a], nhi[a], clo[a], chi[a], nk, p[a], e[a], qlo[a], qhi[a])) {
             atomicAdd(&counters[2], 1);
             p[a] = 0.f; e[a] = 0;
-            continue;
         }
-        for (int j = 0; j < nq; ++j) { qlo[a][qslot[j]] = lo8[j]; qhi[a][qslot[j]] = hi8[j]; }
-    }
     o.px = p[0]; o.py = p[1]; o.pz = p[2];
     o.ex = (uint8_t)(e[0] + 127); o.ey = (uint8_t)(e[1] + 127); o.ez = (uint8_t)(e[2] + 127);
     nodes[w] = o;

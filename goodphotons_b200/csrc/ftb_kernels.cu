@@ -460,7 +460,6 @@ __device__ void hit_attributes(const double* __restrict__ tri_n, const RayCtx& R
 struct RayF {
     float ox, oy, oz, ix, iy, iz;
     bool nx, ny, nz;   // direction component negative: near plane is the box's hi side
-    uint32_t oct;      // slot s of a node is visited at position s ^ oct (octant_slots)
 };
 __device__ __forceinline__ RayF make_rayf(D3 o, D3 d) {
     RayF r;
@@ -473,10 +472,6 @@ __device__ __forceinline__ RayF make_rayf(D3 o, D3 d) {
     dz = fabsf(dz) > 1e-20f ? dz : copysignf(1e-20f, dz);
     r.ix = 1.0f / dx; r.iy = 1.0f / dy; r.iz = 1.0f / dz;
     r.nx = dx < 0.0f; r.ny = dy < 0.0f; r.nz = dz < 0.0f;
-    // slot s holds the child lying farthest toward the direction whose components are
-    // negative where the bits of s are set; the nearest child along this ray is the slot
-    // with bits set where the ray's direction is positive
-    r.oct = (r.nx ? 0u : 1u) | (r.ny ? 0u : 2u) | (r.nz ? 0u : 4u);
     return r;
 }
 
@@ -550,195 +545,6 @@ struct LocalStack {
     __device__ __forceinline__ void put(int i, E v) { loc[i] = v; }
     __device__ __forceinline__ E get(int i) const { return loc[i]; }
 };
-
-#ifndef FTB_GROUP_WALK
-#define FTB_GROUP_WALK 1
-#endif
-
-#if FTB_GROUP_WALK
-// ---- node-group walks ----------------------------------------------------------------
-// A node's children sit in slots by direction (octant_slots in bvh_build.h), so visiting
-// slot s at position s ^ oct (oct per ray) goes approximately near to far without sorting.
-// The closest-hit walk descends into the nearest inner child of a node (by entry distance);
-// the stack holds node groups, one entry per visited node with more inner children still to
-// visit: the children's base index, the node's inner-slot mask, the positions not yet
-// visited and, for the closest-hit walk, the nearest of their entry distances rounded down
-// to 16 bits (bf16), which culls the whole group once a nearer hit is known.  Leaf
-// children are tested right after their node's visit.  The loops are "while-while": a lane
-// steps through inner nodes until one has leaf hits, so the lanes of a warp run the leaf
-// tests together.
-typedef uint2 AnyEntry;
-
-#define INF_F __int_as_float(0x7f800000)
-
-// bit s of m -> bit s ^ x
-__device__ __forceinline__ uint32_t perm8(uint32_t m, uint32_t x) {
-    m = (x & 1u) ? (((m & 0x55u) << 1) | ((m >> 1) & 0x55u)) : m;
-    m = (x & 2u) ? (((m & 0x33u) << 2) | ((m >> 2) & 0x33u)) : m;
-    m = (x & 4u) ? (((m & 0x0fu) << 4) | ((m >> 4) & 0x0fu)) : m;
-    return m;
-}
-// Occupied slots (nonzero meta byte) as an 8-bit mask.
-__device__ __forceinline__ uint32_t valid_slots(uint2 meta) {
-    uint32_t a = __vcmpne4(meta.x, 0u), b = __vcmpne4(meta.y, 0u);
-    a = ((a & 0x01010101u) * 0x01020408u) >> 24;
-    b = ((b & 0x01010101u) * 0x01020408u) >> 24;
-    return (a & 0xfu) | ((b & 0xfu) << 4);
-}
-// Slab test of child i (occupancy is checked separately); entry distance or +inf.
-__device__ __forceinline__ float slot_t(const NodeRay& N, int i, float tmin_f, float tmax_f) {
-    float tnx = __fmaf_rn((float)byte_of(N.lox, i), N.ax, N.bx);
-    float tfx = __fmaf_rn((float)byte_of(N.hix, i), N.ax, N.bx);
-    float tny = __fmaf_rn((float)byte_of(N.loy, i), N.ay, N.by);
-    float tfy = __fmaf_rn((float)byte_of(N.hiy, i), N.ay, N.by);
-    float tnz = __fmaf_rn((float)byte_of(N.loz, i), N.az, N.bz);
-    float tfz = __fmaf_rn((float)byte_of(N.hiz, i), N.az, N.bz);
-    float a = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin_f)) * T_LO;
-    float b = fminf(fminf(tfx, tfy), fminf(tfz, tmax_f)) * T_HI;
-    return a <= b ? a : INF_F;
-}
-__device__ __forceinline__ uint32_t inner_child(uint32_t base, uint32_t imask, uint32_t s) {
-    return base + __popc(imask & ((1u << s) - 1u));
-}
-
-template <bool COUNT, class Stack, class Leaf>
-__device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, const RayF& F, float tmin_f,
-                                              float tmax_f, Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt,
-                                              uint32_t root = 0) {
-    const uint32_t x = F.oct;
-    int sp = 0;
-    uint32_t cur = root;
-    float cur_t = tmin_f;    // entry distance of `cur`
-    bool have = true;
-    while (true) {
-        uint32_t lpos = 0, lnode = 0;
-        while (have) {
-            const uint32_t visit = cur;
-            uint4 n[5];
-            load_node(nodes, visit, n);
-            if (COUNT) cnt.nodes++;
-            const NodeRay N = node_setup(n, F);
-            const uint32_t imask = n[0].w >> 24, child_base = n[1].x;
-            const uint32_t valid = valid_slots(N.meta);
-            // hit slots; of the inner ones, the nearest (t1, slot s1) and the next entry distance
-            uint32_t hits = 0, s1 = 0;
-            float t1 = INF_F, t2 = INF_F;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const float t = slot_t(N, i, tmin_f, tmax_f);
-                const bool hit = t != INF_F && ((valid >> i) & 1u);
-                hits |= hit ? (1u << i) : 0u;
-                const bool in = hit && ((imask >> i) & 1u);
-                const bool nearer = in && t < t1;
-                t2 = nearer ? t1 : (in ? fminf(t2, t) : t2);
-                t1 = nearer ? t : t1;
-                s1 = nearer ? (uint32_t)i : s1;
-            }
-            const uint32_t inner = hits & imask;
-            have = false;
-            if (inner) {   // the nearest inner child next, the others as a group in direction order
-                const uint32_t rest = inner & ~(1u << s1);
-                if (rest) {
-                    if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return tmax_f; }
-                    st.put(sp++, make_uint2(child_base, imask | (perm8(rest, x) << 8) |
-                                                            (__float_as_uint(t2) & 0xffff0000u)));
-                }
-                cur = inner_child(child_base, imask, s1);
-                cur_t = t1;
-                have = true;
-            }
-            const uint32_t leaves = hits & ~imask;
-            if (leaves) { lpos = perm8(leaves, x); lnode = visit; break; }
-        }
-        while (lpos) {   // the node's record base and meta are re-read (L1) per leaf
-            const uint32_t s = (uint32_t)(__ffs(lpos) - 1) ^ x;
-            lpos &= lpos - 1;
-            const uint4 h = __ldg(reinterpret_cast<const uint4*>(nodes + lnode) + 1);
-            const uint32_t m = byte_of(make_uint2(h.z, h.w), (int)s);
-            tmax_f = leaf((int)(h.y + (m & 31u)), (int)(m >> 5), tmax_f);
-        }
-        if (have && cur_t <= tmax_f * T_CULL) continue;
-        // the top group whose nearest remaining child may still be nearer than the closest hit
-        have = false;
-        while (sp > 0) {
-            const uint2 g = st.get(sp - 1);
-            if (__uint_as_float(g.y & 0xffff0000u) > tmax_f * T_CULL) { --sp; continue; }
-            uint32_t gp = (g.y >> 8) & 0xffu;
-            const uint32_t s = (uint32_t)(__ffs(gp) - 1) ^ x;
-            gp &= gp - 1;
-            if (gp) st.put(sp - 1, make_uint2(g.x, (g.y & 0xffff00ffu) | (gp << 8)));
-            else --sp;
-            cur = inner_child(g.x, g.y & 0xffu, s);
-            cur_t = tmin_f;   // not known: visited
-            have = true;
-            break;
-        }
-        if (!have) break;
-    }
-    return tmax_f;
-}
-
-// Any-hit walk: order does not change the answer, so slots are taken in index order, a
-// node's leaves before its inner children; leaf(first, count) returns true on a hit, which
-// ends the walk.
-template <bool COUNT, class Stack, class Leaf>
-__device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const RayF& F, float tmin_f, float tmax_f,
-                                         Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt,
-                                         uint32_t root = 0) {
-    int sp = 0;
-    uint32_t cur = root;
-    bool have = true;
-    while (true) {
-        uint32_t lmask = 0, lnode = 0;
-        while (have) {
-            const uint32_t visit = cur;
-            uint4 n[5];
-            load_node(nodes, visit, n);
-            if (COUNT) cnt.nodes++;
-            const NodeRay N = node_setup(n, F);
-            uint32_t hits = 0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) hits |= (slot_t(N, i, tmin_f, tmax_f) != INF_F) ? (1u << i) : 0u;
-            hits &= valid_slots(N.meta);
-            const uint32_t imask = n[0].w >> 24, child_base = n[1].x;
-            const uint32_t inner = hits & imask;
-            have = false;
-            if (inner) {
-                const uint32_t s = (uint32_t)(__ffs(inner) - 1);
-                const uint32_t rest = inner & (inner - 1);
-                if (rest) {
-                    if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return false; }
-                    st.put(sp++, make_uint2(child_base, imask | (rest << 8)));
-                }
-                cur = inner_child(child_base, imask, s);
-                have = true;
-            }
-            const uint32_t leaves = hits & ~imask;
-            if (leaves) { lmask = leaves; lnode = visit; break; }
-        }
-        while (lmask) {   // the node's record base and meta are re-read (L1) per leaf
-            const uint32_t s = (uint32_t)(__ffs(lmask) - 1);
-            lmask &= lmask - 1;
-            const uint4 h = __ldg(reinterpret_cast<const uint4*>(nodes + lnode) + 1);
-            const uint32_t m = byte_of(make_uint2(h.z, h.w), (int)s);
-            if (leaf((int)(h.y + (m & 31u)), (int)(m >> 5))) return true;
-        }
-        if (have) continue;
-        if (sp == 0) break;
-        const uint2 g = st.get(sp - 1);
-        uint32_t gp = (g.y >> 8) & 0xffu;
-        const uint32_t s = (uint32_t)(__ffs(gp) - 1);
-        gp &= gp - 1;
-        if (gp) st.put(sp - 1, make_uint2(g.x, (g.y & 0xffff00ffu) | (gp << 8)));
-        else --sp;
-        cur = inner_child(g.x, g.y & 0xffu, s);
-        have = true;
-    }
-    return false;
-}
-
-#else   // per-child stack entries, children sorted by entry distance
-typedef uint32_t AnyEntry;
 
 // Closest-hit walk of one wide BVH.  Children of a node are visited near to far (leaves and
 // inner nodes alike, keys sorted by an 8-input network in registers); entries farther than
@@ -849,8 +655,6 @@ __device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const 
     return false;
 }
 
-#endif   // FTB_GROUP_WALK
-
 // Affine::apply / applyDir (linalg.h:105-114) of a 12-double map (3x3 row-major, then t)
 __device__ __forceinline__ D3 xf_point(const double* m, D3 p) {
     return mk(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[9],
@@ -940,7 +744,7 @@ __device__ __noinline__ bool blas_any(const DevInst& I, D3 wo, D3 wd, double tmi
         }
         return false;
     };
-    LocalStack<AnyEntry> st;
+    LocalStack<uint32_t> st;
     return walk_any<COUNT>(I.nodes, F, __double2float_rd(tmin), tmax_f, st, leaf, status, cnt);
 }
 
@@ -1004,7 +808,7 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
         }
         return false;
     };
-    LocalStack<AnyEntry> st;
+    LocalStack<uint32_t> st;
     if (walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt)) return true;
     return SHAPES && sc.root2 > 0 &&
            walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt, (uint32_t)sc.root2);

@@ -236,25 +236,22 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def run_animation(args):
-    """Batched animation: 64 frames of the glass scene (one shared BLAS, a refit clone per
+def animation_batch(n_frames, level, warmup, steps, baseline_frames, budget_log2, local, L):
+    """Batched animation: frames of the glass scene (one shared BLAS, a refit clone per
     frame) rendered in one ftb_render_batch, against rendering the same frames one at a
-    time -- resident clones, and the plain path that bakes every frame as a scene load."""
+    time -- resident clones, and the plain path that bakes every frame as a scene load with
+    the build the drop-in shim picks.  Returns the record."""
     import torch
     from goodphotons_b200 import abi, lib, scenes, workloads
 
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    L = lib.load()
-    frames = workloads.animation_frames(args.frames, seed=0)
-    blob = scenes.blob_tris(args.level)
+    frames = workloads.animation_frames(n_frames, seed=0, budget_log2=budget_log2)
+    blob = scenes.blob_tris(level)
     t = time.perf_counter()
-    d0 = scenes.make_glass_instanced(L, args.level, to_world=frames[0].to_world)
+    d0 = scenes.make_glass_instanced(L, level, to_world=frames[0].to_world)
     mat = int(d0.blas_arrays[0][2][0])
     blas = lib.Blas(blob, mat, device=local, lib=L)
-    base = lib.Scene(scenes.make_glass_instanced(L, args.level, handle=blas), local, L)
+    base = lib.Scene(scenes.make_glass_instanced(L, level, handle=blas), local, L)
     blas_ms = 1e3 * (time.perf_counter() - t)
     t = time.perf_counter()
     clones = [base.clone_instances([f.to_world]) for f in frames]
@@ -273,12 +270,12 @@ def run_animation(args):
     t = time.perf_counter()   # autotuner on frame 0 (untimed)
     tuning = L.autotune(clones[0], cams[frames[0].res], 1 << 23, 16)
     tune_s = time.perf_counter() - t
-    for w in range(args.warmup):   # warm-up at 1/16 of every budget (same wave sizes)
+    for w in range(warmup):   # warm-up at 1/16 of every budget (same wave sizes)
         L.render_batch(jobs(16), stream=stream.cuda_stream, want_energy=False)
     torch.cuda.synchronize(dev)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with ClockSampler(local) as clocks:
-        for k in range(args.steps):
+        for k in range(steps):
             for fl in films:
                 fl.zero_()
             flush.fill_(k & 0xff)
@@ -287,7 +284,7 @@ def run_animation(args):
             ev[k][1].record(stream)
         torch.cuda.synchronize(dev)
     batch_s = sum(a.elapsed_time(b) for a, b in ev) / 1e3
-    value = total * args.steps / batch_s
+    value = total * steps / batch_s
     # launches of one batch, counted by the profiler on an untimed copy of it (direct
     # launches, the same sequence a graph replay makes; progress kernels as in main())
     clones[0].set_profiling(1)
@@ -321,77 +318,93 @@ def run_animation(args):
     torch.cuda.synchronize(dev)
     seq_s = sum(a.elapsed_time(b) for a, b in seq_ev) / 1e3
 
-    # the plain path: every frame baked from world-space triangles, rendered, released
-    nb = min(args.baseline_frames, len(frames))
+    # the plain path: every frame baked from world-space triangles (the shim's build: device
+    # LBVH unless the budget exceeds 4096 photons per primitive), rendered, released
+    nb = min(baseline_frames, len(frames))
     plain_s, plain_ph = 0.0, 0
     for f in frames[:nb]:
-        d = workloads.make_glass_world(L, args.level, f.to_world, blob=blob)
+        d = workloads.make_glass_world(L, level, f.to_world, blob=blob)
         host = np.zeros((f.res, f.res, 4), dtype=np.int64)
         t = time.perf_counter()
-        sc = lib.Scene(d, local, L)
+        sc = lib.Scene(d, local, L, build=abi.BUILD_SAH if f.photons > 4096 * d.n_prims else abi.BUILD_DEVICE)
         sc.render(cams[f.res], f.photons, seed_base=f.seed_base, max_bounce=16, out=host)
         sc.close()
         plain_s += time.perf_counter() - t
         plain_ph += f.photons
 
-    if rank == 0:
-        cfg = {"workload": "animation", "frames": len(frames), "mesh": f"level-{args.level} glass icosphere "
-               f"({20 * 4 ** args.level} triangles) as one shared BLAS, one refit TLAS clone per frame",
-               "resolutions": sorted({f.res for f in frames}), "photons_total": total,
-               "photon_budgets": "log-uniform 2^22-2^27 per frame", "max_bounce": 16,
-               "transforms": "seeded rotation about a random axis 0-360 deg, translation +-0.2 m",
-               "warmup": f"{args.warmup} batches at 1/16 of every budget",
-               "l2": "flushed between timed steps (256 MiB write)", "blas_bake_ms": round(blas_ms, 1),
-               "clone_refit_ms_per_frame": round(clone_ms / len(frames), 3),
-               "tuning": {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
-                          "graph_replay": bool(tuning.use_graphs), "regenerate": bool(tuning.regenerate),
-                          "autotune_s": round(tune_s, 2)}}
-        line = {
-            "metric": "photon paths/s on 1 B200 (batched animation)", "value": value, "unit": "photon paths/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * batch_s / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded scene and transforms)", "config": cfg,
-            "e2e": {"value": total / e2e_s, "unit": "photon paths/s",
-                    "h2d_bytes_per_step": len(frames) * (96 + C.sizeof(abi.Job)),
-                    "d2h_bytes_per_step": film_bytes,
-                    "call": "64 x ftb_scene_set_instance_transforms + ftb_render_batch, films to pinned host"},
-            "one_at_a_time": {
-                "resident_clones": {"value": total / seq_s, "unit": "photon paths/s",
-                                    "call": "ftb_render_forward_device per frame"},
-                "plain_bake_per_frame": {"value": plain_ph / plain_s, "unit": "photon paths/s", "frames": nb,
-                                         "call": "ftb_scene_create + ftb_render_forward + destroy per frame"},
-            },
-            "speedup_e2e_vs_plain": round((total / e2e_s) / (plain_ph / plain_s), 3),
-            "gpu_launches": int(launches),
-            "clocks": clocks.summary(),
-        }
-        print(json.dumps(line), flush=True)
+    cfg = {"workload": "animation", "frames": len(frames), "mesh": f"level-{level} glass icosphere "
+           f"({20 * 4 ** level} triangles) as one shared BLAS, one refit TLAS clone per frame",
+           "resolutions": sorted({f.res for f in frames}), "photons_total": total,
+           "photon_budgets": f"log-uniform 2^{budget_log2[0]:g}-2^{budget_log2[1]:g} per frame", "max_bounce": 16,
+           "transforms": "seeded rotation about a random axis 0-360 deg, translation +-0.2 m",
+           "warmup": f"{warmup} batches at 1/16 of every budget",
+           "l2": "flushed between timed steps (256 MiB write)", "blas_bake_ms": round(blas_ms, 1),
+           "clone_refit_ms_per_frame": round(clone_ms / len(frames), 3),
+           "tuning": {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
+                      "graph_replay": bool(tuning.use_graphs), "regenerate": bool(tuning.regenerate),
+                      "autotune_s": round(tune_s, 2)}}
+    line = {
+        "metric": "photon paths/s on 1 B200 (batched animation)", "value": value, "unit": "photon paths/s",
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * batch_s / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded scene and transforms)", "config": cfg,
+        "e2e": {"value": total / e2e_s, "unit": "photon paths/s",
+                "h2d_bytes_per_step": len(frames) * (96 + C.sizeof(abi.Job)),
+                "d2h_bytes_per_step": film_bytes,
+                "call": "64 x ftb_scene_set_instance_transforms + ftb_render_batch, films to pinned host"},
+        "one_at_a_time": {
+            "resident_clones": {"value": total / seq_s, "unit": "photon paths/s",
+                                "call": "ftb_render_forward_device per frame"},
+            "plain_bake_per_frame": {"value": plain_ph / plain_s, "unit": "photon paths/s", "frames": nb,
+                                     "call": "ftb_scene_create (the shim's build choice) + "
+                                             "ftb_render_forward + destroy per frame"},
+        },
+        "speedup_e2e_vs_plain": round((total / e2e_s) / (plain_ph / plain_s), 3),
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
     for c in clones:
         c.close()
     base.close()
     blas.close()
+    return line
 
 
-def run_serve(args):
-    """Served stream: Poisson arrivals of mixed jobs on resident scenes through the render
-    server (continuous batching), at 80% of the capacity the server measured on the same job
-    mix; p50/p99 latency, aggregate photons/s, and one-job-at-a-time rendering of a sample
-    of the jobs (resident scenes, and baking each job's scene like a scene load)."""
+def run_animation(args):
     import torch
-    from goodphotons_b200 import lib, scenes, workloads
+    from goodphotons_b200 import lib
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    L = lib.load()
-    budget_hi = float(args.serve_budget_log2)
-    probe = workloads.served_jobs(args.jobs, 1.0, seed=0, budget_log2=(20.0, budget_hi))
+    line = animation_batch(args.frames, args.level, args.warmup, args.steps, args.baseline_frames, (22.0, 27.0),
+                           local, lib.load())
+    print(json.dumps(line), flush=True)
+
+
+def serve_stream(n_jobs, budget_hi, sizes, library_build, scene_mb, film_mb, max_active, plain_sample, local, L):
+    """Served stream on resident scenes through the render server (continuous batching) with
+    admission by HBM footprint: the scene library is baked once and held in host memory, the
+    server keeps a working set of it on the device within its HBM budget (wave buffers +
+    film_mb + scene_mb, films and scenes sharing the last two), evicting idle scenes least
+    recently used first.  Poisson
+    arrivals at 80% of the capacity the server measured on the same mix.  Against it: every
+    job of the same stream rendered one at a time on resident scenes (service times measured,
+    latencies of a one-job-at-a-time FIFO server over the same arrivals), and the plain path
+    -- bake the job's scene with the build the drop-in shim picks, render, free -- on a
+    sample of the jobs.  Returns the record."""
+    import torch
+    from goodphotons_b200 import abi, lib, scenes, workloads
+
+    probe = workloads.served_jobs(n_jobs, 1.0, seed=0, budget_log2=(20.0, budget_hi), sizes=sizes)
     keys = sorted({(j.family, j.size) for j in probe})
-    descs, cache, bake_ms = {}, {}, {}
+    descs, cache = {}, {}
+    t = time.perf_counter()
     for key in keys:
         descs[key] = workloads.job_scene(L, *key)
-        t = time.perf_counter()
-        cache[key] = lib.Scene(descs[key], local, L)
-        bake_ms[key] = 1e3 * (time.perf_counter() - t)
+        cache[key] = lib.Scene(descs[key], local, L, build=library_build)
+    library_s = time.perf_counter() - t
+    checkpoint("baking the scene library")
+    library_bytes = sum(sc.footprint(1, 1).scene_bytes for sc in cache.values())
     cams = {}
 
     def cam(res):
@@ -399,15 +412,29 @@ def run_serve(args):
             cams[res] = scenes.default_camera(L, res)
         return cams[res]
 
-    # deployment step: autotune the device's launch shape on a mid-size glass scene of the
-    # mix (the server and the one-at-a-time renders below both use it)
+    # deployment step: autotune the device's launch shape on a mid-size glass scene of the mix
     glass = sorted(k for k in keys if k[0] == "glass") or keys
     t = time.perf_counter()
     tuning = L.autotune(cache[glass[len(glass) // 2]], cam(1024), 1 << 26, 16)
     tune_s = time.perf_counter() - t
+    checkpoint("the serve autotune")
+    film_room = film_mb << 20
+
+    def hbm_budget(srv_waves):
+        return srv_waves + film_room + (scene_mb << 20)
+
+    def evict_all():
+        for sc in cache.values():
+            if sc.resident:
+                sc.evict()
+
+    probe_srv = lib.Server(device=local, max_active=max_active, lib=L)
+    waves = probe_srv.stats().wave_bytes   # the server's two wave buffers at the device's tuning
+    probe_srv.close()
+    checkpoint("the probe server")
 
     def serve(jobs, paced):
-        srv = lib.Server(device=local, max_active=args.max_active, lib=L)
+        srv = lib.Server(device=local, max_active=max_active, hbm_budget=hbm_budget(waves), lib=L)
         ids, films = [None] * len(jobs), [None] * len(jobs)
         t0 = time.perf_counter()
 
@@ -434,72 +461,215 @@ def run_serve(args):
         bad = sum(1 for r in res if r.status != 0)
         makespan = max(r.finish_s for r in res) - min(r.submit_s for r in res)
         lat = np.array([r.finish_s - r.submit_s for r in res])
-        return {"res": res, "makespan": makespan, "lat": lat, "stats": st, "failed": bad}
+        return {"res": res, "makespan": makespan, "lat": lat, "stats": st, "failed": bad,
+                "budget": hbm_budget(waves), "waves": waves}
 
-    # warm-up, then capacity: the whole mix submitted at once (closed loop)
+    # warm-up, then capacity: the whole mix submitted at once (closed loop); the library
+    # starts in host memory each time
+    evict_all()
     serve(probe[: min(8, len(probe))], paced=False)
+    evict_all()
     cap = serve(probe, paced=False)
     photons = sum(j.photons for j in probe)
     cap_jobs_s = len(probe) / cap["makespan"]
     rate = 0.8 * cap_jobs_s
-    jobs = workloads.served_jobs(args.jobs, rate, seed=0, budget_log2=(20.0, budget_hi))
+    jobs = workloads.served_jobs(n_jobs, rate, seed=0, budget_log2=(20.0, budget_hi), sizes=sizes)
+    evict_all()
     with ClockSampler(local) as clocks:
         run = serve(jobs, paced=True)
     lat = run["lat"]
 
-    # one job at a time on a sample: resident scenes, then the plain path (bake per job)
-    sample = jobs[: min(args.serve_sample, len(jobs))]
-    t = time.perf_counter()
-    for j in sample:
+    # one job at a time over the same stream, every scene resident: service time of each job
+    for sc in cache.values():
+        sc.restore()
+    service = np.empty(len(jobs))
+    for i, j in enumerate(jobs):
+        t = time.perf_counter()
         cache[(j.family, j.size)].render(cam(j.res), j.photons, seed_base=j.seed_base, max_bounce=j.max_bounce)
-    seq_s = time.perf_counter() - t
+        service[i] = time.perf_counter() - t
+    seq_lat = workloads.fifo_latencies([j.arrival_s for j in jobs], service)
+
+    # the plain path on a sample: the drop-in shim's per-call bake (device build unless the
+    # budget exceeds 4096 photons per primitive), render, free
+    def shim_build(j):
+        return abi.BUILD_SAH if j.photons > 4096 * descs[(j.family, j.size)].n_prims else abi.BUILD_DEVICE
+
+    sample = jobs[: min(plain_sample, len(jobs))]
     plain_s = 0.0
     for j in sample:
         t = time.perf_counter()
-        sc = lib.Scene(descs[(j.family, j.size)], local, L)
+        sc = lib.Scene(descs[(j.family, j.size)], local, L, build=shim_build(j))
         sc.render(cam(j.res), j.photons, seed_base=j.seed_base, max_bounce=j.max_bounce)
         sc.close()
         plain_s += time.perf_counter() - t
     sample_ph = sum(j.photons for j in sample)
-    served_ph_s = sum(j.photons for j in jobs) / run["makespan"]
+    seq_sample_s = float(service[: len(sample)].sum())
+    total_ph = sum(j.photons for j in jobs)
+    served_ph_s = total_ph / run["makespan"]
     cap_ph_s = photons / cap["makespan"]
+    seq_ph_s = total_ph / float(service.sum())
+    plain_ph_s = sample_ph / plain_s
     for s_ in cache.values():
         s_.close()
-    line = {
-        "metric": "photon paths/s on 1 B200 (served stream)", "value": served_ph_s, "unit": "photon paths/s",
-        "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * run["makespan"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded job stream and scenes)",
-        "config": {"workload": "serve", "jobs": len(jobs), "arrivals": f"Poisson at {rate:.2f} jobs/s "
-                   "(80% of the measured capacity on the same mix)",
-                   "mix": "scene family uniform over cornell / glass / fog_strands; mesh 1k-2M tris log-uniform "
-                          "(glass snapped to icosphere levels, fog to strand counts); resolution 128^2-1024^2 and "
-                          f"photons 2^20-2^{budget_hi:g} log-uniform", "resident_scenes": len(cache),
-                   "scene_bake_ms_total": round(sum(bake_ms.values()), 1), "max_active": args.max_active,
+    st = run["stats"]
+    return {
+        "value": served_ph_s, "makespan_s": run["makespan"],
+        "config": {"jobs": len(jobs), "arrivals": f"Poisson at {rate:.2f} jobs/s (80% of the measured capacity "
+                   "on the same mix)",
+                   "mix": "scene family uniform over cornell / glass / fog_strands; mesh 1k-2M triangles "
+                          f"log-uniform, from a library of {sizes} log-spaced sizes per family (glass: geodesic "
+                          "icospheres of 20 f^2 triangles; fog: strands of 4 segments); resolution 128^2-1024^2 "
+                          f"and photons 2^20-2^{budget_hi:g} log-uniform",
+                   "library": {"scenes": len(cache), "device_bytes": int(library_bytes),
+                               "build": "host SAH" if library_build == abi.BUILD_SAH else "device LBVH",
+                               "bake_s": round(library_s, 2), "held": "host memory; the server restores and "
+                               "evicts scenes on the device within its HBM budget"},
+                   "hbm_budget": {"bytes": int(run["budget"]), "wave_buffers": int(run["waves"]),
+                                  "films_and_scenes": film_room + (scene_mb << 20)},
+                   "max_active": max_active,
                    "tuning": {"wave_slots": tuning.wave_slots, "grid_blocks_per_sm": tuning.grid_mult,
                               "graph_replay": bool(tuning.use_graphs), "sort_rays": bool(tuning.sort_rays),
                               "regenerate": bool(tuning.regenerate), "autotune_s": round(tune_s, 2),
-                              "on": f"{glass[len(glass) // 2][0]} size {glass[len(glass) // 2][1]}"}},
+                              "on": f"glass freq {glass[len(glass) // 2][1]}"}},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "mean": float(lat.mean()), "max": float(lat.max())},
-        "utilization": round(run["stats"].busy_s / run["makespan"], 4),
+        "utilization": round(st.busy_s / run["makespan"], 4),
         "failed_jobs": run["failed"],
+        "scene_residency": {"evictions": int(st.evictions), "restores": int(st.restores)},
         "capacity": {"value": cap_ph_s, "unit": "photon paths/s", "jobs_per_s": cap_jobs_s,
                      "how": f"the {len(probe)}-job mix submitted at once"},
         "one_at_a_time": {
-            "sample_jobs": len(sample),
-            "resident": {"value": sample_ph / seq_s, "unit": "photon paths/s", "call": "ftb_render_forward per job"},
-            "plain_bake_per_job": {"value": sample_ph / plain_s, "unit": "photon paths/s",
-                                   "call": "ftb_scene_create + ftb_render_forward + destroy per job"},
+            "resident": {"value": seq_ph_s, "unit": "photon paths/s", "jobs": len(jobs),
+                         "call": "ftb_render_forward per job, every scene resident",
+                         "latency_s": {"p50": float(np.percentile(seq_lat, 50)),
+                                       "p99": float(np.percentile(seq_lat, 99)), "max": float(seq_lat.max()),
+                                       "how": "FIFO one-job server over the same arrivals, measured service times"}},
+            "plain_bake_per_job": {"value": plain_ph_s, "unit": "photon paths/s", "sample_jobs": len(sample),
+                                   "resident_same_sample": sample_ph / seq_sample_s,
+                                   "call": "ftb_scene_create (the shim's build choice) + ftb_render_forward + "
+                                           "destroy per job"},
         },
-        "capacity_vs_plain": round(cap_ph_s / (sample_ph / plain_s), 3),
-        "capacity_vs_resident_one_at_a_time": round(cap_ph_s / (sample_ph / seq_s), 3),
+        "capacity_vs_plain": round(cap_ph_s / plain_ph_s, 3),
+        "capacity_vs_resident_one_at_a_time": round(cap_ph_s / seq_ph_s, 3),
         "e2e": {"value": served_ph_s, "unit": "photon paths/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(sum(j.res * j.res * 32 for j in jobs)),
                 "call": "ftb_server_submit / ftb_server_wait, films to host"},
-        "gpu_launches": None,
         "clocks": clocks.summary(),
     }
+
+
+def run_serve(args):
+    import torch
+    from goodphotons_b200 import abi, lib
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    L = lib.load()
+    r = serve_stream(args.jobs, float(args.serve_budget_log2), args.serve_sizes, abi.BUILD_SAH, args.serve_scene_mb,
+                     args.serve_film_mb, args.max_active, args.serve_sample, local, L)
+    cfg = dict(workload="serve", **r.pop("config"))
+    line = {"metric": "photon paths/s on 1 B200 (served stream)", "value": r.pop("value"), "unit": "photon paths/s",
+            "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * r.pop("makespan_s"), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded job stream and scenes)",
+            "config": cfg, "gpu_launches": None, **r}
     print(json.dumps(line), flush=True)
+
+
+def plain_config(desc, res, n, mb, lam, steps, local, L):
+    """One configuration of the plain path (one scene, one film, one frame per step) on a
+    resident scene: device-timed frames (CUDA events, L2 flushed between them) and one frame
+    end to end through ftb_render_forward with a pinned host film."""
+    import torch
+    from goodphotons_b200 import lib, scenes
+
+    t = time.perf_counter()
+    sc = lib.Scene(desc, local, L)
+    bake_ms = 1e3 * (time.perf_counter() - t)
+    cam = scenes.default_camera(L, res)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    film = torch.zeros((res, res, 4), dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    sc.render_device(cam, n, film.data_ptr(), seed_base=1 << 40, max_bounce=mb, stream=stream.cuda_stream,
+                     lambda_mode=lam)   # warm-up
+    torch.cuda.synchronize(dev)
+    ms = []
+    for k in range(steps):
+        film.zero_()
+        flush.fill_(k & 0xff)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sc.render_device(cam, n, film.data_ptr(), seed_base=k * n, max_bounce=mb, stream=stream.cuda_stream,
+                         lambda_mode=lam)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(b))
+    host = torch.empty((res, res, 4), dtype=torch.int64, pin_memory=True)
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    sc.render(cam, n, seed_base=1 << 41, max_bounce=mb, out=host.numpy(), lambda_mode=lam)
+    e2e_s = time.perf_counter() - t
+    fp = sc.footprint(res, res)
+    sc.close()
+    return {"value": n * steps / (sum(ms) / 1e3), "unit": "photon paths/s", "steps": steps,
+            "ms_per_step": sum(ms) / steps, "e2e": {"value": n / e2e_s, "unit": "photon paths/s",
+                                                     "call": "ftb_render_forward (resident scene, host film)"},
+            "bake_ms": round(bake_ms, 1), "scene_bytes": int(fp.scene_bytes)}
+
+
+def checkpoint(what):
+    """A checked device-wide wait between untimed phases: a device fault is reported with the
+    phase it followed, not at some later call."""
+    import torch
+    try:
+        torch.cuda.synchronize()
+    except RuntimeError as e:
+        raise RuntimeError(f"device error after {what}: {e}") from e
+
+
+def config_records(args, local, L):
+    """Compact records of the other configurations, measured after the headline: the
+    >= 1M-triangle glass mesh, the Cornell box, fog + strands, a reduced animation batch and a
+    reduced served stream (their full forms: --level 8, --workload cornell | fog_strands |
+    animation | serve)."""
+    from goodphotons_b200 import abi, scenes
+
+    out = {}
+    t = time.perf_counter()
+    r = plain_config(scenes.make_glass(L, level=8), 1024, 1 << 28, 16, abi.LAMBDA_SPD, 2, local, L)
+    r["config"] = {"workload": "glass", "mesh": "level-8 icosphere", "triangles": 20 * 4 ** 8, "film": "1024x1024",
+                   "photons_per_frame": 1 << 28, "max_bounce": 16, "lambda": "emitter SPD"}
+    out["glass_level8"] = r
+    checkpoint("the level-8 glass record")
+    r = plain_config(scenes.make_cornell(L), 256, 1 << 24, 8, abi.LAMBDA_UNIFORM_380_780, 3, local, L)
+    r["config"] = {"workload": "cornell", "film": "256x256", "photons_per_frame": 1 << 24, "max_bounce": 8,
+                   "lambda": "uniform 380-780 nm (FTB_LAMBDA_UNIFORM_380_780)"}
+    out["cornell"] = r
+    checkpoint("the Cornell record")
+    r = plain_config(scenes.make_fog_strands(L), 512, 1 << 26, 32, abi.LAMBDA_SPD, 3, local, L)
+    r["config"] = {"workload": "fog_strands", "strands": 250_000, "segments": 1_000_000, "film": "512x512",
+                   "photons_per_frame": 1 << 26, "max_bounce": 32, "lambda": "emitter SPD"}
+    out["fog_strands"] = r
+    checkpoint("the fog + strands record")
+    a = animation_batch(16, 7, 3, 2, 16, (22.0, 25.0), local, L)
+    out["animation"] = {"value": a["value"], "unit": a["unit"], "ms_per_step": a["ms_per_step"],
+                        "e2e": a["e2e"], "one_at_a_time": a["one_at_a_time"],
+                        "speedup_e2e_vs_plain": a["speedup_e2e_vs_plain"],
+                        "config": {k: a["config"][k] for k in ("frames", "mesh", "resolutions", "photons_total",
+                                                               "photon_budgets")},
+                        "reduced": "16 frames, budgets 2^22-2^25 (full: --workload animation)"}
+    checkpoint("the animation record")
+    sv = serve_stream(150, 25.0, 8, abi.BUILD_DEVICE, 128, 512, 64, 20, local, L)
+    out["serve"] = {"value": sv["value"], "unit": "photon paths/s", "latency_s": sv["latency_s"],
+                    "capacity": sv["capacity"], "one_at_a_time": sv["one_at_a_time"],
+                    "capacity_vs_plain": sv["capacity_vs_plain"],
+                    "capacity_vs_resident_one_at_a_time": sv["capacity_vs_resident_one_at_a_time"],
+                    "scene_residency": sv["scene_residency"], "failed_jobs": sv["failed_jobs"],
+                    "config": sv["config"],
+                    "reduced": "150 jobs, budgets 2^20-2^25, a library of 8 sizes per family on the device build "
+                               "(full: --workload serve)"}
+    out["seconds"] = round(time.perf_counter() - t, 1)
+    return out
 
 
 def main():
@@ -511,13 +681,17 @@ def main():
     ap.add_argument("--workload", default="glass", choices=sorted(WORKLOADS) + ["animation", "serve"])
     ap.add_argument("--jobs", type=int, default=2000, help="serve: jobs in the stream")
     ap.add_argument("--serve-budget-log2", type=float, default=28.0, help="serve: largest photon budget, log2")
-    ap.add_argument("--serve-sample", type=int, default=40, help="serve: jobs rendered one at a time")
+    ap.add_argument("--serve-sample", type=int, default=40, help="serve: jobs of the plain (bake per job) sample")
+    ap.add_argument("--serve-sizes", type=int, default=24, help="serve: library mesh sizes per family")
+    ap.add_argument("--serve-scene-mb", type=int, default=512, help="serve: device MiB for resident scenes")
+    ap.add_argument("--serve-film-mb", type=int, default=4096, help="serve: device MiB for admitted films")
     ap.add_argument("--max-active", type=int, default=64, help="serve: jobs admitted at once")
     ap.add_argument("--frames", type=int, default=64, help="animation: frames")
     ap.add_argument("--baseline-frames", type=int, default=64, help="animation: frames of the plain baseline")
     ap.add_argument("--level", type=int, default=7)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' records")
     ap.add_argument("--photons", type=int, default=0, help="photons per step (default: the workload's frame)")
     ap.add_argument("--tuning", default="",
                     help="wave_slots,blocks_per_sm,graphs[,sort_rays[,regenerate]] instead of the autotuner")
@@ -741,6 +915,10 @@ def main():
         if cpu and lam:
             cpu["lambda"] = "drawn from the emitter SPD: the reference has no uniform-band policy"
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs and args.workload == "glass" and args.hero == 1:
+        configs = config_records(args, local, L)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "photon paths/s", "n_gpus": world,
@@ -750,6 +928,7 @@ def main():
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": gpu_launches,
             "device_bvh_build": device_build,
             "clocks": clocks.summary(),
+            "configs": configs,
             "notes": "fp64 path arithmetic (reference order), fp32 conservative BVH culling, int64 fixed-point film",
         }
         print(json.dumps(line), flush=True)

@@ -9,6 +9,8 @@ FTB_OK = 0
 LAMBDA_SPD = 0
 LAMBDA_UNIFORM_380_780 = 1
 BUILD_SAH, BUILD_DEVICE = 0, 1
+(OK, ERR_INVALID, ERR_NO_DEVICE, ERR_UNSUPPORTED, ERR_CUDA, ERR_OOM, ERR_DEVICE_LIMIT, ERR_TOO_LARGE,
+ ERR_TIMEOUT) = range(9)
 
 STATUS_NAMES = {
     0: "FTB_OK", 1: "FTB_ERR_INVALID", 2: "FTB_ERR_NO_DEVICE", 3: "FTB_ERR_UNSUPPORTED",
@@ -138,7 +140,7 @@ class Tuning(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_active", C.c_int32), ("film_budget", C.c_uint64),
-                ("wave_slots", C.c_int32), ("hero_max", C.c_int32)]
+                ("wave_slots", C.c_int32), ("hero_max", C.c_int32), ("hbm_budget", C.c_uint64)]
 
 
 class Request(C.Structure):
@@ -155,7 +157,9 @@ class JobResult(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("queued", C.c_int64), ("active", C.c_int64), ("photons_done", C.c_int64),
-                ("waves", C.c_int64), ("busy_s", C.c_double), ("film_bytes", C.c_uint64)]
+                ("waves", C.c_int64), ("busy_s", C.c_double), ("film_bytes", C.c_uint64),
+                ("scene_bytes", C.c_uint64), ("wave_bytes", C.c_uint64), ("evictions", C.c_int64),
+                ("restores", C.c_int64)]
 
 
 STRUCTS = {
@@ -172,7 +176,8 @@ STRUCTS = {
 EXPORTS = [
     "ftb_last_error", "ftb_abi_version", "ftb_available", "ftb_device_name", "ftb_mem_info",
     "ftb_forward_supported", "ftb_camera_look_at", "ftb_emission_cdf", "ftb_scene_create",
-    "ftb_scene_destroy", "ftb_scene_footprint", "ftb_scene_power", "ftb_render_forward",
+    "ftb_scene_destroy", "ftb_scene_footprint", "ftb_scene_evict", "ftb_scene_restore",
+    "ftb_scene_resident", "ftb_scene_power", "ftb_render_forward",
     "ftb_render_forward_device", "ftb_session_begin", "ftb_session_batch",
     "ftb_session_hits0", "ftb_session_download", "ftb_session_end", "ftb_trace_log",
     "ftb_scene_set_profiling", "ftb_scene_profile", "ftb_render_forward_noalloc",
@@ -181,4 +186,4 @@ EXPORTS = [
     "ftb_server_get_stats", "ftb_server_destroy", "ftb_get_tuning", "ftb_set_tuning", "ftb_autotune",
 ]
 NOALLOC_MAX_PHOTONS = 32768
-NOALLOC_SCRATCH_BYTES = 21060864
+NOALLOC_SCRATCH_BYTES = 21062912

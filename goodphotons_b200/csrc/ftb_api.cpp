@@ -16,6 +16,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/ftb200.h"
@@ -206,15 +207,23 @@ struct DevBlock {
     int device = 0;
     std::vector<void*> ptrs;
     uint64_t bytes = 0;
+    // Residency (ftb_scene_evict / ftb_scene_restore): the size of each allocation, whether
+    // it came from the stream-ordered allocator (a restore), and host copies of the arrays
+    // (made on the first eviction and kept, so later evictions only free).
+    std::vector<size_t> sizes;
+    std::vector<char> pooled;
+    std::vector<std::vector<unsigned char>> saved;
+    std::vector<void*> evicted;   // the allocations' addresses when they were freed
+    bool resident = true;
     DevBlock() = default;
     DevBlock(const DevBlock&) = delete;
     DevBlock& operator=(const DevBlock&) = delete;
     ~DevBlock() {
-        if (ptrs.empty()) return;
+        if (ptrs.empty() || !resident) return;
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(device);
-        for (void* p : ptrs) cudaFree(p);
+        for (void* p : ptrs) cudaFree(p);   // waits for the device, pooled allocations too
         cudaSetDevice(cur);
     }
 };
@@ -225,6 +234,8 @@ ftb_status upload(DevBlock& blk, const T* host, size_t n, const T** out, const c
     void* p = nullptr;
     CK(cudaMalloc(&p, n * sizeof(T)), what);
     blk.ptrs.push_back(p);
+    blk.sizes.push_back(n * sizeof(T));
+    blk.pooled.push_back(0);
     blk.bytes += n * sizeof(T);
     CK(cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice), what);
     *out = (const T*)p;
@@ -336,6 +347,7 @@ struct ftb_scene {
     DevInst* d_inst = nullptr;
     double power = 0.0;
     uint64_t scene_bytes = 0;
+    std::vector<int> field_alloc;                  // while evicted: the allocation of each device pointer of `dev`
     std::shared_ptr<Engine> eng;                   // render resources of the device
     int32_t prof_mode = 0;
     ProfSink* prof = nullptr;
@@ -376,7 +388,80 @@ ftb_status upload(ftb_scene* s, const T* host, size_t n, const T** out, const ch
 
 bool mat_type_supported(int t) {
     return t == FTB_MAT_DIFFUSE || t == FTB_MAT_DIELECTRIC || t == FTB_MAT_GLOSSY ||
-           t == FTB_MAT_DIFFUSE_TRANSMIT || t == FTB_MAT_FILTER;
+           t == FTB_MAT_DIFFUSE_TRANSMIT || t == FTB_MAT_FILTER || t == FTB_MAT_MIRROR ||
+           t == FTB_MAT_HALF_MIRROR;
+}
+
+// isPlanarMirrorMat (scene.h:356-360)
+bool planar_mirror(const ftb_material& m) {
+    return m.type == FTB_MAT_MIRROR || m.type == FTB_MAT_HALF_MIRROR ||
+           (m.type == FTB_MAT_GLOSSY && m.roughness <= 0.0);
+}
+
+constexpr int kMaxMirrorPlanes = 64;   // Scene::kMaxMirrorPlanes (scene.h:1641)
+
+// Scene::buildMirrorPlanes (scene.h:1646-1720) over the world triangles: each planar-mirror
+// triangle's unit normal (Tri::finalize's, normalized again), flipped so its largest
+// component is positive, and offset d = dot(n, v0) form a key quantized to 1e-6 in
+// direction and 10 um in offset; triangles with equal keys share a plane, planes numbered
+// in first-seen order, each with the AABB of its vertices and its total area; the boxes are
+// padded by 1e-6 (1 + diagonal).  More than 64 planes -- where the reference keeps the 64
+// largest by an unstable sort -- is reported as unsupported.
+ftb_status build_mirror_planes(const ftb_scene_desc* d, std::vector<DevPlane>& out) {
+    out.clear();
+    struct Acc { DevPlane p; long long key[4]; };
+    std::vector<Acc> acc;
+    std::unordered_map<std::string, int> by_key;
+    for (int64_t i = 0; i < d->n_tris; ++i) {
+        if (!planar_mirror(d->mats[d->tri_mat[i]])) continue;
+        const double* v = d->tri_v + 9 * i;
+        const double e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+        const double e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+        double c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        const double cl = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        double n[3] = {c[0] / cl, c[1] / cl, c[2] / cl};   // Tri::finalize: normalize(cross)
+        const double nl = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (nl < 1e-12) continue;
+        const double inv = 1.0 / nl;
+        for (double& x : n) x = x * inv;
+        const double sx = std::fabs(n[0]), sy = std::fabs(n[1]), sz = std::fabs(n[2]);
+        const double lead = (sx >= sy && sx >= sz) ? n[0] : ((sy >= sz) ? n[1] : n[2]);
+        if (lead < 0.0) for (double& x : n) x = -x;
+        const double off = n[0] * v[0] + n[1] * v[1] + n[2] * v[2];
+        const long long key[4] = {std::llround(n[0] * 1e6), std::llround(n[1] * 1e6), std::llround(n[2] * 1e6),
+                                  std::llround(off * 1e5)};
+        const std::string ks(reinterpret_cast<const char*>(key), sizeof key);
+        auto it = by_key.find(ks);
+        int idx;
+        if (it == by_key.end()) {
+            idx = (int)acc.size();
+            by_key.emplace(ks, idx);
+            Acc a;
+            for (int k = 0; k < 3; ++k) { a.p.n[k] = n[k]; a.p.lo[k] = v[k]; a.p.hi[k] = v[k]; }
+            a.p.d = off;
+            std::memcpy(a.key, key, sizeof key);
+            acc.push_back(a);
+        } else {
+            idx = it->second;
+        }
+        DevPlane& p = acc[(size_t)idx].p;
+        for (int q = 0; q < 3; ++q)
+            for (int k = 0; k < 3; ++k) {
+                p.lo[k] = std::min(p.lo[k], v[3 * q + k]);
+                p.hi[k] = std::max(p.hi[k], v[3 * q + k]);
+            }
+    }
+    if ((int)acc.size() > kMaxMirrorPlanes)
+        return fail(FTB_ERR_UNSUPPORTED, "more than 64 mirror planes (the reference keeps the 64 largest by an "
+                    "unstable sort)");
+    for (Acc& a : acc) {
+        DevPlane& p = a.p;
+        const double dx = p.hi[0] - p.lo[0], dy = p.hi[1] - p.lo[1], dz = p.hi[2] - p.lo[2];
+        const double pad = 1e-6 * (1.0 + std::sqrt(dx * dx + dy * dy + dz * dz));
+        for (int k = 0; k < 3; ++k) { p.lo[k] = p.lo[k] - pad; p.hi[k] = p.hi[k] + pad; }
+        out.push_back(p);
+    }
+    return FTB_OK;
 }
 
 // Validation shared by ftb_forward_supported and ftb_scene_create.  Returns FTB_OK,
@@ -427,10 +512,7 @@ ftb_status check_desc(const ftb_scene_desc* d) {
             return fail(FTB_ERR_INVALID, "material " + std::to_string(i) + ": spectrum index out of range");
         if (!mat_type_supported(m.type))
             return fail(FTB_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": type " + std::to_string(m.type) +
-                        " is not on this path (mirror / half-mirror need the specular camera connectors)");
-        if (m.type == FTB_MAT_GLOSSY && !(m.roughness > 0.0))
-            return fail(FTB_ERR_UNSUPPORTED, "material " + std::to_string(i) +
-                        ": glossy with roughness <= 0 is a planar mirror (specular connector)");
+                        " is not on this path");
     }
     for (int64_t i = 0; i < d->n_tris; ++i)
         if (d->tri_mat[i] < 0 || d->tri_mat[i] >= d->n_mats) return fail(FTB_ERR_INVALID, "triangle material out of range");
@@ -439,6 +521,9 @@ ftb_status check_desc(const ftb_scene_desc* d) {
         if (d->mats[d->sph_mat[i]].type == FTB_MAT_DIELECTRIC)
             return fail(FTB_ERR_UNSUPPORTED, "dielectric sphere: the reference splats it through its analytic "
                         "sphere connector, which is not on this path");
+        if (planar_mirror(d->mats[d->sph_mat[i]]))
+            return fail(FTB_ERR_UNSUPPORTED, "mirror sphere: the reference splats it through its spherical "
+                        "mirror connector, which is not on this path");
     }
     for (int64_t i = 0; i < d->n_curves; ++i)
         if (d->curve_mat[i] < 0 || d->curve_mat[i] >= d->n_mats) return fail(FTB_ERR_INVALID, "curve material out of range");
@@ -455,8 +540,8 @@ ftb_status check_desc(const ftb_scene_desc* d) {
             return fail(FTB_ERR_INVALID, "medium spectrum index out of range");
         if (m.bound < FTB_BOUND_NONE || m.bound > FTB_BOUND_SPHERE) return fail(FTB_ERR_INVALID, "bad medium bound");
     }
-    for (int i = 0; i < d->n_spectra; ++i) (void)i;
-    return FTB_OK;
+    std::vector<DevPlane> planes;
+    return build_mirror_planes(d, planes);
 }
 
 // Affine::inverse (linalg.h:129-144): 3x3 row-major then t; identity when singular.
@@ -660,18 +745,19 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         table.clear();
         int64_t g = 0;
         int32_t max_bounce = 0, slots = W;
-        bool inst = false, media = false, shapes = false;
+        bool inst = false, media = false, shapes = false, mirrors = false;
         int bundles = -1, views = -1;
         while (j < base.size() && (int)table.size() < ftb::kWaveJobs) {
             const int64_t left = count[j] - done_in_job;
             if (left <= 0) { ++j; done_in_job = 0; continue; }
             const int is_bundle = base[j].hero_c > 1 ? 1 : 0;
-            const int nv = std::max(1, base[j].n_views);
+            const int nv = ftb::conn_fanout(base[j]);
             if ((bundles >= 0 && is_bundle != bundles) || (views >= 0 && nv != views)) break;
             bundles = is_bundle;
             views = nv;
-            // a path queues at most 2 connections per view per bounce and a refilled slot one
-            // more per view; the shadow queue holds 3W records, so V views get W / V slots
+            // a path queues at most 2 connections per view (and per mirror) per bounce and a
+            // refilled slot one more; the shadow queue holds 3W records, so a fan-out of F
+            // connections per vertex gets W / F slots
             slots = std::max(1, W / nv);
             const int64_t m = std::min<int64_t>(left, (int64_t)1 << 30);
             ftb::DevJob J = base[j];
@@ -684,6 +770,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
             inst |= J.sc.n_inst > 0;
             media |= J.sc.n_med > 0;
             shapes |= ftb::scene_has_shapes(J.sc);
+            mirrors |= J.sc.n_planes > 0;
             g += m;
             done_in_job += m;
             if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
@@ -702,6 +789,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         kind.bundles = bundles == 1;
         kind.media = media;
         kind.shapes = shapes;
+        kind.mirrors = mirrors;
         e = ftb::launch_stream(w, kind, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
                                s->eng->graphs[k & 1]);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
@@ -710,17 +798,17 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
     while (j < base.size()) {
         table.clear();
         int32_t slots = 0, max_bounce = 0;
-        bool inst = false, media = false, shapes = false;
+        bool inst = false, media = false, shapes = false, mirrors = false;
         int bundles = -1;   // a wave holds either one-wavelength jobs or bundles, not both
-        // A path queues at most 2 connections per view per bounce and the shadow queue holds
-        // 2W records, so a wave of multi-camera jobs carries W / views slots.
+        // A path queues at most 2 connections per view (and per mirror) per bounce, so a wave
+        // of jobs with a fan-out of F connections per vertex carries W / F slots.
         int32_t cap = W;
         while (j < base.size() && slots < cap && (int)table.size() < ftb::kWaveJobs) {
             int64_t left = count[j] - done_in_job;
             if (left <= 0) { ++j; done_in_job = 0; continue; }
             const int is_bundle = base[j].hero_c > 1 ? 1 : 0;
             if (bundles >= 0 && is_bundle != bundles) break;
-            const int32_t jcap = std::max(1, W / std::max(1, base[j].n_views));
+            const int32_t jcap = std::max(1, W / ftb::conn_fanout(base[j]));
             if (jcap < cap && slots >= jcap) break;   // this job needs a roomier wave of its own
             cap = std::min(cap, jcap);
             bundles = is_bundle;
@@ -734,6 +822,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
             inst |= J.sc.n_inst > 0;
             media |= J.sc.n_med > 0;
             shapes |= ftb::scene_has_shapes(J.sc);
+            mirrors |= J.sc.n_planes > 0;
             slots += m;
             done_in_job += m;
             if (done_in_job >= count[j]) { ++j; done_in_job = 0; }
@@ -750,6 +839,7 @@ ftb_status run_jobs(ftb_scene* s, const std::vector<ftb::DevJob>& base, const st
         kind.bundles = bundles == 1;
         kind.media = media;
         kind.shapes = shapes;
+        kind.mirrors = mirrors;
         e = ftb::launch_wave(w, max_bounce, kind, f, s->sms, s->eng->shape, ws, s->prof_mode ? s->prof : nullptr,
                              s->eng->graphs[k & 1]);
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
@@ -809,6 +899,100 @@ ftb_status check_params(const ftb_scene* s, const ftb_camera* cam, const ftb_ren
     if (p->lambda_mode != FTB_LAMBDA_SPD && p->lambda_mode != FTB_LAMBDA_UNIFORM_380_780)
         return fail(FTB_ERR_INVALID, "unknown lambda_mode");
     if (!(s->power > 0.0)) return fail(FTB_ERR_UNSUPPORTED, "scene emits no power");
+    if (s->tables && !s->tables->resident) return fail(FTB_ERR_INVALID, "scene is evicted from the device");
+    if (p->hero_c > 1 && s->dev.n_med == 0 && s->dev.n_planes > 0)
+        return fail(FTB_ERR_UNSUPPORTED, "hero bundles in a scene with planar mirrors (use hero_c 1)");
+    return FTB_OK;
+}
+
+// ---- device residency -------------------------------------------------------------------
+// The device pointers of a scene's view, in a fixed order.
+constexpr int kDevPtrFields = 12;
+void dev_ptr_fields(DevScene& d, const void** (&f)[kDevPtrFields]) {
+    f[0] = (const void**)&d.nodes; f[1] = (const void**)&d.recs; f[2] = (const void**)&d.tri_n;
+    f[3] = (const void**)&d.spec; f[4] = (const void**)&d.tw; f[5] = (const void**)&d.tv;
+    f[6] = (const void**)&d.mats; f[7] = (const void**)&d.emit; f[8] = (const void**)&d.emit_cdf;
+    f[9] = (const void**)&d.med; f[10] = (const void**)&d.inst; f[11] = (const void**)&d.planes;
+}
+// A scene can leave the device when its view reads only its own tables: no instances (their
+// TLAS and BLAS assets live elsewhere) and no clones sharing the tables.
+bool evictable(const ftb_scene* s) {
+    return s->tables && !s->own && s->blas.empty() && s->tables.use_count() == 1 && s->dev.n_inst == 0;
+}
+
+// Frees the scene's device tables (host copies are made on the first eviction).  The caller
+// guarantees that no render of the scene is in flight.  stream: where pooled allocations are
+// freed (stream-ordered); allocations of the scene's bake are freed with cudaFree, which waits
+// for the device.  eng->mu held.
+ftb_status evict_locked(ftb_scene* s, cudaStream_t stream) {
+    DevBlock& b = *s->tables;
+    if (!b.resident) return FTB_OK;
+    if (!evictable(s)) return fail(FTB_ERR_UNSUPPORTED, "only a scene without instances or clones can be evicted");
+    const void** f[kDevPtrFields];
+    dev_ptr_fields(s->dev, f);
+    std::vector<int> fa(kDevPtrFields, -1);
+    for (int i = 0; i < kDevPtrFields; ++i) {
+        if (!*f[i]) continue;
+        for (size_t k = 0; k < b.ptrs.size(); ++k)
+            if (b.ptrs[k] == *f[i]) fa[i] = (int)k;
+        if (fa[i] < 0) return fail(FTB_ERR_UNSUPPORTED, "scene view points inside an allocation");
+    }
+    DeviceGuard guard(s->device);
+    if (b.saved.size() != b.ptrs.size()) {
+        b.saved.assign(b.ptrs.size(), {});
+        for (size_t k = 0; k < b.ptrs.size(); ++k) {
+            b.saved[k].resize(b.sizes[k]);
+            CK(cudaMemcpy(b.saved[k].data(), b.ptrs[k], b.sizes[k], cudaMemcpyDeviceToHost), "evict copy");
+        }
+    }
+    b.evicted = b.ptrs;
+    for (size_t k = 0; k < b.ptrs.size(); ++k) {
+        CK(b.pooled[k] ? cudaFreeAsync(b.ptrs[k], stream) : cudaFree(b.ptrs[k]), "evict free");
+        b.ptrs[k] = nullptr;
+    }
+    for (int i = 0; i < kDevPtrFields; ++i) *f[i] = nullptr;
+    s->field_alloc = fa;
+    b.resident = false;
+    return FTB_OK;
+}
+
+// Uploads the tables again (stream-ordered allocations and copies on `stream`; work issued
+// to the same stream afterwards, or ordered after it, sees them).  eng->mu held.
+ftb_status restore_locked(ftb_scene* s, cudaStream_t stream) {
+    DevBlock& b = *s->tables;
+    if (b.resident) return FTB_OK;
+    DeviceGuard guard(s->device);
+    // The emitter table holds device pointers itself (each emitter's wavelength CDF, an
+    // allocation of this block): its host copy is re-pointed at the new allocations as they
+    // are made, before it is uploaded (allocations are restored in upload order, and the
+    // CDFs were uploaded before the table).
+    const int emit_alloc = s->field_alloc[7];
+    for (size_t k = 0; k < b.ptrs.size(); ++k) {
+        if ((int)k == emit_alloc) {
+            DevEmit* em = reinterpret_cast<DevEmit*>(b.saved[k].data());
+            const size_t ne = b.sizes[k] / sizeof(DevEmit);
+            for (size_t e = 0; e < ne; ++e)
+                for (size_t q = 0; q < k; ++q)
+                    if (em[e].cdf && (const void*)em[e].cdf == b.evicted[q]) { em[e].cdf = (const double*)b.ptrs[q]; break; }
+        }
+        void* p = nullptr;
+        cudaError_t e = cudaMallocAsync(&p, b.sizes[k], stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p, b.saved[k].data(), b.sizes[k], cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            if (p) cudaFreeAsync(p, stream);
+            for (size_t q = 0; q < k; ++q) { cudaFreeAsync(b.ptrs[q], stream); b.ptrs[q] = nullptr; }
+            return fail(e == cudaErrorMemoryAllocation ? FTB_ERR_OOM : FTB_ERR_CUDA,
+                        std::string("restore: ") + cudaGetErrorString(e));
+        }
+        b.ptrs[k] = p;
+        b.pooled[k] = 1;
+    }
+    const void** f[kDevPtrFields];
+    dev_ptr_fields(s->dev, f);
+    for (int i = 0; i < kDevPtrFields; ++i)
+        if (s->field_alloc[i] >= 0) *f[i] = b.ptrs[(size_t)s->field_alloc[i]];
+    b.resident = true;
     return FTB_OK;
 }
 
@@ -827,6 +1011,26 @@ ftb_status check_render_params(const ftb_scene* s, const ftb_camera* cam, const 
     return check_params(s, cam, p);
 }
 std::mutex& scene_mutex(const ftb_scene* s) { return s->eng->mu; }
+
+ftb_status scene_evict(const ftb_scene* cs, cudaStream_t stream) {
+    ftb_scene* s = const_cast<ftb_scene*>(cs);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    return evict_locked(s, stream);
+}
+ftb_status scene_restore(const ftb_scene* cs, cudaStream_t stream) {
+    ftb_scene* s = const_cast<ftb_scene*>(cs);
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    return restore_locked(s, stream);
+}
+bool scene_resident(const ftb_scene* s) {
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    return !s->tables || s->tables->resident;
+}
+bool scene_evictable(const ftb_scene* s) {
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    return evictable(s);
+}
+uint64_t scene_device_bytes(const ftb_scene* s) { return s->scene_bytes; }
 
 bool scene_internals(const ftb_scene* s, DevScene* dev, int* device, int* sms, double* power) {
     if (!s) return false;
@@ -1151,6 +1355,12 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
         for (int a = 0; a < 3; ++a) { o.bmin[a] = m.bmin[a]; o.bmax[a] = m.bmax[a]; o.center[a] = m.center[a]; }
     }
     UP(med.data(), med.size(), &D.med, "upload media");
+    {   // planar mirrors the camera connections reflect in (already validated by check_desc)
+        std::vector<DevPlane> planes;
+        build_mirror_planes(d, planes);
+        UP(planes.data(), planes.size(), &D.planes, "upload mirror planes");
+        D.n_planes = (int32_t)planes.size();
+    }
 #undef UP
     D.n_nodes = (int32_t)bvh.nodes.size();
     D.n_recs = (int32_t)recs.size();
@@ -1170,6 +1380,31 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
 ftb_status ftb_scene_destroy(ftb_scene* s) {
     delete s;
     return FTB_OK;
+}
+
+ftb_status ftb_scene_evict(ftb_scene* s) {
+    if (!s) return fail(FTB_ERR_INVALID, "null scene");
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    if (!s->tables || !s->tables->resident) return FTB_OK;
+    if (!evictable(s)) return fail(FTB_ERR_UNSUPPORTED, "only a scene without instances or clones can be evicted");
+    DeviceGuard guard(s->device);
+    CK(cudaDeviceSynchronize(), "evict: wait for the device");   // renders of the scene still in flight
+    return evict_locked(s, nullptr);
+}
+
+ftb_status ftb_scene_restore(ftb_scene* s) {
+    if (!s) return fail(FTB_ERR_INVALID, "null scene");
+    std::lock_guard<std::mutex> lk(s->eng->mu);
+    DeviceGuard guard(s->device);
+    ftb_status st = restore_locked(s, nullptr);
+    if (st != FTB_OK) return st;
+    CK(cudaStreamSynchronize(nullptr), "restore");
+    return FTB_OK;
+}
+
+int ftb_scene_resident(const ftb_scene* s) {
+    if (!s) return 0;
+    return ftb::scene_resident(s) ? 1 : 0;
 }
 
 ftb_status ftb_blas_create(const ftb_blas_desc* d, int32_t device, ftb_blas** out) {
@@ -1556,8 +1791,10 @@ ftb_status ftb_autotune(ftb_scene* s, const ftb_camera* cam, int64_t n, int32_t 
 
 ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cams, int32_t max_bounce,
                              int32_t frac_bits, int32_t hero_c, ftb_session** out) {
-    if (!s || !cams || n_cams < 1 || !out) return fail(FTB_ERR_INVALID, "bad session arguments");
+    if (!s || !cams || n_cams < 1 || n_cams > 65535 || !out) return fail(FTB_ERR_INVALID, "bad session arguments");
     if (max_bounce < 0 || max_bounce > 1024) return fail(FTB_ERR_INVALID, "max_bounce out of range");
+    if (hero_c > 1 && s->dev.n_med == 0 && s->dev.n_planes > 0)
+        return fail(FTB_ERR_UNSUPPORTED, "hero bundles in a scene with planar mirrors (use hero_c 1)");
     DeviceGuard guard(s->device);
     auto ss = new ftb_session();
     ss->scene = s;
@@ -1595,6 +1832,7 @@ ftb_status ftb_session_batch(ftb_session* ss, int64_t n, uint64_t seed_base) {
     if (!ss || n < 0) return fail(FTB_ERR_INVALID, "bad batch arguments");
     ftb_scene* s = ss->scene;
     std::lock_guard<std::mutex> lk(s->eng->mu);
+    if (s->tables && !s->tables->resident) return fail(FTB_ERR_INVALID, "scene is evicted from the device");
     DeviceGuard guard(s->device);
     ftb_status st = ensure_frame(s, 0);
     if (st != FTB_OK) return st;

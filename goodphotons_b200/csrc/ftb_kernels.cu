@@ -1056,6 +1056,77 @@ __device__ void connect_volume(const DevScene& sc, const DevJob& J, const Wave& 
     }
 }
 
+// ------------------------------------------------------------------ planar mirrors -----
+// A mirror connection in the shadow queue (marked by a negative pixel, ~pixel): vertex p,
+// the direction wP toward the eye's mirror image and the distance dP to the mirror point in
+// the origin / direction / max fields, view | plane << 16, the wavelength, the vertex factor
+// beta * (weight * shape) and cieX/Y/Z(lambda) in place of the film increments -- the
+// mirror's reflectance is known only once k_shadow has seen which mirror the eye meets.
+__device__ __forceinline__ void push_mirror(const Wave& w, const Frame& f, int job, int view, int plane, D3 p, D3 wP,
+                                            double dP, double a, double lam, const double* cie, int pix) {
+    int i = agg_inc(&w.counts[kShadowCount]);
+    if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); return; }
+    w.sox[i] = p.x; w.soy[i] = p.y; w.soz[i] = p.z;
+    w.sdx[i] = wP.x; w.sdy[i] = wP.y; w.sdz[i] = wP.z;
+    w.smax[i] = dP; w.spix[i] = ~pix;
+    w.sval[i] = a; w.slam[i] = lam;
+    w.sxyz[i] = cie[0]; w.sxyz[w.S + i] = cie[1]; w.sxyz[2 * (size_t)w.S + i] = cie[2];
+    w.sjob[i] = job; w.sview[i] = view | (plane << 16);
+}
+
+// camSpecularSplatAll / camSpecularSplatVolumeAll (render.h:1515-1585) over the planar
+// mirrors: connectSpecularPlane's geometry (render.h:1334-1366) -- the vertex and the eye on
+// the same side of the plane, the path unfolded through the eye's mirror image, the vertex
+// factor (SpecVtx::shape, render.h:897-901), the mirror point inside the plane's box and in
+// the image -- then a mirror record for k_shadow.  `volume`: a medium scatter with incoming
+// direction nw and HG g; otherwise a surface with normal nw.  `weight`: the vertex's albedo.
+__device__ __noinline__ void connect_mirrors(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f,
+                                             int job, D3 p, bool volume, D3 nw, double g, double lam,
+                                             const double* cie, double beta, double weight) {
+    for (int k = 0; k < sc.n_planes; ++k) {
+        const DevPlane& mp = sc.planes[k];
+        const D3 pn = ld3(mp.n);
+        for (int v = 0; v < view_count(J); ++v) {
+            const DevCam& cam = view_cam(J, v);
+            const D3 eye = ld3(cam.eye);
+            const double se = dot(pn, eye) - mp.d;
+            const double sp = dot(pn, p) - mp.d;
+            if (!(se * sp > 0.0)) continue;
+            const D3 eye_m = eye - pn * (2.0 * se);
+            D3 wP = eye_m - p;
+            const double D = len(wP);
+            if (D < 1e-9) continue;
+            wP = wP * (1.0 / D);
+            double shape;
+            if (volume) {
+                shape = hg_phase(dot(nw, wP), g);
+            } else {
+                const double cs = dot(nw, wP);
+                shape = cs <= 0.0 ? -1.0 : cs / PI_D;
+            }
+            if (shape < 0.0) continue;
+            const double denom = dot(pn, wP);
+            if (fabs(denom) < 1e-12) continue;
+            const double dP = (mp.d - dot(pn, p)) / denom;
+            if (dP <= 1e-7 || dP >= D - 1e-7) continue;
+            const D3 R = p + wP * dP;
+            if (R.x < mp.lo[0] || R.x > mp.hi[0] || R.y < mp.lo[1] || R.y > mp.hi[1] || R.z < mp.lo[2] ||
+                R.z > mp.hi[2])
+                continue;
+            int px, py; double cos_cam, dist2e;
+            if (!cam_project(cam, R, px, py, cos_cam, dist2e)) continue;
+            if (cam_pixel_solid_angle(cam, cos_cam) <= 0.0) continue;
+            push_mirror(w, f, job, v, k, p, wP, dP, beta * (weight * shape), lam, cie, py * cam.rx + px);
+        }
+    }
+}
+
+// isPlanarMirrorMat (scene.h:356-360)
+__device__ __forceinline__ bool planar_mirror(const DevMat& m) {
+    return m.type == FTB_MAT_MIRROR || m.type == FTB_MAT_HALF_MIRROR ||
+           (m.type == FTB_MAT_GLOSSY && m.roughness <= 0.0);
+}
+
 // ------------------------------------------------------------------ tallies ------------
 __device__ __forceinline__ long long to_fixed(double v, double scale_inv, int32_t* status) {
     double s = v * scale_inv;
@@ -1302,7 +1373,7 @@ __device__ __forceinline__ double sample_uniform_band(const DevEmit& em, double 
 }
 
 // ------------------------------------------------------------------ kernels ------------
-template <bool MEDIA, bool STREAM>
+template <bool MEDIA, bool STREAM, bool MIRROR>
 __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
                                               int32_t* out_count) {
     const int32_t n_jobs = w.params[0];
@@ -1337,6 +1408,7 @@ __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit(Wave w, const DevJo
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(beta, J.tally_scale_inv, f.status));
         const double cie[3] = {cie_x(lam), cie_y(lam), cie_z(lam)};
         connect_surface<MEDIA>(sc, J, w, f, j, origin, emit_n, emit_n, emit_n, lam, cie, beta, 1.0);
+        if (MIRROR && sc.n_planes > 0) connect_mirrors(sc, J, w, f, j, origin, false, emit_n, 0.0, lam, cie, beta, 1.0);
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(beta, J.tally_scale_inv, f.status));
@@ -1523,7 +1595,7 @@ __device__ void refract_or_reflect(const DevScene& sc, const DevMat& m, const Hi
 }
 
 // One bounce of Renderer::tracePhoton's loop body (render.h:2013-2238).
-template <bool MEDIA, bool INST, bool SHAPES>
+template <bool MEDIA, bool INST, bool SHAPES, bool MIRROR>
 __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_MINB) k_shade(Wave w, const DevJob* __restrict__ jobs,
                                                                Frame f, PathState in, const int32_t* in_count,
                                                                PathState out, int32_t* out_count) {
@@ -1576,6 +1648,8 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
             const DevMed& sm = sc.med[scatter_med];
             load_cie();
             connect_volume(sc, J, w, f, j, sm, mp, rd, lam, cie, beta);
+            if (MIRROR && sc.n_planes > 0)
+                connect_mirrors(sc, J, w, f, j, mp, true, rd, sm.g, lam, cie, beta, med_albedo(sc, sm, lam));
             if (uniform(rng) >= med_albedo(sc, sm, lam)) fate = 0;
             else { nd = sample_hg(rd, sm.g, rng); no = mp; }
         } else if (!valid) {
@@ -1634,6 +1708,23 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
                 no = h.p + h.n * 1e-6; nd = o;
                 break;
             }
+            case FTB_MAT_MIRROR: {   // render.h:1680-1688
+                double rr = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
+                if (uniform(rng) >= rr) { fate = 0; break; }
+                nd = reflect(rd, h.n);
+                no = h.p + h.n * 1e-6;
+                break;
+            }
+            case FTB_MAT_HALF_MIRROR: {   // render.h:1702-1711
+                double rr = clamp01(spec_slot(sc, m.reflect, lam, 0.5));
+                if (uniform(rng) < rr) {
+                    nd = reflect(rd, h.n);
+                    no = h.p + h.n * 1e-6;
+                } else {
+                    no = h.p + rd * 1e-6;
+                }
+                break;
+            }
             case FTB_MAT_FILTER: {   // render.h:1711-1723
                 double tt = clamp01(spec_slot(sc, m.transmit, lam, 0.0));
                 if (uniform(rng) >= tt) { fate = 0; break; }
@@ -1650,6 +1741,10 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
                 load_cie();
                 connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, cie, beta, rr);
                 connect_surface<MEDIA>(sc, J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, cie, beta, rt);
+                if (MIRROR && sc.n_planes > 0) {
+                    connect_mirrors(sc, J, w, f, j, h.p, false, h.n, 0.0, lam, cie, beta, rr);
+                    connect_mirrors(sc, J, w, f, j, h.p, false, neg(h.n), 0.0, lam, cie, beta, rt);
+                }
                 double u = uniform(rng);
                 if (u < rr) {
                     D3 wo = cosine_hemisphere(h.n, rng);
@@ -1668,6 +1763,7 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
                 load_cie();
                 connect_surface<MEDIA>(sc, J, w, f, j, h.p, h.n, ngo, wi, lam, cie, beta, rho);
+                if (MIRROR && sc.n_planes > 0) connect_mirrors(sc, J, w, f, j, h.p, false, h.n, 0.0, lam, cie, beta, rho);
                 if (uniform(rng) >= rho) { fate = 0; break; }
                 D3 wo = cosine_hemisphere(h.n, rng);
                 beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
@@ -1708,8 +1804,76 @@ __global__ void __launch_bounds__(128, MEDIA ? FTB_SHADE_MEDIA_MINB : FTB_SHADE_
     tally_finish(acc, jobs, multi, n_jobs);
 }
 
-// Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
+__device__ __forceinline__ void splat(const DevJob& J, int view, int pix, double X, double Y, double Z,
+                                      int32_t* status) {
+    long long* px = reinterpret_cast<long long*>(view_film(J, view)) + 4 * (size_t)pix;
+    atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, status));
+    atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, J.film_scale_inv, status));
+    atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, J.film_scale_inv, status));
+    atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
+}
+
+// A mirror record (push_mirror): connectSpecularPlane's tests in its order (render.h:
+// 1366-1379) -- the light leg p -> R, stopping short of the mirror, must be clear; a closest
+// hit from the eye toward R must land on a planar mirror within 1e-4 (1 + dE) of R
+// (mirrorSeenAt, render.h:1294-1308) -- then splatMirrorLegs (render.h:1315-1331) with that
+// mirror's reflectance: (beta * (weight * shape)) * refl / (D^2 Omega), times the two legs'
+// transmittance in media.  The unfolded length D, the mirror point and the pixel's solid
+// angle are recomputed from the record with the push's arithmetic.
 template <bool COUNT, bool INST, bool SHAPES>
+__device__ __noinline__ void mirror_splat(const DevJob& J, const Wave& w, const Frame& f, int i, TravCount& cnt) {
+    const DevScene& sc = J.sc;
+    const int view = w.sview[i] & 0xffff, plane = w.sview[i] >> 16;
+    const DevPlane& mp = sc.planes[plane];
+    const D3 pn = ld3(mp.n);
+    const D3 p = mk(w.sox[i], w.soy[i], w.soz[i]), wP = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
+    const double dP = w.smax[i];
+    {
+        const RayCtx L = make_ray(p + wP * 1e-6, wP);
+        if (traverse_any<COUNT, INST, SHAPES>(sc, L, EPS_RAY, (dP - 2e-6) - EPS_RAY, f.status, cnt)) return;
+    }
+    const DevCam& cam = view_cam(J, view);
+    const D3 eye = ld3(cam.eye);
+    const double se = dot(pn, eye) - mp.d;
+    const D3 eye_m = eye - pn * (2.0 * se);
+    const double D = len(eye_m - p);
+    const D3 R = p + wP * dP;
+    const double dE = D - dP;
+    const D3 wRE = (eye - R) * (1.0 / dE);
+    const D3 wE = neg(wRE);
+    double t;
+    int sub = -1;
+    const int rec = traverse_closest<COUNT, INST, SHAPES>(sc, make_ray(eye, wE), EPS_RAY, t, &sub, f.status, cnt);
+    if (rec < 0) return;
+    if (fabs(t - dE) > 1e-4 * (1.0 + dE)) return;
+    PrimRec r;
+    load_rec(sc.recs, rec, r);
+    int mat = rec_mat(r);
+    if (INST && rec_type(r) == REC_INST) {
+        Hit h;
+        instance_hit(sc.inst[rec_inst(r)], sub, eye, wE, h);
+        mat = h.mat;
+    }
+    if (mat < 0 || mat >= sc.n_mats || !planar_mirror(sc.mats[mat])) return;
+    int px, py; double cos_cam, dist2e;
+    cam_project(cam, R, px, py, cos_cam, dist2e);
+    const double omega = cam_pixel_solid_angle(cam, cos_cam);
+    const double inv_d2_omega = 1.0 / (D * D * omega);
+    const double lam = w.slam[i];
+    const double refl = clamp01(spec_slot(sc, sc.mats[mat].reflect, lam, 0.5));
+    double contrib = w.sval[i] * refl * inv_d2_omega;
+    if (contrib <= 0.0) return;
+    if (sc.n_med > 0) {
+        contrib *= media_transmittance(sc, p, wP, dP, lam);
+        contrib *= media_transmittance(sc, R, wRE, dE, lam);
+    }
+    splat(J, view, ~w.spix[i], w.sxyz[i] * contrib, w.sxyz[w.S + i] * contrib, w.sxyz[2 * (size_t)w.S + i] * contrib,
+          f.status);
+}
+
+// Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
+// MIRROR: the queue may also hold mirror connections (scenes with planar mirrors).
+template <bool COUNT, bool INST, bool SHAPES, bool MIRROR>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const DevJob* __restrict__ jobs,
                                                               Frame f) {
     const int32_t n_jobs = w.params[0];
@@ -1720,17 +1884,16 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow(Wave w, const Dev
     FTB_FOR_WARP_CHUNKS(i, n, &w.counts[kFetchShadow]) {
         const DevJob& J = jobs[n_jobs > 1 ? w.sjob[i] : 0];
         const DevScene& sc = J.sc;
+        if (COUNT) rays++;
+        if (MIRROR && w.spix[i] < 0) {
+            mirror_splat<COUNT, INST, SHAPES>(J, w, f, i, cnt);
+            continue;
+        }
         D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
         double max_dist = w.smax[i];
         RayCtx R = make_ray(o, d);
-        if (COUNT) rays++;
         if (traverse_any<COUNT, INST, SHAPES>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
-        const double X = w.sxyz[i], Y = w.sxyz[w.S + i], Z = w.sxyz[2 * (size_t)w.S + i];
-        long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i])) + 4 * (size_t)w.spix[i];
-        atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)to_fixed(X, J.film_scale_inv, f.status));
-        atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)to_fixed(Y, J.film_scale_inv, f.status));
-        atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)to_fixed(Z, J.film_scale_inv, f.status));
-        atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
+        splat(J, w.sview[i], w.spix[i], w.sxyz[i], w.sxyz[w.S + i], w.sxyz[2 * (size_t)w.S + i], f.status);
     }
     if (COUNT) {
         block_add3(f.stats + 3, rays, cnt.nodes, cnt.recs);
@@ -2215,7 +2378,13 @@ struct LaunchExtend {
 template <bool C, bool I, bool S>
 struct LaunchShadow {
     static void go(int grid, cudaStream_t st, Wave w, const DevJob* jobs, Frame f) {
-        k_shadow<C, I, S><<<grid, 128, 0, st>>>(w, jobs, f);
+        k_shadow<C, I, S, false><<<grid, 128, 0, st>>>(w, jobs, f);
+    }
+};
+template <bool C, bool I, bool S>
+struct LaunchShadowMirror {
+    static void go(int grid, cudaStream_t st, Wave w, const DevJob* jobs, Frame f) {
+        k_shadow<C, I, S, true><<<grid, 128, 0, st>>>(w, jobs, f);
     }
 };
 template <bool C, bool I, bool S>
@@ -2241,15 +2410,19 @@ struct Issue {
     void emit(bool stream, const PathState& out, int32_t* co) {
         mark(K_EMIT, false);
         const DevJob* jobs = w.jobs;
+#define FTB_EMIT(M, S) \
+    (kind.mirrors ? k_emit<M, S, true><<<grid, T, 0, st>>>(w, jobs, f, out, co) \
+                  : k_emit<M, S, false><<<grid, T, 0, st>>>(w, jobs, f, out, co))
         if (stream) {
             if (kind.bundles) k_emit_hero<true><<<grid, T, 0, st>>>(w, jobs, f, out, co);
-            else if (kind.media) k_emit<true, true><<<grid, T, 0, st>>>(w, jobs, f, out, co);
-            else k_emit<false, true><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            else if (kind.media) FTB_EMIT(true, true);
+            else FTB_EMIT(false, true);
         } else {
             if (kind.bundles) k_emit_hero<false><<<grid, T, 0, st>>>(w, jobs, f, out, co);
-            else if (kind.media) k_emit<true, false><<<grid, T, 0, st>>>(w, jobs, f, out, co);
-            else k_emit<false, false><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            else if (kind.media) FTB_EMIT(true, false);
+            else FTB_EMIT(false, false);
         }
+#undef FTB_EMIT
         mark(K_EMIT, true);
     }
     template <template <bool, bool, bool> class K, class... A>
@@ -2266,6 +2439,7 @@ struct Issue {
     void shadow() {
         mark(K_SHADOW, false);
         if (kind.bundles) trav<LaunchShadowHero>(w, (const DevJob*)w.jobs, f);
+        else if (kind.mirrors) trav<LaunchShadowMirror>(w, (const DevJob*)w.jobs, f);
         else trav<LaunchShadow>(w, (const DevJob*)w.jobs, f);
         mark(K_SHADOW, true);
     }
@@ -2288,12 +2462,20 @@ struct Issue {
         if (kind.bundles) {
             if (inst) { if (shp) FTB_SHADE(k_shade_hero<true, true>); else FTB_SHADE(k_shade_hero<true, false>); }
             else { if (shp) FTB_SHADE(k_shade_hero<false, true>); else FTB_SHADE(k_shade_hero<false, false>); }
+        } else if (kind.mirrors) {
+            if (kind.media) {
+                if (inst) { if (shp) FTB_SHADE(k_shade<true, true, true, true>); else FTB_SHADE(k_shade<true, true, false, true>); }
+                else { if (shp) FTB_SHADE(k_shade<true, false, true, true>); else FTB_SHADE(k_shade<true, false, false, true>); }
+            } else {
+                if (inst) { if (shp) FTB_SHADE(k_shade<false, true, true, true>); else FTB_SHADE(k_shade<false, true, false, true>); }
+                else { if (shp) FTB_SHADE(k_shade<false, false, true, true>); else FTB_SHADE(k_shade<false, false, false, true>); }
+            }
         } else if (kind.media) {
-            if (inst) { if (shp) FTB_SHADE(k_shade<true, true, true>); else FTB_SHADE(k_shade<true, true, false>); }
-            else { if (shp) FTB_SHADE(k_shade<true, false, true>); else FTB_SHADE(k_shade<true, false, false>); }
+            if (inst) { if (shp) FTB_SHADE(k_shade<true, true, true, false>); else FTB_SHADE(k_shade<true, true, false, false>); }
+            else { if (shp) FTB_SHADE(k_shade<true, false, true, false>); else FTB_SHADE(k_shade<true, false, false, false>); }
         } else {
-            if (inst) { if (shp) FTB_SHADE(k_shade<false, true, true>); else FTB_SHADE(k_shade<false, true, false>); }
-            else { if (shp) FTB_SHADE(k_shade<false, false, true>); else FTB_SHADE(k_shade<false, false, false>); }
+            if (inst) { if (shp) FTB_SHADE(k_shade<false, true, true, false>); else FTB_SHADE(k_shade<false, true, false, false>); }
+            else { if (shp) FTB_SHADE(k_shade<false, false, true, false>); else FTB_SHADE(k_shade<false, false, false, false>); }
         }
 #undef FTB_SHADE
         mark(K_SHADE, true);
@@ -2344,7 +2526,7 @@ void stream_half(Issue& I, int a, cudaGraphConditionalHandle loop, int32_t set_l
 struct WaveGraphs {
     struct Entry {
         int32_t max_bounce, grid;   // max_bounce -1: a streaming pass
-        bool inst, hero, media, shapes, sorted;
+        bool inst, hero, media, shapes, mirrors, sorted;
         int32_t* status;
         cudaGraphExec_t exec;
     };
@@ -2355,7 +2537,8 @@ struct WaveGraphs {
     cudaGraphExec_t find(int32_t max_bounce, int32_t grid, const WaveKind& kind, bool sorted, int32_t* status) const {
         for (auto& e : entries)
             if (e.max_bounce == max_bounce && e.grid == grid && e.inst == kind.instances && e.hero == kind.bundles &&
-                e.media == kind.media && e.shapes == kind.shapes && e.sorted == sorted && e.status == status)
+                e.media == kind.media && e.shapes == kind.shapes && e.mirrors == kind.mirrors && e.sorted == sorted &&
+                e.status == status)
                 return e.exec;
         return nullptr;
     }
@@ -2394,8 +2577,8 @@ cudaError_t launch_wave(Wave& w, int32_t max_bounce, const WaveKind& kind, const
     issue_wave(I, max_bounce);
     err = cudaStreamEndCapture(st, &g);
     if (err != cudaSuccess) return err;
-    WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, kind.shapes, shape.sort_rays,
-                        f.status, nullptr};
+    WaveGraphs::Entry e{max_bounce, grid, kind.instances, kind.bundles, kind.media, kind.shapes, kind.mirrors,
+                        shape.sort_rays, f.status, nullptr};
     err = cudaGraphInstantiate(&e.exec, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) return err;
@@ -2462,8 +2645,8 @@ cudaError_t launch_stream(Wave& w, const WaveKind& kind, const Frame& f, int32_t
         cudaGraph_t b2 = nullptr;
         err = cudaStreamEndCapture(st, &b2);
     }
-    WaveGraphs::Entry e{-1, grid, kind.instances, kind.bundles, kind.media, kind.shapes, shape.sort_rays, f.status,
-                        nullptr};
+    WaveGraphs::Entry e{-1, grid, kind.instances, kind.bundles, kind.media, kind.shapes, kind.mirrors,
+                        shape.sort_rays, f.status, nullptr};
     if (err == cudaSuccess) err = cudaGraphInstantiate(&e.exec, captured, 0);
     cudaGraphDestroy(captured);
     if (err != cudaSuccess) return err;

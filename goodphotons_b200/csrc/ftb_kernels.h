@@ -189,7 +189,12 @@ struct WaveKind {
     bool bundles = false;     // hero-wavelength jobs (every job of the table has hero_c > 1)
     bool media = false;       // some scene has participating media
     bool shapes = false;      // some scene has spheres or curves (not only triangles)
+    bool mirrors = false;     // some scene has planar mirrors (mirror connections queued)
 };
+// Connection records one path vertex of job J can queue: a camera connection and one per
+// planar mirror, for each of the job's views.  A wave or pass keeps its slots at most
+// W / fanout so that the shadow queue (kShadowPerSlot records per slot) cannot overflow.
+inline int conn_fanout(const DevJob& J) { return (J.n_views > 1 ? J.n_views : 1) * (1 + J.sc.n_planes); }
 // Whether a scene's world records include spheres or curves.
 inline bool scene_has_shapes(const DevScene& sc) { return (int64_t)sc.n_recs > sc.n_tris + sc.n_inst; }
 

@@ -11,6 +11,7 @@
 //             reads them); the last 8 B carry the global primitive index, material and
 //             type.  Leaf children of a node reference a contiguous run of records.
 //   tri_n   : optional per-triangle shading normals (9 doubles), by triangle index.
+//   planes  : DevPlane[n_planes] -- the planar mirrors the camera connections reflect in.
 //   inst    : DevInst[n_inst], 128 B each -- instances of shared BLAS assets.  The world
 //             hierarchy (TLAS) holds one REC_INST record per instance; a BLAS is a wide
 //             BVH and triangle records of its own, in its local space.
@@ -84,6 +85,14 @@ struct DevInst {
 };
 static_assert(sizeof(DevInst) == 128, "DevInst must be 128 bytes");
 
+// A planar mirror (Scene::MirrorPlane, scene.h:1617-1623): the plane dot(n, x) == d of a
+// group of coplanar planar-mirror triangles (unit normal flipped so its largest component
+// is positive) and their AABB padded by 1e-6 (1 + diagonal).
+struct DevPlane {
+    double n[3], d;
+    double lo[3], hi[3];
+};
+
 struct DevScene {
     const WNode* nodes;
     const PrimRec* recs;
@@ -96,9 +105,10 @@ struct DevScene {
     const double* emit_cdf;   // selection CDF over emitters
     const DevMed* med;
     const DevInst* inst;
+    const DevPlane* planes;   // planar mirrors (camera connections by reflection)
     int32_t n_nodes, n_recs, n_mats, n_emit, n_med, n_spec;
     int32_t root2;            // second hierarchy (the curves') in nodes, or -1
-    int32_t pad2;
+    int32_t n_planes;
     int64_t n_tris;
     int64_t n_inst;
     double total_power;

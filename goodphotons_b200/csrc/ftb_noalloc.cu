@@ -10,7 +10,7 @@
 //
 // Its scratch -- the path state, queues and shadow records of one wave of photons, plus the
 // energy tallies and the status word -- lives in one file-scope __device__ array of exactly
-// FTB_NOALLOC_SCRATCH_BYTES (21,060,864 B, 20.1 MiB, for FTB_NOALLOC_MAX_PHOTONS = 32768
+// FTB_NOALLOC_SCRATCH_BYTES (21,062,912 B, 20.1 MiB, for FTB_NOALLOC_MAX_PHOTONS = 32768
 // slots), which every GPU that loads the library holds until the process exits.  Host code
 // cannot use the array's name as a device address (it is a host-side stand-in), so the
 // first call on each device, with that device current, resolves it with
@@ -96,6 +96,13 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
                                               " photons per call (its scratch is a fixed device array); "
                                               "split the render into calls with consecutive seed_base and one "
                                               "explicit frac_bits");
+    // a vertex queues one connection per planar mirror besides the camera's: the one wave's
+    // connection records fit only if the photons times that fan-out stay within the limit
+    if (dev.n_planes > 0 && p->n_photons * (1 + (int64_t)dev.n_planes) > kNoAllocPhotons)
+        return na_fail(FTB_ERR_TOO_LARGE, "ftb_render_forward_noalloc: a scene with " + std::to_string(dev.n_planes) +
+                                              " mirror planes takes at most " +
+                                              std::to_string(kNoAllocPhotons / (1 + dev.n_planes)) +
+                                              " photons per call");
     if (device < 0 || device >= 256) return na_fail(FTB_ERR_INVALID, "device index out of range");
     std::lock_guard<std::mutex> scene_lock(ftb::scene_mutex(scene));
     int prev = 0;
@@ -149,6 +156,7 @@ extern "C" ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_cam
     kind.instances = dev.n_inst > 0;
     kind.media = dev.n_med > 0;
     kind.shapes = ftb::scene_has_shapes(dev);
+    kind.mirrors = dev.n_planes > 0;
     if (e == cudaSuccess && p->n_photons > 0) e = ftb::launch_wave(w, p->max_bounce, kind, f, sms, shape, st);
     if (e != cudaSuccess) out = na_fail(FTB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (out == FTB_OK && info) {

@@ -13,6 +13,12 @@
 //                     reused, its previous pass is retired (event sync, status)
 //   completion thread: copies a finished job's film and tallies out, frees its film
 //
+// With an HBM budget the server also owns the residency of its jobs' scenes: admission
+// counts the two wave buffers, the admitted films and the resident scenes against the
+// budget, evicts idle scenes (least recently used first) to make room and restores a job's
+// scene when the job is admitted -- the "scene BVHs kept resident across jobs" of a serving
+// loop whose scene library is larger than the device.
+//
 // Photons are keyed by index (seed_base + i) and the film is int64 fixed point, so how a
 // job's photons are split over waves and mixed with other jobs cannot change its result.
 #include <cuda_runtime.h>
@@ -48,11 +54,11 @@ enum JobState { kQueued = 0, kActive = 1, kFinishing = 2, kDone = 3 };
 struct Job {
     uint64_t id = 0;
     ftb_request req{};
-    DevScene sc{};
+    DevScene sc{};              // the scene's device view, read again at admission
     double power = 0.0;
     int frac = 0;
     int hero = 1;               // wavelengths per photon (1 or a bundle)
-    int klass = 0;              // kernel variant class: bundles, media, spheres/curves, instances
+    int klass = 0;              // kernel variant class: bundles, media, spheres/curves, instances, mirrors
     uint64_t film_bytes = 0;
     int64_t next = 0;           // photons handed to waves so far
     int32_t pending = 0;        // launched waves holding this job's photons, not yet retired
@@ -62,6 +68,15 @@ struct Job {
     ftb_status error = FTB_OK;
     double t_submit = 0, t_admit = 0, t_finish = 0;
     ftb_energy energy{};
+};
+
+// A scene used by the server's jobs (HBM budget mode).
+struct SceneUse {
+    uint64_t bytes = 0;         // device bytes of its tables
+    int users = 0;              // admitted jobs that use it
+    uint64_t last = 0;          // admission clock of its latest job
+    bool evictable = false;
+    bool counted = false;       // resident and counted in scene_bytes
 };
 
 struct WaveSlot {
@@ -83,7 +98,12 @@ struct ftb_server {
     int32_t W = 1 << 22;
     int32_t hero_max = 4;              // largest bundle the wave buffers hold
     ftb::LaunchShape shape;
-    uint64_t budget = 0;
+    uint64_t budget = 0;               // film budget (no HBM budget)
+    uint64_t hbm = 0;                  // HBM budget: waves + films + resident scenes (0: off)
+    uint64_t wave_bytes = 0;
+    uint64_t scene_bytes = 0;          // resident scenes counted against hbm
+    uint64_t use_clock = 0;
+    std::map<const ftb_scene*, SceneUse> scenes;
     Clock::time_point t0;
 
     std::mutex mu;
@@ -97,7 +117,7 @@ struct ftb_server {
     uint64_t next_id = 1;
     uint64_t film_bytes = 0;
     std::vector<int> free_slots;
-    int skipped[16] = {};              // passes since each kernel class was last served
+    int skipped[32] = {};              // passes since each kernel class was last served
     ftb_server_stats st{};
     int inflight = 0;
     Clock::time_point busy_since;
@@ -119,16 +139,62 @@ namespace {
 
 void set_device(ftb_server* s) { cudaSetDevice(s->device); }
 
-// Admit queued jobs in arrival order while a slot is free and the film fits (mu held).
+// HBM budget mode: make room for job j (its film, and its scene's tables if the scene is
+// not on the device) by evicting scenes no admitted job uses, least recently used first;
+// then restore j's scene.  false: it does not fit yet (mu held).
+bool fit_locked(ftb_server* s, Job* j) {
+    SceneUse& u = s->scenes[j->req.scene];
+    const bool resident = ftb::scene_resident(j->req.scene);
+    const uint64_t need = j->film_bytes + (resident ? 0 : u.bytes);
+    while (s->wave_bytes + s->film_bytes + s->scene_bytes + need > s->hbm) {
+        const ftb_scene* victim = nullptr;
+        uint64_t oldest = UINT64_MAX;
+        for (auto& kv : s->scenes)
+            if (kv.first != j->req.scene && kv.second.counted && kv.second.evictable && kv.second.users == 0 &&
+                kv.second.last < oldest) {
+                victim = kv.first;
+                oldest = kv.second.last;
+            }
+        if (!victim) return false;
+        // every job of the victim has retired (users == 0), so the free can be stream-ordered
+        if (ftb::scene_evict(victim, s->admit_stream) != FTB_OK) { s->scenes[victim].evictable = false; continue; }
+        s->scenes[victim].counted = false;
+        s->scene_bytes -= s->scenes[victim].bytes;
+        s->st.evictions++;
+    }
+    if (!resident) {
+        if (ftb::scene_restore(j->req.scene, s->admit_stream) != FTB_OK) {
+            j->error = FTB_ERR_OOM;
+        } else {
+            u.counted = true;
+            s->scene_bytes += u.bytes;
+            s->st.restores++;
+            s->admitted_since_launch = true;   // passes wait for the restore (admit_ev)
+        }
+    }
+    int dev = 0, sms = 0;
+    double power = 0.0;
+    ftb::scene_internals(j->req.scene, &j->sc, &dev, &sms, &power);
+    u.users++;
+    u.last = ++s->use_clock;
+    return true;
+}
+
+// Admit queued jobs in arrival order while a slot is free and the film (HBM budget: the
+// job's footprint) fits (mu held).
 void admit_locked(ftb_server* s) {
     while (!s->queue.empty() && !s->free_slots.empty()) {
         Job* j = s->queue.front();
-        if (s->film_bytes + j->film_bytes > s->budget) break;
+        if (s->hbm) {
+            if (!fit_locked(s, j)) break;
+        } else if (s->film_bytes + j->film_bytes > s->budget) {
+            break;
+        }
         s->queue.pop_front();
         j->slot = s->free_slots.back();
         s->free_slots.pop_back();
         cudaError_t e = cudaSuccess;
-        if (j->req.n_photons > 0) {   // an empty job needs no device film: its film is zero
+        if (j->req.n_photons > 0 && j->error == FTB_OK) {   // an empty job needs no device film
             void* p = nullptr;
             e = cudaMallocFromPoolAsync(&p, j->film_bytes, s->pool, s->admit_stream);
             if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, j->film_bytes, s->admit_stream);
@@ -147,8 +213,8 @@ void admit_locked(ftb_server* s) {
             if (j->d_film) cudaFreeAsync(j->d_film, s->admit_stream);
             j->d_film = nullptr;
             j->error = e == cudaErrorMemoryAllocation ? FTB_ERR_OOM : FTB_ERR_CUDA;
-            j->next = j->req.n_photons;   // nothing to trace
         }
+        if (j->error != FTB_OK) j->next = j->req.n_photons;   // nothing to trace
         j->state = kActive;
         if (j->next >= j->req.n_photons) {   // empty or failed: straight to completion
             j->state = kFinishing;
@@ -169,7 +235,7 @@ void admit_locked(ftb_server* s) {
 // to the jobs with the least work left.  cap = the pass's photon budget (4 W in a
 // streaming pass, W in a wave).  One entry per job (mu held).
 int64_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::vector<Job*>& members,
-                           int32_t& max_bounce, ftb::WaveKind& kind) {
+                           int32_t& max_bounce, ftb::WaveKind& kind, int& fanout) {
     std::vector<Job*> c;
     for (Job* j : s->active)
         if (j->next < j->req.n_photons) c.push_back(j);
@@ -177,12 +243,12 @@ int64_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
     std::stable_sort(c.begin(), c.end(), [](const Job* a, const Job* b) {
         return a->req.n_photons - a->next < b->req.n_photons - b->next;
     });
-    bool present[16] = {};
+    bool present[32] = {};
     for (Job* j : c) present[j->klass] = true;
     int klass = c[0]->klass;
-    for (int k = 0; k < 16; ++k)
+    for (int k = 0; k < 32; ++k)
         if (present[k] && s->skipped[k] >= 2 && (klass == c[0]->klass || s->skipped[k] > s->skipped[klass])) klass = k;
-    for (int k = 0; k < 16; ++k) s->skipped[k] = (present[k] && k != klass) ? s->skipped[k] + 1 : 0;
+    for (int k = 0; k < 32; ++k) s->skipped[k] = (present[k] && k != klass) ? s->skipped[k] + 1 : 0;
     c.erase(std::remove_if(c.begin(), c.end(), [&](const Job* j) { return j->klass != klass; }), c.end());
     if ((int)c.size() > ftb::kWaveJobs) c.resize(ftb::kWaveJobs);
     std::vector<int64_t> give(c.size(), 0);
@@ -200,6 +266,7 @@ int64_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
     }
     int64_t photons = 0;
     max_bounce = 0;
+    fanout = 1;
     kind = ftb::WaveKind{};
     for (size_t i = 0; i < c.size(); ++i) {
         if (give[i] <= 0) continue;
@@ -229,6 +296,8 @@ int64_t build_table_locked(ftb_server* s, std::vector<ftb::DevJob>& table, std::
         kind.instances |= J.sc.n_inst > 0;
         kind.media |= J.sc.n_med > 0;
         kind.shapes |= ftb::scene_has_shapes(J.sc);
+        kind.mirrors |= J.sc.n_planes > 0;
+        fanout = std::max(fanout, ftb::conn_fanout(J));
     }
     return photons;
 }
@@ -266,11 +335,12 @@ void scheduler(ftb_server* s) {
         members.clear();
         int64_t photons = 0;
         int32_t mb = 0;
+        int fanout = 1;
         ftb::WaveKind kind;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             admit_locked(s);
-            photons = build_table_locked(s, table, members, mb, kind);
+            photons = build_table_locked(s, table, members, mb, kind, fanout);
             if (photons == 0) {
                 bool busy = s->ws[0].busy || s->ws[1].busy;
                 if (!busy) {
@@ -291,7 +361,8 @@ void scheduler(ftb_server* s) {
         // streaming pass: {ranges, paths in flight, photons (int64), half-iteration cap (int64)};
         // wave: {jobs, slots}
         const bool stream = s->shape.regenerate;
-        const int32_t slots = (int32_t)std::min<int64_t>(photons, s->W);
+        // the pass's connection fan-out (planar mirrors) bounds its paths in flight
+        const int32_t slots = (int32_t)std::min<int64_t>(photons, std::max(1, s->W / fanout));
         int32_t* par = reinterpret_cast<int32_t*>(w.table + ftb::kWaveJobs);
         par[0] = (int32_t)table.size();
         par[1] = slots;
@@ -358,6 +429,7 @@ void completer(ftb_server* s) {
             j->d_film = nullptr;
             s->free_slots.push_back(j->slot);
             s->film_bytes -= j->film_bytes;
+            if (s->hbm) s->scenes[j->req.scene].users--;
             s->st.active--;
             if (j->error == FTB_OK) { s->st.completed++; s->st.photons_done += j->req.n_photons; }
             else s->st.failed++;
@@ -425,6 +497,13 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     s->budget = cfg->film_budget ? cfg->film_budget : free_b / 4;
+    s->hbm = cfg->hbm_budget;
+    s->wave_bytes = 2 * (uint64_t)ftb::wave_bytes(s->W, false, s->hero_max);
+    if (s->hbm && s->wave_bytes >= s->hbm) {
+        delete s;
+        cudaSetDevice(prev);
+        return fail(FTB_ERR_TOO_LARGE, "hbm_budget does not cover the wave buffers");
+    }
     auto bad = [&](cudaError_t e, const char* what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
         release(s);
@@ -457,7 +536,8 @@ ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out) {
     pp.location.type = cudaMemLocationTypeDevice;
     pp.location.id = s->device;
     if ((e = cudaMemPoolCreate(&s->pool, &pp)) != cudaSuccess) return bad(e, "film pool");
-    uint64_t keep = s->budget;   // films are recycled without returning memory to the driver
+    // films are recycled without returning memory to the driver (up to what may be admitted)
+    uint64_t keep = s->hbm ? std::min<uint64_t>(s->budget, s->hbm - s->wave_bytes) : s->budget;
     cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     if ((e = cudaEventRecord(s->admit_ev, s->admit_stream)) != cudaSuccess) return bad(e, "event");
     for (int i = s->max_active - 1; i >= 0; --i) s->free_slots.push_back(i);
@@ -487,15 +567,38 @@ ftb_status ftb_server_submit(ftb_server* s, const ftb_request* r, uint64_t* job_
     // bundles as the reference gates them: clamped to kHeroMax, none in scenes with media
     j->hero = (r->hero_c <= 1 || j->sc.n_med > 0) ? 1 : (r->hero_c > ftb::kHeroMax ? ftb::kHeroMax : r->hero_c);
     j->klass = (j->hero > 1 ? 1 : 0) | (j->sc.n_med > 0 ? 2 : 0) | (ftb::scene_has_shapes(j->sc) ? 4 : 0) |
-               (j->sc.n_inst > 0 ? 8 : 0);
+               (j->sc.n_inst > 0 ? 8 : 0) | (j->sc.n_planes > 0 ? 16 : 0);
+    if (j->hero > 1 && j->sc.n_planes > 0) {
+        delete j;
+        return fail(FTB_ERR_UNSUPPORTED, "hero bundles in a scene with planar mirrors (use hero_c 1)");
+    }
     if (j->hero > s->hero_max) {
         delete j;
         return fail(FTB_ERR_TOO_LARGE, "bundle larger than the server's hero_max");
     }
     j->film_bytes = (uint64_t)c.res_x * (uint64_t)c.res_y * 4 * sizeof(int64_t);
-    if (j->film_bytes > s->budget) { delete j; return fail(FTB_ERR_TOO_LARGE, "film exceeds the server's film budget"); }
+    if (!s->hbm && j->film_bytes > s->budget) {
+        delete j;
+        return fail(FTB_ERR_TOO_LARGE, "film exceeds the server's film budget");
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stopping) { delete j; return fail(FTB_ERR_INVALID, "server is stopping"); }
+    if (s->hbm) {   // the footprint: waves + film + the scene's tables
+        auto it = s->scenes.find(r->scene);
+        const uint64_t sb = it != s->scenes.end() ? it->second.bytes : ftb::scene_device_bytes(r->scene);
+        if (s->wave_bytes + j->film_bytes + sb > s->hbm) {
+            delete j;
+            return fail(FTB_ERR_TOO_LARGE, "job footprint (waves + film + scene) exceeds the server's hbm_budget");
+        }
+        if (it == s->scenes.end()) {
+            SceneUse u;
+            u.bytes = sb;
+            u.evictable = ftb::scene_evictable(r->scene);
+            u.counted = ftb::scene_resident(r->scene);
+            if (u.counted) s->scene_bytes += sb;
+            s->scenes[r->scene] = u;
+        }
+    }
     j->id = s->next_id++;
     j->t_submit = s->now();
     s->jobs[j->id] = j;
@@ -536,6 +639,8 @@ ftb_status ftb_server_get_stats(ftb_server* s, ftb_server_stats* out) {
     std::lock_guard<std::mutex> lk(s->mu);
     *out = s->st;
     out->film_bytes = s->film_bytes;
+    out->scene_bytes = s->scene_bytes;
+    out->wave_bytes = s->wave_bytes;
     if (s->inflight > 0) out->busy_s += std::chrono::duration<double>(Clock::now() - s->busy_since).count();
     return FTB_OK;
 }

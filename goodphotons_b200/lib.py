@@ -54,6 +54,9 @@ def load(path=None):
     _sig(L, "ftb_scene_destroy", st, PS)
     _sig(L, "ftb_scene_footprint", st, PS, C.c_int32, C.c_int32, C.POINTER(abi.Footprint))
     _sig(L, "ftb_scene_power", C.c_double, PS)
+    _sig(L, "ftb_scene_evict", st, PS)
+    _sig(L, "ftb_scene_restore", st, PS)
+    _sig(L, "ftb_scene_resident", C.c_int, PS)
     _sig(L, "ftb_render_forward", st, PS, C.POINTER(abi.Camera), C.POINTER(abi.RenderParams),
          C.POINTER(C.c_int64), C.POINTER(abi.FilmInfo), C.POINTER(abi.Energy))
     _sig(L, "ftb_render_forward_device", st, PS, C.POINTER(abi.Camera),
@@ -266,6 +269,18 @@ class Scene:
         self.lib.check(self.lib.L.ftb_scene_footprint(self.h, rx, ry, C.byref(fp)))
         return fp
 
+    def evict(self):
+        """Free the device tables, keeping a host copy (ftb_scene_evict)."""
+        self.lib.check(self.lib.L.ftb_scene_evict(self.h))
+
+    def restore(self):
+        """Upload the tables again (ftb_scene_restore)."""
+        self.lib.check(self.lib.L.ftb_scene_restore(self.h))
+
+    @property
+    def resident(self):
+        return bool(self.lib.L.ftb_scene_resident(self.h))
+
     def render(self, cam, n, seed_base=0, max_bounce=8, frac_bits=0, out=None, hero_c=1, lambda_mode=0):
         """One-shot render into a host film: returns (film int64 [ry, rx, 4], info, energy).
         `out` may be a preallocated (e.g. pinned) int64 array of that shape."""
@@ -306,9 +321,9 @@ class Scene:
 class Server:
     """Resident render server with continuous batching (ftb_server_*)."""
 
-    def __init__(self, device=0, max_active=64, film_budget=0, wave_slots=0, hero_max=0, lib=None):
+    def __init__(self, device=0, max_active=64, film_budget=0, wave_slots=0, hero_max=0, hbm_budget=0, lib=None):
         self.lib = lib or load()
-        cfg = abi.ServerConfig(device, max_active, film_budget, wave_slots, hero_max)
+        cfg = abi.ServerConfig(device, max_active, film_budget, wave_slots, hero_max, hbm_budget)
         h = C.c_void_p()
         self.lib.check(self.lib.L.ftb_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

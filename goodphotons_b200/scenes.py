@@ -388,6 +388,40 @@ def icosphere(level):
     return v, f
 
 
+def geodesic_sphere(freq):
+    """Vertices (unit sphere) and faces of a class-I geodesic sphere: every face of the
+    icosahedron split into freq^2 triangles on a barycentric grid, the grid points pushed
+    out to the sphere.  20 freq^2 faces (freq = 2^L gives the face count of icosphere(L)),
+    so a mesh of any size in steps of ~2/freq relative is available.  Points shared by two
+    faces are merged, so the mesh is watertight; faces are wound outward."""
+    v0, f0 = icosphere(0)
+    n = int(freq)
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    m = (ii + jj) <= n
+    I, J = ii[m], jj[m]
+    grid = -np.ones((n + 1, n + 1), dtype=np.int64)
+    grid[I, J] = np.arange(len(I))
+    ui, uj = np.nonzero((ii + jj) < n)
+    up = np.stack([grid[ui, uj], grid[ui + 1, uj], grid[ui, uj + 1]], 1)
+    di, dj = np.nonzero((ii + jj) < n - 1)
+    down = np.stack([grid[di + 1, dj], grid[di + 1, dj + 1], grid[di, dj + 1]], 1)
+    local = np.concatenate([up, down])
+    A, B, Cv = v0[f0[:, 0]], v0[f0[:, 1]], v0[f0[:, 2]]
+    wa, wb, wc = (n - I - J) / n, I / n, J / n
+    P = (A[:, None, :] * wa[None, :, None] + B[:, None, :] * wb[None, :, None] +
+         Cv[:, None, :] * wc[None, :, None]).reshape(-1, 3)
+    P /= np.linalg.norm(P, axis=1, keepdims=True)
+    F = (local[None, :, :] + (np.arange(len(f0)) * len(I))[:, None, None]).reshape(-1, 3)
+    keys = np.round(P * 1e9).astype(np.int64)
+    _, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+    v = P[first]
+    f = inv.reshape(-1)[F]
+    a, b, c = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    inward = np.einsum("ij,ij->i", np.cross(b - a, c - a), a + b + c) < 0.0
+    f[inward] = f[inward][:, [0, 2, 1]]
+    return v, f
+
+
 def value_noise3(p, seed, octaves=3, base_freq=4.0):
     """Seeded 3-octave value noise in [0, 1]: a hashed lattice of uniform values,
     trilinearly interpolated with a smoothstep fade, octaves at doubling frequency and
@@ -424,9 +458,10 @@ def value_noise3(p, seed, octaves=3, base_freq=4.0):
 GLASS_CENTER = (1.0, 0.55, 1.0)
 
 
-def blob_tris(level=7, center=(0.0, 0.0, 0.0), radius=0.4, amp=0.05, seed=0):
-    """Triangles (n x 9) of a subdivided icosphere displaced radially by value noise."""
-    v, f = icosphere(level)
+def blob_tris(level=7, center=(0.0, 0.0, 0.0), radius=0.4, amp=0.05, seed=0, freq=None):
+    """Triangles (n x 9) of a subdivided icosphere (or, with `freq`, a geodesic sphere of
+    20 freq^2 faces) displaced radially by value noise."""
+    v, f = icosphere(level) if freq is None else geodesic_sphere(freq)
     n = value_noise3(v, seed)
     r = radius + amp * (2.0 * n - 1.0)
     pos = np.asarray(center)[None, :] + v * r[:, None]
@@ -438,8 +473,8 @@ def glass_material(sb: SceneBuilder):
 
 
 def glass_blob(sb: SceneBuilder, level=7, center=GLASS_CENTER, radius=0.4, amp=0.05,
-               seed=0, mat=None):
-    tv = blob_tris(level, center, radius, amp, seed)
+               seed=0, mat=None, freq=None):
+    tv = blob_tris(level, center, radius, amp, seed, freq=freq)
     if mat is None:
         mat = glass_material(sb)
     sb.tris(tv, mat)
@@ -502,11 +537,14 @@ def make_cornell(lib=None, boxes=True):
     return sb.build(lib)
 
 
-def make_glass(lib=None, level=7, seed=0):
+def make_glass(lib=None, level=7, seed=0, freq=None):
+    """The dispersive-caustics scene: the Cornell room (without the two small boxes, which
+    the blob would cut through) holding the noise-displaced glass icosphere of `level`
+    subdivisions, or with `freq` a geodesic sphere of 20 freq^2 triangles."""
     sb = SceneBuilder()
     cornell_box(sb, boxes=False)
-    glass_blob(sb, level=level, seed=seed)
-    sb.meta.update(name="glass", level=level)
+    glass_blob(sb, level=level, seed=seed, freq=freq)
+    sb.meta.update(name="glass", **({"level": level} if freq is None else {"freq": freq}))
     return sb.build(lib)
 
 

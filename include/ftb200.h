@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FTB_ABI_VERSION 5
+#define FTB_ABI_VERSION 6
 
 typedef enum ftb_status {
     FTB_OK = 0,
@@ -319,6 +319,20 @@ ftb_status ftb_scene_clone_instances(const ftb_scene* src, const double* to_worl
                                      ftb_scene** out);
 ftb_status ftb_scene_footprint(const ftb_scene* scene, int32_t res_x, int32_t res_y,
                                ftb_footprint* out);
+
+/* Device residency of a scene (no counterpart in the reference, which bakes and frees a
+ * scene inside every renderForwardCuda call, render_cuda.cu:13712-13756).
+ * ftb_scene_evict frees the scene's device tables (footprint.scene_bytes) and keeps a host
+ * copy of them (made on the first eviction); ftb_scene_restore uploads that copy again, so
+ * a scene library larger than the device can stay baked in host memory while a working set
+ * stays on the device.  Renders of an evicted scene fail with FTB_ERR_INVALID.  Only a scene
+ * that owns all its tables can leave the device -- no instances, not a clone and not the
+ * source of live clones -- others return FTB_ERR_UNSUPPORTED.  ftb_scene_evict waits for
+ * the device first (renders in flight finish).  A render server created with hbm_budget
+ * manages the residency of the scenes its jobs use itself. */
+ftb_status ftb_scene_evict(ftb_scene* scene);
+ftb_status ftb_scene_restore(ftb_scene* scene);
+int ftb_scene_resident(const ftb_scene* scene);   /* 1 on the device, 0 evicted */
 /* Total emitted power the film and energy fixed point are relative to. */
 double ftb_scene_power(const ftb_scene* scene);
 
@@ -418,7 +432,7 @@ ftb_status ftb_trace_log(ftb_scene* scene, const ftb_camera* cam,
  *    media every entry point traces one wavelength per photon and so does this one.
  *  - energy != NULL synchronizes `stream` and also checks the device status word. */
 #define FTB_NOALLOC_MAX_PHOTONS 32768
-#define FTB_NOALLOC_SCRATCH_BYTES 21060864
+#define FTB_NOALLOC_SCRATCH_BYTES 21062912
 ftb_status ftb_render_forward_noalloc(ftb_scene* scene, const ftb_camera* cam,
                                       const ftb_render_params* params, int64_t* d_film,
                                       ftb_film_info* info, ftb_energy* energy, void* stream);
@@ -483,7 +497,17 @@ ftb_status ftb_autotune(ftb_scene* scene, const ftb_camera* cam, int64_t n_photo
  * jobs are not queued behind large ones.  A job's film and energy are exactly those of
  * ftb_render_forward with the same arguments, whatever shares its passes (photons are
  * keyed by index and the film is fixed point).  The scenes referenced by
- * submitted jobs must stay alive until those jobs are done. */
+ * submitted jobs must stay alive until those jobs are done.
+ *
+ * Admission by device-memory footprint (hbm_budget > 0): the server then accounts its two
+ * wave buffers, the films of the admitted jobs and the scenes its jobs use against
+ * hbm_budget, and manages those scenes' residency -- a job is admitted when its film, plus
+ * its scene's tables if the scene is not on the device, fits the budget; to make room the
+ * server evicts scenes that no admitted job uses, least recently used first, and restores a
+ * job's scene on admission (ftb_scene_evict / ftb_scene_restore, stream-ordered).  Scenes
+ * that cannot leave the device (instances, clones) count as resident.  While the server
+ * runs, render its scenes only through it; when it is destroyed, scenes stay as they are
+ * (ftb_scene_resident tells). */
 typedef struct ftb_server ftb_server;
 
 typedef struct ftb_server_config {
@@ -495,6 +519,9 @@ typedef struct ftb_server_config {
                                   ftb_get_tuning) */
     int32_t hero_max;          /* largest hero_c a request may carry, 1..8 (0: 4); the wave
                                   buffers grow by ~260 B per slot at 4 */
+    uint64_t hbm_budget;       /* bytes of wave buffers + admitted films + resident scenes the
+                                  server may hold, with scene residency managed (0: films
+                                  only, against film_budget; scenes stay where they are) */
 } ftb_server_config;
 
 typedef struct ftb_request {
@@ -524,6 +551,9 @@ typedef struct ftb_server_stats {
     int64_t waves;             /* waves launched */
     double busy_s;             /* time with at least one wave in flight */
     uint64_t film_bytes;       /* device film bytes of admitted jobs now */
+    uint64_t scene_bytes;      /* hbm_budget: device bytes of the resident scenes it counts */
+    uint64_t wave_bytes;       /* device bytes of the two wave buffers */
+    int64_t evictions, restores;   /* hbm_budget: scene evictions and restores so far */
 } ftb_server_stats;
 
 ftb_status ftb_server_create(const ftb_server_config* cfg, ftb_server** out);

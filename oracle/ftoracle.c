@@ -287,6 +287,22 @@ typedef struct {
     double radius;
 } Med;
 
+/* Scene::MirrorPlane (scene.h:1617-1623): unit normal n, dot(n, x) == d, padded AABB of the
+ * member faces, their total area */
+typedef struct MPlane {
+    V3 n;
+    double d;
+    V3 lo, hi;
+    double area;
+    long long key[4];
+} MPlane;
+
+/* isPlanarMirrorMat (scene.h:356-360): Mirror, HalfMirror, Glossy with roughness <= 0 */
+static int planar_mirror(const ftb_material* m) {
+    return m->type == FTB_MAT_MIRROR || m->type == FTB_MAT_HALF_MIRROR ||
+           (m->type == FTB_MAT_GLOSSY && m->roughness <= 0.0);
+}
+
 struct fto_ctx {
     int lambda_mode;   /* ftb_lambda_mode; set by fto_set_lambda_mode */
     int64_t ni;
@@ -311,6 +327,8 @@ struct fto_ctx {
     double total_power;
     int n_med;
     Med* med;
+    int n_mp;              /* planar mirrors (Scene::buildMirrorPlanes, scene.h:1646-1720) */
+    struct MPlane* mp;
 };
 
 double fto_total_power(const fto_ctx* c) { return c ? c->total_power : 0.0; }
@@ -1121,6 +1139,78 @@ static inline double slot(const fto_ctx* c, int s, double lam, double dflt) {
     return s >= 0 ? spec_eval(&c->S, s, lam) : dflt;
 }
 
+/* Renderer::SpecVtx (render.h:878-902): the vertex a specular connection starts from -- a
+ * surface (normal np) or a volume scatter (incoming direction win, HG g); shape() is the
+ * vertex's angular factor toward wP, negative when wP leaves the wrong side. */
+typedef struct { int volume; V3 np, win; double g; } SpecVtx;
+static double vtx_shape(const SpecVtx* vt, V3 wP) {
+    if (vt->volume) return hg_phase(vdot(vt->win, wP), vt->g);
+    double cs = vdot(vt->np, wP);
+    return cs <= 0.0 ? -1.0 : cs / PI_D;
+}
+
+/* Renderer::connectSpecularPlane + mirrorSeenAt + splatMirrorLegs, one wavelength
+ * (render.h:1294-1380): vertex p reaches the pinhole by one reflection in the plane of
+ * mirror mp -- through the eye's mirror image -- if the reflection point R lies in the
+ * plane's box and in the image, the light leg p -> R is clear, and a closest hit from the
+ * eye toward R lands on a planar mirror at R; the splat carries that mirror's reflectance. */
+static void connect_specular_plane(Tr* T, const MPlane* mp, V3 p, const SpecVtx* vt, double lam, double beta,
+                                   double w) {
+    const fto_ctx* c = T->c;
+    const Cam* cam = T->cam;
+    const V3 eye = cam->eye;
+    const double se = vdot(mp->n, eye) - mp->d;
+    const double sp = vdot(mp->n, p) - mp->d;
+    if (!(se * sp > 0.0)) return;
+    const V3 eye_m = vsub(eye, vmul(mp->n, 2.0 * se));
+    V3 wP = vsub(eye_m, p);
+    const double D = vlen(wP);
+    if (D < 1e-9) return;
+    wP = vmul(wP, 1.0 / D);
+    const double shape = vtx_shape(vt, wP);
+    if (shape < 0.0) return;
+    const double denom = vdot(mp->n, wP);
+    if (fabs(denom) < 1e-12) return;
+    const double dP = (mp->d - vdot(mp->n, p)) / denom;
+    if (dP <= 1e-7 || dP >= D - 1e-7) return;
+    const V3 R = vadd(p, vmul(wP, dP));
+    if (R.x < mp->lo.x || R.x > mp->hi.x || R.y < mp->lo.y || R.y > mp->hi.y || R.z < mp->lo.z || R.z > mp->hi.z)
+        return;
+    int px, py; double cos_cam, dist2e;
+    if (!cam_project(cam, R, &px, &py, &cos_cam, &dist2e)) return;
+    const double omega = cam_pixel_solid_angle(cam, cos_cam);
+    if (omega <= 0.0) return;
+    const double dE = D - dP;
+    const V3 wRE = vmul(vsub(eye, R), 1.0 / dE);
+    T->rays++;
+    if (occluded(c, vadd(p, vmul(wP, 1e-6)), wP, dP - 2e-6, 1e-6)) return;
+    Hit hm;
+    T->rays++;
+    closest_hit(c, eye, vneg(wRE), 1e-6, &hm);
+    if (!hm.valid) return;
+    if (fabs(hm.t - dE) > 1e-4 * (1.0 + dE)) return;
+    if (hm.mat < 0 || hm.mat >= c->n_mats || !planar_mirror(&c->mats[hm.mat])) return;
+    const double inv_d2_omega = 1.0 / (D * D * omega);
+    const double refl = clamp01(slot(c, c->mats[hm.mat].reflect, lam, 0.5));
+    double contrib = beta * (w * shape) * refl * inv_d2_omega;
+    if (contrib <= 0.0) return;
+    if (c->n_med > 0) {
+        contrib *= media_transmittance(T, p, wP, dP, lam);
+        contrib *= media_transmittance(T, R, wRE, dE, lam);
+    }
+    film_add(T->film, px, py, cie_x(lam) * contrib, cie_y(lam) * contrib, cie_z(lam) * contrib);
+}
+/* camSpecularSplatAll / camSpecularSplatVolumeAll (render.h:1515-1585), planar mirrors only
+ * (scenes with dielectric or mirror spheres are outside this path) */
+static void cam_specular_splat(Tr* T, V3 p, const SpecVtx* vt, double lam, double beta, double w) {
+    for (int k = 0; k < T->c->n_mp; ++k) connect_specular_plane(T, &T->c->mp[k], p, vt, lam, beta, w);
+}
+static void cam_specular_surface(Tr* T, V3 p, V3 n, double lam, double beta, double rho) {
+    if (T->c->n_mp == 0) return;
+    SpecVtx vt; vt.volume = 0; vt.np = n; vt.win = v3(0, 0, 0); vt.g = 0.0;
+    cam_specular_splat(T, p, &vt, lam, beta, rho);
+}
+
 /* Renderer::refractOrReflect (render.h:2657-2697), stochastic branch */
 static void refract_or_reflect(const fto_ctx* c, const ftb_material* m, const Hit* h, V3 d,
                                double lam, Pcg* rng, int* transmitted, double ext_ior,
@@ -1215,6 +1305,7 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
     if (c->lambda_mode == FTB_LAMBDA_UNIFORM_380_780) beta *= wl;
     e[E_EMIT] += beta;
     connect_surface(T, origin, emit_n, emit_n, emit_n, lam, beta, 1.0);
+    cam_specular_surface(T, origin, emit_n, lam, beta, 1.0);
     V3 ro = vadd(origin, vmul(dir, 1e-6)), rd = dir;
     Stack stk; stk.n = 0;
     int fate = 2;
@@ -1244,6 +1335,10 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
         if (medium_event) {   /* render.h:2105-2115 */
             const Med* sm = &c->med[scatter_med];
             connect_volume(T, sm, mp, rd, lam, beta);
+            if (c->n_mp > 0) {
+                SpecVtx vt; vt.volume = 1; vt.np = v3(0, 0, 0); vt.win = rd; vt.g = sm->g;
+                cam_specular_splat(T, mp, &vt, lam, beta, med_albedo(c, sm, lam));
+            }
             if (pcg_uniform(rng) >= med_albedo(c, sm, lam)) { e[E_ABS] += beta; fate = 0; goto done; }
             V3 nd = sample_hg(rd, sm->g, rng);
             ro = mp; rd = nd;
@@ -1294,6 +1389,23 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
             ro = vadd(h.p, vmul(h.n, 1e-6)); rd = o;
             continue;
         }
+        case FTB_MAT_MIRROR: {   /* render.h:1680-1688 */
+            double r = clamp01(slot(c, m->reflect, lam, 0.5));
+            if (pcg_uniform(rng) >= r) { e[E_ABS] += beta; fate = 0; goto done; }
+            V3 o = vreflect(rd, h.n);
+            ro = vadd(h.p, vmul(h.n, 1e-6)); rd = o;
+            continue;
+        }
+        case FTB_MAT_HALF_MIRROR: {   /* render.h:1702-1711 */
+            double r = clamp01(slot(c, m->reflect, lam, 0.5));
+            if (pcg_uniform(rng) < r) {
+                V3 o = vreflect(rd, h.n);
+                ro = vadd(h.p, vmul(h.n, 1e-6)); rd = o;
+            } else {
+                ro = vadd(h.p, vmul(rd, 1e-6));
+            }
+            continue;
+        }
         case FTB_MAT_FILTER: {   /* render.h:1711-1723 */
             double t = clamp01(slot(c, m->transmit, lam, 0.0));
             if (pcg_uniform(rng) >= t) { e[E_ABS] += beta; fate = 0; goto done; }
@@ -1309,6 +1421,8 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
             V3 wi = v3(-rd.x, -rd.y, -rd.z);
             connect_surface(T, h.p, h.n, ngo, wi, lam, beta, rr);
             connect_surface(T, h.p, vneg(h.n), vneg(ngo), wi, lam, beta, rt);
+            cam_specular_surface(T, h.p, h.n, lam, beta, rr);
+            cam_specular_surface(T, h.p, vneg(h.n), lam, beta, rt);
             double u = pcg_uniform(rng);
             if (u < rr) {
                 V3 wo = cosine_hemisphere(h.n, rng);
@@ -1329,6 +1443,7 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
             V3 ngo = oriented_geo_n(&h);
             V3 wi = v3(-rd.x, -rd.y, -rd.z);
             connect_surface(T, h.p, h.n, ngo, wi, lam, beta, rho);
+            cam_specular_surface(T, h.p, h.n, lam, beta, rho);
             if (pcg_uniform(rng) >= rho) { e[E_ABS] += beta; fate = 0; goto done; }
             V3 wo = cosine_hemisphere(h.n, rng);
             beta *= shading_adjoint_corr(wi, wo, h.n, ngo);
@@ -1346,6 +1461,7 @@ done:
 /* ------------------------------------------------------------- setup ---------------- */
 void fto_release(fto_ctx* c) {
     if (!c) return;
+    free(c->mp);
     free(c->spec); free(c->tw); free(c->tv); free(c->mats); free(c->tris); free(c->sph);
     free(c->sph_mat); free(c->crv); free(c->world.nodes); free(c->world.order); free(c->emit);
     free(c->cdf_store); free(c->emitter_cdf); free(c->med);
@@ -1369,6 +1485,83 @@ static void finalize_tri(Tri* t, const double* v, const double* n, int mat) {
     if (vdot(t->n0, t->n0) < 1e-12) t->n0 = t->gn;
     if (vdot(t->n1, t->n1) < 1e-12) t->n1 = t->gn;
     if (vdot(t->n2, t->n2) < 1e-12) t->n2 = t->gn;
+}
+
+static int cmp_plane_area(const void* a, const void* b) {
+    const MPlane* x = (const MPlane*)a;
+    const MPlane* y = (const MPlane*)b;
+    if (x->area != y->area) return x->area < y->area ? 1 : -1;   /* larger area first */
+    return (x->key[0] > y->key[0]) - (x->key[0] < y->key[0]);   /* then first seen */
+}
+
+/* Scene::buildMirrorPlanes (scene.h:1646-1720): the planar-mirror triangles grouped by
+ * plane (unit normal flipped so its largest component is positive, offset d = dot(n, v0),
+ * bucketed by the quantized (n, d) key in first-seen order), each plane's AABB over its
+ * member vertices and total area; at most 64 planes (the largest by area; the reference's
+ * sort is not stable, so a tie in area at the cut is ordered by first sighting here); the
+ * boxes padded by 1e-6 (1 + diagonal). */
+static void build_mirror_planes(fto_ctx* c) {
+    c->n_mp = 0;
+    c->mp = NULL;
+    int cap = 0;
+    for (int64_t i = 0; i < c->nt; ++i) {
+        const Tri* t = &c->tris[i];
+        if (t->mat < 0 || t->mat >= c->n_mats || !planar_mirror(&c->mats[t->mat])) continue;
+        V3 n = t->gn;
+        double nl = vlen(n);
+        if (nl < 1e-12) continue;
+        n = vmul(n, 1.0 / nl);
+        const double sx = fabs(n.x), sy = fabs(n.y), sz = fabs(n.z);
+        const double lead = (sx >= sy && sx >= sz) ? n.x : ((sy >= sz) ? n.y : n.z);
+        if (lead < 0.0) n = v3(-n.x, -n.y, -n.z);
+        double d = vdot(n, t->v0);
+        const double q_pos = 1e5, q_dir = 1e6;
+        long long key[4] = {llround(n.x * q_dir), llround(n.y * q_dir), llround(n.z * q_dir), llround(d * q_pos)};
+        int idx = -1;
+        for (int k = 0; k < c->n_mp && idx < 0; ++k)
+            if (memcmp(c->mp[k].key, key, sizeof key) == 0) idx = k;
+        if (idx < 0) {
+            if (c->n_mp == cap) {
+                cap = cap ? 2 * cap : 8;
+                c->mp = (MPlane*)realloc(c->mp, sizeof(MPlane) * (size_t)cap);
+            }
+            idx = c->n_mp++;
+            MPlane* m = &c->mp[idx];
+            m->n = n; m->d = d; m->lo = t->v0; m->hi = t->v0; m->area = 0.0;
+            memcpy(m->key, key, sizeof key);
+        }
+        MPlane* m = &c->mp[idx];
+        const V3 vs[3] = {t->v0, t->v1, t->v2};
+        for (int k = 0; k < 3; ++k) {   /* std::min(lo, v) / std::max(hi, v) */
+            m->lo.x = vs[k].x < m->lo.x ? vs[k].x : m->lo.x; m->hi.x = m->hi.x < vs[k].x ? vs[k].x : m->hi.x;
+            m->lo.y = vs[k].y < m->lo.y ? vs[k].y : m->lo.y; m->hi.y = m->hi.y < vs[k].y ? vs[k].y : m->hi.y;
+            m->lo.z = vs[k].z < m->lo.z ? vs[k].z : m->lo.z; m->hi.z = m->hi.z < vs[k].z ? vs[k].z : m->hi.z;
+        }
+        m->area += 0.5 * vlen(vcross(vsub(t->v1, t->v0), vsub(t->v2, t->v0)));
+    }
+    if (c->n_mp > 64) {
+        /* qsort is not stable: ties fall back to the first-seen index, kept in key[0] */
+        for (int k = 0; k < c->n_mp; ++k) c->mp[k].key[0] = k;
+        qsort(c->mp, (size_t)c->n_mp, sizeof(MPlane), cmp_plane_area);
+        c->n_mp = 64;
+    }
+    for (int k = 0; k < c->n_mp; ++k) {
+        MPlane* m = &c->mp[k];
+        const double pad = 1e-6 * (1.0 + vlen(vsub(m->hi, m->lo)));
+        m->lo = vsub(m->lo, v3(pad, pad, pad));
+        m->hi = vadd(m->hi, v3(pad, pad, pad));
+    }
+}
+
+int fto_mirror_planes(const fto_ctx* c, double* out, int cap) {
+    if (!c) return -1;
+    for (int k = 0; k < c->n_mp && k < cap; ++k) {
+        const MPlane* m = &c->mp[k];
+        double* o = out + 10 * k;
+        o[0] = m->n.x; o[1] = m->n.y; o[2] = m->n.z; o[3] = m->d;
+        o[4] = m->lo.x; o[5] = m->lo.y; o[6] = m->lo.z; o[7] = m->hi.x; o[8] = m->hi.y; o[9] = m->hi.z;
+    }
+    return c->n_mp;
 }
 
 fto_ctx* fto_prepare(const ftb_scene_desc* d) {
@@ -1498,6 +1691,7 @@ fto_ctx* fto_prepare(const ftb_scene_desc* d) {
         m->g = s->g; m->sa = s->sigma_a; m->ss = s->sigma_s; m->bound = s->bound;
         m->bmin = rd3(s->bmin); m->bmax = rd3(s->bmax); m->center = rd3(s->center); m->radius = s->radius;
     }
+    build_mirror_planes(c);
     return c;
 }
 

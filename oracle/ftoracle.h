@@ -75,6 +75,11 @@ int fto_closest_hit(const fto_ctx* ctx, const double o[3], const double d[3], do
 int fto_occluded(const fto_ctx* ctx, const double o[3], const double d[3], double max_dist,
                  double tmin);
 
+/* The planar mirrors the tracer connects through (Scene::buildMirrorPlanes,
+ * scene.h:1646-1720): writes up to `cap` planes as {n[3], d, lo[3], hi[3]} and returns their
+ * number. */
+int fto_mirror_planes(const fto_ctx* ctx, double* out, int cap);
+
 const char* fto_last_error(void);
 
 #ifdef __cplusplus

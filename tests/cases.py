@@ -55,6 +55,24 @@ def make_instances(L, ramp=0.01, cauchy=True):
     return sb.build(L)
 
 
+def make_mirrors(L, fog=False):
+    """Planar mirrors (the reference's connectSpecularPlane): a Mirror panel in front of the
+    back wall, a HalfMirror pane standing in the room and a roughness-0 Glossy tile beside the
+    left wall, with the two Cornell boxes; `fog` fills the box with the homogeneous medium, so
+    volume vertices connect through the mirrors too."""
+    sb = scenes.SceneBuilder()
+    scenes.cornell_box(sb, boxes=True)
+    mirror = sb.material(abi.MAT_MIRROR, reflect=sb.const(0.9))
+    sb.quad((0.3, 0.3, 0.02), (1.4, 0, 0), (0, 1.4, 0), mirror)
+    half = sb.material(abi.MAT_HALF_MIRROR, reflect=sb.table([(400, 0.3), (700, 0.7)]))
+    sb.quad((1.0, 0.0, 1.2), (0.5, 0, -0.3), (0, 1.0, 0), half)
+    tile = sb.material(abi.MAT_GLOSSY, reflect=sb.const(0.8), roughness=0.0)
+    sb.quad((0.01, 0.6, 0.6), (0, 0.6, 0), (0, 0, 0.8), tile)
+    if fog:
+        sb.medium(sb.const(0.02), sb.const(0.2), 0.6, bmin=(0, 0, 0), bmax=(2, 2, 2))
+    return sb.build(L)
+
+
 CASES = {
     # name: (builder, res, photons, max_bounce, seed_base, wavelengths per photon)
     "cornell": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 0, 1),
@@ -63,6 +81,8 @@ CASES = {
     "fog_strands": (lambda L: scenes.make_fog_strands(L, n_strands=500), 32, 8192, 32, 0, 1),
     "materials": (make_materials, 32, 8192, 16, 7, 1),
     "instances": (make_instances, 32, 8192, 16, 11, 1),
+    "mirrors": (make_mirrors, 32, 8192, 16, 13, 1),
+    "mirrors_fog": (lambda L: make_mirrors(L, fog=True), 32, 8192, 32, 17, 1),
     # hero-wavelength bundles (Renderer::tracePhotonHero): C wavelengths per photon
     "cornell_hero4": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 3, 4),
     "glass_hero4": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 5, 4),

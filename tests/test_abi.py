@@ -70,8 +70,17 @@ def test_supported_gate(L):
     sb = scenes.SceneBuilder()
     scenes.cornell_box(sb, boxes=False)
     sb.quad((0.5, 0.5, 0.5), (0.3, 0, 0), (0, 0.3, 0), sb.material(abi.MAT_MIRROR, reflect=sb.const(0.9)))
+    assert L.supported(sb.build(L))[0] == 1            # planar mirrors: the plane connector
+    sb.sphere((1, 1, 1), 0.2, sb.material(abi.MAT_MIRROR, reflect=sb.const(0.9)))
     r, why = L.supported(sb.build(L))
-    assert r == 0 and "mirror" in why
+    assert r == 0 and "mirror sphere" in why           # the spherical mirror connector is not on the path
+    sb = scenes.SceneBuilder()
+    scenes.cornell_box(sb, boxes=False)
+    tile = sb.material(abi.MAT_GLOSSY, reflect=sb.const(0.9), roughness=0.0)
+    for k in range(65):                                 # 65 distinct planes
+        sb.quad((0.1, 0.1 + 0.01 * k, 0.3), (0.2, 0, 0), (0, 0, 0.2), tile)
+    r, why = L.supported(sb.build(L))
+    assert r == 0 and "64 mirror planes" in why
     sb = scenes.SceneBuilder()
     scenes.cornell_box(sb, boxes=False)
     sb.sphere((1, 1, 1), 0.2, sb.material(abi.MAT_DIELECTRIC, ior=sb.cauchy(1.5, 0.004)))

@@ -900,8 +900,6 @@ ftb_status check_params(const ftb_scene* s, const ftb_camera* cam, const ftb_ren
         return fail(FTB_ERR_INVALID, "unknown lambda_mode");
     if (!(s->power > 0.0)) return fail(FTB_ERR_UNSUPPORTED, "scene emits no power");
     if (s->tables && !s->tables->resident) return fail(FTB_ERR_INVALID, "scene is evicted from the device");
-    if (p->hero_c > 1 && s->dev.n_med == 0 && s->dev.n_planes > 0)
-        return fail(FTB_ERR_UNSUPPORTED, "hero bundles in a scene with planar mirrors (use hero_c 1)");
     return FTB_OK;
 }
 
@@ -1793,8 +1791,6 @@ ftb_status ftb_session_begin(ftb_scene* s, const ftb_camera* cams, int32_t n_cam
                              int32_t frac_bits, int32_t hero_c, ftb_session** out) {
     if (!s || !cams || n_cams < 1 || n_cams > 65535 || !out) return fail(FTB_ERR_INVALID, "bad session arguments");
     if (max_bounce < 0 || max_bounce > 1024) return fail(FTB_ERR_INVALID, "max_bounce out of range");
-    if (hero_c > 1 && s->dev.n_med == 0 && s->dev.n_planes > 0)
-        return fail(FTB_ERR_UNSUPPORTED, "hero bundles in a scene with planar mirrors (use hero_c 1)");
     DeviceGuard guard(s->device);
     auto ss = new ftb_session();
     ss->scene = s;

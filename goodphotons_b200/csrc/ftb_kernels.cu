@@ -1074,49 +1074,81 @@ __device__ __forceinline__ void push_mirror(const Wave& w, const Frame& f, int j
     w.sjob[i] = job; w.sview[i] = view | (plane << 16);
 }
 
+// connectSpecularPlane's geometry (render.h:1334-1366) for one plane and view: the vertex and
+// the eye on the same side of the plane, the path unfolded through the eye's mirror image,
+// the vertex factor (SpecVtx::shape, render.h:897-901), the mirror point inside the plane's
+// box and in the image.  false when the connection is culled; else the direction wP to the
+// mirrored eye, the distance dP to the mirror, `shape` and the pixel.  `volume`: a medium
+// scatter with incoming direction nw and HG g; otherwise a surface with normal nw.
+__device__ __forceinline__ bool mirror_geometry(const DevPlane& mp, const DevCam& cam, D3 p, bool volume, D3 nw,
+                                                double g, D3& wP, double& dP, double& shape, int& pix) {
+    const D3 pn = ld3(mp.n);
+    const D3 eye = ld3(cam.eye);
+    const double se = dot(pn, eye) - mp.d;
+    const double sp = dot(pn, p) - mp.d;
+    if (!(se * sp > 0.0)) return false;
+    const D3 eye_m = eye - pn * (2.0 * se);
+    wP = eye_m - p;
+    const double D = len(wP);
+    if (D < 1e-9) return false;
+    wP = wP * (1.0 / D);
+    if (volume) {
+        shape = hg_phase(dot(nw, wP), g);
+    } else {
+        const double cs = dot(nw, wP);
+        shape = cs <= 0.0 ? -1.0 : cs / PI_D;
+    }
+    if (shape < 0.0) return false;
+    const double denom = dot(pn, wP);
+    if (fabs(denom) < 1e-12) return false;
+    dP = (mp.d - dot(pn, p)) / denom;
+    if (dP <= 1e-7 || dP >= D - 1e-7) return false;
+    const D3 R = p + wP * dP;
+    if (R.x < mp.lo[0] || R.x > mp.hi[0] || R.y < mp.lo[1] || R.y > mp.hi[1] || R.z < mp.lo[2] || R.z > mp.hi[2])
+        return false;
+    int px, py; double cos_cam, dist2e;
+    if (!cam_project(cam, R, px, py, cos_cam, dist2e)) return false;
+    if (cam_pixel_solid_angle(cam, cos_cam) <= 0.0) return false;
+    pix = py * cam.rx + px;
+    return true;
+}
+
 // camSpecularSplatAll / camSpecularSplatVolumeAll (render.h:1515-1585) over the planar
-// mirrors: connectSpecularPlane's geometry (render.h:1334-1366) -- the vertex and the eye on
-// the same side of the plane, the path unfolded through the eye's mirror image, the vertex
-// factor (SpecVtx::shape, render.h:897-901), the mirror point inside the plane's box and in
-// the image -- then a mirror record for k_shadow.  `volume`: a medium scatter with incoming
-// direction nw and HG g; otherwise a surface with normal nw.  `weight`: the vertex's albedo.
+// mirrors: a mirror record for k_shadow per plane and view that the geometry lets through.
+// `weight`: the vertex's albedo.
 __device__ __noinline__ void connect_mirrors(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f,
                                              int job, D3 p, bool volume, D3 nw, double g, double lam,
                                              const double* cie, double beta, double weight) {
     for (int k = 0; k < sc.n_planes; ++k) {
-        const DevPlane& mp = sc.planes[k];
-        const D3 pn = ld3(mp.n);
         for (int v = 0; v < view_count(J); ++v) {
-            const DevCam& cam = view_cam(J, v);
-            const D3 eye = ld3(cam.eye);
-            const double se = dot(pn, eye) - mp.d;
-            const double sp = dot(pn, p) - mp.d;
-            if (!(se * sp > 0.0)) continue;
-            const D3 eye_m = eye - pn * (2.0 * se);
-            D3 wP = eye_m - p;
-            const double D = len(wP);
-            if (D < 1e-9) continue;
-            wP = wP * (1.0 / D);
-            double shape;
-            if (volume) {
-                shape = hg_phase(dot(nw, wP), g);
-            } else {
-                const double cs = dot(nw, wP);
-                shape = cs <= 0.0 ? -1.0 : cs / PI_D;
+            D3 wP; double dP, shape; int pix;
+            if (!mirror_geometry(sc.planes[k], view_cam(J, v), p, volume, nw, g, wP, dP, shape, pix)) continue;
+            push_mirror(w, f, job, v, k, p, wP, dP, beta * (weight * shape), lam, cie, pix);
+        }
+    }
+}
+
+// The same for a bundle's live wavelengths (camSpecularSplatAllHero, render.h:1570-1576): a
+// record carries (lambda_i, beta_i x (rho_i x shape)) per wavelength, as the bundle's camera
+// connections do; k_shadow_hero evaluates the mirror's reflectance per wavelength.
+__device__ __noinline__ void connect_mirrors_hero(const DevScene& sc, const DevJob& J, const Wave& w, const Frame& f,
+                                                  int job, D3 p, D3 n, const double* lam, const double* beta,
+                                                  const double* rho, int nup) {
+    for (int k = 0; k < sc.n_planes; ++k) {
+        for (int v = 0; v < view_count(J); ++v) {
+            D3 wP; double dP, shape; int pix;
+            if (!mirror_geometry(sc.planes[k], view_cam(J, v), p, false, n, 0.0, wP, dP, shape, pix)) continue;
+            const int i = agg_inc(&w.counts[kShadowCount]);
+            if (i >= w.S) { atomicOr(f.status, ST_QUEUE_OVERFLOW); continue; }
+            w.sox[i] = p.x; w.soy[i] = p.y; w.soz[i] = p.z;
+            w.sdx[i] = wP.x; w.sdy[i] = wP.y; w.sdz[i] = wP.z;
+            w.smax[i] = dP; w.spix[i] = ~pix; w.sjob[i] = job; w.sview[i] = v | (k << 16);
+            w.slam[i] = lam[0]; w.sval[i] = beta[0] * (rho[0] * shape);
+            for (int q = 1; q < nup; ++q) {
+                w.xlam[(size_t)(q - 1) * w.S + i] = lam[q];
+                w.xval[(size_t)(q - 1) * w.S + i] = beta[q] * (rho[q] * shape);
             }
-            if (shape < 0.0) continue;
-            const double denom = dot(pn, wP);
-            if (fabs(denom) < 1e-12) continue;
-            const double dP = (mp.d - dot(pn, p)) / denom;
-            if (dP <= 1e-7 || dP >= D - 1e-7) continue;
-            const D3 R = p + wP * dP;
-            if (R.x < mp.lo[0] || R.x > mp.hi[0] || R.y < mp.lo[1] || R.y > mp.hi[1] || R.z < mp.lo[2] ||
-                R.z > mp.hi[2])
-                continue;
-            int px, py; double cos_cam, dist2e;
-            if (!cam_project(cam, R, px, py, cos_cam, dist2e)) continue;
-            if (cam_pixel_solid_angle(cam, cos_cam) <= 0.0) continue;
-            push_mirror(w, f, job, v, k, p, wP, dP, beta * (weight * shape), lam, cie, py * cam.rx + px);
+            w.snup[i] = nup;
         }
     }
 }
@@ -1813,15 +1845,20 @@ __device__ __forceinline__ void splat(const DevJob& J, int view, int pix, double
     atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), 1ull);
 }
 
-// A mirror record (push_mirror): connectSpecularPlane's tests in its order (render.h:
-// 1366-1379) -- the light leg p -> R, stopping short of the mirror, must be clear; a closest
-// hit from the eye toward R must land on a planar mirror within 1e-4 (1 + dE) of R
-// (mirrorSeenAt, render.h:1294-1308) -- then splatMirrorLegs (render.h:1315-1331) with that
-// mirror's reflectance: (beta * (weight * shape)) * refl / (D^2 Omega), times the two legs'
-// transmittance in media.  The unfolded length D, the mirror point and the pixel's solid
-// angle are recomputed from the record with the push's arithmetic.
+// A mirror record's tests, in connectSpecularPlane's order (render.h:1366-1379): the light
+// leg p -> R, stopping short of the mirror, must be clear; a closest hit from the eye toward
+// R must land on a planar mirror within 1e-4 (1 + dE) of R (mirrorSeenAt, render.h:
+// 1294-1308).  On success: the mirror's material, the unfolded length D, the mirror point
+// R, the leg R -> eye (wRE, dE) and the pixel's solid angle, recomputed from the record
+// with the push's arithmetic.
+struct MirrorSeen {
+    int mat;
+    double D, dE, omega;
+    D3 R, wRE;
+};
 template <bool COUNT, bool INST, bool SHAPES>
-__device__ __noinline__ void mirror_splat(const DevJob& J, const Wave& w, const Frame& f, int i, TravCount& cnt) {
+__device__ __forceinline__ bool mirror_seen(const DevJob& J, const Wave& w, const Frame& f, int i, TravCount& cnt,
+                                            MirrorSeen& ms) {
     const DevScene& sc = J.sc;
     const int view = w.sview[i] & 0xffff, plane = w.sview[i] >> 16;
     const DevPlane& mp = sc.planes[plane];
@@ -1830,45 +1867,57 @@ __device__ __noinline__ void mirror_splat(const DevJob& J, const Wave& w, const 
     const double dP = w.smax[i];
     {
         const RayCtx L = make_ray(p + wP * 1e-6, wP);
-        if (traverse_any<COUNT, INST, SHAPES>(sc, L, EPS_RAY, (dP - 2e-6) - EPS_RAY, f.status, cnt)) return;
+        if (traverse_any<COUNT, INST, SHAPES>(sc, L, EPS_RAY, (dP - 2e-6) - EPS_RAY, f.status, cnt)) return false;
     }
     const DevCam& cam = view_cam(J, view);
     const D3 eye = ld3(cam.eye);
     const double se = dot(pn, eye) - mp.d;
     const D3 eye_m = eye - pn * (2.0 * se);
-    const double D = len(eye_m - p);
-    const D3 R = p + wP * dP;
-    const double dE = D - dP;
-    const D3 wRE = (eye - R) * (1.0 / dE);
-    const D3 wE = neg(wRE);
+    ms.D = len(eye_m - p);
+    ms.R = p + wP * dP;
+    ms.dE = ms.D - dP;
+    ms.wRE = (eye - ms.R) * (1.0 / ms.dE);
+    const D3 wE = neg(ms.wRE);
     double t;
     int sub = -1;
     const int rec = traverse_closest<COUNT, INST, SHAPES>(sc, make_ray(eye, wE), EPS_RAY, t, &sub, f.status, cnt);
-    if (rec < 0) return;
-    if (fabs(t - dE) > 1e-4 * (1.0 + dE)) return;
+    if (rec < 0) return false;
+    if (fabs(t - ms.dE) > 1e-4 * (1.0 + ms.dE)) return false;
     PrimRec r;
     load_rec(sc.recs, rec, r);
-    int mat = rec_mat(r);
+    ms.mat = rec_mat(r);
     if (INST && rec_type(r) == REC_INST) {
         Hit h;
         instance_hit(sc.inst[rec_inst(r)], sub, eye, wE, h);
-        mat = h.mat;
+        ms.mat = h.mat;
     }
-    if (mat < 0 || mat >= sc.n_mats || !planar_mirror(sc.mats[mat])) return;
+    if (ms.mat < 0 || ms.mat >= sc.n_mats || !planar_mirror(sc.mats[ms.mat])) return false;
     int px, py; double cos_cam, dist2e;
-    cam_project(cam, R, px, py, cos_cam, dist2e);
-    const double omega = cam_pixel_solid_angle(cam, cos_cam);
-    const double inv_d2_omega = 1.0 / (D * D * omega);
+    cam_project(cam, ms.R, px, py, cos_cam, dist2e);
+    ms.omega = cam_pixel_solid_angle(cam, cos_cam);
+    return true;
+}
+
+// One-wavelength mirror record: splatMirrorLegs (render.h:1315-1331) with the reflectance of
+// the mirror the eye sees: (beta * (weight * shape)) * refl / (D^2 Omega), times the two legs'
+// transmittance in media.
+template <bool COUNT, bool INST, bool SHAPES>
+__device__ __noinline__ void mirror_splat(const DevJob& J, const Wave& w, const Frame& f, int i, TravCount& cnt) {
+    MirrorSeen ms;
+    if (!mirror_seen<COUNT, INST, SHAPES>(J, w, f, i, cnt, ms)) return;
+    const DevScene& sc = J.sc;
+    const double inv_d2_omega = 1.0 / (ms.D * ms.D * ms.omega);
     const double lam = w.slam[i];
-    const double refl = clamp01(spec_slot(sc, sc.mats[mat].reflect, lam, 0.5));
+    const double refl = clamp01(spec_slot(sc, sc.mats[ms.mat].reflect, lam, 0.5));
     double contrib = w.sval[i] * refl * inv_d2_omega;
     if (contrib <= 0.0) return;
     if (sc.n_med > 0) {
-        contrib *= media_transmittance(sc, p, wP, dP, lam);
-        contrib *= media_transmittance(sc, R, wRE, dE, lam);
+        const D3 p = mk(w.sox[i], w.soy[i], w.soz[i]), wP = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
+        contrib *= media_transmittance(sc, p, wP, w.smax[i], lam);
+        contrib *= media_transmittance(sc, ms.R, ms.wRE, ms.dE, lam);
     }
-    splat(J, view, ~w.spix[i], w.sxyz[i] * contrib, w.sxyz[w.S + i] * contrib, w.sxyz[2 * (size_t)w.S + i] * contrib,
-          f.status);
+    splat(J, w.sview[i] & 0xffff, ~w.spix[i], w.sxyz[i] * contrib, w.sxyz[w.S + i] * contrib,
+          w.sxyz[2 * (size_t)w.S + i] * contrib, f.status);
 }
 
 // Camera connections: occlusion (Scene::occluded, default tmin 1e-6) then Film::add.
@@ -1964,7 +2013,7 @@ __device__ __forceinline__ double max_of(const double* a, int n) {   // hero::ma
     return m;
 }
 
-template <bool STREAM>
+template <bool STREAM, bool MIRROR>
 __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit_hero(Wave w, const DevJob* __restrict__ jobs, Frame f, PathState out,
                                                    int32_t* out_count) {
     const int32_t n_jobs = w.params[0];
@@ -2006,6 +2055,7 @@ __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit_hero(Wave w, const 
         }
         tally_add(acc, jobs, multi, j, T_EMIT, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
         connect_surface_hero(J, w, f, j, origin, emit_n, emit_n, emit_n, lam, beta, one, C);
+        if (MIRROR && sc.n_planes > 0) connect_mirrors_hero(sc, J, w, f, j, origin, emit_n, lam, beta, one, C);
         D3 ro = origin + dir * 1e-6;
         if (J.max_bounce <= 0) {
             tally_add(acc, jobs, multi, j, T_RES, to_fixed(sum_of(beta, C), J.tally_scale_inv, f.status));
@@ -2026,7 +2076,7 @@ __global__ void __launch_bounds__(128, FTB_EMIT_MINB) k_emit_hero(Wave w, const 
     tally_finish(acc, jobs, multi, n_jobs);
 }
 
-template <bool INST, bool SHAPES>
+template <bool INST, bool SHAPES, bool MIRROR>
 __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, const DevJob* __restrict__ jobs,
                                                                     Frame f, PathState in, const int32_t* in_count,
                                                                     PathState out, int32_t* out_count) {
@@ -2097,6 +2147,10 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
                 connect_surface_hero(J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rr, nup);
                 connect_surface_hero(J, w, f, j, h.p, neg(h.n), neg(ngo), wi, lam, beta, rt, nup);
+                if (MIRROR && sc.n_planes > 0) {
+                    connect_mirrors_hero(sc, J, w, f, j, h.p, h.n, lam, beta, rr, nup);
+                    connect_mirrors_hero(sc, J, w, f, j, h.p, neg(h.n), lam, beta, rt, nup);
+                }
                 double q_r = max_of(rr, nup), q_t = max_of(rt, nup);
                 double sum_h = q_r + q_t;
                 if (nup > 1 && sum_h > 1.0) { q_r /= sum_h; q_t /= sum_h; sum_h = q_r + q_t; }
@@ -2118,8 +2172,9 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                 }
                 break;
             }
+            case FTB_MAT_MIRROR:
             case FTB_MAT_FILTER:
-            case FTB_MAT_GLOSSY: {   // achromatic lobes (render.h:2505-2537)
+            case FTB_MAT_GLOSSY: {   // achromatic lobes (render.h:2509-2537)
                 double cc[kHeroMax];
                 for (int i = 0; i < nup; ++i)
                     cc[i] = (m.type == FTB_MAT_FILTER) ? clamp01(spec_slot(sc, m.transmit, lam[i], 0.0))
@@ -2131,12 +2186,25 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                     absorbed += to_fixed(beta[i] * (1.0 - wgt), J.tally_scale_inv, f.status);
                     beta[i] *= wgt;
                 }
-                if (m.type == FTB_MAT_FILTER) {
+                if (m.type == FTB_MAT_MIRROR) {
+                    no = h.p + h.n * 1e-6; nd = reflect(rd, h.n);
+                } else if (m.type == FTB_MAT_FILTER) {
                     no = h.p + rd * 1e-6;
                 } else {
                     D3 o = sample_glossy(reflect(rd, h.n), m.roughness, rng);
                     if (dot(o, h.n) <= 0) { fate = 0; break; }
                     no = h.p + h.n * 1e-6; nd = o;
+                }
+                break;
+            }
+            case FTB_MAT_HALF_MIRROR: {   // de-hero, then the scalar half mirror (render.h:2546-2589, 1702-1711)
+                if (nup > 1) { beta[0] *= (double)C; nup = 1; }
+                const double rr = clamp01(spec_slot(sc, m.reflect, lam[0], 0.5));
+                if (uniform(rng) < rr) {
+                    nd = reflect(rd, h.n);
+                    no = h.p + h.n * 1e-6;
+                } else {
+                    no = h.p + rd * 1e-6;
                 }
                 break;
             }
@@ -2180,6 +2248,7 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
                 D3 ngo = oriented_geo_n(h);
                 D3 wi = mk(-rd.x, -rd.y, -rd.z);
                 connect_surface_hero(J, w, f, j, h.p, h.n, ngo, wi, lam, beta, rho, nup);
+                if (MIRROR && sc.n_planes > 0) connect_mirrors_hero(sc, J, w, f, j, h.p, h.n, lam, beta, rho, nup);
                 double q = max_of(rho, nup);
                 if (uniform(rng) >= q) { fate = 0; break; }
                 for (int i = 0; i < nup; ++i) {
@@ -2226,8 +2295,39 @@ __global__ void __launch_bounds__(128, FTB_SHADE_MINB) k_shade_hero(Wave w, cons
     tally_finish(acc, jobs, multi, n_jobs);
 }
 
-// Connections of bundles: one occlusion test, then a splat per wavelength.
+// A bundle's mirror record: every live wavelength is its own splat with its own reflectance
+// (splatMirrorLegs, render.h:1321-1330; bundles run without media); a wavelength whose
+// contribution is not positive adds nothing, not even to the hit count.
 template <bool COUNT, bool INST, bool SHAPES>
+__device__ __noinline__ void mirror_splat_hero(const DevJob& J, const Wave& w, const Frame& f, int i, TravCount& cnt) {
+    MirrorSeen ms;
+    if (!mirror_seen<COUNT, INST, SHAPES>(J, w, f, i, cnt, ms)) return;
+    const DevScene& sc = J.sc;
+    const double inv_d2_omega = 1.0 / (ms.D * ms.D * ms.omega);
+    const int nup = w.snup[i];
+    long long sx = 0, sy = 0, sz = 0, hits = 0;
+    for (int k = 0; k < nup; ++k) {
+        const double lam = k == 0 ? w.slam[i] : w.xlam[(size_t)(k - 1) * w.S + i];
+        const double a = k == 0 ? w.sval[i] : w.xval[(size_t)(k - 1) * w.S + i];
+        const double refl = clamp01(spec_slot(sc, sc.mats[ms.mat].reflect, lam, 0.5));
+        const double contrib = a * refl * inv_d2_omega;
+        if (contrib <= 0.0) continue;
+        sx += to_fixed(cie_x(lam) * contrib, J.film_scale_inv, f.status);
+        sy += to_fixed(cie_y(lam) * contrib, J.film_scale_inv, f.status);
+        sz += to_fixed(cie_z(lam) * contrib, J.film_scale_inv, f.status);
+        ++hits;
+    }
+    if (!hits) return;
+    long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i] & 0xffff)) + 4 * (size_t)~w.spix[i];
+    atomicAdd(reinterpret_cast<unsigned long long*>(px), (unsigned long long)sx);
+    atomicAdd(reinterpret_cast<unsigned long long*>(px + 1), (unsigned long long)sy);
+    atomicAdd(reinterpret_cast<unsigned long long*>(px + 2), (unsigned long long)sz);
+    atomicAdd(reinterpret_cast<unsigned long long*>(px + 3), (unsigned long long)hits);
+}
+
+// Connections of bundles: one occlusion test, then a splat per wavelength.  MIRROR: the queue
+// may also hold mirror records (scenes with planar mirrors).
+template <bool COUNT, bool INST, bool SHAPES, bool MIRROR>
 __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, const DevJob* __restrict__ jobs,
                                                                    Frame f) {
     const int32_t n_jobs = w.params[0];
@@ -2238,10 +2338,14 @@ __global__ void __launch_bounds__(128, FTB_TRAV_MINB) k_shadow_hero(Wave w, cons
     FTB_FOR_WARP_CHUNKS(i, n, &w.counts[kFetchShadow]) {
         const DevJob& J = jobs[n_jobs > 1 ? w.sjob[i] : 0];
         const DevScene& sc = J.sc;
+        if (COUNT) rays++;
+        if (MIRROR && w.spix[i] < 0) {
+            mirror_splat_hero<COUNT, INST, SHAPES>(J, w, f, i, cnt);
+            continue;
+        }
         D3 o = mk(w.sox[i], w.soy[i], w.soz[i]), d = mk(w.sdx[i], w.sdy[i], w.sdz[i]);
         double max_dist = w.smax[i];
         RayCtx R = make_ray(o, d);
-        if (COUNT) rays++;
         if (traverse_any<COUNT, INST, SHAPES>(sc, R, EPS_RAY, max_dist - EPS_RAY, f.status, cnt)) continue;
         long long* px = reinterpret_cast<long long*>(view_film(J, w.sview[i])) + 4 * (size_t)w.spix[i];
         const int nup = w.snup[i];
@@ -2390,7 +2494,13 @@ struct LaunchShadowMirror {
 template <bool C, bool I, bool S>
 struct LaunchShadowHero {
     static void go(int grid, cudaStream_t st, Wave w, const DevJob* jobs, Frame f) {
-        k_shadow_hero<C, I, S><<<grid, 128, 0, st>>>(w, jobs, f);
+        k_shadow_hero<C, I, S, false><<<grid, 128, 0, st>>>(w, jobs, f);
+    }
+};
+template <bool C, bool I, bool S>
+struct LaunchShadowHeroMirror {
+    static void go(int grid, cudaStream_t st, Wave w, const DevJob* jobs, Frame f) {
+        k_shadow_hero<C, I, S, true><<<grid, 128, 0, st>>>(w, jobs, f);
     }
 };
 
@@ -2410,19 +2520,23 @@ struct Issue {
     void emit(bool stream, const PathState& out, int32_t* co) {
         mark(K_EMIT, false);
         const DevJob* jobs = w.jobs;
+#define FTB_EMIT_HERO(S) \
+    (kind.mirrors ? k_emit_hero<S, true><<<grid, T, 0, st>>>(w, jobs, f, out, co) \
+                  : k_emit_hero<S, false><<<grid, T, 0, st>>>(w, jobs, f, out, co))
 #define FTB_EMIT(M, S) \
     (kind.mirrors ? k_emit<M, S, true><<<grid, T, 0, st>>>(w, jobs, f, out, co) \
                   : k_emit<M, S, false><<<grid, T, 0, st>>>(w, jobs, f, out, co))
         if (stream) {
-            if (kind.bundles) k_emit_hero<true><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            if (kind.bundles) FTB_EMIT_HERO(true);
             else if (kind.media) FTB_EMIT(true, true);
             else FTB_EMIT(false, true);
         } else {
-            if (kind.bundles) k_emit_hero<false><<<grid, T, 0, st>>>(w, jobs, f, out, co);
+            if (kind.bundles) FTB_EMIT_HERO(false);
             else if (kind.media) FTB_EMIT(true, false);
             else FTB_EMIT(false, false);
         }
 #undef FTB_EMIT
+#undef FTB_EMIT_HERO
         mark(K_EMIT, true);
     }
     template <template <bool, bool, bool> class K, class... A>
@@ -2438,7 +2552,8 @@ struct Issue {
     }
     void shadow() {
         mark(K_SHADOW, false);
-        if (kind.bundles) trav<LaunchShadowHero>(w, (const DevJob*)w.jobs, f);
+        if (kind.bundles && kind.mirrors) trav<LaunchShadowHeroMirror>(w, (const DevJob*)w.jobs, f);
+        else if (kind.bundles) trav<LaunchShadowHero>(w, (const DevJob*)w.jobs, f);
         else if (kind.mirrors) trav<LaunchShadowMirror>(w, (const DevJob*)w.jobs, f);
         else trav<LaunchShadow>(w, (const DevJob*)w.jobs, f);
         mark(K_SHADOW, true);
@@ -2459,9 +2574,12 @@ struct Issue {
         const DevJob* jobs = w.jobs;
         mark(K_SHADE, false);
 #define FTB_SHADE(...) __VA_ARGS__<<<grid, T, 0, st>>>(w, jobs, f, in, ci, out, co)
-        if (kind.bundles) {
-            if (inst) { if (shp) FTB_SHADE(k_shade_hero<true, true>); else FTB_SHADE(k_shade_hero<true, false>); }
-            else { if (shp) FTB_SHADE(k_shade_hero<false, true>); else FTB_SHADE(k_shade_hero<false, false>); }
+        if (kind.bundles && kind.mirrors) {
+            if (inst) { if (shp) FTB_SHADE(k_shade_hero<true, true, true>); else FTB_SHADE(k_shade_hero<true, false, true>); }
+            else { if (shp) FTB_SHADE(k_shade_hero<false, true, true>); else FTB_SHADE(k_shade_hero<false, false, true>); }
+        } else if (kind.bundles) {
+            if (inst) { if (shp) FTB_SHADE(k_shade_hero<true, true, false>); else FTB_SHADE(k_shade_hero<true, false, false>); }
+            else { if (shp) FTB_SHADE(k_shade_hero<false, true, false>); else FTB_SHADE(k_shade_hero<false, false, false>); }
         } else if (kind.mirrors) {
             if (kind.media) {
                 if (inst) { if (shp) FTB_SHADE(k_shade<true, true, true, true>); else FTB_SHADE(k_shade<true, true, false, true>); }

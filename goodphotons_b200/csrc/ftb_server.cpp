@@ -568,10 +568,6 @@ ftb_status ftb_server_submit(ftb_server* s, const ftb_request* r, uint64_t* job_
     j->hero = (r->hero_c <= 1 || j->sc.n_med > 0) ? 1 : (r->hero_c > ftb::kHeroMax ? ftb::kHeroMax : r->hero_c);
     j->klass = (j->hero > 1 ? 1 : 0) | (j->sc.n_med > 0 ? 2 : 0) | (ftb::scene_has_shapes(j->sc) ? 4 : 0) |
                (j->sc.n_inst > 0 ? 8 : 0) | (j->sc.n_planes > 0 ? 16 : 0);
-    if (j->hero > 1 && j->sc.n_planes > 0) {
-        delete j;
-        return fail(FTB_ERR_UNSUPPORTED, "hero bundles in a scene with planar mirrors (use hero_c 1)");
-    }
     if (j->hero > s->hero_max) {
         delete j;
         return fail(FTB_ERR_TOO_LARGE, "bundle larger than the server's hero_max");

@@ -1154,8 +1154,8 @@ static double vtx_shape(const SpecVtx* vt, V3 wP) {
  * mirror mp -- through the eye's mirror image -- if the reflection point R lies in the
  * plane's box and in the image, the light leg p -> R is clear, and a closest hit from the
  * eye toward R lands on a planar mirror at R; the splat carries that mirror's reflectance. */
-static void connect_specular_plane(Tr* T, const MPlane* mp, V3 p, const SpecVtx* vt, double lam, double beta,
-                                   double w) {
+static void connect_specular_plane(Tr* T, const MPlane* mp, V3 p, const SpecVtx* vt, const double* lam,
+                                   const double* beta, const double* w, int nup) {
     const fto_ctx* c = T->c;
     const Cam* cam = T->cam;
     const V3 eye = cam->eye;
@@ -1191,24 +1191,32 @@ static void connect_specular_plane(Tr* T, const MPlane* mp, V3 p, const SpecVtx*
     if (fabs(hm.t - dE) > 1e-4 * (1.0 + dE)) return;
     if (hm.mat < 0 || hm.mat >= c->n_mats || !planar_mirror(&c->mats[hm.mat])) return;
     const double inv_d2_omega = 1.0 / (D * D * omega);
-    const double refl = clamp01(slot(c, c->mats[hm.mat].reflect, lam, 0.5));
-    double contrib = beta * (w * shape) * refl * inv_d2_omega;
-    if (contrib <= 0.0) return;
-    if (c->n_med > 0) {
-        contrib *= media_transmittance(T, p, wP, dP, lam);
-        contrib *= media_transmittance(T, R, wRE, dE, lam);
+    for (int i = 0; i < nup; ++i) {   /* every live wavelength (splatMirrorLegs) */
+        const double refl = clamp01(slot(c, c->mats[hm.mat].reflect, lam[i], 0.5));
+        double contrib = beta[i] * (w[i] * shape) * refl * inv_d2_omega;
+        if (contrib <= 0.0) continue;
+        if (c->n_med > 0) {
+            contrib *= media_transmittance(T, p, wP, dP, lam[i]);
+            contrib *= media_transmittance(T, R, wRE, dE, lam[i]);
+        }
+        film_add(T->film, px, py, cie_x(lam[i]) * contrib, cie_y(lam[i]) * contrib, cie_z(lam[i]) * contrib);
     }
-    film_add(T->film, px, py, cie_x(lam) * contrib, cie_y(lam) * contrib, cie_z(lam) * contrib);
 }
-/* camSpecularSplatAll / camSpecularSplatVolumeAll (render.h:1515-1585), planar mirrors only
- * (scenes with dielectric or mirror spheres are outside this path) */
-static void cam_specular_splat(Tr* T, V3 p, const SpecVtx* vt, double lam, double beta, double w) {
-    for (int k = 0; k < T->c->n_mp; ++k) connect_specular_plane(T, &T->c->mp[k], p, vt, lam, beta, w);
+/* camSpecularSplatAllVtxN (render.h:1515-1550), planar mirrors only (scenes with dielectric
+ * or mirror spheres are outside this path): the vertex's nup live wavelengths */
+static void cam_specular_splat(Tr* T, V3 p, const SpecVtx* vt, const double* lam, const double* beta,
+                               const double* w, int nup) {
+    for (int k = 0; k < T->c->n_mp; ++k) connect_specular_plane(T, &T->c->mp[k], p, vt, lam, beta, w, nup);
 }
-static void cam_specular_surface(Tr* T, V3 p, V3 n, double lam, double beta, double rho) {
+/* camSpecularSplatAll / camSpecularSplatAllHero (render.h:1559-1576): a surface vertex */
+static void cam_specular_surface_n(Tr* T, V3 p, V3 n, const double* lam, const double* beta, const double* rho,
+                                   int nup) {
     if (T->c->n_mp == 0) return;
     SpecVtx vt; vt.volume = 0; vt.np = n; vt.win = v3(0, 0, 0); vt.g = 0.0;
-    cam_specular_splat(T, p, &vt, lam, beta, rho);
+    cam_specular_splat(T, p, &vt, lam, beta, rho, nup);
+}
+static void cam_specular_surface(Tr* T, V3 p, V3 n, double lam, double beta, double rho) {
+    cam_specular_surface_n(T, p, n, &lam, &beta, &rho, 1);
 }
 
 /* Renderer::refractOrReflect (render.h:2657-2697), stochastic branch */
@@ -1335,9 +1343,10 @@ static void trace_photon(Tr* T, Pcg* rng, int max_bounce, double* e, ftb_photon_
         if (medium_event) {   /* render.h:2105-2115 */
             const Med* sm = &c->med[scatter_med];
             connect_volume(T, sm, mp, rd, lam, beta);
-            if (c->n_mp > 0) {
+            if (c->n_mp > 0) {   /* camSpecularSplatVolumeAll (render.h:1580-1585) */
                 SpecVtx vt; vt.volume = 1; vt.np = v3(0, 0, 0); vt.win = rd; vt.g = sm->g;
-                cam_specular_splat(T, mp, &vt, lam, beta, med_albedo(c, sm, lam));
+                const double alb = med_albedo(c, sm, lam);
+                cam_specular_splat(T, mp, &vt, &lam, &beta, &alb, 1);
             }
             if (pcg_uniform(rng) >= med_albedo(c, sm, lam)) { e[E_ABS] += beta; fate = 0; goto done; }
             V3 nd = sample_hg(rd, sm->g, rng);
@@ -1797,6 +1806,7 @@ static void trace_photon_hero(Tr* T, Pcg* rng, int max_bounce, int C, double* e,
         double one[HERO_MAX];
         for (int i = 0; i < C; ++i) one[i] = 1.0;
         connect_surface_hero(T, origin, emit_n, emit_n, emit_n, lam, beta, one, C);
+        cam_specular_surface_n(T, origin, emit_n, lam, beta, one, C);
     }
     V3 ro = vadd(origin, vmul(dir, 1e-6)), rd = dir;
     Stack stk; stk.n = 0;
@@ -1835,6 +1845,8 @@ static void trace_photon_hero(Tr* T, Pcg* rng, int max_bounce, int C, double* e,
             V3 wi = v3(-rd.x, -rd.y, -rd.z);
             connect_surface_hero(T, h.p, h.n, ngo, wi, lam, beta, rho_r, nup);
             connect_surface_hero(T, h.p, vneg(h.n), vneg(ngo), wi, lam, beta, rho_t, nup);
+            cam_specular_surface_n(T, h.p, h.n, lam, beta, rho_r, nup);
+            cam_specular_surface_n(T, h.p, vneg(h.n), lam, beta, rho_t, nup);
             double q_r = max_of(rho_r, nup), q_t = max_of(rho_t, nup);
             double sum_h = q_r + q_t;
             if (nup > 1 && sum_h > 1.0) { q_r /= sum_h; q_t /= sum_h; sum_h = q_r + q_t; }
@@ -1864,8 +1876,9 @@ static void trace_photon_hero(Tr* T, Pcg* rng, int max_bounce, int C, double* e,
             }
             e[E_ABS] += active_sum(beta, sec_alive ? C : 1); fate = 0; goto done;
         }
+        case FTB_MAT_MIRROR:
         case FTB_MAT_FILTER:
-        case FTB_MAT_GLOSSY: {   /* achromatic lobes (render.h:2505-2537) */
+        case FTB_MAT_GLOSSY: {   /* achromatic lobes (render.h:2509-2537) */
             double cc[HERO_MAX] = {0};
             for (int i = 0; i < nup; ++i)
                 cc[i] = (m->type == FTB_MAT_FILTER) ? clamp01(slot(c, m->transmit, lam[i], 0.0))
@@ -1877,12 +1890,25 @@ static void trace_photon_hero(Tr* T, Pcg* rng, int max_bounce, int C, double* e,
                 e[E_ABS] += beta[i] * (1.0 - w);
                 beta[i] *= w;
             }
-            if (m->type == FTB_MAT_FILTER) {
+            if (m->type == FTB_MAT_MIRROR) {
+                ro = vadd(h.p, vmul(h.n, 1e-6)); rd = vreflect(rd, h.n);
+            } else if (m->type == FTB_MAT_FILTER) {
                 ro = vadd(h.p, vmul(rd, 1e-6));
             } else {
                 V3 o = sample_glossy(vreflect(rd, h.n), m->roughness, rng);
                 if (vdot(o, h.n) <= 0) { e[E_ABS] += active_sum(beta, sec_alive ? C : 1); fate = 0; goto done; }
                 ro = vadd(h.p, vmul(h.n, 1e-6)); rd = o;
+            }
+            continue;
+        }
+        case FTB_MAT_HALF_MIRROR: {   /* de-hero, then the scalar half mirror (render.h:2546-2589, 1702-1711) */
+            if (sec_alive) { beta[0] *= (double)C; sec_alive = 0; }
+            double r = clamp01(slot(c, m->reflect, lam[0], 0.5));
+            if (pcg_uniform(rng) < r) {
+                V3 o = vreflect(rd, h.n);
+                ro = vadd(h.p, vmul(h.n, 1e-6)); rd = o;
+            } else {
+                ro = vadd(h.p, vmul(rd, 1e-6));
             }
             continue;
         }
@@ -1929,6 +1955,7 @@ static void trace_photon_hero(Tr* T, Pcg* rng, int max_bounce, int C, double* e,
             V3 ngo = oriented_geo_n(&h);
             V3 wi = v3(-rd.x, -rd.y, -rd.z);
             connect_surface_hero(T, h.p, h.n, ngo, wi, lam, beta, rho, nup);
+            cam_specular_surface_n(T, h.p, h.n, lam, beta, rho, nup);
             double q = max_of(rho, nup);
             if (pcg_uniform(rng) >= q) { e[E_ABS] += active_sum(beta, sec_alive ? C : 1); fate = 0; goto done; }
             for (int i = 0; i < nup; ++i) {

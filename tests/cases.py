@@ -83,6 +83,7 @@ CASES = {
     "instances": (make_instances, 32, 8192, 16, 11, 1),
     "mirrors": (make_mirrors, 32, 8192, 16, 13, 1),
     "mirrors_fog": (lambda L: make_mirrors(L, fog=True), 32, 8192, 32, 17, 1),
+    "mirrors_hero4": (make_mirrors, 32, 8192, 16, 19, 4),
     # hero-wavelength bundles (Renderer::tracePhotonHero): C wavelengths per photon
     "cornell_hero4": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 3, 4),
     "glass_hero4": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 5, 4),

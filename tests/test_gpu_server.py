@@ -20,6 +20,7 @@ def resident(gpu):
         "materials": lib.Scene(cases.make_materials(gpu), 0, gpu),
         "fog": lib.Scene(scenes.make_fog_strands(gpu, n_strands=300), 0, gpu),
         "instances": lib.Scene(cases.make_instances(gpu), 0, gpu),
+        "mirrors": lib.Scene(cases.make_mirrors(gpu), 0, gpu),
     }
     yield sc
     for s in sc.values():
@@ -107,7 +108,8 @@ def test_bundles_and_classes_in_the_mix(gpu, resident):
     """Hero bundles (C = 4, 3) among one-wavelength jobs of every kernel class: passes hold
     one class at a time, and each job still equals its solo render."""
     specs = [("glass", 32, 400_000, 4), ("cornell", 24, 300_000, 1), ("fog", 16, 50_000, 1),
-             ("cornell", 40, 900_000, 3), ("instances", 24, 200_000, 4), ("materials", 32, 250_000, 1)]
+             ("cornell", 40, 900_000, 3), ("instances", 24, 200_000, 4), ("materials", 32, 250_000, 1),
+             ("mirrors", 32, 300_000, 1), ("mirrors", 24, 300_000, 4)]
     srv = lib.Server(device=0, lib=gpu, wave_slots=1 << 19)
     films, ids = [], []
     for k, (name, res, n, hero) in enumerate(specs):

@@ -55,6 +55,7 @@ SHIM_SCENES = {
     "glass": (lambda L: scenes.make_glass(L, level=3), 16),
     "materials": (cases.make_materials, 16),
     "instances": (cases.make_instances, 16),
+    "mirrors": (cases.make_mirrors, 16),
 }
 
 
@@ -62,7 +63,8 @@ SHIM_SCENES = {
 def test_render_forward_cuda_through_shim(shim, gpu, scene):
     """`glass`: the benchmarked material (Cauchy IOR; wall steps with 0.01 nm ramps);
     `materials`: Sellmeier, nested priorities, filters, glossy; `instances`: the reference
-    Scene's blasList / MeshInstances go through the shim's bake."""
+    Scene's blasList / MeshInstances go through the shim's bake; `mirrors`: the reference
+    Scene's mirror planes (Scene::build) and the plane connector."""
     mk, mb = SHIM_SCENES[scene]
     d = mk(gpu)
     cam = scenes.default_camera(gpu, 48)
@@ -94,7 +96,7 @@ def test_render_forward_cuda_through_shim(shim, gpu, scene):
     np.testing.assert_allclose(en, ce, rtol=1e-9)
 
 
-@pytest.mark.parametrize("scene,hero", [("glass", 1), ("glass", 4), ("cornell", 4)])
+@pytest.mark.parametrize("scene,hero", [("glass", 1), ("glass", 4), ("cornell", 4), ("mirrors", 4)])
 def test_shared_session_through_shim(shim, gpu, oracle, scene, hero):
     """sharedForwardGpuBegin with two cameras and heroC, two batches with the cumulative
     seedBase: camera 0's running total equals the reference CPU tracer's film of the same

@@ -61,3 +61,62 @@ def render_sharded(scene, cam, n, film, seed_base=0, max_bounce=8, frac_bits=0, 
                          dtype=torch.int64, device=film.device)
     reduce_film(film, tally, dst=dst, group=group)
     return tally
+
+
+class ServerPool:
+    """Serving on several GPUs of one node: one render server per device (replicas of the
+    scene library), each job sent whole to one device -- the one with the least photons
+    queued or running -- so jobs never span GPUs and no collective is involved (a job's film
+    is its server's, exactly what one GPU renders for it).
+
+    `scene_of(key, device)` returns the resident scene of library entry `key` on `device`
+    (it is asked once per pair and the result kept); `server_cfg` goes to every server
+    (max_active, hbm_budget, ...).  `make_server(device, **cfg)` builds a server (the
+    library's lib.Server by default)."""
+
+    def __init__(self, devices, scene_of, lib=None, make_server=None, **server_cfg):
+        if not devices:
+            raise ValueError("no devices")
+        if make_server is None:
+            from . import lib as lib_mod
+            L = lib or lib_mod.load()
+
+            def make_server(device, **cfg):
+                return lib_mod.Server(device=device, lib=L, **cfg)
+        self.devices = list(devices)
+        self.servers = {d: make_server(d, **server_cfg) for d in self.devices}
+        self.scene_of = scene_of
+        self.scenes = {}
+        self.load = {d: 0 for d in self.devices}   # photons submitted and not yet waited on
+        self.jobs = {}                              # handle -> (device, server job id, photons)
+        self.next_handle = 1
+
+    def pick(self):
+        """The device with the least outstanding photons (ties to the first listed)."""
+        return min(self.devices, key=lambda d: (self.load[d], self.devices.index(d)))
+
+    def submit(self, key, cam, n, **kw):
+        d = self.pick()
+        if (key, d) not in self.scenes:
+            self.scenes[(key, d)] = self.scene_of(key, d)
+        jid = self.servers[d].submit(self.scenes[(key, d)], cam, n, **kw)
+        h = self.next_handle
+        self.next_handle += 1
+        self.jobs[h] = (d, jid, n)
+        self.load[d] += n
+        return h
+
+    def device_of(self, handle):
+        return self.jobs[handle][0]
+
+    def wait(self, handle, timeout=-1.0):
+        d, jid, n = self.jobs[handle]
+        r = self.servers[d].wait(jid, timeout)
+        del self.jobs[handle]
+        self.load[d] -= n
+        return r
+
+    def close(self):
+        for s in self.servers.values():
+            s.close()
+        self.servers = {}

@@ -126,3 +126,25 @@ def test_bundles_and_classes_in_the_mix(gpu, resident):
                                             hero_c=hero)
         np.testing.assert_array_equal(film, solo, err_msg=f"{name} hero {hero}")
         assert list(r.energy.fx) == list(en.fx), f"{name} hero {hero} energy"
+
+
+def test_server_pool_jobs_equal_solo_renders(gpu, resident):
+    """multigpu.ServerPool over the devices this box has (one here): jobs routed to a
+    device's server render exactly their solo films."""
+    from goodphotons_b200 import multigpu
+    pool = multigpu.ServerPool([0], lambda key, d: resident[key], lib=gpu, wave_slots=1 << 19)
+    specs = [("glass", 24, 200_000), ("mirrors", 32, 150_000), ("fog", 16, 60_000)]
+    films, hs = [], []
+    for k, (name, res, n) in enumerate(specs):
+        films.append(np.full((res, res, 4), -1, dtype=np.int64))
+        mb = {"cornell": 8, "fog": 32}.get(name, 16)
+        hs.append(pool.submit(name, scenes.default_camera(gpu, res), n, seed_base=31 * k, max_bounce=mb,
+                              host_film=films[k]))
+    results = [pool.wait(h) for h in hs]
+    pool.close()
+    for k, ((name, res, n), film, r) in enumerate(zip(specs, films, results)):
+        assert r.status == 0, name
+        mb = {"cornell": 8, "fog": 32}.get(name, 16)
+        solo, _, en = resident[name].render(scenes.default_camera(gpu, res), n, seed_base=31 * k, max_bounce=mb)
+        np.testing.assert_array_equal(film, solo, err_msg=name)
+        assert list(r.energy.fx) == list(en.fx), name

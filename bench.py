@@ -672,6 +672,25 @@ def config_records(args, local, L):
     return out
 
 
+def config_records_child(local, tuning, timeout_s=900):
+    """config_records in a child process (its own CUDA context, `--configs-only`, the
+    headline's launch tuning), so that a failure there is reported in the record instead of
+    ending the headline's run."""
+    t = ",".join(str(int(x)) for x in (tuning.wave_slots, tuning.grid_mult, tuning.use_graphs, tuning.sort_rays,
+                                       tuning.regenerate))
+    cmd = [sys.executable, os.path.abspath(__file__), "--configs-only", "--tuning", t]
+    env = dict(os.environ, LOCAL_RANK=str(local))
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env)
+    except subprocess.TimeoutExpired:
+        return {"error": f"the configuration records did not finish within {timeout_s} s"}
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr or r.stdout).strip().splitlines()[-3:]
+        return {"error": f"exit {r.returncode}: " + " | ".join(tail)}
+    return json.loads(lines[-1])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -692,6 +711,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' records")
+    ap.add_argument("--configs-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--photons", type=int, default=0, help="photons per step (default: the workload's frame)")
     ap.add_argument("--tuning", default="",
                     help="wave_slots,blocks_per_sm,graphs[,sort_rays[,regenerate]] instead of the autotuner")
@@ -701,6 +721,17 @@ def main():
                          "(uniform for the Cornell configuration, which specifies it; SPD otherwise)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.configs_only:   # the child of config_records_child
+        import torch
+        from goodphotons_b200 import lib
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        L = lib.load()
+        if args.tuning:
+            v = [int(x) for x in args.tuning.split(",")]
+            L.set_tuning(local, wave_slots=v[0], grid_mult=v[1], use_graphs=v[2], sort_rays=v[3], regenerate=v[4])
+        print(json.dumps(config_records(args, local, L)), flush=True)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
         return
@@ -917,7 +948,7 @@ def main():
 
     configs = None
     if rank == 0 and world == 1 and not args.no_configs and args.workload == "glass" and args.hero == 1:
-        configs = config_records(args, local, L)
+        configs = config_records_child(local, tuning)
 
     if rank == 0:
         line = {

@@ -504,10 +504,12 @@ ftb_status ftb_autotune(ftb_scene* scene, const ftb_camera* cam, int64_t n_photo
  * hbm_budget, and manages those scenes' residency -- a job is admitted when its film, plus
  * its scene's tables if the scene is not on the device, fits the budget; to make room the
  * server evicts scenes that no admitted job uses, least recently used first, and restores a
- * job's scene on admission (ftb_scene_evict / ftb_scene_restore, stream-ordered).  Scenes
- * that cannot leave the device (instances, clones) count as resident.  While the server
- * runs, render its scenes only through it; when it is destroyed, scenes stay as they are
- * (ftb_scene_resident tells). */
+ * job's scene on admission (ftb_scene_evict / ftb_scene_restore, stream-ordered; a scene's
+ * first eviction copies its tables to host memory and waits for the device, later ones only
+ * free).  Scenes that cannot leave the device (instances, clones) count as resident.  The
+ * server may evict or restore any scene its jobs have used until it is destroyed, so such
+ * scenes must outlive the server, and while it runs they are rendered only through it; when
+ * it is destroyed, scenes stay as they are (ftb_scene_resident tells). */
 typedef struct ftb_server ftb_server;
 
 typedef struct ftb_server_config {

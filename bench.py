@@ -702,8 +702,8 @@ def main():
     ap.add_argument("--serve-budget-log2", type=float, default=28.0, help="serve: largest photon budget, log2")
     ap.add_argument("--serve-sample", type=int, default=40, help="serve: jobs of the plain (bake per job) sample")
     ap.add_argument("--serve-sizes", type=int, default=24, help="serve: library mesh sizes per family")
-    ap.add_argument("--serve-scene-mb", type=int, default=512, help="serve: device MiB for resident scenes")
-    ap.add_argument("--serve-film-mb", type=int, default=4096, help="serve: device MiB for admitted films")
+    ap.add_argument("--serve-scene-mb", type=int, default=256, help="serve: device MiB for resident scenes")
+    ap.add_argument("--serve-film-mb", type=int, default=1024, help="serve: device MiB for admitted films")
     ap.add_argument("--max-active", type=int, default=64, help="serve: jobs admitted at once")
     ap.add_argument("--frames", type=int, default=64, help="animation: frames")
     ap.add_argument("--baseline-frames", type=int, default=64, help="animation: frames of the plain baseline")

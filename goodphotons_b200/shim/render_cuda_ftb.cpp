@@ -298,10 +298,12 @@ void bake(const Scene& sc, Baked& b) {
         o.to_world[9] = mi.toWorld.t.x; o.to_world[10] = mi.toWorld.t.y; o.to_world[11] = mi.toWorld.t.z;
         b.instances.push_back(o);
     }
-    if (!sc.implicits.empty() || !sc.emissiveVolumes.empty() ||
-        sc.envMap || !sc.mirrorPlanes.empty() || !sc.dielSphereIdx.empty() || !sc.mirrorSphereIdx.empty()) {
+    // planar mirrors are on the path: the library groups the mirror triangles into planes
+    // itself, as Scene::buildMirrorPlanes does (scene.h:1646-1720)
+    if (!sc.implicits.empty() || !sc.emissiveVolumes.empty() || sc.envMap || !sc.dielSphereIdx.empty() ||
+        !sc.mirrorSphereIdx.empty()) {
         b.supported = false;
-        b.why = "implicits, emissive volumes, environment maps and specular connectors are not on this path";
+        b.why = "implicits, emissive volumes, environment maps and the sphere connectors are not on this path";
     }
     for (const Emitter& e : sc.emitters) {
         ftb_emitter o{};

@@ -605,6 +605,7 @@ def plain_config(desc, res, n, mb, lam, steps, local, L):
         torch.cuda.synchronize(dev)
         ms.append(a.elapsed_time(b))
     host = torch.empty((res, res, 4), dtype=torch.int64, pin_memory=True)
+    sc.render(cam, 1 << 20, seed_base=1 << 42, max_bounce=mb, out=host.numpy(), lambda_mode=lam)   # warm-up
     torch.cuda.synchronize(dev)
     t = time.perf_counter()
     sc.render(cam, n, seed_base=1 << 41, max_bounce=mb, out=host.numpy(), lambda_mode=lam)
@@ -632,9 +633,11 @@ def config_records(args, local, L):
     >= 1M-triangle glass mesh, the Cornell box, fog + strands, a reduced animation batch and a
     reduced served stream (their full forms: --level 8, --workload cornell | fog_strands |
     animation | serve)."""
-    from goodphotons_b200 import abi, scenes
+    from goodphotons_b200 import abi, lib, scenes
 
     out = {}
+    # first use of the device builder loads its kernels (untimed, as in a long-running host)
+    lib.Scene(scenes.make_cornell(L), local, L, build=abi.BUILD_DEVICE).close()
     t = time.perf_counter()
     r = plain_config(scenes.make_glass(L, level=8), 1024, 1 << 28, 16, abi.LAMBDA_SPD, 2, local, L)
     r["config"] = {"workload": "glass", "mesh": "level-8 icosphere", "triangles": 20 * 4 ** 8, "film": "1024x1024",

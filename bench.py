@@ -43,7 +43,8 @@ WORKLOADS = {
     "fog_strands": (512, 1 << 26, 32),
 }
 METRIC = "photon paths/s on 1 B200"
-NODE_BYTES = 80     # WNode
+NODE_BYTES = 80     # a node in its compressed form (WNode, 8-bit child planes): the algorithmic
+                    # unit, although the device reads the 208-byte widened form (FNode)
 REC_BYTES = 80      # PrimRec
 RAY_IO_BYTES = 64   # extend: queue index 4 + ray 48 read, hit t 8 + record 4 written
 SHADOW_IO_BYTES = 140   # shadow: record read (origin 24, direction 24, max 8, XYZ 24, pixel, job,
@@ -887,6 +888,8 @@ def main():
         "peak_source": f"{peak_kind} hbm_gbs (copy)",
         "algorithmic_bytes_per_unit": round(unit_bytes, 1),
         "algorithmic_bytes_per_ray": round(bytes_per_ray, 1),
+        "node_bytes_counted": f"{NODE_BYTES} per visit (the compressed node; the kernel reads the "
+                              f"208-byte widened node, which this figure does not credit)",
         "node_visits_per_ray": round(nodes_c / max(1, rays_c), 3),
         "record_tests_per_ray": round(recs_c / max(1, rays_c), 3),
         "closest_hit_rays_per_photon": round(rays_per_photon, 4),

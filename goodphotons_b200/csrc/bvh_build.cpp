@@ -17,6 +17,29 @@
 
 namespace ftb {
 
+float round_down(double x) {
+    float f = (float)x;
+    if ((double)f > x) f = std::nextafterf(f, -INFINITY);
+    return f;
+}
+
+float round_up(double x) {
+    float f = (float)x;
+    if ((double)f < x) f = std::nextafterf(f, INFINITY);
+    return f;
+}
+
+namespace {
+// A node's child boxes, outward to float, into its FTB_PLANES floats (n filled slots).
+void put_planes(float* dst, const double (&clo)[3][8], const double (&chi)[3][8], int n) {
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < FTB_WIDTH; ++k) {
+            dst[8 * a + k] = k < n ? round_down(clo[a][k]) : INFINITY;
+            dst[24 + 8 * a + k] = k < n ? round_up(chi[a][k]) : -INFINITY;
+        }
+}
+}  // namespace
+
 namespace {
 
 // Largest leaf of the binary build (<= FTB_LEAF_MAX, which the node encoding allows);
@@ -119,11 +142,6 @@ struct Builder {
 // Float value the device computes for a quantized plane: fmaf(q, 2^e, p).
 inline float plane(int q, float scale, float p) { return std::fmaf((float)q, scale, p); }
 
-float round_down(double x) {
-    float f = (float)x;
-    if ((double)f > x) f = std::nextafterf(f, -INFINITY);
-    return f;
-}
 
 struct Quant {
     float p;
@@ -201,6 +219,7 @@ bool collapse_to_wide(const std::vector<BinNode>& bnodes, const std::vector<int>
     } B{bnodes, bidx};
     out.nodes.clear();
     out.order.clear();
+    out.planes.clear();
     if (bnodes.empty()) return true;
     // Collapse.  A wide node is described by the binary node ids of its (<= 8) children.
     struct Pending { int bnode; int wide; };
@@ -266,14 +285,51 @@ bool collapse_to_wide(const std::vector<BinNode>& bnodes, const std::vector<int>
         w.px = p[0]; w.py = p[1]; w.pz = p[2];
         w.ex = (uint8_t)(e[0] + 127); w.ey = (uint8_t)(e[1] + 127); w.ez = (uint8_t)(e[2] + 127);
         out.nodes[pd.wide] = w;
+        out.planes.resize(out.nodes.size() * FTB_PLANES);
+        put_planes(&out.planes[(size_t)pd.wide * FTB_PLANES], clo, chi, (int)kids.size());
     }
     return true;
+}
+
+std::vector<FNode> widen_nodes(const WideBvh& bvh) {
+    const std::vector<WNode>& nodes = bvh.nodes;
+    const bool tight = bvh.planes.size() == nodes.size() * FTB_PLANES;
+    std::vector<FNode> out(nodes.size());
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        const WNode& w = nodes[i];
+        FNode& f = out[i];
+        f.child_base = w.child_base;
+        f.prim_base = w.prim_base;
+        const float p[3] = {w.px, w.py, w.pz};
+        const int e[3] = {(int)w.ex - 127, (int)w.ey - 127, (int)w.ez - 127};
+        const uint8_t* qlo[3] = {w.qlo_x, w.qlo_y, w.qlo_z};
+        const uint8_t* qhi[3] = {w.qhi_x, w.qhi_y, w.qhi_z};
+        for (int k = 0; k < FTB_WIDTH; ++k) {
+            const uint8_t m = w.meta[k];
+            f.meta[k] = (m != 0 && ((w.imask >> k) & 1u)) ? (uint8_t)((FNODE_INNER << 5) | (m & 31u)) : m;
+            for (int a = 0; a < 3; ++a) {
+                const float s = std::ldexp(1.0f, e[a]);
+                if (!m) {
+                    f.lo[a][k] = INFINITY;
+                    f.hi[a][k] = -INFINITY;
+                } else if (tight) {
+                    f.lo[a][k] = bvh.planes[i * FTB_PLANES + 8 * a + k];
+                    f.hi[a][k] = bvh.planes[i * FTB_PLANES + 24 + 8 * a + k];
+                } else {
+                    f.lo[a][k] = plane(qlo[a][k], s, p[a]);
+                    f.hi[a][k] = plane(qhi[a][k], s, p[a]);
+                }
+            }
+        }
+    }
+    return out;
 }
 
 bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, std::string& err) {
     const size_t nn = b.nodes.size();
     if (b.order.empty()) return true;
     std::vector<Box> nb(nn);
+    b.planes.resize(nn * FTB_PLANES);
     // children always follow their parent, so a reverse sweep sees every child first
     for (size_t i = nn; i-- > 0;) {
         WNode& w = b.nodes[i];
@@ -308,6 +364,7 @@ bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, st
             }
         w.px = p[0]; w.py = p[1]; w.pz = p[2];
         w.ex = (uint8_t)(e[0] + 127); w.ey = (uint8_t)(e[1] + 127); w.ez = (uint8_t)(e[2] + 127);
+        put_planes(&b.planes[i * FTB_PLANES], clo, chi, n);
     }
     return true;
 }

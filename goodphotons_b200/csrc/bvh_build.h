@@ -28,7 +28,12 @@ struct Box {
 struct WideBvh {
     std::vector<WNode> nodes;   // root at 0
     std::vector<int> order;     // record i holds primitive order[i]
+    // Per node, FTB_PLANES floats: lo[3][8] then hi[3][8], each child's (grown) box rounded
+    // outward to float; an empty slot is +inf / -inf.  Empty when a producer keeps only the
+    // 8-bit planes (the device form then uses their decoded values).
+    std::vector<float> planes;
 };
+#define FTB_PLANES 48
 
 // A binary tree: root 0; a node with count > 0 is a leaf over idx[first, first + count).
 struct BinNode {
@@ -61,6 +66,16 @@ bool build_wide_lbvh_device(const std::vector<Box>& boxes, int leaf_size, int de
 // child boxes are recomputed bottom-up and quantized afresh, so the result is exactly as
 // conservative as a build; only the tree's shape may be worse for the new boxes.
 bool refit_wide_bvh(WideBvh& b, const std::vector<Box>& boxes, double margin, std::string& err);
+
+// The device form of a tree: each child's box as `planes` holds it (the exact box rounded
+// outward to float), or, without planes, as the floats its bytes decode to (fmaf(q, 2^e, p),
+// the values the quantization was checked against); inner children marked in the meta byte,
+// empty children as boxes no ray enters.
+std::vector<FNode> widen_nodes(const WideBvh& bvh);
+
+// Outward float rounding of a box bound.
+float round_down(double x);
+float round_up(double x);
 
 // Structural check run on every bake: child and record indices in range, every node
 // reachable once, every primitive referenced exactly once, children after parents.

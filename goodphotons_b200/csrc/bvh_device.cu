@@ -188,8 +188,8 @@ __device__ bool quantize_axis_dev(double nlo, double nhi, const double* clo, con
 // One level of the collapse: wide node w (in [begin, end)) is rooted at binary node src[w].
 // counters[0] = wide nodes allocated, counters[1] = records allocated, counters[2] = errors.
 __global__ void k_collapse_level(const DBin* __restrict__ bins, const int* __restrict__ idx, int begin, int end,
-                                 int* __restrict__ src, WNode* __restrict__ nodes, int* __restrict__ order,
-                                 int* __restrict__ counters) {
+                                 int* __restrict__ src, WNode* __restrict__ nodes, float* __restrict__ planes,
+                                 int* __restrict__ order, int* __restrict__ counters) {
     const int w = begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= end) return;
     const int root = src[w];
@@ -254,6 +254,13 @@ __global__ void k_collapse_level(const DBin* __restrict__ bins, const int* __res
     o.px = p[0]; o.py = p[1]; o.pz = p[2];
     o.ex = (uint8_t)(e[0] + 127); o.ey = (uint8_t)(e[1] + 127); o.ez = (uint8_t)(e[2] + 127);
     nodes[w] = o;
+    // the child boxes rounded outward to float (empty slots: +inf / -inf)
+    float* pl = planes + (size_t)w * FTB_PLANES;
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < FTB_WIDTH; ++k) {
+            pl[8 * a + k] = k < nk ? __double2float_rd(clo[a][k]) : __int_as_float(0x7f800000);
+            pl[24 + 8 * a + k] = k < nk ? __double2float_ru(chi[a][k]) : __int_as_float(0xff800000);
+        }
 }
 
 struct DevBuf {
@@ -308,13 +315,15 @@ bool build_wide_lbvh_device(const std::vector<Box>& boxes, int leaf_size, int de
         int *d_id, *d_ids, *d_left, *d_right, *d_parent, *d_first, *d_count, *d_visit, *d_src, *d_order, *d_ctr;
         DBin* d_bins;
         WNode* d_nodes;
+        float* d_planes;
         const size_t nn = (size_t)n;
         if ((e = buf.get(&d_boxes, nn)) || (e = buf.get(&d_nb, 2 * nn)) || (e = buf.get(&d_k, nn)) ||
             (e = buf.get(&d_ks, nn)) || (e = buf.get(&d_id, nn)) || (e = buf.get(&d_ids, nn)) ||
             (e = buf.get(&d_left, nn)) || (e = buf.get(&d_right, nn)) || (e = buf.get(&d_parent, 2 * nn)) ||
             (e = buf.get(&d_first, nn)) || (e = buf.get(&d_count, nn)) || (e = buf.get(&d_visit, nn)) ||
             (e = buf.get(&d_bins, 2 * nn)) || (e = buf.get(&d_src, nn + 1)) || (e = buf.get(&d_order, nn)) ||
-            (e = buf.get(&d_nodes, nn + 1)) || (e = buf.get(&d_ctr, 4)))
+            (e = buf.get(&d_nodes, nn + 1)) || (e = buf.get(&d_planes, (nn + 1) * FTB_PLANES)) ||
+            (e = buf.get(&d_ctr, 4)))
             return fail("allocation");
         if ((e = cudaMemcpy(d_boxes, hb.data(), sizeof(DBox) * nn, cudaMemcpyHostToDevice))) return fail("upload");
         const int T = 256, G = (n + T - 1) / T, G2 = (2 * n - 1 + T - 1) / T;
@@ -353,8 +362,8 @@ bool build_wide_lbvh_device(const std::vector<Box>& boxes, int leaf_size, int de
             return fail("upload");
         int begin = 0, end = 1, ctr[4] = {0, 0, 0, 0};
         while (begin < end) {
-            k_collapse_level<<<(end - begin + 127) / 128, 128>>>(d_bins, d_ids, begin, end, d_src, d_nodes, d_order,
-                                                                d_ctr);
+            k_collapse_level<<<(end - begin + 127) / 128, 128>>>(d_bins, d_ids, begin, end, d_src, d_nodes, d_planes,
+                                                                d_order, d_ctr);
             if ((e = cudaGetLastError())) return fail("collapse");
             if ((e = cudaMemcpy(ctr, d_ctr, sizeof ctr, cudaMemcpyDeviceToHost))) return fail("collapse");
             if (ctr[0] > n + 1 || ctr[1] > n) { e = cudaSuccess; return fail("collapse overran its arrays"); }
@@ -365,7 +374,9 @@ bool build_wide_lbvh_device(const std::vector<Box>& boxes, int leaf_size, int de
         if (ctr[1] != n) { e = cudaSuccess; return fail("collapse lost records"); }
         out.nodes.resize((size_t)ctr[0]);
         out.order.resize(nn);
+        out.planes.resize((size_t)ctr[0] * FTB_PLANES);
         if ((e = cudaMemcpy(out.nodes.data(), d_nodes, sizeof(WNode) * out.nodes.size(), cudaMemcpyDeviceToHost)) ||
+            (e = cudaMemcpy(out.planes.data(), d_planes, sizeof(float) * out.planes.size(), cudaMemcpyDeviceToHost)) ||
             (e = cudaMemcpy(out.order.data(), d_order, sizeof(int) * nn, cudaMemcpyDeviceToHost)))
             return fail("download");
     }

@@ -245,7 +245,7 @@ ftb_status upload(DevBlock& blk, const T* host, size_t n, const T** out, const c
 // A baked BLAS (Blas, scene.h:996-1033): wide BVH and triangle records in local space.
 struct BlasDev {
     DevBlock mem;
-    const WNode* nodes = nullptr;
+    const FNode* nodes = nullptr;
     const PrimRec* recs = nullptr;
     const double* tri_n = nullptr;
     int64_t n_tris = 0;
@@ -343,7 +343,7 @@ struct ftb_scene {
     std::vector<std::shared_ptr<BlasDev>> blas;    // BLAS assets the instances place
     std::unique_ptr<DevBlock> own;                 // this scene's TLAS nodes and instance table
     TlasHost tlas;                                 // for refits (scenes with instances)
-    WNode* d_nodes = nullptr;                      // mutable TLAS nodes (in `own`)
+    FNode* d_nodes = nullptr;                      // mutable TLAS nodes (in `own`)
     DevInst* d_inst = nullptr;
     double power = 0.0;
     uint64_t scene_bytes = 0;
@@ -623,7 +623,8 @@ ftb_status bake_blas(const ftb_blas_desc& d, int device, ftb::BuildMethod method
         any_smooth |= smooth != 0;
         R.info = d.tri_mat[p] | (REC_TRI << 24) | (smooth << 30);
     }
-    ftb_status st = upload(b->mem, bvh.nodes.data(), bvh.nodes.size(), &b->nodes, "upload BLAS nodes");
+    const std::vector<FNode> fn = ftb::widen_nodes(bvh);
+    ftb_status st = upload(b->mem, fn.data(), fn.size(), &b->nodes, "upload BLAS nodes");
     if (st == FTB_OK) st = upload(b->mem, recs.data(), recs.size(), &b->recs, "upload BLAS records");
     if (st == FTB_OK && any_smooth) st = upload(b->mem, d.tri_n, (size_t)nt * 9, &b->tri_n, "upload BLAS normals");
     if (st != FTB_OK) return st;
@@ -1245,6 +1246,10 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
             nd.prim_base += rec_shift;
             bvh.nodes.push_back(nd);
         }
+        if (a.planes.size() == node_shift * FTB_PLANES && b.planes.size() == b.nodes.size() * FTB_PLANES) {
+            bvh.planes = std::move(a.planes);
+            bvh.planes.insert(bvh.planes.end(), b.planes.begin(), b.planes.end());
+        }
         for (int p : b.order) bvh.order.push_back(p + (int)n_other);
     } else {
         if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err, method, device)) {
@@ -1255,6 +1260,7 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
     }
     if (np == 0) {   // an empty root with no children
         bvh.nodes.resize(1);
+        bvh.planes.clear();
         std::memset(&bvh.nodes[0], 0, sizeof(WNode));
     }
     // records in leaf order
@@ -1298,24 +1304,25 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
         mats[i] = DevMat{m.type, m.priority, m.reflect, m.ior, m.absorb, m.transmit, m.roughness};
     }
     DevScene& D = s->dev;
-    const WNode* dn; const PrimRec* dr;
+    const FNode* dn; const PrimRec* dr;
+    const std::vector<FNode> fn = ftb::widen_nodes(bvh);
 #define UP(host, n, out, what) do { ftb_status u_ = upload(s, host, n, out, what); if (u_ != FTB_OK) { delete s; return u_; } } while (0)
     UP(recs.data(), recs.size(), &dr, "upload records");
     if (ni > 0) {   // the nodes and the instance table are this scene's own: refits rewrite them
         s->own.reset(new DevBlock());
         s->own->device = device;
         const DevInst* di = nullptr;
-        ftb_status us = upload(*s->own, bvh.nodes.data(), bvh.nodes.size(), &dn, "upload nodes");
+        ftb_status us = upload(*s->own, fn.data(), fn.size(), &dn, "upload nodes");
         if (us == FTB_OK) us = upload(*s->own, T.inst.data(), T.inst.size(), &di, "upload instances");
         if (us != FTB_OK) { delete s; return us; }
-        s->d_nodes = const_cast<WNode*>(dn);
+        s->d_nodes = const_cast<FNode*>(dn);
         s->d_inst = const_cast<DevInst*>(di);
         D.inst = di;
         D.n_inst = ni;
         T.bvh = bvh;
         T.boxes = std::move(boxes);
     } else {
-        UP(bvh.nodes.data(), bvh.nodes.size(), &dn, "upload nodes");
+        UP(fn.data(), fn.size(), &dn, "upload nodes");
     }
     D.nodes = dn; D.recs = dr;
     D.root2 = root2;
@@ -1448,8 +1455,8 @@ ftb_status set_transforms(ftb_scene* s, const double* to_world, int64_t n) {
     std::string err;
     if (!ftb::refit_wide_bvh(T.bvh, T.boxes, std::ldexp(maxabs, -18), err)) return fail(FTB_ERR_INVALID, err);
     DeviceGuard guard(s->device);
-    CK(cudaMemcpy(s->d_nodes, T.bvh.nodes.data(), T.bvh.nodes.size() * sizeof(WNode), cudaMemcpyHostToDevice),
-       "upload refit nodes");
+    const std::vector<FNode> fn = ftb::widen_nodes(T.bvh);
+    CK(cudaMemcpy(s->d_nodes, fn.data(), fn.size() * sizeof(FNode), cudaMemcpyHostToDevice), "upload refit nodes");
     CK(cudaMemcpy(s->d_inst, T.inst.data(), T.inst.size() * sizeof(DevInst), cudaMemcpyHostToDevice),
        "upload instances");
     return FTB_OK;
@@ -1481,12 +1488,13 @@ ftb_status ftb_scene_clone_instances(const ftb_scene* src, const double* to_worl
     if (src->dev.n_inst > 0) {
         c->own.reset(new DevBlock());
         c->own->device = c->device;
-        const WNode* dn = nullptr;
+        const FNode* dn = nullptr;
         const DevInst* di = nullptr;
-        ftb_status st = upload(*c->own, c->tlas.bvh.nodes.data(), c->tlas.bvh.nodes.size(), &dn, "upload nodes");
+        const std::vector<FNode> fn = ftb::widen_nodes(c->tlas.bvh);
+        ftb_status st = upload(*c->own, fn.data(), fn.size(), &dn, "upload nodes");
         if (st == FTB_OK) st = upload(*c->own, c->tlas.inst.data(), c->tlas.inst.size(), &di, "upload instances");
         if (st != FTB_OK) { delete c; return st; }
-        c->d_nodes = const_cast<WNode*>(dn);
+        c->d_nodes = const_cast<FNode*>(dn);
         c->d_inst = const_cast<DevInst*>(di);
         c->dev.nodes = dn;
         c->dev.inst = di;

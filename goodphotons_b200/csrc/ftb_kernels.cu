@@ -457,13 +457,20 @@ __device__ void hit_attributes(const double* __restrict__ tri_n, const RayCtx& R
 }
 
 // ------------------------------------------------------------------ traversal (fp32) ---
+// Culling is conservative by construction.  Child planes are floats that enclose the child's
+// box grown by 2^-18 x the scene's largest coordinate M (the builders check each against the
+// exact box), and a plane x is entered at t = fmaf(x, ix, cx) with ix = 1/d and cx = -o*ix
+// rounded to float.  The rounding of o, of cx and of the fma move t by at most ~2^-23 M |ix|
+// (far inside the box growth, 2^-18 M |ix|); the rounding of d, of 1/d and of the fma's
+// result scale t by at most ~(1 +- 2^-22), inside the interval's widening by 2^-21 (T_LO,
+// T_HI).  So no ray culls a child whose primitives the exact fp64 test would hit.
 struct RayF {
-    float ox, oy, oz, ix, iy, iz;
-    bool nx, ny, nz;   // direction component negative: near plane is the box's hi side
+    float ix, iy, iz;
+    float cx, cy, cz;   // -o * ix per axis
+    bool nx, ny, nz;    // direction component negative: near plane is the box's hi side
 };
 __device__ __forceinline__ RayF make_rayf(D3 o, D3 d) {
     RayF r;
-    r.ox = (float)o.x; r.oy = (float)o.y; r.oz = (float)o.z;
     float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
     // a zero component is replaced by +-1e-20: the ray moves by at most 1e-20*t, far below
     // the box margin, and the reciprocals stay finite (no inf*0 NaNs in the slab test)
@@ -471,6 +478,7 @@ __device__ __forceinline__ RayF make_rayf(D3 o, D3 d) {
     dy = fabsf(dy) > 1e-20f ? dy : copysignf(1e-20f, dy);
     dz = fabsf(dz) > 1e-20f ? dz : copysignf(1e-20f, dz);
     r.ix = 1.0f / dx; r.iy = 1.0f / dy; r.iz = 1.0f / dz;
+    r.cx = -(float)o.x * r.ix; r.cy = -(float)o.y * r.iy; r.cz = -(float)o.z * r.iz;
     r.nx = dx < 0.0f; r.ny = dy < 0.0f; r.nz = dz < 0.0f;
     return r;
 }
@@ -484,43 +492,39 @@ __device__ __forceinline__ uint32_t byte_of(uint2 w, int i) {
 #define T_HI (1.0f + 4.76837158203125e-7f)
 #define T_CULL (1.0f + 1.9073486328125e-6f)  // 1 + 2^-19: covers the key's slot bits (< 8 ulps)
 
-struct NodeRay {   // per-node slab constants: t(q) = q * a + b
-    float ax, bx, ay, by, az, bz;
-    uint2 lox, loy, loz, hix, hiy, hiz, meta;
-};
-__device__ __forceinline__ NodeRay node_setup(const uint4 (&n)[5], const RayF& R) {
-    NodeRay N;
-    float px = __uint_as_float(n[0].x), py = __uint_as_float(n[0].y), pz = __uint_as_float(n[0].z);
-    float sx = __uint_as_float((n[0].w & 0xffu) << 23);
-    float sy = __uint_as_float(((n[0].w >> 8) & 0xffu) << 23);
-    float sz = __uint_as_float(((n[0].w >> 16) & 0xffu) << 23);
-    N.ax = sx * R.ix; N.bx = (px - R.ox) * R.ix;
-    N.ay = sy * R.iy; N.by = (py - R.oy) * R.iy;
-    N.az = sz * R.iz; N.bz = (pz - R.oz) * R.iz;
-    N.lox = make_uint2(n[2].x, n[2].y); N.loy = make_uint2(n[2].z, n[2].w); N.loz = make_uint2(n[3].x, n[3].y);
-    N.hix = make_uint2(n[3].z, n[3].w); N.hiy = make_uint2(n[4].x, n[4].y); N.hiz = make_uint2(n[4].z, n[4].w);
-    if (R.nx) { uint2 t = N.lox; N.lox = N.hix; N.hix = t; }
-    if (R.ny) { uint2 t = N.loy; N.loy = N.hiy; N.hiy = t; }
-    if (R.nz) { uint2 t = N.loz; N.loz = N.hiz; N.hiz = t; }
-    N.meta = make_uint2(n[1].z, n[1].w);
-    return N;
-}
-// Slab test of child i; returns the entry distance or +inf when missed / empty.
-__device__ __forceinline__ float child_t(const NodeRay& N, int i, float tmin_f, float tmax_f) {
-    float tnx = __fmaf_rn((float)byte_of(N.lox, i), N.ax, N.bx);
-    float tfx = __fmaf_rn((float)byte_of(N.hix, i), N.ax, N.bx);
-    float tny = __fmaf_rn((float)byte_of(N.loy, i), N.ay, N.by);
-    float tfy = __fmaf_rn((float)byte_of(N.hiy, i), N.ay, N.by);
-    float tnz = __fmaf_rn((float)byte_of(N.loz, i), N.az, N.bz);
-    float tfz = __fmaf_rn((float)byte_of(N.hiz, i), N.az, N.bz);
-    float a = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin_f)) * T_LO;
-    float b = fminf(fminf(tfx, tfy), fminf(tfz, tmax_f)) * T_HI;
-    return (a <= b && byte_of(N.meta, i) != 0) ? a : __int_as_float(0x7f800000);
+// Slab test of one child from its near and far planes; the entry distance, or +inf when
+// missed.  An empty child's planes (+inf near, -inf far on every axis) give +inf.
+__device__ __forceinline__ float slab(float nx, float fx, float ny, float fy, float nz, float fz, const RayF& R,
+                                      float tmin_f, float tmax_f) {
+    const float a = fmaxf(fmaxf(__fmaf_rn(nx, R.ix, R.cx), __fmaf_rn(ny, R.iy, R.cy)),
+                          fmaxf(__fmaf_rn(nz, R.iz, R.cz), tmin_f)) * T_LO;
+    const float b = fminf(fminf(__fmaf_rn(fx, R.ix, R.cx), __fmaf_rn(fy, R.iy, R.cy)),
+                          fminf(__fmaf_rn(fz, R.iz, R.cz), tmax_f)) * T_HI;
+    return a <= b ? a : __int_as_float(0x7f800000);
 }
 
-__device__ __forceinline__ void load_node(const WNode* nodes, uint32_t i, uint4 (&n)[5]) {
-    const uint4* p = reinterpret_cast<const uint4*>(nodes + i);
-    n[0] = __ldg(p); n[1] = __ldg(p + 1); n[2] = __ldg(p + 2); n[3] = __ldg(p + 3); n[4] = __ldg(p + 4);
+// Entry distances of the eight children of node i, and the node's header (child_base,
+// prim_base, meta).  The near planes of an axis are the box's lo side unless the ray's
+// direction is negative there.
+__device__ __forceinline__ void node_children(const FNode* __restrict__ nodes, uint32_t i, const RayF& R,
+                                              float tmin_f, float tmax_f, float (&t)[8], uint4& hdr) {
+    const FNode* n = nodes + i;
+    hdr = __ldg(reinterpret_cast<const uint4*>(n));
+    const float4* nx = reinterpret_cast<const float4*>(R.nx ? n->hi[0] : n->lo[0]);
+    const float4* fx = reinterpret_cast<const float4*>(R.nx ? n->lo[0] : n->hi[0]);
+    const float4* ny = reinterpret_cast<const float4*>(R.ny ? n->hi[1] : n->lo[1]);
+    const float4* fy = reinterpret_cast<const float4*>(R.ny ? n->lo[1] : n->hi[1]);
+    const float4* nz = reinterpret_cast<const float4*>(R.nz ? n->hi[2] : n->lo[2]);
+    const float4* fz = reinterpret_cast<const float4*>(R.nz ? n->lo[2] : n->hi[2]);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const float4 a = __ldg(nx + h), b = __ldg(fx + h), c = __ldg(ny + h);
+        const float4 d = __ldg(fy + h), e = __ldg(nz + h), f = __ldg(fz + h);
+        t[4 * h + 0] = slab(a.x, b.x, c.x, d.x, e.x, f.x, R, tmin_f, tmax_f);
+        t[4 * h + 1] = slab(a.y, b.y, c.y, d.y, e.y, f.y, R, tmin_f, tmax_f);
+        t[4 * h + 2] = slab(a.z, b.z, c.z, d.z, e.z, f.z, R, tmin_f, tmax_f);
+        t[4 * h + 3] = slab(a.w, b.w, c.w, d.w, e.w, f.w, R, tmin_f, tmax_f);
+    }
 }
 
 struct TravCount { unsigned long long nodes, recs, exact; };
@@ -528,10 +532,9 @@ struct TravCount { unsigned long long nodes, recs, exact; };
 
 // Stack entry: a node index, or (bit 31) a leaf: first record << 2 | (count - 1).
 #define LEAF_BIT 0x80000000u
-__device__ __forceinline__ uint32_t child_entry(uint32_t child_base, uint32_t prim_base, uint32_t imask,
-                                                uint2 meta, int i) {
+__device__ __forceinline__ uint32_t child_entry(uint32_t child_base, uint32_t prim_base, uint2 meta, int i) {
     uint32_t m = byte_of(meta, i);
-    if ((imask >> i) & 1u) return child_base + (m & 31u);
+    if ((m >> 5) == FNODE_INNER) return child_base + (m & 31u);
     return LEAF_BIT | ((prim_base + (m & 31u)) << 2) | ((m >> 5) - 1u);
 }
 
@@ -553,7 +556,7 @@ struct LocalStack {
 // together rather than interleaved with node steps.  leaf(first, count, tmax_f) tests a
 // leaf's records and returns the (possibly lowered) fp32 bound on t.
 template <bool COUNT, class Stack, class Leaf>
-__device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, const RayF& F, float tmin_f,
+__device__ __forceinline__ float walk_closest(const FNode* __restrict__ nodes, const RayF& F, float tmin_f,
                                               float tmax_f, Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt,
                                               uint32_t root = 0) {
     int sp = 0;
@@ -561,34 +564,33 @@ __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, c
     bool live = true;
     while (live) {
         while (!(cur & LEAF_BIT)) {
-            uint4 n[5];
-            load_node(nodes, cur, n);
+            float t[8];
+            uint4 hdr;
+            node_children(nodes, cur, F, tmin_f, tmax_f, t, hdr);
             if (COUNT) cnt.nodes++;
-            NodeRay N = node_setup(n, F);
             uint32_t k[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                float t = child_t(N, i, tmin_f, tmax_f);
-                k[i] = (t == __int_as_float(0x7f800000)) ? 0xffffffffu : ((__float_as_uint(t) & ~7u) | (uint32_t)i);
-            }
+            for (int i = 0; i < 8; ++i)
+                k[i] = (t[i] == __int_as_float(0x7f800000)) ? 0xffffffffu
+                                                           : ((__float_as_uint(t[i]) & ~7u) | (uint32_t)i);
             CSWAP(k[0], k[2]); CSWAP(k[1], k[3]); CSWAP(k[4], k[6]); CSWAP(k[5], k[7]);
             CSWAP(k[0], k[4]); CSWAP(k[1], k[5]); CSWAP(k[2], k[6]); CSWAP(k[3], k[7]);
             CSWAP(k[0], k[1]); CSWAP(k[2], k[3]); CSWAP(k[4], k[5]); CSWAP(k[6], k[7]);
             CSWAP(k[2], k[4]); CSWAP(k[3], k[5]);
             CSWAP(k[1], k[4]); CSWAP(k[3], k[6]);
             CSWAP(k[1], k[2]); CSWAP(k[3], k[4]); CSWAP(k[5], k[6]);
-            const uint32_t imask = n[0].w >> 24, child_base = n[1].x, prim_base = n[1].y;
+            const uint32_t child_base = hdr.x, prim_base = hdr.y;
+            const uint2 meta = make_uint2(hdr.z, hdr.w);
 #pragma unroll
             for (int i = 7; i >= 1; --i) {
                 if (k[i] != 0xffffffffu) {
                     if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return tmax_f; }
-                    st.put(sp, make_uint2(child_entry(child_base, prim_base, imask, N.meta, (int)(k[i] & 7u)),
-                                          k[i] & ~7u));
+                    st.put(sp, make_uint2(child_entry(child_base, prim_base, meta, (int)(k[i] & 7u)), k[i] & ~7u));
                     ++sp;
                 }
             }
             if (k[0] != 0xffffffffu) {
-                cur = child_entry(child_base, prim_base, imask, N.meta, (int)(k[0] & 7u));
+                cur = child_entry(child_base, prim_base, meta, (int)(k[0] & 7u));
                 continue;
             }
             bool found = false;
@@ -615,7 +617,7 @@ __device__ __forceinline__ float walk_closest(const WNode* __restrict__ nodes, c
 // Any-hit walk: order does not change the answer, so children are taken in slot order,
 // leaves first; leaf(first, count) returns true on a hit, which ends the walk.
 template <bool COUNT, class Stack, class Leaf>
-__device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const RayF& F, float tmin_f, float tmax_f,
+__device__ __forceinline__ bool walk_any(const FNode* __restrict__ nodes, const RayF& F, float tmin_f, float tmax_f,
                                          Stack& st, Leaf& leaf, int32_t* status, TravCount& cnt,
                                          uint32_t root = 0) {
     int sp = 0;
@@ -623,22 +625,25 @@ __device__ __forceinline__ bool walk_any(const WNode* __restrict__ nodes, const 
     bool live = true;
     while (live) {
         while (!(cur & LEAF_BIT)) {
-            uint4 n[5];
-            load_node(nodes, cur, n);
+            float t[8];
+            uint4 hdr;
+            node_children(nodes, cur, F, tmin_f, tmax_f, t, hdr);
             if (COUNT) cnt.nodes++;
-            NodeRay N = node_setup(n, F);
-            uint32_t hit = 0;
+            const uint2 meta = make_uint2(hdr.z, hdr.w);
+            uint32_t hit = 0, imask = 0;
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
-                if (child_t(N, i, tmin_f, tmax_f) != __int_as_float(0x7f800000)) hit |= 1u << i;
-            const uint32_t imask = n[0].w >> 24, child_base = n[1].x, prim_base = n[1].y;
+            for (int i = 0; i < 8; ++i) {
+                if (t[i] != __int_as_float(0x7f800000)) hit |= 1u << i;
+                if ((byte_of(meta, i) >> 5) == FNODE_INNER) imask |= 1u << i;
+            }
+            const uint32_t child_base = hdr.x, prim_base = hdr.y;
             uint32_t order = (hit & ~imask) | ((hit & imask) << 8);
             bool have_next = false;
             uint32_t next = 0;
             while (order) {
                 int b = __ffs(order) - 1;
                 order &= order - 1;
-                uint32_t e = child_entry(child_base, prim_base, imask, N.meta, b & 7);
+                uint32_t e = child_entry(child_base, prim_base, meta, b & 7);
                 if (!have_next) { next = e; have_next = true; continue; }
                 if (sp >= FTB_STACK) { atomicOr(status, ST_STACK_OVERFLOW); return false; }
                 st.put(sp++, e);

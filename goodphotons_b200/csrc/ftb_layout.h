@@ -2,10 +2,11 @@
 // bvh_build.cpp) and the kernels (ftb_kernels.cu).
 //
 // HBM layout of a baked scene:
-//   nodes   : WNode[n_nodes], 80 B each, 16 B aligned -- compressed 8-wide BVH.  Child
-//             boxes are 8-bit quantized against the node's float grid (p, 2^e) and rounded
-//             outward, so the fp32 traversal never culls a primitive the exact fp64 test
-//             would accept.
+//   nodes   : FNode[n_nodes], 208 B each, 16 B aligned -- 8-wide BVH.  The builders make
+//             compressed 80-byte WNodes (child boxes 8-bit quantized against the node's
+//             float grid (p, 2^e), rounded outward, so the fp32 traversal never culls a
+//             primitive the exact fp64 test would accept); the upload widens each to an
+//             FNode holding the float planes that the bytes decode to.
 //   recs    : PrimRec[n_recs], 80 B each -- one record per primitive, in leaf order.
 //             Triangles keep their three vertices in double (the exact watertight test
 //             reads them); the last 8 B carry the global primitive index, material and
@@ -38,6 +39,23 @@ struct alignas(16) WNode {
     uint8_t qhi_x[8], qhi_y[8], qhi_z[8];
 };
 static_assert(sizeof(WNode) == 80, "WNode must be 80 bytes");
+
+// The device form of a wide node: the same children, with each child plane stored as the
+// float the 8-bit form decodes to (fmaf(q, 2^e, p), the value the builders check against
+// the exact box), so traversal reads planes instead of decoding bytes.  Planes are kept
+// per axis and side, so a ray takes its near and far planes by its direction's signs with
+// no per-child select.  meta byte: 0 = empty; count<<5 | offset for a leaf (count 1..4,
+// offset from prim_base); 7<<5 | offset for an inner child (offset from child_base).  An
+// empty child has lo = +inf and hi = -inf on every axis, which every ray's slab test misses.
+struct alignas(16) FNode {
+    uint32_t child_base;
+    uint32_t prim_base;
+    uint8_t meta[8];
+    float lo[3][8];
+    float hi[3][8];
+};
+static_assert(sizeof(FNode) == 208, "FNode must be 208 bytes");
+#define FNODE_INNER 7u
 
 // 80-byte primitive record.  d[9] holds two int32: prim (global index) and
 // info = mat | type << 24 | smooth << 30.  An instance record (REC_INST) keeps its instance
@@ -78,7 +96,7 @@ struct DevMed {
 // One placement of a BLAS (MeshInstance, scene.h:1035-1063).
 struct DevInst {
     double xl[12];            // world -> local map (toLocal): 3x3 row-major, then translation
-    const WNode* nodes;       // the BLAS hierarchy and triangle records
+    const FNode* nodes;       // the BLAS hierarchy and triangle records
     const PrimRec* recs;
     const double* tri_n;      // 9 per BLAS triangle or null
     int32_t mat_override, pad;
@@ -94,7 +112,7 @@ struct DevPlane {
 };
 
 struct DevScene {
-    const WNode* nodes;
+    const FNode* nodes;
     const PrimRec* recs;
     const double* tri_n;      // 9 per triangle (global index) or null
     const DevSpec* spec;

@@ -663,7 +663,7 @@ def config_records(args, local, L):
                                                                "photon_budgets")},
                         "reduced": "16 frames, budgets 2^22-2^25 (full: --workload animation)"}
     checkpoint("the animation record")
-    sv = serve_stream(150, 25.0, 8, abi.BUILD_DEVICE, 128, 512, 64, 20, local, L)
+    sv = serve_stream(150, 25.0, 8, abi.BUILD_DEVICE, 512, 512, 64, 20, local, L)
     out["serve"] = {"value": sv["value"], "unit": "photon paths/s", "latency_s": sv["latency_s"],
                     "capacity": sv["capacity"], "one_at_a_time": sv["one_at_a_time"],
                     "capacity_vs_plain": sv["capacity_vs_plain"],
@@ -706,7 +706,7 @@ def main():
     ap.add_argument("--serve-budget-log2", type=float, default=28.0, help="serve: largest photon budget, log2")
     ap.add_argument("--serve-sample", type=int, default=40, help="serve: jobs of the plain (bake per job) sample")
     ap.add_argument("--serve-sizes", type=int, default=24, help="serve: library mesh sizes per family")
-    ap.add_argument("--serve-scene-mb", type=int, default=256, help="serve: device MiB for resident scenes")
+    ap.add_argument("--serve-scene-mb", type=int, default=512, help="serve: device MiB for resident scenes")
     ap.add_argument("--serve-film-mb", type=int, default=1024, help="serve: device MiB for admitted films")
     ap.add_argument("--max-active", type=int, default=64, help="serve: jobs admitted at once")
     ap.add_argument("--frames", type=int, default=64, help="animation: frames")

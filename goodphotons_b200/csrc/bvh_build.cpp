@@ -301,14 +301,17 @@ std::vector<FNode> widen_nodes(const WideBvh& bvh) {
         f.child_base = w.child_base;
         f.prim_base = w.prim_base;
         const float p[3] = {w.px, w.py, w.pz};
-        const int e[3] = {(int)w.ex - 127, (int)w.ey - 127, (int)w.ez - 127};
+        const int eb[3] = {w.ex, w.ey, w.ez};
+        float sc[3] = {0.0f, 0.0f, 0.0f};
+        if (!tight)
+            for (int a = 0; a < 3; ++a) sc[a] = std::ldexp(1.0f, eb[a] - 127);
         const uint8_t* qlo[3] = {w.qlo_x, w.qlo_y, w.qlo_z};
         const uint8_t* qhi[3] = {w.qhi_x, w.qhi_y, w.qhi_z};
         for (int k = 0; k < FTB_WIDTH; ++k) {
             const uint8_t m = w.meta[k];
             f.meta[k] = (m != 0 && ((w.imask >> k) & 1u)) ? (uint8_t)((FNODE_INNER << 5) | (m & 31u)) : m;
             for (int a = 0; a < 3; ++a) {
-                const float s = std::ldexp(1.0f, e[a]);
+                const float s = sc[a];
                 if (!m) {
                     f.lo[a][k] = INFINITY;
                     f.hi[a][k] = -INFINITY;

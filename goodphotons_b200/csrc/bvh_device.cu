@@ -18,6 +18,7 @@
 
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -315,15 +316,14 @@ bool build_wide_lbvh_device(const std::vector<Box>& boxes, int leaf_size, int de
         int *d_id, *d_ids, *d_left, *d_right, *d_parent, *d_first, *d_count, *d_visit, *d_src, *d_order, *d_ctr;
         DBin* d_bins;
         WNode* d_nodes;
-        float* d_planes;
+        float* d_planes = nullptr;
         const size_t nn = (size_t)n;
         if ((e = buf.get(&d_boxes, nn)) || (e = buf.get(&d_nb, 2 * nn)) || (e = buf.get(&d_k, nn)) ||
             (e = buf.get(&d_ks, nn)) || (e = buf.get(&d_id, nn)) || (e = buf.get(&d_ids, nn)) ||
             (e = buf.get(&d_left, nn)) || (e = buf.get(&d_right, nn)) || (e = buf.get(&d_parent, 2 * nn)) ||
             (e = buf.get(&d_first, nn)) || (e = buf.get(&d_count, nn)) || (e = buf.get(&d_visit, nn)) ||
             (e = buf.get(&d_bins, 2 * nn)) || (e = buf.get(&d_src, nn + 1)) || (e = buf.get(&d_order, nn)) ||
-            (e = buf.get(&d_nodes, nn + 1)) || (e = buf.get(&d_planes, (nn + 1) * FTB_PLANES)) ||
-            (e = buf.get(&d_ctr, 4)))
+            (e = buf.get(&d_nodes, nn + 1)) || (e = buf.get(&d_ctr, 4)))
             return fail("allocation");
         if ((e = cudaMemcpy(d_boxes, hb.data(), sizeof(DBox) * nn, cudaMemcpyHostToDevice))) return fail("upload");
         const int T = 256, G = (n + T - 1) / T, G2 = (2 * n - 1 + T - 1) / T;
@@ -361,7 +361,24 @@ bool build_wide_lbvh_device(const std::vector<Box>& boxes, int leaf_size, int de
             (e = cudaMemcpy(d_src, &zero, sizeof zero, cudaMemcpyHostToDevice)))
             return fail("upload");
         int begin = 0, end = 1, ctr[4] = {0, 0, 0, 0};
+        // the planes of the wide nodes grow with the levels (a tree has far fewer wide nodes
+        // than primitives; nn + 1 bounds them)
+        size_t cap = std::min(nn + 1, nn / 4 + 64);
+        if ((e = cudaMalloc(&d_planes, cap * FTB_PLANES * sizeof(float)))) return fail("allocation");
+        struct PlaneBuf { float*& p; ~PlaneBuf() { if (p) cudaFree(p); } } planes_guard{d_planes};
         while (begin < end) {
+            if ((size_t)end > cap) {
+                const size_t nc = std::min(nn + 1, std::max((size_t)end, 2 * cap));
+                float* np = nullptr;
+                if ((e = cudaMalloc(&np, nc * FTB_PLANES * sizeof(float)))) return fail("allocation");
+                if ((e = cudaMemcpy(np, d_planes, (size_t)begin * FTB_PLANES * sizeof(float), cudaMemcpyDeviceToDevice))) {
+                    cudaFree(np);
+                    return fail("planes");
+                }
+                cudaFree(d_planes);
+                d_planes = np;
+                cap = nc;
+            }
             k_collapse_level<<<(end - begin + 127) / 128, 128>>>(d_bins, d_ids, begin, end, d_src, d_nodes, d_planes,
                                                                 d_order, d_ctr);
             if ((e = cudaGetLastError())) return fail("collapse");

@@ -209,21 +209,25 @@ struct DevBlock {
     uint64_t bytes = 0;
     // Residency (ftb_scene_evict / ftb_scene_restore): the size of each allocation, whether
     // it came from the stream-ordered allocator (a restore), and host copies of the arrays
-    // (made on the first eviction and kept, so later evictions only free).
+    // (made on the first eviction and kept, so later evictions only free).  The copies are
+    // pinned, so a restore's uploads are asynchronous: a render server restores scenes
+    // without stalling the thread that launches its passes.
     std::vector<size_t> sizes;
     std::vector<char> pooled;
-    std::vector<std::vector<unsigned char>> saved;
+    std::vector<unsigned char*> saved;
     std::vector<void*> evicted;   // the allocations' addresses when they were freed
     bool resident = true;
     DevBlock() = default;
     DevBlock(const DevBlock&) = delete;
     DevBlock& operator=(const DevBlock&) = delete;
     ~DevBlock() {
-        if (ptrs.empty() || !resident) return;
+        if (ptrs.empty()) return;
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(device);
-        for (void* p : ptrs) cudaFree(p);   // waits for the device, pooled allocations too
+        if (resident)
+            for (void* p : ptrs) cudaFree(p);   // waits for the device, pooled allocations too
+        for (unsigned char* h : saved) if (h) cudaFreeHost(h);
         cudaSetDevice(cur);
     }
 };
@@ -938,11 +942,19 @@ ftb_status evict_locked(ftb_scene* s, cudaStream_t stream) {
     }
     DeviceGuard guard(s->device);
     if (b.saved.size() != b.ptrs.size()) {
-        b.saved.assign(b.ptrs.size(), {});
-        for (size_t k = 0; k < b.ptrs.size(); ++k) {
-            b.saved[k].resize(b.sizes[k]);
-            CK(cudaMemcpy(b.saved[k].data(), b.ptrs[k], b.sizes[k], cudaMemcpyDeviceToHost), "evict copy");
+        std::vector<unsigned char*> host(b.ptrs.size(), nullptr);
+        cudaError_t e = cudaSuccess;
+        for (size_t k = 0; k < b.ptrs.size() && e == cudaSuccess; ++k) {
+            e = cudaHostAlloc((void**)&host[k], b.sizes[k], cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaMemcpy(host[k], b.ptrs[k], b.sizes[k], cudaMemcpyDeviceToHost);
         }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            for (unsigned char* h : host) if (h) cudaFreeHost(h);
+            return fail(e == cudaErrorMemoryAllocation ? FTB_ERR_OOM : FTB_ERR_CUDA,
+                        std::string("evict copy: ") + cudaGetErrorString(e));
+        }
+        b.saved = std::move(host);
     }
     b.evicted = b.ptrs;
     for (size_t k = 0; k < b.ptrs.size(); ++k) {
@@ -968,7 +980,7 @@ ftb_status restore_locked(ftb_scene* s, cudaStream_t stream) {
     const int emit_alloc = s->field_alloc[7];
     for (size_t k = 0; k < b.ptrs.size(); ++k) {
         if ((int)k == emit_alloc) {
-            DevEmit* em = reinterpret_cast<DevEmit*>(b.saved[k].data());
+            DevEmit* em = reinterpret_cast<DevEmit*>(b.saved[k]);
             const size_t ne = b.sizes[k] / sizeof(DevEmit);
             for (size_t e = 0; e < ne; ++e)
                 for (size_t q = 0; q < k; ++q)
@@ -976,7 +988,7 @@ ftb_status restore_locked(ftb_scene* s, cudaStream_t stream) {
         }
         void* p = nullptr;
         cudaError_t e = cudaMallocAsync(&p, b.sizes[k], stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(p, b.saved[k].data(), b.sizes[k], cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p, b.saved[k], b.sizes[k], cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             if (p) cudaFreeAsync(p, stream);

@@ -1263,6 +1263,45 @@ ftb_status ftb_scene_create(const ftb_scene_desc* d, int32_t device, ftb_scene**
             bvh.planes.insert(bvh.planes.end(), b.planes.begin(), b.planes.end());
         }
         for (int p : b.order) bvh.order.push_back(p + (int)n_other);
+        // Occlusion walks take both trees in one walk: three nodes appended after them, a top
+        // node whose two children are copies of the roots (children of a node are
+        // consecutive).  Closest-hit walks keep the two separate walks, which measured faster
+        // for them; occlusion walks measured faster over the top node.
+        if (bvh.planes.size() != bvh.nodes.size() * FTB_PLANES) {   // planes from the decoded bytes
+            const std::vector<FNode> dec = ftb::widen_nodes(bvh);
+            bvh.planes.resize(dec.size() * FTB_PLANES);
+            for (size_t i = 0; i < dec.size(); ++i) {
+                std::memcpy(&bvh.planes[i * FTB_PLANES], dec[i].lo, 24 * sizeof(float));
+                std::memcpy(&bvh.planes[i * FTB_PLANES + 24], dec[i].hi, 24 * sizeof(float));
+            }
+        }
+        const size_t top = bvh.nodes.size();
+        WNode t;
+        std::memset(&t, 0, sizeof t);
+        t.child_base = (uint32_t)top + 1;
+        t.meta[0] = (uint8_t)((1 << 5) | 0);
+        t.meta[1] = (uint8_t)((1 << 5) | 1);
+        t.imask = 3;
+        const WNode ra = bvh.nodes[0], rb = bvh.nodes[node_shift];
+        bvh.nodes.push_back(t);
+        bvh.nodes.push_back(ra);
+        bvh.nodes.push_back(rb);
+        std::vector<float> tp(FTB_PLANES);
+        for (int a = 0; a < 3; ++a)
+            for (int k = 0; k < 8; ++k) { tp[8 * a + k] = INFINITY; tp[24 + 8 * a + k] = -INFINITY; }
+        const size_t roots[2] = {0, node_shift};
+        for (int c = 0; c < 2; ++c)
+            for (int a = 0; a < 3; ++a)
+                for (int k = 0; k < 8; ++k) {   // the root's box: the union of its children's (empty: +inf / -inf)
+                    tp[8 * a + c] = std::min(tp[8 * a + c], bvh.planes[roots[c] * FTB_PLANES + 8 * a + k]);
+                    tp[24 + 8 * a + c] = std::max(tp[24 + 8 * a + c], bvh.planes[roots[c] * FTB_PLANES + 24 + 8 * a + k]);
+                }
+        bvh.planes.insert(bvh.planes.end(), tp.begin(), tp.end());
+        for (int c = 0; c < 2; ++c) {
+            const std::vector<float> copy(bvh.planes.begin() + (ptrdiff_t)(roots[c] * FTB_PLANES),
+                                          bvh.planes.begin() + (ptrdiff_t)((roots[c] + 1) * FTB_PLANES));
+            bvh.planes.insert(bvh.planes.end(), copy.begin(), copy.end());
+        }
     } else {
         if (np > 0 && !ftb::build_wide_bvh(boxes, margin, bvh, err, method, device)) {
             delete s;

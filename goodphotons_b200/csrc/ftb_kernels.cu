@@ -814,9 +814,9 @@ __device__ bool traverse_any(const DevScene& sc, const RayCtx& R, double tmin, d
         return false;
     };
     LocalStack<uint32_t> st;
-    if (walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt)) return true;
-    return SHAPES && sc.root2 > 0 &&
-           walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt, (uint32_t)sc.root2);
+    // a scene with two hierarchies keeps a top node over both in its last three nodes
+    const uint32_t root = (SHAPES && sc.root2 > 0) ? (uint32_t)(sc.n_nodes - 3) : 0u;
+    return walk_any<COUNT>(sc.nodes, F, tmin_f, tmax_f, st, leaf, status, cnt, root);
 }
 
 // Hit on BLAS record `sub` of instance I, in world terms: the local hit's attributes

@@ -125,7 +125,8 @@ struct DevScene {
     const DevInst* inst;
     const DevPlane* planes;   // planar mirrors (camera connections by reflection)
     int32_t n_nodes, n_recs, n_mats, n_emit, n_med, n_spec;
-    int32_t root2;            // second hierarchy (the curves') in nodes, or -1
+    int32_t root2;            // second hierarchy (the curves') in nodes, or -1; with two, the
+                              // last three nodes are a top node over both and copies of the roots
     int32_t n_planes;
     int64_t n_tris;
     int64_t n_inst;

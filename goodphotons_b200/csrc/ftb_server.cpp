@@ -104,6 +104,8 @@ struct ftb_server {
     uint64_t scene_bytes = 0;          // resident scenes counted against hbm
     uint64_t use_clock = 0;
     std::map<const ftb_scene*, SceneUse> scenes;
+    uint64_t blocked = 0;              // id of the queue's head while it waits for room
+    int64_t blocked_wave = 0;          // passes launched when it started waiting
     Clock::time_point t0;
 
     std::mutex mu;
@@ -142,6 +144,17 @@ void set_device(ftb_server* s) { cudaSetDevice(s->device); }
 // HBM budget mode: make room for job j (its film, and its scene's tables if the scene is
 // not on the device) by evicting scenes no admitted job uses, least recently used first;
 // then restore j's scene.  false: it does not fit yet (mu held).
+// An admitted job takes its scene's device view (re-read at admission: a restore moves the
+// tables) and counts as one of the scene's users.
+void use_scene_locked(ftb_server* s, Job* j) {
+    SceneUse& u = s->scenes[j->req.scene];
+    int dev = 0, sms = 0;
+    double power = 0.0;
+    ftb::scene_internals(j->req.scene, &j->sc, &dev, &sms, &power);
+    u.users++;
+    u.last = ++s->use_clock;
+}
+
 bool fit_locked(ftb_server* s, Job* j) {
     SceneUse& u = s->scenes[j->req.scene];
     const bool resident = ftb::scene_resident(j->req.scene);
@@ -172,59 +185,87 @@ bool fit_locked(ftb_server* s, Job* j) {
             s->admitted_since_launch = true;   // passes wait for the restore (admit_ev)
         }
     }
-    int dev = 0, sms = 0;
-    double power = 0.0;
-    ftb::scene_internals(j->req.scene, &j->sc, &dev, &sms, &power);
-    u.users++;
-    u.last = ++s->use_clock;
+    use_scene_locked(s, j);
     return true;
 }
 
 // Admit queued jobs in arrival order while a slot is free and the film (HBM budget: the
 // job's footprint) fits (mu held).
+void start_job_locked(ftb_server* s, Job* j);
+
+// With an HBM budget, a job waiting at the head of the queue for room holds back the jobs
+// behind it.  Those whose scene is on the device and whose film fits the room left -- no
+// eviction, no restore -- are admitted past it, during the two passes after the head began
+// to wait; then admission waits for the head, so it is not starved.
+void backfill_locked(ftb_server* s) {
+    const uint64_t head = s->queue.front()->id;
+    if (s->blocked != head) { s->blocked = head; s->blocked_wave = s->st.waves; }
+    if (s->st.waves - s->blocked_wave >= 2) return;
+    int scanned = 0;
+    for (auto it = std::next(s->queue.begin()); it != s->queue.end() && !s->free_slots.empty() && scanned < 256;
+         ++scanned) {
+        Job* j = *it;
+        auto u = s->scenes.find(j->req.scene);
+        if (u != s->scenes.end() && u->second.counted &&
+            s->wave_bytes + s->film_bytes + s->scene_bytes + j->film_bytes <= s->hbm) {
+            it = s->queue.erase(it);
+            use_scene_locked(s, j);
+            start_job_locked(s, j);
+        } else {
+            ++it;
+        }
+    }
+}
+
 void admit_locked(ftb_server* s) {
     while (!s->queue.empty() && !s->free_slots.empty()) {
         Job* j = s->queue.front();
         if (s->hbm) {
-            if (!fit_locked(s, j)) break;
+            if (!fit_locked(s, j)) { backfill_locked(s); break; }
         } else if (s->film_bytes + j->film_bytes > s->budget) {
             break;
         }
         s->queue.pop_front();
-        j->slot = s->free_slots.back();
-        s->free_slots.pop_back();
-        cudaError_t e = cudaSuccess;
-        if (j->req.n_photons > 0 && j->error == FTB_OK) {   // an empty job needs no device film
-            void* p = nullptr;
-            e = cudaMallocFromPoolAsync(&p, j->film_bytes, s->pool, s->admit_stream);
-            if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, j->film_bytes, s->admit_stream);
-            if (e == cudaSuccess)
-                e = cudaMemsetAsync(s->d_tally + 8 * (size_t)j->slot, 0, 8 * sizeof(unsigned long long),
-                                    s->admit_stream);
-            j->d_film = (int64_t*)p;
-            s->admitted_since_launch = true;
-        }
-        j->t_admit = s->now();
-        s->film_bytes += j->film_bytes;
-        s->st.queued--;
-        s->st.active++;
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            if (j->d_film) cudaFreeAsync(j->d_film, s->admit_stream);
-            j->d_film = nullptr;
-            j->error = e == cudaErrorMemoryAllocation ? FTB_ERR_OOM : FTB_ERR_CUDA;
-        }
-        if (j->error != FTB_OK) j->next = j->req.n_photons;   // nothing to trace
-        j->state = kActive;
-        if (j->next >= j->req.n_photons) {   // empty or failed: straight to completion
-            j->state = kFinishing;
-            s->finishing.push_back(j);
-            s->cv_fin.notify_one();
-        } else {
-            s->active.push_back(j);
-        }
+        start_job_locked(s, j);
     }
     if (s->admitted_since_launch) cudaEventRecord(s->admit_ev, s->admit_stream);
+}
+
+// An admitted job: a slot, a zeroed device film and tallies (stream-ordered on the admission
+// stream), and a place among the active jobs.
+void start_job_locked(ftb_server* s, Job* j) {
+    j->slot = s->free_slots.back();
+    s->free_slots.pop_back();
+    cudaError_t e = cudaSuccess;
+    if (j->req.n_photons > 0 && j->error == FTB_OK) {   // an empty job needs no device film
+        void* p = nullptr;
+        e = cudaMallocFromPoolAsync(&p, j->film_bytes, s->pool, s->admit_stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, j->film_bytes, s->admit_stream);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(s->d_tally + 8 * (size_t)j->slot, 0, 8 * sizeof(unsigned long long),
+                                s->admit_stream);
+        j->d_film = (int64_t*)p;
+        s->admitted_since_launch = true;
+    }
+    j->t_admit = s->now();
+    s->film_bytes += j->film_bytes;
+    s->st.queued--;
+    s->st.active++;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (j->d_film) cudaFreeAsync(j->d_film, s->admit_stream);
+        j->d_film = nullptr;
+        j->error = e == cudaErrorMemoryAllocation ? FTB_ERR_OOM : FTB_ERR_CUDA;
+    }
+    if (j->error != FTB_OK) j->next = j->req.n_photons;   // nothing to trace
+    j->state = kActive;
+    if (j->next >= j->req.n_photons) {   // empty or failed: straight to completion
+        j->state = kFinishing;
+        s->finishing.push_back(j);
+        s->cv_fin.notify_one();
+    } else {
+        s->active.push_back(j);
+    }
 }
 
 // The table of the next pass (or wave).  Its jobs share one kernel class -- bundles or not,

@@ -506,7 +506,10 @@ ftb_status ftb_autotune(ftb_scene* scene, const ftb_camera* cam, int64_t n_photo
  * server evicts scenes that no admitted job uses, least recently used first, and restores a
  * job's scene on admission (ftb_scene_evict / ftb_scene_restore, stream-ordered; a scene's
  * first eviction copies its tables to host memory and waits for the device, later ones only
- * free).  Scenes that cannot leave the device (instances, clones) count as resident.  The
+ * free).  Jobs are admitted in arrival order, except that while the job at the head waits
+ * for room, later jobs whose scene is on the device and whose film fits are admitted past
+ * it, for two passes; then admission waits for the head.  Scenes that cannot leave the
+ * device (instances, clones) count as resident.  The
  * server may evict or restore any scene its jobs have used until it is destroyed, so such
  * scenes must outlive the server, and while it runs they are rendered only through it; when
  * it is destroyed, scenes stay as they are (ftb_scene_resident tells). */

@@ -73,6 +73,25 @@ def make_mirrors(L, fog=False):
     return sb.build(L)
 
 
+def make_smooth(L):
+    """Smooth shading, modelled on the reference's -checktrinormal (main.cpp:8123): diffuse
+    spheres tessellated with exact outward vertex normals (n = p - centre), one wound outward
+    and one wound inward without touching its vertex normals, so its geometric normal opposes
+    the shading normal everywhere; and a smooth glossy sphere.  Exercises the interpolated
+    normal, the oriented geometric normal and the shading-normal adjoint correction."""
+    sb = scenes.SceneBuilder()
+    scenes.cornell_box(sb, boxes=False)
+    v, f = scenes.icosphere(2)
+    tri = v[f]                              # (n, 3, 3) on the unit sphere, wound outward
+    inward = tri[:, [0, 2, 1], :]
+    for centre, r, mat, t in (((0.6, 0.4, 1.0), 0.3, sb.diffuse(sb.const(0.7)), tri),
+                              ((1.4, 0.35, 0.8), 0.25, sb.diffuse(sb.table([(400, 0.2), (600, 0.8)])), inward),
+                              ((1.0, 1.2, 0.6), 0.2, sb.material(abi.MAT_GLOSSY, reflect=sb.const(0.85),
+                                                                 roughness=0.15), tri)):
+        sb.tris((t * r + np.asarray(centre)).reshape(-1, 9), mat, normals=t.reshape(-1, 9))
+    return sb.build(L)
+
+
 CASES = {
     # name: (builder, res, photons, max_bounce, seed_base, wavelengths per photon)
     "cornell": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 0, 1),
@@ -84,6 +103,8 @@ CASES = {
     "mirrors": (make_mirrors, 32, 8192, 16, 13, 1),
     "mirrors_fog": (lambda L: make_mirrors(L, fog=True), 32, 8192, 32, 17, 1),
     "mirrors_hero4": (make_mirrors, 32, 8192, 16, 19, 4),
+    "smooth": (make_smooth, 32, 8192, 16, 23, 1),
+    "smooth_hero4": (make_smooth, 32, 8192, 16, 29, 4),
     # hero-wavelength bundles (Renderer::tracePhotonHero): C wavelengths per photon
     "cornell_hero4": (lambda L: scenes.make_cornell(L), 32, 8192, 8, 3, 4),
     "glass_hero4": (lambda L: scenes.make_glass(L, level=2), 32, 8192, 16, 5, 4),

@@ -70,7 +70,12 @@ def test_per_photon_paths_match_oracle(name, scenes_cache, gpu, oracle):
     same = (gl["n_hits"] == ol["n_hits"]) & (gl["prim_hash"] == ol["prim_hash"]) & (gl["fate"] == ol["fate"])
     allowed = max(1, int(1e-5 * n))
     assert (~same).sum() <= allowed, f"{(~same).sum()} of {n} photon paths differ; first {np.nonzero(~same)[0][:5]}"
-    np.testing.assert_allclose(gl["beta"][same], ol["beta"][same], rtol=1e-12, atol=0)
+    # Sampled directions carry last-bit differences of CUDA's sin / cos / pow against the
+    # C library's.  On flat surfaces they never reach the throughput; at a smooth-shaded
+    # diffuse vertex the shading-normal adjoint correction (a ratio of dot products with those
+    # directions) multiplies them into beta, and they compound over the bounces.
+    rtol = 1e-10 if name.startswith("smooth") else 1e-12
+    np.testing.assert_allclose(gl["beta"][same], ol["beta"][same], rtol=rtol, atol=0)
     np.testing.assert_array_equal(gl["prims"][same], ol["prims"][same])
 
 

@@ -71,7 +71,7 @@ def test_trace_matches_golden(name, oracle, L):
 
 
 @pytest.mark.parametrize("name,hero", [("cornell", 1), ("materials", 1), ("fog_strands", 1), ("materials", 4),
-                                       ("instances", 8), ("fog_strands", 4)])
+                                       ("instances", 8), ("fog_strands", 4), ("smooth", 1)])
 def test_trace_matches_reference_live(name, hero, oracle, reference, L):
     mk, res, n, mb, _, _ = cases.CASES[name]
     d = mk(L)
